@@ -1,0 +1,393 @@
+#!/usr/bin/env python3
+"""Benchmark: the full DDGI probe update on the Sponza-scale atrium.
+
+Workload (one "step" = one full update of every probe): the seeded
+262,267-triangle atrium (30 meshes, 25 materials, 1 directional + 32 clustered
+point lights), 16^3 = 4,096 probes x 64 rays = 262,144 primary rays, with the
+per-frame motion lanes: 1 deforming mesh (sinusoidal 2 cm vertex offset: BLAS
+refit) and 3 rigidly moving meshes (instance rows + TLAS refit).
+
+  value  probe Mrays/s (primary rays / device time of a step: refit -> TLAS
+         refit -> trace + shade -> blend + upload), inputs resident in HBM;
+         L2 flushed (256 MiB write) before every timed step.
+  e2e    the same metric through the public facade (markDeformsDirty,
+         markTransformsDirty, update, atlas read-back) with the step's vertex
+         and matrix uploads from page-locked host memory and both RGBA16F
+         atlases read back, wall-clock per step.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+FP32 CPU restatement of the path, all host threads) on the same workload.
+With --gpus N > 1 (torchrun), every rank runs an independent replica.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "probe Mrays/s (full DDGI update)"
+UNIT = "Mrays/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, n):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.barrier()
+            self.pg.destroy_process_group()
+
+
+# ------------------------------------------------------------------ workload
+def make_workload():
+    from speedball_b200 import synth
+    scene = synth.atrium(1)
+    return scene
+
+
+def field_for(scene, device):
+    from speedball_b200.field import ProbeField
+    g = scene.meta["grid"]
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
+    f.setHysteresisNormalization(False)
+    f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)  # one solve updates all 4,096 probes
+    return f
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("SB_CLOCKS_CSV", "/tmp/sb_clocks_%d.csv" % os.getpid()))
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cudart():
+    from cuda import cudart as rt  # cuda-python: streams, events, L2 flush buffer
+    return rt
+
+
+def ck(res):
+    err = res[0] if isinstance(res, tuple) else res
+    if int(err) != 0:
+        raise RuntimeError(f"CUDA runtime error {err}")
+    return res[1] if isinstance(res, tuple) and len(res) > 1 else None
+
+
+# --------------------------------------------------------------- our arm
+def run_ours(args, dist: Dist):
+    from speedball_b200 import _abi
+    from speedball_b200 import synth
+    from speedball_b200.scene import column_major
+
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    scene = make_workload()
+    f = field_for(scene, device)
+    lib, ctx, pool = f._lib, f.ctx, f.pool
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
+    flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
+    P = f._probeTotal
+    rays = P * f.getRays()
+    dm = scene.meta["deformer"]
+    movers = scene.meta["movers"]
+    root, end = int(pool.blas_root[dm]), int(pool.blas_end[dm])
+    W, K = args.warmup, args.steps
+    e0 = ck(rt.cudaEventCreate())
+    e1 = ck(rt.cudaEventCreate())
+
+    def flush_l2(i):
+        ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+
+    def device_step():
+        _abi.check(lib.sb_refit_blas(ctx, root, end), ctx)
+        _abi.check(lib.sb_update_transforms(ctx, None, None, 0), ctx)
+        f.tick()
+
+    # ---- counted run (untimed): traversal work of one step for the roofline
+    _abi.check(lib.sb_enable_counters(ctx, 1), ctx)
+    device_step()
+    f.synchronize()
+    st = _abi.sb_stats()
+    _abi.check(lib.sb_get_stats(ctx, C.byref(st)), ctx)
+    ray_data = np.zeros(rays * 4, np.float32)
+    _abi.check(lib.sb_read_buffer(ctx, _abi.BUF["RAY_DATA"], 0, rays * 4, _abi.ptr(ray_data)), ctx)
+    hits = int((ray_data[3::4] >= 0).sum())
+    _abi.check(lib.sb_enable_counters(ctx, 0), ctx)
+    counted = dict(primary=st.primaryRays, shadow=st.shadowRays, tlas=st.tlasNodeVisits, inst=st.instanceVisits,
+                   blas=st.blasNodeVisits, tri=st.triangleTests, hits=hits)
+    # algorithmic bytes of one trace launch (per-unit figures: 32 B TLAS node, 64 B instance record,
+    # 32 B BLAS node, 48 B triangle, 16 B ray record write, 40 B material + 256 B bounce taps per hit)
+    trace_bytes = (32 * counted["tlas"] + 64 * counted["inst"] + 32 * counted["blas"] + 48 * counted["tri"]
+                   + 16 * rays + 296 * hits)
+
+    # ---- device-resident timed loop
+    for i in range(W):
+        device_step()
+        flush_l2(i)
+    f.synchronize()
+    dist.barrier()
+    clocks = Clocks(device)
+    clocks.start()
+    launches0 = _stats(lib, ctx).kernelLaunches
+    total_ms, trace_ms = 0.0, []
+    for i in range(K):
+        flush_l2(i)
+        ck(rt.cudaEventRecord(e0, stream))
+        device_step()
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        total_ms += ck(rt.cudaEventElapsedTime(e0, e1))
+        s = _stats(lib, ctx)
+        trace_ms.append(s.lastTraceMs)
+    launches = _stats(lib, ctx).kernelLaunches - launches0
+    clk = clocks.stop()
+    f.synchronize()
+    ms_step = dist.max(total_ms / K)
+    value = dist.world * rays / (ms_step * 1e-3) / 1e6
+
+    # ---- e2e through the public facade (pinned host buffers)
+    frames = [synth.atrium_motion(scene, fr) for fr in range(W + K)]
+    r = f.getResolution()
+    atl = _abi.PinnedArray((r[1] * r[2] * 8, r[0] * 8, 4), np.uint16)
+    datl = _abi.PinnedArray((r[1] * r[2] * 8, r[0] * 8, 4), np.uint16)
+    base_pos = scene.meshes[dm].positions
+
+    def e2e_step(fr):
+        mats, pos = frames[fr]
+        scene.meshes[dm].positions = pos
+        for i, m in mats.items():
+            scene.instances[i].world = m
+        f.markDeformsDirty()
+        f.markTransformsDirty(list(mats))
+        f.tick()
+        f._debugRead("atlas", out=atl.array)
+        f._debugRead("depthAtlas", out=datl.array)
+
+    for i in range(W):
+        e2e_step(i)
+        flush_l2(i)
+    f.synchronize()
+    dist.barrier()
+    e2e_total = 0.0
+    for i in range(K):
+        flush_l2(i)
+        ck(rt.cudaStreamSynchronize(stream))
+        t0 = time.perf_counter()
+        e2e_step(W + i)
+        e2e_total += time.perf_counter() - t0
+    e2e_ms = dist.max(e2e_total / K * 1e3)
+    e2e_value = dist.world * rays / (e2e_ms * 1e-3) / 1e6
+    h2d = base_pos.shape[0] * 32 + len(movers) * (16 * 8 + 4)
+    d2h = atl.array.nbytes + datl.array.nbytes
+    scene.meshes[dm].positions = base_pos
+
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    trace_avg = sum(trace_ms) / len(trace_ms)
+    achieved = trace_bytes / (trace_avg * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "trace_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded procedural atrium standing in for Sponza)",
+        "config": {"workload": "atrium 262,267 tris / 30 meshes, 16^3 probes x 64 rays, 32 clustered point + 1 "
+                               "directional light, 1 deforming + 3 moving meshes per frame",
+                   "probes": P, "rays_per_probe": f.getRays(), "primary_rays_per_step": rays,
+                   "triangles": int(pool.triIndex.shape[0]), "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if dist.world > 1 else "single GPU"},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e_ms, 4),
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "k_trace_shade", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_launch": int(trace_bytes), "trace_ms": round(trace_avg, 4),
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s"},
+        "work": {k: int(v) for k, v in counted.items()},
+        "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene, target_s=12.0)
+    f.dispose()
+    ck(rt.cudaFree(flush))
+    return line
+
+
+def _stats(lib, ctx):
+    from speedball_b200 import _abi
+    st = _abi.sb_stats()
+    _abi.check(lib.sb_get_stats(ctx, C.byref(st)), ctx)
+    return st
+
+
+# ----------------------------------------------------- CPU (reference arm)
+def _cpu_setup(scene):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import orc
+    from speedball_b200 import scene as sc
+    from speedball_b200.field import selectGiLightRecords
+    pool = sc.build_pool(scene)
+    mats, order, live, aabb = orc.compute_tail(pool)
+    keep = []
+    S = orc.scene_struct(pool, mats, keep=keep)
+    g = dict(scene.meta["grid"])
+    gs = np.asarray(g["gridSize"], np.float32)
+    g["maxDist"] = float(np.linalg.norm(gs.astype(np.float64)))
+    res = g["res"]
+    g["cellMin"] = float(max(1e-4, min(gs[a] / max(1, res[a] - 1) for a in range(3))))
+    recs, _, _ = selectGiLightRecords(scene.lights, True, g["gridMin"], [g["gridMin"][a] + g["gridSize"][a] for a in range(3)])
+    arena = orc.light_arena(recs, True, g)
+    from speedball_b200 import _abi
+    p = _abi.default_params()
+    p.hysteresis = scene.meta["hysteresis"]
+    return orc, S, keep, g, orc.grid_struct(g), arena, recs.shape[0], p.to_array()
+
+
+def cpu_solve_rate(scene, probes: int, reps: int = 1):
+    orc, S, keep, g, G, arena, nl, prm = _cpu_setup(scene)
+    irr, depth, atlas, datlas = orc.new_state(g, fp32=True)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.solve(S, arena, nl, True, G, G, prm, 0, probes, irr, depth, atlas, datlas, fp32=True)
+    dt = time.perf_counter() - t0
+    return probes * g["rays"] * reps / dt / 1e6, dt
+
+
+def cpu_baseline(scene, target_s=12.0):
+    threads = os.cpu_count() or 1
+    rate, dt = cpu_solve_rate(scene, 64)
+    probes = int(min(4096, max(64, 64 * target_s / max(dt, 1e-3))))
+    rate, dt = cpu_solve_rate(scene, probes)
+    return {"value": round(rate, 4), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{probes} of 4096 probes x 64 rays of the atrium step (FP32 CPU restatement, "
+                      f"{threads} threads), {dt:.1f} s"}
+
+
+def run_reference(args, dist: Dist):
+    if dist.rank != 0:
+        return None
+    scene = make_workload()
+    threads = os.cpu_count() or 1
+    rate, dt = cpu_solve_rate(scene, 64)
+    probes = int(min(4096, max(64, 64 * 4.0 / max(dt, 1e-3))))  # ~4 s per step
+    for _ in range(args.warmup if args.warmup < 2 else 1):
+        cpu_solve_rate(scene, probes)
+    total, rays = 0.0, 0
+    for _ in range(args.steps if args.steps <= 3 else 3):
+        r, d = cpu_solve_rate(scene, probes)
+        total += d
+        rays += probes * 64
+    value = rays / total / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(4096 * 64 / (value * 1e6) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural atrium)",
+            "config": {"workload": "atrium 262,267 tris, 16^3 probes x 64 rays (per-step sample of "
+                                   f"{probes} probes)"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{probes} probes x 64 rays per step, FP32 CPU restatement of the reference "
+                                       f"path on {threads} threads (the reference itself is WebGPU/JS: no runtime here)"},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    try:
+        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if dist.rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,303 @@
+/*
+ * speedball_cuda.h — C ABI of the B200-native DDGI probe update.
+ *
+ * One context (sb_ctx) is one probe field over one resident scene on one GPU.
+ * The host (the reference's JavaScript facade through an N-API addon, or the
+ * Python mirror in speedball_b200/) keeps the scene build and the per-tick
+ * scheduling; everything the reference submits through renderer.computeAsync
+ * (gi_probes.js:3236, 3812, 3836) and the CPU refit / TLAS lanes
+ * (gi_refit.js, spectral_scene.js:973-1003, 1402-1514, 1831-1927) run here
+ * as CUDA kernels for sm_100a.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only. Host arrays are owned by the caller and
+ *    copied; device memory is owned by the library.
+ *  - Every call returns sb_status. No exception or abort crosses the ABI.
+ *    sb_last_error() returns a message for the last non-OK status.
+ *  - Work is enqueued on the context's stream (sb_set_stream). Calls that
+ *    enqueue device work do not block; device-side faults found by the
+ *    kernels' own checks (layout violations, traversal watchdogs) are latched
+ *    in a device error word and returned by the next sb_synchronize().
+ *  - A context is not thread-safe: one host thread per context, mirroring the
+ *    reference's single-threaded tick with its inFlight guard
+ *    (gi_probes.js:3141, 3473).
+ *  - Buffers use the reference's wire layouts (spectral_scene.js:35-55,
+ *    724-733, 1188-1240, 1339-1366); the library derives its own B200
+ *    layouts (pre-gathered triangles, compact TLAS, instance rows) on device.
+ */
+#ifndef SPEEDBALL_CUDA_H
+#define SPEEDBALL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_ABI_VERSION 1u
+
+/* Geometry of the reference's layouts (spectral_scene.js:35-55, gi_probes.js:53-56). */
+#define SB_NODE_STRIDE_U32 8u   /* bvhNodes: 6 f32 bounds + miss + payload        */
+#define SB_MAT_STRIDE 28u       /* materials / instance records (floats)           */
+#define SB_TLAS_STRIDE_F32 12u  /* TLAS nodes in the materials tail (floats)       */
+#define SB_LIGHT_STRIDE 17u     /* light records (floats)                          */
+#define SB_VERTEX_STRIDE 8u     /* vertexData: pos(3) normal(3) uv(2)              */
+#define SB_OCT_RES 6u           /* interior octahedral texels per axis             */
+#define SB_TILE 8u              /* tile incl. 1-texel gutter                       */
+#define SB_MAX_LIGHTS 64u       /* gi_probes.js:132                                */
+#define SB_LIGHTS_PER_CELL 16u  /* gi_probes.js:135                                */
+#define SB_MAX_CASCADES 4u
+
+typedef enum sb_status {
+    SB_OK = 0,
+    SB_ERR_INVALID_ARG = 1,        /* bad pointer, size or range                     */
+    SB_ERR_LAYOUT_VIOLATION = 2,   /* threaded-layout invariant broken: the caller
+                                      must fall back to a full rebuild, as the
+                                      reference does when refit returns false
+                                      (gi_refit.js:30-33, gi_probes.js:4170, 4220) */
+    SB_ERR_OOM = 3,
+    SB_ERR_CUDA = 4,
+    SB_ERR_DEVICE_WATCHDOG = 5,    /* a bounded device loop hit its iteration cap    */
+    SB_ERR_UNSUPPORTED = 6,        /* a feature outside this library's scope         */
+    SB_ERR_NO_DEVICE = 7,
+    SB_ERR_NOT_READY = 8           /* call order: e.g. solve before scene upload     */
+} sb_status;
+
+typedef struct sb_ctx sb_ctx;
+
+/* ---------------------------------------------------------------- lifetime */
+
+typedef struct sb_device_opts {
+    int32_t device;        /* CUDA ordinal                                         */
+    uint32_t flags;        /* SB_CTX_* below                                       */
+} sb_device_opts;
+
+#define SB_CTX_RECORD_HITS 1u  /* keep 16-byte hit records + visibility masks of the
+                                  last solve (needed by sb_backward and replay)     */
+
+/* createProbeField (gi_probes.js:945) minus the renderer: allocates the context. */
+sb_status sb_create(const sb_device_opts* opts, sb_ctx** out);
+/* dispose() (install.js:488-502): frees every device allocation. NULL is a no-op. */
+void sb_destroy(sb_ctx* ctx);
+const char* sb_last_error(const sb_ctx* ctx);
+uint32_t sb_abi_version(void);
+/* Attach a caller stream (a cudaStream_t passed as void*); NULL = library stream. */
+sb_status sb_set_stream(sb_ctx* ctx, void* cuda_stream);
+/* Wait for the context's stream and return the latched device error, if any. */
+sb_status sb_synchronize(sb_ctx* ctx);
+/* Page-locked host staging memory for the per-frame uploads (vertex gathers,
+ * matrices) and read-backs, so copies run at full PCIe / C2C rate. The JS addon
+ * wraps such blocks as external ArrayBuffers. */
+sb_status sb_host_alloc(size_t bytes, void** out);
+void sb_host_free(void* p);
+
+/* ------------------------------------------------------------------ scene */
+
+/* The typed arrays buildSpectralScene returns (spectral_scene.js:2011-2033).
+ * materials = [uberCount*28 | instCount*28 instance records | tlasNodeCount*12]. */
+typedef struct sb_scene_view {
+    const uint32_t* bvhNodes;   uint32_t nodeCount;
+    const uint32_t* triIndex;   uint32_t triCount;
+    const float* vertexData;    uint32_t vertexCount;
+    const uint32_t* triMaterial;
+    const float* materials;     uint32_t materialsLen;   /* floats */
+    uint32_t materialCount;     /* uber records                                  */
+    uint32_t instBase;          /* float index of instance 0 (= materialCount*28) */
+    uint32_t instCount;
+    uint32_t tlasBase;          /* float index of TLAS node 0                    */
+    uint32_t tlasNodeCount;
+} sb_scene_view;
+
+sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* scene);
+
+typedef enum sb_buffer {
+    SB_BUF_BVH_NODES = 0,    /* u32 units            */
+    SB_BUF_TRI_INDEX = 1,    /* u32 units            */
+    SB_BUF_VERTEX_DATA = 2,  /* f32 units            */
+    SB_BUF_TRI_MATERIAL = 3, /* u32 units            */
+    SB_BUF_MATERIALS = 4,    /* f32 units (incl. instance + TLAS tail) */
+    SB_BUF_LIGHTS = 5,       /* f32 units            */
+    SB_BUF_IRRADIANCE_HISTORY = 6, /* f32, 4 per texel, probeTotal*64 texels (per cascade) */
+    SB_BUF_DEPTH_HISTORY = 7,      /* f32, 2 per texel                                   */
+    SB_BUF_IRRADIANCE_ATLAS = 8,   /* u16 binary16 RGBA, atlasW*atlasH*4                 */
+    SB_BUF_DEPTH_ATLAS = 9,        /* u16 binary16 RGBA                                  */
+    SB_BUF_RAY_DATA = 10,          /* f32, 4 per ray: rgb + hitT (-1 = miss)             */
+    SB_BUF_HIT_RECORDS = 11,       /* u32, 4 per ray: tri, inst, t bits, packed uv        */
+    SB_BUF_VISIBILITY = 12,        /* u32, 2 per ray: NEE shadow bits, lights 0..63      */
+    SB_BUF_TLAS_ORDER = 13,        /* u32, slot -> source instance                       */
+    SB_BUF_INSTANCE_BOUNDS = 14    /* f32, 6 per slot (liveInstanceBounds)               */
+} sb_buffer;
+
+/* Ranged host->device write into a reference buffer (the copySceneStorageRanges /
+ * markStorageDirty seam, gi_probes.js:1543-1561, 4239-4251). Derived layouts are
+ * refreshed before the next solve. For history buffers `cascade` selects the
+ * cascade through the high byte of `which` (which | cascade << 8). */
+sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count,
+                          const void* src);
+/* Device->host read of any buffer above (the _debugRead seam, gi_probes.js:4830-4841).
+ * Synchronous: waits for the stream. */
+sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count,
+                         void* dst);
+
+/* ------------------------------------------------------------------ lights */
+
+/* Light records of stride 17 (collectLights, spectral_scene.js:724-813), already
+ * selected into the fixed arena by the host (fillLegacyLightArena /
+ * fillGiLightArena, gi_probes.js:4297-4349). clustered != 0 builds the C0 cell
+ * lists on device (lightGridKernel, gi_probes.js:1888-1938) from cascade 0's grid. */
+sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count,
+                           uint32_t emitterBase, uint32_t emitterCount, int32_t clustered);
+
+/* ----------------------------------------------------------- probe field */
+
+/* Per-cascade uniforms (makeCascadeU, gi_probes.js:1010-1024; rebuild 3341-3367). */
+typedef struct sb_grid {
+    float gridMin[3];
+    float gridSize[3];
+    uint32_t res[3];          /* probes per axis, 2..32                            */
+    uint32_t raysPerProbe;    /* 32..256, multiple of 16 (gi_probes.js:988-992)    */
+    float maxDist;            /* |gridSize| (gi_probes.js:3151)                    */
+    float cellMin;            /* max(1e-4, min cell edge) (gi_probes.js:3364)      */
+} sb_grid;
+
+/* Shared compute uniforms U (gi_probes.js:1198-1255). */
+typedef struct sb_params {
+    float frameJitter, emitterVisSeed;
+    float hysteresis, hysteresisExponent;
+    float depthSharpness, radianceClamp, classifyStrength;
+    float filterStrength, filterSmooth;
+    float tempChangeSigma1, tempChangeHDrop, tempClampSigma;
+    float nirGate, nirGain;
+    float skyIntensity;
+    float skySH[27];          /* 9 coefficients x RGB, THREE.SphericalHarmonics3 order */
+    float debugTraceBiasScale, debugRayEpsScale, debugDirectScale, debugEmissiveScale;
+    float debugAlbedoScale, debugBounceScale, debugCosinePower;
+    float debugTempNoiseHBoost, debugTempChangeSigma0, debugTempMinChangeH;
+    float debugTempVarEps, debugTempVarRel, debugDepthHistoryScale;
+    float debugFilterKScale, debugFilterRelScale, debugFilterEpsScale;
+} sb_params;
+
+/* The reference's defaults (hysteresis = gated 0.60, gi_probes.js:146-149). */
+void sb_params_defaults(sb_params* p);
+
+/* (Re)configure a cascade: allocates ray scratch, histories and both RGBA16F
+ * atlases, cleared (clearAtlasKernel, gi_probes.js:2690-2707). A same-dimension
+ * reconfigure keeps the live history, as the reference's `reuse` does
+ * (gi_probes.js:3124-3197). */
+sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t cascade, const sb_grid* grid);
+sb_status sb_set_params(sb_ctx* ctx, const sb_params* params);
+
+/* One solve of one cascade: trace -> NEE/bounce shade -> blend -> upload for
+ * probes (probeOffset + slot) mod probeTotal, slot < updatedCount (the
+ * solveKernels pass, gi_probes.js:3815-3836). Enqueue only. */
+sb_status sb_solve(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount);
+
+/* The batched form: solves of several contexts (scenes) and cascades in ONE
+ * persistent trace launch over a shared ray queue, then one blend/upload launch.
+ * All contexts must live on the same device; work runs on ctxs[0]'s stream. */
+typedef struct sb_solve_item {
+    sb_ctx* ctx;
+    uint32_t cascade, probeOffset, updatedCount;
+} sb_solve_item;
+sb_status sb_solve_batch(const sb_solve_item* items, uint32_t count);
+
+/* Arbitrary-ray queries through the same two-level traversal (the reference's
+ * traverseClosest / traverseAny, spectral_traverse.js:441-474, 539-569), host
+ * arrays in and out; synchronous. ro/rd: 3 floats per ray. tri = -1 on a miss. */
+sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, float* tOut,
+                     int32_t* triOut, int32_t* instOut);
+sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist,
+                      uint32_t n, uint8_t* blockedOut);
+
+/* ------------------------------------------------- refit / TLAS lanes (GPU) */
+
+/* BLAS refit over node range [root, end) from the current vertexData
+ * (refitFlatBlasRange, gi_refit.js:34-165): exact min/max, bit-identical to the
+ * reference's CPU walk. Layout violations latch SB_ERR_LAYOUT_VIOLATION. */
+sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end);
+
+/* Deform lane for one BLAS (updateDeforms, spectral_scene.js:1831-1927): writes
+ * vertexCount pooled vertices (8 floats each) from vertexStart, then refits the
+ * BLAS [root, end) and re-gathers its triangles. The vertices must be the
+ * BLAS's own pooled slice. Follow with sb_update_transforms(ctx, NULL, NULL, 0)
+ * to carry the new root bounds into the TLAS, as the reference does. */
+sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCount,
+                           const float* vertexData, uint32_t root, uint32_t end);
+
+/* Per-source-instance transform table (computeDynamic inputs,
+ * spectral_scene.js:1256-1298): column-major 4x4 world matrices in FP64
+ * (three's Matrix4.elements), the active flag and the BLAS node range. */
+sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16,
+                           const uint8_t* active, const uint32_t* blasRoot,
+                           const uint32_t* blasEnd);
+/* TLAS build on device (buildTlasRecords, spectral_scene.js:973-1003, and
+ * writeDynamic 1339-1366): FP64 instance AABBs, longest-axis median split with a
+ * stable FP64-centroid order; writes instance records in slot order, the TLAS
+ * tail and liveInstanceBounds. Order and bounds are bit-exact. */
+sb_status sb_build_tlas(sb_ctx* ctx);
+/* Transform lane (updateTransforms, spectral_scene.js:1402-1514): new world
+ * matrices for `count` source instances; rewrites their instance rows and
+ * bounds, then refits the frozen TLAS exactly (refitFlatTlasRange /
+ * refitFlatTlasDirty, gi_refit.js:245-430). count == 0 with src == NULL re-derives
+ * every slot's bounds from the current BLAS roots (rewriteInstanceRows:false). */
+sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* srcInstances, const double* world16,
+                               uint32_t count);
+
+/* ------------------------------------------------------ differentiation */
+
+/* Adjoint of shade+blend+upload with hit records and visibility held fixed.
+ * Parameters: per-material albedo RGB and emissive RGB, per-light intensity. */
+typedef struct sb_grads {
+    float* dAlbedo;      /* materialCount*3 */
+    float* dEmissive;    /* materialCount*3 */
+    float* dIntensity;   /* lightCount      */
+} sb_grads;
+
+/* Differentiable forward: `solves` feedback solves of one cascade from a cleared
+ * history with fixed hit records; stores the per-solve tape on device and returns
+ * the loss sum_texels (E - target)^2 over the interior irradiance texels of the
+ * last solve when target != NULL (f32 RGB per interior texel, probe-major). */
+sb_status sb_forward_record(sb_ctx* ctx, uint32_t cascade, uint32_t solves,
+                            const float* target, double* loss);
+/* Reverse pass of the last sb_forward_record: fills the gradients (host pointers). */
+sb_status sb_backward(sb_ctx* ctx, sb_grads* grads);
+
+/* -------------------------------------------------- graphs and autotuning */
+
+/* Capture the per-frame chain (refit -> TLAS refit -> solve) of this context as
+ * one CUDA graph and replay it; sb_graph_launch re-runs the captured frame. */
+sb_status sb_graph_capture_frame(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset,
+                                 uint32_t updatedCount, const uint32_t* refitRoots,
+                                 const uint32_t* refitEnds, uint32_t refitCount,
+                                 int32_t refitTlas);
+sb_status sb_graph_launch(sb_ctx* ctx);
+
+typedef struct sb_tuning {
+    uint32_t traceBlock;      /* threads per block of the trace kernels            */
+    uint32_t sortKey;         /* 0 = probe order, 1 = direction-octant ray order   */
+    uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
+    uint32_t bvhKind;         /* 0 = reference threaded FP32 nodes, 1 = wide8 q8   */
+} sb_tuning;
+sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
+sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);
+/* Time candidate tunings on the current scene and cascade; keeps the fastest. */
+sb_status sb_autotune(sb_ctx* ctx, uint32_t cascade, sb_tuning* chosen);
+
+/* Device-side counters of the last solve (rays, shadow rays, node/tri visits). */
+typedef struct sb_stats {
+    uint64_t primaryRays, shadowRays;
+    uint64_t tlasNodeVisits, instanceVisits, blasNodeVisits, triangleTests;
+    float lastSolveMs;        /* trace + blend/upload of the last sb_solve (device time) */
+    float lastTraceMs;        /* trace + shade kernel alone                               */
+    float lastBlendMs;        /* blend + upload kernel alone                              */
+    uint64_t kernelLaunches;  /* kernels this library launched, process-wide              */
+} sb_stats;
+sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
+/* Counting costs a few percent; off by default. */
+sb_status sb_enable_counters(sb_ctx* ctx, int32_t on);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPEEDBALL_CUDA_H */

@@ -1,0 +1,260 @@
+// orc_api.cpp — extern "C" surface of the oracle for the tests (ctypes) and
+// bench.py's CPU baseline. TEST INFRASTRUCTURE ONLY (see orc_core.hpp).
+#include "orc_probes.hpp"
+#include "orc_scene.hpp"
+
+#include <atomic>
+#include <thread>
+
+using namespace orc;
+
+
+struct OrcScene {
+    const uint32_t* nodes; uint32_t nodeCount;
+    const uint32_t* triIndex; uint32_t triCount;
+    const float* vertexData; uint32_t vertexCount;
+    const uint32_t* triMaterial;
+    const float* materials; uint32_t materialsLen;
+    uint32_t instBase, instCount, tlasBase, tlasNodeCount;
+};
+struct OrcLights { const float* data; uint32_t dataLen; uint32_t lightCount; int32_t clustered; };
+struct OrcGrid { double gridMin[3], gridSize[3]; uint32_t res[3]; uint32_t rays; double maxDist, cellMin; };
+
+// Optional per-ray outputs / replay inputs of a solve. Any pointer may be null.
+struct OrcSolveIO {
+    void* rayOut;             // R[updated*rays*4]: rgb + hitT
+    int32_t* hitTri; int32_t* hitInst;
+    void* secondT;            // R per ray
+    uint64_t* tested; uint64_t* blocked;
+    const int32_t* replayTri; const int32_t* replayInst; const uint64_t* replayBlocked;
+    const void* rayIn;        // R rays to blend instead of tracing (replay of the blend alone)
+    void* preRound;           // R[probeTotal*36*3]: unrounded upload RGB
+    uint64_t* counters;       // [tlasNodes, instances, blasNodes, triTests] (primary + shadow)
+};
+
+
+static Scene to_scene(const OrcScene* s) {
+    Scene sc;
+    sc.nodes = s->nodes; sc.nodeCount = s->nodeCount; sc.triIndex = s->triIndex; sc.triCount = s->triCount;
+    sc.vertexData = s->vertexData; sc.vertexCount = s->vertexCount; sc.triMaterial = s->triMaterial;
+    sc.materials = s->materials; sc.materialsLen = s->materialsLen; sc.instBase = s->instBase;
+    sc.instCount = s->instCount; sc.tlasBase = s->tlasBase; sc.tlasNodeCount = s->tlasNodeCount;
+    return sc;
+}
+static Grid to_grid(const OrcGrid* g) {
+    Grid o;
+    for (int i = 0; i < 3; ++i) { o.gridMin[i] = g->gridMin[i]; o.gridSize[i] = g->gridSize[i]; o.res[i] = g->res[i]; }
+    o.rays = g->rays; o.maxDist = g->maxDist; o.cellMin = g->cellMin;
+    return o;
+}
+
+template <class F> static void parallel_for(size_t n, int threads, F&& f) {
+    if (threads <= 1 || n < 64) { for (size_t i = 0; i < n; ++i) f(i, 0); return; }
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> ts;
+    const size_t chunk = 64;
+    for (int t = 0; t < threads; ++t)
+        ts.emplace_back([&, t] {
+            for (;;) {
+                size_t b = next.fetch_add(chunk);
+                if (b >= n) break;
+                size_t e = std::min(n, b + chunk);
+                for (size_t i = b; i < e; ++i) f(i, t);
+            }
+        });
+    for (auto& th : ts) th.join();
+}
+
+extern "C" {
+
+int orc_version(void) { return 1; }
+
+// -------------------------------------------------------------- traversal
+void orc_closest(const OrcScene* s, const float* ro, const float* rd, uint32_t n, int32_t track2, int32_t brute,
+                 double* tOut, int32_t* triOut, int32_t* instOut, double* secondOut, int32_t threads) {
+    Scene sc = to_scene(s);
+    parallel_for(n, threads, [&](size_t i, int) {
+        Traverser<double> tr(sc);
+        tr.track2 = track2 != 0;
+        V3<double> o(ro[i * 3], ro[i * 3 + 1], ro[i * 3 + 2]), d(rd[i * 3], rd[i * 3 + 1], rd[i * 3 + 2]);
+        double t, t2 = T_MAX;
+        int tri, inst;
+        if (brute) tr.brute_closest(o, d, t, tri, inst);
+        else tr.closest(o, d, t, tri, inst, t2);
+        tOut[i] = t; triOut[i] = tri; instOut[i] = inst;
+        if (secondOut) secondOut[i] = t2;
+    });
+}
+
+void orc_any(const OrcScene* s, const float* ro, const float* rd, const float* maxDist, uint32_t n, uint8_t* blocked,
+             int32_t threads) {
+    Scene sc = to_scene(s);
+    parallel_for(n, threads, [&](size_t i, int) {
+        Traverser<double> tr(sc);
+        V3<double> o(ro[i * 3], ro[i * 3 + 1], ro[i * 3 + 2]), d(rd[i * 3], rd[i * 3 + 1], rd[i * 3 + 2]);
+        blocked[i] = tr.any(o, d, (double)maxDist[i]) ? 1 : 0;
+    });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ solve
+template <class R>
+static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, const OrcGrid* g0p, const double* params,
+                      uint32_t probeOffset, uint32_t updated, R* irr, R* depth, uint16_t* atlas, uint16_t* depthAtlas,
+                      OrcSolveIO* io, int32_t threads) {
+    Scene sc = to_scene(s);
+    Grid g = to_grid(gp), g0 = to_grid(g0p ? g0p : gp);
+    Params P;
+    std::memcpy(&P, params, sizeof(Params));
+    Lights L;
+    L.data = l->data; L.dataLen = l->dataLen; L.lightCount = l->lightCount; L.clustered = l->clustered;
+    const uint32_t N = g.rays, total = g.probeTotal();
+    if (updated > total) updated = total;
+    const size_t nr = (size_t)updated * N;
+    std::vector<R> rays;
+    const R* rayBuf;
+    Replay rp{nullptr, nullptr, nullptr};
+    if (io && io->replayTri) { rp.tri = io->replayTri; rp.inst = io->replayInst; rp.blocked = io->replayBlocked; }
+    if (io && io->rayIn) {
+        rayBuf = static_cast<const R*>(io->rayIn);
+    } else {
+        rays.assign(nr * 4, R(0));
+        int nt = std::max(1, threads);
+        std::vector<Counters> cnts(nt);
+        parallel_for(nr, nt, [&](size_t i, int t) {
+            Tracer<R> tc(sc, L, g, g0, P, atlas);
+            if (io && io->counters) tc.tr.cnt = &cnts[t];
+            RayOut<R> o;
+            uint32_t slot = (uint32_t)(i / N), k = (uint32_t)(i % N);
+            tc.trace(slot, k, probeOffset, o, rp.tri ? &rp : nullptr, i);
+            rays[i * 4] = o.rgb[0]; rays[i * 4 + 1] = o.rgb[1]; rays[i * 4 + 2] = o.rgb[2]; rays[i * 4 + 3] = o.hitT;
+            if (io) {
+                if (io->hitTri) io->hitTri[i] = o.tri;
+                if (io->hitInst) io->hitInst[i] = o.inst;
+                if (io->secondT) static_cast<R*>(io->secondT)[i] = o.secondT;
+                if (io->tested) io->tested[i] = o.tested;
+                if (io->blocked) io->blocked[i] = o.blocked;
+            }
+        });
+        if (io && io->counters) {
+            Counters c;
+            for (auto& x : cnts) c.add(x);
+            io->counters[0] = c.tlasNodes; io->counters[1] = c.instances; io->counters[2] = c.blasNodes; io->counters[3] = c.triTests;
+        }
+        rayBuf = rays.data();
+        if (io && io->rayOut) std::memcpy(io->rayOut, rays.data(), nr * 4 * sizeof(R));
+    }
+    R* pre = io ? static_cast<R*>(io->preRound) : nullptr;
+    parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
+        uint32_t p = (uint32_t)((probeOffset + slot) % total);
+        blend_probe<R>(g, P, rayBuf + slot * N * 4, p, irr, depth);
+    });
+    // the upload runs after every blend of the solve (separate kernel)
+    parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
+        uint32_t p = (uint32_t)((probeOffset + slot) % total);
+        upload_probe<R>(g, P, p, irr, depth, atlas, depthAtlas, pre);
+    });
+    return 0;
+}
+
+extern "C" {
+
+int orc_solve_f64(const OrcScene* s, const OrcLights* l, const OrcGrid* g, const OrcGrid* g0, const double* params,
+                  uint32_t probeOffset, uint32_t updated, double* irr, double* depth, uint16_t* atlas,
+                  uint16_t* depthAtlas, OrcSolveIO* io, int32_t threads) {
+    return solve_impl<double>(s, l, g, g0, params, probeOffset, updated, irr, depth, atlas, depthAtlas, io, threads);
+}
+int orc_solve_f32(const OrcScene* s, const OrcLights* l, const OrcGrid* g, const OrcGrid* g0, const double* params,
+                  uint32_t probeOffset, uint32_t updated, float* irr, float* depth, uint16_t* atlas,
+                  uint16_t* depthAtlas, OrcSolveIO* io, int32_t threads) {
+    return solve_impl<float>(s, l, g, g0, params, probeOffset, updated, irr, depth, atlas, depthAtlas, io, threads);
+}
+
+uint32_t orc_params_size(void) { return (uint32_t)(sizeof(Params) / sizeof(double)); }
+
+// ------------------------------------------------------------ light grid
+void orc_light_grid(const OrcGrid* g0, const float* lights, uint32_t lightCount, float* out, int32_t fp32) {
+    Grid g = to_grid(g0);
+    if (fp32) light_grid<float>(g, lights, lightCount, out);
+    else light_grid<double>(g, lights, lightCount, out);
+}
+
+// ------------------------------------------------------------ small KATs
+void orc_oct_encode(const double* n, double* uv) { oct_encode(V3<double>(n[0], n[1], n[2]), uv[0], uv[1]); }
+void orc_oct_decode(const double* uv, double* n) {
+    V3<double> d = oct_decode(uv[0], uv[1]);
+    n[0] = d.x; n[1] = d.y; n[2] = d.z;
+}
+uint16_t orc_to_half(double v) { return to_half(v); }
+double orc_from_half(uint16_t h) { return from_half(h); }
+void orc_ray_dir(uint32_t k, uint32_t rays, double jitter, double* out) {
+    V3<double> d = ray_dir<double>(k, rays, jitter);
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+void orc_probe_world_pos(const OrcGrid* g, uint32_t p, double* out) {
+    Grid gg = to_grid(g);
+    V3<double> d = probe_world_pos<double>(gg, p);
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+double orc_hysteresis_exponent(double dtMs, int32_t normalize) { return hysteresis_exponent_for_interval(dtMs, normalize != 0); }
+void orc_grid_resolution(const double* size, int32_t target, uint32_t* out) { compute_grid_resolution(size, target, out); }
+int32_t orc_gutter_source_lane(int32_t lane) { return gutter_source_lane(lane); }
+void orc_sample_atlas(const OrcGrid* g, const uint16_t* atlas, const double* P, const double* N, double* out) {
+    Grid gg = to_grid(g);
+    V3<double> r = sample_atlas<double>(gg, atlas, V3<double>(P[0], P[1], P[2]), V3<double>(N[0], N[1], N[2]));
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+// ------------------------------------------------------- refit and TLAS
+int32_t orc_refit_blas(uint32_t* nodes, uint64_t nodesLen, const uint32_t* triIndex, uint64_t triIndexLen,
+                       const float* vertexData, uint64_t vdLen, int64_t root, int64_t end) {
+    return refit_blas(nodes, nodesLen, triIndex, triIndexLen, vertexData, vdLen, root, end) ? 1 : 0;
+}
+int32_t orc_refit_tlas_range(float* nodes, uint64_t nodesLen, const float* ib, uint64_t ibLen, int64_t root, int64_t end) {
+    return refit_tlas_range(nodes, nodesLen, ib, ibLen, root, end) ? 1 : 0;
+}
+int32_t orc_refit_tlas_dirty(float* nodes, uint64_t nodesLen, const float* ib, uint64_t ibLen, int64_t end,
+                             const uint32_t* dirty, uint64_t nDirty, uint32_t* touchedOut, uint32_t* touchedCount) {
+    std::vector<uint32_t> t;
+    if (!refit_tlas_dirty(nodes, nodesLen, ib, ibLen, end, dirty, nDirty, t)) return 0;
+    for (size_t i = 0; i < t.size(); ++i) touchedOut[i] = t[i];
+    *touchedCount = (uint32_t)t.size();
+    return 1;
+}
+// aabbs9: per instance min xyz, max xyz, centroid xyz (FP64)
+uint32_t orc_build_tlas(const double* aabbs9, uint32_t n, float* nodes12Out, uint32_t* orderOut, double* bounds64Out) {
+    std::vector<Aabb> a(n);
+    for (uint32_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            a[i].mn[k] = aabbs9[i * 9 + k]; a[i].mx[k] = aabbs9[i * 9 + 3 + k]; a[i].c[k] = aabbs9[i * 9 + 6 + k];
+        }
+    std::vector<TlasRec> recs;
+    std::vector<uint32_t> order;
+    build_tlas(a, recs, order);
+    for (size_t i = 0; i < recs.size(); ++i) {
+        float* o = nodes12Out + i * 12;
+        for (int k = 0; k < 6; ++k) o[k] = (float)recs[i].bx[k];
+        o[6] = (float)recs[i].miss;
+        o[7] = recs[i].leaf ? (float)recs[i].off : 0.0f;
+        o[8] = recs[i].leaf ? (float)recs[i].cnt : 0.0f;
+        o[9] = o[10] = o[11] = 0.0f;
+        if (bounds64Out) for (int k = 0; k < 6; ++k) bounds64Out[i * 6 + k] = recs[i].bx[k];
+    }
+    for (uint32_t i = 0; i < n; ++i) orderOut[i] = order[i];
+    return (uint32_t)recs.size();
+}
+// computeDynamic per source instance: world16 column-major FP64, local bounds f32.
+void orc_compute_instances(const double* world16, const uint8_t* active, const float* lbounds6, uint32_t n,
+                           float* invRows12, float* detSign, double* aabbs9) {
+    for (uint32_t i = 0; i < n; ++i) {
+        Aabb b;
+        compute_instance(world16 + (size_t)i * 16, active[i] != 0, lbounds6 + (size_t)i * 6, invRows12 + (size_t)i * 12,
+                         detSign[i], b);
+        for (int k = 0; k < 3; ++k) {
+            aabbs9[i * 9 + k] = b.mn[k]; aabbs9[i * 9 + 3 + k] = b.mx[k]; aabbs9[i * 9 + 6 + k] = b.c[k];
+        }
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,232 @@
+// sb_blend.cu — temporal blend of the probe histories and the RGBA16F atlas
+// upload, fused into one kernel (blendKernel gi_probes.js:2317-2532 followed by
+// uploadKernel 2737-2846: the upload's 3x3 filter only reads texels of the same
+// probe tile, so one CTA per probe finishes both without a second launch).
+// Also: the clustered light grid (lightGridKernel 1888-1938) and atlas clears
+// (clearAtlasKernel 2690-2707).
+#include "sb_math.cuh"
+#include "sb_kernels.cuh"
+
+namespace sb {
+
+// Kahan-compensated FP32 accumulator.
+struct Kahan {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+};
+
+__global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) {
+    __shared__ float4 rayC[256];
+    __shared__ float4 dirC[256];
+    __shared__ float4 irrS[36];
+    __shared__ float2 depS[36];
+    __shared__ float4 outI[36];
+    const uint32_t slot = blockIdx.x;
+    const uint32_t lane = threadIdx.x;
+    if (slot >= C.updatedCount) return;  // uniform per block
+    const uint32_t N = C.rays;
+    const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+    for (uint32_t k = lane; k < N; k += 64) {
+        rayC[k] = C.rayData[(size_t)slot * N + k];
+        float3 d = ray_dir(k, N, P.frameJitter);
+        dirC[k] = make_float4(d.x, d.y, d.z, 0.0f);
+    }
+    __syncthreads();
+
+    if (lane < 36) {
+        const uint32_t lx = lane % OCT + BORDER, ly = lane / OCT + BORDER;
+        const uint32_t local = ly * TILE + lx;
+        float u = (float(lx) - 1.0f + 0.5f) / 6.0f, v = (float(ly) - 1.0f + 0.5f) / 6.0f;
+        float3 dir = oct_decode(u, v);
+        Kahan ar, ag, ab, wsum, lAcc, lAcc2, dAcc, dAcc2, dwsum;
+        const float cosPow = fmaxf(P.debugCosinePower, 1e-4f);
+        for (uint32_t k = 0; k < N; ++k) {
+            float4 r = rayC[k];
+            float4 d = dirC[k];
+            float cd = fmaxf(dir.x * d.x + dir.y * d.y + dir.z * d.z, 0.0f);
+            float cw = powf(cd, cosPow);
+            ar.add(r.x * cw);
+            ag.add(r.y * cw);
+            ab.add(r.z * cw);
+            wsum.add(cw);
+            float rl = luma3(mk(r.x, r.y, r.z));
+            lAcc.add(rl * cw);
+            lAcc2.add(rl * rl * cw);
+            float hitT = r.w;
+            float decoded = hitT < -1.5f ? -hitT - 2.0f : hitT;
+            float rdist = hitT == -1.0f ? C.maxDist : decoded;
+            float dw = powf(cw, P.depthSharpness);
+            dAcc.add(rdist * dw);
+            dAcc2.add(rdist * rdist * dw);
+            dwsum.add(dw);
+        }
+        float wden = fmaxf(wsum.s, 1e-4f);
+        float3 meanRad = mk(ar.s / wden, ag.s / wden, ab.s / wden);
+        float curL = lAcc.s / wden, curM2 = lAcc2.s / wden;
+        float dden = fmaxf(dwsum.s, 1e-4f);
+        float meanR = dAcc.s / dden, meanR2 = dAcc2.s / dden;
+
+        const size_t ib = (size_t)probeIndex * 64u + local;
+        float4 prev4 = C.irr[ib];
+        float3 prev = xyz(prev4);
+        bool wasBlack = (prev.x + prev.y + prev.z) < 1e-6f;
+        float prevL = luma3(prev);
+        float prevM2 = prev4.w;
+        float prevVar = fmaxf(prevM2 - prevL * prevL, 0.0f);
+        float curVar = fmaxf(curM2 - curL * curL, 0.0f);
+        float lumRef = fmaxf(fmaxf(curL, prevL), 0.0f);
+        float varFloor = P.debugTempVarEps + lumRef * lumRef * P.debugTempVarRel;
+        float sigma = sqrtf(prevVar + curVar + varFloor);
+        float absDelta = fabsf(curL - prevL);
+        float s0 = sigma * P.debugTempChangeSigma0;
+        float s1 = sigma * fmaxf(P.tempChangeSigma1, P.debugTempChangeSigma0 + 0.01f);
+        float changeW = clampf((absDelta - s0) / fmaxf(s1 - s0, 1e-6f), 0.0f, 1.0f);
+        float H = P.hysteresis;
+        float rawNoiseH = H + (1.0f - H) * P.debugTempNoiseHBoost;
+        float rawChangeH = fmaxf(H - P.tempChangeHDrop, P.debugTempMinChangeH);
+        float rawHEff = mixf(rawNoiseH, rawChangeH, changeW);
+        float hEff = powf(clampf(rawHEff, 1e-6f, 1.0f), P.hysteresisExponent);
+        float h = wasBlack ? 0.0f : hEff;
+        float band = sqrtf(prevVar + varFloor) * P.tempClampSigma;
+        float clampScale = fminf(1.0f, band / fmaxf(absDelta, 1e-6f));
+        float3 clipped = prev + (meanRad - prev) * clampScale;
+        float3 cand = wasBlack ? meanRad : clipped;
+        float3 blended = mk(mixf(cand.x, prev.x, h), mixf(cand.y, prev.y, h), mixf(cand.z, prev.z, h));
+        float m2 = mixf(curM2, prevM2, h);
+        float4 outIrr = make_float4(blended.x, blended.y, blended.z, m2);
+        C.irr[ib] = outIrr;
+
+        float2 dprev = C.depth[ib];
+        bool dWasZero = dprev.x < 1e-6f;
+        float rawDepthH = clampf(H * P.debugDepthHistoryScale, 0.0f, 0.999f);
+        float depthH = powf(fmaxf(rawDepthH, 1e-6f), P.hysteresisExponent);
+        float dh = dWasZero ? 0.0f : depthH;
+        float2 outDep = make_float2(mixf(meanR, dprev.x, dh), mixf(meanR2, dprev.y, dh));
+        C.depth[ib] = outDep;
+        irrS[lane] = outIrr;
+        depS[lane] = outDep;
+    }
+    __syncthreads();
+
+    // upload: 3x3 bilateral filter of the new history (reads this tile only)
+    if (lane < 36) {
+        const int sx = (int)(lane % OCT), sy = (int)(lane / OCT);
+        float4 c4 = irrS[lane];
+        float3 eC = xyz(c4);
+        float lumaC = luma3(eC);
+        float varC = fmaxf(c4.w - lumaC * lumaC, 0.0f);
+        float smW = 1.0f + P.filterSmooth * 6.0f;
+        float kEff = 8.0f * smW * P.debugFilterKScale;
+        float relEff = 0.0225f * smW * P.debugFilterRelScale;
+        float den = fmaxf(varC * kEff + fmaxf(0.001f * P.debugFilterEpsScale, lumaC * lumaC * relEff), 1e-8f);
+        float3 facc = mk(0.f, 0.f, 0.f);
+        float fw = 0.0f;
+#pragma unroll
+        for (int jy = -1; jy <= 1; ++jy)
+#pragma unroll
+            for (int jx = -1; jx <= 1; ++jx) {
+                const float gw = (jx == 0 && jy == 0) ? 1.0f
+                                 : (jx == 0 || jy == 0) ? 0.6065306597126334f   // exp(-0.5)
+                                                        : 0.36787944117144233f; // exp(-1)
+                int nx = min(max(sx + jx, 0), OCT - 1), ny = min(max(sy + jy, 0), OCT - 1);
+                float3 en = xyz(irrS[ny * OCT + nx]);
+                float dl = luma3(en) - lumaC;
+                float es = expf(dl * dl / den * -1.0f);
+                float w = gw * es;
+                facc = facc + en * w;
+                fw += w;
+            }
+        float fden = fmaxf(fw, 1e-4f);
+        float3 filt = mk(facc.x / fden, facc.y / fden, facc.z / fden);
+        float s = P.filterStrength;
+        outI[lane] = make_float4(mixf(eC.x, filt.x, s), mixf(eC.y, filt.y, s), mixf(eC.z, filt.z, s), 1.0f);
+    }
+    __syncthreads();
+
+    // 64 lanes: interior + canonical mirrored gutter (gi_probes.js:2816-2839)
+    {
+        const int edge = TILE - 1, lo = BORDER, hi = BORDER + OCT - 1;
+        int lx = (int)(lane % TILE), ly = (int)(lane / TILE);
+        bool onLeft = lx == 0, onRight = lx == edge, onTop = ly == 0, onBottom = ly == edge;
+        bool colB = onLeft || onRight, rowB = onTop || onBottom, corner = colB && rowB;
+        int sx = corner ? (onLeft ? hi : lo) : (rowB ? edge - lx : (colB ? (onLeft ? lo : hi) : lx));
+        int sy = corner ? (onTop ? hi : lo) : (rowB ? (onTop ? lo : hi) : (colB ? edge - ly : ly));
+        int src = (sy - BORDER) * OCT + (sx - BORDER);
+        uint32_t col = probeIndex % C.res[0];
+        uint32_t row = (probeIndex / (C.res[0] * C.res[1])) * C.res[1] + (probeIndex / C.res[0]) % C.res[1];
+        size_t t = (size_t)(row * TILE + ly) * C.atlasW + col * TILE + lx;
+        C.atlas[t] = float4_to_half4(outI[src]);
+        float2 d = depS[src];
+        C.depthAtlas[t] = float4_to_half4(make_float4(d.x, d.y, 0.0f, 1.0f));
+    }
+}
+
+cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st) {
+    if (C.updatedCount == 0) return cudaSuccess;
+    k_blend_upload<<<C.updatedCount, 64, 0, st>>>(C, P); note_launch();
+    return cudaGetLastError();
+}
+
+// lightGridKernel, gi_probes.js:1893-1937. Every operation is separately
+// rounded (no contraction) so the lists match an FP32 evaluation exactly.
+__global__ void k_light_grid(float* lights, uint32_t lightCount, DevCascade g0, uint32_t cells) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    uint32_t cellsX = g0.res[0] - 1u, cellsY = g0.res[1] - 1u, cellsZ = g0.res[2] - 1u;
+    uint32_t ix = c % cellsX, iy = (c / cellsX) % cellsY, iz = c / (cellsX * cellsY);
+    float csx = __fdiv_rn(g0.gridSize[0], float(cellsX));
+    float csy = __fdiv_rn(g0.gridSize[1], float(cellsY));
+    float csz = __fdiv_rn(g0.gridSize[2], float(cellsZ));
+    float mnx = __fadd_rn(g0.gridMin[0], __fmul_rn(float(ix), csx));
+    float mny = __fadd_rn(g0.gridMin[1], __fmul_rn(float(iy), csy));
+    float mnz = __fadd_rn(g0.gridMin[2], __fmul_rn(float(iz), csz));
+    float mxx = __fadd_rn(mnx, csx), mxy = __fadd_rn(mny, csy), mxz = __fadd_rn(mnz, csz);
+    float* list = lights + LIGHT_DATA + c * 17u;
+    uint32_t count = 0;
+    for (uint32_t li = 0; li < lightCount; ++li) {
+        const float* L = lights + li * 17u;
+        float ltype = L[0], px = L[1], py = L[2], pz = L[3], lrange = L[10];
+        float dx = fmaxf(fmaxf(__fsub_rn(mnx, px), 0.0f), __fsub_rn(px, mxx));
+        float dy = fmaxf(fmaxf(__fsub_rn(mny, py), 0.0f), __fsub_rn(py, mxy));
+        float dz = fmaxf(fmaxf(__fsub_rn(mnz, pz), 0.0f), __fsub_rn(pz, mxz));
+        float padded = __fadd_rn(lrange, fmaxf(1e-4f, __fmul_rn(lrange, 1e-5f)));
+        float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+        bool intersects = d2 <= __fmul_rn(padded, padded);
+        bool member = ltype < 2.5f && (ltype < 0.5f || lrange <= 0.0f || intersects);
+        if (member) {
+            if (count < 16u) list[1 + count] = float(li);
+            count++;
+        }
+    }
+    list[0] = float(count > 16u ? 17u : count);
+}
+
+cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st) {
+    uint32_t cells = (g0.res[0] - 1u) * (g0.res[1] - 1u) * (g0.res[2] - 1u);
+    if (cells == 0) return cudaSuccess;
+    k_light_grid<<<(cells + 127) / 128, 128, 0, st>>>(lights, lightCount, g0, cells); note_launch();
+    return cudaGetLastError();
+}
+
+// clearAtlasKernel, gi_probes.js:2690-2707: atlases to (0,0,0,1); histories to 0.
+__global__ void k_clear_cascade(DevCascade C) {
+    size_t n = (size_t)C.atlasW * C.atlasH;
+    size_t h = (size_t)C.probeTotal * 64u;
+    uint2 v = float4_to_half4(make_float4(0.f, 0.f, 0.f, 1.f));
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n || i < h; i += (size_t)gridDim.x * blockDim.x) {
+        if (i < n) { C.atlas[i] = v; C.depthAtlas[i] = v; }
+        if (i < h) { C.irr[i] = make_float4(0.f, 0.f, 0.f, 0.f); C.depth[i] = make_float2(0.f, 0.f); }
+    }
+}
+
+cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st) {
+    k_clear_cascade<<<148 * 4, 256, 0, st>>>(C); note_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace sb

@@ -1,0 +1,826 @@
+// sb_ctx.cu — the C ABI (include/speedball_cuda.h): context lifetime, scene and
+// light uploads in the reference layouts, cascade configuration, solves, the
+// refit / TLAS lanes and read-back. Host code; all device work is enqueued on
+// the context's stream.
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sb_kernels.cuh"
+
+using namespace sb;
+
+namespace sb {
+static std::atomic<uint64_t> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+uint64_t launches() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace sb
+
+namespace {
+
+struct Cascade {
+    sb_grid grid{};
+    bool configured = false;
+    uint32_t probeTotal = 0, atlasW = 0, atlasH = 0;
+    float4* irr = nullptr;
+    float2* depth = nullptr;
+    uint2* atlas = nullptr;
+    uint2* depthAtlas = nullptr;
+    float4* rayData = nullptr;
+    uint4* hits = nullptr;
+    uint2* vis = nullptr;
+    size_t rayCap = 0;
+};
+
+}  // namespace
+
+struct sb_ctx {
+    int device = 0;
+    uint32_t flags = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t ownStream = nullptr;
+    std::string err;
+    int numSms = 148;
+
+    SceneBuffers B;
+    bool sceneLoaded = false;
+    bool needPack = false;     // full validation + derived re-pack before the next solve
+    bool tlasPending = false;  // TLAS tail must be built on device (sb_build_tlas)
+    bool tlasOnDevice = false; // the TLAS (and its slot maps) came from sb_build_tlas
+    size_t cap[6] = {0, 0, 0, 0, 0, 0};  // element capacities of the six scene buffers
+
+    InstanceTable I;
+    bool instancesSet = false;
+    uint32_t* instOwner = nullptr;
+    uint32_t* dStage = nullptr;   // staging for src lists
+    double* dStageM = nullptr;    // staging for matrices
+    size_t stageCap = 0;
+
+    uint32_t* dErr = nullptr;
+    uint32_t* dGate = nullptr;
+    uint32_t* dWork = nullptr;
+    unsigned long long* dCounters = nullptr;
+    bool countersOn = false;
+
+    Cascade casc[SB_MAX_CASCADES];
+    sb_params params{};
+    uint32_t lightCount = 0, emitterBase = 0, emitterCount = 0;
+    int32_t clustered = 0;
+    bool lightGridDirty = false;
+    std::vector<float> hostLights;
+
+    TraceTuning tune{256u, 2048u, 0u, 148};
+    cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr;
+    bool timed = false;
+};
+
+namespace {
+
+sb_status fail(sb_ctx* c, sb_status s, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+sb_status fail(sb_ctx* c, sb_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return s;
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess)                                                                   \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? SB_ERR_OOM : SB_ERR_CUDA, "%s: %s", \
+                        #call, cudaGetErrorString(e_));                                          \
+    } while (0)
+
+template <class T> cudaError_t grow(T*& p, size_t& cap, size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(T));
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+template <class T> void release(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+uint32_t tlas_nodes_for(uint32_t n) {
+    // node count of the median split with leaf size 2 (buildTlasRecords)
+    if (n == 0) return 0;
+    std::vector<uint32_t> t(n + 1);
+    t[0] = 1;
+    for (uint32_t m = 1; m <= n; ++m) t[m] = m <= 2 ? 1u : 1u + t[m >> 1] + t[m - (m >> 1)];
+    return t[n];
+}
+
+DevScene dev_scene(const sb_ctx* c) {
+    DevScene S;
+    S.nodes = reinterpret_cast<const uint4*>(c->B.nodes);
+    S.tris = c->B.tris;
+    S.triMaterial = c->B.triMaterial;
+    S.materials = c->B.materials;
+    S.inst = c->B.inst;
+    S.tlas = c->B.tlas;
+    S.lights = c->B.lights;
+    S.nodeCount = c->B.nodeCount;
+    S.triCount = c->B.triCount;
+    S.instCount = c->B.instCount;
+    S.tlasNodeCount = c->B.tlasNodeCount;
+    S.materialCount = c->B.materialCount;
+    S.lightCount = c->lightCount;
+    S.clustered = c->clustered;
+    S.valid = c->B.valid;
+    return S;
+}
+
+void fill_grid(DevCascade& D, const sb_grid& g) {
+    for (int a = 0; a < 3; ++a) {
+        D.gridMin[a] = g.gridMin[a];
+        D.gridSize[a] = g.gridSize[a];
+        D.res[a] = g.res[a];
+    }
+    D.rays = g.raysPerProbe;
+    D.maxDist = g.maxDist;
+    D.cellMin = g.cellMin;
+    D.probeTotal = g.res[0] * g.res[1] * g.res[2];
+    D.atlasW = g.res[0] * 8u;
+    D.atlasH = g.res[1] * g.res[2] * 8u;
+}
+
+DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint32_t updated) {
+    const Cascade& K = c->casc[ci];
+    DevCascade D{};
+    fill_grid(D, K.grid);
+    const sb_grid& g0 = c->casc[0].configured ? c->casc[0].grid : K.grid;
+    for (int a = 0; a < 3; ++a) {
+        D.g0Min[a] = g0.gridMin[a];
+        D.g0Size[a] = g0.gridSize[a];
+        D.g0Res[a] = g0.res[a];
+    }
+    D.probeOffset = probeOffset;
+    D.updatedCount = updated;
+    D.rayData = K.rayData;
+    D.hits = K.hits;
+    D.vis = K.vis;
+    D.irr = K.irr;
+    D.depth = K.depth;
+    D.atlasPrev = K.atlas;
+    D.atlas = K.atlas;
+    D.depthAtlas = K.depthAtlas;
+    return D;
+}
+
+sb_status pack_if_needed(sb_ctx* ctx) {
+    if (!ctx->needPack) return SB_OK;
+    uint32_t one = 1u;
+    CK(cudaMemcpyAsync(ctx->B.valid, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_pack_scene(ctx->B, ctx->dErr, ctx->stream));
+    if (!ctx->tlasPending && ctx->B.tlasNodeCount && ctx->instancesSet)
+        CK(launch_tlas_index(ctx->B, ctx->I, ctx->instOwner, ctx->dErr, ctx->stream));
+    ctx->needPack = false;
+    return SB_OK;
+}
+
+sb_status light_grid_if_needed(sb_ctx* ctx) {
+    if (!ctx->lightGridDirty || !ctx->clustered || !ctx->casc[0].configured) return SB_OK;
+    DevCascade g0{};
+    fill_grid(g0, ctx->casc[0].grid);
+    CK(launch_light_grid(ctx->B.lights, ctx->lightCount, g0, ctx->stream));
+    ctx->lightGridDirty = false;
+    return SB_OK;
+}
+
+sb_status check_grid(sb_ctx* ctx, const sb_grid* g) {
+    if (!g) return fail(ctx, SB_ERR_INVALID_ARG, "grid is null");
+    for (int a = 0; a < 3; ++a)
+        if (g->res[a] < 2 || g->res[a] > 32) return fail(ctx, SB_ERR_INVALID_ARG, "res[%d]=%u outside [2,32]", a, g->res[a]);
+    if (g->raysPerProbe < 32 || g->raysPerProbe > 256 || g->raysPerProbe % 16)
+        return fail(ctx, SB_ERR_INVALID_ARG, "raysPerProbe=%u: must be 32..256 in steps of 16", g->raysPerProbe);
+    return SB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t sb_abi_version(void) { return SB_ABI_VERSION; }
+
+void sb_params_defaults(sb_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->frameJitter = 0.0f;
+    p->emitterVisSeed = 0.0f;
+    p->hysteresis = 0.60f;              // JITTER_HYSTERESIS_DEFAULTS.gated
+    p->hysteresisExponent = 1.0f;
+    p->depthSharpness = 7.0f;
+    p->radianceClamp = 8.0f;
+    p->classifyStrength = 0.0f;
+    p->filterStrength = 1.0f;
+    p->filterSmooth = 0.5f;
+    p->tempChangeSigma1 = 2.5f;
+    p->tempChangeHDrop = 0.30f;
+    p->tempClampSigma = 6.0f;
+    p->nirGate = 0.0f;
+    p->nirGain = 1.0f;
+    p->skyIntensity = 1.0f;
+    p->debugTraceBiasScale = p->debugRayEpsScale = p->debugDirectScale = p->debugEmissiveScale = 1.0f;
+    p->debugAlbedoScale = p->debugBounceScale = p->debugCosinePower = 1.0f;
+    p->debugTempNoiseHBoost = 0.25f;
+    p->debugTempChangeSigma0 = 0.75f;
+    p->debugTempMinChangeH = 0.55f;
+    p->debugTempVarEps = 0.000025f;
+    p->debugTempVarRel = 0.0025f;
+    p->debugDepthHistoryScale = 1.0f;
+    p->debugFilterKScale = p->debugFilterRelScale = p->debugFilterEpsScale = 1.0f;
+}
+
+sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
+    if (!out) return SB_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return SB_ERR_NO_DEVICE;
+    sb_ctx* ctx = new sb_ctx();
+    ctx->device = opts ? opts->device : 0;
+    ctx->flags = opts ? opts->flags : 0;
+    if (ctx->device < 0 || ctx->device >= n) {
+        delete ctx;
+        return SB_ERR_INVALID_ARG;
+    }
+    sb_status st = SB_OK;
+    do {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) { st = SB_ERR_CUDA; break; }
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess) { st = SB_ERR_CUDA; break; }
+        if (prop.major < 10) { st = SB_ERR_UNSUPPORTED; break; }  // sm_100a build
+        ctx->numSms = prop.multiProcessorCount;
+        ctx->tune.numSms = ctx->numSms;
+        if (cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking) != cudaSuccess) { st = SB_ERR_CUDA; break; }
+        ctx->stream = ctx->ownStream;
+        if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 4) != cudaSuccess ||
+            cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 8 * 8) != cudaSuccess ||
+            cudaMalloc(&ctx->B.valid, 4) != cudaSuccess) { st = SB_ERR_OOM; break; }
+        cudaMemset(ctx->dErr, 0, 4);
+        cudaMemset(ctx->B.valid, 0, 4);
+        cudaMemset(ctx->dCounters, 0, 64);
+        cudaEventCreate(&ctx->ev0);
+        cudaEventCreate(&ctx->evMid);
+        cudaEventCreate(&ctx->ev1);
+        sb_params_defaults(&ctx->params);
+        if (cudaDeviceSynchronize() != cudaSuccess) { st = SB_ERR_CUDA; break; }
+    } while (0);
+    if (st != SB_OK) {
+        sb_destroy(ctx);
+        return st;
+    }
+    *out = ctx;
+    return SB_OK;
+}
+
+void sb_destroy(sb_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    SceneBuffers& B = ctx->B;
+    release(B.nodes); release(B.triIndex); release(B.vertexData); release(B.triMaterial); release(B.materials);
+    release(B.lights); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
+    release(B.arrive); release(B.valid);
+    InstanceTable& I = ctx->I;
+    release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb); release(I.invRows);
+    release(I.detSign); release(I.order); release(I.slotOf); release(I.liveBounds); release(I.nodeDepth);
+    release(I.scratch); release(ctx->instOwner); release(ctx->dStage); release(ctx->dStageM);
+    for (auto& K : ctx->casc) {
+        release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.rayData); release(K.hits);
+        release(K.vis);
+    }
+    release(ctx->dErr); release(ctx->dGate); release(ctx->dWork); release(ctx->dCounters);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->evMid) cudaEventDestroy(ctx->evMid);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
+    delete ctx;
+}
+
+const char* sb_last_error(const sb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+sb_status sb_host_alloc(size_t bytes, void** out) {
+    if (!out || bytes == 0) return SB_ERR_INVALID_ARG;
+    *out = nullptr;
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        return e == cudaErrorMemoryAllocation ? SB_ERR_OOM : SB_ERR_CUDA;
+    }
+    return SB_OK;
+}
+
+void sb_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
+sb_status sb_set_stream(sb_ctx* ctx, void* s) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    ctx->stream = s ? (cudaStream_t)s : ctx->ownStream;
+    return SB_OK;
+}
+
+sb_status sb_synchronize(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    uint32_t e = 0;
+    CK(cudaMemcpy(&e, ctx->dErr, 4, cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(ctx->dErr, 0, 4));
+        if (e & ERR_LAYOUT) return fail(ctx, SB_ERR_LAYOUT_VIOLATION, "device check: threaded-layout or index violation");
+        if (e & ERR_WATCHDOG) return fail(ctx, SB_ERR_DEVICE_WATCHDOG, "device check: traversal iteration cap reached");
+        if (e & ERR_NAN_KEY) return fail(ctx, SB_ERR_INVALID_ARG, "device check: NaN instance bounds");
+        return fail(ctx, SB_ERR_CUDA, "device error word 0x%x", e);
+    }
+    return SB_OK;
+}
+
+sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
+    if (!ctx || !v) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!v->bvhNodes || !v->triIndex || !v->vertexData || !v->triMaterial || !v->materials)
+        return fail(ctx, SB_ERR_INVALID_ARG, "null scene array");
+    if (v->nodeCount == 0 || v->triCount == 0 || v->vertexCount == 0 || v->materialCount == 0 || v->instCount == 0)
+        return fail(ctx, SB_ERR_INVALID_ARG, "empty scene");
+    if (v->triCount >= (1u << 24) || v->nodeCount >= (1u << 24))
+        return fail(ctx, SB_ERR_INVALID_ARG, "BVH pool exceeds the 24-bit index ceiling");
+    if (v->instBase != v->materialCount * SB_MAT_STRIDE)
+        return fail(ctx, SB_ERR_INVALID_ARG, "instBase %u != materialCount*28", v->instBase);
+    uint32_t tlasBase = v->instBase + v->instCount * SB_MAT_STRIDE;
+    if (v->tlasNodeCount && v->tlasBase != tlasBase)
+        return fail(ctx, SB_ERR_INVALID_ARG, "tlasBase %u != instBase + instCount*28", v->tlasBase);
+    uint32_t tlasNodes = v->tlasNodeCount ? v->tlasNodeCount : tlas_nodes_for(v->instCount);
+    size_t matLen = (size_t)tlasBase + (size_t)tlasNodes * SB_TLAS_STRIDE_F32;
+    if (v->tlasNodeCount && v->materialsLen < matLen)
+        return fail(ctx, SB_ERR_INVALID_ARG, "materialsLen %u < %zu", v->materialsLen, matLen);
+    if (!v->tlasNodeCount && v->materialsLen < tlasBase)
+        return fail(ctx, SB_ERR_INVALID_ARG, "materialsLen %u < %u", v->materialsLen, tlasBase);
+    cudaSetDevice(ctx->device);
+    SceneBuffers& B = ctx->B;
+    size_t nN = (size_t)v->nodeCount * 8, nT = (size_t)v->triCount * 3, nV = (size_t)v->vertexCount * 8;
+    CK(grow(B.nodes, ctx->cap[0], nN));
+    CK(grow(B.triIndex, ctx->cap[1], nT));
+    CK(grow(B.vertexData, ctx->cap[2], nV));
+    CK(grow(B.triMaterial, ctx->cap[3], (size_t)v->triCount));
+    CK(grow(B.materials, ctx->cap[4], matLen));
+    size_t cTris = 0, cInst = 0, cTlas = 0, cBits = 0, cPar = 0, cArr = 0;
+    release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent); release(B.arrive);
+    CK(grow(B.tris, cTris, (size_t)v->triCount * 3));
+    CK(grow(B.inst, cInst, (size_t)v->instCount * 4));
+    CK(grow(B.tlas, cTlas, (size_t)tlasNodes * 2));
+    CK(grow(B.matBits, cBits, (size_t)v->materialCount));
+    CK(grow(B.parent, cPar, (size_t)v->nodeCount));
+    CK(grow(B.arrive, cArr, (size_t)v->nodeCount));
+    CK(cudaMemcpyAsync(B.nodes, v->bvhNodes, nN * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(B.triIndex, v->triIndex, nT * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(B.vertexData, v->vertexData, nV * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(B.triMaterial, v->triMaterial, (size_t)v->triCount * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(B.materials, 0, matLen * 4, ctx->stream));
+    CK(cudaMemcpyAsync(B.materials, v->materials, (v->tlasNodeCount ? matLen : tlasBase) * 4, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    B.nodeCount = v->nodeCount;
+    B.triCount = v->triCount;
+    B.vertexCount = v->vertexCount;
+    B.materialsLen = (uint32_t)matLen;
+    B.materialCount = v->materialCount;
+    B.instBase = v->instBase;
+    B.instCount = v->instCount;
+    B.tlasBase = tlasBase;
+    B.tlasNodeCount = tlasNodes;
+    ctx->tlasPending = v->tlasNodeCount == 0;
+    ctx->tlasOnDevice = false;
+    ctx->sceneLoaded = true;
+    if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
+    // validation + derived layouts; a pending TLAS is packed by sb_build_tlas
+    uint32_t one = 1u;
+    CK(cudaMemcpyAsync(B.valid, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_pack_scene(ctx->tlasPending ? [&] { SceneBuffers t = B; t.instCount = 0; t.tlasNodeCount = 0; return t; }() : B,
+                         ctx->dErr, ctx->stream));
+    ctx->needPack = false;
+    return SB_OK;
+}
+
+sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, const void* src) {
+    if (!ctx || (!src && count)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    uint32_t buf = which & 0xFFu, ci = which >> 8;
+    cudaSetDevice(ctx->device);
+    void* dst = nullptr;
+    size_t len = 0, esz = 4;
+    SceneBuffers& B = ctx->B;
+    switch (buf) {
+        case SB_BUF_BVH_NODES: dst = B.nodes; len = (size_t)B.nodeCount * 8; break;
+        case SB_BUF_TRI_INDEX: dst = B.triIndex; len = (size_t)B.triCount * 3; break;
+        case SB_BUF_VERTEX_DATA: dst = B.vertexData; len = (size_t)B.vertexCount * 8; break;
+        case SB_BUF_TRI_MATERIAL: dst = B.triMaterial; len = B.triCount; break;
+        case SB_BUF_MATERIALS: dst = B.materials; len = B.materialsLen; break;
+        case SB_BUF_LIGHTS: dst = B.lights; len = ctx->B.lightsLen; break;
+        case SB_BUF_IRRADIANCE_HISTORY:
+        case SB_BUF_DEPTH_HISTORY: {
+            if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+                return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+            Cascade& K = ctx->casc[ci];
+            dst = buf == SB_BUF_IRRADIANCE_HISTORY ? (void*)K.irr : (void*)K.depth;
+            len = (size_t)K.probeTotal * 64 * (buf == SB_BUF_IRRADIANCE_HISTORY ? 4 : 2);
+            break;
+        }
+        case SB_BUF_IRRADIANCE_ATLAS:
+        case SB_BUF_DEPTH_ATLAS: {
+            if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+                return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+            Cascade& K = ctx->casc[ci];
+            dst = buf == SB_BUF_IRRADIANCE_ATLAS ? (void*)K.atlas : (void*)K.depthAtlas;
+            len = (size_t)K.atlasW * K.atlasH * 4;
+            esz = 2;
+            break;
+        }
+        default: return fail(ctx, SB_ERR_INVALID_ARG, "buffer %u is not writable", buf);
+    }
+    if (!dst) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not allocated", buf);
+    if ((size_t)start + count > len) return fail(ctx, SB_ERR_INVALID_ARG, "range [%u,+%u) outside %zu", start, count, len);
+    CK(cudaMemcpyAsync((char*)dst + (size_t)start * esz, src, (size_t)count * esz, cudaMemcpyHostToDevice, ctx->stream));
+    if (buf <= SB_BUF_MATERIALS) ctx->needPack = true;
+    if (buf == SB_BUF_LIGHTS && ctx->clustered) ctx->lightGridDirty = true;
+    return SB_OK;
+}
+
+sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, void* dstHost) {
+    if (!ctx || (!dstHost && count)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    uint32_t buf = which & 0xFFu, ci = which >> 8;
+    cudaSetDevice(ctx->device);
+    const void* srcp = nullptr;
+    size_t len = 0, esz = 4;
+    SceneBuffers& B = ctx->B;
+    Cascade* K = ci < SB_MAX_CASCADES ? &ctx->casc[ci] : nullptr;
+    switch (buf) {
+        case SB_BUF_BVH_NODES: srcp = B.nodes; len = (size_t)B.nodeCount * 8; break;
+        case SB_BUF_TRI_INDEX: srcp = B.triIndex; len = (size_t)B.triCount * 3; break;
+        case SB_BUF_VERTEX_DATA: srcp = B.vertexData; len = (size_t)B.vertexCount * 8; break;
+        case SB_BUF_TRI_MATERIAL: srcp = B.triMaterial; len = B.triCount; break;
+        case SB_BUF_MATERIALS: srcp = B.materials; len = B.materialsLen; break;
+        case SB_BUF_LIGHTS: srcp = B.lights; len = B.lightsLen; break;
+        case SB_BUF_IRRADIANCE_HISTORY: if (K) { srcp = K->irr; len = (size_t)K->probeTotal * 256; } break;
+        case SB_BUF_DEPTH_HISTORY: if (K) { srcp = K->depth; len = (size_t)K->probeTotal * 128; } break;
+        case SB_BUF_IRRADIANCE_ATLAS: if (K) { srcp = K->atlas; len = (size_t)K->atlasW * K->atlasH * 4; esz = 2; } break;
+        case SB_BUF_DEPTH_ATLAS: if (K) { srcp = K->depthAtlas; len = (size_t)K->atlasW * K->atlasH * 4; esz = 2; } break;
+        case SB_BUF_RAY_DATA: if (K) { srcp = K->rayData; len = K->rayCap * 4; } break;
+        case SB_BUF_HIT_RECORDS: if (K) { srcp = K->hits; len = K->hits ? K->rayCap * 4 : 0; } break;
+        case SB_BUF_VISIBILITY: if (K) { srcp = K->vis; len = K->vis ? K->rayCap * 2 : 0; } break;
+        case SB_BUF_TLAS_ORDER: srcp = ctx->I.order; len = ctx->instancesSet ? ctx->I.count : 0; break;
+        case SB_BUF_INSTANCE_BOUNDS: srcp = ctx->I.liveBounds; len = ctx->instancesSet ? (size_t)ctx->I.count * 6 : 0; break;
+        default: return fail(ctx, SB_ERR_INVALID_ARG, "unknown buffer %u", buf);
+    }
+    if (!srcp) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not available", buf);
+    if ((size_t)start + count > len) return fail(ctx, SB_ERR_INVALID_ARG, "range [%u,+%u) outside %zu", start, count, len);
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpy(dstHost, (const char*)srcp + (size_t)start * esz, (size_t)count * esz, cudaMemcpyDeviceToHost));
+    return SB_OK;
+}
+
+sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count, uint32_t emitterBase,
+                           uint32_t emitterCount, int32_t clustered) {
+    if (!ctx || (!records && count)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (count > SB_MAX_LIGHTS) return fail(ctx, SB_ERR_INVALID_ARG, "%u lights > %u", count, SB_MAX_LIGHTS);
+    if (emitterCount > 0)
+        return fail(ctx, SB_ERR_UNSUPPORTED, "giEmitter records (emitter visibility / virtual rays) are not built");
+    cudaSetDevice(ctx->device);
+    uint32_t cells = 0;
+    if (clustered) {
+        if (!ctx->casc[0].configured) return fail(ctx, SB_ERR_NOT_READY, "clustered lights need cascade 0 configured");
+        const sb_grid& g = ctx->casc[0].grid;
+        cells = (g.res[0] - 1) * (g.res[1] - 1) * (g.res[2] - 1);
+    }
+    uint32_t len = SB_MAX_LIGHTS * SB_LIGHT_STRIDE + cells * (SB_LIGHTS_PER_CELL + 1);
+    ctx->hostLights.assign(len, 0.0f);
+    if (count) std::memcpy(ctx->hostLights.data(), records, (size_t)count * SB_LIGHT_STRIDE * 4);
+    size_t cap = ctx->cap[5];
+    CK(grow(ctx->B.lights, cap, len));
+    ctx->cap[5] = cap;
+    ctx->B.lightsLen = len;
+    CK(cudaMemcpyAsync(ctx->B.lights, ctx->hostLights.data(), (size_t)len * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->lightCount = count;
+    ctx->emitterBase = emitterBase;
+    ctx->emitterCount = emitterCount;
+    ctx->clustered = clustered ? 1 : 0;
+    ctx->lightGridDirty = ctx->clustered != 0;
+    return SB_OK;
+}
+
+sb_status sb_set_params(sb_ctx* ctx, const sb_params* p) {
+    if (!ctx || !p) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (p->classifyStrength != 0.0f)
+        return fail(ctx, SB_ERR_UNSUPPORTED, "probe classification / relocation (classifyStrength > 0) is not built");
+    ctx->params = *p;
+    return SB_OK;
+}
+
+sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (ci >= SB_MAX_CASCADES) return fail(ctx, SB_ERR_INVALID_ARG, "cascade %u >= %u", ci, SB_MAX_CASCADES);
+    sb_status s = check_grid(ctx, g);
+    if (s != SB_OK) return s;
+    cudaSetDevice(ctx->device);
+    Cascade& K = ctx->casc[ci];
+    uint32_t probeTotal = g->res[0] * g->res[1] * g->res[2];
+    bool sameDims = K.configured && K.grid.res[0] == g->res[0] && K.grid.res[1] == g->res[1] &&
+                    K.grid.res[2] == g->res[2];
+    size_t rays = (size_t)probeTotal * g->raysPerProbe;
+    if (!sameDims) {
+        release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas);
+        size_t c = 0;
+        CK(grow(K.irr, c, (size_t)probeTotal * 64)); c = 0;
+        CK(grow(K.depth, c, (size_t)probeTotal * 64)); c = 0;
+        CK(grow(K.atlas, c, (size_t)probeTotal * 64)); c = 0;
+        CK(grow(K.depthAtlas, c, (size_t)probeTotal * 64));
+    }
+    if (rays > K.rayCap || !K.rayData) {
+        release(K.rayData); release(K.hits); release(K.vis);
+        size_t c = 0;
+        CK(grow(K.rayData, c, rays));
+        if (ctx->flags & SB_CTX_RECORD_HITS) {
+            c = 0; CK(grow(K.hits, c, rays));
+            c = 0; CK(grow(K.vis, c, rays));
+        }
+        K.rayCap = rays;
+    }
+    K.grid = *g;
+    K.probeTotal = probeTotal;
+    K.atlasW = g->res[0] * 8;
+    K.atlasH = g->res[1] * g->res[2] * 8;
+    K.configured = true;
+    if (!sameDims) {
+        DevCascade D = dev_cascade(ctx, ci, 0, 0);
+        CK(launch_clear_cascade(D, ctx->stream));
+    }
+    if (ci == 0 && ctx->clustered) {
+        // the cell lists follow C0's grid: re-size the light arena
+        const sb_grid& gg = ctx->casc[0].grid;
+        uint32_t cells = (gg.res[0] - 1) * (gg.res[1] - 1) * (gg.res[2] - 1);
+        uint32_t len = SB_MAX_LIGHTS * SB_LIGHT_STRIDE + cells * (SB_LIGHTS_PER_CELL + 1);
+        if (len != ctx->B.lightsLen) {
+            std::vector<float> rec(ctx->hostLights.begin(), ctx->hostLights.begin() + SB_MAX_LIGHTS * SB_LIGHT_STRIDE);
+            s = sb_upload_lights(ctx, rec.data(), ctx->lightCount, ctx->emitterBase, ctx->emitterCount, 1);
+            if (s != SB_OK) return s;
+        }
+        ctx->lightGridDirty = true;
+    }
+    return SB_OK;
+}
+
+sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t updatedCount) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+        return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if (ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "TLAS not built (sb_build_tlas)");
+    if (!ctx->B.lights) return fail(ctx, SB_ERR_NOT_READY, "no lights uploaded (sb_upload_lights, count may be 0)");
+    Cascade& K = ctx->casc[ci];
+    if (updatedCount > K.probeTotal) updatedCount = K.probeTotal;
+    probeOffset %= K.probeTotal;
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    s = light_grid_if_needed(ctx);
+    if (s != SB_OK) return s;
+    DevScene S = dev_scene(ctx);
+    DevCascade D = dev_cascade(ctx, ci, probeOffset, updatedCount);
+    DevParams P;
+    std::memcpy(&P, &ctx->params, sizeof P);
+    if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 64, ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune, ctx->stream));
+    CK(cudaEventRecord(ctx->evMid, ctx->stream));
+    CK(launch_blend_upload(D, P, ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->timed = true;
+    return SB_OK;
+}
+
+sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, float* tOut, int32_t* triOut,
+                     int32_t* instOut) {
+    if (!ctx || (n && (!ro || !rd || !tOut || !triOut || !instOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!ctx->sceneLoaded || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "scene / TLAS not ready");
+    if (n == 0) return SB_OK;
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    float *dro = nullptr, *drd = nullptr, *dt = nullptr;
+    int32_t *dtri = nullptr, *dinst = nullptr;
+    CK(cudaMallocAsync(&dro, (size_t)n * 12, ctx->stream));
+    CK(cudaMallocAsync(&drd, (size_t)n * 12, ctx->stream));
+    CK(cudaMallocAsync(&dt, (size_t)n * 4, ctx->stream));
+    CK(cudaMallocAsync(&dtri, (size_t)n * 4, ctx->stream));
+    CK(cudaMallocAsync(&dinst, (size_t)n * 4, ctx->stream));
+    CK(cudaMemcpyAsync(dro, ro, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(drd, rd, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_raycast(dev_scene(ctx), dro, drd, n, dt, dtri, dinst, ctx->dErr, ctx->stream));
+    CK(cudaMemcpyAsync(tOut, dt, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(triOut, dtri, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(instOut, dinst, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    cudaFreeAsync(dro, ctx->stream); cudaFreeAsync(drd, ctx->stream); cudaFreeAsync(dt, ctx->stream);
+    cudaFreeAsync(dtri, ctx->stream); cudaFreeAsync(dinst, ctx->stream);
+    return sb_synchronize(ctx);
+}
+
+sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist, uint32_t n, uint8_t* out) {
+    if (!ctx || (n && (!ro || !rd || !maxDist || !out))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!ctx->sceneLoaded || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "scene / TLAS not ready");
+    if (n == 0) return SB_OK;
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    float *dro = nullptr, *drd = nullptr, *dm = nullptr;
+    uint8_t* dout = nullptr;
+    CK(cudaMallocAsync(&dro, (size_t)n * 12, ctx->stream));
+    CK(cudaMallocAsync(&drd, (size_t)n * 12, ctx->stream));
+    CK(cudaMallocAsync(&dm, (size_t)n * 4, ctx->stream));
+    CK(cudaMallocAsync(&dout, (size_t)n, ctx->stream));
+    CK(cudaMemcpyAsync(dro, ro, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(drd, rd, (size_t)n * 12, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(dm, maxDist, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_occluded(dev_scene(ctx), dro, drd, dm, n, dout, ctx->dErr, ctx->stream));
+    CK(cudaMemcpyAsync(out, dout, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    cudaFreeAsync(dro, ctx->stream); cudaFreeAsync(drd, ctx->stream); cudaFreeAsync(dm, ctx->stream);
+    cudaFreeAsync(dout, ctx->stream);
+    return sb_synchronize(ctx);
+}
+
+// ----------------------------------------------------------- refit / TLAS
+sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if (!(end > root && end <= ctx->B.nodeCount))
+        return fail(ctx, SB_ERR_LAYOUT_VIOLATION, "refit range [%u,%u) outside the node pool", root, end);
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    CK(launch_refit_blas(ctx->B, root, end, ctx->dErr, ctx->dGate, ctx->stream));
+    return SB_OK;
+}
+
+sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, const uint8_t* active,
+                           const uint32_t* blasRoot, const uint32_t* blasEnd) {
+    if (!ctx || !world16 || !active || !blasRoot || !blasEnd) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if (count != ctx->B.instCount)
+        return fail(ctx, SB_ERR_INVALID_ARG, "instance count %u != scene instCount %u", count, ctx->B.instCount);
+    for (uint32_t i = 0; i < count; ++i)
+        if (!(blasRoot[i] < blasEnd[i] && blasEnd[i] <= ctx->B.nodeCount))
+            return fail(ctx, SB_ERR_LAYOUT_VIOLATION, "instance %u BLAS range [%u,%u) invalid", i, blasRoot[i], blasEnd[i]);
+    cudaSetDevice(ctx->device);
+    InstanceTable& I = ctx->I;
+    if (!ctx->instancesSet || I.count != count) {
+        release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb);
+        release(I.invRows); release(I.detSign); release(I.order); release(I.slotOf); release(I.liveBounds);
+        release(I.nodeDepth); release(I.scratch); release(ctx->instOwner);
+        size_t c;
+        c = 0; CK(grow(I.world, c, (size_t)count * 16));
+        c = 0; CK(grow(I.active, c, (size_t)count));
+        c = 0; CK(grow(I.blasRoot, c, (size_t)count));
+        c = 0; CK(grow(I.blasEnd, c, (size_t)count));
+        c = 0; CK(grow(I.aabb, c, (size_t)count * 9));
+        c = 0; CK(grow(I.invRows, c, (size_t)count * 12));
+        c = 0; CK(grow(I.detSign, c, (size_t)count));
+        c = 0; CK(grow(I.order, c, (size_t)count));
+        c = 0; CK(grow(I.slotOf, c, (size_t)count));
+        c = 0; CK(grow(I.liveBounds, c, (size_t)count * 6));
+        c = 0; CK(grow(I.nodeDepth, c, (size_t)ctx->B.tlasNodeCount));
+        c = 0; CK(grow(I.scratch, c, (size_t)4));
+        c = 0; CK(grow(ctx->instOwner, c, (size_t)count));
+        I.count = count;
+    }
+    CK(cudaMemcpyAsync(I.world, world16, (size_t)count * 128, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(I.active, active, count, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(I.blasRoot, blasRoot, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(I.blasEnd, blasEnd, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->instancesSet = true;
+    if (!ctx->tlasPending) {
+        // the uploaded TLAS stays; derive the slot maps from it on the next pack
+        ctx->needPack = true;
+    }
+    return SB_OK;
+}
+
+sb_status sb_build_tlas(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (!ctx->instancesSet) return fail(ctx, SB_ERR_NOT_READY, "sb_set_instances first");
+    if (ctx->I.count > TLAS_BUILD_MAX)
+        return fail(ctx, SB_ERR_UNSUPPORTED, "%u instances > %u (single-CTA TLAS build)", ctx->I.count, TLAS_BUILD_MAX);
+    cudaSetDevice(ctx->device);
+    uint32_t nodes = tlas_nodes_for(ctx->I.count);
+    if (nodes != ctx->B.tlasNodeCount)
+        return fail(ctx, SB_ERR_INVALID_ARG, "TLAS capacity %u != %u nodes", ctx->B.tlasNodeCount, nodes);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    CK(launch_tlas_build(ctx->B, ctx->I, ctx->dErr, ctx->stream));
+    ctx->tlasPending = false;
+    ctx->tlasOnDevice = true;
+    return SB_OK;
+}
+
+sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* src, const double* world16, uint32_t count) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (!ctx->instancesSet || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "instances / TLAS not ready");
+    if (!ctx->tlasOnDevice)
+        return fail(ctx, SB_ERR_NOT_READY, "the transform lane needs the slot order of a TLAS built by sb_build_tlas");
+    if (count && (!src || !world16)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    cudaSetDevice(ctx->device);
+    for (uint32_t i = 0; i < count; ++i)
+        if (src[i] >= ctx->I.count) return fail(ctx, SB_ERR_INVALID_ARG, "instance %u out of range", src[i]);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    if (count) {
+        if (count > ctx->stageCap) {
+            release(ctx->dStage); release(ctx->dStageM);
+            size_t c = 0;
+            CK(grow(ctx->dStage, c, (size_t)count));
+            c = 0;
+            CK(grow(ctx->dStageM, c, (size_t)count * 16));
+            ctx->stageCap = count;
+        }
+        CK(cudaMemcpyAsync(ctx->dStage, src, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->dStageM, world16, (size_t)count * 128, cudaMemcpyHostToDevice, ctx->stream));
+        CK(launch_update_instances(ctx->B, ctx->I, ctx->dStage, ctx->dStageM, count, 1, ctx->dErr, ctx->stream));
+    } else {
+        // rewriteInstanceRows:false — bounds from the (refit) BLAS roots
+        CK(launch_update_instances(ctx->B, ctx->I, nullptr, nullptr, 0, 0, ctx->dErr, ctx->stream));
+    }
+    CK(launch_tlas_refit(ctx->B, ctx->I, ctx->dErr, ctx->stream));
+    return SB_OK;
+}
+
+// ---------------------------------------------------------------- stats
+sb_status sb_enable_counters(sb_ctx* ctx, int32_t on) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    ctx->countersOn = on != 0;
+    return SB_OK;
+}
+
+sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
+    if (!ctx || !out) return SB_ERR_INVALID_ARG;
+    std::memset(out, 0, sizeof *out);
+    cudaSetDevice(ctx->device);
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->countersOn) {
+        unsigned long long c[8];
+        CK(cudaMemcpy(c, ctx->dCounters, 64, cudaMemcpyDeviceToHost));
+        out->primaryRays = c[0];
+        out->shadowRays = c[1];
+        out->tlasNodeVisits = c[2];
+        out->instanceVisits = c[3];
+        out->blasNodeVisits = c[4];
+        out->triangleTests = c[5];
+    }
+    if (ctx->timed) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) out->lastSolveMs = ms;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evMid) == cudaSuccess) out->lastTraceMs = ms;
+        if (cudaEventElapsedTime(&ms, ctx->evMid, ctx->ev1) == cudaSuccess) out->lastBlendMs = ms;
+    }
+    out->kernelLaunches = launches();
+    return SB_OK;
+}
+
+sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out) {
+    if (!ctx || !out) return SB_ERR_INVALID_ARG;
+    out->traceBlock = ctx->tune.block;
+    out->sortKey = ctx->tune.sortKey;
+    out->smemTlasNodes = ctx->tune.smemTlasNodes;
+    out->bvhKind = 0;
+    return SB_OK;
+}
+
+sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
+    if (!ctx || !t) return SB_ERR_INVALID_ARG;
+    if (t->traceBlock == 0 || t->traceBlock > 256 || t->traceBlock % 32)
+        return fail(ctx, SB_ERR_INVALID_ARG, "traceBlock %u: multiple of 32 in [32,256]", t->traceBlock);
+    if (t->bvhKind != 0) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
+    ctx->tune.block = t->traceBlock;
+    ctx->tune.sortKey = t->sortKey;
+    ctx->tune.smemTlasNodes = t->smemTlasNodes;
+    return SB_OK;
+}
+
+}  // extern "C"
+
+extern "C" sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCount,
+                                      const float* vertexData, uint32_t root, uint32_t end) {
+    if (!ctx || (vertexCount && !vertexData)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if ((uint64_t)vertexStart + vertexCount > ctx->B.vertexCount)
+        return fail(ctx, SB_ERR_INVALID_ARG, "vertex range [%u,+%u) outside the pool", vertexStart, vertexCount);
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpyAsync(ctx->B.vertexData + (size_t)vertexStart * 8, vertexData, (size_t)vertexCount * 32,
+                       cudaMemcpyHostToDevice, ctx->stream));
+    return sb_refit_blas(ctx, root, end);
+}

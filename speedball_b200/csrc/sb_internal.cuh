@@ -1,0 +1,106 @@
+// sb_internal.cuh — device-side structures and helpers shared by the CUDA
+// translation units of libspeedball_cuda.so (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include "../../include/speedball_cuda.h"
+
+namespace sb {
+
+// Device error word bits (latched; read back by sb_synchronize).
+enum : uint32_t {
+    ERR_LAYOUT = 1u,      // threaded-layout / index-range violation
+    ERR_WATCHDOG = 2u,    // a bounded loop ran out of iterations
+    ERR_NAN_KEY = 4u,     // NaN TLAS build key (instance AABB)
+    ERR_CAPACITY = 8u,    // a device-side capacity was exceeded
+};
+
+constexpr uint32_t INTERIOR = 0xFFFFFFFFu;
+constexpr float RAY_EPS = 1e-3f;
+constexpr float T_MAX = 1e30f;
+constexpr float PI_F = 3.141592653589793f;
+constexpr int OCT = 6, TILE = 8, BORDER = 1;
+constexpr uint32_t LIGHT_DATA = 64u * 17u;  // records before the C0 cell lists
+
+// Per-triangle accept bits packed in the w lane of the first float4 of a
+// pre-gathered triangle (materialSideAccepts / materialAlphaAccepts /
+// traversal flags, spectral_traverse.js:193-222 with no map bound).
+enum : uint32_t {
+    TB_SIDE_MASK = 3u,      // 0 front, 1 back, 2 double
+    TB_CLOSEST_OK = 4u,     // closest-hit alpha acceptance
+    TB_SHADOW_OK = 8u,      // any-hit: shadow-block flag and alpha acceptance
+};
+
+// Scene as the kernels see it. Reference layouts are kept for refit and
+// read-back; the kernels traverse the derived layouts.
+struct DevScene {
+    const uint4* nodes;        // 2 x uint4 per BLAS node: bmin.xyz bmax.x | bmax.yz miss payload
+    const float4* tris;        // 3 x float4 per triangle: (p0, bits) (e1, -) (e2, -)
+    const uint32_t* triMaterial;
+    const float* materials;    // uber records (28 floats)
+    const float4* inst;        // 4 x float4 per instance slot: 3 inverse rows, (root, end, dSign, active)
+    const uint4* tlas;         // 2 x uint4 per TLAS node, same encoding as BLAS nodes, payload (cnt<<24)|off
+    const float* lights;       // 64 x 17 records (+ C0 cell lists)
+    uint32_t nodeCount, triCount, instCount, tlasNodeCount, materialCount;
+    uint32_t lightCount;
+    int32_t clustered;
+    const uint32_t* valid;     // nonzero when the last pack validated the layout
+};
+
+// One cascade solve as the kernels see it.
+struct DevCascade {
+    float gridMin[3], gridSize[3];
+    uint32_t res[3];
+    uint32_t rays;
+    float maxDist, cellMin;
+    uint32_t probeTotal, atlasW, atlasH;
+    uint32_t probeOffset, updatedCount;
+    // cascade 0's grid, for the clustered cell lookup
+    float g0Min[3], g0Size[3];
+    uint32_t g0Res[3];
+    float4* rayData;           // updatedCount*rays
+    uint4* hits;               // optional 16-byte hit records
+    uint2* vis;                // optional NEE shadow bits
+    float4* irr;               // history, probeTotal*64
+    float2* depth;             // history
+    const uint2* atlasPrev;    // RGBA16F texels as 4 halves (the previous upload)
+    uint2* atlas;              // RGBA16F output
+    uint2* depthAtlas;
+};
+
+struct DevParams {
+    float frameJitter, emitterVisSeed;
+    float hysteresis, hysteresisExponent;
+    float depthSharpness, radianceClamp, classifyStrength;
+    float filterStrength, filterSmooth;
+    float tempChangeSigma1, tempChangeHDrop, tempClampSigma;
+    float nirGate, nirGain;
+    float skyIntensity;
+    float skySH[27];
+    float debugTraceBiasScale, debugRayEpsScale, debugDirectScale, debugEmissiveScale;
+    float debugAlbedoScale, debugBounceScale, debugCosinePower;
+    float debugTempNoiseHBoost, debugTempChangeSigma0, debugTempMinChangeH;
+    float debugTempVarEps, debugTempVarRel, debugDepthHistoryScale;
+    float debugFilterKScale, debugFilterRelScale, debugFilterEpsScale;
+};
+static_assert(sizeof(DevParams) == sizeof(sb_params), "DevParams mirrors sb_params");
+
+__device__ __forceinline__ void latch(uint32_t* err, uint32_t bit) {
+    if (err) atomicOr(err, bit);
+}
+
+// JS Math.min / Math.max on floats: NaN-propagating, -0 < +0 (the interior
+// unions of gi_refit.js use them).
+__device__ __forceinline__ float js_min(float a, float b) {
+    if (a != a || b != b) return __int_as_float(0x7fc00000);
+    if (a == b) return signbit(a) ? a : b;
+    return a < b ? a : b;
+}
+__device__ __forceinline__ float js_max(float a, float b) {
+    if (a != a || b != b) return __int_as_float(0x7fc00000);
+    if (a == b) return signbit(a) ? b : a;
+    return a > b ? a : b;
+}
+
+}  // namespace sb

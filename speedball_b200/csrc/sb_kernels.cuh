@@ -1,0 +1,86 @@
+// sb_kernels.cuh — launcher declarations shared by the host side (sb_ctx.cu).
+#pragma once
+#include "sb_internal.cuh"
+
+namespace sb {
+
+// Process-wide count of kernels this library launched (reported in sb_stats).
+void note_launch();
+uint64_t launches();
+
+struct TraceTuning {
+    uint32_t block;          // threads per block of the trace kernel
+    uint32_t smemTlasNodes;  // stage the TLAS in shared memory when it has at most this many nodes
+    uint32_t sortKey;        // ray issue order (0 = probe-major)
+    int numSms;
+};
+
+// Scene buffers in the reference layouts plus the derived layouts.
+struct SceneBuffers {
+    uint32_t* nodes = nullptr;        // nodeCount*8
+    uint32_t* triIndex = nullptr;     // triCount*3
+    float* vertexData = nullptr;      // vertexCount*8
+    uint32_t* triMaterial = nullptr;  // triCount
+    float* materials = nullptr;       // materialsLen
+    float* lights = nullptr;          // lightsLen
+    float4* tris = nullptr;           // derived, triCount*3
+    float4* inst = nullptr;           // derived, instCount*4
+    uint4* tlas = nullptr;            // derived, tlasNodeCount*2
+    uint32_t* matBits = nullptr;      // derived, per material accept bits
+    uint32_t* parent = nullptr;       // nodeCount: parent of each BLAS node (refit)
+    uint32_t* arrive = nullptr;       // nodeCount: refit arrival counters
+    uint32_t* valid = nullptr;        // 1 word
+    uint32_t nodeCount = 0, triCount = 0, vertexCount = 0, materialsLen = 0, materialCount = 0;
+    uint32_t instBase = 0, instCount = 0, tlasBase = 0, tlasNodeCount = 0, lightsLen = 0;
+};
+
+cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
+                         unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st);
+cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
+cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st);
+cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st);
+
+// Validation + derived-layout packing (sb_pack.cu).
+cudaError_t launch_pack_scene(const SceneBuffers& B, uint32_t* err, cudaStream_t st);
+cudaError_t launch_pack_tris(const SceneBuffers& B, uint32_t triBegin, uint32_t triEnd, uint32_t* err, cudaStream_t st);
+cudaError_t launch_pack_dynamic(const SceneBuffers& B, uint32_t* err, cudaStream_t st);
+
+// Refit and TLAS lanes (sb_refit.cu).
+cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
+                              cudaStream_t st);
+
+struct InstanceTable {
+    double* world = nullptr;       // 16 per source instance (column-major)
+    uint8_t* active = nullptr;
+    uint32_t* blasRoot = nullptr;
+    uint32_t* blasEnd = nullptr;
+    double* aabb = nullptr;        // 9 per source instance: min, max, centroid
+    float* invRows = nullptr;      // 12 per source instance
+    float* detSign = nullptr;
+    uint32_t* order = nullptr;     // slot -> source
+    uint32_t* slotOf = nullptr;    // source -> slot
+    float* liveBounds = nullptr;   // 6 per slot
+    uint32_t* nodeDepth = nullptr; // TLAS node depth (level-order refit)
+    uint32_t* scratch = nullptr;   // TLAS build scratch
+    uint32_t count = 0;
+    uint32_t maxDepth = 0;
+};
+constexpr uint32_t TLAS_BUILD_MAX = 4096;  // instances per single-CTA TLAS build
+
+cudaError_t launch_tlas_build(const SceneBuffers& B, const InstanceTable& I, uint32_t* err, cudaStream_t st);
+// srcList/world16 are device arrays (count entries); srcList == null updates every
+// source instance from its stored matrix (rewriteRows = 0 after a BLAS refit).
+cudaError_t launch_update_instances(const SceneBuffers& B, const InstanceTable& I, const uint32_t* srcList,
+                                    const double* world16, uint32_t count, int rewriteRows, uint32_t* err,
+                                    cudaStream_t st);
+cudaError_t launch_tlas_refit(const SceneBuffers& B, const InstanceTable& I, uint32_t* err, cudaStream_t st);
+cudaError_t launch_tlas_index(const SceneBuffers& B, const InstanceTable& I, uint32_t* owner, uint32_t* err,
+                              cudaStream_t st);
+
+// Arbitrary-ray queries through the same traversal (raycastFirst-like).
+cudaError_t launch_raycast(const DevScene& S, const float* ro, const float* rd, uint32_t n, float* tOut,
+                           int32_t* triOut, int32_t* instOut, uint32_t* err, cudaStream_t st);
+cudaError_t launch_occluded(const DevScene& S, const float* ro, const float* rd, const float* maxDist, uint32_t n,
+                            uint8_t* out, uint32_t* err, cudaStream_t st);
+
+}  // namespace sb

@@ -1,0 +1,535 @@
+"""Host mirror of the reference's probe-field facade, driving the CUDA library.
+
+``createProbeField`` mirrors gi_probes.js:945-4846 and ``installSpeedballGI``
+mirrors install.js:216-503 for the update path: the same entry names, option
+names and defaults, the same per-tick scheduling (round-robin probe cursor,
+ray budget, jitter epochs, hysteresis exponent; gi_probes.js:2947-2962,
+3732-3840) and the same dirty lanes (``markTransformsDirty``,
+``markDeformsDirty``, ``markMaterialValuesDirty``, ``markTopologyDirty``;
+3869-3937). Scenes are ``speedball_b200.scene.SceneDesc`` instead of a three.js
+scene; every device step goes through libspeedball_cuda.so.
+
+Not mirrored (outside the update path): the raster lights node, the material
+graph receiver, reflection lobes, probe classification/relocation, the
+frame-pacing auto-throttle and the idle gate of structural rebuilds.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Callable
+
+import numpy as np
+
+from . import _abi
+from .scene import SceneDesc, build_pool, column_major
+
+TILE = 8
+MAX_PROBES_PER_AXIS = 32
+TARGET_PROBES_LONG_AXIS = 12
+RAYS_PER_PROBE_DEFAULT = 64
+RAYS_MIN, RAYS_MAX = 32, 256
+RAYS_PER_TICK = 98_304
+MAX_PROBES_PER_TICK = 2048
+MAX_RAY_BUDGET = 524_288
+MAX_LIGHTS = 64
+GI_EMITTER_INJECT_CAP = 16
+SURFACE_NORMAL_BIAS_CELL = 0.03
+JITTER_HYSTERESIS_DEFAULTS = {"gated": 0.60, "montecarlo": 0.90}
+HYSTERESIS_DT_REF_MS = 1000.0 / 60.0
+
+
+def hysteresisExponentForInterval(updateDtMs: float, normalize: bool = True) -> float:
+    """gi_probes.js:235-251."""
+    if not normalize:
+        return 1.0
+    dt = max(0.0, updateDtMs) if math.isfinite(updateDtMs) else HYSTERESIS_DT_REF_MS
+    return min(1.0, dt / HYSTERESIS_DT_REF_MS)
+
+
+def probeUpdateIntervalTicks(probeTotal, probesPerTick, solveEveryTicks=1) -> float:
+    """gi_probes.js:197-202."""
+    total = max(0.0, float(probeTotal or 0))
+    cap = max(1.0, float(probesPerTick or 1))
+    schedule = max(1.0, float(solveEveryTicks or 1))
+    return schedule * max(1.0, total / cap)
+
+
+def computeGridResolution(size, targetLongAxis=TARGET_PROBES_LONG_AXIS):
+    """gi_probes.js:938-943 (Math.round = floor(x + 0.5))."""
+    longest = max(size[0], size[1], size[2], 1e-3)
+    spacing = longest / max(1, targetLongAxis)
+    return tuple(int(min(MAX_PROBES_PER_AXIS, max(2, math.floor(s / spacing + 0.5) + 1))) for s in size)
+
+
+def _normalize_jitter_mode(mode) -> str:
+    m = str(mode or "").lower().replace(" ", "").replace("_", "").replace("-", "")
+    return "montecarlo" if m in ("montecarlo", "mc") else "gated"
+
+
+def selectGiLightRecords(records: np.ndarray, importanceRanked: bool, gridMin=None, gridMax=None):
+    """gi_probes.js:4262-4289: analytic records first (importance top-K when
+    clustered), then the emitter suffix (type 3)."""
+    recs = [np.asarray(r, np.float32) for r in np.asarray(records, np.float32).reshape(-1, 17)]
+    analytic = [r for r in recs if r[0] < 2.5]
+    emitters = [r for r in recs if abs(r[0] - 3) < 0.5]
+    emitter_count = min(GI_EMITTER_INJECT_CAP, len(emitters))
+    budget = MAX_LIGHTS - emitter_count
+    if importanceRanked and len(analytic) > budget:
+        def score(rec):
+            if rec[0] < 0.5:
+                return math.inf
+            power = max(rec[7], rec[8], rec[9])
+            cone = max(0.02, (1 - rec[12]) * 0.5) if abs(rec[0] - 2) < 0.5 else 1.0
+            d = [max(gridMin[a] - rec[1 + a], 0.0, rec[1 + a] - gridMax[a]) for a in range(3)]
+            return (power * cone) / (1 + d[0] ** 2 + d[1] ** 2 + d[2] ** 2)
+        ranked = sorted(range(len(analytic)), key=lambda i: (-score(analytic[i]), i))[:budget]
+        selected = [analytic[i] for i in ranked]
+    else:
+        selected = analytic[:budget]
+    out = selected + emitters[:emitter_count]
+    arr = np.stack(out) if out else np.zeros((0, 17), np.float32)
+    return arr, len(selected), emitter_count
+
+
+class ProbeField:
+    """createProbeField (gi_probes.js:945) over one scene and one GPU."""
+
+    def __init__(self, scene: SceneDesc, *, intensity=1.0, hysteresis=None, jitterMode="gated", divisions=12,
+                 rays=RAYS_PER_PROBE_DEFAULT, cascades=2, clusteredLighting=False, volumes=None, device=0,
+                 recordHits=False, onRebuilt: Callable | None = None):
+        self._lib = _abi.load()
+        self._scene = scene
+        self._intensity = float(intensity)
+        self._jitterMode = _normalize_jitter_mode(jitterMode)
+        base_h = hysteresis if (hysteresis is not None and math.isfinite(hysteresis)) else \
+            JITTER_HYSTERESIS_DEFAULTS[self._jitterMode]
+        self._hysteresis = min(0.99, max(0.0, float(base_h)))
+        self._targetLongAxis = int(min(MAX_PROBES_PER_AXIS, max(2, round(divisions) or TARGET_PROBES_LONG_AXIS)))
+        self._rays = int(min(RAYS_MAX, max(RAYS_MIN, round(float(rays) / 16) * 16 or RAYS_PER_PROBE_DEFAULT)))
+        # one cascade is solved here; C1 placement (fitFineBox) is outside the built scope
+        self._cascades = 1
+        self._clustered = clusteredLighting is True or isinstance(clusteredLighting, dict)
+        self._volumes = volumes
+        self._rayBudget = RAYS_PER_TICK
+        self._maxProbesPerTick = MAX_PROBES_PER_TICK
+        self._hysteresisNormalize = True
+        self._frameCounter = 0
+        self._probeCursor = 0
+        self._lastSolveAt = 0.0
+        self._solveDtEma = 0.0
+        self._disposed = False
+        self._onRebuilt = onRebuilt
+        self._pendingTransforms: set[int] = set()
+        self._pendingAllTransforms = False
+        self._pendingDeform = False
+        self._pendingMaterials: set[int] = set()
+        self._pendingTopology = False
+        self._deformVersions = {}
+        self._staging = {}
+        self._params = _abi.default_params()
+        self._params.hysteresis = self._hysteresis
+        self._frameJitterOverride = None
+        flags = _abi.SB_CTX_RECORD_HITS if recordHits else 0
+        opts = _abi.sb_device_opts(device, flags)
+        h = C.c_void_p()
+        _abi.check(self._lib.sb_create(C.byref(opts), C.byref(h)))
+        self._ctx = h
+        self.stats = {"solves": 0, "refits": 0, "transformUpdates": 0, "rebuilds": 0}
+        self._rebuild()
+
+    # ------------------------------------------------------------- plumbing
+    def _ck(self, status):
+        _abi.check(status, self._ctx)
+
+    def _rebuild(self):
+        """rebuild() (gi_probes.js:3269-3455): pool, upload, TLAS, grid fit, lights."""
+        lib = self._lib
+        self._pool = pool = build_pool(self._scene)
+        self._ck(lib.sb_upload_scene(self._ctx, C.byref(pool.view())))
+        self._ck(lib.sb_set_instances(self._ctx, pool.instCount, _abi.ptr(pool.inst_world),
+                                      _abi.ptr(pool.inst_active), _abi.ptr(pool.inst_root), _abi.ptr(pool.inst_end)))
+        self._ck(lib.sb_build_tlas(self._ctx))
+        self._deformVersions = {i: self._version(m) for i, m in enumerate(self._scene.meshes)}
+        self._fit_grid()
+        self._upload_lights()
+        self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
+        self._probeCursor = 0
+        self.stats["rebuilds"] += 1
+        if self._onRebuilt:
+            self._onRebuilt()
+
+    @staticmethod
+    def _version(mesh):
+        """Identity of a mesh's position data (the attribute version of the reference,
+        spectral_scene.js:1846-1861): the array object plus an explicit counter."""
+        return (id(mesh.positions), getattr(mesh, "version", 0))
+
+    def _scene_bounds(self):
+        lo = np.full(3, np.inf)
+        hi = np.full(3, -np.inf)
+        for inst in self._scene.instances:
+            if not inst.active:
+                continue
+            P = self._scene.meshes[inst.mesh].positions.astype(np.float64)
+            W = inst.world
+            Q = P @ W[:3, :3].T + W[:3, 3]
+            lo = np.minimum(lo, Q.min(0))
+            hi = np.maximum(hi, Q.max(0))
+        return lo, hi
+
+    def _fit_grid(self):
+        """C0 placement (gi_probes.js:3341-3367): manual volume or padded scene bounds."""
+        vol = self._volumes
+        if vol:
+            box_min = np.asarray(vol["gridMin"], np.float64)
+            size = np.asarray(vol["gridSize"], np.float64)
+            res = tuple(int(min(MAX_PROBES_PER_AXIS, max(2, round(r)))) for r in vol["res"]) if vol.get("res") \
+                else computeGridResolution(size, self._targetLongAxis)
+        else:
+            lo, hi = self._scene_bounds()
+            size = hi - lo
+            pad = size * 0.06
+            box_min = lo - pad
+            size = size + 2 * pad
+            res = computeGridResolution(size, self._targetLongAxis)
+        g = _abi.sb_grid()
+        for a in range(3):
+            g.gridMin[a] = float(box_min[a])
+            g.gridSize[a] = float(size[a])
+            g.res[a] = int(res[a])
+        g.raysPerProbe = self._rays
+        gs = np.array([g.gridSize[a] for a in range(3)], np.float64)
+        g.maxDist = float(np.linalg.norm(gs))
+        g.cellMin = float(max(1e-4, min(gs[a] / max(1, res[a] - 1) for a in range(3))))
+        self._grid = g
+        self._res = res
+        self._probeTotal = int(res[0] * res[1] * res[2])
+        self._ck(self._lib.sb_configure_cascade(self._ctx, 0, C.byref(g)))
+
+    def _upload_lights(self):
+        gmin = [self._grid.gridMin[a] for a in range(3)]
+        gmax = [self._grid.gridMin[a] + self._grid.gridSize[a] for a in range(3)]
+        recs, analytic, emitters = selectGiLightRecords(self._scene.lights, self._clustered, gmin, gmax)
+        recs = np.ascontiguousarray(recs, np.float32)
+        self._lightCount = recs.shape[0]
+        self._ck(self._lib.sb_upload_lights(self._ctx, _abi.ptr(recs) if recs.size else None, recs.shape[0],
+                                            analytic, emitters, 1 if self._clustered else 0))
+
+    # ------------------------------------------------------------ scheduling
+    def updatedCap(self) -> int:
+        """gi_probes.js:2947-2958."""
+        return max(1, min(self._maxProbesPerTick, self._rayBudget // max(1, self._rays)))
+
+    def tick(self, idleMs: float = math.inf, playing: bool = False, nowMs: float | None = None) -> dict:
+        """One tick: dirty lanes, then one solve of C0 (gi_probes.js:3472-3849)."""
+        if self._disposed:
+            return {}
+        lib = self._lib
+        if self._pendingTopology:
+            self._pendingTopology = False
+            self._rebuild()
+        self._refresh_lanes()
+        C0 = 0
+        updated = min(self.updatedCap(), self._probeTotal)
+        if nowMs is not None and self._lastSolveAt > 0:
+            dt = nowMs - self._lastSolveAt
+            self._solveDtEma = (self._solveDtEma * 0.8 + dt * 0.2 if self._solveDtEma > 0 else dt) \
+                if 0 < dt < 200 else 0.0
+        serviceDt = self._solveDtEma if self._solveDtEma > 0 else HYSTERESIS_DT_REF_MS
+        revisit = probeUpdateIntervalTicks(self._probeTotal, updated)
+        self._params.hysteresisExponent = hysteresisExponentForInterval(serviceDt * revisit, self._hysteresisNormalize)
+        if self._jitterMode == "montecarlo":
+            self._frameCounter = (self._frameCounter + 1) & 0xFFFFFFFF
+            self._params.frameJitter = self._frameJitterOverride if self._frameJitterOverride is not None \
+                else (self._frameCounter * 0.61803398875) % 1
+        elif self._frameJitterOverride is not None:
+            self._params.frameJitter = self._frameJitterOverride
+        self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
+        offset = self._probeCursor
+        self._ck(lib.sb_solve(self._ctx, C0, offset, updated))
+        self._probeCursor = (self._probeCursor + updated) % self._probeTotal if self._probeTotal else 0
+        if nowMs is not None:
+            self._lastSolveAt = nowMs
+        self.stats["solves"] += 1
+        return {"cascade": C0, "probeOffset": offset, "updatedCount": updated}
+
+    def _refresh_lanes(self):
+        lib = self._lib
+        if self._pendingMaterials:
+            ub = np.ascontiguousarray(self._scene.materials, np.float32).reshape(-1)
+            for m in sorted(self._pendingMaterials):
+                rec = np.ascontiguousarray(ub[m * 28:(m + 1) * 28])
+                self._ck(lib.sb_upload_range(self._ctx, _abi.BUF["MATERIALS"], m * 28, 28, _abi.ptr(rec)))
+            self._pendingMaterials.clear()
+        if self._pendingDeform:
+            self._pendingDeform = False
+            self.refreshDeforms()
+        if self._pendingAllTransforms or self._pendingTransforms:
+            idx = range(len(self._scene.instances)) if self._pendingAllTransforms else sorted(self._pendingTransforms)
+            self._pendingAllTransforms = False
+            self._pendingTransforms.clear()
+            self.refreshTransforms(list(idx))
+
+    def refreshTransforms(self, instances):
+        """refreshTransforms -> updateTransforms (gi_probes.js:4164-4179, spectral_scene.js:1402-1514)."""
+        if not instances:
+            return
+        src = np.ascontiguousarray(np.asarray(instances, np.uint32))
+        world = np.ascontiguousarray(np.stack([column_major(self._scene.instances[i].world) for i in instances]))
+        self._ck(self._lib.sb_update_transforms(self._ctx, _abi.ptr(src), _abi.ptr(world), src.shape[0]))
+        self.stats["transformUpdates"] += 1
+
+    def refreshDeforms(self, meshes=None):
+        """refreshDeforms -> updateDeforms (gi_probes.js:4209-4234, spectral_scene.js:1831-1927):
+        re-gather each deformed mesh's pooled vertices, refit its BLAS on the GPU,
+        then carry the new root bounds into the TLAS (rewriteInstanceRows:false)."""
+        pool = self._pool
+        if meshes is None:
+            # same-topology deforms only: a mesh counts as changed when its positions
+            # array was replaced or written since the last refresh
+            changed = [i for i, m in enumerate(self._scene.meshes) if self._version(m) != self._deformVersions.get(i)]
+        else:
+            changed = list(meshes)
+        n = 0
+        for i in changed:
+            m = self._scene.meshes[i]
+            if m.positions.shape[0] != int(pool.vert_count[i]):
+                raise _abi.SbError(_abi.SB_ERR_LAYOUT_VIOLATION, f"mesh {i}: vertex count changed (topology edit)")
+            self._deformVersions[i] = self._version(m)
+            stage = self._staging.get(i)
+            if stage is None or stage.array.shape[0] != m.positions.shape[0]:
+                stage = _abi.PinnedArray((m.positions.shape[0], 8), np.float32)
+                self._staging[i] = stage
+            vd = stage.array
+            vd[:, 0:3] = m.positions
+            if m.normals is not None:
+                vd[:, 3:6] = m.normals
+            if m.uvs is not None:
+                vd[:, 6:8] = m.uvs
+            self._ck(self._lib.sb_update_deform(self._ctx, int(pool.vert_base[i]), int(pool.vert_count[i]),
+                                                _abi.ptr(vd), int(pool.blas_root[i]), int(pool.blas_end[i])))
+            n += 1
+        if n:
+            self._ck(self._lib.sb_update_transforms(self._ctx, None, None, 0))
+            self.stats["refits"] += n
+
+    # ------------------------------------------------------------ dirty API
+    def markTransformsDirty(self, target=None):
+        """gi_probes.js:3869-3878: an instance index, {'object': i}, a list, or None for all."""
+        if target is None:
+            self._pendingAllTransforms = True
+            return
+        targets = target if isinstance(target, (list, tuple, set)) else [target]
+        for t in targets:
+            i = t.get("object", t.get("instanceIndex")) if isinstance(t, dict) else t
+            if isinstance(i, (int, np.integer)) and 0 <= i < len(self._scene.instances):
+                self._pendingTransforms.add(int(i))
+
+    def markDeformsDirty(self):
+        self._pendingDeform = True
+
+    def markMaterialValuesDirty(self, targets=None):
+        n = np.asarray(self._scene.materials).reshape(-1, 28).shape[0]
+        if targets is None:
+            self._pendingMaterials.update(range(n))
+        else:
+            for t in (targets if isinstance(targets, (list, tuple, set)) else [targets]):
+                if 0 <= int(t) < n:
+                    self._pendingMaterials.add(int(t))
+
+    def markTopologyDirty(self):
+        self._pendingTopology = True
+
+    def notifySceneChange(self, change: dict | None = None):
+        change = change or {}
+        if change.get("topology"):
+            self.markTopologyDirty()
+        if change.get("transforms") is not None:
+            self.markTransformsDirty(change.get("transforms") or None)
+        if change.get("deforms"):
+            self.markDeformsDirty()
+        if change.get("materials") is not None:
+            self.markMaterialValuesDirty(change.get("materials") or None)
+
+    # -------------------------------------------------------------- setters
+    def setHysteresis(self, h):
+        self._hysteresis = min(0.99, max(0.0, float(h)))
+        self._params.hysteresis = self._hysteresis
+
+    def getHysteresis(self):
+        return self._hysteresis
+
+    def setHysteresisNormalization(self, on):
+        self._hysteresisNormalize = on is not False
+
+    def setJitterMode(self, mode):
+        self._jitterMode = _normalize_jitter_mode(mode)
+
+    def getJitterMode(self):
+        return self._jitterMode
+
+    def setRayBudget(self, rays, maxProbesPerTick=None):
+        self._rayBudget = int(min(MAX_RAY_BUDGET if maxProbesPerTick is None else 1 << 30, max(2048, int(rays))))
+        if maxProbesPerTick is not None:
+            self._maxProbesPerTick = max(1, int(maxProbesPerTick))
+
+    def getRayBudget(self):
+        return self._rayBudget
+
+    def setRadianceClamp(self, v):
+        self._params.radianceClamp = max(0.0, float(v))
+
+    def setDepthSharpness(self, v):
+        self._params.depthSharpness = max(0.01, float(v))
+
+    def setFilterStrength(self, v):
+        self._params.filterStrength = min(1.0, max(0.0, float(v)))
+
+    def setSmoothness(self, v):
+        self._params.filterSmooth = min(1.0, max(0.0, float(v)))
+
+    def setSky(self, sh9=None):
+        sh = np.zeros(27, np.float32) if sh9 is None else np.asarray(sh9, np.float32).reshape(27)
+        for i in range(27):
+            self._params.skySH[i] = float(sh[i])
+
+    def setSkyIntensity(self, v):
+        self._params.skyIntensity = max(0.0, float(v))
+
+    def setNirSensing(self, on):
+        self._params.nirGate = 1.0 if on else 0.0
+
+    def setDebugKnobs(self, **knobs):
+        for k, v in knobs.items():
+            if k == "frameJitter":
+                self._frameJitterOverride = None if v is None else float(v)
+            elif hasattr(self._params, k):
+                setattr(self._params, k, float(v))
+            else:
+                raise KeyError(k)
+
+    def getResolution(self):
+        return tuple(self._res)
+
+    def getRays(self):
+        return self._rays
+
+    def getStats(self):
+        st = _abi.sb_stats()
+        self._ck(self._lib.sb_get_stats(self._ctx, C.byref(st)))
+        d = dict(self.stats)
+        d.update(probeTotal=self._probeTotal, rays=self._rays, lastSolveMs=st.lastSolveMs)
+        return d
+
+    # ------------------------------------------------------------- read-back
+    def synchronize(self):
+        self._ck(self._lib.sb_synchronize(self._ctx))
+
+    def _debugRead(self, which: str, cascade: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Read a device buffer (the _debugRead seam, gi_probes.js:4830-4841).
+        `out` may be a preallocated (e.g. page-locked) array of the right shape."""
+        r = self._res
+        W, H = r[0] * TILE, r[1] * r[2] * TILE
+        P = self._probeTotal
+        shapes = {"atlas": ((H, W, 4), np.uint16, "IRRADIANCE_ATLAS"),
+                  "depthAtlas": ((H, W, 4), np.uint16, "DEPTH_ATLAS"),
+                  "irr": ((P * 64, 4), np.float32, "IRRADIANCE_HISTORY"),
+                  "depth": ((P * 64, 2), np.float32, "DEPTH_HISTORY")}
+        shape, dt, key = shapes[which]
+        if out is None:
+            out = np.zeros(shape, dt)
+        assert out.shape == shape and out.dtype == dt and out.flags["C_CONTIGUOUS"]
+        self._ck(self._lib.sb_read_buffer(self._ctx, _abi.BUF[key] | (cascade << 8), 0, out.size, _abi.ptr(out)))
+        return out
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    @property
+    def pool(self):
+        return self._pool
+
+    @property
+    def grid(self):
+        return self._grid
+
+    def dispose(self):
+        if self._disposed:
+            return
+        self._disposed = True
+        self._lib.sb_destroy(self._ctx)
+        self._ctx = None
+        for st in self._staging.values():
+            st.free()
+        self._staging.clear()
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+def createProbeField(scene: SceneDesc, **opts) -> ProbeField:
+    return ProbeField(scene, **opts)
+
+
+class SpeedballGIHandle:
+    """The object installSpeedballGI returns (install.js:362-503), update path only."""
+
+    def __init__(self, field: ProbeField, onError=None):
+        self._gi = field
+        self._onError = onError
+        self._disposed = False
+        self._failureWarned = False
+        self.advanced = {"field": field, "tick": field.tick, "setDebugKnobs": field.setDebugKnobs,
+                         "debug": {"read": field._debugRead, "state": field.getStats}}
+
+    def update(self, camera=None, playing=False):
+        """install.js:364-385: tick, and report failures once per failure streak."""
+        if self._disposed:
+            return None
+        try:
+            r = self._gi.tick(playing=playing)
+            self._failureWarned = False
+            return r
+        except Exception as e:  # routed like the reference's promise rejection
+            if self._failureWarned:
+                return None
+            self._failureWarned = True
+            if self._onError:
+                self._onError(e)
+            return None
+
+    def __getattr__(self, name):
+        gi = self.__dict__.get("_gi")
+        if gi is None or name.startswith("_"):
+            raise AttributeError(name)
+        target = getattr(gi, name)
+        if callable(target) and name.startswith(("set", "mark", "notify")):
+            def guarded(*a, **k):
+                if self._disposed:
+                    return None
+                return target(*a, **k)
+            return guarded
+        return target
+
+    def dispose(self):
+        if self._disposed:
+            return
+        self._disposed = True
+        self._gi.dispose()
+
+
+def installSpeedballGI(scene: SceneDesc, *, enabled=True, intensity=10, divisions=16, rays=64, cascades=2,
+                       hysteresis=None, jitterMode="gated", clusteredLighting=False, volumes=None, device=0,
+                       onError=None, **_ignored) -> SpeedballGIHandle:
+    """install.js:216-239 with the renderer/camera replaced by the scene description."""
+    if onError is not None and not callable(onError):
+        raise TypeError("installSpeedballGI: onError must be a function when provided.")
+    field = createProbeField(scene, intensity=intensity, hysteresis=hysteresis, jitterMode=jitterMode,
+                             divisions=divisions, rays=rays, cascades=cascades, clusteredLighting=clusteredLighting,
+                             volumes=volumes, device=device)
+    return SpeedballGIHandle(field, onError)

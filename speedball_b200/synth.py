@@ -1,0 +1,281 @@
+"""Seeded synthetic scenes for the probe-update workloads.
+
+No public dataset is involved: the reference's Sponza mesh is absent from its
+tree, so the 262k-triangle atrium below stands in for it at the same scale.
+Every scene is a pure function of its seed (numpy PCG64).
+
+  room_spheres   10 m box room (12 triangles) + 64 icospheres (subdivision 3,
+                 1280 triangles, radius U[0.2,0.8]); one BLAS per mesh, 65
+                 instances; 16 Lambertian materials; 1 directional + 4 point
+                 lights; 8^3 probes, 64 rays.
+  atrium         262,267 triangles in 30 meshes (log-uniform 500-60k) of
+                 column prisms, arched wall panels and subdivided floor slabs;
+                 25 materials; 1 directional + 32 point lights (clustered);
+                 16^3 probes, 64 rays; 3 rigid movers and 1 deforming mesh.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .scene import Instance, Mesh, SceneDesc, light_record, material_record
+
+
+# ----------------------------------------------------------------- meshes
+def icosphere(subdiv: int, radius: float = 1.0):
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in v]
+    faces = list(f)
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    P = np.array(verts) * radius
+    F = np.array(faces, dtype=np.uint32)
+    return P.astype(np.float32), F, (np.array(verts)).astype(np.float32)
+
+
+def box_room(size: float):
+    """Inward-facing box [0,size]^3 (front faces toward the interior)."""
+    s = size
+    P = np.array([(0, 0, 0), (s, 0, 0), (s, s, 0), (0, s, 0), (0, 0, s), (s, 0, s), (s, s, s), (0, s, s)],
+                 dtype=np.float32)
+    # outward CCW quads, then reversed for an inward front face
+    quads = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (3, 7, 6, 2), (0, 4, 7, 3), (1, 2, 6, 5)]
+    F = []
+    for a, b, c, d in quads:
+        F += [(a, c, b), (a, d, c)]
+    return P, np.array(F, dtype=np.uint32)
+
+
+def grid_mesh(nu: int, nv: int, fn):
+    """Parametric grid (nu x nv quads) -> positions and CCW triangles; fn(u, v) -> (x, y, z)."""
+    u = np.linspace(0.0, 1.0, nu + 1)
+    v = np.linspace(0.0, 1.0, nv + 1)
+    U, V = np.meshgrid(u, v, indexing="xy")
+    P = np.stack(fn(U, V), axis=-1).reshape(-1, 3).astype(np.float32)
+    i = np.arange(nu)[None, :] + (nu + 1) * np.arange(nv)[:, None]
+    a, b, c, d = i, i + 1, i + nu + 2, i + nu + 1
+    F = np.concatenate([np.stack([a, b, c], -1).reshape(-1, 3), np.stack([a, c, d], -1).reshape(-1, 3)], 0)
+    # interleave so truncation removes whole rows last
+    F = np.stack([np.stack([a, b, c], -1), np.stack([a, c, d], -1)], -2).reshape(-1, 3)
+    return P, F.astype(np.uint32)
+
+
+def _dims_for(n_tris: int, aspect: float):
+    quads = (n_tris + 1) // 2
+    nv = max(1, int(round(math.sqrt(quads / aspect))))
+    nu = max(1, -(-quads // nv))
+    return nu, nv
+
+
+def column_prism(n_tris: int, rng):
+    """Extruded n-gon column with sinusoidal fluting: a closed tube grid."""
+    sides = int(rng.integers(6, 17))
+    radius = float(rng.uniform(0.25, 0.7))
+    height = float(rng.uniform(4.0, 12.0))
+    nu, nv = _dims_for(n_tris, aspect=sides / 4.0)
+    flute = float(rng.uniform(0.0, 0.06))
+
+    def fn(u, v):
+        a = u * 2 * math.pi
+        r = radius * (1.0 + flute * np.cos(a * sides))
+        return r * np.cos(a), v * height, r * np.sin(a)
+    P, F = grid_mesh(nu, nv, fn)
+    return P, F[:n_tris]
+
+
+def arched_panel(n_tris: int, rng):
+    """Wall panel with an arched top edge, slightly curved in depth."""
+    w = float(rng.uniform(4.0, 12.0))
+    h = float(rng.uniform(4.0, 10.0))
+    arch = float(rng.uniform(0.5, 2.5))
+    bow = float(rng.uniform(0.0, 0.6))
+    nu, nv = _dims_for(n_tris, aspect=w / h)
+
+    def fn(u, v):
+        x = (u - 0.5) * w
+        top = h + arch * np.sin(np.pi * u)
+        return x, v * top, bow * np.sin(np.pi * u) * (1.0 - v)
+    P, F = grid_mesh(nu, nv, fn)
+    return P, F[:n_tris]
+
+
+def floor_slab(n_tris: int, rng):
+    """Rectangular slab, 2-level subdivided grid with a shallow relief."""
+    w = float(rng.uniform(6.0, 20.0))
+    d = float(rng.uniform(6.0, 20.0))
+    relief = float(rng.uniform(0.0, 0.05))
+    nu, nv = _dims_for(n_tris, aspect=w / d)
+
+    def fn(u, v):
+        return (u - 0.5) * w, relief * np.sin(13.0 * u) * np.cos(11.0 * v), (v - 0.5) * d
+    P, F = grid_mesh(nu, nv, fn)
+    # slabs face up: CCW seen from +y
+    F = F[:, [0, 2, 1]]
+    return P, F[:n_tris]
+
+
+def _rot(axis, ang):
+    axis = np.asarray(axis, np.float64)
+    axis = axis / np.linalg.norm(axis)
+    x, y, z = axis
+    c, s = math.cos(ang), math.sin(ang)
+    C = 1 - c
+    return np.array([[c + x * x * C, x * y * C - z * s, x * z * C + y * s],
+                     [y * x * C + z * s, c + y * y * C, y * z * C - x * s],
+                     [z * x * C - y * s, z * y * C + x * s, c + z * z * C]])
+
+
+def trs(t, r=None, s=1.0):
+    m = np.eye(4)
+    m[:3, :3] = (r if r is not None else np.eye(3)) * s
+    m[:3, 3] = t
+    return m
+
+
+# ----------------------------------------------------------------- scenes
+def room_spheres(seed: int = 0, n_materials: int = 16, n_point: int = 4):
+    """The 82k-triangle room + 64 icospheres scene (plain DDGI, CPU-checkable size)."""
+    rng = np.random.default_rng(seed)
+    S = 10.0
+    meshes, instances = [], []
+    mats = [material_record(rng.uniform(0.1, 0.9, 3)) for _ in range(n_materials)]
+    P, F = box_room(S)
+    meshes.append(Mesh(P, F, np.full(F.shape[0], rng.integers(n_materials), np.uint32)))
+    instances.append(Instance(0, np.eye(4)))
+    unit, uf, un = icosphere(3)
+    for i in range(64):
+        r = float(rng.uniform(0.2, 0.8))
+        c = rng.uniform(0.0, S, 3)
+        m = int(rng.integers(n_materials))
+        meshes.append(Mesh(unit * r, uf, np.full(uf.shape[0], m, np.uint32), normals=un))
+        instances.append(Instance(len(meshes) - 1, trs(c)))
+    lights = []
+    d = rng.normal(size=3)
+    d /= np.linalg.norm(d)
+    lights.append(light_record(0, pos=(5, 5, 5), direction=tuple(d), intensity=3.0))
+    for _ in range(n_point):
+        lights.append(light_record(1, pos=tuple(rng.uniform(0.0, S, 3)), intensity=float(rng.uniform(5, 20)),
+                                   range_=8.0, decay=2.0))
+    grid = dict(gridMin=(0.5, 0.5, 0.5), gridSize=(9.0, 9.0, 9.0), res=(8, 8, 8), rays=64)
+    return SceneDesc(meshes, instances, np.stack(mats), np.stack(lights), name="room_spheres",
+                     meta=dict(grid=grid, clustered=False, hysteresis=0.97, jitter="gated", seed=seed))
+
+
+ATRIUM_TRIS = 262_267
+
+
+def atrium(seed: int = 1, total_tris: int = ATRIUM_TRIS, n_meshes: int = 30, n_materials: int = 25,
+           n_point: int = 32):
+    """Sponza-scale procedural atrium (262,267 triangles in 30 meshes)."""
+    rng = np.random.default_rng(seed)
+    W, H, D = 40.0, 20.0, 30.0
+    raw = np.exp(rng.uniform(math.log(500), math.log(60_000), n_meshes))
+    counts = np.maximum(500, np.round(raw * total_tris / raw.sum())).astype(np.int64)
+    counts = np.minimum(counts, 60_000)
+    diff = total_tris - int(counts.sum())
+    order = np.argsort(-counts)
+    k = 0
+    while diff != 0:
+        i = order[k % n_meshes]
+        step = max(-diff, min(diff, 60_000 - counts[i])) if diff > 0 else max(diff, 500 - counts[i])
+        counts[i] += step
+        diff -= step
+        k += 1
+        if k > 10_000:
+            break
+    assert counts.sum() == total_tris
+    mats = [material_record(rng.uniform(0.05, 0.95, 3)) for _ in range(n_materials)]
+    meshes, instances = [], []
+    kinds = []
+    for i, n in enumerate(counts):
+        kind = ["slab", "panel", "column"][i % 3] if i >= 3 else ["slab", "panel", "panel"][i]
+        if kind == "column":
+            P, F = column_prism(int(n), rng)
+            t = (rng.uniform(2, W - 2), 0.0, rng.uniform(2, D - 2))
+            R = _rot((0, 1, 0), rng.uniform(0, 2 * math.pi))
+        elif kind == "panel":
+            P, F = arched_panel(int(n), rng)
+            side = int(rng.integers(4))
+            if side == 0:
+                t, R = (rng.uniform(6, W - 6), 0.0, 0.3), _rot((0, 1, 0), 0.0)
+            elif side == 1:
+                t, R = (rng.uniform(6, W - 6), 0.0, D - 0.3), _rot((0, 1, 0), math.pi)
+            elif side == 2:
+                t, R = (0.3, 0.0, rng.uniform(6, D - 6)), _rot((0, 1, 0), math.pi / 2)
+            else:
+                t, R = (W - 0.3, 0.0, rng.uniform(6, D - 6)), _rot((0, 1, 0), -math.pi / 2)
+        else:
+            P, F = floor_slab(int(n), rng)
+            level = float(rng.choice([0.0, 0.0, 6.0, 12.0, H]))
+            t = (rng.uniform(8, W - 8), level, rng.uniform(8, D - 8))
+            R = _rot((0, 1, 0), rng.uniform(0, 2 * math.pi))
+        assert F.shape[0] == n, (kind, F.shape[0], n)
+        m = int(rng.integers(n_materials))
+        # panels and slabs are seen from both sides
+        meshes.append(Mesh(P, F, np.full(F.shape[0], m, np.uint32)))
+        instances.append(Instance(i, trs(t, R)))
+        kinds.append(kind)
+    # double-sided variants of the materials for panels / slabs
+    base = len(mats)
+    mats += [np.where(np.arange(28) == 22, 2.0, r).astype(np.float32) for r in mats[:]]
+    for i, kind in enumerate(kinds):
+        if kind != "column":
+            meshes[i].tri_material = meshes[i].tri_material + base
+    lights = []
+    d = np.array([0.3, -1.0, 0.2])
+    d /= np.linalg.norm(d)
+    lights.append(light_record(0, pos=(W / 2, H, D / 2), direction=tuple(d), intensity=2.0))
+    for _ in range(n_point):
+        lights.append(light_record(1, pos=(rng.uniform(1, W - 1), rng.uniform(0.5, H - 0.5), rng.uniform(1, D - 1)),
+                                   intensity=float(rng.uniform(20, 120)), range_=float(rng.uniform(5, 12)),
+                                   decay=2.0))
+    movers = [int(i) for i in rng.choice([i for i, k in enumerate(kinds) if k == "column"], 3, replace=False)]
+    deformer = int(np.argmin([abs(int(c) - 20_000) for c in counts]))
+    if deformer in movers:
+        deformer = [i for i in range(n_meshes) if i not in movers][0]
+    grid = dict(gridMin=(0.5, 0.25, 0.5), gridSize=(W - 1.0, H - 0.5, D - 1.0), res=(16, 16, 16), rays=64)
+    return SceneDesc(meshes, instances, np.stack(mats), np.stack(lights), name="atrium",
+                     meta=dict(grid=grid, clustered=True, hysteresis=0.97, jitter="gated", seed=seed,
+                               movers=movers, deformer=deformer, kinds=kinds))
+
+
+def atrium_motion(scene: SceneDesc, frame: int, seed: int = 7):
+    """Per-frame motion: new world matrices for the 3 movers and the deformed
+    positions of the deforming mesh (sinusoidal offset, amplitude 2 cm)."""
+    rng = np.random.default_rng(seed * 1_000_003 + frame)
+    mats = {}
+    for i in scene.meta["movers"]:
+        base = scene.instances[i].world
+        ang = rng.uniform(-0.2, 0.2)
+        off = rng.uniform(-0.5, 0.5, 3) * np.array([1.0, 0.0, 1.0])
+        m = base.copy()
+        m[:3, :3] = _rot((0, 1, 0), ang) @ base[:3, :3]
+        m[:3, 3] = base[:3, 3] + off
+        mats[i] = m
+    dm = scene.meshes[scene.meta["deformer"]]
+    P = dm.positions.astype(np.float64)
+    ph = 0.35 * frame
+    offs = 0.02 * np.sin(P[:, 0] * 1.7 + ph) * np.cos(P[:, 2] * 1.3 + 0.5 * ph)
+    Pn = P.copy()
+    Pn[:, 1] += offs
+    return mats, Pn.astype(np.float32)
