@@ -44,8 +44,8 @@ L2_FLUSH_BYTES = 256 << 20
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -315,7 +315,7 @@ def _cpu_setup(scene):
     from speedball_b200.field import selectGiLightRecords
     pool = sc.build_pool(scene)
     mats, order, live, aabb = orc.compute_tail(pool)
-    keep = []
+    keep = [pool]  # the scene struct points into the pool's arrays
     S = orc.scene_struct(pool, mats, keep=keep)
     g = dict(scene.meta["grid"])
     gs = np.asarray(g["gridSize"], np.float32)
@@ -341,13 +341,15 @@ def cpu_solve_rate(scene, probes: int, reps: int = 1):
 
 
 def cpu_baseline(scene, target_s=12.0):
+    """The FP32 CPU restatement on every host thread: whole-atrium solves
+    (all 4,096 probes) repeated for about `target_s` seconds."""
     threads = os.cpu_count() or 1
-    rate, dt = cpu_solve_rate(scene, 64)
-    probes = int(min(4096, max(64, 64 * target_s / max(dt, 1e-3))))
-    rate, dt = cpu_solve_rate(scene, probes)
+    rate, dt = cpu_solve_rate(scene, 4096)
+    reps = max(1, int(round(target_s / max(dt, 1e-3))))
+    rate, dt = cpu_solve_rate(scene, 4096, reps)
     return {"value": round(rate, 4), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{probes} of 4096 probes x 64 rays of the atrium step (FP32 CPU restatement, "
-                      f"{threads} threads), {dt:.1f} s"}
+            "sample": f"{reps} full atrium solves (4,096 probes x 64 rays each) on {threads} threads, "
+                      f"FP32 CPU restatement, {dt:.1f} s"}
 
 
 def run_reference(args, dist: Dist):
@@ -355,14 +357,24 @@ def run_reference(args, dist: Dist):
         return None
     scene = make_workload()
     threads = os.cpu_count() or 1
-    rate, dt = cpu_solve_rate(scene, 64)
-    probes = int(min(4096, max(64, 64 * 4.0 / max(dt, 1e-3))))  # ~4 s per step
-    for _ in range(args.warmup if args.warmup < 2 else 1):
-        cpu_solve_rate(scene, probes)
+    rate, dt = cpu_solve_rate(scene, 4096)
+    # each step: a whole-atrium solve, or a probe sample sized so K+W steps fit ~2 minutes
+    budget_s = 120.0
+    per_step = budget_s / max(1, args.steps + args.warmup)
+    probes = int(min(4096, max(64, 4096 * per_step / max(dt, 1e-3))))
+    orc, S, keep, g, G, arena, nl, prm = _cpu_setup(scene)
+    irr, depth, atlas, datlas = orc.new_state(g, fp32=True)
+
+    def step():
+        t0 = time.perf_counter()
+        orc.solve(S, arena, nl, True, G, G, prm, 0, probes, irr, depth, atlas, datlas, fp32=True)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        step()
     total, rays = 0.0, 0
-    for _ in range(args.steps if args.steps <= 3 else 3):
-        r, d = cpu_solve_rate(scene, probes)
-        total += d
+    for _ in range(args.steps):
+        total += step()
         rays += probes * 64
     value = rays / total / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world,

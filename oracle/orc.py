@@ -152,7 +152,7 @@ def scene_struct(pool, materials: np.ndarray, nodes: np.ndarray | None = None, v
     s.instBase = pool.instBase; s.instCount = pool.instCount
     s.tlasBase = pool.tlasBase; s.tlasNodeCount = pool.tlasNodeCount
     if keep is not None:
-        keep.extend([nodes, vertex, materials])
+        keep.extend([nodes, vertex, materials, pool.triIndex, pool.triMaterial])
     return s
 
 

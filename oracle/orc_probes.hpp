@@ -208,9 +208,12 @@ template <class R> struct Tracer {
         o.tested = o.blocked = 0;
         R bestT, secondT;
         int bestTri, bestInst;
+        int replayFacing = -1;  // the GPU's facing decision (instance word bit 31)
         if (rp) {
             bestTri = rp->tri[rayIdx];
-            bestInst = rp->inst[rayIdx];
+            uint32_t w = (uint32_t)rp->inst[rayIdx];
+            bestInst = (int)(w & 0x7FFFFFFFu);
+            replayFacing = (int)(w >> 31);
             secondT = R(T_MAX);
             bestT = R(T_MAX);
             if (bestTri >= 0) {
@@ -238,7 +241,7 @@ template <class R> struct Tracer {
             V3<R> p0 = tr.fetch_vert(tr.tri_vert(tri, 0)), p1 = tr.fetch_vert(tr.tri_vert(tri, 1)),
                   p2 = tr.fetch_vert(tr.tri_vert(tri, 2));
             V3<R> ngRaw = tr.inst_normal_to_world(inst, normalize(cross(p1 - p0, p2 - p0)));
-            bool faceFwd = dot(ngRaw, rd) < R(0);
+            bool faceFwd = replayFacing >= 0 ? replayFacing == 1 : dot(ngRaw, rd) < R(0);
             V3<R> ng = ngRaw * (faceFwd ? R(1) : R(-1));
             V3<R> hitPoint = ro + rd * bestT;
             R traceBias = std::max(R(g.cellMin) * R(TRACE_SURFACE_BIAS_CELL) * R(P.debugTraceBiasScale),

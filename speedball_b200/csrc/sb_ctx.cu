@@ -130,6 +130,8 @@ DevScene dev_scene(const sb_ctx* c) {
     S.inst = c->B.inst;
     S.tlas = c->B.tlas;
     S.lights = c->B.lights;
+    S.triIndex = c->B.triIndex;
+    S.vertexData = c->B.vertexData;
     S.nodeCount = c->B.nodeCount;
     S.triCount = c->B.triCount;
     S.instCount = c->B.instCount;

@@ -42,6 +42,8 @@ struct DevScene {
     const float4* inst;        // 4 x float4 per instance slot: 3 inverse rows, (root, end, dSign, active)
     const uint4* tlas;         // 2 x uint4 per TLAS node, same encoding as BLAS nodes, payload (cnt<<24)|off
     const float* lights;       // 64 x 17 records (+ C0 cell lists)
+    const uint32_t* triIndex;  // reference triangle indices (final-hit refinement)
+    const float* vertexData;   // reference vertices, 8 floats each
     uint32_t nodeCount, triCount, instCount, tlasNodeCount, materialCount;
     uint32_t lightCount;
     int32_t clustered;

@@ -23,6 +23,54 @@ __device__ __forceinline__ float luma3(float3 c) { return c.x * 0.2126f + c.y * 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 __device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 
+// ---- double-float (unevaluated sum hi + lo) arithmetic from FP32 error-free
+// transformations (Knuth two-sum, FMA two-product; Dekker 1971). Used where
+// FP32 alone would miss the FP64 tolerances: ray angles and the final hit t.
+struct dfl { float hi, lo; };
+__device__ __forceinline__ dfl two_sum(float a, float b) {
+    float s = a + b;
+    float bb = s - a;
+    return {s, (a - (s - bb)) + (b - bb)};
+}
+__device__ __forceinline__ dfl fast_two_sum(float a, float b) {
+    float s = a + b;
+    return {s, b - (s - a)};
+}
+__device__ __forceinline__ dfl two_prod(float a, float b) {
+    float p = a * b;
+    return {p, fmaf(a, b, -p)};
+}
+__device__ __forceinline__ dfl df(float a) { return {a, 0.0f}; }
+__device__ __forceinline__ dfl df_add(dfl a, dfl b) {
+    dfl s = two_sum(a.hi, b.hi);
+    dfl t = two_sum(a.lo, b.lo);
+    s.lo += t.hi;
+    s = fast_two_sum(s.hi, s.lo);
+    s.lo += t.lo;
+    return fast_two_sum(s.hi, s.lo);
+}
+__device__ __forceinline__ dfl df_neg(dfl a) { return {-a.hi, -a.lo}; }
+__device__ __forceinline__ dfl df_sub(dfl a, dfl b) { return df_add(a, df_neg(b)); }
+__device__ __forceinline__ dfl df_mul(dfl a, dfl b) {
+    dfl p = two_prod(a.hi, b.hi);
+    p.lo = fmaf(a.hi, b.lo, fmaf(a.lo, b.hi, p.lo));
+    return fast_two_sum(p.hi, p.lo);
+}
+__device__ __forceinline__ float df_div(dfl a, dfl b) {
+    float q = a.hi / b.hi;
+    dfl r = df_sub(a, df_mul(df(q), b));
+    return q + r.hi / b.hi;
+}
+struct df3 { dfl x, y, z; };
+__device__ __forceinline__ df3 df3_sub(df3 a, df3 b) { return {df_sub(a.x, b.x), df_sub(a.y, b.y), df_sub(a.z, b.z)}; }
+__device__ __forceinline__ dfl df3_dot(df3 a, df3 b) {
+    return df_add(df_add(df_mul(a.x, b.x), df_mul(a.y, b.y)), df_mul(a.z, b.z));
+}
+__device__ __forceinline__ df3 df3_cross(df3 a, df3 b) {
+    return {df_sub(df_mul(a.y, b.z), df_mul(a.z, b.y)), df_sub(df_mul(a.z, b.x), df_mul(a.x, b.z)),
+            df_sub(df_mul(a.x, b.y), df_mul(a.y, b.x))};
+}
+
 // Probe position, gi_probes.js:1714-1726 (relocation x classifyStrength = 0).
 __device__ __forceinline__ float3 probe_world_pos(const DevCascade& C, uint32_t p) {
     uint32_t ix = p % C.res[0], iy = (p / C.res[0]) % C.res[1], iz = p / (C.res[0] * C.res[1]);
@@ -33,18 +81,29 @@ __device__ __forceinline__ float3 probe_world_pos(const DevCascade& C, uint32_t 
 }
 
 // Spherical-Fibonacci ray k of N with Cranley-Patterson rotation by the frame
-// jitter, normalized (gi_probes.js:1692-1704, 1984, 2331).
+// jitter, normalized (gi_probes.js:1692-1704, 1984, 2331):
+//   z = 1 - 2 frac((k + 0.5)/N + j),  phi = k * pi (3 - sqrt 5) + 2 pi j.
+// phi reaches hundreds of radians; evaluated naively in FP32 its rounding tilts
+// the ray by ~1e-5 rad. Here phi / pi is formed in double-float, reduced mod 2
+// exactly and fed to sincospif with a first-order correction for the low part,
+// so the direction carries ~1e-7 rad of error.
 __device__ __forceinline__ float3 ray_dir(uint32_t k, uint32_t N, float jitter) {
-    const float GOLDEN = 2.399963229728653f;  // pi * (3 - sqrt(5))
+    const float G_HI = 0.7639320492744446f;       // 3 - sqrt(5) = G_HI + G_LO
+    const float G_LO = -2.6774234385129603e-08f;
     float sk = (float(k) + 0.5f) / float(N);
     float u = sk + jitter;
     float uw = u - floorf(u);
     float z = 1.0f - uw * 2.0f;
     float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
-    float phi = float(k) * GOLDEN + jitter * 6.283185307179586f;
+    dfl x = df_add(two_prod(float(k), G_HI), df(float(k) * G_LO));
+    x = df_add(x, df(2.0f * jitter));
+    float n2 = 2.0f * floorf(x.hi * 0.5f);
+    x = df_add(x, df(-n2));
     float s, c;
-    sincosf(phi, &s, &c);
-    return normalize3(mk(r * c, r * s, z));
+    sincospif(x.hi, &s, &c);
+    float d = 3.141592653589793f * x.lo;
+    float s1 = fmaf(c, d, s), c1 = fmaf(-s, d, c);
+    return normalize3(mk(r * c1, r * s1, z));
 }
 
 // octEncodeNode / octDecodeNode, gi_oct.js:61-85

@@ -280,8 +280,9 @@ __device__ __forceinline__ unsigned long long sortable(double d) {
     return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
 
-// Sort record: key, then (segment << 13 | position) so that ties keep the
-// current order (a stable sort) and segments stay in place.
+// Sort record: (group << 13 | position) and key; ordered by group, then key,
+// then position, so ties keep the current order (a stable sort) and groups
+// stay in place.
 struct BuildRec {
     unsigned long long key;
     uint32_t segpos;
@@ -345,6 +346,9 @@ __global__ void __launch_bounds__(1024) k_tlas_build(SceneBuffers B, InstanceTab
     Seg* cur = segA;
     Seg* nxt = segB;
     while (nSeg > 0) {
+        // positions whose leaf was emitted at an earlier level belong to no segment
+        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) segOf[j] = NONE;
+        __syncthreads();
         // (a) bounds + node record per segment, one warp per segment
         for (uint32_t s = warp; s < nSeg; s += nWarps) {
             Seg sg = cur[s];
@@ -387,13 +391,16 @@ __global__ void __launch_bounds__(1024) k_tlas_build(SceneBuffers B, InstanceTab
             }
         }
         __syncthreads();
-        // (b) sort records; leaf segments keep their order (constant key)
+        // (b) sort records grouped by the first position of their segment (or by their
+        // own position when finished), so every group stays inside its range; leaf
+        // segments and finished positions keep their order (constant key)
         for (uint32_t j = threadIdx.x; j < P; j += blockDim.x) {
             BuildRec r;
             if (j < n) {
                 uint32_t s = segOf[j];
-                uint32_t ax = axisOf[s];
-                r.segpos = (s << 13) | j;
+                uint32_t ax = s == NONE ? 255u : axisOf[s];
+                uint32_t group = s == NONE ? j : (uint32_t)cur[s].lo;
+                r.segpos = (group << 13) | j;
                 r.key = ax == 255 ? 0ull : sortable(I.aabb[(size_t)order[j] * 9u + 6u + ax]);
             } else {
                 r.segpos = 0xFFFFFFFFu;

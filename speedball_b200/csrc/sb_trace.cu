@@ -164,6 +164,35 @@ __device__ void trace_closest(const DevScene& S, const uint4* tl, float3 ro, flo
     }
 }
 
+// The chosen hit's ray parameter re-evaluated in double-float: the same
+// Möller–Trumbore expression (spectral_traverse.js:396-408) on the local ray
+// (instLocalRay, 149-153), with the edges taken exactly from the pooled
+// vertices. FP32 alone loses ~1e-5 relative on near hits (the local origin is
+// rounded at scene scale); this keeps t within ~1e-7 of the exact value.
+__device__ float refine_t(const DevScene& S, uint32_t tri, uint32_t inst, float3 wro, float3 wrd) {
+    float4 r[3] = {__ldg(S.inst + 4 * inst), __ldg(S.inst + 4 * inst + 1), __ldg(S.inst + 4 * inst + 2)};
+    dfl lo[3], ld[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = df_add(df_add(df_add(two_prod(r[k].x, wro.x), two_prod(r[k].y, wro.y)), two_prod(r[k].z, wro.z)),
+                       df(r[k].w));
+        ld[k] = df_add(df_add(two_prod(r[k].x, wrd.x), two_prod(r[k].y, wrd.y)), two_prod(r[k].z, wrd.z));
+    }
+    const float* p[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) p[k] = S.vertexData + (size_t)__ldg(S.triIndex + 3 * tri + k) * 8u;
+    df3 p0 = {df(__ldg(p[0])), df(__ldg(p[0] + 1)), df(__ldg(p[0] + 2))};
+    df3 p1 = {df(__ldg(p[1])), df(__ldg(p[1] + 1)), df(__ldg(p[1] + 2))};
+    df3 p2 = {df(__ldg(p[2])), df(__ldg(p[2] + 1)), df(__ldg(p[2] + 2))};
+    df3 e1 = df3_sub(p1, p0), e2 = df3_sub(p2, p0);
+    df3 o = {lo[0], lo[1], lo[2]}, d = {ld[0], ld[1], ld[2]};
+    df3 pv = df3_cross(d, e2);
+    dfl det = df3_dot(e1, pv);
+    df3 tv = df3_sub(o, p0);
+    df3 qv = df3_cross(tv, e1);
+    return df_div(df3_dot(e2, qv), det);
+}
+
 // blasAny, spectral_traverse.js:477-536
 __device__ __forceinline__ bool blas_any(const DevScene& S, uint32_t inst, float3 wro, float3 wrd, float maxDist,
                                          Visits& vis, uint32_t* err) {
@@ -347,8 +376,9 @@ __device__ void trace_one(const TraceCtx& T, const uint4* tl, uint32_t gid, Visi
     float hitT = -1.0f;
     uint2 blockedBits = make_uint2(0u, 0u);
     if (bestTri >= 0) {
-        hitT = bestT;
         uint32_t tri = (uint32_t)bestTri, inst = (uint32_t)bestInst;
+        bestT = refine_t(T.S, tri, inst, ro, rd);
+        hitT = bestT;
         uint32_t m = __ldg(T.S.triMaterial + tri);
         float4 b = __ldg(T.S.tris + 3 * tri + 1), c = __ldg(T.S.tris + 3 * tri + 2);
         float3 nl = normalize3(cross3(xyz(b), xyz(c)));
@@ -400,7 +430,8 @@ __device__ void trace_one(const TraceCtx& T, const uint4* tl, uint32_t gid, Visi
         if (C.hits) {
             uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
             uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
-            C.hits[gid] = make_uint4(tri, inst, __float_as_uint(bestT), uq | (vq << 16));
+            // bit 31 of the instance word records the facing decision (normal flipped or not)
+            C.hits[gid] = make_uint4(tri, inst | (faceFwd ? 0x80000000u : 0u), __float_as_uint(bestT), uq | (vq << 16));
         }
     } else {
         outRgb = sky_sh(T.P, rd);
@@ -481,8 +512,9 @@ __global__ void k_raycast(DevScene S, const float* ro, const float* rd, uint32_t
     Visits vis = {0, 0, 0, 0};
     float t, bu, bv;
     int tri, inst;
-    trace_closest(S, S.tlas, mk(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]), mk(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]),
-                  t, tri, inst, bu, bv, vis, err);
+    float3 o = mk(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]), d = mk(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]);
+    trace_closest(S, S.tlas, o, d, t, tri, inst, bu, bv, vis, err);
+    if (tri >= 0) t = refine_t(S, (uint32_t)tri, (uint32_t)inst, o, d);
     tOut[i] = t;
     triOut[i] = tri;
     instOut[i] = inst;

@@ -103,10 +103,10 @@ def column_prism(n_tris: int, rng):
     return P, F[:n_tris]
 
 
-def arched_panel(n_tris: int, rng):
+def arched_panel(n_tris: int, rng, w=None, h=None):
     """Wall panel with an arched top edge, slightly curved in depth."""
-    w = float(rng.uniform(4.0, 12.0))
-    h = float(rng.uniform(4.0, 10.0))
+    w = float(rng.uniform(4.0, 12.0)) if w is None else float(w)
+    h = float(rng.uniform(4.0, 10.0)) if h is None else float(h)
     arch = float(rng.uniform(0.5, 2.5))
     bow = float(rng.uniform(0.0, 0.6))
     nu, nv = _dims_for(n_tris, aspect=w / h)
@@ -119,10 +119,10 @@ def arched_panel(n_tris: int, rng):
     return P, F[:n_tris]
 
 
-def floor_slab(n_tris: int, rng):
+def floor_slab(n_tris: int, rng, w=None, d=None):
     """Rectangular slab, 2-level subdivided grid with a shallow relief."""
-    w = float(rng.uniform(6.0, 20.0))
-    d = float(rng.uniform(6.0, 20.0))
+    w = float(rng.uniform(6.0, 20.0)) if w is None else float(w)
+    d = float(rng.uniform(6.0, 20.0)) if d is None else float(d)
     relief = float(rng.uniform(0.0, 0.05))
     nu, nv = _dims_for(n_tris, aspect=w / d)
 
@@ -204,12 +204,37 @@ def atrium(seed: int = 1, total_tris: int = ATRIUM_TRIS, n_meshes: int = 30, n_m
         if k > 10_000:
             break
     assert counts.sum() == total_tris
-    mats = [material_record(rng.uniform(0.05, 0.95, 3)) for _ in range(n_materials)]
+    # double-sided (side 2) like most of Sponza's materials in three.js scenes
+    mats = [material_record(rng.uniform(0.05, 0.95, 3), side=2) for _ in range(n_materials)]
     meshes, instances = [], []
     kinds = []
+    # the five largest meshes close the atrium: a floor slab and four arched
+    # perimeter walls facing inward (open to the sky above, like Sponza's court)
+    big = [int(i) for i in np.argsort(-counts, kind="stable")[:5]]
+    envelope = {big[0]: "floor", big[1]: "wall0", big[2]: "wall1", big[3]: "wall2", big[4]: "wall3"}
+    interior = 0
     for i, n in enumerate(counts):
-        kind = ["slab", "panel", "column"][i % 3] if i >= 3 else ["slab", "panel", "panel"][i]
-        if kind == "column":
+        if i in envelope:
+            kind = envelope[i]
+        else:
+            kind = ["slab", "panel", "column", "column"][interior % 4]
+            interior += 1
+        if kind == "floor":
+            P, F = floor_slab(int(n), rng, w=W, d=D)
+            t, R = (W / 2, 0.0, D / 2), _rot((0, 1, 0), 0.0)
+        elif kind.startswith("wall"):
+            side = int(kind[-1])
+            span = W if side < 2 else D
+            P, F = arched_panel(int(n), rng, w=span, h=H * 0.8)
+            if side == 0:
+                t, R = (W / 2, 0.0, 0.0), _rot((0, 1, 0), 0.0)
+            elif side == 1:
+                t, R = (W / 2, 0.0, D), _rot((0, 1, 0), math.pi)
+            elif side == 2:
+                t, R = (0.0, 0.0, D / 2), _rot((0, 1, 0), math.pi / 2)
+            else:
+                t, R = (W, 0.0, D / 2), _rot((0, 1, 0), -math.pi / 2)
+        elif kind == "column":
             P, F = column_prism(int(n), rng)
             t = (rng.uniform(2, W - 2), 0.0, rng.uniform(2, D - 2))
             R = _rot((0, 1, 0), rng.uniform(0, 2 * math.pi))
@@ -226,21 +251,14 @@ def atrium(seed: int = 1, total_tris: int = ATRIUM_TRIS, n_meshes: int = 30, n_m
                 t, R = (W - 0.3, 0.0, rng.uniform(6, D - 6)), _rot((0, 1, 0), -math.pi / 2)
         else:
             P, F = floor_slab(int(n), rng)
-            level = float(rng.choice([0.0, 0.0, 6.0, 12.0, H]))
+            level = float(rng.choice([0.05, 6.0, 12.0]))
             t = (rng.uniform(8, W - 8), level, rng.uniform(8, D - 8))
             R = _rot((0, 1, 0), rng.uniform(0, 2 * math.pi))
         assert F.shape[0] == n, (kind, F.shape[0], n)
         m = int(rng.integers(n_materials))
-        # panels and slabs are seen from both sides
         meshes.append(Mesh(P, F, np.full(F.shape[0], m, np.uint32)))
         instances.append(Instance(i, trs(t, R)))
         kinds.append(kind)
-    # double-sided variants of the materials for panels / slabs
-    base = len(mats)
-    mats += [np.where(np.arange(28) == 22, 2.0, r).astype(np.float32) for r in mats[:]]
-    for i, kind in enumerate(kinds):
-        if kind != "column":
-            meshes[i].tri_material = meshes[i].tri_material + base
     lights = []
     d = np.array([0.3, -1.0, 0.2])
     d /= np.linalg.norm(d)
@@ -250,9 +268,8 @@ def atrium(seed: int = 1, total_tris: int = ATRIUM_TRIS, n_meshes: int = 30, n_m
                                    intensity=float(rng.uniform(20, 120)), range_=float(rng.uniform(5, 12)),
                                    decay=2.0))
     movers = [int(i) for i in rng.choice([i for i, k in enumerate(kinds) if k == "column"], 3, replace=False)]
-    deformer = int(np.argmin([abs(int(c) - 20_000) for c in counts]))
-    if deformer in movers:
-        deformer = [i for i in range(n_meshes) if i not in movers][0]
+    candidates = [i for i in range(n_meshes) if i not in movers and i not in envelope]
+    deformer = min(candidates, key=lambda i: abs(int(counts[i]) - 20_000))
     grid = dict(gridMin=(0.5, 0.25, 0.5), gridSize=(W - 1.0, H - 0.5, D - 1.0), res=(16, 16, 16), rays=64)
     return SceneDesc(meshes, instances, np.stack(mats), np.stack(lights), name="atrium",
                      meta=dict(grid=grid, clustered=True, hysteresis=0.97, jitter="gated", seed=seed,

@@ -81,12 +81,10 @@ class OracleMirror:
             io.rayOut = orc._p(out["rays"]); io.hitTri = orc._p(out["tri"]); io.hitInst = orc._p(out["inst"])
             io.secondT = orc._p(out["second"]); io.tested = orc._p(out["tested"]); io.blocked = orc._p(out["blocked"])
         if replay is not None:
-            io.replayTri = orc._p(replay["tri"]); io.replayInst = orc._p(replay["inst"])
+            io.replayTri = orc._p(replay["tri"]); io.replayInst = orc._p(replay["inst_word"])
             io.replayBlocked = orc._p(replay["blocked"])
-        pre = np.zeros(self.pool.instCount, np.float64)  # placeholder for keep-alive symmetry
         orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid, self.params(),
                   offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io)
-        del pre
         return out
 
 
@@ -94,10 +92,13 @@ def gpu_records(field: ProbeField, n: int) -> dict:
     hits = read(field, "HIT_RECORDS", n * 4, np.uint32).reshape(n, 4)
     vis = read(field, "VISIBILITY", n * 2, np.uint32).reshape(n, 2)
     tri = hits[:, 0].view(np.int32).copy()
-    inst = hits[:, 1].view(np.int32).copy()
+    word = hits[:, 1].copy()
+    inst = np.where(tri >= 0, word & 0x7FFFFFFF, 0xFFFFFFFF).astype(np.uint32).view(np.int32)
     t = hits[:, 2].view(np.float32).copy()
     blocked = vis[:, 0].astype(np.uint64) | (vis[:, 1].astype(np.uint64) << np.uint64(32))
-    return dict(tri=np.ascontiguousarray(tri), inst=np.ascontiguousarray(inst), t=t,
+    # replay input keeps the facing bit in bit 31 of the instance word
+    return dict(tri=np.ascontiguousarray(tri), inst=np.ascontiguousarray(inst),
+                inst_word=np.ascontiguousarray(word.view(np.int32)), facing=(word >> 31).astype(bool), t=t,
                 blocked=np.ascontiguousarray(blocked))
 
 
