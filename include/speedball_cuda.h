@@ -73,8 +73,9 @@ typedef struct sb_device_opts {
     uint32_t flags;        /* SB_CTX_* below                                       */
 } sb_device_opts;
 
-#define SB_CTX_RECORD_HITS 1u  /* keep 16-byte hit records + visibility masks of the
-                                  last solve (needed by sb_backward and replay)     */
+#define SB_CTX_RECORD_HITS 1u  /* accepted, no effect: the 16-byte hit records and
+                                  visibility masks of the last solve are always kept
+                                  (the shade stage and sb_backward read them)        */
 
 /* createProbeField (gi_probes.js:945) minus the renderer: allocates the context. */
 sb_status sb_create(const sb_device_opts* opts, sb_ctx** out);
@@ -124,7 +125,8 @@ typedef enum sb_buffer {
     SB_BUF_DEPTH_ATLAS = 9,        /* u16 binary16 RGBA                                  */
     SB_BUF_RAY_DATA = 10,          /* f32, 4 per ray: rgb + hitT (-1 = miss)             */
     SB_BUF_HIT_RECORDS = 11,       /* u32, 4 per ray: tri, inst, t bits, packed uv        */
-    SB_BUF_VISIBILITY = 12,        /* u32, 2 per ray: NEE shadow bits, lights 0..63      */
+    SB_BUF_VISIBILITY = 12,        /* u32, 4 per ray: lights shadow-tested (lo, hi) and
+                                      left unblocked (lo, hi), bit = light index 0..63   */
     SB_BUF_TLAS_ORDER = 13,        /* u32, slot -> source instance                       */
     SB_BUF_INSTANCE_BOUNDS = 14    /* f32, 6 per slot (liveInstanceBounds)               */
 } sb_buffer;

@@ -31,7 +31,7 @@ struct Cascade {
     uint2* depthAtlas = nullptr;
     float4* rayData = nullptr;
     uint4* hits = nullptr;
-    uint2* vis = nullptr;
+    uint4* vis = nullptr;
     size_t rayCap = 0;
 };
 
@@ -73,6 +73,8 @@ struct sb_ctx {
     std::vector<float> hostLights;
 
     TraceTuning tune{256u, 2048u, 0u, 148};
+    float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
+    uint32_t jobCap = 0;
     cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr;
     bool timed = false;
 };
@@ -111,6 +113,8 @@ template <class T> void release(T*& p) {
     if (p) cudaFree(p);
     p = nullptr;
 }
+
+constexpr uint64_t kJobCapMax = 64ull << 20;  // 64 Mi shadow jobs (2 GiB) per trace chunk
 
 uint32_t tlas_nodes_for(uint32_t n) {
     // node count of the median split with leaf size 2 (buildTlasRecords)
@@ -302,6 +306,7 @@ void sb_destroy(sb_ctx* ctx) {
         release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.rayData); release(K.hits);
         release(K.vis);
     }
+    release(ctx->jobs);
     release(ctx->dErr); release(ctx->dGate); release(ctx->dWork); release(ctx->dCounters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->evMid) cudaEventDestroy(ctx->evMid);
@@ -477,7 +482,7 @@ sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t c
         case SB_BUF_DEPTH_ATLAS: if (K) { srcp = K->depthAtlas; len = (size_t)K->atlasW * K->atlasH * 4; esz = 2; } break;
         case SB_BUF_RAY_DATA: if (K) { srcp = K->rayData; len = K->rayCap * 4; } break;
         case SB_BUF_HIT_RECORDS: if (K) { srcp = K->hits; len = K->hits ? K->rayCap * 4 : 0; } break;
-        case SB_BUF_VISIBILITY: if (K) { srcp = K->vis; len = K->vis ? K->rayCap * 2 : 0; } break;
+        case SB_BUF_VISIBILITY: if (K) { srcp = K->vis; len = K->vis ? K->rayCap * 4 : 0; } break;
         case SB_BUF_TLAS_ORDER: srcp = ctx->I.order; len = ctx->instancesSet ? ctx->I.count : 0; break;
         case SB_BUF_INSTANCE_BOUNDS: srcp = ctx->I.liveBounds; len = ctx->instancesSet ? (size_t)ctx->I.count * 6 : 0; break;
         default: return fail(ctx, SB_ERR_INVALID_ARG, "unknown buffer %u", buf);
@@ -549,10 +554,8 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
         release(K.rayData); release(K.hits); release(K.vis);
         size_t c = 0;
         CK(grow(K.rayData, c, rays));
-        if (ctx->flags & SB_CTX_RECORD_HITS) {
-            c = 0; CK(grow(K.hits, c, rays));
-            c = 0; CK(grow(K.vis, c, rays));
-        }
+        c = 0; CK(grow(K.hits, c, rays));
+        c = 0; CK(grow(K.vis, c, rays));
         K.rayCap = rays;
     }
     K.grid = *g;
@@ -598,9 +601,26 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     DevCascade D = dev_cascade(ctx, ci, probeOffset, updatedCount);
     DevParams P;
     std::memcpy(&P, &ctx->params, sizeof P);
+    // shadow-job queue: up to one job per (ray, light); solves larger than the
+    // queue cap run as several probe-slot chunks before the blend
+    const uint64_t perProbe = (uint64_t)K.grid.raysPerProbe * (ctx->lightCount ? ctx->lightCount : 1u);
+    uint64_t want = perProbe * updatedCount;
+    if (want > kJobCapMax) want = kJobCapMax - kJobCapMax % perProbe;
+    if (want < perProbe) want = perProbe;
+    if (want > ctx->jobCap) {
+        release(ctx->jobs);
+        size_t c = 0;
+        CK(grow(ctx->jobs, c, (size_t)want * 2));
+        ctx->jobCap = (uint32_t)want;
+    }
+    const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
     if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 64, ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune, ctx->stream));
+    for (uint32_t s0 = 0; s0 < updatedCount; s0 += chunk) {
+        uint32_t n = updatedCount - s0 < chunk ? updatedCount - s0 : chunk;
+        CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune,
+                        ctx->stream, ctx->jobs, ctx->jobCap, s0, n));
+    }
     CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));

@@ -62,8 +62,8 @@ struct DevCascade {
     float g0Min[3], g0Size[3];
     uint32_t g0Res[3];
     float4* rayData;           // updatedCount*rays
-    uint4* hits;               // optional 16-byte hit records
-    uint2* vis;                // optional NEE shadow bits
+    uint4* hits;               // 16-byte hit records: tri, inst | facing << 31, t, packed uv
+    uint4* vis;                // NEE masks: tested lights (lo, hi), unblocked lights (lo, hi)
     float4* irr;               // history, probeTotal*64
     float2* depth;             // history
     const uint2* atlasPrev;    // RGBA16F texels as 4 halves (the previous upload)

@@ -34,8 +34,11 @@ struct SceneBuffers {
     uint32_t instBase = 0, instCount = 0, tlasBase = 0, tlasNodeCount = 0, lightsLen = 0;
 };
 
+// The three trace stages over probe slots [slotBegin, slotBegin + slotCount);
+// `jobs` holds up to jobCap shadow-ray jobs (32 bytes each).
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
-                         unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st);
+                         unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
+                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st);
 cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st);

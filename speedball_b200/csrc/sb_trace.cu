@@ -1,355 +1,284 @@
-// sb_trace.cu — probe ray trace + hit shading (traceKernel, gi_probes.js:1977-2214)
-// over the two-level BVH (spectral_traverse.js:354-569), for sm_100a.
+// sb_trace.cu — the probe trace as a three-stage wavefront (traceKernel,
+// gi_probes.js:1977-2214, split where its per-ray work diverges):
 //
-// One thread per (probe slot, ray). Warps pull 32-ray batches from a global
-// work counter (persistent, work-stealing), the TLAS is staged in shared
-// memory, BLAS nodes / pre-gathered triangles are read as 16-byte vectors.
-#include "sb_math.cuh"
-#include "sb_kernels.cuh"
+//   A  k_trace_primary  closest hit per probe ray (traverseClosest) -> 16-byte
+//                       hit record; NEE pre-tests per candidate light (the
+//                       reference's ndl * peak > 0 and range gates) emit
+//                       shadow-ray jobs, warp-ballot compacted into a queue.
+//   B  k_trace_shadow   any hit per job (traverseAny); blocked lights are
+//                       cleared from the ray's visibility mask.
+//   C  k_shade          emissive + unblocked NEE terms (ascending light index,
+//                       the reference's summation order) + one-bounce atlas
+//                       read, or the SH-9 sky on a miss -> rayData.
+//
+// A and B are persistent and work-stealing (warps pull 32 items per atomic).
+// A issues rays direction-major: a warp holds ray k of 32 neighbouring probes,
+// i.e. 32 parallel rays, which keeps the BVH walks of a warp together.
+#include "sb_traverse.cuh"
 
 namespace sb {
 
-struct TraceCtx {
+struct WaveCtx {
     DevScene S;
     DevCascade C;
     DevParams P;
     uint32_t* err;
     unsigned long long* counters;  // [rays, shadowRays, tlasNodes, instances, blasNodes, triTests] or null
-    uint32_t* work;                // work-stealing cursor (reset to 0 before launch)
-    uint32_t totalRays;
-    uint32_t smemTlas;             // TLAS nodes staged in shared memory
+    uint32_t* work;                // [0] primary cursor, [1] shadow cursor, [2] job count
+    float4* jobs;                  // 2 float4 per job: (origin, maxDist), (dir, ray << 6 | light)
+    uint32_t jobCap;
+    uint32_t slotBegin, slotCount; // probe slots of this chunk
+    uint32_t smemTlas;             // TLAS nodes staged in shared memory (0 = read from global)
+    uint32_t order;                // 0 probe-major, 1 direction-major
 };
 
-struct Visits { uint32_t tlas, inst, blas, tri; };
-
-__device__ __forceinline__ bool slab(float3 bmin, float3 bmax, float3 ro, float3 invD, float tlim) {
-    float t0x = (bmin.x - ro.x) * invD.x, t1x = (bmax.x - ro.x) * invD.x;
-    float t0y = (bmin.y - ro.y) * invD.y, t1y = (bmax.y - ro.y) * invD.y;
-    float t0z = (bmin.z - ro.z) * invD.z, t1z = (bmax.z - ro.z) * invD.z;
-    float tNear = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
-    float tFar = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
-    return tFar >= fmaxf(tNear, 0.0f) && tNear < tlim;
-}
-
-__device__ __forceinline__ void load_node(const uint4* nodes, uint32_t c, float3& bmin, float3& bmax, uint32_t& miss,
-                                          uint32_t& payload) {
-    uint4 a = __ldg(nodes + 2 * c), b = __ldg(nodes + 2 * c + 1);
-    bmin = mk(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z));
-    bmax = mk(__uint_as_float(a.w), __uint_as_float(b.x), __uint_as_float(b.y));
-    miss = b.z;
-    payload = b.w;
-}
-
-// Möller–Trumbore on a pre-gathered triangle, spectral_traverse.js:393-409.
-__device__ __forceinline__ bool mt_hit(const float4* tris, uint32_t tri, float3 ro, float3 rd, float tmax, float& t,
-                                       float& det, float& u, float& v, uint32_t& bits) {
-    float4 a = __ldg(tris + 3 * tri), b = __ldg(tris + 3 * tri + 1), c = __ldg(tris + 3 * tri + 2);
-    float3 p0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
-    float3 pv = cross3(rd, e2);
-    det = dot3(e1, pv);
-    if (!(fabsf(det) > 1e-12f)) return false;
-    float invDet = 1.0f / det;
-    float3 tv = ro - p0;
-    u = dot3(tv, pv) * invDet;
-    if (!(u >= 0.0f && u <= 1.0f)) return false;
-    float3 qv = cross3(tv, e1);
-    v = dot3(rd, qv) * invDet;
-    if (!(v >= 0.0f && u + v <= 1.0f)) return false;
-    t = dot3(e2, qv) * invDet;
-    bits = __float_as_uint(a.w);
-    return t > RAY_EPS && t < tmax;
-}
-
-__device__ __forceinline__ bool side_ok(uint32_t bits, float det) {
-    uint32_t side = bits & TB_SIDE_MASK;
-    return side == 2u || (side == 0u && det > 0.0f) || (side == 1u && det < 0.0f);
-}
-
-struct InstRay { float3 ro, rd, invD; uint32_t root, end; float dSign; };
-
-__device__ __forceinline__ InstRay inst_ray(const float4* inst, uint32_t i, float3 wro, float3 wrd) {
-    float4 r0 = __ldg(inst + 4 * i), r1 = __ldg(inst + 4 * i + 1), r2 = __ldg(inst + 4 * i + 2), m = __ldg(inst + 4 * i + 3);
-    InstRay r;
-    r.ro = mk(dot3(xyz(r0), wro) + r0.w, dot3(xyz(r1), wro) + r1.w, dot3(xyz(r2), wro) + r2.w);
-    r.rd = mk(dot3(xyz(r0), wrd), dot3(xyz(r1), wrd), dot3(xyz(r2), wrd));
-    r.invD = mk(1.0f / r.rd.x, 1.0f / r.rd.y, 1.0f / r.rd.z);
-    r.root = __float_as_uint(m.x);
-    r.end = __float_as_uint(m.y);
-    r.dSign = m.z;
-    return r;
-}
-
-// blasClosest, spectral_traverse.js:354-435 (threaded, left-first).
-__device__ __forceinline__ void blas_closest(const DevScene& S, uint32_t inst, float3 wro, float3 wrd, float& bestT,
-                                             int& bestTri, int& bestInst, float& bu, float& bv, Visits& vis,
-                                             uint32_t* err) {
-    InstRay r = inst_ray(S.inst, inst, wro, wrd);
-    uint32_t cursor = r.root;
-    uint32_t it = 0;
-    for (; it < S.nodeCount; ++it) {
-        if (cursor >= r.end) break;
-        float3 bmin, bmax;
-        uint32_t miss, payload;
-        load_node(S.nodes, cursor, bmin, bmax, miss, payload);
-        ++vis.blas;
-        if (slab(bmin, bmax, r.ro, r.invD, bestT)) {
-            if (payload == INTERIOR) {
-                cursor = cursor + 1;
-            } else {
-                uint32_t off = payload & 0x00FFFFFFu, cnt = payload >> 24;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    uint32_t tri = off + i;
-                    float t, det, u, v;
-                    uint32_t bits;
-                    ++vis.tri;
-                    if (!mt_hit(S.tris, tri, r.ro, r.rd, bestT, t, det, u, v, bits)) continue;
-                    if (side_ok(bits, det * r.dSign) && (bits & TB_CLOSEST_OK)) {
-                        bestT = t;
-                        bestTri = (int)tri;
-                        bestInst = (int)inst;
-                        bu = u;
-                        bv = v;
-                    }
-                }
-                cursor = miss;
-            }
-        } else {
-            cursor = miss;
-        }
+__device__ __forceinline__ const uint4* stage_tlas(const WaveCtx& W, uint4* sTlas) {
+    const DevScene& S = W.S;
+    if (W.smemTlas >= S.tlasNodeCount && S.tlasNodeCount > 0) {
+        for (uint32_t i = threadIdx.x; i < 2 * S.tlasNodeCount; i += blockDim.x) sTlas[i] = __ldg(S.tlas + i);
+        __syncthreads();
+        return sTlas;
     }
-    if (it == S.nodeCount && cursor < r.end) latch(err, ERR_WATCHDOG);
+    return S.tlas;
 }
 
-__device__ __forceinline__ void load_tlas(const uint4* tl, uint32_t c, float3& bmin, float3& bmax, uint32_t& miss,
-                                          uint32_t& payload) {
-    uint4 a = tl[2 * c], b = tl[2 * c + 1];
-    bmin = mk(__uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z));
-    bmax = mk(__uint_as_float(a.w), __uint_as_float(b.x), __uint_as_float(b.y));
-    miss = b.z;
-    payload = b.w;
+struct HitFrame {
+    float3 ng, hitPos;
+    float traceBias;
+    bool faceFwd;
+};
+
+// Geometric normal through (M^-1)^T, flipped toward the ray, and the biased
+// hit position (gi_probes.js:2003-2017).
+__device__ __forceinline__ HitFrame hit_frame(const WaveCtx& W, uint32_t tri, uint32_t inst, float3 ro, float3 rd,
+                                              float t, int facing) {
+    float4 b = __ldg(W.S.tris + 3 * tri + 1), c = __ldg(W.S.tris + 3 * tri + 2);
+    float3 nl = normalize3(cross3(xyz(b), xyz(c)));
+    float4 r0 = __ldg(W.S.inst + 4 * inst), r1 = __ldg(W.S.inst + 4 * inst + 1), r2 = __ldg(W.S.inst + 4 * inst + 2);
+    float3 ngRaw = normalize3(xyz(r0) * nl.x + xyz(r1) * nl.y + xyz(r2) * nl.z);
+    HitFrame f;
+    f.faceFwd = facing >= 0 ? facing == 1 : dot3(ngRaw, rd) < 0.0f;
+    f.ng = ngRaw * (f.faceFwd ? 1.0f : -1.0f);
+    f.traceBias = fmaxf(W.C.cellMin * 0.005f * W.P.debugTraceBiasScale, RAY_EPS * W.P.debugRayEpsScale);
+    f.hitPos = (ro + rd * t) + f.ng * f.traceBias;
+    return f;
 }
 
-// traverseClosest, spectral_traverse.js:441-474
-__device__ void trace_closest(const DevScene& S, const uint4* tl, float3 ro, float3 rd, float& bestT, int& bestTri,
-                              int& bestInst, float& bu, float& bv, Visits& vis, uint32_t* err) {
-    bestT = T_MAX;
-    bestTri = -1;
-    bestInst = -1;
-    bu = bv = 0.0f;
-    float3 invD = mk(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
-    uint32_t cursor = 0;
-    for (uint32_t it = 0; it < S.tlasNodeCount; ++it) {
-        if (cursor >= S.tlasNodeCount) break;
-        float3 bmin, bmax;
-        uint32_t miss, payload;
-        load_tlas(tl, cursor, bmin, bmax, miss, payload);
-        ++vis.tlas;
-        if (slab(bmin, bmax, ro, invD, bestT)) {
-            uint32_t cnt = payload >> 24;
-            if (cnt == 0) {
-                cursor = cursor + 1;
-            } else {
-                uint32_t off = payload & 0x00FFFFFFu;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    uint32_t inst = off + i;
-                    ++vis.inst;
-                    if (__ldg(&S.inst[4 * inst + 3].w) > 0.5f)
-                        blas_closest(S, inst, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, err);
-                }
-                cursor = miss;
-            }
-        } else {
-            cursor = miss;
-        }
-    }
+// Candidate lights of a hit: the C0 cell list in clustered mode
+// (gi_probes.js:2109-2127), else every light.
+struct LightList {
+    const float* list;
+    uint32_t count;
+};
+__device__ __forceinline__ LightList light_list(const WaveCtx& W, float3 hitPos) {
+    LightList L{nullptr, W.S.lightCount};
+    if (!W.S.clustered) return L;
+    const DevCascade& C = W.C;
+    float3 cellCount = mk(float(C.g0Res[0]) - 1.0f, float(C.g0Res[1]) - 1.0f, float(C.g0Res[2]) - 1.0f);
+    float3 cellSize = mk(C.g0Size[0] / cellCount.x, C.g0Size[1] / cellCount.y, C.g0Size[2] / cellCount.z);
+    float3 cf = mk(floorf((hitPos.x - C.g0Min[0]) / cellSize.x), floorf((hitPos.y - C.g0Min[1]) / cellSize.y),
+                   floorf((hitPos.z - C.g0Min[2]) / cellSize.z));
+    bool outside = cf.x < 0.f || cf.y < 0.f || cf.z < 0.f || cf.x >= cellCount.x || cf.y >= cellCount.y ||
+                   cf.z >= cellCount.z;
+    uint32_t cx = (uint32_t)clampf(cf.x, 0.f, cellCount.x - 1.0f);
+    uint32_t cy = (uint32_t)clampf(cf.y, 0.f, cellCount.y - 1.0f);
+    uint32_t cz = (uint32_t)clampf(cf.z, 0.f, cellCount.z - 1.0f);
+    uint32_t cellsX = C.g0Res[0] - 1u, cellsY = C.g0Res[1] - 1u;
+    uint32_t cellIndex = cz * (cellsX * cellsY) + cy * cellsX + cx;
+    const float* list = W.S.lights + LIGHT_DATA + cellIndex * 17u;
+    uint32_t listCount = (uint32_t)__ldg(list);
+    if (outside || listCount > 16u) return L;
+    L.list = list;
+    L.count = listCount;
+    return L;
+}
+__device__ __forceinline__ uint32_t light_at(const LightList& L, uint32_t i) {
+    return L.list ? (uint32_t)__ldg(L.list + 1 + i) : i;
 }
 
-// The chosen hit's ray parameter re-evaluated in double-float: the same
-// Möller–Trumbore expression (spectral_traverse.js:396-408) on the local ray
-// (instLocalRay, 149-153), with the edges taken exactly from the pooled
-// vertices. FP32 alone loses ~1e-5 relative on near hits (the local origin is
-// rounded at scene scale); this keeps t within ~1e-7 of the exact value.
-__device__ float refine_t(const DevScene& S, uint32_t tri, uint32_t inst, float3 wro, float3 wrd) {
-    float4 r[3] = {__ldg(S.inst + 4 * inst), __ldg(S.inst + 4 * inst + 1), __ldg(S.inst + 4 * inst + 2)};
-    dfl lo[3], ld[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        lo[k] = df_add(df_add(df_add(two_prod(r[k].x, wro.x), two_prod(r[k].y, wro.y)), two_prod(r[k].z, wro.z)),
-                       df(r[k].w));
-        ld[k] = df_add(df_add(two_prod(r[k].x, wrd.x), two_prod(r[k].y, wrd.y)), two_prod(r[k].z, wrd.z));
-    }
-    const float* p[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) p[k] = S.vertexData + (size_t)__ldg(S.triIndex + 3 * tri + k) * 8u;
-    df3 p0 = {df(__ldg(p[0])), df(__ldg(p[0] + 1)), df(__ldg(p[0] + 2))};
-    df3 p1 = {df(__ldg(p[1])), df(__ldg(p[1] + 1)), df(__ldg(p[1] + 2))};
-    df3 p2 = {df(__ldg(p[2])), df(__ldg(p[2] + 1)), df(__ldg(p[2] + 2))};
-    df3 e1 = df3_sub(p1, p0), e2 = df3_sub(p2, p0);
-    df3 o = {lo[0], lo[1], lo[2]}, d = {ld[0], ld[1], ld[2]};
-    df3 pv = df3_cross(d, e2);
-    dfl det = df3_dot(e1, pv);
-    df3 tv = df3_sub(o, p0);
-    df3 qv = df3_cross(tv, e1);
-    return df_div(df3_dot(e2, qv), det);
-}
+struct LightEval {
+    float3 wi, lcol, ldir;
+    float dist, ndl, lrange, ldecay, lcosAngle, lcosPen;
+    bool isDir, isSpot, pass;
+};
 
-// blasAny, spectral_traverse.js:477-536
-__device__ __forceinline__ bool blas_any(const DevScene& S, uint32_t inst, float3 wro, float3 wrd, float maxDist,
-                                         Visits& vis, uint32_t* err) {
-    InstRay r = inst_ray(S.inst, inst, wro, wrd);
-    uint32_t cursor = r.root;
-    uint32_t it = 0;
-    for (; it < S.nodeCount; ++it) {
-        if (cursor >= r.end) break;
-        float3 bmin, bmax;
-        uint32_t miss, payload;
-        load_node(S.nodes, cursor, bmin, bmax, miss, payload);
-        ++vis.blas;
-        if (slab(bmin, bmax, r.ro, r.invD, maxDist)) {
-            if (payload == INTERIOR) {
-                cursor = cursor + 1;
-            } else {
-                uint32_t off = payload & 0x00FFFFFFu, cnt = payload >> 24;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    float t, det, u, v;
-                    uint32_t bits;
-                    ++vis.tri;
-                    if (!mt_hit(S.tris, off + i, r.ro, r.rd, maxDist, t, det, u, v, bits)) continue;
-                    if ((bits & TB_SHADOW_OK) && side_ok(bits, det * r.dSign)) return true;
-                }
-                cursor = miss;
-            }
-        } else {
-            cursor = miss;
-        }
-    }
-    if (it == S.nodeCount && cursor < r.end) latch(err, ERR_WATCHDOG);
-    return false;
-}
-
-// traverseAny, spectral_traverse.js:539-569
-__device__ bool trace_any(const DevScene& S, const uint4* tl, float3 ro, float3 rd, float maxDist, Visits& vis,
-                          uint32_t* err) {
-    float3 invD = mk(1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z);
-    uint32_t cursor = 0;
-    for (uint32_t it = 0; it < S.tlasNodeCount; ++it) {
-        if (cursor >= S.tlasNodeCount) break;
-        float3 bmin, bmax;
-        uint32_t miss, payload;
-        load_tlas(tl, cursor, bmin, bmax, miss, payload);
-        ++vis.tlas;
-        if (slab(bmin, bmax, ro, invD, maxDist)) {
-            uint32_t cnt = payload >> 24;
-            if (cnt == 0) {
-                cursor = cursor + 1;
-            } else {
-                uint32_t off = payload & 0x00FFFFFFu;
-                for (uint32_t i = 0; i < cnt; ++i) {
-                    uint32_t inst = off + i;
-                    ++vis.inst;
-                    if (__ldg(&S.inst[4 * inst + 3].w) > 0.5f && blas_any(S, inst, ro, rd, maxDist, vis, err))
-                        return true;
-                }
-                cursor = miss;
-            }
-        } else {
-            cursor = miss;
-        }
-    }
-    return false;
-}
-
-// sampleAtlas, gi_probes.js:1941-1974: 8-tap trilinear over the cage probes,
-// each tap a bilinear fetch of the previous RGBA16F atlas (exact weights).
-__device__ float3 sample_atlas(const DevCascade& C, float3 P, float3 N) {
-    float3 cell = mk(C.gridSize[0] / fmaxf(1.0f, float(C.res[0]) - 1.0f),
-                     C.gridSize[1] / fmaxf(1.0f, float(C.res[1]) - 1.0f),
-                     C.gridSize[2] / fmaxf(1.0f, float(C.res[2]) - 1.0f));
-    float gf[3] = {(P.x - C.gridMin[0]) / fmaxf(cell.x, 1e-6f), (P.y - C.gridMin[1]) / fmaxf(cell.y, 1e-6f),
-                   (P.z - C.gridMin[2]) / fmaxf(cell.z, 1e-6f)};
-    float base[3], frac[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        base[a] = clampf(floorf(gf[a]), 0.0f, fmaxf(float(C.res[a]) - 2.0f, 0.0f));
-        frac[a] = clampf(gf[a] - base[a], 0.0f, 1.0f);
-    }
-    float2 ouv = oct_encode(normalize3(N));
-    float3 acc = mk(0.f, 0.f, 0.f);
-    float wsum = 0.0f;
-    const float W = float(C.atlasW), H = float(C.atlasH);
-    const int Wi = (int)C.atlasW, Hi = (int)C.atlasH;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
-        float px = base[0] + float(dx), py = base[1] + float(dy), pz = base[2] + float(dz);
-        float wx = dx ? frac[0] : 1.0f - frac[0];
-        float wy = dy ? frac[1] : 1.0f - frac[1];
-        float wz = dz ? frac[2] : 1.0f - frac[2];
-        float w = wx * wy * wz + 1e-4f;
-        float row = pz * float(C.res[1]) + py;
-        float ox = px * 8.0f + 1.0f + ouv.x * 6.0f;
-        float oy = row * 8.0f + 1.0f + ouv.y * 6.0f;
-        float x = (ox / W) * W - 0.5f, y = (oy / H) * H - 0.5f;
-        float fx0 = floorf(x), fy0 = floorf(y);
-        float fx = x - fx0, fy = y - fy0;
-        int x0 = (int)fx0, y0 = (int)fy0;
-        int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
-        int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
-        float4 t00 = half4_to_float4(__ldg(C.atlasPrev + (size_t)ya * Wi + xa));
-        float4 t10 = half4_to_float4(__ldg(C.atlasPrev + (size_t)ya * Wi + xb));
-        float4 t01 = half4_to_float4(__ldg(C.atlasPrev + (size_t)yb * Wi + xa));
-        float4 t11 = half4_to_float4(__ldg(C.atlasPrev + (size_t)yb * Wi + xb));
-        float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
-        float3 s = mk(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
-                      t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
-                      t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
-        acc = acc + s * w;
-        wsum += w;
-    }
-    return acc * (1.0f / fmaxf(wsum, 1e-4f));
-}
-
-// shadeLight: NEE for one light, gi_probes.js:2065-2107 / 2130-2175.
-__device__ __forceinline__ void shade_light(const TraceCtx& T, const uint4* tl, uint32_t li, float3 hitPos, float3 ng,
-                                            float3 kd, float traceBias, float3& radiance, uint2& blockedBits,
-                                            uint32_t& shadowRays, Visits& vis) {
-    const float* L = T.S.lights + li * 17u;
+// The light record and the gates ahead of the shadow query
+// (gi_probes.js:2137-2157 / 2066-2084).
+__device__ __forceinline__ LightEval light_eval(const WaveCtx& W, uint32_t li, float3 hitPos, float3 ng) {
+    const float* L = W.S.lights + li * 17u;
+    LightEval e;
     float ltype = __ldg(L);
-    if (!(ltype < 2.5f)) return;
+    e.pass = false;
+    if (!(ltype < 2.5f)) return e;
     float3 lpos = mk(__ldg(L + 1), __ldg(L + 2), __ldg(L + 3));
-    float3 ldir = mk(__ldg(L + 4), __ldg(L + 5), __ldg(L + 6));
+    e.ldir = mk(__ldg(L + 4), __ldg(L + 5), __ldg(L + 6));
     float eclass = __ldg(L + 16);
     bool isIr = fabsf(eclass - 4.0f) < 0.25f;
-    float irs = isIr ? T.P.nirGate * T.P.nirGain : 1.0f;
-    float3 lcol = mk(__ldg(L + 7), __ldg(L + 8), __ldg(L + 9)) * irs;
-    float lrange = __ldg(L + 10), ldecay = __ldg(L + 11), lcosAngle = __ldg(L + 12), lcosPen = __ldg(L + 13);
-    bool isDir = ltype < 0.5f;
-    bool isSpot = fabsf(ltype - 2.0f) < 0.5f;
-    float3 toLight = isDir ? ldir * -1.0f : lpos - hitPos;
-    float dist = isDir ? 1e4f : fmaxf(sqrtf(dot3(toLight, toLight)), 1e-4f);
-    float3 wi = normalize3(toLight);
-    float ndl = fmaxf(dot3(ng, wi), 0.0f);
-    float lpeak = fmaxf(fmaxf(lcol.x, lcol.y), lcol.z);
-    if (!(ndl * lpeak > 0.0f && (isDir || lrange <= 0.0f || dist < lrange))) return;
-    ++shadowRays;
-    bool blocked = trace_any(T.S, tl, hitPos, wi, dist - traceBias, vis, T.err);
-    if (blocked) {
-        if (li < 32) blockedBits.x |= 1u << li;
-        else blockedBits.y |= 1u << (li - 32);
-        return;
-    }
-    float falloff = 1.0f / fmaxf(powf(dist, ldecay), 0.01f);
-    float rr = dist / fmaxf(lrange, 1e-4f);
+    float irs = isIr ? W.P.nirGate * W.P.nirGain : 1.0f;
+    e.lcol = mk(__ldg(L + 7), __ldg(L + 8), __ldg(L + 9)) * irs;
+    e.lrange = __ldg(L + 10);
+    e.ldecay = __ldg(L + 11);
+    e.lcosAngle = __ldg(L + 12);
+    e.lcosPen = __ldg(L + 13);
+    e.isDir = ltype < 0.5f;
+    e.isSpot = fabsf(ltype - 2.0f) < 0.5f;
+    float3 toLight = e.isDir ? e.ldir * -1.0f : lpos - hitPos;
+    e.dist = e.isDir ? 1e4f : fmaxf(sqrtf(dot3(toLight, toLight)), 1e-4f);
+    e.wi = normalize3(toLight);
+    e.ndl = fmaxf(dot3(ng, e.wi), 0.0f);
+    float lpeak = fmaxf(fmaxf(e.lcol.x, e.lcol.y), e.lcol.z);
+    e.pass = e.ndl * lpeak > 0.0f && (e.isDir || e.lrange <= 0.0f || e.dist < e.lrange);
+    return e;
+}
+
+// The unshadowed Lambert NEE term (gi_probes.js:2160-2171).
+__device__ __forceinline__ float3 light_term(const WaveCtx& W, const LightEval& e, float3 kd) {
+    float falloff = 1.0f / fmaxf(powf(e.dist, e.ldecay), 0.01f);
+    float rr = e.dist / fmaxf(e.lrange, 1e-4f);
     float rr2 = rr * rr;
     float win = clampf(1.0f - rr2 * rr2, 0.0f, 1.0f);
     float ranged = falloff * (win * win);
-    float posAtten = lrange > 0.0f ? ranged : falloff;
-    float distAtten = isDir ? 1.0f : posAtten;
-    float angleCos = dot3(wi, ldir) * -1.0f;
-    float spotAtten = clampf((angleCos - lcosAngle) / fmaxf(lcosPen - lcosAngle, 1e-4f), 0.0f, 1.0f);
-    float atten = distAtten * (isSpot ? spotAtten : 1.0f);
+    float posAtten = e.lrange > 0.0f ? ranged : falloff;
+    float distAtten = e.isDir ? 1.0f : posAtten;
+    float angleCos = dot3(e.wi, e.ldir) * -1.0f;
+    float spotAtten = clampf((angleCos - e.lcosAngle) / fmaxf(e.lcosPen - e.lcosAngle, 1e-4f), 0.0f, 1.0f);
+    float atten = distAtten * (e.isSpot ? spotAtten : 1.0f);
     float3 diffuse = kd * (1.0f / PI_F);
-    radiance = radiance + mul3(diffuse * ndl, lcol) * atten * T.P.debugDirectScale;
+    return mul3(diffuse * e.ndl, e.lcol) * (atten * W.P.debugDirectScale);
+}
+
+__device__ __forceinline__ void ray_of(const WaveCtx& W, uint32_t g, bool dirMajor, uint32_t& slot, uint32_t& k) {
+    const uint32_t N = W.C.rays;
+    uint32_t s;
+    if (dirMajor) {
+        k = g / W.slotCount;
+        s = g - k * W.slotCount;
+    } else {
+        s = g / N;
+        k = g - s * N;
+    }
+    slot = W.slotBegin + s;
+}
+
+__global__ void __launch_bounds__(256) k_trace_primary(WaveCtx W) {
+    extern __shared__ uint4 sTlas[];
+    const uint4* tl = stage_tlas(W, sTlas);
+    if (!*W.S.valid) return;
+    const DevCascade& C = W.C;
+    const uint32_t N = C.rays, total = W.slotCount * N;
+    const uint32_t lane = threadIdx.x & 31u;
+    const bool dirMajor = W.order != 0;
+    Visits vis = {0, 0, 0, 0};
+    uint32_t nRays = 0, nJobs = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&W.work[0], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= total) break;
+        const uint32_t g = base + lane;
+        const bool live = g < total;
+        uint32_t slot = 0, k = 0, rayIdx = 0;
+        float3 ro = mk(0.f, 0.f, 0.f), rd = mk(0.f, 0.f, 1.f);
+        float bestT = T_MAX, bu = 0.f, bv = 0.f;
+        int tri = -1, inst = -1;
+        HitFrame fr;
+        fr.hitPos = ro;
+        fr.ng = rd;
+        fr.faceFwd = true;
+        fr.traceBias = 0.f;
+        if (live) {
+            ray_of(W, g, dirMajor, slot, k);
+            rayIdx = slot * N + k;
+            uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+            ro = probe_world_pos(C, probeIndex);
+            rd = ray_dir(k, N, W.P.frameJitter);
+            trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err);
+            ++nRays;
+            if (tri >= 0) {
+                bestT = refine_t(W.S, (uint32_t)tri, (uint32_t)inst, ro, rd);
+                fr = hit_frame(W, (uint32_t)tri, (uint32_t)inst, ro, rd, bestT, -1);
+            }
+        }
+        // NEE candidates -> shadow-ray jobs, one ballot-compacted round per list position
+        LightList L{nullptr, 0u};
+        if (tri >= 0) L = light_list(W, fr.hitPos);
+        uint32_t maxCount = __reduce_max_sync(0xFFFFFFFFu, L.count);
+        uint32_t tested0 = 0u, tested1 = 0u;
+        for (uint32_t i = 0; i < maxCount; ++i) {
+            bool has = false;
+            uint32_t li = 0;
+            LightEval e;
+            if (i < L.count) {
+                li = light_at(L, i);
+                e = light_eval(W, li, fr.hitPos, fr.ng);
+                has = e.pass;
+            }
+            uint32_t mask = __ballot_sync(0xFFFFFFFFu, has);
+            if (mask == 0u) continue;
+            uint32_t jb = 0;
+            if (lane == 0) jb = atomicAdd(&W.work[2], (uint32_t)__popc(mask));
+            jb = __shfl_sync(0xFFFFFFFFu, jb, 0);
+            if (has) {
+                uint32_t j = jb + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+                if (j < W.jobCap) {
+                    W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, e.dist - fr.traceBias);
+                    W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float((rayIdx << 6) | li));
+                    if (li < 32) tested0 |= 1u << li;
+                    else tested1 |= 1u << (li - 32);
+                    ++nJobs;
+                } else {
+                    latch(W.err, ERR_CAPACITY);
+                }
+            }
+        }
+        if (live) {
+            uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
+            uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
+            C.hits[rayIdx] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst | (fr.faceFwd ? 0x80000000u : 0u),
+                                                   __float_as_uint(bestT), uq | (vq << 16))
+                                      : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
+            C.vis[rayIdx] = make_uint4(tested0, tested1, tested0, tested1);
+        }
+    }
+    if (W.counters) {
+        atomicAdd(&W.counters[0], (unsigned long long)nRays);
+        atomicAdd(&W.counters[1], (unsigned long long)nJobs);
+        atomicAdd(&W.counters[2], (unsigned long long)vis.tlas);
+        atomicAdd(&W.counters[3], (unsigned long long)vis.inst);
+        atomicAdd(&W.counters[4], (unsigned long long)vis.blas);
+        atomicAdd(&W.counters[5], (unsigned long long)vis.tri);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_trace_shadow(WaveCtx W) {
+    extern __shared__ uint4 sTlas[];
+    const uint4* tl = stage_tlas(W, sTlas);
+    if (!*W.S.valid) return;
+    const uint32_t total = min(*(volatile uint32_t*)&W.work[2], W.jobCap);
+    const uint32_t lane = threadIdx.x & 31u;
+    Visits vis = {0, 0, 0, 0};
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&W.work[1], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= total) break;
+        uint32_t j = base + lane;
+        if (j >= total) continue;
+        float4 a = W.jobs[2 * j], b = W.jobs[2 * j + 1];
+        if (trace_any(W.S, tl, xyz(a), xyz(b), a.w, vis, W.err)) {
+            uint32_t packed = __float_as_uint(b.w);
+            uint32_t ray = packed >> 6, li = packed & 63u;
+            uint4* v = W.C.vis + ray;
+            if (li < 32) atomicAnd(&v->z, ~(1u << li));
+            else atomicAnd(&v->w, ~(1u << (li - 32)));
+        }
+    }
+    if (W.counters) {
+        atomicAdd(&W.counters[2], (unsigned long long)vis.tlas);
+        atomicAdd(&W.counters[3], (unsigned long long)vis.inst);
+        atomicAdd(&W.counters[4], (unsigned long long)vis.blas);
+        atomicAdd(&W.counters[5], (unsigned long long)vis.tri);
+    }
 }
 
 __device__ __forceinline__ float3 sky_sh(const DevParams& P, float3 rd) {
@@ -362,145 +291,96 @@ __device__ __forceinline__ float3 sky_sh(const DevParams& P, float3 rd) {
     return mk(fmaxf(s.x, 0.f), fmaxf(s.y, 0.f), fmaxf(s.z, 0.f)) * P.skyIntensity;
 }
 
-__device__ void trace_one(const TraceCtx& T, const uint4* tl, uint32_t gid, Visits& vis, uint32_t& shadowRays) {
-    const DevCascade& C = T.C;
+__global__ void __launch_bounds__(128) k_shade(WaveCtx W) {
+    if (!*W.S.valid) return;
+    const DevCascade& C = W.C;
     const uint32_t N = C.rays;
-    uint32_t slot = gid / N, k = gid - slot * N;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= W.slotCount * N) return;
+    uint32_t slot, k;
+    ray_of(W, g, false, slot, k);
+    const uint32_t rayIdx = slot * N + k;
     uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
     float3 ro = probe_world_pos(C, probeIndex);
-    float3 rd = ray_dir(k, N, T.P.frameJitter);
-    float bestT, bu, bv;
-    int bestTri, bestInst;
-    trace_closest(T.S, tl, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, T.err);
+    float3 rd = ray_dir(k, N, W.P.frameJitter);
+    uint4 h = C.hits[rayIdx];
     float3 outRgb;
     float hitT = -1.0f;
-    uint2 blockedBits = make_uint2(0u, 0u);
-    if (bestTri >= 0) {
-        uint32_t tri = (uint32_t)bestTri, inst = (uint32_t)bestInst;
-        bestT = refine_t(T.S, tri, inst, ro, rd);
-        hitT = bestT;
-        uint32_t m = __ldg(T.S.triMaterial + tri);
-        float4 b = __ldg(T.S.tris + 3 * tri + 1), c = __ldg(T.S.tris + 3 * tri + 2);
-        float3 nl = normalize3(cross3(xyz(b), xyz(c)));
-        float4 r0 = __ldg(T.S.inst + 4 * inst), r1 = __ldg(T.S.inst + 4 * inst + 1), r2 = __ldg(T.S.inst + 4 * inst + 2);
-        float3 ngRaw = normalize3(xyz(r0) * nl.x + xyz(r1) * nl.y + xyz(r2) * nl.z);
-        bool faceFwd = dot3(ngRaw, rd) < 0.0f;
-        float3 ng = ngRaw * (faceFwd ? 1.0f : -1.0f);
-        float3 hitPoint = ro + rd * bestT;
-        float traceBias = fmaxf(C.cellMin * 0.005f * T.P.debugTraceBiasScale, RAY_EPS * T.P.debugRayEpsScale);
-        float3 hitPos = hitPoint + ng * traceBias;
-        const float* M = T.S.materials + (size_t)m * 28u;
+    if (h.x != 0xFFFFFFFFu) {
+        uint32_t tri = h.x, inst = h.y & 0x7FFFFFFFu;
+        float t = __uint_as_float(h.z);
+        hitT = t;
+        HitFrame fr = hit_frame(W, tri, inst, ro, rd, t, (int)(h.y >> 31));
+        uint32_t m = __ldg(W.S.triMaterial + tri);
+        const float* M = W.S.materials + (size_t)m * 28u;
         float3 baseColor = mk(__ldg(M), __ldg(M + 1), __ldg(M + 2));
         float3 emissive = mk(__ldg(M + 7), __ldg(M + 8), __ldg(M + 9));
-        float3 radiance = emissive * T.P.debugEmissiveScale;
+        float3 radiance = emissive * W.P.debugEmissiveScale;
         float metal = __ldg(M + 4), transm = __ldg(M + 5);
-        float3 kdr = baseColor * T.P.debugAlbedoScale * (1.0f - metal) * (1.0f - transm);
+        float3 kdr = baseColor * W.P.debugAlbedoScale * (1.0f - metal) * (1.0f - transm);
         float3 kd = mk(clampf(kdr.x, 0.f, 0.95f), clampf(kdr.y, 0.f, 0.95f), clampf(kdr.z, 0.f, 0.95f));
-        if (T.S.clustered) {
-            float3 cellCount = mk(float(C.g0Res[0]) - 1.0f, float(C.g0Res[1]) - 1.0f, float(C.g0Res[2]) - 1.0f);
-            float3 cellSize = mk(C.g0Size[0] / cellCount.x, C.g0Size[1] / cellCount.y, C.g0Size[2] / cellCount.z);
-            float3 cf = mk(floorf((hitPos.x - C.g0Min[0]) / cellSize.x), floorf((hitPos.y - C.g0Min[1]) / cellSize.y),
-                           floorf((hitPos.z - C.g0Min[2]) / cellSize.z));
-            bool outside = cf.x < 0.f || cf.y < 0.f || cf.z < 0.f || cf.x >= cellCount.x || cf.y >= cellCount.y ||
-                           cf.z >= cellCount.z;
-            uint32_t cx = (uint32_t)clampf(cf.x, 0.f, cellCount.x - 1.0f);
-            uint32_t cy = (uint32_t)clampf(cf.y, 0.f, cellCount.y - 1.0f);
-            uint32_t cz = (uint32_t)clampf(cf.z, 0.f, cellCount.z - 1.0f);
-            uint32_t cellsX = C.g0Res[0] - 1u, cellsY = C.g0Res[1] - 1u;
-            uint32_t cellIndex = cz * (cellsX * cellsY) + cy * cellsX + cx;
-            const float* list = T.S.lights + LIGHT_DATA + cellIndex * 17u;
-            uint32_t listCount = (uint32_t)__ldg(list);
-            if (outside || listCount > 16u) {
-                for (uint32_t li = 0; li < T.S.lightCount; ++li)
-                    shade_light(T, tl, li, hitPos, ng, kd, traceBias, radiance, blockedBits, shadowRays, vis);
-            } else {
-                for (uint32_t i = 0; i < listCount; ++i)
-                    shade_light(T, tl, (uint32_t)__ldg(list + 1 + i), hitPos, ng, kd, traceBias, radiance, blockedBits,
-                                shadowRays, vis);
-            }
-        } else {
-            for (uint32_t li = 0; li < T.S.lightCount; ++li)
-                shade_light(T, tl, li, hitPos, ng, kd, traceBias, radiance, blockedBits, shadowRays, vis);
+        uint4 v = C.vis[rayIdx];
+        unsigned long long ok = (unsigned long long)v.z | ((unsigned long long)v.w << 32);
+        while (ok) {
+            uint32_t li = (uint32_t)(__ffsll((long long)ok) - 1);
+            ok &= ok - 1ull;
+            LightEval e = light_eval(W, li, fr.hitPos, fr.ng);
+            radiance = radiance + light_term(W, e, kd);
         }
-        float3 bounce = mul3(sample_atlas(C, hitPos, ng), kd) * (1.0f / PI_F);
+        float3 bounce = mul3(sample_atlas(C, fr.hitPos, fr.ng), kd) * (1.0f / PI_F);
         float bl = luma3(bounce);
-        float roll = T.P.radianceClamp / fmaxf(fmaxf(T.P.radianceClamp, bl), 1e-6f);
-        radiance = radiance + bounce * roll * T.P.debugBounceScale;
-        outRgb = radiance;
-        if (C.hits) {
-            uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
-            uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
-            // bit 31 of the instance word records the facing decision (normal flipped or not)
-            C.hits[gid] = make_uint4(tri, inst | (faceFwd ? 0x80000000u : 0u), __float_as_uint(bestT), uq | (vq << 16));
-        }
+        float roll = W.P.radianceClamp / fmaxf(fmaxf(W.P.radianceClamp, bl), 1e-6f);
+        outRgb = radiance + bounce * roll * W.P.debugBounceScale;
     } else {
-        outRgb = sky_sh(T.P, rd);
-        if (C.hits) C.hits[gid] = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
+        outRgb = sky_sh(W.P, rd);
     }
-    if (C.vis) C.vis[gid] = blockedBits;
-    C.rayData[gid] = make_float4(outRgb.x, outRgb.y, outRgb.z, hitT);
+    C.rayData[rayIdx] = make_float4(outRgb.x, outRgb.y, outRgb.z, hitT);
 }
 
-__global__ void __launch_bounds__(256) k_trace_shade(TraceCtx T) {
-    extern __shared__ uint4 sTlas[];
-    const DevScene& S = T.S;
-    const uint4* tl = S.tlas;
-    if (T.smemTlas >= S.tlasNodeCount && S.tlasNodeCount > 0) {
-        for (uint32_t i = threadIdx.x; i < 2 * S.tlasNodeCount; i += blockDim.x) sTlas[i] = __ldg(S.tlas + i);
-        __syncthreads();
-        tl = sTlas;
-    }
-    if (!*S.valid) return;
-    Visits vis = {0, 0, 0, 0};
-    uint32_t shadowRays = 0, rays = 0;
-    const uint32_t lane = threadIdx.x & 31u;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(T.work, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= T.totalRays) break;
-        uint32_t gid = base + lane;
-        if (gid < T.totalRays) {
-            trace_one(T, tl, gid, vis, shadowRays);
-            ++rays;
-        }
-    }
-    if (T.counters) {
-        atomicAdd(&T.counters[0], (unsigned long long)rays);
-        atomicAdd(&T.counters[1], (unsigned long long)shadowRays);
-        atomicAdd(&T.counters[2], (unsigned long long)vis.tlas);
-        atomicAdd(&T.counters[3], (unsigned long long)vis.inst);
-        atomicAdd(&T.counters[4], (unsigned long long)vis.blas);
-        atomicAdd(&T.counters[5], (unsigned long long)vis.tri);
-    }
+static int persistent_grid(const void* kernel, int block, size_t smem, const TraceTuning& tune, uint32_t items) {
+    int perSm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, block, smem);
+    if (perSm < 1) perSm = 1;
+    int grid = tune.numSms * perSm;
+    uint32_t needed = (items + block - 1) / block;
+    if ((uint32_t)grid > needed) grid = (int)needed;
+    return grid < 1 ? 1 : grid;
 }
 
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
-                         unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st) {
-    TraceCtx T;
-    T.S = S;
-    T.C = C;
-    T.P = P;
-    T.err = err;
-    T.counters = counters;
-    T.work = work;
-    T.totalRays = C.updatedCount * C.rays;
-    if (T.totalRays == 0) return cudaSuccess;
+                         unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
+                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount) {
+    if (slotCount == 0) return cudaSuccess;
+    WaveCtx W;
+    W.S = S;
+    W.C = C;
+    W.P = P;
+    W.err = err;
+    W.counters = counters;
+    W.work = work;
+    W.jobs = jobs;
+    W.jobCap = jobCap;
+    W.slotBegin = slotBegin;
+    W.slotCount = slotCount;
+    W.order = tune.sortKey == 0 ? 1u : 0u;  // default direction-major; sortKey 1 = probe-major
     uint32_t smemNodes = S.tlasNodeCount <= tune.smemTlasNodes ? S.tlasNodeCount : 0u;
-    T.smemTlas = smemNodes ? smemNodes : 0u;
+    W.smemTlas = smemNodes;
     size_t smem = (size_t)smemNodes * 32u;
     if (smem > 48u * 1024u) {
-        cudaFuncSetAttribute(k_trace_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_trace_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
-    cudaMemsetAsync(work, 0, sizeof(uint32_t), st);
+    cudaError_t e = cudaMemsetAsync(work, 0, 3 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t rays = slotCount * C.rays;
     int block = (int)tune.block;
-    int blocksPerSm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, k_trace_shade, block, smem);
-    if (blocksPerSm < 1) blocksPerSm = 1;
-    int grid = tune.numSms * blocksPerSm;
-    uint32_t needed = (T.totalRays + block - 1) / block;
-    if ((uint32_t)grid > needed) grid = (int)needed;
-    k_trace_shade<<<grid, block, smem, st>>>(T); note_launch();
+    k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smem, tune, rays), block, smem, st>>>(W);
+    note_launch();
+    // shadow jobs: at most lightCount per ray (the queue is sized for it)
+    k_trace_shadow<<<persistent_grid((const void*)k_trace_shadow, block, smem, tune, rays * 4u), block, smem, st>>>(W);
+    note_launch();
+    k_shade<<<(rays + 127) / 128, 128, 0, st>>>(W);
+    note_launch();
     return cudaGetLastError();
 }
 
@@ -534,14 +414,16 @@ __global__ void k_occluded(DevScene S, const float* ro, const float* rd, const f
 cudaError_t launch_raycast(const DevScene& S, const float* ro, const float* rd, uint32_t n, float* tOut,
                            int32_t* triOut, int32_t* instOut, uint32_t* err, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    k_raycast<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, n, tOut, triOut, instOut, err); note_launch();
+    k_raycast<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, n, tOut, triOut, instOut, err);
+    note_launch();
     return cudaGetLastError();
 }
 
 cudaError_t launch_occluded(const DevScene& S, const float* ro, const float* rd, const float* maxDist, uint32_t n,
                             uint8_t* out, uint32_t* err, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
-    k_occluded<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, maxDist, n, out, err); note_launch();
+    k_occluded<<<(n + 127) / 128, 128, 0, st>>>(S, ro, rd, maxDist, n, out, err);
+    note_launch();
     return cudaGetLastError();
 }
 

@@ -90,12 +90,14 @@ class OracleMirror:
 
 def gpu_records(field: ProbeField, n: int) -> dict:
     hits = read(field, "HIT_RECORDS", n * 4, np.uint32).reshape(n, 4)
-    vis = read(field, "VISIBILITY", n * 2, np.uint32).reshape(n, 2)
+    vis = read(field, "VISIBILITY", n * 4, np.uint32).reshape(n, 4)
     tri = hits[:, 0].view(np.int32).copy()
     word = hits[:, 1].copy()
     inst = np.where(tri >= 0, word & 0x7FFFFFFF, 0xFFFFFFFF).astype(np.uint32).view(np.int32)
     t = hits[:, 2].view(np.float32).copy()
-    blocked = vis[:, 0].astype(np.uint64) | (vis[:, 1].astype(np.uint64) << np.uint64(32))
+    tested = vis[:, 0].astype(np.uint64) | (vis[:, 1].astype(np.uint64) << np.uint64(32))
+    unblocked = vis[:, 2].astype(np.uint64) | (vis[:, 3].astype(np.uint64) << np.uint64(32))
+    blocked = tested & ~unblocked
     # replay input keeps the facing bit in bit 31 of the instance word
     return dict(tri=np.ascontiguousarray(tri), inst=np.ascontiguousarray(inst),
                 inst_word=np.ascontiguousarray(word.view(np.int32)), facing=(word >> 31).astype(bool), t=t,
