@@ -196,11 +196,27 @@ def run_ours(args, dist: Dist):
     hits = int((ray_data[3::4] >= 0).sum())
     _abi.check(lib.sb_enable_counters(ctx, 0), ctx)
     counted = dict(primary=st.primaryRays, shadow=st.shadowRays, tlas=st.tlasNodeVisits, inst=st.instanceVisits,
-                   blas=st.blasNodeVisits, tri=st.triangleTests, hits=hits)
-    # algorithmic bytes of one trace launch (per-unit figures: 32 B TLAS node, 64 B instance record,
-    # 32 B BLAS node, 48 B triangle, 16 B ray record write, 40 B material + 256 B bounce taps per hit)
-    trace_bytes = (32 * counted["tlas"] + 64 * counted["inst"] + 32 * counted["blas"] + 48 * counted["tri"]
-                   + 16 * rays + 296 * hits)
+                   blas=st.blasNodeVisits, tri=st.triangleTests, hits=hits,
+                   shadow_tlas=st.shadowTlasNodeVisits, shadow_inst=st.shadowInstanceVisits,
+                   shadow_blas=st.shadowBlasNodeVisits, shadow_tri=st.shadowTriangleTests)
+    # algorithmic bytes per launch of each stage. Per-unit figures: 32 B TLAS node, 64 B instance
+    # record, 32 B BLAS node, 48 B pre-gathered triangle; 16 B hit record + 16 B visibility mask per
+    # ray; 32 B per shadow job (written by the primary stage, read by the shadow stage); per hit 80 B
+    # of triangle/instance rows, 40 B material, 256 B of bounce taps (8 taps x 4 texels x 8 B); 16 B
+    # ray record write; 3,776 B per probe for blend + upload.
+    def trav(t, i, b, tr):
+        return 32 * t + 64 * i + 32 * b + 48 * tr
+    jobs = counted["shadow"]
+    stage_bytes = {
+        "k_trace_primary": trav(counted["tlas"] - counted["shadow_tlas"], counted["inst"] - counted["shadow_inst"],
+                                counted["blas"] - counted["shadow_blas"], counted["tri"] - counted["shadow_tri"])
+        + 32 * rays + 32 * jobs,
+        "k_trace_shadow": trav(counted["shadow_tlas"], counted["shadow_inst"], counted["shadow_blas"],
+                               counted["shadow_tri"]) + 32 * jobs,
+        "k_shade": 48 * rays + 376 * hits,
+        "k_blend_upload": 3776 * P,
+    }
+    trace_bytes = sum(stage_bytes.values())
 
     # ---- device-resident timed loop
     for i in range(W):
@@ -211,7 +227,8 @@ def run_ours(args, dist: Dist):
     clocks = Clocks(device)
     clocks.start()
     launches0 = _stats(lib, ctx).kernelLaunches
-    total_ms, trace_ms = 0.0, []
+    total_ms = 0.0
+    stage_ms = {k: [] for k in stage_bytes}
     for i in range(K):
         flush_l2(i)
         ck(rt.cudaEventRecord(e0, stream))
@@ -220,7 +237,9 @@ def run_ours(args, dist: Dist):
         ck(rt.cudaEventSynchronize(e1))
         total_ms += ck(rt.cudaEventElapsedTime(e0, e1))
         s = _stats(lib, ctx)
-        trace_ms.append(s.lastTraceMs)
+        for k, v in (("k_trace_primary", s.lastPrimaryMs), ("k_trace_shadow", s.lastShadowMs),
+                     ("k_shade", s.lastShadeMs), ("k_blend_upload", s.lastBlendMs)):
+            stage_ms[k].append(v)
     launches = _stats(lib, ctx).kernelLaunches - launches0
     clk = clocks.stop()
     f.synchronize()
@@ -265,15 +284,17 @@ def run_ours(args, dist: Dist):
 
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    trace_avg = sum(trace_ms) / len(trace_ms)
-    achieved = trace_bytes / (trace_avg * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "trace_traffic.json"
+    stage_avg = {k: sum(v) / len(v) for k, v in stage_ms.items()}
+    dominant = max(stage_avg, key=stage_avg.get)
+    achieved = stage_bytes[dominant] / (stage_avg[dominant] * 1e-3) / 1e9
+    # DRAM bytes per launch from the committed ncu summary (lines "kernel bytes"); null when absent
+    traffic = {}
+    tf = ROOT / "profiles" / "dram_traffic.txt"
     if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("dram_bytes_per_launch")
-        except Exception:
-            traffic = None
+        for ln in tf.read_text().splitlines():
+            parts = ln.split()
+            if len(parts) >= 2 and parts[0].startswith("k_") and parts[1].isdigit():
+                traffic[parts[0]] = int(parts[1])
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -286,9 +307,13 @@ def run_ours(args, dist: Dist):
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e_ms, 4),
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": "k_trace_shade", "achieved": round(achieved, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "algorithmic_bytes_per_launch": int(trace_bytes), "trace_ms": round(trace_avg, 4),
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic.get(dominant),
+                     "algorithmic_bytes_per_launch": int(stage_bytes[dominant]),
+                     "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
+                     "stage_gbs": {k: round(stage_bytes[k] / (stage_avg[k] * 1e-3) / 1e9, 1) for k in stage_avg},
+                     "update_algorithmic_bytes": int(trace_bytes),
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s"},
         "work": {k: int(v) for k, v in counted.items()},
         "clocks": clk,

@@ -291,9 +291,14 @@ typedef struct sb_stats {
     uint64_t primaryRays, shadowRays;
     uint64_t tlasNodeVisits, instanceVisits, blasNodeVisits, triangleTests;
     float lastSolveMs;        /* trace + blend/upload of the last sb_solve (device time) */
-    float lastTraceMs;        /* trace + shade kernel alone                               */
+    float lastTraceMs;        /* the three trace stages (primary, shadow, shade)          */
     float lastBlendMs;        /* blend + upload kernel alone                              */
     uint64_t kernelLaunches;  /* kernels this library launched, process-wide              */
+    float lastPrimaryMs;      /* per stage, for solves that fit one shadow-job chunk      */
+    float lastShadowMs;
+    float lastShadeMs;
+    /* the shadow-ray share of the visit counters above */
+    uint64_t shadowTlasNodeVisits, shadowInstanceVisits, shadowBlasNodeVisits, shadowTriangleTests;
 } sb_stats;
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
 /* Counting costs a few percent; off by default. */

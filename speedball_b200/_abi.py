@@ -7,12 +7,14 @@ through the CUDA path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "libspeedball_cuda.so"
+# SB_LIB_PATH selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = Path(os.environ.get("SB_LIB_PATH", HERE / "libspeedball_cuda.so"))
 
 SB_OK = 0
 STATUS_NAMES = {
@@ -112,7 +114,10 @@ class sb_stats(C.Structure):
                 ("tlasNodeVisits", C.c_uint64), ("instanceVisits", C.c_uint64),
                 ("blasNodeVisits", C.c_uint64), ("triangleTests", C.c_uint64),
                 ("lastSolveMs", C.c_float), ("lastTraceMs", C.c_float), ("lastBlendMs", C.c_float),
-                ("kernelLaunches", C.c_uint64)]
+                ("kernelLaunches", C.c_uint64), ("lastPrimaryMs", C.c_float), ("lastShadowMs", C.c_float),
+                ("lastShadeMs", C.c_float), ("shadowTlasNodeVisits", C.c_uint64),
+                ("shadowInstanceVisits", C.c_uint64), ("shadowBlasNodeVisits", C.c_uint64),
+                ("shadowTriangleTests", C.c_uint64)]
 
 
 _P = C.c_void_p

@@ -21,6 +21,9 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
+VARIANT_SOURCES = ("sb_trace.cu",)  # the only sources that read the tuning macros
+
+
 def sources():
     return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
 
@@ -32,26 +35,37 @@ def _stale(target: Path, deps) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, defines=(), out: Path | None = None) -> Path:
+    """Compile and link. `defines` (e.g. ["SB_PRIMARY_MIN_BLOCKS=3"]) and `out`
+    build a variant library elsewhere without touching the default one."""
+    build_dir = BUILD if not defines else BUILD / ("v_" + "_".join(d.replace("=", "") for d in defines))
+    build_dir.mkdir(parents=True, exist_ok=True)
+    lib = out or LIB
     headers = list(CSRC.glob("*.cuh")) + list((HERE.parent / "include").glob("*.h"))
     objs = []
+    dflags = [f"-D{d}" for d in defines]
     for src in sources():
-        obj = BUILD / (src.stem + ".o")
+        obj = build_dir / (src.stem + ".o")
+        if defines and src.name not in VARIANT_SOURCES:
+            obj = BUILD / (src.stem + ".o")  # unaffected by the variant macros: reuse
+            if force or _stale(obj, [src] + headers):
+                subprocess.run([NVCC, *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)], check=True)
+            objs.append(obj)
+            continue
         objs.append(obj)
         if force or _stale(obj, [src] + headers):
-            cmd = [NVCC, *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
+            cmd = [NVCC, *ARCH, *FLAGS, *dflags, "-c", str(src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
-    if force or _stale(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-cudart", "static"]
+    if force or _stale(lib, objs):
+        cmd = [NVCC, *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-cudart", "static"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    build(verbose=True, force="--force" in sys.argv)
+    build(verbose="-v" in sys.argv, force="--force" in sys.argv)
     print(LIB)

@@ -75,8 +75,9 @@ struct sb_ctx {
     TraceTuning tune{256u, 2048u, 0u, 148};
     float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
     uint32_t jobCap = 0;
-    cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
     bool timed = false;
+    bool singleChunk = true;
 };
 
 namespace {
@@ -271,14 +272,16 @@ sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
         if (cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking) != cudaSuccess) { st = SB_ERR_CUDA; break; }
         ctx->stream = ctx->ownStream;
         if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 4) != cudaSuccess ||
-            cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 8 * 8) != cudaSuccess ||
+            cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 16 * 8) != cudaSuccess ||
             cudaMalloc(&ctx->B.valid, 4) != cudaSuccess) { st = SB_ERR_OOM; break; }
         cudaMemset(ctx->dErr, 0, 4);
         cudaMemset(ctx->B.valid, 0, 4);
-        cudaMemset(ctx->dCounters, 0, 64);
+        cudaMemset(ctx->dCounters, 0, 128);
         cudaEventCreate(&ctx->ev0);
         cudaEventCreate(&ctx->evMid);
         cudaEventCreate(&ctx->ev1);
+        cudaEventCreate(&ctx->evA);
+        cudaEventCreate(&ctx->evB);
         sb_params_defaults(&ctx->params);
         if (cudaDeviceSynchronize() != cudaSuccess) { st = SB_ERR_CUDA; break; }
     } while (0);
@@ -310,6 +313,8 @@ void sb_destroy(sb_ctx* ctx) {
     release(ctx->dErr); release(ctx->dGate); release(ctx->dWork); release(ctx->dCounters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->evMid) cudaEventDestroy(ctx->evMid);
+    if (ctx->evA) cudaEventDestroy(ctx->evA);
+    if (ctx->evB) cudaEventDestroy(ctx->evB);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
     delete ctx;
@@ -614,12 +619,13 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
         ctx->jobCap = (uint32_t)want;
     }
     const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
-    if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 64, ctx->stream));
+    if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 128, ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    ctx->singleChunk = updatedCount <= chunk;
     for (uint32_t s0 = 0; s0 < updatedCount; s0 += chunk) {
         uint32_t n = updatedCount - s0 < chunk ? updatedCount - s0 : chunk;
         CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune,
-                        ctx->stream, ctx->jobs, ctx->jobCap, s0, n));
+                        ctx->stream, ctx->jobs, ctx->jobCap, s0, n, ctx->evA, ctx->evB));
     }
     CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
@@ -794,20 +800,29 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->countersOn) {
-        unsigned long long c[8];
-        CK(cudaMemcpy(c, ctx->dCounters, 64, cudaMemcpyDeviceToHost));
+        unsigned long long c[16];
+        CK(cudaMemcpy(c, ctx->dCounters, sizeof c, cudaMemcpyDeviceToHost));
         out->primaryRays = c[0];
         out->shadowRays = c[1];
-        out->tlasNodeVisits = c[2];
-        out->instanceVisits = c[3];
-        out->blasNodeVisits = c[4];
-        out->triangleTests = c[5];
+        out->tlasNodeVisits = c[2] + c[6];
+        out->instanceVisits = c[3] + c[7];
+        out->blasNodeVisits = c[4] + c[8];
+        out->triangleTests = c[5] + c[9];
+        out->shadowTlasNodeVisits = c[6];
+        out->shadowInstanceVisits = c[7];
+        out->shadowBlasNodeVisits = c[8];
+        out->shadowTriangleTests = c[9];
     }
     if (ctx->timed) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) out->lastSolveMs = ms;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evMid) == cudaSuccess) out->lastTraceMs = ms;
         if (cudaEventElapsedTime(&ms, ctx->evMid, ctx->ev1) == cudaSuccess) out->lastBlendMs = ms;
+        if (ctx->singleChunk) {
+            if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evA) == cudaSuccess) out->lastPrimaryMs = ms;
+            if (cudaEventElapsedTime(&ms, ctx->evA, ctx->evB) == cudaSuccess) out->lastShadowMs = ms;
+            if (cudaEventElapsedTime(&ms, ctx->evB, ctx->evMid) == cudaSuccess) out->lastShadeMs = ms;
+        }
     }
     out->kernelLaunches = launches();
     return SB_OK;

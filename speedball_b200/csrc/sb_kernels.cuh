@@ -38,7 +38,8 @@ struct SceneBuffers {
 // `jobs` holds up to jobCap shadow-ray jobs (32 bytes each).
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
                          unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
-                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount);
+                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
+                         cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st);
 cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st);

@@ -160,7 +160,16 @@ __device__ __forceinline__ void ray_of(const WaveCtx& W, uint32_t g, bool dirMaj
     slot = W.slotBegin + s;
 }
 
-__global__ void __launch_bounds__(256) k_trace_primary(WaveCtx W) {
+// Resident 256-thread blocks per SM the register allocation must allow
+// (4 x 256 threads: 64 registers; measured best for both traversal stages).
+#ifndef SB_PRIMARY_MIN_BLOCKS
+#define SB_PRIMARY_MIN_BLOCKS 4
+#endif
+#ifndef SB_SHADOW_MIN_BLOCKS
+#define SB_SHADOW_MIN_BLOCKS 4
+#endif
+
+__global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(WaveCtx W) {
     extern __shared__ uint4 sTlas[];
     const uint4* tl = stage_tlas(W, sTlas);
     if (!*W.S.valid) return;
@@ -250,7 +259,7 @@ __global__ void __launch_bounds__(256) k_trace_primary(WaveCtx W) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_trace_shadow(WaveCtx W) {
+__global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(WaveCtx W) {
     extern __shared__ uint4 sTlas[];
     const uint4* tl = stage_tlas(W, sTlas);
     if (!*W.S.valid) return;
@@ -274,10 +283,10 @@ __global__ void __launch_bounds__(256) k_trace_shadow(WaveCtx W) {
         }
     }
     if (W.counters) {
-        atomicAdd(&W.counters[2], (unsigned long long)vis.tlas);
-        atomicAdd(&W.counters[3], (unsigned long long)vis.inst);
-        atomicAdd(&W.counters[4], (unsigned long long)vis.blas);
-        atomicAdd(&W.counters[5], (unsigned long long)vis.tri);
+        atomicAdd(&W.counters[6], (unsigned long long)vis.tlas);
+        atomicAdd(&W.counters[7], (unsigned long long)vis.inst);
+        atomicAdd(&W.counters[8], (unsigned long long)vis.blas);
+        atomicAdd(&W.counters[9], (unsigned long long)vis.tri);
     }
 }
 
@@ -349,7 +358,8 @@ static int persistent_grid(const void* kernel, int block, size_t smem, const Tra
 
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
                          unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
-                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount) {
+                         float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
+                         cudaEvent_t afterPrimary, cudaEvent_t afterShadow) {
     if (slotCount == 0) return cudaSuccess;
     WaveCtx W;
     W.S = S;
@@ -376,9 +386,11 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     int block = (int)tune.block;
     k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smem, tune, rays), block, smem, st>>>(W);
     note_launch();
+    if (afterPrimary) cudaEventRecord(afterPrimary, st);
     // shadow jobs: at most lightCount per ray (the queue is sized for it)
     k_trace_shadow<<<persistent_grid((const void*)k_trace_shadow, block, smem, tune, rays * 4u), block, smem, st>>>(W);
     note_launch();
+    if (afterShadow) cudaEventRecord(afterShadow, st);
     k_shade<<<(rays + 127) / 128, 128, 0, st>>>(W);
     note_launch();
     return cudaGetLastError();
