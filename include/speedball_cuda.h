@@ -219,6 +219,32 @@ sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float
  * reference's CPU walk. Layout violations latch SB_ERR_LAYOUT_VIOLATION. */
 sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end);
 
+/* BLAS refit that allocates nothing. No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: hosts whose device memory belongs to
+ * another allocator (an engine heap or interop pool that hands out only its own
+ * buffers), and per-frame paths where an allocation's implicit device-wide
+ * synchronisation would stall the frame. sb_create allocates, so this entry
+ * point takes no context: the caller passes device pointers to its own node
+ * (8 x u32 per node, updated in place), triangle-index (3 x u32) and vertex
+ * (8 x f32) buffers. Node bounds over [root, end) come out bit-identical to
+ * sb_refit_blas on the same inputs; the pre-gathered triangles of a context are
+ * not touched. The refit's scratch (parent links, arrival counters, the layout
+ * gate) is one file-scope device array of 2 * SB_REFIT_STATIC_MAX_NODES + 64
+ * u32 (4 MiB), held by every device that loads the library until exit; ranges
+ * of more than SB_REFIT_STATIC_MAX_NODES nodes return SB_ERR_INVALID_ARG.
+ * The first call on a device, with that device current, looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any stream
+ * capture. Every call shares the array and clears the part it uses; calls that
+ * overlap on the GPU (other streams or host threads) race on it. The call runs
+ * on `cuda_stream` (NULL = legacy default stream) and synchronises it to read
+ * the gate. Errors: SB_ERR_INVALID_ARG, SB_ERR_LAYOUT_VIOLATION (rebuild),
+ * SB_ERR_NO_DEVICE, SB_ERR_CUDA; `msg` (may be NULL) receives the text. */
+#define SB_REFIT_STATIC_MAX_NODES 524288u
+sb_status sb_refit_blas_static(uint32_t* nodes, uint32_t nodeCount, const uint32_t* triIndex,
+                               uint32_t triCount, const float* vertexData, uint32_t vertexCount,
+                               uint32_t root, uint32_t end, void* cuda_stream, char* msg,
+                               size_t msgLen);
+
 /* Deform lane for one BLAS (updateDeforms, spectral_scene.js:1831-1927): writes
  * vertexCount pooled vertices (8 floats each) from vertexStart, then refits the
  * BLAS [root, end) and re-gathers its triangles. The vertices must be the
