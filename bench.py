@@ -115,10 +115,18 @@ class Clocks:
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.fh,
                                          stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        # nvidia-smi takes a moment to start: wait for its first sample so the
+        # samples cover the timed region rather than the time after it
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if self.path.stat().st_size > 0:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if not self.proc:

@@ -9,67 +9,122 @@
 
 namespace sb {
 
-// Kahan-compensated FP32 accumulator.
-struct Kahan {
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x) {
-        float y = x - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
+// One CTA blends BLEND_PROBES probes, one thread per (probe, interior texel).
+// The cosine weight pow(max(dot(texelDir, rayDir), 0), cosPow) and the depth
+// weight pow(cw, depthSharpness) depend on (texel, ray) only, not on the probe,
+// so the CTA builds that 36 x rays table once in shared memory and every probe
+// reuses it; per (texel, ray) the loop is then 9 FMA/ADD on shared operands.
+// Per-ray features (radiance, luma, luma^2, hit distance, distance^2) are also
+// formed once per ray instead of once per (texel, ray). Sums run in ray order
+// in FP32; every term is non-negative, so the relative error of a sum stays
+// under rays * 2^-24 (1.5e-5 at 256 rays).
+constexpr int BLEND_PROBES = 8;
+constexpr int BLEND_TEXELS = OCT * OCT;
+constexpr int BLEND_THREADS = BLEND_PROBES * BLEND_TEXELS;  // 288 = 9 warps
+constexpr int BLEND_CHUNK = 64;                             // rays staged per pass
+
+struct BlendSmem {
+    float4 texDir[BLEND_TEXELS];
+    float4 rayDir[BLEND_CHUNK];
+    float wc[BLEND_CHUNK][BLEND_TEXELS];  // cosine weight  [ray][texel]
+    float wd[BLEND_CHUNK][BLEND_TEXELS];  // depth weight   [ray][texel]
+    union {
+        struct {
+            float4 fa[BLEND_PROBES][BLEND_CHUNK + 1];  // r, g, b, luma (row pad shifts banks)
+            float4 fb[BLEND_PROBES][BLEND_CHUNK + 1];  // luma^2, dist, dist^2, -
+        } f;
+        float4 out[BLEND_PROBES][BLEND_TEXELS];        // filtered irradiance (after the sums)
+    } u;
+    float4 irr[BLEND_PROBES][BLEND_TEXELS];
+    float2 dep[BLEND_PROBES][BLEND_TEXELS];
 };
 
-__global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) {
-    __shared__ float4 rayC[256];
-    __shared__ float4 dirC[256];
-    __shared__ float4 irrS[36];
-    __shared__ float2 depS[36];
-    __shared__ float4 outI[36];
-    const uint32_t slot = blockIdx.x;
-    const uint32_t lane = threadIdx.x;
-    if (slot >= C.updatedCount) return;  // uniform per block
+__global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, DevParams P) {
+    __shared__ BlendSmem S;
+    const int tid = threadIdx.x;
+    const int p = tid / BLEND_TEXELS, lane = tid % BLEND_TEXELS;
+    const uint32_t base = blockIdx.x * BLEND_PROBES;
+    const uint32_t slot = base + p;
+    const bool live = slot < C.updatedCount;
     const uint32_t N = C.rays;
-    const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
-    for (uint32_t k = lane; k < N; k += 64) {
-        rayC[k] = C.rayData[(size_t)slot * N + k];
-        float3 d = ray_dir(k, N, P.frameJitter);
-        dirC[k] = make_float4(d.x, d.y, d.z, 0.0f);
+    const uint32_t nProbes = min((uint32_t)BLEND_PROBES, C.updatedCount - base);
+    const float cosPow = fmaxf(P.debugCosinePower, 1e-4f);
+    const bool cosUnit = cosPow == 1.0f;  // pow(x, 1) == x exactly
+    const uint32_t sharpN = (uint32_t)P.depthSharpness;
+    const bool sharpInt = P.depthSharpness >= 1.0f && P.depthSharpness <= 16.0f && float(sharpN) == P.depthSharpness;
+    if (tid < BLEND_TEXELS) {
+        float u = (float(tid % OCT) + 0.5f) / 6.0f, v = (float(tid / OCT) + 0.5f) / 6.0f;
+        float3 d = oct_decode(u, v);
+        S.texDir[tid] = make_float4(d.x, d.y, d.z, 0.0f);
     }
-    __syncthreads();
 
-    if (lane < 36) {
-        const uint32_t lx = lane % OCT + BORDER, ly = lane / OCT + BORDER;
-        const uint32_t local = ly * TILE + lx;
-        float u = (float(lx) - 1.0f + 0.5f) / 6.0f, v = (float(ly) - 1.0f + 0.5f) / 6.0f;
-        float3 dir = oct_decode(u, v);
-        Kahan ar, ag, ab, wsum, lAcc, lAcc2, dAcc, dAcc2, dwsum;
-        const float cosPow = fmaxf(P.debugCosinePower, 1e-4f);
-        for (uint32_t k = 0; k < N; ++k) {
-            float4 r = rayC[k];
-            float4 d = dirC[k];
-            float cd = fmaxf(dir.x * d.x + dir.y * d.y + dir.z * d.z, 0.0f);
-            float cw = powf(cd, cosPow);
-            ar.add(r.x * cw);
-            ag.add(r.y * cw);
-            ab.add(r.z * cw);
-            wsum.add(cw);
+    float sr = 0.f, sg = 0.f, sb = 0.f, sl = 0.f, sl2 = 0.f, ws = 0.f, sd = 0.f, sd2 = 0.f, dws = 0.f;
+    for (uint32_t c = 0; c < N; c += BLEND_CHUNK) {
+        const uint32_t n = min((uint32_t)BLEND_CHUNK, N - c);
+        __syncthreads();  // previous pass done with the table and features
+        for (uint32_t e = tid; e < nProbes * n; e += BLEND_THREADS) {
+            uint32_t q = e / n, k = e % n;
+            float4 r = C.rayData[(size_t)(base + q) * N + c + k];
             float rl = luma3(mk(r.x, r.y, r.z));
-            lAcc.add(rl * cw);
-            lAcc2.add(rl * rl * cw);
             float hitT = r.w;
             float decoded = hitT < -1.5f ? -hitT - 2.0f : hitT;
             float rdist = hitT == -1.0f ? C.maxDist : decoded;
-            float dw = powf(cw, P.depthSharpness);
-            dAcc.add(rdist * dw);
-            dAcc2.add(rdist * rdist * dw);
-            dwsum.add(dw);
+            S.u.f.fa[q][k] = make_float4(r.x, r.y, r.z, rl);
+            S.u.f.fb[q][k] = make_float4(rl * rl, rdist, rdist * rdist, 0.0f);
         }
-        float wden = fmaxf(wsum.s, 1e-4f);
-        float3 meanRad = mk(ar.s / wden, ag.s / wden, ab.s / wden);
-        float curL = lAcc.s / wden, curM2 = lAcc2.s / wden;
-        float dden = fmaxf(dwsum.s, 1e-4f);
-        float meanR = dAcc.s / dden, meanR2 = dAcc2.s / dden;
+        if ((uint32_t)tid < n) {
+            float3 d = ray_dir(c + tid, N, P.frameJitter);
+            S.rayDir[tid] = make_float4(d.x, d.y, d.z, 0.0f);
+        }
+        __syncthreads();
+        for (uint32_t e = tid; e < n * BLEND_TEXELS; e += BLEND_THREADS) {
+            uint32_t k = e / BLEND_TEXELS, j = e % BLEND_TEXELS;
+            float4 a = S.texDir[j], b = S.rayDir[k];
+            float cd = fmaxf(a.x * b.x + a.y * b.y + a.z * b.z, 0.0f);
+            float cw = cosUnit ? cd : powf(cd, cosPow);
+            float dw;
+            if (sharpInt) {  // small integer exponent: square-and-multiply (a few ulp of powf)
+                dw = 1.0f;
+                float x = cw;
+                for (uint32_t m = sharpN; m; m >>= 1) {
+                    if (m & 1u) dw *= x;
+                    x *= x;
+                }
+            } else {
+                dw = powf(cw, P.depthSharpness);
+            }
+            S.wc[k][j] = cw;
+            S.wd[k][j] = dw;
+        }
+        __syncthreads();
+        if (live) {
+#pragma unroll 4
+            for (uint32_t k = 0; k < n; ++k) {
+                float w = S.wc[k][lane], v = S.wd[k][lane];
+                float4 a = S.u.f.fa[p][k], b = S.u.f.fb[p][k];
+                sr = fmaf(w, a.x, sr);
+                sg = fmaf(w, a.y, sg);
+                sb = fmaf(w, a.z, sb);
+                sl = fmaf(w, a.w, sl);
+                sl2 = fmaf(w, b.x, sl2);
+                ws += w;
+                sd = fmaf(v, b.y, sd);
+                sd2 = fmaf(v, b.z, sd2);
+                dws += v;
+            }
+        }
+    }
+    __syncthreads();  // features no longer read: S.u.out may be written
+
+    const uint32_t probeIndex = live ? (C.probeOffset + slot) % C.probeTotal : 0u;
+    if (live) {
+        const uint32_t lx = lane % OCT + BORDER, ly = lane / OCT + BORDER;
+        const uint32_t local = ly * TILE + lx;
+        float wden = fmaxf(ws, 1e-4f);
+        float3 meanRad = mk(sr / wden, sg / wden, sb / wden);
+        float curL = sl / wden, curM2 = sl2 / wden;
+        float dden = fmaxf(dws, 1e-4f);
+        float meanR = sd / dden, meanR2 = sd2 / dden;
 
         const size_t ib = (size_t)probeIndex * 64u + local;
         float4 prev4 = C.irr[ib];
@@ -108,15 +163,15 @@ __global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) 
         float dh = dWasZero ? 0.0f : depthH;
         float2 outDep = make_float2(mixf(meanR, dprev.x, dh), mixf(meanR2, dprev.y, dh));
         C.depth[ib] = outDep;
-        irrS[lane] = outIrr;
-        depS[lane] = outDep;
+        S.irr[p][lane] = outIrr;
+        S.dep[p][lane] = outDep;
     }
     __syncthreads();
 
     // upload: 3x3 bilateral filter of the new history (reads this tile only)
-    if (lane < 36) {
+    if (live) {
         const int sx = (int)(lane % OCT), sy = (int)(lane / OCT);
-        float4 c4 = irrS[lane];
+        float4 c4 = S.irr[p][lane];
         float3 eC = xyz(c4);
         float lumaC = luma3(eC);
         float varC = fmaxf(c4.w - lumaC * lumaC, 0.0f);
@@ -134,7 +189,7 @@ __global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) 
                                  : (jx == 0 || jy == 0) ? 0.6065306597126334f   // exp(-0.5)
                                                         : 0.36787944117144233f; // exp(-1)
                 int nx = min(max(sx + jx, 0), OCT - 1), ny = min(max(sy + jy, 0), OCT - 1);
-                float3 en = xyz(irrS[ny * OCT + nx]);
+                float3 en = xyz(S.irr[p][ny * OCT + nx]);
                 float dl = luma3(en) - lumaC;
                 float es = expf(dl * dl / den * -1.0f);
                 float w = gw * es;
@@ -144,14 +199,16 @@ __global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) 
         float fden = fmaxf(fw, 1e-4f);
         float3 filt = mk(facc.x / fden, facc.y / fden, facc.z / fden);
         float s = P.filterStrength;
-        outI[lane] = make_float4(mixf(eC.x, filt.x, s), mixf(eC.y, filt.y, s), mixf(eC.z, filt.z, s), 1.0f);
+        S.u.out[p][lane] = make_float4(mixf(eC.x, filt.x, s), mixf(eC.y, filt.y, s), mixf(eC.z, filt.z, s), 1.0f);
     }
     __syncthreads();
 
-    // 64 lanes: interior + canonical mirrored gutter (gi_probes.js:2816-2839)
-    {
+    // 64 texels per probe: interior + canonical mirrored gutter (gi_probes.js:2816-2839)
+    for (uint32_t e = tid; e < nProbes * 64u; e += BLEND_THREADS) {
+        const uint32_t q = e / 64u, texel = e % 64u;
+        const uint32_t probeIndex = (C.probeOffset + base + q) % C.probeTotal;
         const int edge = TILE - 1, lo = BORDER, hi = BORDER + OCT - 1;
-        int lx = (int)(lane % TILE), ly = (int)(lane / TILE);
+        int lx = (int)(texel % TILE), ly = (int)(texel / TILE);
         bool onLeft = lx == 0, onRight = lx == edge, onTop = ly == 0, onBottom = ly == edge;
         bool colB = onLeft || onRight, rowB = onTop || onBottom, corner = colB && rowB;
         int sx = corner ? (onLeft ? hi : lo) : (rowB ? edge - lx : (colB ? (onLeft ? lo : hi) : lx));
@@ -160,15 +217,16 @@ __global__ void __launch_bounds__(64) k_blend_upload(DevCascade C, DevParams P) 
         uint32_t col = probeIndex % C.res[0];
         uint32_t row = (probeIndex / (C.res[0] * C.res[1])) * C.res[1] + (probeIndex / C.res[0]) % C.res[1];
         size_t t = (size_t)(row * TILE + ly) * C.atlasW + col * TILE + lx;
-        C.atlas[t] = float4_to_half4(outI[src]);
-        float2 d = depS[src];
+        C.atlas[t] = float4_to_half4(S.u.out[q][src]);
+        float2 d = S.dep[q][src];
         C.depthAtlas[t] = float4_to_half4(make_float4(d.x, d.y, 0.0f, 1.0f));
     }
 }
 
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st) {
     if (C.updatedCount == 0) return cudaSuccess;
-    k_blend_upload<<<C.updatedCount, 64, 0, st>>>(C, P); note_launch();
+    const uint32_t blocks = (C.updatedCount + BLEND_PROBES - 1) / BLEND_PROBES;
+    k_blend_upload<<<blocks, BLEND_THREADS, 0, st>>>(C, P); note_launch();
     return cudaGetLastError();
 }
 
