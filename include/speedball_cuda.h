@@ -303,9 +303,13 @@ sb_status sb_graph_launch(sb_ctx* ctx);
 
 typedef struct sb_tuning {
     uint32_t traceBlock;      /* threads per block of the trace kernels            */
-    uint32_t sortKey;         /* 0 = probe order, 1 = direction-octant ray order   */
+    uint32_t sortKey;         /* ray issue order: 0 = direction-major (ray k of
+                                 neighbouring probes per warp), 1 = probe-major   */
     uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
-    uint32_t bvhKind;         /* 0 = reference threaded FP32 nodes, 1 = wide8 q8   */
+    uint32_t bvhKind;         /* 2 = scene BVH over (triangle, instance) items,
+                                 rebuilt on structural changes (default);
+                                 0 = the reference's TLAS + BLASes;
+                                 1 = wide 8-bit quantised (not built)             */
 } sb_tuning;
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);

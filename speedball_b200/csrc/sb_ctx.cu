@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "sb_flat_scene.cuh"
 #include "sb_kernels.cuh"
 
 using namespace sb;
@@ -72,7 +73,9 @@ struct sb_ctx {
     bool lightGridDirty = false;
     std::vector<float> hostLights;
 
-    TraceTuning tune{256u, 2048u, 0u, 148};
+    TraceTuning tune{256u, 512u, 0u, 148};  // 512 TLAS nodes = 32 KB of child pairs per CTA
+    uint32_t bvhKind = 2;          // 0 = the reference's TLAS + BLASes, 2 = scene BVH (sb_flat.h)
+    FlatScene flat;
     float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
     uint32_t jobCap = 0;
     cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
@@ -137,6 +140,11 @@ DevScene dev_scene(const sb_ctx* c) {
     S.lights = c->B.lights;
     S.triIndex = c->B.triIndex;
     S.vertexData = c->B.vertexData;
+    S.pairs = c->B.pairs;
+    S.tlasPairs = c->B.tlasPairs;
+    S.depth = c->B.depth;
+    c->flat.fill(S);
+    S.slotBounds = c->instancesSet && c->tlasOnDevice ? c->I.liveBounds : nullptr;
     S.nodeCount = c->B.nodeCount;
     S.triCount = c->B.triCount;
     S.instCount = c->B.instCount;
@@ -193,6 +201,17 @@ sb_status pack_if_needed(sb_ctx* ctx) {
     if (!ctx->tlasPending && ctx->B.tlasNodeCount && ctx->instancesSet)
         CK(launch_tlas_index(ctx->B, ctx->I, ctx->instOwner, ctx->dErr, ctx->stream));
     ctx->needPack = false;
+    return SB_OK;
+}
+
+// The scene BVH of bvhKind 2: rebuilt after structural changes, marks of moved
+// slots uploaded. A build that cannot serve (too deep, too large) leaves the
+// reference two-level walk in use.
+sb_status flat_if_needed(sb_ctx* ctx) {
+    ctx->flat.enabled = ctx->bvhKind == 2;
+    std::string why;
+    const bool order = ctx->tlasOnDevice && ctx->instancesSet;
+    CK(ctx->flat.prepare(ctx->B, order ? ctx->I.order : nullptr, order ? ctx->I.count : 0u, ctx->stream, why));
     return SB_OK;
 }
 
@@ -273,9 +292,13 @@ sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
         ctx->stream = ctx->ownStream;
         if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 4) != cudaSuccess ||
             cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 16 * 8) != cudaSuccess ||
-            cudaMalloc(&ctx->B.valid, 4) != cudaSuccess) { st = SB_ERR_OOM; break; }
+            cudaMalloc(&ctx->B.valid, 4) != cudaSuccess || cudaMalloc(&ctx->B.depth, 8) != cudaSuccess) {
+            st = SB_ERR_OOM;
+            break;
+        }
         cudaMemset(ctx->dErr, 0, 4);
         cudaMemset(ctx->B.valid, 0, 4);
+        cudaMemset(ctx->B.depth, 0xFF, 8);
         cudaMemset(ctx->dCounters, 0, 128);
         cudaEventCreate(&ctx->ev0);
         cudaEventCreate(&ctx->evMid);
@@ -300,7 +323,8 @@ void sb_destroy(sb_ctx* ctx) {
     SceneBuffers& B = ctx->B;
     release(B.nodes); release(B.triIndex); release(B.vertexData); release(B.triMaterial); release(B.materials);
     release(B.lights); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
-    release(B.arrive); release(B.valid);
+    release(B.arrive); release(B.valid); release(B.pairs); release(B.tlasPairs); release(B.depth);
+    ctx->flat.release();
     InstanceTable& I = ctx->I;
     release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb); release(I.invRows);
     release(I.detSign); release(I.order); release(I.slotOf); release(I.liveBounds); release(I.nodeDepth);
@@ -386,14 +410,18 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     CK(grow(B.vertexData, ctx->cap[2], nV));
     CK(grow(B.triMaterial, ctx->cap[3], (size_t)v->triCount));
     CK(grow(B.materials, ctx->cap[4], matLen));
-    size_t cTris = 0, cInst = 0, cTlas = 0, cBits = 0, cPar = 0, cArr = 0;
+    size_t cTris = 0, cInst = 0, cTlas = 0, cBits = 0, cPar = 0, cArr = 0, cPairs = 0, cTlasPairs = 0;
     release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent); release(B.arrive);
+    release(B.pairs); release(B.tlasPairs);
     CK(grow(B.tris, cTris, (size_t)v->triCount * 3));
     CK(grow(B.inst, cInst, (size_t)v->instCount * 4));
     CK(grow(B.tlas, cTlas, (size_t)tlasNodes * 2));
     CK(grow(B.matBits, cBits, (size_t)v->materialCount));
     CK(grow(B.parent, cPar, (size_t)v->nodeCount));
     CK(grow(B.arrive, cArr, (size_t)v->nodeCount));
+    if (v->nodeCount < PE_BLAS_MAX_NODES) CK(grow(B.pairs, cPairs, (size_t)v->nodeCount * 4));
+    CK(grow(B.tlasPairs, cTlasPairs, (size_t)tlasNodes * 4));
+    CK(cudaMemsetAsync(B.depth, 0xFF, 8, ctx->stream));  // no pair layout until the pack derives it
     CK(cudaMemcpyAsync(B.nodes, v->bvhNodes, nN * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(B.triIndex, v->triIndex, nT * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(B.vertexData, v->vertexData, nV * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -413,6 +441,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     ctx->tlasPending = v->tlasNodeCount == 0;
     ctx->tlasOnDevice = false;
     ctx->sceneLoaded = true;
+    ctx->flat.dirty = true;
     if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
     // validation + derived layouts; a pending TLAS is packed by sb_build_tlas
     uint32_t one = 1u;
@@ -461,7 +490,10 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
     if (!dst) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not allocated", buf);
     if ((size_t)start + count > len) return fail(ctx, SB_ERR_INVALID_ARG, "range [%u,+%u) outside %zu", start, count, len);
     CK(cudaMemcpyAsync((char*)dst + (size_t)start * esz, src, (size_t)count * esz, cudaMemcpyHostToDevice, ctx->stream));
-    if (buf <= SB_BUF_MATERIALS) ctx->needPack = true;
+    if (buf <= SB_BUF_MATERIALS) {
+        ctx->needPack = true;
+        ctx->flat.dirty = true;
+    }
     if (buf == SB_BUF_LIGHTS && ctx->clustered) ctx->lightGridDirty = true;
     return SB_OK;
 }
@@ -602,6 +634,8 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     if (s != SB_OK) return s;
     s = light_grid_if_needed(ctx);
     if (s != SB_OK) return s;
+    s = flat_if_needed(ctx);
+    if (s != SB_OK) return s;
     DevScene S = dev_scene(ctx);
     DevCascade D = dev_cascade(ctx, ci, probeOffset, updatedCount);
     DevParams P;
@@ -642,6 +676,8 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
     cudaSetDevice(ctx->device);
     sb_status s = pack_if_needed(ctx);
     if (s != SB_OK) return s;
+    s = flat_if_needed(ctx);
+    if (s != SB_OK) return s;
     float *dro = nullptr, *drd = nullptr, *dt = nullptr;
     int32_t *dtri = nullptr, *dinst = nullptr;
     CK(cudaMallocAsync(&dro, (size_t)n * 12, ctx->stream));
@@ -666,6 +702,8 @@ sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float
     if (n == 0) return SB_OK;
     cudaSetDevice(ctx->device);
     sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    s = flat_if_needed(ctx);
     if (s != SB_OK) return s;
     float *dro = nullptr, *drd = nullptr, *dm = nullptr;
     uint8_t* dout = nullptr;
@@ -693,6 +731,7 @@ sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end) {
     sb_status s = pack_if_needed(ctx);
     if (s != SB_OK) return s;
     CK(launch_refit_blas(ctx->B, root, end, ctx->dErr, ctx->dGate, ctx->stream));
+    ctx->flat.mark_blas_range(root, end);  // its instances leave the scene BVH
     return SB_OK;
 }
 
@@ -732,6 +771,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
     CK(cudaMemcpyAsync(I.blasRoot, blasRoot, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(I.blasEnd, blasEnd, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
     ctx->instancesSet = true;
+    ctx->flat.dirty = true;
     if (!ctx->tlasPending) {
         // the uploaded TLAS stays; derive the slot maps from it on the next pack
         ctx->needPack = true;
@@ -751,6 +791,8 @@ sb_status sb_build_tlas(sb_ctx* ctx) {
     sb_status s = pack_if_needed(ctx);
     if (s != SB_OK) return s;
     CK(launch_tlas_build(ctx->B, ctx->I, ctx->dErr, ctx->stream));
+    CK(launch_tlas_pairs(ctx->B, ctx->stream));
+    ctx->flat.dirty = true;
     ctx->tlasPending = false;
     ctx->tlasOnDevice = true;
     return SB_OK;
@@ -779,6 +821,7 @@ sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* src, const double* w
         CK(cudaMemcpyAsync(ctx->dStage, src, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemcpyAsync(ctx->dStageM, world16, (size_t)count * 128, cudaMemcpyHostToDevice, ctx->stream));
         CK(launch_update_instances(ctx->B, ctx->I, ctx->dStage, ctx->dStageM, count, 1, ctx->dErr, ctx->stream));
+        for (uint32_t i = 0; i < count; ++i) ctx->flat.mark_source(src[i]);  // moved: out of the scene BVH
     } else {
         // rewriteInstanceRows:false — bounds from the (refit) BLAS roots
         CK(launch_update_instances(ctx->B, ctx->I, nullptr, nullptr, 0, 0, ctx->dErr, ctx->stream));
@@ -833,7 +876,7 @@ sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out) {
     out->traceBlock = ctx->tune.block;
     out->sortKey = ctx->tune.sortKey;
     out->smemTlasNodes = ctx->tune.smemTlasNodes;
-    out->bvhKind = 0;
+    out->bvhKind = ctx->bvhKind;
     return SB_OK;
 }
 
@@ -841,7 +884,9 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (!ctx || !t) return SB_ERR_INVALID_ARG;
     if (t->traceBlock == 0 || t->traceBlock > 256 || t->traceBlock % 32)
         return fail(ctx, SB_ERR_INVALID_ARG, "traceBlock %u: multiple of 32 in [32,256]", t->traceBlock);
-    if (t->bvhKind != 0) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
+    if (t->bvhKind != 0 && t->bvhKind != 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
+    if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
+    ctx->bvhKind = t->bvhKind;
     ctx->tune.block = t->traceBlock;
     ctx->tune.sortKey = t->sortKey;
     ctx->tune.smemTlasNodes = t->smemTlasNodes;

@@ -1,0 +1,226 @@
+// sb_flat.cu — building and maintaining a context's scene BVH (sb_flat.h).
+//
+// A structural change (scene upload, ranged upload of scene buffers, instance
+// set, TLAS build) marks the tree dirty; the next trace reads the instance
+// records, BLAS nodes, triangle indices and vertices back, forms one item per
+// (triangle, active instance slot) with its world-space bounds (the vertices
+// under the inverse of the instance's inverse rows, in FP64, widened), builds
+// the binned-SAH tree on the host and uploads it.
+//
+// Per frame nothing is rebuilt: a slot whose transform changes, or whose BLAS
+// is refit, is marked; the traversal skips that slot's items and walks its
+// current BLAS instead. More than kMaxDynamic marked slots trigger a rebuild.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "sb_flat_scene.cuh"
+
+namespace sb {
+
+namespace {
+
+template <class T>
+cudaError_t grow_dev(T*& p, size_t& cap, size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, (n ? n : 1) * sizeof(T));
+    if (e == cudaSuccess) cap = n;
+    return e;
+}
+
+uint32_t f_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// Inverse of the affine map local = A * world + b given as three rows (A | b).
+bool invert_rows(const float* r, double M[12]) {
+    double a[9];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) a[3 * i + j] = r[4 * i + j];
+    double c00 = a[4] * a[8] - a[5] * a[7], c01 = a[5] * a[6] - a[3] * a[8], c02 = a[3] * a[7] - a[4] * a[6];
+    double det = a[0] * c00 + a[1] * c01 + a[2] * c02;
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+    double inv[9] = {c00 / det, (a[2] * a[7] - a[1] * a[8]) / det, (a[1] * a[5] - a[2] * a[4]) / det,
+                     c01 / det, (a[0] * a[8] - a[2] * a[6]) / det, (a[2] * a[3] - a[0] * a[5]) / det,
+                     c02 / det, (a[1] * a[6] - a[0] * a[7]) / det, (a[0] * a[4] - a[1] * a[3]) / det};
+    const double b[3] = {r[3], r[7], r[11]};
+    for (int i = 0; i < 3; ++i) {
+        M[4 * i] = inv[3 * i];
+        M[4 * i + 1] = inv[3 * i + 1];
+        M[4 * i + 2] = inv[3 * i + 2];
+        M[4 * i + 3] = -(inv[3 * i] * b[0] + inv[3 * i + 1] * b[1] + inv[3 * i + 2] * b[2]);
+    }
+    return true;
+}
+
+}  // namespace
+
+cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uint32_t orderCount, cudaStream_t st,
+                               std::string& why) {
+    if (!enabled) {
+        ready = false;
+        return cudaSuccess;
+    }
+    if (dirty) {
+        auto t0 = std::chrono::steady_clock::now();
+        ready = false;
+        const uint32_t slots = B.instCount;
+        std::vector<float> inst((size_t)slots * 16);
+        std::vector<uint32_t> hn((size_t)B.nodeCount * 8), tri((size_t)B.triCount * 3), ord(orderCount);
+        std::vector<float> vert((size_t)B.vertexCount * 8);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && slots) e = cudaMemcpy(inst.data(), B.inst, inst.size() * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && B.nodeCount) e = cudaMemcpy(hn.data(), B.nodes, hn.size() * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && B.triCount) e = cudaMemcpy(tri.data(), B.triIndex, tri.size() * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && B.vertexCount)
+            e = cudaMemcpy(vert.data(), B.vertexData, vert.size() * 4, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && order && orderCount)
+            e = cudaMemcpy(ord.data(), order, ord.size() * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return e;
+
+        slotRoot.assign(slots, 0);
+        slotEnd.assign(slots, 0);
+        srcToSlot.assign(slots, 0xFFFFFFFFu);
+        for (uint32_t s = 0; s < slots; ++s) {
+            uint32_t src = (order && s < orderCount) ? ord[s] : s;
+            if (src < slots) srcToSlot[src] = s;
+        }
+        std::vector<float> boxes;
+        std::vector<uint32_t> itTri, itSlot;
+        boxes.reserve((size_t)B.triCount * 6);
+        itTri.reserve(B.triCount);
+        itSlot.reserve(B.triCount);
+        for (uint32_t s = 0; s < slots; ++s) {
+            const float* R = inst.data() + (size_t)s * 16;
+            uint32_t root = f_bits(R[12]), end = f_bits(R[13]);
+            slotRoot[s] = root;
+            slotEnd[s] = end;
+            if (!(R[15] > 0.5f) || !(root < end && end <= B.nodeCount)) continue;  // inactive or no BLAS
+            double M[12];
+            if (!invert_rows(R, M)) continue;  // singular: the local test never hits
+            for (uint32_t n = root; n < end; ++n) {
+                uint32_t payload = hn[8 * (size_t)n + 7];
+                if (payload == 0xFFFFFFFFu) continue;
+                uint32_t off = payload & 0x00FFFFFFu, cnt = payload >> 24;
+                for (uint32_t t = off; t < off + cnt && t < B.triCount; ++t) {
+                    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                    bool ok = true;
+                    for (int k = 0; k < 3; ++k) {
+                        uint32_t v = tri[3 * (size_t)t + k];
+                        if (v >= B.vertexCount) { ok = false; break; }
+                        const float* p = vert.data() + 8 * (size_t)v;
+                        for (int a = 0; a < 3; ++a) {
+                            double w = M[4 * a] * p[0] + M[4 * a + 1] * p[1] + M[4 * a + 2] * p[2] + M[4 * a + 3];
+                            lo[a] = std::fmin(lo[a], w);
+                            hi[a] = std::fmax(hi[a], w);
+                        }
+                    }
+                    if (!ok || !std::isfinite(lo[0] + lo[1] + lo[2] + hi[0] + hi[1] + hi[2])) continue;
+                    // margin well above the FP32 rounding of the local ray and vertices
+                    double mag = 0.0, ext = 0.0;
+                    for (int a = 0; a < 3; ++a) {
+                        mag = std::fmax(mag, std::fmax(std::fabs(lo[a]), std::fabs(hi[a])));
+                        ext = std::fmax(ext, hi[a] - lo[a]);
+                    }
+                    const double m = 1e-5 * mag + 1e-5 * ext + 1e-7;
+                    for (int a = 0; a < 3; ++a) boxes.push_back(std::nextafterf((float)(lo[a] - m), -INFINITY));
+                    for (int a = 0; a < 3; ++a) boxes.push_back(std::nextafterf((float)(hi[a] + m), INFINITY));
+                    itTri.push_back(t);
+                    itSlot.push_back(s);
+                }
+            }
+        }
+        flat::Tree tree;
+        const uint32_t n = (uint32_t)itTri.size();
+        if (!flat::build(boxes.data(), itTri.data(), itSlot.data(), n, tree)) {
+            why = "scene BVH: too many items";
+            dirty = false;
+            return cudaSuccess;
+        }
+        if (tree.depth + 1 > (uint32_t)SB_STACK) {
+            why = "scene BVH deeper than the traversal stack";
+            dirty = false;
+            return cudaSuccess;
+        }
+        const size_t nn = tree.nodes.size() / 16;
+        e = grow_dev(nodes, nodeCap, nn ? nn * 4 : 4);
+        if (e == cudaSuccess) e = grow_dev(items, itemCap, n ? n : 1);
+        if (e == cudaSuccess && nn) e = cudaMemcpy(nodes, tree.nodes.data(), tree.nodes.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && n) e = cudaMemcpy(items, tree.items.data(), tree.items.size() * 4, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        root = tree.root;
+        depth = tree.depth;
+        itemCount = n;
+        skip.assign(slots, 0);
+        dyn.clear();
+        marksDirty = true;
+        dirty = false;
+        ready = true;
+        lastBuildMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    if (ready && marksDirty) {
+        cudaError_t e = grow_dev(dSkip, skipCap, skip.size() ? skip.size() : 1);
+        if (e == cudaSuccess) e = grow_dev(dDyn, dynCap, kMaxDynamic);
+        if (e == cudaSuccess && !skip.empty())
+            e = cudaMemcpyAsync(dSkip, skip.data(), skip.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess && !dyn.empty())
+            e = cudaMemcpyAsync(dDyn, dyn.data(), dyn.size() * 4, cudaMemcpyHostToDevice, st);
+        // pageable sources: wait so the vectors may change after return
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return e;
+        marksDirty = false;
+    }
+    return cudaSuccess;
+}
+
+void FlatScene::mark_slot(uint32_t s) {
+    if (!ready || dirty || s >= skip.size() || skip[s]) return;
+    if (dyn.size() >= kMaxDynamic) {
+        dirty = true;  // rebuild with the current placements instead
+        return;
+    }
+    skip[s] = 1;
+    dyn.push_back(s);
+    marksDirty = true;
+}
+
+void FlatScene::mark_source(uint32_t src) {
+    if (src < srcToSlot.size()) mark_slot(srcToSlot[src]);
+}
+
+void FlatScene::mark_blas_range(uint32_t r0, uint32_t r1) {
+    for (uint32_t s = 0; s < slotRoot.size(); ++s)
+        if (slotRoot[s] < r1 && r0 < slotEnd[s]) mark_slot(s);
+}
+
+void FlatScene::fill(DevScene& S) const {
+    const bool on = enabled && ready;
+    S.flatOn = on ? 1 : 0;
+    S.flatNodes = on ? nodes : nullptr;
+    S.flatItems = on ? items : nullptr;
+    S.flatRoot = on ? root : flat::ENTRY_NONE;
+    S.slotSkip = on ? dSkip : nullptr;
+    S.dynList = on ? dDyn : nullptr;
+    S.dynCount = on ? (uint32_t)dyn.size() : 0u;
+}
+
+void FlatScene::release() {
+    if (nodes) cudaFree(nodes);
+    if (items) cudaFree(items);
+    if (dSkip) cudaFree(dSkip);
+    if (dDyn) cudaFree(dDyn);
+    nodes = nullptr;
+    items = nullptr;
+    dSkip = nullptr;
+    dDyn = nullptr;
+    nodeCap = itemCap = skipCap = dynCap = 0;
+    ready = false;
+    dirty = true;
+}
+
+}  // namespace sb

@@ -1,0 +1,46 @@
+// sb_flat_scene.cuh — a context's scene BVH (layout in sb_flat.h): when it is
+// rebuilt, which instance slots it no longer covers, and what the kernels see.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "sb_flat.h"
+#include "sb_kernels.cuh"
+
+namespace sb {
+
+struct FlatScene {
+    static constexpr uint32_t kMaxDynamic = 256;  // more moved slots than this: rebuild
+
+    bool enabled = true;  // bvhKind 2
+    bool dirty = true;    // rebuild before the next trace
+    bool ready = false;   // device copy current
+    uint4* nodes = nullptr;
+    size_t nodeCap = 0;
+    uint2* items = nullptr;
+    size_t itemCap = 0;
+    uint8_t* dSkip = nullptr;
+    size_t skipCap = 0;
+    uint32_t* dDyn = nullptr;
+    size_t dynCap = 0;
+    uint32_t root = flat::ENTRY_NONE, depth = 0, itemCount = 0;
+    std::vector<uint8_t> skip;        // per slot
+    std::vector<uint32_t> dyn;        // slots walked through their BLAS
+    std::vector<uint32_t> slotRoot, slotEnd, srcToSlot;
+    bool marksDirty = false;
+    float lastBuildMs = 0.0f;
+
+    // Rebuilds when dirty and uploads pending slot marks. `order` (slot ->
+    // source instance, device, may be null) maps transform updates to slots.
+    cudaError_t prepare(const SceneBuffers& B, const uint32_t* order, uint32_t orderCount, cudaStream_t st,
+                        std::string& why);
+    void mark_source(uint32_t src);
+    void mark_blas_range(uint32_t root, uint32_t end);
+    void fill(DevScene& S) const;
+    void release();
+
+   private:
+    void mark_slot(uint32_t s);
+};
+
+}  // namespace sb

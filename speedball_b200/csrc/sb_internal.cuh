@@ -23,6 +23,27 @@ constexpr float PI_F = 3.141592653589793f;
 constexpr int OCT = 6, TILE = 8, BORDER = 1;
 constexpr uint32_t LIGHT_DATA = 64u * 17u;  // records before the C0 cell lists
 
+// Child-pair nodes (derived, 64 bytes per interior node, indexed like the
+// reference nodes): q0 = child0 (minx, maxx, miny, maxy), q1 = child1 (same),
+// q2 = (child0 minz, maxz, child1 minz, maxz), q3 = (entry0, entry1, 0, 0).
+// An entry names what a traversal does next with that child:
+//   top byte != 0           BLAS leaf: the reference payload (cnt << 24) | triOffset
+//   PE_BLAS | node          BLAS interior node (node < 2^23)
+//   PE_TLEAF | cnt<<12 | s  TLAS leaf: cnt instance slots from s (s < 4096, cnt < 1024)
+//   node                    TLAS interior node (node < 2^22)
+//   PE_NONE                 nothing to visit (an empty leaf)
+constexpr uint32_t PE_NONE = 0xFFFFFFFFu;
+constexpr uint32_t PE_BLAS = 0x00800000u;
+constexpr uint32_t PE_TLEAF = 0x00400000u;
+constexpr uint32_t PE_BLAS_MAX_NODES = 1u << 23;
+constexpr uint32_t PE_TLAS_MAX_SLOTS = 4096u;
+constexpr uint32_t DEPTH_UNKNOWN = 0xFFFFFFFFu;
+
+// Entries of the per-thread traversal stack (child-pair and scene-BVH walks).
+#ifndef SB_STACK
+#define SB_STACK 40
+#endif
+
 // Per-triangle accept bits packed in the w lane of the first float4 of a
 // pre-gathered triangle (materialSideAccepts / materialAlphaAccepts /
 // traversal flags, spectral_traverse.js:193-222 with no map bound).
@@ -44,6 +65,19 @@ struct DevScene {
     const float* lights;       // 64 x 17 records (+ C0 cell lists)
     const uint32_t* triIndex;  // reference triangle indices (final-hit refinement)
     const float* vertexData;   // reference vertices, 8 floats each
+    const uint4* pairs;        // 4 x uint4 per interior BLAS node: both children's boxes + entries
+    const uint4* tlasPairs;    // the same for interior TLAS nodes
+    const uint32_t* depth;     // [0] deepest BLAS node, [1] deepest TLAS node (NONE: pairs unusable)
+    // scene BVH (sb_flat.h): world-space tree over (triangle, slot) items;
+    // slots marked in slotSkip moved or deformed since its build and are
+    // walked through their own BLAS instead (dynList)
+    const uint4* flatNodes;
+    const uint2* flatItems;
+    const uint8_t* slotSkip;
+    const uint32_t* dynList;
+    const float* slotBounds;   // world AABB per slot (the TLAS leaf bounds), or null
+    uint32_t flatRoot, dynCount;
+    int32_t flatOn;
     uint32_t nodeCount, triCount, instCount, tlasNodeCount, materialCount;
     uint32_t lightCount;
     int32_t clustered;

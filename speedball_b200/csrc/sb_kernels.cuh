@@ -27,6 +27,9 @@ struct SceneBuffers {
     float4* inst = nullptr;           // derived, instCount*4
     uint4* tlas = nullptr;            // derived, tlasNodeCount*2
     uint32_t* matBits = nullptr;      // derived, per material accept bits
+    uint4* pairs = nullptr;           // derived, nodeCount*4: child-pair nodes of the BLASes
+    uint4* tlasPairs = nullptr;       // derived, tlasNodeCount*4: child-pair nodes of the TLAS
+    uint32_t* depth = nullptr;        // 2 words: deepest BLAS / TLAS node (DEPTH_UNKNOWN = no pairs)
     uint32_t* parent = nullptr;       // nodeCount: parent of each BLAS node (refit)
     uint32_t* arrive = nullptr;       // nodeCount: refit arrival counters
     uint32_t* valid = nullptr;        // 1 word
@@ -80,6 +83,13 @@ cudaError_t launch_update_instances(const SceneBuffers& B, const InstanceTable& 
 cudaError_t launch_tlas_refit(const SceneBuffers& B, const InstanceTable& I, uint32_t* err, cudaStream_t st);
 cudaError_t launch_tlas_index(const SceneBuffers& B, const InstanceTable& I, uint32_t* owner, uint32_t* err,
                               cudaStream_t st);
+
+// Child-pair layouts (sb_pairs.cu). launch_blas_pairs derives every BLAS pair
+// node and the deepest BLAS node from the reference nodes (structural changes);
+// refits keep them current. launch_tlas_pairs does the same for the TLAS after
+// a structural TLAS change (pack or build); TLAS refits rewrite their pairs.
+cudaError_t launch_blas_pairs(const SceneBuffers& B, cudaStream_t st);
+cudaError_t launch_tlas_pairs(const SceneBuffers& B, cudaStream_t st);
 
 // Arbitrary-ray queries through the same traversal (raycastFirst-like).
 cudaError_t launch_raycast(const DevScene& S, const float* ro, const float* rd, uint32_t n, float* tOut,

@@ -144,7 +144,8 @@ cudaError_t launch_pack_dynamic(const SceneBuffers& B, uint32_t* err, cudaStream
                                                                   B.instCount, B.tlas, B.valid, err);
         note_launch();
     }
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    return e != cudaSuccess ? e : launch_tlas_pairs(B, st);
 }
 
 cudaError_t launch_pack_scene(const SceneBuffers& B, uint32_t* err, cudaStream_t st) {
@@ -156,7 +157,9 @@ cudaError_t launch_pack_scene(const SceneBuffers& B, uint32_t* err, cudaStream_t
         k_check_nodes<<<blocks(B.nodeCount, 256), 256, 0, st>>>(B.nodes, B.nodeCount, B.triCount, B.valid, err);
         note_launch();
     }
-    cudaError_t e = launch_pack_tris(B, 0, B.triCount, err, st);
+    cudaError_t e = launch_blas_pairs(B, st);
+    if (e != cudaSuccess) return e;
+    e = launch_pack_tris(B, 0, B.triCount, err, st);
     if (e != cudaSuccess) return e;
     return launch_pack_dynamic(B, err, st);
 }

@@ -13,6 +13,7 @@
 //     level first.
 // min/max are exact, so all bounds are bit-identical to the reference walk.
 #include "sb_kernels.cuh"
+#include "sb_pairs.cuh"
 
 namespace sb {
 
@@ -68,7 +69,7 @@ __device__ __forceinline__ float vload(const uint32_t* p) { return __uint_as_flo
 __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
                             const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
                             const uint32_t* parent, uint32_t* arrive, uint32_t root, uint32_t end,
-                            const uint32_t* gate) {
+                            const uint32_t* gate, uint4* pairs) {
     uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= end || *gate == 0u) return;
     uint32_t info = nodes[8 * i + 7];
@@ -110,13 +111,19 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
         uint32_t r = *(const volatile uint32_t*)(nodes + 8 * l + 6);
         const uint32_t* L = nodes + 8 * l;
         const uint32_t* R = nodes + 8 * r;
+        uint32_t lb[6], rb[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            lb[k] = *(const volatile uint32_t*)(L + k);
+            rb[k] = *(const volatile uint32_t*)(R + k);
+        }
         uint32_t* n = nodes + 8 * p;
-        n[0] = __float_as_uint(js_min(vload(L + 0), vload(R + 0)));
-        n[1] = __float_as_uint(js_min(vload(L + 1), vload(R + 1)));
-        n[2] = __float_as_uint(js_min(vload(L + 2), vload(R + 2)));
-        n[3] = __float_as_uint(js_max(vload(L + 3), vload(R + 3)));
-        n[4] = __float_as_uint(js_max(vload(L + 4), vload(R + 4)));
-        n[5] = __float_as_uint(js_max(vload(L + 5), vload(R + 5)));
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            n[k] = __float_as_uint(js_min(__uint_as_float(lb[k]), __uint_as_float(rb[k])));
+            n[3 + k] = __float_as_uint(js_max(__uint_as_float(lb[3 + k]), __uint_as_float(rb[3 + k])));
+        }
+        if (pairs) store_pair_boxes(pairs + 4u * p, lb, rb);  // the traversal's copy of both child boxes
         node = p;
     }
 }
@@ -133,7 +140,7 @@ cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end
                                     B.parent, root, end, gate, err); note_launch();
     k_refit_orphans<<<g, 256, 0, st>>>(B.parent, root, end, gate, err); note_launch();
     k_refit_run<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.vertexData, B.triMaterial, B.matBits, B.tris, B.parent,
-                                   B.arrive, root, end, gate); note_launch();
+                                   B.arrive, root, end, gate, B.pairs); note_launch();
     return cudaGetLastError();
 }
 
@@ -524,6 +531,18 @@ __global__ void __launch_bounds__(1024) k_tlas_refit(SceneBuffers B, InstanceTab
             }
         }
         __syncthreads();
+    }
+    // the traversal's child-pair copy of the refit bounds (entries are structural)
+    if (!B.tlasPairs) return;
+    for (uint32_t i = threadIdx.x; i < nn; i += blockDim.x) {
+        uint4 b = B.tlas[2 * i + 1];
+        if ((b.w >> 24) != 0u || i + 1 >= nn) continue;
+        uint32_t l = i + 1, r = B.tlas[2 * l + 1].z;
+        if (!(r > l && r < nn)) continue;
+        uint4 la = B.tlas[2 * l], lb = B.tlas[2 * l + 1], ra = B.tlas[2 * r], rb = B.tlas[2 * r + 1];
+        const uint32_t b0[6] = {la.x, la.y, la.z, la.w, lb.x, lb.y};
+        const uint32_t b1[6] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y};
+        store_pair_boxes(B.tlasPairs + 4u * i, b0, b1);
     }
 }
 

@@ -32,14 +32,18 @@ struct WaveCtx {
     uint32_t order;                // 0 probe-major, 1 direction-major
 };
 
-__device__ __forceinline__ const uint4* stage_tlas(const WaveCtx& W, uint4* sTlas) {
+// The TLAS the walk reads (child pairs when `pairs`, else the 32-byte nodes),
+// staged in shared memory when it fits.
+__device__ __forceinline__ const uint4* stage_tlas(const WaveCtx& W, uint4* sTlas, bool pairs) {
     const DevScene& S = W.S;
+    const uint4* src = pairs ? S.tlasPairs : S.tlas;
     if (W.smemTlas >= S.tlasNodeCount && S.tlasNodeCount > 0) {
-        for (uint32_t i = threadIdx.x; i < 2 * S.tlasNodeCount; i += blockDim.x) sTlas[i] = __ldg(S.tlas + i);
+        const uint32_t n = (pairs ? 4u : 2u) * S.tlasNodeCount;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sTlas[i] = __ldg(src + i);
         __syncthreads();
         return sTlas;
     }
-    return S.tlas;
+    return src;
 }
 
 struct HitFrame {
@@ -171,7 +175,8 @@ __device__ __forceinline__ void ray_of(const WaveCtx& W, uint32_t g, bool dirMaj
 
 __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(WaveCtx W) {
     extern __shared__ uint4 sTlas[];
-    const uint4* tl = stage_tlas(W, sTlas);
+    const bool pairs = closest_pairs(W.S);
+    const uint4* tl = stage_tlas(W, sTlas, pairs);
     if (!*W.S.valid) return;
     const DevCascade& C = W.C;
     const uint32_t N = C.rays, total = W.slotCount * N;
@@ -201,7 +206,7 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
             uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
             ro = probe_world_pos(C, probeIndex);
             rd = ray_dir(k, N, W.P.frameJitter);
-            trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err);
+            trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
             ++nRays;
             if (tri >= 0) {
                 bestT = refine_t(W.S, (uint32_t)tri, (uint32_t)inst, ro, rd);
@@ -261,7 +266,8 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
 
 __global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(WaveCtx W) {
     extern __shared__ uint4 sTlas[];
-    const uint4* tl = stage_tlas(W, sTlas);
+    const bool pairs = any_pairs(W.S);
+    const uint4* tl = stage_tlas(W, sTlas, pairs);
     if (!*W.S.valid) return;
     const uint32_t total = min(*(volatile uint32_t*)&W.work[2], W.jobCap);
     const uint32_t lane = threadIdx.x & 31u;
@@ -274,7 +280,7 @@ __global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(Wave
         uint32_t j = base + lane;
         if (j >= total) continue;
         float4 a = W.jobs[2 * j], b = W.jobs[2 * j + 1];
-        if (trace_any(W.S, tl, xyz(a), xyz(b), a.w, vis, W.err)) {
+        if (trace_any(W.S, tl, xyz(a), xyz(b), a.w, vis, W.err, pairs)) {
             uint32_t packed = __float_as_uint(b.w);
             uint32_t ray = packed >> 6, li = packed & 63u;
             uint4* v = W.C.vis + ray;
@@ -373,9 +379,10 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     W.slotBegin = slotBegin;
     W.slotCount = slotCount;
     W.order = tune.sortKey == 0 ? 1u : 0u;  // default direction-major; sortKey 1 = probe-major
-    uint32_t smemNodes = S.tlasNodeCount <= tune.smemTlasNodes ? S.tlasNodeCount : 0u;
+    // the scene-BVH walk reads no TLAS
+    uint32_t smemNodes = !S.flatOn && S.tlasNodeCount <= tune.smemTlasNodes ? S.tlasNodeCount : 0u;
     W.smemTlas = smemNodes;
-    size_t smem = (size_t)smemNodes * 32u;
+    size_t smem = (size_t)smemNodes * 64u;  // room for the child-pair TLAS (the 32-byte nodes need half)
     if (smem > 48u * 1024u) {
         cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(k_trace_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -405,7 +412,8 @@ __global__ void k_raycast(DevScene S, const float* ro, const float* rd, uint32_t
     float t, bu, bv;
     int tri, inst;
     float3 o = mk(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]), d = mk(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]);
-    trace_closest(S, S.tlas, o, d, t, tri, inst, bu, bv, vis, err);
+    const bool pairs = closest_pairs(S);
+    trace_closest(S, pairs ? S.tlasPairs : S.tlas, o, d, t, tri, inst, bu, bv, vis, err, pairs);
     if (tri >= 0) t = refine_t(S, (uint32_t)tri, (uint32_t)inst, o, d);
     tOut[i] = t;
     triOut[i] = tri;
@@ -417,8 +425,9 @@ __global__ void k_occluded(DevScene S, const float* ro, const float* rd, const f
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !*S.valid) return;
     Visits vis = {0, 0, 0, 0};
-    out[i] = trace_any(S, S.tlas, mk(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]), mk(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]),
-                       maxDist[i], vis, err)
+    const bool pairs = any_pairs(S);
+    out[i] = trace_any(S, pairs ? S.tlasPairs : S.tlas, mk(ro[3 * i], ro[3 * i + 1], ro[3 * i + 2]),
+                       mk(rd[3 * i], rd[3 * i + 1], rd[3 * i + 2]), maxDist[i], vis, err, pairs)
                  ? 1
                  : 0;
 }
