@@ -208,16 +208,22 @@ def run_ours(args, dist: Dist):
                    shadow_tlas=st.shadowTlasNodeVisits, shadow_inst=st.shadowInstanceVisits,
                    shadow_blas=st.shadowBlasNodeVisits, shadow_tri=st.shadowTriangleTests)
     # algorithmic bytes per launch of each stage. Per-unit figures: 32 B TLAS node, 64 B instance
-    # record, 32 B BLAS node, 48 B pre-gathered triangle; 16 B hit record + 16 B visibility mask per
-    # ray; 32 B per shadow job (written by the primary stage, read by the shadow stage); per hit 80 B
-    # of triangle/instance rows, 40 B material, 256 B of bounce taps (8 taps x 4 texels x 8 B); 16 B
-    # ray record write; 3,776 B per probe for blend + upload.
-    def trav(t, i, b, tr):
-        return 32 * t + 64 * i + 32 * b + 48 * tr
+    # record, 48 B pre-gathered triangle; per box test 32 B (a BLAS node, or half a 64 B child-pair
+    # node) or 10 B on the 8-wide closest-hit tree (80 B node / 8 boxes); 16 B hit record + 16 B
+    # visibility mask per ray; 32 B per shadow job (written by the primary stage, read by the shadow
+    # stage); per hit 80 B of triangle/instance rows, 40 B material, 256 B of bounce taps (8 taps x
+    # 4 texels x 8 B); 16 B ray record write; 3,776 B per probe for blend + upload.
+    tun = _abi.sb_tuning()
+    _abi.check(lib.sb_get_tuning(ctx, C.byref(tun)), ctx)
+    closest_box = 10 if tun.bvhKind == 1 else 32
+
+    def trav(t, i, b, tr, box=32):
+        return 32 * t + 64 * i + box * b + 48 * tr
     jobs = counted["shadow"]
     stage_bytes = {
         "k_trace_primary": trav(counted["tlas"] - counted["shadow_tlas"], counted["inst"] - counted["shadow_inst"],
-                                counted["blas"] - counted["shadow_blas"], counted["tri"] - counted["shadow_tri"])
+                                counted["blas"] - counted["shadow_blas"], counted["tri"] - counted["shadow_tri"],
+                                closest_box)
         + 32 * rays + 32 * jobs,
         "k_trace_shadow": trav(counted["shadow_tlas"], counted["shadow_inst"], counted["shadow_blas"],
                                counted["shadow_tri"]) + 32 * jobs,

@@ -306,10 +306,11 @@ typedef struct sb_tuning {
     uint32_t sortKey;         /* ray issue order: 0 = direction-major (ray k of
                                  neighbouring probes per warp), 1 = probe-major   */
     uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
-    uint32_t bvhKind;         /* 2 = scene BVH over (triangle, instance) items,
-                                 rebuilt on structural changes (default);
-                                 0 = the reference's TLAS + BLASes;
-                                 1 = wide 8-bit quantised (not built)             */
+    uint32_t bvhKind;         /* scene BVH over (triangle, instance) items, rebuilt
+                                 on structural changes: 1 = 8-wide nodes with 8-bit
+                                 boxes for closest hits + binary for any hits
+                                 (default); 2 = binary only.
+                                 0 = the reference's TLAS + BLASes                */
 } sb_tuning;
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);

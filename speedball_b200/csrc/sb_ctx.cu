@@ -74,7 +74,8 @@ struct sb_ctx {
     std::vector<float> hostLights;
 
     TraceTuning tune{256u, 512u, 0u, 148};  // 512 TLAS nodes = 32 KB of child pairs per CTA
-    uint32_t bvhKind = 2;          // 0 = the reference's TLAS + BLASes, 2 = scene BVH (sb_flat.h)
+    uint32_t bvhKind = 1;          // 1 = scene BVH, 8-wide for closest hits (default); 2 = binary scene
+                                   // BVH only; 0 = the reference's TLAS + BLASes (sb_flat.h)
     FlatScene flat;
     float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
     uint32_t jobCap = 0;
@@ -204,11 +205,12 @@ sb_status pack_if_needed(sb_ctx* ctx) {
     return SB_OK;
 }
 
-// The scene BVH of bvhKind 2: rebuilt after structural changes, marks of moved
-// slots uploaded. A build that cannot serve (too deep, too large) leaves the
-// reference two-level walk in use.
+// The scene BVH of bvhKind 1 and 2: rebuilt after structural changes, marks of
+// moved slots uploaded. A build that cannot serve (too deep, too large) leaves
+// the reference two-level walk in use.
 sb_status flat_if_needed(sb_ctx* ctx) {
-    ctx->flat.enabled = ctx->bvhKind == 2;
+    ctx->flat.enabled = ctx->bvhKind == 1 || ctx->bvhKind == 2;
+    ctx->flat.wide = ctx->bvhKind == 1;
     std::string why;
     const bool order = ctx->tlasOnDevice && ctx->instancesSet;
     CK(ctx->flat.prepare(ctx->B, order ? ctx->I.order : nullptr, order ? ctx->I.count : 0u, ctx->stream, why));
@@ -884,7 +886,7 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (!ctx || !t) return SB_ERR_INVALID_ARG;
     if (t->traceBlock == 0 || t->traceBlock > 256 || t->traceBlock % 32)
         return fail(ctx, SB_ERR_INVALID_ARG, "traceBlock %u: multiple of 32 in [32,256]", t->traceBlock);
-    if (t->bvhKind != 0 && t->bvhKind != 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
+    if (t->bvhKind > 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
     if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
     ctx->bvhKind = t->bvhKind;
     ctx->tune.block = t->traceBlock;

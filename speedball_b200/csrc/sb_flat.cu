@@ -135,8 +135,8 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
                 }
             }
         }
-        flat::Tree tree;
         const uint32_t n = (uint32_t)itTri.size();
+        flat::Tree tree;
         if (!flat::build(boxes.data(), itTri.data(), itSlot.data(), n, tree)) {
             why = "scene BVH: too many items";
             dirty = false;
@@ -147,14 +147,28 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
             dirty = false;
             return cudaSuccess;
         }
-        const size_t nn = tree.nodes.size() / 16;
-        e = grow_dev(nodes, nodeCap, nn ? nn * 4 : 4);
+        const size_t nq = tree.nodes.size() / 4;  // uint4 count
+        e = grow_dev(nodes, nodeCap, nq ? nq : 4);
         if (e == cudaSuccess) e = grow_dev(items, itemCap, n ? n : 1);
-        if (e == cudaSuccess && nn) e = cudaMemcpy(nodes, tree.nodes.data(), tree.nodes.size() * 4, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && nq) e = cudaMemcpy(nodes, tree.nodes.data(), tree.nodes.size() * 4, cudaMemcpyHostToDevice);
         if (e == cudaSuccess && n) e = cudaMemcpy(items, tree.items.data(), tree.items.size() * 4, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) return e;
-        root = tree.root;
-        depth = tree.depth;
+        const uint32_t treeRoot = tree.root, treeDepth = tree.depth;
+        wideReady = false;
+        if (wide && n) {
+            flat::WideTree wt;
+            if (flat::build_wide(boxes.data(), itTri.data(), itSlot.data(), n, wt) && wt.depth + 1 <= (uint32_t)SB_STACK) {
+                const size_t wq = wt.nodes.size() / 4;
+                e = grow_dev(wnodes, wnodeCap, wq);
+                if (e == cudaSuccess) e = grow_dev(witems, witemCap, n);
+                if (e == cudaSuccess) e = cudaMemcpy(wnodes, wt.nodes.data(), wt.nodes.size() * 4, cudaMemcpyHostToDevice);
+                if (e == cudaSuccess) e = cudaMemcpy(witems, wt.items.data(), wt.items.size() * 4, cudaMemcpyHostToDevice);
+                if (e != cudaSuccess) return e;
+                wideReady = true;
+            }
+        }
+        root = treeRoot;
+        depth = treeDepth;
         itemCount = n;
         skip.assign(slots, 0);
         dyn.clear();
@@ -203,6 +217,8 @@ void FlatScene::fill(DevScene& S) const {
     S.flatOn = on ? 1 : 0;
     S.flatNodes = on ? nodes : nullptr;
     S.flatItems = on ? items : nullptr;
+    S.wideNodes = on && wide && wideReady ? wnodes : nullptr;
+    S.wideItems = on && wide && wideReady ? witems : nullptr;
     S.flatRoot = on ? root : flat::ENTRY_NONE;
     S.slotSkip = on ? dSkip : nullptr;
     S.dynList = on ? dDyn : nullptr;
@@ -214,6 +230,12 @@ void FlatScene::release() {
     if (items) cudaFree(items);
     if (dSkip) cudaFree(dSkip);
     if (dDyn) cudaFree(dDyn);
+    if (wnodes) cudaFree(wnodes);
+    if (witems) cudaFree(witems);
+    wnodes = nullptr;
+    witems = nullptr;
+    wnodeCap = witemCap = 0;
+    wideReady = false;
     nodes = nullptr;
     items = nullptr;
     dSkip = nullptr;

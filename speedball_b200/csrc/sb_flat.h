@@ -34,5 +34,29 @@ struct Tree {
 // does not fit the entry encoding.
 bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot, uint32_t n, Tree& out);
 
+// The same items as an 8-wide tree with 8-bit child boxes (80-byte nodes,
+// 20 words), collapsed from the binary SAH tree built with leaves of at most
+// WIDE_LEAF_MAX items:
+//   w0..w2  node origin p (f32)          w3  ex | ey<<8 | ez<<16 | imask<<24
+//   w4      first interior child node    w5  first item of the leaf children
+//   w6..w7  meta byte per slot 0..7      w8..w19  qlo x,y,z then qhi x,y,z,
+//                                                 two words (slots 0-3, 4-7) each
+// Child box on axis a: p + q * 2^(e_a - 127), q rounded outward. imask bit s:
+// slot s holds an interior child, the (popcount of imask below s)-th node
+// from w4. meta: 0 empty; interior (1 << 5) | (24 + s); leaf ((1 << cnt) - 1)
+// << 5 | its first item's offset from w5 (0..23). Slot bits (x, y, z) place a
+// child toward +x, +y, +z of the node centre, so visiting slots in increasing
+// order of (slot XOR ray-octant) goes roughly near to far.
+constexpr uint32_t WIDE_WORDS = 20;
+constexpr uint32_t WIDE_LEAF_MAX = 3;
+
+struct WideTree {
+    std::vector<uint32_t> nodes;  // WIDE_WORDS per node, root first
+    std::vector<uint32_t> items;  // (triangle, slot) per item
+    uint32_t depth = 0;           // deepest node level below the root
+};
+
+bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot, uint32_t n, WideTree& out);
+
 }  // namespace flat
 }  // namespace sb

@@ -20,7 +20,6 @@ namespace flat {
 namespace {
 
 constexpr int BINS = 16;
-constexpr uint32_t MAX_LEAF = 4;
 
 struct Box {
     float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -45,6 +44,7 @@ struct Box {
 };
 
 struct Builder {
+    uint32_t maxLeaf = 4;
     const float* boxes;  // 6 per item
     std::vector<float> cen;
     std::vector<uint32_t> order;
@@ -113,7 +113,7 @@ struct Builder {
         }
         // SAH: traversal step ~ one item test; stop when splitting costs more
         const float leafCost = nb.area() * n;
-        if (n <= MAX_LEAF && (bestAxis < 0 || best + nb.area() >= leafCost)) return hi;
+        if (n <= maxLeaf && (bestAxis < 0 || best + nb.area() >= leafCost)) return hi;
         uint32_t mid = lo + n / 2;
         if (bestAxis >= 0) {
             const float c0 = cb.lo[bestAxis], scale = BINS / (cb.hi[bestAxis] - c0);
@@ -229,6 +229,157 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
     out.depth = maxDepth;
     std::memcpy(out.rootBox, B.nodeBox[0].lo, 12);
     std::memcpy(out.rootBox + 3, B.nodeBox[0].hi, 12);
+    return true;
+}
+
+}  // namespace flat
+}  // namespace sb
+
+namespace sb {
+namespace flat {
+
+namespace {
+
+// Outward-rounded 8-bit grid of one axis: lo + q * 2^e covers [lo, hi] for q
+// in 0..255. Returns the biased exponent (e + 127) stored in the node.
+int axis_exponent(float lo, float hi) {
+    double extent = (double)hi - (double)lo;
+    int e = -126;
+    if (extent > 0.0) {
+        e = (int)std::ceil(std::log2(extent / 255.0));
+        while (std::ldexp(255.0, e) < extent) ++e;
+        e = std::max(e, -126);
+    }
+    return std::min(e, 127) + 127;
+}
+
+}  // namespace
+
+bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot, uint32_t n, WideTree& out) {
+    out = WideTree{};
+    if (n == 0) return true;
+    if (n >= (1u << 24)) return false;
+    Builder B;
+    B.maxLeaf = WIDE_LEAF_MAX;
+    B.boxes = boxes;
+    B.cen.resize(3 * (size_t)n);
+    B.order.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        for (int a = 0; a < 3; ++a) B.cen[3 * (size_t)i + a] = 0.5f * (boxes[6 * (size_t)i + a] + boxes[6 * (size_t)i + 3 + a]);
+        B.order[i] = i;
+    }
+    B.build(n);
+    for (size_t v = 0; v < B.count.size(); ++v) {
+        if (B.count[v] == 0) continue;
+        std::stable_sort(B.order.begin() + B.first[v], B.order.begin() + B.first[v] + B.count[v],
+                         [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+    }
+
+    struct Task { uint32_t v, w, depth; };
+    std::vector<Task> queue{{0, 0, 0}};
+    out.nodes.assign(WIDE_WORDS, 0u);
+    uint32_t maxDepth = 0;
+    for (size_t qi = 0; qi < queue.size(); ++qi) {
+        const Task t = queue[qi];
+        maxDepth = std::max(maxDepth, t.depth);
+        // children: open the largest interior child until eight (a leaf root is its own child)
+        std::vector<uint32_t> kids;
+        if (B.count[t.v]) kids.push_back(t.v);
+        else { kids.push_back(B.left[t.v]); kids.push_back(B.right[t.v]); }
+        while (kids.size() < 8) {
+            int best = -1;
+            float bestArea = -1.0f;
+            for (size_t k = 0; k < kids.size(); ++k)
+                if (B.count[kids[k]] == 0 && B.nodeBox[kids[k]].area() > bestArea) {
+                    bestArea = B.nodeBox[kids[k]].area();
+                    best = (int)k;
+                }
+            if (best < 0) break;
+            uint32_t v = kids[best];
+            kids[best] = B.left[v];
+            kids.push_back(B.right[v]);
+        }
+        // slots by octant: slot bit a set = the child lies toward +a of the node centre
+        Box nb;
+        for (uint32_t k : kids) nb.grow(B.nodeBox[k]);
+        float ctr[3];
+        for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
+        struct Cand { float cost; int kid, slot; };
+        std::vector<Cand> cands;
+        for (size_t k = 0; k < kids.size(); ++k) {
+            const Box& b = B.nodeBox[kids[k]];
+            for (int s = 0; s < 8; ++s) {
+                float c = 0.0f;
+                for (int a = 0; a < 3; ++a) {
+                    float d = 0.5f * (b.lo[a] + b.hi[a]) - ctr[a];
+                    c += (s >> a & 1) ? -d : d;
+                }
+                cands.push_back({c, (int)k, s});
+            }
+        }
+        std::stable_sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.cost < y.cost; });
+        int slotKid[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+        std::vector<int> kidSlot(kids.size(), -1);
+        for (const Cand& c : cands)
+            if (slotKid[c.slot] < 0 && kidSlot[c.kid] < 0) {
+                slotKid[c.slot] = c.kid;
+                kidSlot[c.kid] = c.slot;
+            }
+        // header, children and items
+        uint32_t* w = out.nodes.data() + (size_t)t.w * WIDE_WORDS;
+        int ex[3];
+        for (int a = 0; a < 3; ++a) ex[a] = axis_exponent(nb.lo[a], nb.hi[a]);
+        std::memcpy(w + 0, &nb.lo[0], 4);
+        std::memcpy(w + 1, &nb.lo[1], 4);
+        std::memcpy(w + 2, &nb.lo[2], 4);
+        uint32_t imask = 0;
+        const uint32_t childBase = (uint32_t)(out.nodes.size() / WIDE_WORDS);
+        const uint32_t itemBase = (uint32_t)(out.items.size() / 2);
+        uint32_t itemOff = 0;
+        uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        uint8_t q[6][8];
+        for (int s = 0; s < 8; ++s) {
+            for (int a = 0; a < 3; ++a) { q[a][s] = 255; q[3 + a][s] = 0; }  // empty slots
+            if (slotKid[s] < 0) continue;
+            const uint32_t v = kids[slotKid[s]];
+            const Box& b = B.nodeBox[v];
+            for (int a = 0; a < 3; ++a) {
+                const double sc = std::ldexp(1.0, ex[a] - 127);
+                double lo = std::floor(((double)b.lo[a] - (double)nb.lo[a]) / sc);
+                double hi = std::ceil(((double)b.hi[a] - (double)nb.lo[a]) / sc);
+                q[a][s] = (uint8_t)std::min(255.0, std::max(0.0, lo));
+                q[3 + a][s] = (uint8_t)std::min(255.0, std::max(0.0, hi));
+            }
+            if (B.count[v] == 0) {
+                imask |= 1u << s;
+                meta[s] = (uint8_t)((1u << 5) | (24u + s));
+                queue.push_back({v, 0, t.depth + 1});  // node index assigned below, in slot order
+            } else {
+                const uint32_t cnt = B.count[v];
+                meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
+                for (uint32_t k = 0; k < cnt; ++k) {
+                    out.items.push_back(itemTri[B.order[B.first[v] + k]]);
+                    out.items.push_back(itemSlot[B.order[B.first[v] + k]]);
+                }
+                itemOff += cnt;
+            }
+        }
+        // interior children get consecutive node indices in slot order
+        uint32_t next = childBase;
+        for (size_t k = queue.size() - __builtin_popcount(imask); k < queue.size(); ++k) queue[k].w = next++;
+        out.nodes.resize((size_t)next * WIDE_WORDS, 0u);
+        w = out.nodes.data() + (size_t)t.w * WIDE_WORDS;
+        w[3] = (uint32_t)ex[0] | (uint32_t)ex[1] << 8 | (uint32_t)ex[2] << 16 | imask << 24;
+        w[4] = childBase;
+        w[5] = itemBase;
+        w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | (uint32_t)meta[3] << 24;
+        w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | (uint32_t)meta[7] << 24;
+        for (int r = 0; r < 6; ++r) {
+            w[8 + 2 * r] = q[r][0] | q[r][1] << 8 | q[r][2] << 16 | (uint32_t)q[r][3] << 24;
+            w[9 + 2 * r] = q[r][4] | q[r][5] << 8 | q[r][6] << 16 | (uint32_t)q[r][7] << 24;
+        }
+    }
+    out.depth = maxDepth;
     return true;
 }
 

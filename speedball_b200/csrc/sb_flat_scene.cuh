@@ -12,13 +12,19 @@ namespace sb {
 struct FlatScene {
     static constexpr uint32_t kMaxDynamic = 256;  // more moved slots than this: rebuild
 
-    bool enabled = true;  // bvhKind 2
+    bool enabled = true;  // bvhKind 1 or 2
+    bool wide = true;     // bvhKind 1: also the 8-wide tree, which answers closest hits
     bool dirty = true;    // rebuild before the next trace
     bool ready = false;   // device copy current
-    uint4* nodes = nullptr;
+    uint4* nodes = nullptr;   // binary child-pair tree (any hit; closest hit without `wide`)
     size_t nodeCap = 0;
     uint2* items = nullptr;
     size_t itemCap = 0;
+    uint4* wnodes = nullptr;  // 8-wide tree with 8-bit boxes (closest hit)
+    size_t wnodeCap = 0;
+    uint2* witems = nullptr;
+    size_t witemCap = 0;
+    bool wideReady = false;
     uint8_t* dSkip = nullptr;
     size_t skipCap = 0;
     uint32_t* dDyn = nullptr;

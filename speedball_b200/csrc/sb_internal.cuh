@@ -71,8 +71,10 @@ struct DevScene {
     // scene BVH (sb_flat.h): world-space tree over (triangle, slot) items;
     // slots marked in slotSkip moved or deformed since its build and are
     // walked through their own BLAS instead (dynList)
-    const uint4* flatNodes;
+    const uint4* flatNodes;    // binary child pairs (any hit; closest hit when wideNodes is null)
     const uint2* flatItems;
+    const uint4* wideNodes;    // the same items as 8-wide nodes with 8-bit boxes (closest hit), or null
+    const uint2* wideItems;
     const uint8_t* slotSkip;
     const uint32_t* dynList;
     const float* slotBounds;   // world AABB per slot (the TLAS leaf bounds), or null

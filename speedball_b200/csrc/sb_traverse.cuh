@@ -592,6 +592,157 @@ __device__ __forceinline__ bool flat_walk(const DevScene& S, float3 wro, float3 
     return ANY ? false : bestTri >= 0;
 }
 
+// ------------------------------------------------------ wide scene-BVH walk
+// The scene BVH as 8-wide nodes with 8-bit child boxes (sb_flat.h). One node
+// visit tests all eight child boxes and forms one hit mask: interior children
+// at bit 24 + (slot XOR ray octant), so taking the lowest bit first visits
+// them roughly near to far; leaf items at their offsets in bits 0..23. A
+// group (child base, remaining interior bits, interior mask) waits on the stack
+// while the nearest child is visited; a node's items are tested before its
+// children. Box tests are conservative (outward-rounded grid, widened item
+// bounds); the items are tested exactly as in flat_walk.
+
+// q (a byte of w, 0..255) as an exact float: 2^23 + q minus 2^23
+__device__ __forceinline__ float q_at(uint32_t w, uint32_t byteSel) {
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | byteSel)) - 8388608.0f;
+}
+
+template <bool ANY>
+__device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 wrd, float& tmax, int& bestTri,
+                                          int& bestInst, float& bu, float& bv, Visits& vis, uint32_t* err) {
+    const float3 winv = mk(1.0f / wrd.x, 1.0f / wrd.y, 1.0f / wrd.z);
+    if (SB_DYN_FIRST && dyn_walk<ANY>(S, wro, wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
+    // Box tests use the inverse clamped to +-1e30. An infinite one (a zero
+    // direction component) would give q * inf = NaN for every child plane at
+    // q = 0 and pass that axis for all of them: axis-parallel rays then visit
+    // about 25x the nodes. Clamped, the plane distances stay finite and
+    // signed, so the test still only keeps boxes the ray can reach.
+    const float3 binv = mk(fminf(fmaxf(winv.x, -1e30f), 1e30f), fminf(fmaxf(winv.y, -1e30f), 1e30f),
+                           fminf(fmaxf(winv.z, -1e30f), 1e30f));
+    const uint32_t oct = (binv.x < 0.0f ? 1u : 0u) | (binv.y < 0.0f ? 2u : 0u) | (binv.z < 0.0f ? 4u : 0u);
+    uint2 stk[SB_STACK];
+    int sp = 0;
+    uint32_t node = 0;  // the root (the wide tree is only built when non-empty)
+    uint32_t gBase = 0, gBits = 0;  // interior hits << 24 | imask << 16
+    uint32_t tBase = 0, tBits = 0;  // item hits
+    uint32_t lslot = FLAT_NONE;
+    float3 lro = wro, lrd = wrd;
+    float dSign = 1.0f;
+    uint32_t iter = 0;
+    for (;;) {
+        bool done = false;
+        // node phase: until this lane holds items to test or has nothing left
+        for (;;) {
+            if (node == FLAT_NONE) {
+                if (gBits >> 24) {
+                    const uint32_t key = __ffs(gBits >> 24) - 1u;
+                    gBits &= ~(1u << (24u + key));
+                    const uint32_t slot = key ^ oct;
+                    node = gBase + __popc((gBits >> 16) & 0xFFu & ((1u << slot) - 1u));
+                    if (gBits >> 24) {
+                        if (sp >= SB_STACK) {  // unreachable: the tree's depth was checked on build
+                            latch(err, ERR_CAPACITY);
+                            done = true;
+                            break;
+                        }
+                        stk[sp++] = make_uint2(gBase, gBits);
+                    }
+                    gBits = 0;
+                } else if (sp > 0) {
+                    --sp;
+                    gBase = stk[sp].x;
+                    gBits = stk[sp].y;
+                    continue;
+                } else {
+                    done = true;
+                    break;
+                }
+            }
+            if (++iter > (1u << 26)) {
+                latch(err, ERR_WATCHDOG);
+                done = true;
+                break;
+            }
+            const uint4* p = S.wideNodes + 5u * node;
+            const uint4 h0 = __ldg(p), h1 = __ldg(p + 1), qa = __ldg(p + 2), qb = __ldg(p + 3), qc = __ldg(p + 4);
+            node = FLAT_NONE;
+            vis.blas += 8;
+            // per axis: t = q * (2^e * inv) + (p - o) * inv, near plane first
+            const float sx = __uint_as_float((h0.w & 0xFFu) << 23) * binv.x;
+            const float sy = __uint_as_float(((h0.w >> 8) & 0xFFu) << 23) * binv.y;
+            const float sz = __uint_as_float(((h0.w >> 16) & 0xFFu) << 23) * binv.z;
+            const float ox = (__uint_as_float(h0.x) - wro.x) * binv.x;
+            const float oy = (__uint_as_float(h0.y) - wro.y) * binv.y;
+            const float oz = (__uint_as_float(h0.z) - wro.z) * binv.z;
+            // lo words: x (qa.x, qa.y) y (qa.z, qa.w) z (qb.x, qb.y); hi words: x (qb.z, qb.w) y (qc.x, qc.y) z (qc.z, qc.w)
+            const bool nx = oct & 1u, ny = oct & 2u, nz = oct & 4u;
+            const uint32_t nearX0 = nx ? qb.z : qa.x, nearX1 = nx ? qb.w : qa.y;
+            const uint32_t farX0 = nx ? qa.x : qb.z, farX1 = nx ? qa.y : qb.w;
+            const uint32_t nearY0 = ny ? qc.x : qa.z, nearY1 = ny ? qc.y : qa.w;
+            const uint32_t farY0 = ny ? qa.z : qc.x, farY1 = ny ? qa.w : qc.y;
+            const uint32_t nearZ0 = nz ? qc.z : qb.x, nearZ1 = nz ? qc.w : qb.y;
+            const uint32_t farZ0 = nz ? qb.x : qc.z, farZ1 = nz ? qb.y : qc.w;
+            uint32_t bits = 0;
+#pragma unroll
+            for (uint32_t s = 0; s < 8; ++s) {
+                const uint32_t b = s & 3u;
+                const float tnx = fmaf(q_at(s < 4 ? nearX0 : nearX1, b), sx, ox);
+                const float tny = fmaf(q_at(s < 4 ? nearY0 : nearY1, b), sy, oy);
+                const float tnz = fmaf(q_at(s < 4 ? nearZ0 : nearZ1, b), sz, oz);
+                const float tfx = fmaf(q_at(s < 4 ? farX0 : farX1, b), sx, ox);
+                const float tfy = fmaf(q_at(s < 4 ? farY0 : farY1, b), sy, oy);
+                const float tfz = fmaf(q_at(s < 4 ? farZ0 : farZ1, b), sz, oz);
+                const float tNear = fmaxf(fmaxf(tnx, tny), tnz);
+                const float tFar = fminf(fminf(tfx, tfy), tfz);
+                if (tFar >= fmaxf(tNear, 0.0f) && tNear < tmax) {
+                    const uint32_t m = (s < 4 ? h1.z : h1.w) >> (8u * b) & 0xFFu;
+                    uint32_t sh = m & 31u;
+                    if (sh >= 24u) sh ^= oct;
+                    bits |= (m >> 5) << sh;
+                }
+            }
+            gBase = h1.x;
+            gBits = (bits & 0xFF000000u) | ((h0.w >> 24) << 16);
+            tBase = h1.y;
+            tBits = bits & 0x00FFFFFFu;
+            if (tBits) break;
+        }
+        if (done) break;
+        // leaf phase (warp-aligned): items in slot order share the local ray
+        while (tBits) {
+            const uint32_t k = __ffs(tBits) - 1u;
+            tBits &= tBits - 1u;
+            const uint2 it = __ldg(S.wideItems + tBase + k);
+            const uint32_t tri = it.x, slot = it.y;
+            if (slot != lslot) {
+                if (__ldg(S.slotSkip + slot)) continue;
+                const float4 r0 = __ldg(S.inst + 4 * slot), r1 = __ldg(S.inst + 4 * slot + 1),
+                             r2 = __ldg(S.inst + 4 * slot + 2);
+                lro = mk(dot3(xyz(r0), wro) + r0.w, dot3(xyz(r1), wro) + r1.w, dot3(xyz(r2), wro) + r2.w);
+                lrd = mk(dot3(xyz(r0), wrd), dot3(xyz(r1), wrd), dot3(xyz(r2), wrd));
+                dSign = __ldg(&S.inst[4 * slot + 3].z);
+                lslot = slot;
+                ++vis.inst;
+            }
+            float t, det, u, v;
+            uint32_t hb;
+            ++vis.tri;
+            if (!mt_hit(S.tris, tri, lro, lrd, tmax, t, det, u, v, hb)) continue;
+            if (ANY) {
+                if ((hb & TB_SHADOW_OK) && side_ok(hb, det * dSign)) return true;
+            } else if (side_ok(hb, det * dSign) && (hb & TB_CLOSEST_OK)) {
+                tmax = t;
+                bestTri = (int)tri;
+                bestInst = (int)slot;
+                bu = u;
+                bv = v;
+            }
+        }
+    }
+    if (!SB_DYN_FIRST && dyn_walk<ANY>(S, wro, wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
+    return ANY ? false : bestTri >= 0;
+}
+
 // Traversal schedule per query kind: 0 nested (as the reference), 1 unified
 // two-level loop, 2 nested with while-while BLAS walks. Measured on the
 // 262k-triangle atrium (B200): closest hit 0.51 / 0.41 / 0.57 ms, any hit
@@ -623,6 +774,10 @@ __device__ __forceinline__ void trace_closest(const DevScene& S, const uint4* tl
     bestTri = -1;
     bestInst = -1;
     bu = bv = 0.0f;
+    if (S.wideNodes) {
+        wide_walk<false>(S, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, err);
+        return;
+    }
     if (S.flatOn) {
         flat_walk<false>(S, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, err);
         return;
