@@ -61,7 +61,12 @@ struct sb_ctx {
     size_t stageCap = 0;
 
     uint32_t* dErr = nullptr;
-    uint32_t* dGate = nullptr;
+    uint32_t* dGate = nullptr;     // 16 layout verdicts, one per cached refit range
+    // Refit ranges whose parent links and layout checks are current: valid while
+    // packEpoch is unchanged (no upload touched nodes, indices or materials since).
+    struct RefitRange { uint32_t root = 0, end = 0, epoch = 0; bool used = false; };
+    RefitRange refitRanges[16];
+    uint32_t packEpoch = 1, refitNext = 0;
     uint32_t* dWork = nullptr;
     unsigned long long* dCounters = nullptr;
     bool countersOn = false;
@@ -196,6 +201,7 @@ DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint3
 
 sb_status pack_if_needed(sb_ctx* ctx) {
     if (!ctx->needPack) return SB_OK;
+    ++ctx->packEpoch;  // cached refit verdicts refer to the old layout
     uint32_t one = 1u;
     CK(cudaMemcpyAsync(ctx->B.valid, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(launch_pack_scene(ctx->B, ctx->dErr, ctx->stream));
@@ -292,7 +298,7 @@ sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
         ctx->tune.numSms = ctx->numSms;
         if (cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking) != cudaSuccess) { st = SB_ERR_CUDA; break; }
         ctx->stream = ctx->ownStream;
-        if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 4) != cudaSuccess ||
+        if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 16 * 4) != cudaSuccess ||
             cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 16 * 8) != cudaSuccess ||
             cudaMalloc(&ctx->B.valid, 4) != cudaSuccess || cudaMalloc(&ctx->B.depth, 8) != cudaSuccess) {
             st = SB_ERR_OOM;
@@ -447,6 +453,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
     // validation + derived layouts; a pending TLAS is packed by sb_build_tlas
     uint32_t one = 1u;
+    ++ctx->packEpoch;
     CK(cudaMemcpyAsync(B.valid, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(launch_pack_scene(ctx->tlasPending ? [&] { SceneBuffers t = B; t.instCount = 0; t.tlasNodeCount = 0; return t; }() : B,
                          ctx->dErr, ctx->stream));
@@ -732,7 +739,21 @@ sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end) {
     cudaSetDevice(ctx->device);
     sb_status s = pack_if_needed(ctx);
     if (s != SB_OK) return s;
-    CK(launch_refit_blas(ctx->B, root, end, ctx->dErr, ctx->dGate, ctx->stream));
+    // a range checked on the current layout refits with the bottom-up pass alone
+    int slot = -1;
+    for (int k = 0; k < 16; ++k) {
+        const auto& r = ctx->refitRanges[k];
+        if (r.used && r.root == root && r.end == end && r.epoch == ctx->packEpoch) slot = k;
+    }
+    const bool validated = slot >= 0;
+    if (!validated) {
+        // relinking rewrites the parents of [root, end): overlapping cached ranges are stale
+        for (auto& r : ctx->refitRanges)
+            if (r.used && r.root < end && root < r.end) r.used = false;
+        slot = (int)(ctx->refitNext++ % 16u);
+        ctx->refitRanges[slot] = {root, end, ctx->packEpoch, true};
+    }
+    CK(launch_refit_blas(ctx->B, root, end, ctx->dErr, ctx->dGate + slot, ctx->stream, validated));
     ctx->flat.mark_blas_range(root, end);  // its instances leave the scene BVH
     return SB_OK;
 }

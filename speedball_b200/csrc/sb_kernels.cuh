@@ -52,9 +52,11 @@ cudaError_t launch_pack_scene(const SceneBuffers& B, uint32_t* err, cudaStream_t
 cudaError_t launch_pack_tris(const SceneBuffers& B, uint32_t triBegin, uint32_t triEnd, uint32_t* err, cudaStream_t st);
 cudaError_t launch_pack_dynamic(const SceneBuffers& B, uint32_t* err, cudaStream_t st);
 
-// Refit and TLAS lanes (sb_refit.cu).
+// Refit and TLAS lanes (sb_refit.cu). `validated`: the range's parent links
+// and layout checks from an earlier call on the same layout are still current
+// (their verdict is in *gate), so only the bottom-up pass runs.
 cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
-                              cudaStream_t st);
+                              cudaStream_t st, bool validated = false);
 
 struct InstanceTable {
     double* world = nullptr;       // 16 per source instance (column-major)

@@ -69,9 +69,13 @@ __device__ __forceinline__ float vload(const uint32_t* p) { return __uint_as_flo
 __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
                             const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
                             const uint32_t* parent, uint32_t* arrive, uint32_t root, uint32_t end,
-                            const uint32_t* gate, uint4* pairs) {
+                            const uint32_t* gate, uint4* pairs, uint32_t* err) {
     uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end || *gate == 0u) return;
+    if (i >= end) return;
+    if (*gate == 0u) {
+        if (i == root) latch(err, ERR_LAYOUT);  // the range's layout verdict stands until a new upload
+        return;
+    }
     uint32_t info = nodes[8 * i + 7];
     if (info == INTERIOR) return;
     uint32_t off = info & 0x00FFFFFFu, cnt = info >> 24;
@@ -107,6 +111,7 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
         __threadfence();
         if (atomicAdd(&arrive[p], 1u) == 0u) break;
         __threadfence();
+        arrive[p] = 0u;  // both children arrived: ready for the next refit of this range
         uint32_t l = p + 1;
         uint32_t r = *(const volatile uint32_t*)(nodes + 8 * l + 6);
         const uint32_t* L = nodes + 8 * l;
@@ -129,18 +134,20 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
 }
 
 cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
-                              cudaStream_t st) {
+                              cudaStream_t st, bool validated) {
     if (end <= root) return cudaSuccess;
     uint32_t n = end - root;
     unsigned g = (n + 255) / 256;
-    uint32_t one = 1u;
-    cudaMemcpyAsync(gate, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
-    k_refit_reset<<<g, 256, 0, st>>>(B.parent, B.arrive, root, end); note_launch();
-    k_refit_link<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.triMaterial, B.triCount, B.vertexCount, B.materialCount,
-                                    B.parent, root, end, gate, err); note_launch();
-    k_refit_orphans<<<g, 256, 0, st>>>(B.parent, root, end, gate, err); note_launch();
+    if (!validated) {
+        cudaError_t e = cudaMemsetAsync(gate, 1, sizeof(uint32_t), st);  // nonzero: valid until a check fails
+        if (e != cudaSuccess) return e;
+        k_refit_reset<<<g, 256, 0, st>>>(B.parent, B.arrive, root, end); note_launch();
+        k_refit_link<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.triMaterial, B.triCount, B.vertexCount,
+                                        B.materialCount, B.parent, root, end, gate, err); note_launch();
+        k_refit_orphans<<<g, 256, 0, st>>>(B.parent, root, end, gate, err); note_launch();
+    }
     k_refit_run<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.vertexData, B.triMaterial, B.matBits, B.tris, B.parent,
-                                   B.arrive, root, end, gate, B.pairs); note_launch();
+                                   B.arrive, root, end, gate, B.pairs, err); note_launch();
     return cudaGetLastError();
 }
 

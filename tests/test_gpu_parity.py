@@ -202,6 +202,45 @@ def test_layout_violation_reported_not_faulted():
         f.dispose()
 
 
+def test_repeated_refits_reuse_the_layout_checks():
+    """Later refits of a range checked on the same layout run the bottom-up pass
+    alone; bounds stay bit-exact, a failed range keeps failing, and an
+    overlapping range is checked again."""
+    s = synth.room_spheres(0)
+    f = gu.make_field(s, record=False)
+    try:
+        pool = f.pool
+        lib = f._lib
+        rng = np.random.default_rng(9)
+        m = 5
+        r, e = int(pool.blas_root[m]), int(pool.blas_end[m])
+        vb, vc = int(pool.vert_base[m]), int(pool.vert_count[m])
+        vd = pool.vertexData.copy()
+
+        def deform_and_check():
+            vd[vb:vb + vc, 0:3] += rng.normal(0, 0.04, (vc, 3)).astype(np.float32)
+            sl = np.ascontiguousarray(vd[vb:vb + vc])
+            _abi.check(lib.sb_update_deform(f.ctx, vb, vc, _abi.ptr(sl), r, e), f.ctx)
+            f.synchronize()
+            got = gu.read(f, "BVH_NODES", pool.bvhNodes.size, np.uint32).reshape(-1, 8)
+            want = pool.bvhNodes.copy()
+            assert orc.load().orc_refit_blas(orc._p(want), want.size, orc._p(pool.triIndex), pool.triIndex.size,
+                                             orc._p(vd), vd.size, r, e) == 1
+            assert np.array_equal(got[r:e], want[r:e])
+
+        for _ in range(3):
+            deform_and_check()
+        # a range that fails its checks keeps failing when refit again on the same layout
+        for _ in range(2):
+            _abi.check(lib.sb_refit_blas(f.ctx, r, e - 1), f.ctx)
+            assert lib.sb_synchronize(f.ctx) == _abi.SB_ERR_LAYOUT_VIOLATION
+        # the overlapping valid range is relinked and checked again
+        deform_and_check()
+        deform_and_check()
+    finally:
+        f.dispose()
+
+
 @pytest.fixture(scope="module")
 def atrium_field():
     s = synth.atrium(1)
