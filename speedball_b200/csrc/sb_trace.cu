@@ -1,10 +1,12 @@
 // sb_trace.cu — the probe trace as a three-stage wavefront (traceKernel,
 // gi_probes.js:1977-2214, split where its per-ray work diverges):
 //
-//   A  k_trace_primary  closest hit per probe ray (traverseClosest) -> 16-byte
-//                       hit record; NEE pre-tests per candidate light (the
-//                       reference's ndl * peak > 0 and range gates) emit
-//                       shadow-ray jobs, warp-ballot compacted into a queue.
+//   A  k_trace_primary  closest hit per probe ray (traverseClosest) -> raw
+//                       16-byte hit record.
+//      k_emit           per ray: hit t in double-float, hit frame, and the NEE
+//                       pre-tests per candidate light (the reference's
+//                       ndl * peak > 0 and range gates); passing candidates
+//                       become shadow-ray jobs, one atomic per warp.
 //   B  k_trace_shadow   any hit per job (traverseAny); blocked lights are
 //                       cleared from the ray's visibility mask.
 //   C  k_shade          emissive + unblocked NEE terms (ascending light index,
@@ -183,84 +185,118 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
     const uint32_t lane = threadIdx.x & 31u;
     const bool dirMajor = W.order != 0;
     Visits vis = {0, 0, 0, 0};
-    uint32_t nRays = 0, nJobs = 0;
+    uint32_t nRays = 0;
     for (;;) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&W.work[0], 32u);
         base = __shfl_sync(0xFFFFFFFFu, base, 0);
         if (base >= total) break;
         const uint32_t g = base + lane;
-        const bool live = g < total;
-        uint32_t slot = 0, k = 0, rayIdx = 0;
-        float3 ro = mk(0.f, 0.f, 0.f), rd = mk(0.f, 0.f, 1.f);
-        float bestT = T_MAX, bu = 0.f, bv = 0.f;
-        int tri = -1, inst = -1;
-        HitFrame fr;
-        fr.hitPos = ro;
-        fr.ng = rd;
-        fr.faceFwd = true;
-        fr.traceBias = 0.f;
-        if (live) {
-            ray_of(W, g, dirMajor, slot, k);
-            rayIdx = slot * N + k;
-            uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
-            ro = probe_world_pos(C, probeIndex);
-            rd = ray_dir(k, N, W.P.frameJitter);
-            trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
-            ++nRays;
-            if (tri >= 0) {
-                bestT = refine_t(W.S, (uint32_t)tri, (uint32_t)inst, ro, rd);
-                fr = hit_frame(W, (uint32_t)tri, (uint32_t)inst, ro, rd, bestT, -1);
-            }
-        }
-        // NEE candidates -> shadow-ray jobs, one ballot-compacted round per list position
-        LightList L{nullptr, 0u};
-        if (tri >= 0) L = light_list(W, fr.hitPos);
-        uint32_t maxCount = __reduce_max_sync(0xFFFFFFFFu, L.count);
-        uint32_t tested0 = 0u, tested1 = 0u;
-        for (uint32_t i = 0; i < maxCount; ++i) {
-            bool has = false;
-            uint32_t li = 0;
-            LightEval e;
-            if (i < L.count) {
-                li = light_at(L, i);
-                e = light_eval(W, li, fr.hitPos, fr.ng);
-                has = e.pass;
-            }
-            uint32_t mask = __ballot_sync(0xFFFFFFFFu, has);
-            if (mask == 0u) continue;
-            uint32_t jb = 0;
-            if (lane == 0) jb = atomicAdd(&W.work[2], (uint32_t)__popc(mask));
-            jb = __shfl_sync(0xFFFFFFFFu, jb, 0);
-            if (has) {
-                uint32_t j = jb + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-                if (j < W.jobCap) {
-                    W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, e.dist - fr.traceBias);
-                    W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float((rayIdx << 6) | li));
-                    if (li < 32) tested0 |= 1u << li;
-                    else tested1 |= 1u << (li - 32);
-                    ++nJobs;
-                } else {
-                    latch(W.err, ERR_CAPACITY);
-                }
-            }
-        }
-        if (live) {
-            uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
-            uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
-            C.hits[rayIdx] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst | (fr.faceFwd ? 0x80000000u : 0u),
-                                                   __float_as_uint(bestT), uq | (vq << 16))
-                                      : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
-            C.vis[rayIdx] = make_uint4(tested0, tested1, tested0, tested1);
-        }
+        if (g >= total) continue;
+        uint32_t slot, k;
+        ray_of(W, g, dirMajor, slot, k);
+        const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+        const float3 ro = probe_world_pos(C, probeIndex);
+        const float3 rd = ray_dir(k, N, W.P.frameJitter);
+        float bestT, bu, bv;
+        int tri, inst;
+        trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
+        ++nRays;
+        // raw record (FP32 t, no facing bit): k_emit finishes it
+        uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
+        uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
+        C.hits[slot * N + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(bestT),
+                                                     uq | (vq << 16))
+                                        : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
     }
     if (W.counters) {
         atomicAdd(&W.counters[0], (unsigned long long)nRays);
-        atomicAdd(&W.counters[1], (unsigned long long)nJobs);
         atomicAdd(&W.counters[2], (unsigned long long)vis.tlas);
         atomicAdd(&W.counters[3], (unsigned long long)vis.inst);
         atomicAdd(&W.counters[4], (unsigned long long)vis.blas);
         atomicAdd(&W.counters[5], (unsigned long long)vis.tri);
+    }
+}
+
+// Stage A2, one thread per probe ray in the issue order of A: the hit
+// parameter re-evaluated in double-float, the hit frame, and the NEE gates of
+// every candidate light. Each lane runs the gates with no warp sync; one warp
+// scan and one atomicAdd then reserve the warp's shadow-ray jobs, and each
+// ray's passing candidates (gates evaluated again: the same pure function) are
+// written together in list order, so a shadow warp mostly holds rays that share
+// an origin.
+__global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
+    if (!*W.S.valid) return;
+    const DevCascade& C = W.C;
+    const uint32_t N = C.rays, total = W.slotCount * N;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t rayIdx = 0;
+    int tri = -1;
+    HitFrame fr;
+    fr.hitPos = mk(0.f, 0.f, 0.f);
+    fr.ng = mk(0.f, 0.f, 1.f);
+    fr.faceFwd = true;
+    fr.traceBias = 0.f;
+    uint4 h = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u);
+    if (g < total) {
+        uint32_t slot, k;
+        ray_of(W, g, W.order != 0, slot, k);
+        rayIdx = slot * N + k;
+        h = C.hits[rayIdx];
+        if (h.x != 0xFFFFFFFFu) {
+            tri = (int)h.x;
+            const uint32_t inst = h.y;
+            const float3 ro = probe_world_pos(C, (C.probeOffset + slot) % C.probeTotal);
+            const float3 rd = ray_dir(k, N, W.P.frameJitter);
+            const float t = refine_t(W.S, (uint32_t)tri, inst, ro, rd);
+            fr = hit_frame(W, (uint32_t)tri, inst, ro, rd, t, -1);
+            h.y = inst | (fr.faceFwd ? 0x80000000u : 0u);
+            h.z = __float_as_uint(t);
+        }
+    }
+    LightList L{nullptr, 0u};
+    if (tri >= 0) L = light_list(W, fr.hitPos);
+    unsigned long long pass = 0ull;
+    for (uint32_t i = 0; i < L.count; ++i)
+        if (light_eval(W, light_at(L, i), fr.hitPos, fr.ng).pass) pass |= 1ull << i;
+    const uint32_t mine = (uint32_t)__popcll(pass);
+    uint32_t incl = mine;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const uint32_t warpJobs = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t jb = 0;
+    if (warpJobs) {
+        if (lane == 0) jb = atomicAdd(&W.work[2], warpJobs);
+        jb = __shfl_sync(0xFFFFFFFFu, jb, 0);
+    }
+    uint32_t j = jb + incl - mine, tested0 = 0u, tested1 = 0u, nJobs = 0;
+    while (pass) {
+        const uint32_t i = (uint32_t)(__ffsll((long long)pass) - 1);
+        pass &= pass - 1ull;
+        const uint32_t li = light_at(L, i);
+        const LightEval e = light_eval(W, li, fr.hitPos, fr.ng);
+        if (j < W.jobCap) {
+            W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, e.dist - fr.traceBias);
+            W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float((rayIdx << 6) | li));
+            if (li < 32) tested0 |= 1u << li;
+            else tested1 |= 1u << (li - 32);
+            ++nJobs;
+        } else {
+            latch(W.err, ERR_CAPACITY);
+        }
+        ++j;
+    }
+    if (g < total) {
+        if (tri >= 0) C.hits[rayIdx] = h;
+        C.vis[rayIdx] = make_uint4(tested0, tested1, tested0, tested1);
+    }
+    if (W.counters) {
+        const uint32_t warpDone = __reduce_add_sync(0xFFFFFFFFu, nJobs);
+        if (lane == 0 && warpDone) atomicAdd(&W.counters[1], (unsigned long long)warpDone);
     }
 }
 
@@ -392,6 +428,8 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     const uint32_t rays = slotCount * C.rays;
     int block = (int)tune.block;
     k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smem, tune, rays), block, smem, st>>>(W);
+    note_launch();
+    k_emit<<<(rays + 127) / 128, 128, 0, st>>>(W);
     note_launch();
     if (afterPrimary) cudaEventRecord(afterPrimary, st);
     // shadow jobs: at most lightCount per ray (the queue is sized for it)
