@@ -275,8 +275,7 @@ def run_ours(args, dist: Dist):
         f.markDeformsDirty()
         f.markTransformsDirty(list(mats))
         f.tick()
-        f._debugRead("atlas", out=atl.array)
-        f._debugRead("depthAtlas", out=datl.array)
+        f._debugReadMany([("atlas", atl.array), ("depthAtlas", datl.array)])
 
     for i in range(W):
         e2e_step(i)

@@ -138,9 +138,15 @@ typedef enum sb_buffer {
 sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count,
                           const void* src);
 /* Device->host read of any buffer above (the _debugRead seam, gi_probes.js:4830-4841).
- * Synchronous: waits for the stream. */
+ * Synchronous: the copy is queued behind the context's work and waited for. */
 sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count,
                          void* dst);
+/* The same read, only queued on the context's stream (the reference's read is
+ * asynchronous too: _debugRead resolves a mapAsync). `dst` is valid after the
+ * next sb_synchronize; page-locked memory (sb_host_alloc) lets the copy run
+ * without a host round trip between several reads. */
+sb_status sb_read_buffer_async(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count,
+                               void* dst);
 
 /* ------------------------------------------------------------------ lights */
 

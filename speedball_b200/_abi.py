@@ -133,6 +133,7 @@ SIGNATURES = {
     "sb_upload_scene": (C.c_int, [_P, C.POINTER(sb_scene_view)]),
     "sb_upload_range": (C.c_int, [_P, _U32, _U32, _U32, _P]),
     "sb_read_buffer": (C.c_int, [_P, _U32, _U32, _U32, _P]),
+    "sb_read_buffer_async": (C.c_int, [_P, _U32, _U32, _U32, _P]),
     "sb_upload_lights": (C.c_int, [_P, _P, _U32, _U32, _U32, C.c_int32]),
     "sb_params_defaults": (None, [C.POINTER(sb_params)]),
     "sb_configure_cascade": (C.c_int, [_P, _U32, C.POINTER(sb_grid)]),

@@ -507,7 +507,8 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
     return SB_OK;
 }
 
-sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, void* dstHost) {
+// Validates a read and enqueues its copy on the context stream.
+static sb_status read_enqueue(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, void* dstHost) {
     if (!ctx || (!dstHost && count)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     uint32_t buf = which & 0xFFu, ci = which >> 8;
     cudaSetDevice(ctx->device);
@@ -535,9 +536,20 @@ sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t c
     }
     if (!srcp) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not available", buf);
     if ((size_t)start + count > len) return fail(ctx, SB_ERR_INVALID_ARG, "range [%u,+%u) outside %zu", start, count, len);
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaMemcpy(dstHost, (const char*)srcp + (size_t)start * esz, (size_t)count * esz, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(dstHost, (const char*)srcp + (size_t)start * esz, (size_t)count * esz, cudaMemcpyDeviceToHost,
+                       ctx->stream));
     return SB_OK;
+}
+
+sb_status sb_read_buffer(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, void* dstHost) {
+    sb_status s = read_enqueue(ctx, which, start, count, dstHost);
+    if (s != SB_OK) return s;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+}
+
+sb_status sb_read_buffer_async(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t count, void* dstHost) {
+    return read_enqueue(ctx, which, start, count, dstHost);
 }
 
 sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count, uint32_t emitterBase,

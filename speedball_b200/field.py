@@ -262,14 +262,22 @@ class ProbeField:
                 rec = np.ascontiguousarray(ub[m * 28:(m + 1) * 28])
                 self._ck(lib.sb_upload_range(self._ctx, _abi.BUF["MATERIALS"], m * 28, 28, _abi.ptr(rec)))
             self._pendingMaterials.clear()
+        moving = self._pendingAllTransforms or bool(self._pendingTransforms)
+        deformed = []
         if self._pendingDeform:
             self._pendingDeform = False
-            self.refreshDeforms()
-        if self._pendingAllTransforms or self._pendingTransforms:
-            idx = range(len(self._scene.instances)) if self._pendingAllTransforms else sorted(self._pendingTransforms)
+            # with a transform lane in the same tick, one instance update carries both
+            deformed = self.refreshDeforms(carryTlas=not moving)
+        if moving:
+            if self._pendingAllTransforms:
+                idx = set(range(len(self._scene.instances)))
+            else:
+                idx = set(self._pendingTransforms)
+                meshes = set(deformed)
+                idx.update(i for i, inst in enumerate(self._scene.instances) if inst.mesh in meshes)
             self._pendingAllTransforms = False
             self._pendingTransforms.clear()
-            self.refreshTransforms(list(idx))
+            self.refreshTransforms(sorted(idx))
 
     def refreshTransforms(self, instances):
         """refreshTransforms -> updateTransforms (gi_probes.js:4164-4179, spectral_scene.js:1402-1514)."""
@@ -280,10 +288,13 @@ class ProbeField:
         self._ck(self._lib.sb_update_transforms(self._ctx, _abi.ptr(src), _abi.ptr(world), src.shape[0]))
         self.stats["transformUpdates"] += 1
 
-    def refreshDeforms(self, meshes=None):
+    def refreshDeforms(self, meshes=None, carryTlas: bool = True):
         """refreshDeforms -> updateDeforms (gi_probes.js:4209-4234, spectral_scene.js:1831-1927):
         re-gather each deformed mesh's pooled vertices, refit its BLAS on the GPU,
-        then carry the new root bounds into the TLAS (rewriteInstanceRows:false)."""
+        then carry the new root bounds into the TLAS (rewriteInstanceRows:false).
+        carryTlas=False leaves that last step to a following refreshTransforms over
+        the deformed meshes' instances (same bounds, one TLAS refit). Returns the
+        indices of the meshes refit."""
         pool = self._pool
         if meshes is None:
             # same-topology deforms only: a mesh counts as changed when its positions
@@ -311,8 +322,10 @@ class ProbeField:
                                                 _abi.ptr(vd), int(pool.blas_root[i]), int(pool.blas_end[i])))
             n += 1
         if n:
-            self._ck(self._lib.sb_update_transforms(self._ctx, None, None, 0))
+            if carryTlas:
+                self._ck(self._lib.sb_update_transforms(self._ctx, None, None, 0))
             self.stats["refits"] += n
+        return changed
 
     # ------------------------------------------------------------ dirty API
     def markTransformsDirty(self, target=None):
@@ -426,9 +439,7 @@ class ProbeField:
     def synchronize(self):
         self._ck(self._lib.sb_synchronize(self._ctx))
 
-    def _debugRead(self, which: str, cascade: int = 0, out: np.ndarray | None = None) -> np.ndarray:
-        """Read a device buffer (the _debugRead seam, gi_probes.js:4830-4841).
-        `out` may be a preallocated (e.g. page-locked) array of the right shape."""
+    def _read_target(self, which: str, out: np.ndarray | None):
         r = self._res
         W, H = r[0] * TILE, r[1] * r[2] * TILE
         P = self._probeTotal
@@ -440,8 +451,26 @@ class ProbeField:
         if out is None:
             out = np.zeros(shape, dt)
         assert out.shape == shape and out.dtype == dt and out.flags["C_CONTIGUOUS"]
+        return key, out
+
+    def _debugRead(self, which: str, cascade: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Read a device buffer (the _debugRead seam, gi_probes.js:4830-4841).
+        `out` may be a preallocated (e.g. page-locked) array of the right shape."""
+        key, out = self._read_target(which, out)
         self._ck(self._lib.sb_read_buffer(self._ctx, _abi.BUF[key] | (cascade << 8), 0, out.size, _abi.ptr(out)))
         return out
+
+    def _debugReadMany(self, reads, cascade: int = 0) -> list:
+        """Several reads queued back to back behind the pending work and waited
+        for once: `reads` is a list of (which, out) as for _debugRead."""
+        outs = []
+        for which, out in reads:
+            key, out = self._read_target(which, out)
+            self._ck(self._lib.sb_read_buffer_async(self._ctx, _abi.BUF[key] | (cascade << 8), 0, out.size,
+                                                    _abi.ptr(out)))
+            outs.append(out)
+        self.synchronize()
+        return outs
 
     @property
     def ctx(self):
