@@ -128,7 +128,10 @@ typedef enum sb_buffer {
     SB_BUF_VISIBILITY = 12,        /* u32, 4 per ray: lights shadow-tested (lo, hi) and
                                       left unblocked (lo, hi), bit = light index 0..63   */
     SB_BUF_TLAS_ORDER = 13,        /* u32, slot -> source instance                       */
-    SB_BUF_INSTANCE_BOUNDS = 14    /* f32, 6 per slot (liveInstanceBounds)               */
+    SB_BUF_INSTANCE_BOUNDS = 14,   /* f32, 6 per slot (liveInstanceBounds)               */
+    SB_BUF_RECORD_E = 15           /* f32, 4 per interior texel (rgb, 1), probeTotal*36:
+                                      the FP32 upload output of the last solve of the
+                                      last sb_forward_record (read-only)                 */
 } sb_buffer;
 
 /* Ranged host->device write into a reference buffer (the copySceneStorageRanges /
@@ -281,20 +284,34 @@ sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* srcInstances, const 
 /* ------------------------------------------------------ differentiation */
 
 /* Adjoint of shade+blend+upload with hit records and visibility held fixed.
- * Parameters: per-material albedo RGB and emissive RGB, per-light intensity. */
+ * Parameters: per-material albedo RGB (material record floats 0..2) and
+ * emissive RGB (floats 7..9), and per light a scale s of its record colour
+ * (floats 7..9) at s = 1: dIntensity[l] = dL/ds_l, so a light of intensity I
+ * has dL/dI = dIntensity[l] / I. Every branch of the forward (clamps, the
+ * temporal mix's selects) is held at its recorded side; the RGBA16F rounding
+ * of the atlas a later solve reads is passed straight through. */
 typedef struct sb_grads {
     float* dAlbedo;      /* materialCount*3 */
     float* dEmissive;    /* materialCount*3 */
     float* dIntensity;   /* lightCount      */
 } sb_grads;
 
-/* Differentiable forward: `solves` feedback solves of one cascade from a cleared
- * history with fixed hit records; stores the per-solve tape on device and returns
- * the loss sum_texels (E - target)^2 over the interior irradiance texels of the
- * last solve when target != NULL (f32 RGB per interior texel, probe-major). */
+/* Differentiable forward: clears the cascade's histories and atlases, then runs
+ * `solves` (1..8) feedback solves over all its probes, each a full sb_solve,
+ * and records the tape on device: per solve the 16-byte hit records and
+ * visibility masks, the history it starts from and the atlas its bounce reads;
+ * after the last, the final history and the FP32 upload output E
+ * (SB_BUF_RECORD_E). With target != NULL (f32 RGB per interior texel,
+ * probe-major, probeTotal*36*3) it also returns the loss
+ * sum over the interior irradiance texels of the last solve of (E - target)^2,
+ * accumulated in FP64. Synchronizes when target != NULL. */
 sb_status sb_forward_record(sb_ctx* ctx, uint32_t cascade, uint32_t solves,
                             const float* target, double* loss);
-/* Reverse pass of the last sb_forward_record: fills the gradients (host pointers). */
+/* Reverse pass of the last sb_forward_record (which must have had a target):
+ * re-shades each solve from its recorded hits and runs the adjoint kernels from
+ * the last solve back to the first. Fills the gradients (host pointers; any may
+ * be NULL) and synchronizes. SB_ERR_NOT_READY when no tape is recorded or a
+ * scene, light, parameter or cascade change happened since it was. */
 sb_status sb_backward(sb_ctx* ctx, sb_grads* grads);
 
 /* -------------------------------------------------- graphs and autotuning */
@@ -336,6 +353,8 @@ typedef struct sb_stats {
     float lastShadeMs;
     /* the shadow-ray share of the visit counters above */
     uint64_t shadowTlasNodeVisits, shadowInstanceVisits, shadowBlasNodeVisits, shadowTriangleTests;
+    float lastForwardRecordMs;  /* device time of the last sb_forward_record (all solves + loss) */
+    float lastBackwardMs;       /* device time of the last sb_backward                       */
 } sb_stats;
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
 /* Counting costs a few percent; off by default. */

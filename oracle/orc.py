@@ -49,7 +49,7 @@ class OrcSolveIO(C.Structure):
     _fields_ = [("rayOut", C.c_void_p), ("hitTri", C.c_void_p), ("hitInst", C.c_void_p), ("secondT", C.c_void_p),
                 ("tested", C.c_void_p), ("blocked", C.c_void_p), ("replayTri", C.c_void_p),
                 ("replayInst", C.c_void_p), ("replayBlocked", C.c_void_p), ("rayIn", C.c_void_p),
-                ("preRound", C.c_void_p), ("counters", C.c_void_p)]
+                ("preRound", C.c_void_p), ("counters", C.c_void_p), ("hitFacing", C.c_void_p)]
 
 
 def load() -> C.CDLL:
@@ -210,3 +210,41 @@ def new_state(grid: dict, fp32: bool = False):
     atlas = np.zeros((H, W, 4), np.uint16)
     atlas[..., 3] = 0x3C00  # (0,0,0,1), clearAtlasKernel
     return (np.zeros(P * 64 * 4, dt), np.zeros(P * 64 * 2, dt), atlas, atlas.copy())
+
+
+def adjoint(scene: OrcScene, arena: np.ndarray, light_count: int, clustered: bool, grid: OrcGrid,
+            params: np.ndarray, tri: np.ndarray, inst: np.ndarray, blocked: np.ndarray, solves: int,
+            albedo: np.ndarray, emissive: np.ndarray, light_scale: np.ndarray, target: np.ndarray | None = None,
+            round_atlas: bool = True, grad: bool = True, nthreads: int | None = None):
+    """FP64 differentiable solve sequence (orc_adjoint.hpp).
+
+    Replays fixed per-ray hit records (tri, inst | facing << 31) and blocked
+    shadow bits for every solve. Returns (loss, E[probes*36*3], grad or None)
+    with grad = [albedo (mc*3) | emissive (mc*3) | light scale (lights)]."""
+    lib = load()
+    if not hasattr(lib, "_adj"):
+        P = C.c_void_p
+        lib.orc_adjoint.restype = C.c_int
+        lib.orc_adjoint.argtypes = [P, P, P, P, P, P, P, C.c_uint32, C.c_int32, P, P, P, C.c_uint32, C.c_uint32,
+                                    P, P, P, P, C.c_int32]
+        lib._adj = True
+    L = OrcLights()
+    L.data = _p(arena); L.dataLen = arena.shape[0]; L.lightCount = light_count; L.clustered = 1 if clustered else 0
+    prm = np.ascontiguousarray(params, np.float64)
+    mc = albedo.size // 3
+    alb = np.ascontiguousarray(albedo, np.float64)
+    emi = np.ascontiguousarray(emissive, np.float64)
+    ls = np.ascontiguousarray(light_scale, np.float64)
+    tri = np.ascontiguousarray(tri, np.int32)
+    inst = np.ascontiguousarray(inst, np.int32)
+    blocked = np.ascontiguousarray(blocked, np.uint64)
+    probes = grid.res[0] * grid.res[1] * grid.res[2]
+    E = np.zeros(probes * 36 * 3, np.float64)
+    loss = C.c_double(0.0)
+    tgt = None if target is None else np.ascontiguousarray(target, np.float64)
+    g = np.zeros(6 * mc + ls.size, np.float64) if (grad and tgt is not None) else None
+    rc = lib.orc_adjoint(C.byref(scene), C.byref(L), C.byref(grid), _p(prm), _p(tri), _p(inst), _p(blocked),
+                         solves, 1 if round_atlas else 0, _p(alb), _p(emi), _p(ls), mc, ls.size, _p(tgt),
+                         C.byref(loss), _p(E), _p(g), nthreads or threads())
+    assert rc == 0
+    return loss.value, E, g

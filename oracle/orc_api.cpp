@@ -30,6 +30,7 @@ struct OrcSolveIO {
     const void* rayIn;        // R rays to blend instead of tracing (replay of the blend alone)
     void* preRound;           // R[probeTotal*36*3]: unrounded upload RGB
     uint64_t* counters;       // [tlasNodes, instances, blasNodes, triTests] (primary + shadow)
+    int32_t* hitFacing;       // per ray: 1 front, 0 back, -1 miss
 };
 
 
@@ -135,6 +136,7 @@ static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, 
                 if (io->secondT) static_cast<R*>(io->secondT)[i] = o.secondT;
                 if (io->tested) io->tested[i] = o.tested;
                 if (io->blocked) io->blocked[i] = o.blocked;
+                if (io->hitFacing) io->hitFacing[i] = o.tri >= 0 ? o.facing : -1;
             }
         });
         if (io && io->counters) {
@@ -255,6 +257,46 @@ void orc_compute_instances(const double* world16, const uint8_t* active, const f
             aabbs9[i * 9 + k] = b.mn[k]; aabbs9[i * 9 + 3 + k] = b.mx[k]; aabbs9[i * 9 + 6 + k] = b.c[k];
         }
     }
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- adjoint
+#include "orc_adjoint.hpp"
+
+extern "C" {
+
+// Differentiable solve sequence in FP64 (orc_adjoint.hpp). Replay records are
+// per ray of one solve (probe-major, probe index = slot) and serve every solve.
+// Parameters: albedo / emissive (materialCount x 3), lightScale (lightCount).
+// Outputs (any may be null): loss (needs target), E (probes x 36 x 3), grad
+// ([albedo | emissive | light scale], needs target).
+int orc_adjoint(const OrcScene* s, const OrcLights* l, const OrcGrid* g, const double* params, const int32_t* tri,
+                const int32_t* inst, const uint64_t* blocked, uint32_t solves, int32_t roundAtlas,
+                const double* albedo, const double* emissive, const double* lightScale, uint32_t materialCount,
+                uint32_t lightCount, const double* target, double* lossOut, double* eOut, double* gradOut,
+                int32_t threads) {
+    Scene sc = to_scene(s);
+    Lights L;
+    L.data = l->data; L.dataLen = l->dataLen; L.lightCount = l->lightCount; L.clustered = l->clustered;
+    AdjProblem A;
+    A.sc = &sc;
+    A.L = &L;
+    A.g = to_grid(g);
+    std::memcpy(&A.P, params, sizeof(Params));
+    A.tri = tri; A.inst = inst; A.blocked = blocked;
+    A.solves = solves;
+    A.roundAtlas = roundAtlas != 0;
+    A.materialCount = materialCount;
+    A.lightCount = lightCount;
+    A.albedo = albedo; A.emissive = emissive; A.lightScale = lightScale;
+    A.threads = std::max(1, (int)threads);
+    AdjTape T;
+    double loss = adj_forward(A, T, target);
+    if (lossOut) *lossOut = loss;
+    if (eOut) std::memcpy(eOut, T.E.data(), T.E.size() * sizeof(double));
+    if (gradOut && target) adj_backward(A, T, target, gradOut);
+    return 0;
 }
 
 }  // extern "C"

@@ -41,6 +41,7 @@ template <class R> struct RayOut {
     R secondT;            // second-nearest accepted candidate (near-tie rule)
     uint64_t tested;      // NEE lights whose shadow ray was traced
     uint64_t blocked;     // ... and found blocked
+    int facing = -1;      // hit: 1 when the geometric normal faced the ray (front side)
 };
 
 // Replay input: the GPU's own hit decision and shadow bits for one ray.
@@ -83,7 +84,12 @@ template <class R> void light_grid(const Grid& g0, const float* lightsIn, uint32
 
 // Hardware bilinear on an RGBA16F texture with clamp-to-edge addressing,
 // evaluated with exact weights (texel centres at i + 0.5).
-template <class R> inline V3<R> bilinear_rgb(const uint16_t* atlas, uint32_t W, uint32_t H, R u, R v) {
+inline double texel_value(uint16_t h) { return from_half(h); }
+inline double texel_value(double d) { return d; }
+
+// `atlas` holds RGBA16F texels (uint16_t) or, for the unrounded feedback of the
+// adjoint checks, the same texels as doubles.
+template <class R, class T> inline V3<R> bilinear_rgb(const T* atlas, uint32_t W, uint32_t H, R u, R v) {
     R x = u * R(W) - R(0.5), y = v * R(H) - R(0.5);
     R fx0 = std::floor(x), fy0 = std::floor(y);
     R fx = x - fx0, fy = y - fy0;
@@ -94,15 +100,15 @@ template <class R> inline V3<R> bilinear_rgb(const uint16_t* atlas, uint32_t W, 
     R wxs[2] = {R(1) - fx, fx}, wys[2] = {R(1) - fy, fy};
     for (int j = 0; j < 2; ++j)
         for (int i = 0; i < 2; ++i) {
-            const uint16_t* t = atlas + ((size_t)ys[j] * W + xs[i]) * 4;
+            const T* t = atlas + ((size_t)ys[j] * W + xs[i]) * 4;
             R w = wxs[i] * wys[j];
-            out = out + V3<R>(R(from_half(t[0])), R(from_half(t[1])), R(from_half(t[2]))) * w;
+            out = out + V3<R>(R(texel_value(t[0])), R(texel_value(t[1])), R(texel_value(t[2]))) * w;
         }
     return out;
 }
 
 // sampleAtlas, gi_probes.js:1941-1974
-template <class R> V3<R> sample_atlas(const Grid& g, const uint16_t* atlas, V3<R> P, V3<R> N) {
+template <class R, class T> V3<R> sample_atlas(const Grid& g, const T* atlas, V3<R> P, V3<R> N) {
     V3<R> cell(R(g.gridSize[0]) / std::max(R(1), R(g.res[0]) - R(1)),
                R(g.gridSize[1]) / std::max(R(1), R(g.res[1]) - R(1)),
                R(g.gridSize[2]) / std::max(R(1), R(g.res[2]) - R(1)));
@@ -155,6 +161,26 @@ template <class R> struct Tracer {
     const Params& P;
     const uint16_t* atlasPrev;  // previous upload's irradiance atlas (RGBA16F)
     Traverser<R> tr;
+    // Adjoint checks: the previous atlas as unrounded doubles, and shading
+    // parameters in FP64 that replace the material / light record values
+    // (albedo = floats 0..2, emissive = floats 7..9, a scale of the light
+    // colour 7..9). Null = use the records.
+    const double* atlasPrevD = nullptr;
+    const double* albedo = nullptr;
+    const double* emissive = nullptr;
+    const double* lightScale = nullptr;
+    // Intermediates of one hit's shading, filled when non-null (adjoint checks):
+    // the unblocked lights' terms are kd (.) X[i].
+    struct ShadeRecord {
+        bool hit = false;
+        uint32_t m = 0;
+        R kdScale = 0;
+        V3<R> kdr, kd, smp, bounce, hitPos, ng;
+        uint32_t nLights = 0;
+        uint32_t li[MAX_LIGHTS];
+        V3<R> X[MAX_LIGHTS];
+    };
+    mutable ShadeRecord* rec = nullptr;
     Tracer(const Scene& sc, const Lights& l, const Grid& gg, const Grid& gg0, const Params& pp, const uint16_t* ap)
         : s(sc), L(l), g(gg), g0(gg0), P(pp), atlasPrev(ap), tr(sc) {}
 
@@ -169,6 +195,7 @@ template <class R> struct Tracer {
         bool isIr = std::fabs(eclass - R(4)) < R(0.25);
         R irs = isIr ? R(P.nirGate) * R(P.nirGain) : R(1);
         V3<R> lcol = V3<R>(R(Lr[7]), R(Lr[8]), R(Lr[9])) * irs;
+        if (lightScale) lcol = lcol * R(lightScale[li]);
         R lrange = R(Lr[10]), ldecay = R(Lr[11]), lcosAngle = R(Lr[12]), lcosPen = R(Lr[13]);
         bool isDir = ltype < R(0.5);
         bool isSpot = std::fabs(ltype - R(2)) < R(0.5);
@@ -198,6 +225,10 @@ template <class R> struct Tracer {
         R atten = distAtten * (isSpot ? spotAtten : R(1));
         V3<R> diffuse = kd * (R(1) / R(PI));
         radiance = radiance + mulv(diffuse * ndl, lcol) * atten * R(P.debugDirectScale);
+        if (rec && rec->nLights < (uint32_t)MAX_LIGHTS) {
+            rec->li[rec->nLights] = li;
+            rec->X[rec->nLights++] = mulv(V3<R>(R(1), R(1), R(1)) * (ndl / R(PI)), lcol) * atten * R(P.debugDirectScale);
+        }
     }
 
     // traceKernel body for one (slot, k), gi_probes.js:1977-2214.
@@ -242,17 +273,30 @@ template <class R> struct Tracer {
                   p2 = tr.fetch_vert(tr.tri_vert(tri, 2));
             V3<R> ngRaw = tr.inst_normal_to_world(inst, normalize(cross(p1 - p0, p2 - p0)));
             bool faceFwd = replayFacing >= 0 ? replayFacing == 1 : dot(ngRaw, rd) < R(0);
+            o.facing = faceFwd ? 1 : 0;
             V3<R> ng = ngRaw * (faceFwd ? R(1) : R(-1));
             V3<R> hitPoint = ro + rd * bestT;
             R traceBias = std::max(R(g.cellMin) * R(TRACE_SURFACE_BIAS_CELL) * R(P.debugTraceBiasScale),
                                    R(RAY_EPS) * R(P.debugRayEpsScale));
             V3<R> hitPos = hitPoint + ng * traceBias;
             V3<R> baseColor(tr.mat_f(m, 0), tr.mat_f(m, 1), tr.mat_f(m, 2));
-            V3<R> emissive(tr.mat_f(m, 7), tr.mat_f(m, 8), tr.mat_f(m, 9));
-            V3<R> radiance = emissive * R(P.debugEmissiveScale);
+            V3<R> emis(tr.mat_f(m, 7), tr.mat_f(m, 8), tr.mat_f(m, 9));
+            if (albedo) baseColor = V3<R>(R(albedo[3 * m]), R(albedo[3 * m + 1]), R(albedo[3 * m + 2]));
+            if (emissive) emis = V3<R>(R(emissive[3 * m]), R(emissive[3 * m + 1]), R(emissive[3 * m + 2]));
+            V3<R> radiance = emis * R(P.debugEmissiveScale);
             R metal = tr.mat_f(m, 4), transm = tr.mat_f(m, 5);
             V3<R> kdr = baseColor * R(P.debugAlbedoScale) * (R(1) - metal) * (R(1) - transm);
             V3<R> kd(clampv(kdr.x, R(0), R(0.95)), clampv(kdr.y, R(0), R(0.95)), clampv(kdr.z, R(0), R(0.95)));
+            if (rec) {
+                rec->hit = true;
+                rec->m = m;
+                rec->kdScale = R(P.debugAlbedoScale) * (R(1) - metal) * (R(1) - transm);
+                rec->kdr = kdr;
+                rec->kd = kd;
+                rec->hitPos = hitPos;
+                rec->ng = ng;
+                rec->nLights = 0;
+            }
             const uint64_t* rb = rp ? &rp->blocked[rayIdx] : nullptr;
             if (L.clustered) {
                 V3<R> cellCount{R(g0.res[0]) - R(1), R(g0.res[1]) - R(1), R(g0.res[2]) - R(1)};
@@ -280,12 +324,18 @@ template <class R> struct Tracer {
                 for (uint32_t li = 0; li < L.lightCount; ++li)
                     shade_light(li, hitPos, ng, kd, traceBias, radiance, o, rb);
             }
-            V3<R> bounce = mulv(sample_atlas<R>(g, atlasPrev, hitPos, ng), kd) * (R(1) / R(PI));
+            V3<R> smp = atlasPrevD ? sample_atlas<R>(g, atlasPrevD, hitPos, ng) : sample_atlas<R>(g, atlasPrev, hitPos, ng);
+            V3<R> bounce = mulv(smp, kd) * (R(1) / R(PI));
+            if (rec) {
+                rec->smp = smp;
+                rec->bounce = bounce;
+            }
             R bl = luma(bounce);
             R roll = R(P.radianceClamp) / std::max(std::max(R(P.radianceClamp), bl), R(1e-6));
             radiance = radiance + bounce * roll * R(P.debugBounceScale);
             outRgb = radiance;
         } else {
+            if (rec) rec->hit = false;
             outRgb = sky<R>(P, rd);
         }
         o.rgb[0] = outRgb.x;

@@ -200,6 +200,7 @@ __global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, De
         float3 filt = mk(facc.x / fden, facc.y / fden, facc.z / fden);
         float s = P.filterStrength;
         S.u.out[p][lane] = make_float4(mixf(eC.x, filt.x, s), mixf(eC.y, filt.y, s), mixf(eC.z, filt.z, s), 1.0f);
+        if (C.eOut) C.eOut[(size_t)probeIndex * BLEND_TEXELS + lane] = S.u.out[p][lane];  // pre-FP16 value
     }
     __syncthreads();
 

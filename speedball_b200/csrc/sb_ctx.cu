@@ -87,6 +87,31 @@ struct sb_ctx {
     cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
     bool timed = false;
     bool singleChunk = true;
+
+    // Differentiable solves (sb_forward_record / sb_backward). `epoch` counts
+    // changes to anything the shading reads; a tape is only replayed under the
+    // epoch it was recorded in.
+    uint64_t epoch = 1;
+    float4* recordE = nullptr;     // set while a recorded solve runs: FP32 upload output
+    struct Tape {
+        uint32_t cascade = 0, solves = 0, probes = 0, rays = 0, texels = 0;
+        uint64_t epoch = 0;
+        bool ready = false, hasTarget = false, timedF = false, timedB = false;
+        uint4* hits = nullptr; size_t hitsCap = 0;       // solves x probes x rays
+        uint4* vis = nullptr; size_t visCap = 0;
+        float4* hist = nullptr; size_t histCap = 0;      // (solves + 1) x probes x 64: history before each solve
+        uint2* atlas = nullptr; size_t atlasCap = 0;     // solves x texels: the atlas each solve's bounce reads
+        float4* E = nullptr; size_t ECap = 0;            // probes x 36: last solve's upload output
+        float4* gE = nullptr; size_t gECap = 0;
+        float* target = nullptr; size_t targetCap = 0;   // probes x 36 x 3
+        float4* shaded = nullptr; size_t shadedCap = 0;  // probes x rays: re-shaded radiance
+        float4* gR = nullptr; size_t gRCap = 0;
+        float4* gH = nullptr; size_t gHCap = 0;          // 2 x probes x 64 (ping-pong)
+        float4* gA = nullptr; size_t gACap = 0;          // 2 x texels (ping-pong)
+        double* gParam = nullptr; size_t gParamCap = 0;  // materials x 6 + lights
+        double* loss = nullptr; size_t lossCap = 0;
+        cudaEvent_t evF0 = nullptr, evF1 = nullptr, evB0 = nullptr, evB1 = nullptr;
+    } tape;
 };
 
 namespace {
@@ -196,6 +221,7 @@ DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint3
     D.atlasPrev = K.atlas;
     D.atlas = K.atlas;
     D.depthAtlas = K.depthAtlas;
+    D.eOut = c->recordE;
     return D;
 }
 
@@ -230,6 +256,19 @@ sb_status light_grid_if_needed(sb_ctx* ctx) {
     CK(launch_light_grid(ctx->B.lights, ctx->lightCount, g0, ctx->stream));
     ctx->lightGridDirty = false;
     return SB_OK;
+}
+
+// A material-buffer range that lies inside the material records and writes
+// none of the fields the packer reads (opacity 10, side 22, alpha test 23,
+// flags 26): the derived layouts and the scene BVH stay valid.
+bool shading_only(const SceneBuffers& B, uint32_t start, uint32_t count) {
+    const uint64_t end = (uint64_t)start + count;
+    if (end > (uint64_t)B.materialCount * SB_MAT_STRIDE) return false;
+    for (uint64_t i = start; i < end; ++i) {
+        const uint32_t f = (uint32_t)(i % SB_MAT_STRIDE);
+        if (f == 10 || f == 22 || f == 23 || f == 26) return false;
+    }
+    return true;
 }
 
 sb_status check_grid(sb_ctx* ctx, const sb_grid* g) {
@@ -342,6 +381,12 @@ void sb_destroy(sb_ctx* ctx) {
         release(K.vis);
     }
     release(ctx->jobs);
+    auto& T = ctx->tape;
+    release(T.hits); release(T.vis); release(T.hist); release(T.atlas); release(T.E); release(T.gE);
+    release(T.target); release(T.shaded); release(T.gR); release(T.gH); release(T.gA); release(T.gParam);
+    release(T.loss);
+    for (cudaEvent_t e : {T.evF0, T.evF1, T.evB0, T.evB1})
+        if (e) cudaEventDestroy(e);
     release(ctx->dErr); release(ctx->dGate); release(ctx->dWork); release(ctx->dCounters);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->evMid) cudaEventDestroy(ctx->evMid);
@@ -450,6 +495,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     ctx->tlasOnDevice = false;
     ctx->sceneLoaded = true;
     ctx->flat.dirty = true;
+    ++ctx->epoch;
     if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
     // validation + derived layouts; a pending TLAS is packed by sb_build_tlas
     uint32_t one = 1u;
@@ -499,7 +545,8 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
     if (!dst) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not allocated", buf);
     if ((size_t)start + count > len) return fail(ctx, SB_ERR_INVALID_ARG, "range [%u,+%u) outside %zu", start, count, len);
     CK(cudaMemcpyAsync((char*)dst + (size_t)start * esz, src, (size_t)count * esz, cudaMemcpyHostToDevice, ctx->stream));
-    if (buf <= SB_BUF_MATERIALS) {
+    ++ctx->epoch;
+    if (buf <= SB_BUF_MATERIALS && !(buf == SB_BUF_MATERIALS && shading_only(B, start, count))) {
         ctx->needPack = true;
         ctx->flat.dirty = true;
     }
@@ -532,6 +579,7 @@ static sb_status read_enqueue(sb_ctx* ctx, uint32_t which, uint32_t start, uint3
         case SB_BUF_VISIBILITY: if (K) { srcp = K->vis; len = K->vis ? K->rayCap * 4 : 0; } break;
         case SB_BUF_TLAS_ORDER: srcp = ctx->I.order; len = ctx->instancesSet ? ctx->I.count : 0; break;
         case SB_BUF_INSTANCE_BOUNDS: srcp = ctx->I.liveBounds; len = ctx->instancesSet ? (size_t)ctx->I.count * 6 : 0; break;
+        case SB_BUF_RECORD_E: srcp = ctx->tape.E; len = ctx->tape.ready ? (size_t)ctx->tape.probes * 36 * 4 : 0; break;
         default: return fail(ctx, SB_ERR_INVALID_ARG, "unknown buffer %u", buf);
     }
     if (!srcp) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not available", buf);
@@ -578,6 +626,7 @@ sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count, ui
     ctx->emitterCount = emitterCount;
     ctx->clustered = clustered ? 1 : 0;
     ctx->lightGridDirty = ctx->clustered != 0;
+    ++ctx->epoch;
     return SB_OK;
 }
 
@@ -586,6 +635,7 @@ sb_status sb_set_params(sb_ctx* ctx, const sb_params* p) {
     if (p->classifyStrength != 0.0f)
         return fail(ctx, SB_ERR_UNSUPPORTED, "probe classification / relocation (classifyStrength > 0) is not built");
     ctx->params = *p;
+    ++ctx->epoch;
     return SB_OK;
 }
 
@@ -621,6 +671,7 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
     K.atlasW = g->res[0] * 8;
     K.atlasH = g->res[1] * g->res[2] * 8;
     K.configured = true;
+    ++ctx->epoch;
     if (!sameDims) {
         DevCascade D = dev_cascade(ctx, ci, 0, 0);
         CK(launch_clear_cascade(D, ctx->stream));
@@ -689,6 +740,128 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     return SB_OK;
 }
 
+// ---------------------------------------------------------------- adjoint
+
+sb_status sb_forward_record(sb_ctx* ctx, uint32_t ci, uint32_t solves, const float* target, double* loss) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (solves < 1 || solves > 8) return fail(ctx, SB_ERR_INVALID_ARG, "solves=%u outside [1,8]", solves);
+    if (target && !loss) return fail(ctx, SB_ERR_INVALID_ARG, "loss is null");
+    if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+        return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+    cudaSetDevice(ctx->device);
+    Cascade& K = ctx->casc[ci];
+    auto& T = ctx->tape;
+    T.ready = false;
+    const uint32_t probes = K.probeTotal, rays = K.grid.raysPerProbe;
+    const size_t nRay = (size_t)probes * rays, texels = (size_t)K.atlasW * K.atlasH;
+    CK(grow(T.hits, T.hitsCap, solves * nRay));
+    CK(grow(T.vis, T.visCap, solves * nRay));
+    CK(grow(T.hist, T.histCap, (solves + 1) * (size_t)probes * 64));
+    CK(grow(T.atlas, T.atlasCap, solves * texels));
+    CK(grow(T.E, T.ECap, (size_t)probes * 36));
+    CK(grow(T.loss, T.lossCap, 1));
+    if (!T.evF0) {
+        for (cudaEvent_t* e : {&T.evF0, &T.evF1, &T.evB0, &T.evB1}) CK(cudaEventCreate(e));
+    }
+    CK(cudaEventRecord(T.evF0, ctx->stream));
+    CK(launch_clear_cascade(dev_cascade(ctx, ci, 0, 0), ctx->stream));
+    const size_t histBytes = (size_t)probes * 64 * sizeof(float4), atlasBytes = texels * sizeof(uint2);
+    for (uint32_t s = 0; s < solves; ++s) {
+        CK(cudaMemcpyAsync(T.hist + s * (size_t)probes * 64, K.irr, histBytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(T.atlas + s * texels, K.atlas, atlasBytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->recordE = s + 1 == solves ? T.E : nullptr;
+        sb_status st = sb_solve(ctx, ci, 0, probes);
+        ctx->recordE = nullptr;
+        if (st != SB_OK) return st;
+        CK(cudaMemcpyAsync(T.hits + s * nRay, K.hits, nRay * sizeof(uint4), cudaMemcpyDeviceToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(T.vis + s * nRay, K.vis, nRay * sizeof(uint4), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(T.hist + solves * (size_t)probes * 64, K.irr, histBytes, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    T.hasTarget = target != nullptr;
+    if (target) {
+        CK(grow(T.target, T.targetCap, (size_t)probes * 36 * 3));
+        CK(grow(T.gE, T.gECap, (size_t)probes * 36));
+        CK(cudaMemcpyAsync(T.target, target, (size_t)probes * 36 * 3 * sizeof(float), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(launch_adjoint_loss(T.E, T.target, probes * 36, T.gE, T.loss, ctx->stream));
+    }
+    CK(cudaEventRecord(T.evF1, ctx->stream));
+    T.timedF = true;
+    T.cascade = ci;
+    T.solves = solves;
+    T.probes = probes;
+    T.rays = rays;
+    T.texels = (uint32_t)texels;
+    T.epoch = ctx->epoch;
+    T.ready = true;
+    if (target) {
+        CK(cudaMemcpyAsync(loss, T.loss, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        return sb_synchronize(ctx);
+    }
+    return SB_OK;
+}
+
+sb_status sb_backward(sb_ctx* ctx, sb_grads* grads) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    auto& T = ctx->tape;
+    if (!T.ready || !T.hasTarget) return fail(ctx, SB_ERR_NOT_READY, "no recorded forward with a target");
+    if (T.epoch != ctx->epoch)
+        return fail(ctx, SB_ERR_NOT_READY, "scene, lights, parameters or cascade changed since sb_forward_record");
+    cudaSetDevice(ctx->device);
+    const uint32_t probes = T.probes, mc = ctx->B.materialCount, lc = ctx->lightCount;
+    const size_t nRay = (size_t)probes * T.rays, hist = (size_t)probes * 64;
+    const size_t nParam = 6 * (size_t)mc + lc;
+    CK(grow(T.shaded, T.shadedCap, nRay));
+    CK(grow(T.gR, T.gRCap, nRay));
+    CK(grow(T.gH, T.gHCap, 2 * hist));
+    CK(grow(T.gA, T.gACap, 2 * (size_t)T.texels));
+    CK(grow(T.gParam, T.gParamCap, nParam ? nParam : 1));
+    CK(cudaEventRecord(T.evB0, ctx->stream));
+    CK(cudaMemsetAsync(T.gParam, 0, nParam * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(T.gH, 0, hist * sizeof(float4), ctx->stream));
+    const DevScene S = dev_scene(ctx);
+    DevParams P;
+    std::memcpy(&P, &ctx->params, sizeof P);
+    float4* gHnext = T.gH;              // dL/dH after solve s (from solve s + 1's blend)
+    const float4* gAnext = nullptr;     // dL/dAtlas written by solve s (read by solve s + 1)
+    for (int s = (int)T.solves - 1; s >= 0; --s) {
+        DevCascade D = dev_cascade(ctx, T.cascade, 0, probes);
+        D.hits = T.hits + s * nRay;
+        D.vis = T.vis + s * nRay;
+        D.atlasPrev = T.atlas + (size_t)s * T.texels;
+        D.rayData = T.shaded;
+        D.eOut = nullptr;
+        const float4* Hs = T.hist + (size_t)s * hist;
+        const float4* Hs1 = T.hist + (size_t)(s + 1) * hist;
+        const bool last = s + 1 == (int)T.solves;
+        CK(launch_upload_bwd(D, P, Hs1, last ? T.gE : nullptr, gAnext, gHnext, ctx->stream));
+        float4* gAcur = T.gA + (size_t)(s & 1) * T.texels;
+        float4* gHprev = gHnext == T.gH ? T.gH + hist : T.gH;
+        CK(cudaMemsetAsync(gAcur, 0, (size_t)T.texels * sizeof(float4), ctx->stream));
+        CK(launch_shade(S, D, P, probes, ctx->stream));
+        CK(launch_blend_bwd(D, P, T.shaded, Hs, gHnext, gHprev, T.gR, ctx->stream));
+        CK(launch_shade_bwd(S, D, P, T.gR, T.gParam, gAcur, ctx->stream));
+        gHnext = gHprev;
+        gAnext = gAcur;
+    }
+    CK(cudaEventRecord(T.evB1, ctx->stream));
+    T.timedB = true;
+    std::vector<double> g(nParam);
+    if (nParam) CK(cudaMemcpyAsync(g.data(), T.gParam, nParam * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    sb_status st = sb_synchronize(ctx);
+    if (st != SB_OK) return st;
+    if (grads) {
+        for (uint32_t i = 0; i < 3 * mc; ++i) {
+            if (grads->dAlbedo) grads->dAlbedo[i] = (float)g[i];
+            if (grads->dEmissive) grads->dEmissive[i] = (float)g[3 * (size_t)mc + i];
+        }
+        if (grads->dIntensity)
+            for (uint32_t l = 0; l < lc; ++l) grads->dIntensity[l] = (float)g[6 * (size_t)mc + l];
+    }
+    return SB_OK;
+}
+
 sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, float* tOut, int32_t* triOut,
                      int32_t* instOut) {
     if (!ctx || (n && (!ro || !rd || !tOut || !triOut || !instOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
@@ -745,6 +918,7 @@ sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float
 // ----------------------------------------------------------- refit / TLAS
 sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end) {
     if (!ctx) return SB_ERR_INVALID_ARG;
+    ++ctx->epoch;
     if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
     if (!(end > root && end <= ctx->B.nodeCount))
         return fail(ctx, SB_ERR_LAYOUT_VIOLATION, "refit range [%u,%u) outside the node pool", root, end);
@@ -774,6 +948,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
                            const uint32_t* blasRoot, const uint32_t* blasEnd) {
     if (!ctx || !world16 || !active || !blasRoot || !blasEnd) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    ++ctx->epoch;
     if (count != ctx->B.instCount)
         return fail(ctx, SB_ERR_INVALID_ARG, "instance count %u != scene instCount %u", count, ctx->B.instCount);
     for (uint32_t i = 0; i < count; ++i)
@@ -816,6 +991,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
 
 sb_status sb_build_tlas(sb_ctx* ctx) {
     if (!ctx) return SB_ERR_INVALID_ARG;
+    ++ctx->epoch;
     if (!ctx->instancesSet) return fail(ctx, SB_ERR_NOT_READY, "sb_set_instances first");
     if (ctx->I.count > TLAS_BUILD_MAX)
         return fail(ctx, SB_ERR_UNSUPPORTED, "%u instances > %u (single-CTA TLAS build)", ctx->I.count, TLAS_BUILD_MAX);
@@ -835,6 +1011,7 @@ sb_status sb_build_tlas(sb_ctx* ctx) {
 
 sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* src, const double* world16, uint32_t count) {
     if (!ctx) return SB_ERR_INVALID_ARG;
+    ++ctx->epoch;
     if (!ctx->instancesSet || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "instances / TLAS not ready");
     if (!ctx->tlasOnDevice)
         return fail(ctx, SB_ERR_NOT_READY, "the transform lane needs the slot order of a TLAS built by sb_build_tlas");
@@ -902,6 +1079,11 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
             if (cudaEventElapsedTime(&ms, ctx->evB, ctx->evMid) == cudaSuccess) out->lastShadeMs = ms;
         }
     }
+    float fms = 0.0f;
+    if (ctx->tape.timedF && cudaEventElapsedTime(&fms, ctx->tape.evF0, ctx->tape.evF1) == cudaSuccess)
+        out->lastForwardRecordMs = fms;
+    if (ctx->tape.timedB && cudaEventElapsedTime(&fms, ctx->tape.evB0, ctx->tape.evB1) == cudaSuccess)
+        out->lastBackwardMs = fms;
     out->kernelLaunches = launches();
     return SB_OK;
 }
@@ -934,6 +1116,7 @@ extern "C" sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_
                                       const float* vertexData, uint32_t root, uint32_t end) {
     if (!ctx || (vertexCount && !vertexData)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    ++ctx->epoch;
     if ((uint64_t)vertexStart + vertexCount > ctx->B.vertexCount)
         return fail(ctx, SB_ERR_INVALID_ARG, "vertex range [%u,+%u) outside the pool", vertexStart, vertexCount);
     cudaSetDevice(ctx->device);

@@ -105,6 +105,7 @@ struct DevCascade {
     const uint2* atlasPrev;    // RGBA16F texels as 4 halves (the previous upload)
     uint2* atlas;              // RGBA16F output
     uint2* depthAtlas;
+    float4* eOut;              // optional: FP32 upload output of the 36 interior texels per probe (adjoint tape)
 };
 
 struct DevParams {

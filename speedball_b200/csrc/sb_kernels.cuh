@@ -44,6 +44,22 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
                          float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
                          cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
+cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t slotCount,
+                         cudaStream_t st);
+
+// Adjoint of shade + blend + upload (sb_adjoint.cu), over every probe of a
+// cascade (probe slot = probe index). Gradient layouts: gE / E per interior
+// texel (36 per probe, probe-major), gH per history texel (64 per probe: rgb,
+// m2), gA per atlas texel (rgb), gR per ray (rgb), gParam in doubles:
+// [albedo materialCount*3 | emissive materialCount*3 | light scale lightCount].
+cudaError_t launch_adjoint_loss(const float4* E, const float* target, uint32_t n, float4* gE, double* loss,
+                                cudaStream_t st);
+cudaError_t launch_upload_bwd(const DevCascade& C, const DevParams& P, const float4* H, const float4* gE,
+                              const float4* gA, float4* gH, cudaStream_t st);
+cudaError_t launch_blend_bwd(const DevCascade& C, const DevParams& P, const float4* rays, const float4* Hprev,
+                             const float4* gH, float4* gHprev, float4* gR, cudaStream_t st);
+cudaError_t launch_shade_bwd(const DevScene& S, const DevCascade& C, const DevParams& P, const float4* gR,
+                             double* gParam, float4* gA, cudaStream_t st);
 cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st);
 cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st);
 

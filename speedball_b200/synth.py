@@ -153,8 +153,11 @@ def trs(t, r=None, s=1.0):
 
 
 # ----------------------------------------------------------------- scenes
-def room_spheres(seed: int = 0, n_materials: int = 16, n_point: int = 4):
-    """The 82k-triangle room + 64 icospheres scene (plain DDGI, CPU-checkable size)."""
+def room_spheres(seed: int = 0, n_materials: int = 16, n_point: int = 4, n_dir: int = 1):
+    """The 82k-triangle room + 64 icospheres scene (plain DDGI, CPU-checkable size).
+
+    The differentiated workload uses n_materials=64, n_point=32, n_dir=0: 416
+    parameters (64 x 3 albedo, 64 x 3 emissive, 32 light intensities)."""
     rng = np.random.default_rng(seed)
     S = 10.0
     meshes, instances = [], []
@@ -172,7 +175,8 @@ def room_spheres(seed: int = 0, n_materials: int = 16, n_point: int = 4):
     lights = []
     d = rng.normal(size=3)
     d /= np.linalg.norm(d)
-    lights.append(light_record(0, pos=(5, 5, 5), direction=tuple(d), intensity=3.0))
+    if n_dir:
+        lights.append(light_record(0, pos=(5, 5, 5), direction=tuple(d), intensity=3.0))
     for _ in range(n_point):
         lights.append(light_record(1, pos=tuple(rng.uniform(0.0, S, 3)), intensity=float(rng.uniform(5, 20)),
                                    range_=8.0, decay=2.0))
