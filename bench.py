@@ -47,6 +47,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["atrium", "adjoint"], default="atrium",
+                    help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
+                         "differentiated update (64 materials, 32 point lights, 2 feedback solves)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -428,11 +431,139 @@ def run_reference(args, dist: Dist):
     return line
 
 
+ADJ_METRIC = "adjoint / forward device time"
+
+
+def adjoint_field(device):
+    from speedball_b200 import synth
+    from speedball_b200.field import ProbeField
+    scene = synth.room_spheres(0, n_materials=64, n_point=32, n_dir=0)
+    g = scene.meta["grid"]
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+                   hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
+    f.setHysteresisNormalization(False)
+    f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)
+    return scene, f
+
+
+def run_adjoint(args, dist: Dist):
+    """One step = one gradient evaluation: sb_forward_record (2 feedback solves
+    from a cleared history, tape, loss) + sb_backward (re-shade + reverse
+    kernels), 416 parameters. value = backward device time / forward-record
+    device time; the plain forward (the same 2 solves, nothing recorded) is
+    timed beside it."""
+    from speedball_b200 import _abi
+    from speedball_b200.adjoint import GIAdjoint
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    scene, f = adjoint_field(device)
+    lib, ctx = f._lib, f.ctx
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
+    flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
+    adj = GIAdjoint(f, solves=2)
+    rng = np.random.default_rng(7)
+    base = adj.parameters()
+    adj.setParameters(albedo=base["albedo"] * rng.uniform(0.8, 1.2, (64, 3)), lightScale=rng.uniform(0.5, 2.0, 32))
+    target = _abi.PinnedArray((adj.probes, 36, 3), np.float32)
+    target.array[...] = adj.forward()
+    adj.setParameters(albedo=base["albedo"], lightScale=np.ones(32))
+    W, K = args.warmup, args.steps
+    e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
+
+    def flush_l2(i):
+        ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+        ck(rt.cudaStreamSynchronize(stream))
+
+    def plain_forward():
+        # the same two solves without the tape (their work does not depend on
+        # the history they start from)
+        for _ in range(2):
+            _abi.check(lib.sb_solve(ctx, 0, 0, adj.probes), ctx)
+
+    for i in range(W):
+        adj.forward(target.array)
+        adj.backward()
+        flush_l2(i)
+    dist.barrier()
+    clocks = Clocks(device)
+    clocks.start()
+    launches0 = _stats(lib, ctx).kernelLaunches
+    fwd, bwd, wall = [], [], []
+    for i in range(K):
+        flush_l2(i)
+        t0 = time.perf_counter()
+        adj.forward(target.array)
+        adj.backward()
+        wall.append(time.perf_counter() - t0)
+        tm = adj.timings()
+        fwd.append(tm["forwardMs"])
+        bwd.append(tm["backwardMs"])
+    launches = _stats(lib, ctx).kernelLaunches - launches0
+    plain = []
+    for i in range(K):
+        flush_l2(i)
+        ck(rt.cudaEventRecord(e0, stream))
+        plain_forward()
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        plain.append(ck(rt.cudaEventElapsedTime(e0, e1)))
+    clk = clocks.stop()
+    fwd_ms, bwd_ms = dist.max(statistics.mean(fwd)), dist.max(statistics.mean(bwd))
+    plain_ms = dist.max(statistics.mean(plain))
+    wall_ms = dist.max(statistics.mean(wall) * 1e3)
+    nparam = 6 * adj.materialCount + adj.lightCount
+    line = {
+        "metric": ADJ_METRIC, "value": round(bwd_ms / fwd_ms, 4), "unit": "x", "n_gpus": dist.world, "steps": K,
+        "warmup": W, "ms_per_step": round(fwd_ms + bwd_ms, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded room + 64 icospheres)",
+        "config": {"workload": "differentiated update: room + 64 icospheres (81,932 tris), 64 materials, 32 point "
+                               "lights, 8^3 probes x 64 rays, 2 feedback solves, 416 parameters",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "forward_record_ms": round(fwd_ms, 4), "backward_ms": round(bwd_ms, 4),
+        "plain_forward_ms": round(plain_ms, 4), "backward_over_plain_forward": round(bwd_ms / plain_ms, 4),
+        "e2e": {"value": round(wall_ms / plain_ms, 4), "unit": "x (gradient wall time / plain forward device time)",
+                "ms_per_step": round(wall_ms, 4), "h2d_bytes_per_step": int(target.array.nbytes),
+                "d2h_bytes_per_step": int(8 + nparam * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_adjoint_baseline(f, adj, target.array)
+    f.dispose()
+    ck(rt.cudaFree(flush))
+    return line
+
+
+def cpu_adjoint_baseline(f, adj, target):
+    """The oracle's FP64 adjoint (forward + reverse pass) of the same gradient
+    on every host thread, replaying the GPU's hit records."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "tests"))
+    from gpu_util import OracleMirror, gpu_records
+    import orc
+    mirror = OracleMirror(f)
+    rec = gpu_records(f, adj.probes * f.getRays())
+    base = adj.parameters()
+    t0 = time.perf_counter()
+    orc.adjoint(mirror.scene, mirror.arena, mirror.light_count, mirror.clustered, mirror.grid, mirror.params(),
+                rec["tri"], rec["inst_word"], rec["blocked"], 2, base["albedo"].reshape(-1),
+                base["emissive"].reshape(-1), np.ones(adj.lightCount), target=target.astype(np.float64).reshape(-1))
+    dt = time.perf_counter() - t0
+    return {"value": round(dt * 1e3, 2), "unit": "ms per gradient", "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": "one FP64 oracle gradient (2 solves forward + reverse, 416 parameters) on all host threads"}
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
     try:
-        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if args.workload == "adjoint":
+            line = run_adjoint(args, dist) if args.impl == "ours" else \
+                {"impl": "reference", "unavailable": "the reference has no adjoint of the probe update"}
+        else:
+            line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
         if dist.rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:
