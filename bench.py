@@ -47,9 +47,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["atrium", "adjoint"], default="atrium",
+    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch"], default="atrium",
                     help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
-                         "differentiated update (64 materials, 32 point lights, 2 feedback solves)")
+                         "differentiated update (64 materials, 32 point lights, 2 feedback solves); batch: 3 "
+                         "nested cascades of the atrium + 8 independent atria per frame, batched vs plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -555,11 +556,126 @@ def cpu_adjoint_baseline(f, adj, target):
             "sample": "one FP64 oracle gradient (2 solves forward + reverse, 416 parameters) on all host threads"}
 
 
+BATCH_METRIC = "batched probe Mrays/s (11 solves per frame)"
+
+
+def batch_fields(device):
+    """The atrium with 3 nested cascades (16^3, 12^3, 8^3; each twice the
+    previous extent) and 8 independent atria of 20k-500k triangles with their
+    own grids and ray counts, montecarlo jitter, full updates every frame."""
+    from speedball_b200 import synth
+    from speedball_b200.field import ProbeField
+
+    def make(scene, jitter):
+        g = scene.meta["grid"]
+        f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]),
+                       rays=g["rays"], clusteredLighting=True, hysteresis=scene.meta["hysteresis"],
+                       jitterMode=jitter, device=device)
+        f.setHysteresisNormalization(False)
+        f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)
+        return f
+
+    main_scene = make_workload()
+    fields = [make(main_scene, "montecarlo")]
+    for ci, c in enumerate(synth.nested_cascades(main_scene.meta["grid"])[1:], start=1):
+        fields[0].configureCascade(ci, c["gridMin"], c["gridSize"], c["res"])
+    scenes = [main_scene] + synth.batch_scenes()
+    fields += [make(s, "montecarlo") for s in scenes[1:]]
+    return scenes, fields
+
+
+def run_batch(args, dist: Dist):
+    """One step = one frame: every scene's motion lanes on the device (deformer
+    refit, instance bounds + TLAS refit) and 11 solves (the atrium's 3
+    cascades, the 8 atria's C0). value = batched frames' primary rays / device
+    time; the same frames with per-solve launches are timed beside it."""
+    from speedball_b200 import _abi
+    from speedball_b200.batch import BatchedFrame
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    scenes, fields = batch_fields(device)
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    frame = BatchedFrame(fields, extra=[(fields[0], 1), (fields[0], 2)])
+    frame.setStream(int(stream))
+    flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
+    lanes = []
+    for s, f in zip(scenes, fields):
+        dm = s.meta["deformer"]
+        lanes.append((f, int(f.pool.blas_root[dm]), int(f.pool.blas_end[dm])))
+    rays = sum(f._probeTotal * f.getRays() for f in fields)
+    rays += sum(fields[0].cascadeProbes(ci) * fields[0].getRays() for ci in (1, 2))
+    tris = sum(int(f.pool.triIndex.shape[0]) for f in fields)
+    W, K = args.warmup, args.steps
+    e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
+
+    def motion():
+        for f, root, end in lanes:
+            _abi.check(f._lib.sb_refit_blas(f.ctx, root, end), f.ctx)
+            _abi.check(f._lib.sb_update_transforms(f.ctx, None, None, 0), f.ctx)
+
+    def timed(step):
+        for i in range(W):
+            step()
+            ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+        ck(rt.cudaStreamSynchronize(stream))
+        dist.barrier()
+        l0 = _stats(fields[0]._lib, fields[0].ctx).kernelLaunches
+        total = 0.0
+        for i in range(K):
+            ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+            ck(rt.cudaEventRecord(e0, stream))
+            step()
+            ck(rt.cudaEventRecord(e1, stream))
+            ck(rt.cudaEventSynchronize(e1))
+            total += ck(rt.cudaEventElapsedTime(e0, e1))
+        launches = _stats(fields[0]._lib, fields[0].ctx).kernelLaunches - l0
+        return dist.max(total / K), launches
+
+    def batched():
+        motion()
+        frame.tick()
+
+    def plain():
+        motion()
+        frame.tickPlain()
+
+    clocks = Clocks(device)
+    clocks.start()
+    ms_plain, _ = timed(plain)
+    ms_batch, launches = timed(batched)
+    clk = clocks.stop()
+    value = dist.world * rays / (ms_batch * 1e-3) / 1e6
+    plain_value = dist.world * rays / (ms_plain * 1e-3) / 1e6
+    line = {
+        "metric": BATCH_METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": dist.world, "steps": K,
+        "warmup": W, "ms_per_step": round(ms_batch, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural atria)",
+        "config": {"workload": "atrium 262,267 tris with 3 nested cascades (16^3, 12^3, 8^3 probes x 64 rays; "
+                               "extents x1, x2, x4) + 8 atria of 20k-500k tris with 8^3-16^3 probes at 32-128 "
+                               "rays; montecarlo jitter; per frame every scene's deformer refit + TLAS refit",
+                   "solves_per_frame": 11, "primary_rays_per_step": int(rays), "triangles": tris,
+                   "grids": [list(f.getResolution()) + [f.getRays()] for f in fields],
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "plain_value": round(plain_value, 3), "plain_ms_per_step": round(ms_plain, 4),
+        "batched_over_plain": round(ms_plain / ms_batch, 4),
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    for f in fields:
+        f.dispose()
+    ck(rt.cudaFree(flush))
+    return line
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
     try:
-        if args.workload == "adjoint":
+        if args.workload == "batch":
+            line = run_batch(args, dist) if args.impl == "ours" else \
+                {"impl": "reference", "unavailable": "the reference has no batched multi-scene form"}
+        elif args.workload == "adjoint":
             line = run_adjoint(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference has no adjoint of the probe update"}
         else:

@@ -204,9 +204,15 @@ sb_status sb_set_params(sb_ctx* ctx, const sb_params* params);
  * solveKernels pass, gi_probes.js:3815-3836). Enqueue only. */
 sb_status sb_solve(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount);
 
-/* The batched form: solves of several contexts (scenes) and cascades in ONE
- * persistent trace launch over a shared ray queue, then one blend/upload launch.
- * All contexts must live on the same device; work runs on ctxs[0]'s stream. */
+/* The batched form: solves of several contexts (scenes) and cascades through
+ * one launch per stage: one persistent closest-hit launch over a shared ray
+ * queue, one job-emission launch, one persistent shadow launch over a shared
+ * job queue, one shade launch and one blend/upload launch for all items.
+ * At most 16 items, all on one device, no (context, cascade) twice; the batch
+ * runs on items[0].ctx's stream (which also owns the queues), ordered after
+ * the other contexts' pending work and before their later work. Each item's
+ * results equal those of sb_solve with the same arguments. Enqueue only;
+ * device errors latch in each item's own context. */
 typedef struct sb_solve_item {
     sb_ctx* ctx;
     uint32_t cascade, probeOffset, updatedCount;

@@ -1,0 +1,79 @@
+"""Batched probe updates: several fields (independent scenes) and cascades of
+different divisions through one launch per stage (sb_solve_batch).
+
+The reference updates one field's cascades with one compute pass each
+(gi_probes.js:3732-3840); there is no cross-scene batching in it. Here a frame
+of many fields runs every field's tick lanes (beginTick), one batched solve of
+all their probe ranges plus any extra cascades, then endTick on each. The
+per-item arithmetic is the per-solve arithmetic, so a batched frame produces
+the same atlases as the same solves run one by one.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+from . import _abi
+from .field import ProbeField
+
+
+@dataclass
+class SolveItem:
+    field: ProbeField
+    cascade: int
+    probeOffset: int
+    updatedCount: int
+
+
+def solveBatch(items) -> None:
+    """One sb_solve_batch over `items` (SolveItem); the first item's field
+    owns the launch's stream and queues."""
+    items = list(items)
+    if not items:
+        return
+    arr = (_abi.sb_solve_item * len(items))()
+    for i, it in enumerate(items):
+        arr[i].ctx = it.field.ctx
+        arr[i].cascade = it.cascade
+        arr[i].probeOffset = it.probeOffset
+        arr[i].updatedCount = it.updatedCount
+    lead = items[0].field
+    _abi.check(lead._lib.sb_solve_batch(arr, len(items)), lead.ctx)
+
+
+class BatchedFrame:
+    """Per-frame driver of several fields: each field's C0 tick range, plus
+    extra cascades (field, ci) solved in full every frame."""
+
+    def __init__(self, fields, extra=()):
+        self.fields = list(fields)
+        self.extra = list(extra)
+
+    def items(self, frames) -> list:
+        out = [SolveItem(f, fr["cascade"], fr["probeOffset"], fr["updatedCount"])
+               for f, fr in zip(self.fields, frames)]
+        out += [SolveItem(f, ci, 0, f.cascadeProbes(ci)) for f, ci in self.extra]
+        return out
+
+    def tick(self) -> list:
+        """All solves of the frame in one batched launch."""
+        frames = [f.beginTick() for f in self.fields]
+        solveBatch(self.items(frames))
+        for f, fr in zip(self.fields, frames):
+            f.endTick(fr)
+        return frames
+
+    def tickPlain(self) -> list:
+        """The same solves as per-field launches, one after another."""
+        frames = [f.beginTick() for f in self.fields]
+        for it in self.items(frames):
+            _abi.check(it.field._lib.sb_solve(it.field.ctx, it.cascade, it.probeOffset, it.updatedCount),
+                       it.field.ctx)
+        for f, fr in zip(self.fields, frames):
+            f.endTick(fr)
+        return frames
+
+    def setStream(self, stream) -> None:
+        """Put every field on one CUDA stream (an int handle)."""
+        for f in self.fields:
+            _abi.check(f._lib.sb_set_stream(f.ctx, C.c_void_p(int(stream))), f.ctx)

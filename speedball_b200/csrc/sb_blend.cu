@@ -39,11 +39,13 @@ struct BlendSmem {
     float2 dep[BLEND_PROBES][BLEND_TEXELS];
 };
 
-__global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, DevParams P) {
-    __shared__ BlendSmem S;
+// Blend + upload of probe slots [block * BLEND_PROBES, + BLEND_PROBES) of one
+// solve; the body of the per-solve and the batched kernels.
+__device__ __forceinline__ void blend_upload_block(const DevCascade& C, const DevParams& P, uint32_t block,
+                                                   BlendSmem& S) {
     const int tid = threadIdx.x;
     const int p = tid / BLEND_TEXELS, lane = tid % BLEND_TEXELS;
-    const uint32_t base = blockIdx.x * BLEND_PROBES;
+    const uint32_t base = block * BLEND_PROBES;
     const uint32_t slot = base + p;
     const bool live = slot < C.updatedCount;
     const uint32_t N = C.rays;
@@ -224,12 +226,35 @@ __global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, De
     }
 }
 
+__global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, DevParams P) {
+    __shared__ BlendSmem S;
+    blend_upload_block(C, P, blockIdx.x, S);
+}
+
+// Every item of a batch: CTAs [blendBase, blendBase + blendBlocks) belong to item i.
+__global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload_batch(const __grid_constant__ BatchArgs B) {
+    __shared__ BlendSmem S;
+    uint32_t i = 0;
+    while (i + 1 < B.n && blockIdx.x >= B.it[i + 1].blendBase) ++i;
+    const BatchItem& I = B.it[i];
+    if (blockIdx.x - I.blendBase >= I.blendBlocks) return;
+    blend_upload_block(I.W.C, I.W.P, blockIdx.x - I.blendBase, S);
+}
+
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st) {
     if (C.updatedCount == 0) return cudaSuccess;
     const uint32_t blocks = (C.updatedCount + BLEND_PROBES - 1) / BLEND_PROBES;
     k_blend_upload<<<blocks, BLEND_THREADS, 0, st>>>(C, P); note_launch();
     return cudaGetLastError();
 }
+
+cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st) {
+    if (B.n == 0 || B.blendBlocks == 0) return cudaSuccess;
+    k_blend_upload_batch<<<B.blendBlocks, BLEND_THREADS, 0, st>>>(B); note_launch();
+    return cudaGetLastError();
+}
+
+uint32_t blend_blocks(uint32_t updatedCount) { return (updatedCount + BLEND_PROBES - 1) / BLEND_PROBES; }
 
 // lightGridKernel, gi_probes.js:1893-1937. Every operation is separately
 // rounded (no contraction) so the lists match an FP32 evaluation exactly.

@@ -85,8 +85,10 @@ struct sb_ctx {
     float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
     uint32_t jobCap = 0;
     cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
+    cudaEvent_t syncEv = nullptr;  // cross-context ordering of batched solves
     bool timed = false;
     bool singleChunk = true;
+    bool capturing = false;        // enqueueing into a CUDA graph capture: no timing events
 
     // Differentiable solves (sb_forward_record / sb_backward). `epoch` counts
     // changes to anything the shading reads; a tape is only replayed under the
@@ -388,6 +390,7 @@ void sb_destroy(sb_ctx* ctx) {
     for (cudaEvent_t e : {T.evF0, T.evF1, T.evB0, T.evB1})
         if (e) cudaEventDestroy(e);
     release(ctx->dErr); release(ctx->dGate); release(ctx->dWork); release(ctx->dCounters);
+    if (ctx->syncEv) cudaEventDestroy(ctx->syncEv);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->evMid) cudaEventDestroy(ctx->evMid);
     if (ctx->evA) cudaEventDestroy(ctx->evA);
@@ -726,18 +729,153 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     }
     const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
     if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 128, ctx->stream));
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const bool timing = !ctx->capturing;  // events inside a capture would not be re-recorded by replays
+    if (timing) CK(cudaEventRecord(ctx->ev0, ctx->stream));
     ctx->singleChunk = updatedCount <= chunk;
     for (uint32_t s0 = 0; s0 < updatedCount; s0 += chunk) {
         uint32_t n = updatedCount - s0 < chunk ? updatedCount - s0 : chunk;
         CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune,
-                        ctx->stream, ctx->jobs, ctx->jobCap, s0, n, ctx->evA, ctx->evB));
+                        ctx->stream, ctx->jobs, ctx->jobCap, s0, n, timing ? ctx->evA : nullptr,
+                        timing ? ctx->evB : nullptr));
     }
-    CK(cudaEventRecord(ctx->evMid, ctx->stream));
+    if (timing) CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    ctx->timed = true;
+    if (timing) CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    ctx->timed = ctx->timed || timing;
     return SB_OK;
+}
+
+// Host-side preparation a solve of cascade ci needs (validation, derived
+// layouts, light grid, scene BVH and its marks): done before any enqueue.
+static sb_status solve_prepare(sb_ctx* ctx, uint32_t ci) {
+    if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+        return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if (ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "TLAS not built (sb_build_tlas)");
+    if (!ctx->B.lights) return fail(ctx, SB_ERR_NOT_READY, "no lights uploaded (sb_upload_lights, count may be 0)");
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s == SB_OK) s = light_grid_if_needed(ctx);
+    if (s == SB_OK) s = flat_if_needed(ctx);
+    return s;
+}
+
+static cudaError_t ensure_sync_event(sb_ctx* c) {
+    return c->syncEv ? cudaSuccess : cudaEventCreateWithFlags(&c->syncEv, cudaEventDisableTiming);
+}
+
+// One launch per stage over every item (sb_solve_batch); the items' contexts
+// share a device, and the first item's context owns the ray queue, the job
+// queue and the stream the batch runs on.
+static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
+    sb_ctx* lead = items[0].ctx;
+    sb_ctx* ctx = lead;  // error reporting (CK)
+    static thread_local BatchArgs B;
+    std::memset(&B, 0, sizeof B);
+    uint64_t rayBase = 0, jobs = 0;
+    uint32_t blend = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+        sb_ctx* c = items[i].ctx;
+        const uint32_t ci = items[i].cascade;
+        Cascade& K = c->casc[ci];
+        const uint32_t cnt = items[i].updatedCount > K.probeTotal ? K.probeTotal : items[i].updatedCount;
+        BatchItem& I = B.it[i];
+        I.W.S = dev_scene(c);
+        I.W.C = dev_cascade(c, ci, items[i].probeOffset % K.probeTotal, cnt);
+        std::memcpy(&I.W.P, &c->params, sizeof I.W.P);
+        I.W.err = c->dErr;
+        I.W.counters = nullptr;
+        I.W.work = lead->dWork;
+        I.W.slotBegin = 0;
+        I.W.slotCount = cnt;
+        I.W.smemTlas = 0;
+        I.W.order = lead->tune.sortKey == 0 ? 1u : 0u;
+        const uint64_t rays = (uint64_t)cnt * K.grid.raysPerProbe;
+        I.rayBase = (uint32_t)rayBase;
+        I.rays = (uint32_t)rays;
+        rayBase = (rayBase + rays + 31) & ~31ull;
+        I.blendBase = blend;
+        I.blendBlocks = blend_blocks(cnt);
+        blend += I.blendBlocks;
+        jobs += rays * (c->lightCount ? c->lightCount : 1u);
+    }
+    if (rayBase >= (1ull << 26))
+        return fail(lead, SB_ERR_INVALID_ARG, "batch of %llu rays exceeds the 2^26 job tag range",
+                    (unsigned long long)rayBase);
+    if (jobs > kJobCapMax)
+        return fail(lead, SB_ERR_UNSUPPORTED, "batch needs %llu shadow-job slots (max %llu): split it",
+                    (unsigned long long)jobs, (unsigned long long)kJobCapMax);
+    if (jobs > lead->jobCap) {
+        if (lead->capturing) return fail(lead, SB_ERR_NOT_READY, "job queue must grow outside a capture");
+        release(lead->jobs);
+        size_t c = 0;
+        CK(grow(lead->jobs, c, (size_t)jobs * 2));
+        lead->jobCap = (uint32_t)jobs;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        B.it[i].W.jobs = lead->jobs;
+        B.it[i].W.jobCap = lead->jobCap;
+    }
+    B.n = count;
+    B.totalRays = (uint32_t)rayBase;
+    B.blendBlocks = blend;
+    B.work = lead->dWork;
+    B.counters = lead->countersOn ? lead->dCounters : nullptr;
+    // the other contexts' pending work runs before the batch, their later work after it
+    for (uint32_t i = 1; i < count; ++i) {
+        sb_ctx* c = items[i].ctx;
+        if (c->stream == lead->stream) continue;
+        CK(ensure_sync_event(c));
+        CK(cudaEventRecord(c->syncEv, c->stream));
+        CK(cudaStreamWaitEvent(lead->stream, c->syncEv, 0));
+    }
+    const bool timing = !lead->capturing;
+    if (B.counters) CK(cudaMemsetAsync(lead->dCounters, 0, 128, lead->stream));
+    if (timing) CK(cudaEventRecord(lead->ev0, lead->stream));
+    CK(launch_trace_batch(B, lead->tune, lead->stream, timing ? lead->evA : nullptr, timing ? lead->evB : nullptr));
+    if (timing) CK(cudaEventRecord(lead->evMid, lead->stream));
+    CK(launch_blend_upload_batch(B, lead->stream));
+    if (timing) {
+        CK(cudaEventRecord(lead->ev1, lead->stream));
+        lead->timed = true;
+        lead->singleChunk = true;
+    }
+    CK(ensure_sync_event(lead));
+    bool joined = false;
+    for (uint32_t i = 1; i < count; ++i) {
+        sb_ctx* c = items[i].ctx;
+        if (c->stream == lead->stream) continue;
+        if (!joined) CK(cudaEventRecord(lead->syncEv, lead->stream));
+        joined = true;
+        CK(cudaStreamWaitEvent(c->stream, lead->syncEv, 0));
+    }
+    return SB_OK;
+}
+
+static sb_status check_batch(const sb_solve_item* items, uint32_t count) {
+    if (!items || count == 0 || !items[0].ctx) return SB_ERR_INVALID_ARG;
+    sb_ctx* lead = items[0].ctx;
+    if (count > SB_BATCH_MAX) return fail(lead, SB_ERR_INVALID_ARG, "%u items > %u per batch", count, SB_BATCH_MAX);
+    for (uint32_t i = 0; i < count; ++i) {
+        sb_ctx* c = items[i].ctx;
+        if (!c || c->device != lead->device) return fail(lead, SB_ERR_INVALID_ARG, "item %u: null context or another device", i);
+        for (uint32_t j = 0; j < i; ++j)
+            if (items[j].ctx == c && items[j].cascade == items[i].cascade)
+                return fail(lead, SB_ERR_INVALID_ARG, "items %u and %u solve the same cascade", j, i);
+        sb_status s = solve_prepare(c, items[i].cascade);
+        if (s != SB_OK) {
+            if (c != lead) lead->err = "item " + std::to_string(i) + ": " + c->err;
+            return s;
+        }
+    }
+    return SB_OK;
+}
+
+sb_status sb_solve_batch(const sb_solve_item* items, uint32_t count) {
+    sb_status s = check_batch(items, count);
+    if (s != SB_OK) return s;
+    cudaSetDevice(items[0].ctx->device);
+    return enqueue_batch(items, count);
 }
 
 // ---------------------------------------------------------------- adjoint

@@ -125,6 +125,50 @@ struct DevParams {
 };
 static_assert(sizeof(DevParams) == sizeof(sb_params), "DevParams mirrors sb_params");
 
+// One solve of the trace wavefront as its kernels see it.
+struct WaveCtx {
+    DevScene S;
+    DevCascade C;
+    DevParams P;
+    uint32_t* err;
+    unsigned long long* counters;  // [rays, shadowRays, tlasNodes, instances, blasNodes, triTests] or null
+    uint32_t* work;                // [0] primary cursor, [1] shadow cursor, [2] job count
+    float4* jobs;                  // 2 float4 per job: (origin, maxDist), (dir, ray << 6 | light)
+    uint32_t jobCap;
+    uint32_t slotBegin, slotCount; // probe slots of this chunk
+    uint32_t smemTlas;             // TLAS nodes staged in shared memory (0 = read from global)
+    uint32_t order;                // 0 probe-major, 1 direction-major
+};
+
+// Several solves (scenes, cascades) through one launch of each stage: a
+// shared ray index space in which item i owns [rayBase, rayBase + rays), with
+// rayBase a multiple of 32 so a warp's 32 rays never straddle two items, and a
+// shared shadow-job queue whose jobs carry the global ray index. The blend
+// grid is split the same way (blendBase / blendBlocks CTAs per item). Passed
+// by value as a __grid_constant__ kernel parameter and indexed in place.
+constexpr uint32_t SB_BATCH_MAX = 16;
+struct BatchItem {
+    WaveCtx W;                     // W.work / W.jobs / W.jobCap are the batch's shared ones
+    uint32_t rayBase, rays;
+    uint32_t blendBase, blendBlocks;
+};
+struct BatchArgs {
+    BatchItem it[SB_BATCH_MAX];
+    uint32_t n;
+    uint32_t totalRays;            // padded ray index space
+    uint32_t blendBlocks;
+    uint32_t* work;
+    unsigned long long* counters;  // one set for the whole batch, or null
+};
+static_assert(sizeof(BatchArgs) <= 32000, "BatchArgs must fit the kernel parameter space");
+
+__device__ __forceinline__ uint32_t batch_item(const BatchArgs& B, uint32_t g) {
+    uint32_t i = 0;
+#pragma unroll 1
+    while (i + 1 < B.n && g >= B.it[i + 1].rayBase) ++i;
+    return i;
+}
+
 __device__ __forceinline__ void latch(uint32_t* err, uint32_t bit) {
     if (err) atomicOr(err, bit);
 }

@@ -47,6 +47,13 @@ cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStr
 cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t slotCount,
                          cudaStream_t st);
 
+// Batched stages (every item of B in one launch per stage). B.work must hold
+// 3 words; every item's W.jobs / W.jobCap / W.work are the batch's shared ones.
+cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cudaStream_t st,
+                               cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
+cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st);
+uint32_t blend_blocks(uint32_t updatedCount);  // CTAs of the blend for one solve
+
 // Adjoint of shade + blend + upload (sb_adjoint.cu), over every probe of a
 // cascade (probe slot = probe index). Gradient layouts: gE / E per interior
 // texel (36 per probe, probe-major), gH per history texel (64 per probe: rgb,

@@ -3,7 +3,6 @@
 #include "sb_kernels.cuh"
 
 extern "C" {
-sb_status sb_solve_batch(const sb_solve_item*, uint32_t) { return SB_ERR_UNSUPPORTED; }
 sb_status sb_graph_capture_frame(sb_ctx*, uint32_t, uint32_t, uint32_t, const uint32_t*, const uint32_t*, uint32_t,
                                  int32_t) { return SB_ERR_UNSUPPORTED; }
 sb_status sb_graph_launch(sb_ctx*) { return SB_ERR_UNSUPPORTED; }

@@ -29,61 +29,50 @@ namespace sb {
 #define SB_SHADOW_MIN_BLOCKS 4
 #endif
 
-__global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(WaveCtx W) {
-    extern __shared__ uint4 sTlas[];
-    const bool pairs = closest_pairs(W.S);
-    const uint4* tl = stage_tlas(W, sTlas, pairs);
-    if (!*W.S.valid) return;
-    const DevCascade& C = W.C;
-    const uint32_t N = C.rays, total = W.slotCount * N;
-    const uint32_t lane = threadIdx.x & 31u;
-    const bool dirMajor = W.order != 0;
-    Visits vis = {0, 0, 0, 0};
-    uint32_t nRays = 0;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&W.work[0], 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= total) break;
-        const uint32_t g = base + lane;
-        if (g >= total) continue;
-        uint32_t slot, k;
-        ray_of(W, g, dirMajor, slot, k);
-        const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
-        const float3 ro = probe_world_pos(C, probeIndex);
-        const float3 rd = ray_dir(k, N, W.P.frameJitter);
-        float bestT, bu, bv;
-        int tri, inst;
-        trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
-        ++nRays;
-        // raw record (FP32 t, no facing bit): k_emit finishes it
-        uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
-        uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
-        C.hits[slot * N + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(bestT),
-                                                     uq | (vq << 16))
-                                        : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
-    }
-    if (W.counters) {
-        atomicAdd(&W.counters[0], (unsigned long long)nRays);
-        atomicAdd(&W.counters[2], (unsigned long long)vis.tlas);
-        atomicAdd(&W.counters[3], (unsigned long long)vis.inst);
-        atomicAdd(&W.counters[4], (unsigned long long)vis.blas);
-        atomicAdd(&W.counters[5], (unsigned long long)vis.tri);
-    }
+// ---------------------------------------------------------------- bodies
+// Each stage's per-item work is a device function over `const WaveCtx&`; the
+// per-solve kernels pass their parameter, the batched kernels an item of the
+// __grid_constant__ BatchArgs (indexed in the parameter space, warp-uniform).
+
+__device__ __forceinline__ void add_visits(unsigned long long* c, int at, uint32_t rays, const Visits& v) {
+    if (!c) return;
+    if (rays) atomicAdd(&c[0], (unsigned long long)rays);
+    atomicAdd(&c[at], (unsigned long long)v.tlas);
+    atomicAdd(&c[at + 1], (unsigned long long)v.inst);
+    atomicAdd(&c[at + 2], (unsigned long long)v.blas);
+    atomicAdd(&c[at + 3], (unsigned long long)v.tri);
 }
 
-// Stage A2, one thread per probe ray in the issue order of A: the hit
-// parameter re-evaluated in double-float, the hit frame, and the NEE gates of
-// every candidate light. Each lane runs the gates with no warp sync; one warp
-// scan and one atomicAdd then reserve the warp's shadow-ray jobs, and each
-// ray's passing candidates (gates evaluated again: the same pure function) are
-// written together in list order, so a shadow warp mostly holds rays that share
-// an origin.
-__global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
-    if (!*W.S.valid) return;
+// Stage A: the closest hit of one probe ray (item-local issue index g) as a
+// raw record (FP32 t, no facing bit): k_emit finishes it.
+__device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, bool pairs, uint32_t g, Visits& vis) {
     const DevCascade& C = W.C;
-    const uint32_t N = C.rays, total = W.slotCount * N;
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = C.rays;
+    uint32_t slot, k;
+    ray_of(W, g, W.order != 0, slot, k);
+    const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+    const float3 ro = probe_world_pos(C, probeIndex);
+    const float3 rd = ray_dir(k, N, W.P.frameJitter);
+    float bestT, bu, bv;
+    int tri, inst;
+    trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
+    uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
+    uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
+    C.hits[slot * N + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(bestT),
+                                                 uq | (vq << 16))
+                                    : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
+}
+
+// Stage A2, warp-collective (all 32 lanes call it; `active` lanes hold ray g):
+// the hit parameter re-evaluated in double-float, the hit frame, and the NEE
+// gates of every candidate light. Each lane runs the gates with no warp sync;
+// one warp scan and one atomicAdd then reserve the warp's shadow-ray jobs, and
+// each ray's passing candidates (gates evaluated again: the same pure
+// function) are written together in list order, so a shadow warp mostly holds
+// rays that share an origin. Jobs carry tagBase + the ray's record index.
+__device__ __forceinline__ uint32_t emit_ray(const WaveCtx& W, bool active, uint32_t g, uint32_t tagBase) {
+    const DevCascade& C = W.C;
+    const uint32_t N = C.rays;
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t rayIdx = 0;
     int tri = -1;
@@ -93,7 +82,7 @@ __global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
     fr.faceFwd = true;
     fr.traceBias = 0.f;
     uint4 h = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u);
-    if (g < total) {
+    if (active) {
         uint32_t slot, k;
         ray_of(W, g, W.order != 0, slot, k);
         rayIdx = slot * N + k;
@@ -128,6 +117,7 @@ __global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
         jb = __shfl_sync(0xFFFFFFFFu, jb, 0);
     }
     uint32_t j = jb + incl - mine, tested0 = 0u, tested1 = 0u, nJobs = 0;
+    const uint32_t tag = (tagBase + rayIdx) << 6;
     while (pass) {
         const uint32_t i = (uint32_t)(__ffsll((long long)pass) - 1);
         pass &= pass - 1ull;
@@ -135,7 +125,7 @@ __global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
         const LightEval e = light_eval(W, li, fr.hitPos, fr.ng);
         if (j < W.jobCap) {
             W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, e.dist - fr.traceBias);
-            W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float((rayIdx << 6) | li));
+            W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float(tag | li));
             if (li < 32) tested0 |= 1u << li;
             else tested1 |= 1u << (li - 32);
             ++nJobs;
@@ -144,55 +134,29 @@ __global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
         }
         ++j;
     }
-    if (g < total) {
+    if (active) {
         if (tri >= 0) C.hits[rayIdx] = h;
         C.vis[rayIdx] = make_uint4(tested0, tested1, tested0, tested1);
     }
-    if (W.counters) {
-        const uint32_t warpDone = __reduce_add_sync(0xFFFFFFFFu, nJobs);
-        if (lane == 0 && warpDone) atomicAdd(&W.counters[1], (unsigned long long)warpDone);
+    return nJobs;
+}
+
+// Stage B: one shadow job; a blocked light is cleared from the ray's mask.
+__device__ __forceinline__ void shadow_job(const WaveCtx& W, const uint4* tl, bool pairs, float4 a, float4 b,
+                                           uint32_t rayIdx, Visits& vis) {
+    if (trace_any(W.S, tl, xyz(a), xyz(b), a.w, vis, W.err, pairs)) {
+        const uint32_t li = __float_as_uint(b.w) & 63u;
+        uint4* v = W.C.vis + rayIdx;
+        if (li < 32) atomicAnd(&v->z, ~(1u << li));
+        else atomicAnd(&v->w, ~(1u << (li - 32)));
     }
 }
 
-__global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(WaveCtx W) {
-    extern __shared__ uint4 sTlas[];
-    const bool pairs = any_pairs(W.S);
-    const uint4* tl = stage_tlas(W, sTlas, pairs);
-    if (!*W.S.valid) return;
-    const uint32_t total = min(*(volatile uint32_t*)&W.work[2], W.jobCap);
-    const uint32_t lane = threadIdx.x & 31u;
-    Visits vis = {0, 0, 0, 0};
-    for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&W.work[1], 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= total) break;
-        uint32_t j = base + lane;
-        if (j >= total) continue;
-        float4 a = W.jobs[2 * j], b = W.jobs[2 * j + 1];
-        if (trace_any(W.S, tl, xyz(a), xyz(b), a.w, vis, W.err, pairs)) {
-            uint32_t packed = __float_as_uint(b.w);
-            uint32_t ray = packed >> 6, li = packed & 63u;
-            uint4* v = W.C.vis + ray;
-            if (li < 32) atomicAnd(&v->z, ~(1u << li));
-            else atomicAnd(&v->w, ~(1u << (li - 32)));
-        }
-    }
-    if (W.counters) {
-        atomicAdd(&W.counters[6], (unsigned long long)vis.tlas);
-        atomicAdd(&W.counters[7], (unsigned long long)vis.inst);
-        atomicAdd(&W.counters[8], (unsigned long long)vis.blas);
-        atomicAdd(&W.counters[9], (unsigned long long)vis.tri);
-    }
-}
-
-
-__global__ void __launch_bounds__(128) k_shade(WaveCtx W) {
-    if (!*W.S.valid) return;
+// Stage C: emissive + unblocked NEE terms + bounce, or the sky, of one ray
+// (item-local probe-major index g).
+__device__ __forceinline__ void shade_ray(const WaveCtx& W, uint32_t g) {
     const DevCascade& C = W.C;
     const uint32_t N = C.rays;
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= W.slotCount * N) return;
     uint32_t slot, k;
     ray_of(W, g, false, slot, k);
     const uint32_t rayIdx = slot * N + k;
@@ -231,6 +195,69 @@ __global__ void __launch_bounds__(128) k_shade(WaveCtx W) {
         outRgb = sky_sh(W.P, rd);
     }
     C.rayData[rayIdx] = make_float4(outRgb.x, outRgb.y, outRgb.z, hitT);
+}
+
+// ---------------------------------------------------------------- per solve
+
+__global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(WaveCtx W) {
+    extern __shared__ uint4 sTlas[];
+    const bool pairs = closest_pairs(W.S);
+    const uint4* tl = stage_tlas(W, sTlas, pairs);
+    if (!*W.S.valid) return;
+    const uint32_t total = W.slotCount * W.C.rays;
+    const uint32_t lane = threadIdx.x & 31u;
+    Visits vis = {0, 0, 0, 0};
+    uint32_t nRays = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&W.work[0], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= total) break;
+        const uint32_t g = base + lane;
+        if (g >= total) continue;
+        primary_ray(W, tl, pairs, g, vis);
+        ++nRays;
+    }
+    add_visits(W.counters, 2, nRays, vis);
+}
+
+__global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
+    if (!*W.S.valid) return;
+    const uint32_t total = W.slotCount * W.C.rays;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t nJobs = emit_ray(W, g < total, g, 0u);
+    if (W.counters) {
+        const uint32_t warpDone = __reduce_add_sync(0xFFFFFFFFu, nJobs);
+        if ((threadIdx.x & 31u) == 0 && warpDone) atomicAdd(&W.counters[1], (unsigned long long)warpDone);
+    }
+}
+
+__global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(WaveCtx W) {
+    extern __shared__ uint4 sTlas[];
+    const bool pairs = any_pairs(W.S);
+    const uint4* tl = stage_tlas(W, sTlas, pairs);
+    if (!*W.S.valid) return;
+    const uint32_t total = min(*(volatile uint32_t*)&W.work[2], W.jobCap);
+    const uint32_t lane = threadIdx.x & 31u;
+    Visits vis = {0, 0, 0, 0};
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&W.work[1], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= total) break;
+        uint32_t j = base + lane;
+        if (j >= total) continue;
+        const float4 a = W.jobs[2 * j], b = W.jobs[2 * j + 1];
+        shadow_job(W, tl, pairs, a, b, __float_as_uint(b.w) >> 6, vis);
+    }
+    add_visits(W.counters, 6, 0u, vis);
+}
+
+__global__ void __launch_bounds__(128) k_shade(WaveCtx W) {
+    if (!*W.S.valid) return;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= W.slotCount * W.C.rays) return;
+    shade_ray(W, g);
 }
 
 // Stage C alone over probe slots [0, slotCount) from the records already in
@@ -299,6 +326,94 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     note_launch();
     if (afterShadow) cudaEventRecord(afterShadow, st);
     k_shade<<<(rays + 127) / 128, 128, 0, st>>>(W);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- batched
+// The same four stages over every item of a BatchArgs: one launch per stage
+// for all scenes and cascades, one shared ray index space and job queue.
+
+__global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary_batch(const __grid_constant__ BatchArgs B) {
+    const uint32_t lane = threadIdx.x & 31u;
+    Visits vis = {0, 0, 0, 0};
+    uint32_t nRays = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&B.work[0], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= B.totalRays) break;
+        const BatchItem& I = B.it[batch_item(B, base)];
+        const uint32_t g = base + lane - I.rayBase;
+        if (g >= I.rays || !*I.W.S.valid) continue;
+        const bool pairs = closest_pairs(I.W.S);
+        primary_ray(I.W, pairs ? I.W.S.tlasPairs : I.W.S.tlas, pairs, g, vis);
+        ++nRays;
+    }
+    add_visits(B.counters, 2, nRays, vis);
+}
+
+__global__ void __launch_bounds__(128) k_emit_batch(const __grid_constant__ BatchArgs B) {
+    const uint32_t gg = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gg - (threadIdx.x & 31u) >= B.totalRays) return;  // whole warps only
+    const BatchItem& I = B.it[batch_item(B, gg & ~31u)];
+    if (!*I.W.S.valid) return;
+    const uint32_t g = gg - I.rayBase;
+    const uint32_t nJobs = emit_ray(I.W, g < I.rays, g, I.rayBase);
+    if (B.counters) {
+        const uint32_t warpDone = __reduce_add_sync(0xFFFFFFFFu, nJobs);
+        if ((threadIdx.x & 31u) == 0 && warpDone) atomicAdd(&B.counters[1], (unsigned long long)warpDone);
+    }
+}
+
+__global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow_batch(const __grid_constant__ BatchArgs B) {
+    const BatchItem& I0 = B.it[0];
+    const uint32_t total = min(*(volatile uint32_t*)&B.work[2], I0.W.jobCap);
+    const uint32_t lane = threadIdx.x & 31u;
+    Visits vis = {0, 0, 0, 0};
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&B.work[1], 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= total) break;
+        uint32_t j = base + lane;
+        if (j >= total) continue;
+        const float4 a = I0.W.jobs[2 * j], b = I0.W.jobs[2 * j + 1];
+        const uint32_t ray = __float_as_uint(b.w) >> 6;
+        const BatchItem& I = B.it[batch_item(B, ray)];
+        const bool pairs = any_pairs(I.W.S);
+        shadow_job(I.W, pairs ? I.W.S.tlasPairs : I.W.S.tlas, pairs, a, b, ray - I.rayBase, vis);
+    }
+    add_visits(B.counters, 6, 0u, vis);
+}
+
+__global__ void __launch_bounds__(128) k_shade_batch(const __grid_constant__ BatchArgs B) {
+    const uint32_t gg = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gg >= B.totalRays) return;
+    const BatchItem& I = B.it[batch_item(B, gg & ~31u)];
+    const uint32_t g = gg - I.rayBase;
+    if (g >= I.rays || !*I.W.S.valid) return;
+    shade_ray(I.W, g);
+}
+
+cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cudaStream_t st,
+                               cudaEvent_t afterPrimary, cudaEvent_t afterShadow) {
+    if (B.n == 0 || B.totalRays == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(B.work, 0, 3 * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const int block = (int)tune.block;
+    const uint32_t rays = B.totalRays;
+    k_trace_primary_batch<<<persistent_grid((const void*)k_trace_primary_batch, block, 0, tune, rays), block, 0,
+                            st>>>(B);
+    note_launch();
+    k_emit_batch<<<(rays + 127) / 128, 128, 0, st>>>(B);
+    note_launch();
+    if (afterPrimary) cudaEventRecord(afterPrimary, st);
+    k_trace_shadow_batch<<<persistent_grid((const void*)k_trace_shadow_batch, block, 0, tune, rays * 4u), block, 0,
+                           st>>>(B);
+    note_launch();
+    if (afterShadow) cudaEventRecord(afterShadow, st);
+    k_shade_batch<<<(rays + 127) / 128, 128, 0, st>>>(B);
     note_launch();
     return cudaGetLastError();
 }

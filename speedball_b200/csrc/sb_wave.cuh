@@ -6,20 +6,6 @@
 
 namespace sb {
 
-struct WaveCtx {
-    DevScene S;
-    DevCascade C;
-    DevParams P;
-    uint32_t* err;
-    unsigned long long* counters;  // [rays, shadowRays, tlasNodes, instances, blasNodes, triTests] or null
-    uint32_t* work;                // [0] primary cursor, [1] shadow cursor, [2] job count
-    float4* jobs;                  // 2 float4 per job: (origin, maxDist), (dir, ray << 6 | light)
-    uint32_t jobCap;
-    uint32_t slotBegin, slotCount; // probe slots of this chunk
-    uint32_t smemTlas;             // TLAS nodes staged in shared memory (0 = read from global)
-    uint32_t order;                // 0 probe-major, 1 direction-major
-};
-
 // The TLAS the walk reads (child pairs when `pairs`, else the 32-byte nodes),
 // staged in shared memory when it fits.
 __device__ __forceinline__ const uint4* stage_tlas(const WaveCtx& W, uint4* sTlas, bool pairs) {

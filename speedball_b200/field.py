@@ -127,6 +127,7 @@ class ProbeField:
         self._pendingTopology = False
         self._deformVersions = {}
         self._staging = {}
+        self._cascades = {}  # extra cascade boxes (ci >= 1) configured by configureCascade
         self._params = _abi.default_params()
         self._params.hysteresis = self._hysteresis
         self._frameJitterOverride = None
@@ -225,6 +226,16 @@ class ProbeField:
         """One tick: dirty lanes, then one solve of C0 (gi_probes.js:3472-3849)."""
         if self._disposed:
             return {}
+        frame = self.beginTick(nowMs)
+        self._ck(self._lib.sb_solve(self._ctx, frame["cascade"], frame["probeOffset"], frame["updatedCount"]))
+        self.endTick(frame, nowMs)
+        return frame
+
+    def beginTick(self, nowMs: float | None = None) -> dict:
+        """The part of a tick ahead of its solve: dirty lanes, the solve's probe
+        range and its uniforms (jitter epoch, hysteresis exponent). A batched
+        frame (speedball_b200.batch) solves several fields' ranges in one launch
+        between beginTick and endTick."""
         lib = self._lib
         if self._pendingTopology:
             self._pendingTopology = False
@@ -246,13 +257,35 @@ class ProbeField:
         elif self._frameJitterOverride is not None:
             self._params.frameJitter = self._frameJitterOverride
         self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
-        offset = self._probeCursor
-        self._ck(lib.sb_solve(self._ctx, C0, offset, updated))
+        return {"cascade": C0, "probeOffset": self._probeCursor, "updatedCount": updated}
+
+    def endTick(self, frame: dict, nowMs: float | None = None) -> None:
+        updated = frame["updatedCount"]
         self._probeCursor = (self._probeCursor + updated) % self._probeTotal if self._probeTotal else 0
         if nowMs is not None:
             self._lastSolveAt = nowMs
         self.stats["solves"] += 1
-        return {"cascade": C0, "probeOffset": offset, "updatedCount": updated}
+
+    def configureCascade(self, ci: int, gridMin, gridSize, res, rays: int | None = None) -> None:
+        """An extra cascade box of this field (ci >= 1), solved through
+        speedball_b200.batch or sb_solve directly; cascade 0 stays the fitted one."""
+        if ci < 1:
+            raise ValueError("cascade 0 is the field's fitted grid")
+        g = _abi.sb_grid()
+        for a in range(3):
+            g.gridMin[a] = float(gridMin[a])
+            g.gridSize[a] = float(gridSize[a])
+            g.res[a] = int(res[a])
+        g.raysPerProbe = int(rays or self._rays)
+        gs = np.array([g.gridSize[a] for a in range(3)], np.float64)
+        g.maxDist = float(np.linalg.norm(gs))
+        g.cellMin = float(max(1e-4, min(gs[a] / max(1, g.res[a] - 1) for a in range(3))))
+        self._ck(self._lib.sb_configure_cascade(self._ctx, ci, C.byref(g)))
+        self._cascades[ci] = g
+
+    def cascadeProbes(self, ci: int) -> int:
+        g = self._grid if ci == 0 else self._cascades[ci]
+        return int(g.res[0] * g.res[1] * g.res[2])
 
     def _refresh_lanes(self):
         lib = self._lib

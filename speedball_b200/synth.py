@@ -300,3 +300,35 @@ def atrium_motion(scene: SceneDesc, frame: int, seed: int = 7):
     Pn = P.copy()
     Pn[:, 1] += offs
     return mats, Pn.astype(np.float32)
+
+
+BATCH_SCENE_TRIS = (20_000, 45_000, 80_000, 120_000, 200_000, 262_000, 350_000, 500_000)
+
+
+def batch_scenes(seed: int = 2, sizes=BATCH_SCENE_TRIS):
+    """The batched workload's independent scenes: atria built like the 262k one
+    with uneven triangle counts, each with its own cubic probe grid of 8^3 to
+    16^3 probes at 32 to 128 rays per probe (multiples of 16) drawn from the
+    seed, montecarlo jitter."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i, n in enumerate(sizes):
+        s = atrium(seed=100 + i, total_tris=int(n))
+        r = int(rng.integers(8, 17))
+        rays = int(rng.choice(np.arange(32, 129, 16)))
+        s.meta["grid"] = dict(s.meta["grid"], res=(r, r, r), rays=rays)
+        s.meta["jitter"] = "montecarlo"
+        s.name = f"atrium_{n}"
+        out.append(s)
+    return out
+
+
+def nested_cascades(grid: dict, res=((16, 16, 16), (12, 12, 12), (8, 8, 8)), scale: float = 2.0):
+    """Cascade boxes sharing a centre, each `scale` times the previous extent."""
+    c = np.asarray(grid["gridMin"], np.float64) + 0.5 * np.asarray(grid["gridSize"], np.float64)
+    size = np.asarray(grid["gridSize"], np.float64)
+    out = []
+    for i, r in enumerate(res):
+        s = size * scale ** i
+        out.append(dict(gridMin=tuple(c - 0.5 * s), gridSize=tuple(s), res=tuple(r), rays=grid["rays"]))
+    return out
