@@ -322,13 +322,42 @@ sb_status sb_backward(sb_ctx* ctx, sb_grads* grads);
 
 /* -------------------------------------------------- graphs and autotuning */
 
-/* Capture the per-frame chain (refit -> TLAS refit -> solve) of this context as
- * one CUDA graph and replay it; sb_graph_launch re-runs the captured frame. */
+/* The device-side motion lane of one context in a captured frame: BLAS
+ * refits of the given node ranges (the deform lane after its vertices are in
+ * place), then, with refitTlas, instance bounds from the BLAS roots and the
+ * TLAS refit (sb_update_transforms(ctx, NULL, NULL, 0)). */
+typedef struct sb_frame_lane {
+    sb_ctx* ctx;
+    const uint32_t* refitRoots;
+    const uint32_t* refitEnds;
+    uint32_t refitCount;
+    int32_t refitTlas;
+} sb_frame_lane;
+
+/* Capture the per-frame chain refit -> TLAS refit -> trace -> shade -> blend
+ * of several contexts as one CUDA graph owned by items[0].ctx: every lane a
+ * parallel branch, joined ahead of one batched solve of `items` (the kernels
+ * of sb_solve_batch). The call runs the frame once as ordinary launches (that
+ * run applies host-side effects such as layout checks and queue growth) and
+ * captures it; it does not replay it. Synchronizes. */
+sb_status sb_graph_capture_batch(const sb_frame_lane* lanes, uint32_t laneCount,
+                                 const sb_solve_item* items, uint32_t itemCount);
+/* The single-context form: lane (ctx, refit ranges, refitTlas) and one solve. */
 sb_status sb_graph_capture_frame(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset,
                                  uint32_t updatedCount, const uint32_t* refitRoots,
                                  const uint32_t* refitEnds, uint32_t refitCount,
                                  int32_t refitTlas);
+/* Replay the frame captured by this context: one cudaGraphLaunch on its
+ * stream, after the other member contexts' pending work. Each replay takes the
+ * members' current parameters (sb_set_params: jitter, hysteresis, ...),
+ * lights, materials and scene-BVH marks. When a member's buffers or layouts
+ * changed since the capture (scene / range uploads that repack, instances,
+ * TLAS build, cascade configuration, tuning) the frame runs as ordinary
+ * launches and is captured again. Member contexts must outlive the graph.
+ * sb_get_stats' lastSolveMs then covers the whole frame. Enqueue only. */
 sb_status sb_graph_launch(sb_ctx* ctx);
+/* Free the captured frame (also done by sb_destroy of the owner). */
+sb_status sb_graph_destroy(sb_ctx* ctx);
 
 typedef struct sb_tuning {
     uint32_t traceBlock;      /* threads per block of the trace kernels            */

@@ -100,6 +100,11 @@ class sb_solve_item(C.Structure):
                 ("updatedCount", C.c_uint32)]
 
 
+class sb_frame_lane(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("refitRoots", C.c_void_p), ("refitEnds", C.c_void_p),
+                ("refitCount", C.c_uint32), ("refitTlas", C.c_int32)]
+
+
 class sb_grads(C.Structure):
     _fields_ = [("dAlbedo", C.c_void_p), ("dEmissive", C.c_void_p), ("dIntensity", C.c_void_p)]
 
@@ -153,6 +158,8 @@ SIGNATURES = {
     "sb_backward": (C.c_int, [_P, C.POINTER(sb_grads)]),
     "sb_graph_capture_frame": (C.c_int, [_P, _U32, _U32, _U32, _P, _P, _U32, C.c_int32]),
     "sb_graph_launch": (C.c_int, [_P]),
+    "sb_graph_capture_batch": (C.c_int, [C.POINTER(sb_frame_lane), _U32, C.POINTER(sb_solve_item), _U32]),
+    "sb_graph_destroy": (C.c_int, [_P]),
     "sb_get_tuning": (C.c_int, [_P, C.POINTER(sb_tuning)]),
     "sb_set_tuning": (C.c_int, [_P, C.POINTER(sb_tuning)]),
     "sb_autotune": (C.c_int, [_P, _U32, C.POINTER(sb_tuning)]),

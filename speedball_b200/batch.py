@@ -77,3 +77,68 @@ class BatchedFrame:
         """Put every field on one CUDA stream (an int handle)."""
         for f in self.fields:
             _abi.check(f._lib.sb_set_stream(f.ctx, C.c_void_p(int(stream))), f.ctx)
+
+
+@dataclass
+class Lane:
+    """A field's device-side motion lane in a captured frame."""
+    field: ProbeField
+    refits: list          # [(root, end)] BLAS node ranges refit every frame
+    refitTlas: bool = True
+
+
+class GraphFrame:
+    """A BatchedFrame whose per-frame chain (every lane's refits and TLAS
+    refit, then the batched solve) is one CUDA graph (sb_graph_capture_batch,
+    sb_graph_launch). Each launch takes the fields' current uniforms (jitter
+    epoch, hysteresis exponent); a changed probe range captures again."""
+
+    def __init__(self, frame: BatchedFrame, lanes):
+        self.frame = frame
+        self.lanes = list(lanes)
+        self._captured = None
+        self._keep = []
+
+    def _capture(self, items) -> None:
+        lanes = (_abi.sb_frame_lane * max(1, len(self.lanes)))()
+        self._keep = []
+        for i, l in enumerate(self.lanes):
+            roots = (C.c_uint32 * max(1, len(l.refits)))(*[r for r, _ in l.refits])
+            ends = (C.c_uint32 * max(1, len(l.refits)))(*[e for _, e in l.refits])
+            self._keep += [roots, ends]
+            lanes[i].ctx = l.field.ctx
+            lanes[i].refitRoots = C.cast(roots, C.c_void_p)
+            lanes[i].refitEnds = C.cast(ends, C.c_void_p)
+            lanes[i].refitCount = len(l.refits)
+            lanes[i].refitTlas = 1 if l.refitTlas else 0
+        arr = (_abi.sb_solve_item * len(items))()
+        for i, it in enumerate(items):
+            arr[i].ctx = it.field.ctx
+            arr[i].cascade = it.cascade
+            arr[i].probeOffset = it.probeOffset
+            arr[i].updatedCount = it.updatedCount
+        lead = items[0].field
+        _abi.check(lead._lib.sb_graph_capture_batch(lanes, len(self.lanes), arr, len(items)), lead.ctx)
+        self._captured = [(it.field.ctx, it.cascade, it.probeOffset, it.updatedCount) for it in items]
+
+    def tick(self) -> list:
+        """One frame: captured (and run) the first time or when a probe range
+        changed, replayed otherwise."""
+        fr = self.frame
+        frames = [f.beginTick() for f in fr.fields]
+        items = fr.items(frames)
+        key = [(it.field.ctx, it.cascade, it.probeOffset, it.updatedCount) for it in items]
+        if key != self._captured:
+            self._capture(items)
+        else:
+            lead = items[0].field
+            _abi.check(lead._lib.sb_graph_launch(lead.ctx), lead.ctx)
+        for f, x in zip(fr.fields, frames):
+            f.endTick(x)
+        return frames
+
+    def dispose(self) -> None:
+        if self._captured:
+            lead = self.frame.fields[0]
+            lead._lib.sb_graph_destroy(lead.ctx)
+        self._captured = None

@@ -248,6 +248,8 @@ cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStr
     return cudaGetLastError();
 }
 
+const void* blend_batch_kernel() { return (const void*)k_blend_upload_batch; }
+
 cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st) {
     if (B.n == 0 || B.blendBlocks == 0) return cudaSuccess;
     k_blend_upload_batch<<<B.blendBlocks, BLEND_THREADS, 0, st>>>(B); note_launch();

@@ -87,8 +87,33 @@ struct sb_ctx {
     cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
     cudaEvent_t syncEv = nullptr;  // cross-context ordering of batched solves
     bool timed = false;
+    bool lastWasGraph = false;     // ev0..ev1 bracket a graph launch (whole frame, no stage events)
     bool singleChunk = true;
     bool capturing = false;        // enqueueing into a CUDA graph capture: no timing events
+
+    // Buffers, layouts and configuration a captured graph refers to: bumped by
+    // every call that may reallocate or re-lay them out.
+    uint64_t structGen = 1;
+    // The per-frame CUDA graph this context owns (sb_graph_capture_*).
+    struct Graph {
+        struct Lane {
+            sb_ctx* ctx;
+            std::vector<uint32_t> roots, ends;
+            int32_t refitTlas;
+        };
+        std::vector<Lane> lanes;
+        std::vector<sb_solve_item> items;
+        std::vector<std::pair<sb_ctx*, std::pair<uint64_t, uint32_t>>> keys;  // (structGen, packEpoch) per context
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t nodes[5] = {};        // the batched kernels, in stage order
+        cudaKernelNodeParams params[5] = {};
+        std::vector<cudaStream_t> branches;   // one per lane while capturing
+        std::vector<cudaEvent_t> joins;
+        cudaEvent_t fork = nullptr;
+        uint32_t kernelNodes = 0;             // kernels one replay launches
+        bool timed = false;
+    } graph;
 
     // Differentiable solves (sb_forward_record / sb_backward). `epoch` counts
     // changes to anything the shading reads; a tape is only replayed under the
@@ -229,6 +254,7 @@ DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint3
 
 sb_status pack_if_needed(sb_ctx* ctx) {
     if (!ctx->needPack) return SB_OK;
+    if (ctx->capturing) return fail(ctx, SB_ERR_NOT_READY, "a re-pack cannot run inside a graph capture");
     ++ctx->packEpoch;  // cached refit verdicts refer to the old layout
     uint32_t one = 1u;
     CK(cudaMemcpyAsync(ctx->B.valid, &one, 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -383,6 +409,12 @@ void sb_destroy(sb_ctx* ctx) {
         release(K.vis);
     }
     release(ctx->jobs);
+    auto& G = ctx->graph;
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.graph) cudaGraphDestroy(G.graph);
+    for (cudaStream_t s : G.branches) cudaStreamDestroy(s);
+    for (cudaEvent_t e : G.joins) cudaEventDestroy(e);
+    if (G.fork) cudaEventDestroy(G.fork);
     auto& T = ctx->tape;
     release(T.hits); release(T.vis); release(T.hist); release(T.atlas); release(T.E); release(T.gE);
     release(T.target); release(T.shaded); release(T.gR); release(T.gH); release(T.gA); release(T.gParam);
@@ -499,6 +531,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     ctx->sceneLoaded = true;
     ctx->flat.dirty = true;
     ++ctx->epoch;
+    ++ctx->structGen;
     if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
     // validation + derived layouts; a pending TLAS is packed by sb_build_tlas
     uint32_t one = 1u;
@@ -550,6 +583,7 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
     CK(cudaMemcpyAsync((char*)dst + (size_t)start * esz, src, (size_t)count * esz, cudaMemcpyHostToDevice, ctx->stream));
     ++ctx->epoch;
     if (buf <= SB_BUF_MATERIALS && !(buf == SB_BUF_MATERIALS && shading_only(B, start, count))) {
+        ++ctx->structGen;
         ctx->needPack = true;
         ctx->flat.dirty = true;
     }
@@ -675,6 +709,7 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
     K.atlasH = g->res[1] * g->res[2] * 8;
     K.configured = true;
     ++ctx->epoch;
+    ++ctx->structGen;
     if (!sameDims) {
         DevCascade D = dev_cascade(ctx, ci, 0, 0);
         CK(launch_clear_cascade(D, ctx->stream));
@@ -742,6 +777,7 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     CK(launch_blend_upload(D, P, ctx->stream));
     if (timing) CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->timed = ctx->timed || timing;
+    if (timing) ctx->lastWasGraph = false;
     return SB_OK;
 }
 
@@ -764,13 +800,11 @@ static cudaError_t ensure_sync_event(sb_ctx* c) {
     return c->syncEv ? cudaSuccess : cudaEventCreateWithFlags(&c->syncEv, cudaEventDisableTiming);
 }
 
-// One launch per stage over every item (sb_solve_batch); the items' contexts
-// share a device, and the first item's context owns the ray queue, the job
-// queue and the stream the batch runs on.
-static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
+// The kernel arguments of a batch from the items' current state (scenes,
+// cascades, parameters); grows the lead context's job queue when allowed.
+static sb_status build_batch(const sb_solve_item* items, uint32_t count, BatchArgs& B, bool mayGrow) {
     sb_ctx* lead = items[0].ctx;
     sb_ctx* ctx = lead;  // error reporting (CK)
-    static thread_local BatchArgs B;
     std::memset(&B, 0, sizeof B);
     uint64_t rayBase = 0, jobs = 0;
     uint32_t blend = 0;
@@ -806,7 +840,7 @@ static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
         return fail(lead, SB_ERR_UNSUPPORTED, "batch needs %llu shadow-job slots (max %llu): split it",
                     (unsigned long long)jobs, (unsigned long long)kJobCapMax);
     if (jobs > lead->jobCap) {
-        if (lead->capturing) return fail(lead, SB_ERR_NOT_READY, "job queue must grow outside a capture");
+        if (!mayGrow) return fail(lead, SB_ERR_NOT_READY, "the batch's job queue must grow outside a graph");
         release(lead->jobs);
         size_t c = 0;
         CK(grow(lead->jobs, c, (size_t)jobs * 2));
@@ -821,14 +855,44 @@ static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
     B.blendBlocks = blend;
     B.work = lead->dWork;
     B.counters = lead->countersOn ? lead->dCounters : nullptr;
-    // the other contexts' pending work runs before the batch, their later work after it
+    return SB_OK;
+}
+
+// Cross-context ordering around work on the lead's stream: `before` makes the
+// lead wait for the other contexts' pending work, else the others wait for
+// the lead's.
+static sb_status join_streams(const sb_solve_item* items, uint32_t count, bool before) {
+    sb_ctx* lead = items[0].ctx;
+    sb_ctx* ctx = lead;
+    bool recorded = false;
     for (uint32_t i = 1; i < count; ++i) {
         sb_ctx* c = items[i].ctx;
         if (c->stream == lead->stream) continue;
-        CK(ensure_sync_event(c));
-        CK(cudaEventRecord(c->syncEv, c->stream));
-        CK(cudaStreamWaitEvent(lead->stream, c->syncEv, 0));
+        if (before) {
+            CK(ensure_sync_event(c));
+            CK(cudaEventRecord(c->syncEv, c->stream));
+            CK(cudaStreamWaitEvent(lead->stream, c->syncEv, 0));
+        } else {
+            CK(ensure_sync_event(lead));
+            if (!recorded) CK(cudaEventRecord(lead->syncEv, lead->stream));
+            recorded = true;
+            CK(cudaStreamWaitEvent(c->stream, lead->syncEv, 0));
+        }
     }
+    return SB_OK;
+}
+
+// One launch per stage over every item (sb_solve_batch); the items' contexts
+// share a device, and the first item's context owns the ray queue, the job
+// queue and the stream the batch runs on.
+static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
+    sb_ctx* lead = items[0].ctx;
+    sb_ctx* ctx = lead;  // error reporting (CK)
+    static thread_local BatchArgs B;
+    sb_status s = build_batch(items, count, B, !lead->capturing);
+    if (s != SB_OK) return s;
+    // inside a capture the graph's launch does the joins
+    if (!lead->capturing && (s = join_streams(items, count, true)) != SB_OK) return s;
     const bool timing = !lead->capturing;
     if (B.counters) CK(cudaMemsetAsync(lead->dCounters, 0, 128, lead->stream));
     if (timing) CK(cudaEventRecord(lead->ev0, lead->stream));
@@ -839,16 +903,9 @@ static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
         CK(cudaEventRecord(lead->ev1, lead->stream));
         lead->timed = true;
         lead->singleChunk = true;
+        lead->lastWasGraph = false;
     }
-    CK(ensure_sync_event(lead));
-    bool joined = false;
-    for (uint32_t i = 1; i < count; ++i) {
-        sb_ctx* c = items[i].ctx;
-        if (c->stream == lead->stream) continue;
-        if (!joined) CK(cudaEventRecord(lead->syncEv, lead->stream));
-        joined = true;
-        CK(cudaStreamWaitEvent(c->stream, lead->syncEv, 0));
-    }
+    if (!lead->capturing) return join_streams(items, count, false);
     return SB_OK;
 }
 
@@ -876,6 +933,232 @@ sb_status sb_solve_batch(const sb_solve_item* items, uint32_t count) {
     if (s != SB_OK) return s;
     cudaSetDevice(items[0].ctx->device);
     return enqueue_batch(items, count);
+}
+
+// ---------------------------------------------------------------- graphs
+
+static void graph_release(sb_ctx* ctx) {
+    auto& G = ctx->graph;
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.graph) cudaGraphDestroy(G.graph);
+    G.exec = nullptr;
+    G.graph = nullptr;
+    G.lanes.clear();
+    G.items.clear();
+    G.keys.clear();
+}
+
+static void graph_free_streams(sb_ctx* ctx) {
+    auto& G = ctx->graph;
+    for (cudaStream_t s : G.branches) cudaStreamDestroy(s);
+    for (cudaEvent_t e : G.joins) cudaEventDestroy(e);
+    if (G.fork) cudaEventDestroy(G.fork);
+    G.branches.clear();
+    G.joins.clear();
+    G.fork = nullptr;
+}
+
+// Every context a frame touches, once.
+static std::vector<sb_ctx*> frame_contexts(const std::vector<sb_ctx::Graph::Lane>& lanes,
+                                           const std::vector<sb_solve_item>& items) {
+    std::vector<sb_ctx*> out;
+    auto add = [&](sb_ctx* c) {
+        for (sb_ctx* o : out)
+            if (o == c) return;
+        out.push_back(c);
+    };
+    for (const auto& it : items) add(it.ctx);
+    for (const auto& l : lanes) add(l.ctx);
+    return out;
+}
+
+static sb_status run_lane(const sb_ctx::Graph::Lane& l) {
+    for (size_t r = 0; r < l.roots.size(); ++r) {
+        sb_status s = sb_refit_blas(l.ctx, l.roots[r], l.ends[r]);
+        if (s != SB_OK) return s;
+    }
+    return l.refitTlas ? sb_update_transforms(l.ctx, nullptr, nullptr, 0) : SB_OK;
+}
+
+// Runs the frame once as ordinary launches (it applies the host-side effects:
+// packs, refit layout checks, moved-slot marks, queue growth), then captures
+// it: each lane a branch forked from the owner's stream, joined ahead of the
+// batched solve. The batched kernels' nodes are kept so replays refresh their
+// parameters.
+static sb_status graph_capture(sb_ctx* lead, std::vector<sb_ctx::Graph::Lane> lanes,
+                               std::vector<sb_solve_item> items) {
+    sb_ctx* ctx = lead;
+    const std::vector<sb_ctx*> all = frame_contexts(lanes, items);
+    for (const auto& l : lanes) {
+        sb_status s = run_lane(l);
+        if (s != SB_OK) return s;
+    }
+    sb_status s = sb_solve_batch(items.data(), (uint32_t)items.size());
+    if (s != SB_OK) return s;
+    for (sb_ctx* c : all)
+        if ((s = sb_synchronize(c)) != SB_OK) return s;
+    graph_release(lead);
+    auto& G = lead->graph;
+    while (G.branches.size() < lanes.size()) {
+        cudaStream_t st;
+        cudaEvent_t ev;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        G.branches.push_back(st);
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        G.joins.push_back(ev);
+    }
+    if (!G.fork) CK(cudaEventCreateWithFlags(&G.fork, cudaEventDisableTiming));
+    for (sb_ctx* c : all) c->capturing = true;
+    cudaError_t e = cudaStreamBeginCapture(lead->stream, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaEventRecord(G.fork, lead->stream);
+    for (size_t i = 0; i < lanes.size() && e == cudaSuccess && s == SB_OK; ++i) {
+        sb_ctx* c = lanes[i].ctx;
+        e = cudaStreamWaitEvent(G.branches[i], G.fork, 0);
+        if (e != cudaSuccess) break;
+        cudaStream_t saved = c->stream;
+        c->stream = G.branches[i];
+        s = run_lane(lanes[i]);
+        c->stream = saved;
+        if (s == SB_OK) e = cudaEventRecord(G.joins[i], G.branches[i]);
+        if (e == cudaSuccess && s == SB_OK) e = cudaStreamWaitEvent(lead->stream, G.joins[i], 0);
+    }
+    if (e == cudaSuccess && s == SB_OK) s = enqueue_batch(items.data(), (uint32_t)items.size());
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(lead->stream, &graph);
+    for (sb_ctx* c : all) c->capturing = false;
+    if (e == cudaSuccess) e = e2;
+    if (s != SB_OK || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (s != SB_OK) return s;
+        CK(e);
+    }
+    G.graph = graph;
+    size_t n = 0;
+    CK(cudaGraphGetNodes(graph, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CK(cudaGraphGetNodes(graph, nodes.data(), &n));
+    const void* fn[5] = {trace_batch_kernel(0), trace_batch_kernel(1), trace_batch_kernel(2), trace_batch_kernel(3),
+                         blend_batch_kernel()};
+    int found = 0;
+    G.kernelNodes = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType t;
+        CK(cudaGraphNodeGetType(node, &t));
+        if (t != cudaGraphNodeTypeKernel) continue;
+        ++G.kernelNodes;
+        cudaKernelNodeParams p;
+        CK(cudaGraphKernelNodeGetParams(node, &p));
+        for (int k = 0; k < 5; ++k)
+            if (p.func == fn[k]) {
+                G.nodes[k] = node;
+                G.params[k] = p;
+                ++found;
+            }
+    }
+    if (found != 5) {
+        graph_release(lead);
+        return fail(lead, SB_ERR_CUDA, "captured frame holds %d of the 5 batched kernels", found);
+    }
+    CK(cudaGraphInstantiate(&G.exec, graph, 0));
+    G.lanes = std::move(lanes);
+    G.items = std::move(items);
+    for (sb_ctx* c : all) G.keys.push_back({c, {c->structGen, c->packEpoch}});
+    return SB_OK;
+}
+
+static sb_status graph_launch(sb_ctx* lead) {
+    sb_ctx* ctx = lead;
+    auto& G = lead->graph;
+    if (!G.exec) return fail(lead, SB_ERR_NOT_READY, "no captured frame (sb_graph_capture_frame / _batch)");
+    for (const auto& k : G.keys)
+        if (k.first->structGen != k.second.first || k.first->packEpoch != k.second.second) {
+            // buffers or layouts changed since the capture: this frame runs as
+            // ordinary launches and is captured again for the next replays
+            auto lanes = G.lanes;
+            auto items = G.items;
+            return graph_capture(lead, std::move(lanes), std::move(items));
+        }
+    const uint32_t count = (uint32_t)G.items.size();
+    for (const auto& it : G.items) {
+        sb_status s = solve_prepare(it.ctx, it.cascade);
+        if (s != SB_OK) return s;
+    }
+    static thread_local BatchArgs B;
+    sb_status s = build_batch(G.items.data(), count, B, false);
+    if (s != SB_OK) return s;
+    void* args[1] = {&B};
+    for (int k = 0; k < 5; ++k) {
+        cudaKernelNodeParams p = G.params[k];
+        p.kernelParams = args;
+        p.extra = nullptr;
+        CK(cudaGraphExecKernelNodeSetParams(G.exec, G.nodes[k], &p));
+    }
+    const std::vector<sb_ctx*> all = frame_contexts(G.lanes, G.items);
+    for (sb_ctx* c : all) {
+        if (c == lead || c->stream == lead->stream) continue;
+        CK(ensure_sync_event(c));
+        CK(cudaEventRecord(c->syncEv, c->stream));
+        CK(cudaStreamWaitEvent(lead->stream, c->syncEv, 0));
+    }
+    CK(cudaEventRecord(lead->ev0, lead->stream));
+    CK(cudaGraphLaunch(G.exec, lead->stream));
+    for (uint32_t k = 0; k < G.kernelNodes; ++k) note_launch();
+    CK(cudaEventRecord(lead->ev1, lead->stream));
+    G.timed = true;
+    lead->timed = true;
+    lead->lastWasGraph = true;
+    CK(ensure_sync_event(lead));
+    CK(cudaEventRecord(lead->syncEv, lead->stream));
+    for (sb_ctx* c : all)
+        if (c != lead && c->stream != lead->stream) CK(cudaStreamWaitEvent(c->stream, lead->syncEv, 0));
+    return SB_OK;
+}
+
+sb_status sb_graph_capture_batch(const sb_frame_lane* lanes, uint32_t laneCount, const sb_solve_item* items,
+                                 uint32_t itemCount) {
+    if (!items || itemCount == 0 || !items[0].ctx || (laneCount && !lanes)) return SB_ERR_INVALID_ARG;
+    sb_ctx* lead = items[0].ctx;
+    if (laneCount > 64) return fail(lead, SB_ERR_INVALID_ARG, "%u lanes > 64", laneCount);
+    std::vector<sb_ctx::Graph::Lane> L;
+    for (uint32_t i = 0; i < laneCount; ++i) {
+        const sb_frame_lane& l = lanes[i];
+        if (!l.ctx || l.ctx->device != lead->device || (l.refitCount && (!l.refitRoots || !l.refitEnds)))
+            return fail(lead, SB_ERR_INVALID_ARG, "lane %u: bad context or refit ranges", i);
+        for (uint32_t j = 0; j < i; ++j)
+            if (lanes[j].ctx == l.ctx) return fail(lead, SB_ERR_INVALID_ARG, "lanes %u and %u share a context", j, i);
+        sb_ctx::Graph::Lane x{l.ctx, {}, {}, l.refitTlas};
+        x.roots.assign(l.refitRoots, l.refitRoots + l.refitCount);
+        x.ends.assign(l.refitEnds, l.refitEnds + l.refitCount);
+        L.push_back(std::move(x));
+    }
+    sb_status s = check_batch(items, itemCount);
+    if (s != SB_OK) return s;
+    cudaSetDevice(lead->device);
+    return graph_capture(lead, std::move(L), std::vector<sb_solve_item>(items, items + itemCount));
+}
+
+sb_status sb_graph_capture_frame(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount,
+                                 const uint32_t* refitRoots, const uint32_t* refitEnds, uint32_t refitCount,
+                                 int32_t refitTlas) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    sb_frame_lane lane{ctx, refitRoots, refitEnds, refitCount, refitTlas};
+    sb_solve_item item{ctx, cascade, probeOffset, updatedCount};
+    const bool anyLane = refitCount > 0 || refitTlas;
+    return sb_graph_capture_batch(anyLane ? &lane : nullptr, anyLane ? 1u : 0u, &item, 1);
+}
+
+sb_status sb_graph_launch(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    return graph_launch(ctx);
+}
+
+sb_status sb_graph_destroy(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    graph_release(ctx);
+    graph_free_streams(ctx);
+    return SB_OK;
 }
 
 // ---------------------------------------------------------------- adjoint
@@ -1087,6 +1370,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
     if (!ctx || !world16 || !active || !blasRoot || !blasEnd) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
     ++ctx->epoch;
+    ++ctx->structGen;
     if (count != ctx->B.instCount)
         return fail(ctx, SB_ERR_INVALID_ARG, "instance count %u != scene instCount %u", count, ctx->B.instCount);
     for (uint32_t i = 0; i < count; ++i)
@@ -1130,6 +1414,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
 sb_status sb_build_tlas(sb_ctx* ctx) {
     if (!ctx) return SB_ERR_INVALID_ARG;
     ++ctx->epoch;
+    ++ctx->structGen;
     if (!ctx->instancesSet) return fail(ctx, SB_ERR_NOT_READY, "sb_set_instances first");
     if (ctx->I.count > TLAS_BUILD_MAX)
         return fail(ctx, SB_ERR_UNSUPPORTED, "%u instances > %u (single-CTA TLAS build)", ctx->I.count, TLAS_BUILD_MAX);
@@ -1206,7 +1491,10 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
         out->shadowBlasNodeVisits = c[8];
         out->shadowTriangleTests = c[9];
     }
-    if (ctx->timed) {
+    if (ctx->timed && ctx->lastWasGraph) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) out->lastSolveMs = ms;  // whole frame
+    } else if (ctx->timed) {
         float ms = 0.0f;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) out->lastSolveMs = ms;
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evMid) == cudaSuccess) out->lastTraceMs = ms;
@@ -1242,6 +1530,7 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (t->bvhKind > 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
     if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
     ctx->bvhKind = t->bvhKind;
+    ++ctx->structGen;
     ctx->tune.block = t->traceBlock;
     ctx->tune.sortKey = t->sortKey;
     ctx->tune.smemTlasNodes = t->smemTlasNodes;

@@ -53,6 +53,10 @@ cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cuda
                                cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
 cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st);
 uint32_t blend_blocks(uint32_t updatedCount);  // CTAs of the blend for one solve
+// The batched kernels (stage 0 primary, 1 emit, 2 shadow, 3 shade; blend):
+// a captured graph refreshes their BatchArgs parameter on every replay.
+const void* trace_batch_kernel(int stage);
+const void* blend_batch_kernel();
 
 // Adjoint of shade + blend + upload (sb_adjoint.cu), over every probe of a
 // cascade (probe slot = probe index). Gradient layouts: gE / E per interior

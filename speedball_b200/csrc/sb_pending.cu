@@ -3,8 +3,5 @@
 #include "sb_kernels.cuh"
 
 extern "C" {
-sb_status sb_graph_capture_frame(sb_ctx*, uint32_t, uint32_t, uint32_t, const uint32_t*, const uint32_t*, uint32_t,
-                                 int32_t) { return SB_ERR_UNSUPPORTED; }
-sb_status sb_graph_launch(sb_ctx*) { return SB_ERR_UNSUPPORTED; }
 sb_status sb_autotune(sb_ctx*, uint32_t, sb_tuning*) { return SB_ERR_UNSUPPORTED; }
 }

@@ -396,6 +396,16 @@ __global__ void __launch_bounds__(128) k_shade_batch(const __grid_constant__ Bat
     shade_ray(I.W, g);
 }
 
+const void* trace_batch_kernel(int stage) {
+    switch (stage) {
+        case 0: return (const void*)k_trace_primary_batch;
+        case 1: return (const void*)k_emit_batch;
+        case 2: return (const void*)k_trace_shadow_batch;
+        case 3: return (const void*)k_shade_batch;
+        default: return nullptr;
+    }
+}
+
 cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cudaStream_t st,
                                cudaEvent_t afterPrimary, cudaEvent_t afterShadow) {
     if (B.n == 0 || B.totalRays == 0) return cudaSuccess;
