@@ -587,8 +587,10 @@ def batch_fields(device):
 def run_batch(args, dist: Dist):
     """One step = one frame: every scene's motion lanes on the device (deformer
     refit, instance bounds + TLAS refit) and 11 solves (the atrium's 3
-    cascades, the 8 atria's C0). value = batched frames' primary rays / device
-    time; the same frames with per-solve launches are timed beside it."""
+    cascades, the 8 atria's C0), after sb_autotune on every context. value =
+    primary rays / device time of the frame as one CUDA graph (lanes as
+    parallel branches, one batched solve); beside it the same frames as
+    ordinary batched launches and as per-solve launches (the plain form)."""
     from speedball_b200 import _abi
     from speedball_b200.batch import BatchedFrame
     device = dist.local
@@ -640,12 +642,23 @@ def run_batch(args, dist: Dist):
         motion()
         frame.tickPlain()
 
-    from speedball_b200.batch import GraphFrame, Lane
+    from speedball_b200.batch import GraphFrame, Lane, autotune
+    # every context gets its autotuned traversal parameters (plain and batched
+    # frames alike; the batch runs with the lead context's block size and ray
+    # order, and each scene's own BVH kind)
+    t0 = time.perf_counter()
+    tunings = [autotune(f) for f in fields]
+    tune_s = time.perf_counter() - t0
     graph = GraphFrame(frame, [Lane(f, [(root, end)]) for f, root, end in lanes])
 
     clocks = Clocks(device)
     clocks.start()
     ms_plain, _ = timed(plain)
+    from speedball_b200.batch import autotuneBatch
+    full = [dict(cascade=0, probeOffset=0, updatedCount=f._probeTotal) for f in fields]
+    t0 = time.perf_counter()
+    batch_tuning = autotuneBatch(frame.items(full))
+    tune_s += time.perf_counter() - t0
     ms_nograph, _ = timed(batched)
     ms_batch, launches = timed(graph.tick)
     clk = clocks.stop()
@@ -664,6 +677,7 @@ def run_batch(args, dist: Dist):
                    "l2": "flushed (256 MiB write) before every timed step"},
         "plain_value": round(plain_value, 3), "plain_ms_per_step": round(ms_plain, 4),
         "batched_no_graph_ms_per_step": round(ms_nograph, 4),
+        "autotuned": tunings, "autotuned_batch": batch_tuning, "autotune_s": round(tune_s, 2),
         "batched_over_plain": round(ms_plain / ms_batch, 4),
         "gpu_launches": int(launches),
         "clocks": clk,

@@ -372,8 +372,15 @@ typedef struct sb_tuning {
 } sb_tuning;
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);
-/* Time candidate tunings on the current scene and cascade; keeps the fastest. */
+/* Time full solves of `cascade` under candidate tunings (bvhKind 1 / 2 / 0,
+ * traceBlock 128 / 192 / 256, both sort keys, and for bvhKind 0 TLAS staging
+ * off / 512 nodes), keep the fastest on the context and return it. The
+ * cascade's histories and atlases are restored afterwards. Synchronizes. */
 sb_status sb_autotune(sb_ctx* ctx, uint32_t cascade, sb_tuning* chosen);
+/* The same for a batch: the lead context's traceBlock and sortKey (the batched
+ * launches' parameters) timed on sb_solve_batch(items); each context keeps its
+ * own bvhKind. Every item's probe state is restored. Synchronizes. */
+sb_status sb_autotune_batch(const sb_solve_item* items, uint32_t count, sb_tuning* chosen);
 
 /* Device-side counters of the last solve (rays, shadow rays, node/tri visits). */
 typedef struct sb_stats {

@@ -163,6 +163,7 @@ SIGNATURES = {
     "sb_get_tuning": (C.c_int, [_P, C.POINTER(sb_tuning)]),
     "sb_set_tuning": (C.c_int, [_P, C.POINTER(sb_tuning)]),
     "sb_autotune": (C.c_int, [_P, _U32, C.POINTER(sb_tuning)]),
+    "sb_autotune_batch": (C.c_int, [C.POINTER(sb_solve_item), _U32, C.POINTER(sb_tuning)]),
     "sb_get_stats": (C.c_int, [_P, C.POINTER(sb_stats)]),
     "sb_enable_counters": (C.c_int, [_P, C.c_int32]),
     "sbh_build_blas": (_U32, [_P, _U32, _P, _U32, _U32, _P, _P]),

@@ -79,6 +79,30 @@ class BatchedFrame:
             _abi.check(f._lib.sb_set_stream(f.ctx, C.c_void_p(int(stream))), f.ctx)
 
 
+def autotune(field: ProbeField, cascade: int = 0) -> dict:
+    """sb_autotune on one field: the fastest of the candidate traversal
+    tunings for its scene, kept on its context; the probe state is restored."""
+    t = _abi.sb_tuning()
+    _abi.check(field._lib.sb_autotune(field.ctx, cascade, C.byref(t)), field.ctx)
+    return dict(traceBlock=t.traceBlock, sortKey=t.sortKey, smemTlasNodes=t.smemTlasNodes, bvhKind=t.bvhKind)
+
+
+def autotuneBatch(items) -> dict:
+    """sb_autotune_batch: the batched launches' block size and ray order timed
+    on the batch itself, kept on the lead context."""
+    items = list(items)
+    arr = (_abi.sb_solve_item * len(items))()
+    for i, it in enumerate(items):
+        arr[i].ctx = it.field.ctx
+        arr[i].cascade = it.cascade
+        arr[i].probeOffset = it.probeOffset
+        arr[i].updatedCount = it.updatedCount
+    t = _abi.sb_tuning()
+    lead = items[0].field
+    _abi.check(lead._lib.sb_autotune_batch(arr, len(items), C.byref(t)), lead.ctx)
+    return dict(traceBlock=t.traceBlock, sortKey=t.sortKey)
+
+
 @dataclass
 class Lane:
     """A field's device-side motion lane in a captured frame."""

@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -1151,6 +1152,153 @@ sb_status sb_graph_launch(sb_ctx* ctx) {
     if (!ctx) return SB_ERR_INVALID_ARG;
     cudaSetDevice(ctx->device);
     return graph_launch(ctx);
+}
+
+// ---------------------------------------------------------------- autotuner
+
+// A copy of one cascade's probe state (histories, atlases), so trial solves
+// leave it as they found it.
+struct CascadeSnapshot {
+    sb_ctx* ctx = nullptr;
+    uint32_t ci = 0;
+    float4* irr = nullptr;
+    float2* depth = nullptr;
+    uint2 *atlas = nullptr, *datlas = nullptr;
+
+    cudaError_t copy(bool save) {
+        Cascade& K = ctx->casc[ci];
+        const size_t hist = (size_t)K.probeTotal * 64, texels = (size_t)K.atlasW * K.atlasH;
+        struct { void* a; void* b; size_t n; } m[4] = {{irr, K.irr, hist * 16}, {depth, K.depth, hist * 8},
+                                                      {atlas, K.atlas, texels * 8}, {datlas, K.depthAtlas, texels * 8}};
+        for (auto& x : m) {
+            cudaError_t r = cudaMemcpyAsync(save ? x.a : x.b, save ? x.b : x.a, x.n, cudaMemcpyDeviceToDevice,
+                                            ctx->stream);
+            if (r != cudaSuccess) return r;
+        }
+        return cudaSuccess;
+    }
+    cudaError_t save(sb_ctx* c, uint32_t cascade) {
+        ctx = c;
+        ci = cascade;
+        Cascade& K = c->casc[cascade];
+        const size_t hist = (size_t)K.probeTotal * 64, texels = (size_t)K.atlasW * K.atlasH;
+        size_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+        cudaError_t e = grow(irr, c0, hist);
+        if (e == cudaSuccess) e = grow(depth, c1, hist);
+        if (e == cudaSuccess) e = grow(atlas, c2, texels);
+        if (e == cudaSuccess) e = grow(datlas, c3, texels);
+        return e == cudaSuccess ? copy(true) : e;
+    }
+    cudaError_t restore() {
+        cudaError_t e = copy(false);
+        return e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
+    }
+    ~CascadeSnapshot() {
+        release(irr);
+        release(depth);
+        release(atlas);
+        release(datlas);
+    }
+};
+
+// Minimum device time (lead->ev0 .. ev1) of `reps` runs after one warm-up.
+static sb_status time_min(sb_ctx* lead, const std::vector<sb_ctx*>& all, const std::function<sb_status()>& run,
+                          int reps, float& best) {
+    best = 3.4e38f;
+    for (int rep = 0; rep <= reps; ++rep) {
+        sb_status s = run();
+        for (sb_ctx* c : all)
+            if (s == SB_OK) s = sb_synchronize(c);
+        if (s != SB_OK) return s;
+        float m = 0.0f;
+        if (rep > 0 && cudaEventElapsedTime(&m, lead->ev0, lead->ev1) == cudaSuccess && m < best) best = m;
+    }
+    return SB_OK;
+}
+
+// Times full solves of cascade ci under each candidate tuning and keeps the
+// fastest. Candidates: the scene BVH kinds (8-wide / binary / the reference's
+// two-level walk), traversal block sizes 128 / 192 / 256, both ray issue
+// orders, and for the two-level walk TLAS staging in shared memory off / up to
+// 512 nodes. The cascade's histories and atlases are restored afterwards, so
+// tuning leaves the probe state as it found it.
+sb_status sb_autotune(sb_ctx* ctx, uint32_t ci, sb_tuning* chosen) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    sb_status s = solve_prepare(ctx, ci);
+    if (s != SB_OK) return s;
+    const uint32_t probes = ctx->casc[ci].probeTotal;
+    CascadeSnapshot snap;
+    CK(snap.save(ctx, ci));
+    const sb_tuning saved{ctx->tune.block, ctx->tune.sortKey, ctx->tune.smemTlasNodes, ctx->bvhKind};
+    const bool savedCounters = ctx->countersOn;
+    ctx->countersOn = false;
+    sb_tuning best = saved;
+    float bestMs = 3.4e38f;
+    const uint32_t kinds[3] = {1u, 2u, 0u}, blocks[3] = {128u, 192u, 256u};
+    for (uint32_t kind : kinds)
+        for (uint32_t block : blocks)
+            for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort)
+                for (uint32_t sm = 0; sm < (kind == 0 ? 2u : 1u) && s == SB_OK; ++sm) {
+                    sb_tuning t{block, sort, kind == 0 ? (sm ? 512u : 0u) : saved.smemTlasNodes, kind};
+                    if ((s = sb_set_tuning(ctx, &t)) != SB_OK) break;
+                    float ms = 0.0f;
+                    s = time_min(ctx, {ctx}, [&] { return sb_solve(ctx, ci, 0, probes); }, 3, ms);
+                    if (s == SB_OK && ms < bestMs) {
+                        bestMs = ms;
+                        best = t;
+                    }
+                }
+    cudaError_t e = snap.restore();
+    ctx->countersOn = savedCounters;
+    sb_status s2 = sb_set_tuning(ctx, s == SB_OK && e == cudaSuccess ? &best : &saved);
+    if (s != SB_OK) return s;
+    CK(e);
+    if (s2 != SB_OK) return s2;
+    if (chosen) *chosen = best;
+    return SB_OK;
+}
+
+// The batch's launch parameters (the lead context's block size and ray issue
+// order) timed on the batched solve itself; each context keeps its own scene
+// BVH kind. Every item's probe state is restored afterwards.
+sb_status sb_autotune_batch(const sb_solve_item* items, uint32_t count, sb_tuning* chosen) {
+    sb_status s = check_batch(items, count);
+    if (s != SB_OK) return s;
+    sb_ctx* lead = items[0].ctx;
+    sb_ctx* ctx = lead;
+    cudaSetDevice(lead->device);
+    std::vector<CascadeSnapshot> snaps(count);
+    std::vector<sb_ctx*> all;
+    for (uint32_t i = 0; i < count; ++i) {
+        CK(snaps[i].save(items[i].ctx, items[i].cascade));
+        bool seen = false;
+        for (sb_ctx* c : all) seen = seen || c == items[i].ctx;
+        if (!seen) all.push_back(items[i].ctx);
+    }
+    const sb_tuning saved{lead->tune.block, lead->tune.sortKey, lead->tune.smemTlasNodes, lead->bvhKind};
+    sb_tuning best = saved;
+    float bestMs = 3.4e38f;
+    const uint32_t blocks[3] = {128u, 192u, 256u};
+    for (uint32_t block : blocks)
+        for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort) {
+            sb_tuning t{block, sort, saved.smemTlasNodes, saved.bvhKind};
+            if ((s = sb_set_tuning(lead, &t)) != SB_OK) break;
+            float ms = 0.0f;
+            s = time_min(lead, all, [&] { return sb_solve_batch(items, count); }, 3, ms);
+            if (s == SB_OK && ms < bestMs) {
+                bestMs = ms;
+                best = t;
+            }
+        }
+    cudaError_t e = cudaSuccess;
+    for (auto& sn : snaps)
+        if (e == cudaSuccess) e = sn.restore();
+    sb_status s2 = sb_set_tuning(lead, s == SB_OK && e == cudaSuccess ? &best : &saved);
+    if (s != SB_OK) return s;
+    CK(e);
+    if (s2 != SB_OK) return s2;
+    if (chosen) *chosen = best;
+    return SB_OK;
 }
 
 sb_status sb_graph_destroy(sb_ctx* ctx) {

@@ -135,3 +135,28 @@ def test_batch_rejects_bad_items():
     finally:
         a.dispose()
         b.dispose()
+
+
+def test_autotune_picks_a_candidate_and_restores_the_probes():
+    from speedball_b200 import _abi as abi
+    import ctypes as C
+    f = make_field(synth.room_spheres(0))
+    try:
+        for _ in range(2):
+            f.tick()
+        f.synchronize()
+        before = _state(f, 0)
+        t = abi.sb_tuning()
+        abi.check(f._lib.sb_autotune(f.ctx, 0, C.byref(t)), f.ctx)
+        after = _state(f, 0)
+        for key in ("irr", "depth", "atlas", "datlas"):
+            assert np.array_equal(before[key], after[key]), key
+        assert t.bvhKind in (0, 1, 2) and t.traceBlock in (128, 192, 256) and t.sortKey in (0, 1)
+        cur = abi.sb_tuning()
+        abi.check(f._lib.sb_get_tuning(f.ctx, C.byref(cur)), f.ctx)
+        assert (cur.traceBlock, cur.sortKey, cur.smemTlasNodes, cur.bvhKind) == \
+               (t.traceBlock, t.sortKey, t.smemTlasNodes, t.bvhKind)
+        f.tick()  # the tuned context keeps solving
+        f.synchronize()
+    finally:
+        f.dispose()
