@@ -47,10 +47,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch"], default="atrium",
+    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch", "large"], default="atrium",
                     help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
                          "differentiated update (64 materials, 32 point lights, 2 feedback solves); batch: 3 "
-                         "nested cascades of the atrium + 8 independent atria per frame, batched vs plain")
+                         "nested cascades of the atrium + 8 independent atria per frame, batched vs plain; "
+                         "large: 2.1M unique / 12.8M instanced triangles, 32^3 probes x 256 rays x 2 cascades, "
+                         "binary vs 8-wide scene BVH vs the reference two-level walk")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -688,11 +690,135 @@ def run_batch(args, dist: Dist):
     return line
 
 
+LARGE_METRIC = "probe Mrays/s (large scene, 2 cascades)"
+
+
+def large_field(device):
+    """The large scene's field: 32^3 probes x 256 rays over the world box, and
+    a second cascade of 32^3 probes over the half-extent box around its
+    centre; clustered lights, gated jitter, full updates."""
+    from speedball_b200 import synth
+    from speedball_b200.field import ProbeField
+    scene = synth.large_scene()
+    g = scene.meta["grid"]
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
+    f.setHysteresisNormalization(False)
+    f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)
+    c1 = synth.nested_cascades(g, res=(g["res"], g["res"]), scale=0.5)[1]
+    f.configureCascade(1, c1["gridMin"], c1["gridSize"], c1["res"])
+    return scene, f
+
+
+def run_large(args, dist: Dist):
+    """One step = one frame: the skinned mesh posed (bone rotations <= 15 deg),
+    its vertices uploaded from page-locked memory, its BLAS refit, instance
+    bounds + TLAS refit, then full solves of both cascades (16.8M primary
+    rays). Timed once per scene-BVH layout: bvhKind 2 (binary, FP32 boxes),
+    1 (8-wide, 8-bit boxes for closest hits) and 0 (the reference's TLAS +
+    BLAS walk); hit records of the layouts are compared on a fixed pose."""
+    from speedball_b200 import _abi, synth
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    t0 = time.perf_counter()
+    scene, f = large_field(device)
+    setup_s = time.perf_counter() - t0
+    lib, ctx = f._lib, f.ctx
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
+    flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
+    sk = scene.meta["skinned"]
+    W, K = args.warmup, args.steps
+    poses = [synth.large_pose(scene, fr) for fr in range(W + K + 1)]
+    rays = (f._probeTotal + f.cascadeProbes(1)) * f.getRays()
+    e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
+
+    def frame(i):
+        scene.meshes[sk].positions = poses[i]
+        f.refreshDeforms([sk])           # pinned upload + BLAS refit + TLAS refit
+        fr = f.beginTick()
+        _abi.check(lib.sb_solve(ctx, 0, fr["probeOffset"], fr["updatedCount"]), ctx)
+        _abi.check(lib.sb_solve(ctx, 1, 0, f.cascadeProbes(1)), ctx)
+        f.endTick(fr)
+
+    def hits(ci):
+        n = f.cascadeProbes(ci) * f.getRays()
+        h = np.zeros(n * 4, np.uint32)
+        _abi.check(lib.sb_read_buffer(ctx, _abi.BUF["HIT_RECORDS"] | (ci << 8), 0, n * 4, _abi.ptr(h)), ctx)
+        return h.reshape(n, 4)
+
+    results, records = {}, {}
+    clocks = Clocks(device)
+    clocks.start()
+    launches = 0
+    for kind in (2, 1, 0):
+        t = _abi.sb_tuning()
+        _abi.check(lib.sb_get_tuning(ctx, C.byref(t)), ctx)
+        t.bvhKind = kind
+        _abi.check(lib.sb_set_tuning(ctx, C.byref(t)), ctx)
+        tb = time.perf_counter()
+        for i in range(W):
+            frame(i)
+            ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+        f.synchronize()
+        warm_s = time.perf_counter() - tb
+        dist.barrier()
+        l0 = _stats(lib, ctx).kernelLaunches
+        total = 0.0
+        for i in range(K):
+            ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+            ck(rt.cudaEventRecord(e0, stream))
+            frame(W + i)
+            ck(rt.cudaEventRecord(e1, stream))
+            ck(rt.cudaEventSynchronize(e1))
+            total += ck(rt.cudaEventElapsedTime(e0, e1))
+        launches += _stats(lib, ctx).kernelLaunches - l0
+        ms = dist.max(total / K)
+        frame(W + K)                      # the same pose for every layout: compare hit records
+        f.synchronize()
+        records[kind] = (hits(0), hits(1))
+        results[kind] = {"ms_per_step": round(ms, 3), "mrays_s": round(dist.world * rays / (ms * 1e-3) / 1e6, 2),
+                         "warmup_s": round(warm_s, 2)}
+    clk = clocks.stop()
+
+    def agree(a, b):
+        same = (a[:, 0] == b[:, 0]) & ((a[:, 1] & 0x7FFFFFFF) == (b[:, 1] & 0x7FFFFFFF))
+        t_a, t_b = a[:, 2].view(np.float32), b[:, 2].view(np.float32)
+        hit = a[:, 0] != 0xFFFFFFFF
+        rel = np.abs(t_a - t_b) / np.maximum(np.abs(t_a), 1e-30)
+        return {"hit_id_agreement": round(float(same.mean()), 7),
+                "t_rel_max_where_ids_agree": float(rel[same & hit].max()) if (same & hit).any() else 0.0,
+                "differing_rays": int((~same).sum())}
+    cmp = {f"kind{k}_vs_kind2": {f"c{ci}": agree(records[k][ci], records[2][ci]) for ci in (0, 1)} for k in (1, 0)}
+    best = min(results, key=lambda k: results[k]["ms_per_step"])
+    line = {
+        "metric": LARGE_METRIC, "value": results[1]["mrays_s"], "unit": "Mrays/s", "n_gpus": dist.world, "steps": K,
+        "warmup": W, "ms_per_step": results[1]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded large instanced scene)",
+        "config": {"workload": "8 archetypes of 2k-600k tris (2,101,000 unique), 400 instances (12,810,000 "
+                               "instanced), a 120k-tri skinned tube refit every frame (8 bones, <=15 deg), 64 "
+                               "clustered point lights, 2 cascades of 32^3 probes x 256 rays",
+                   "primary_rays_per_step": int(rays), "layout_of_value": "bvhKind 1 (8-wide, 8-bit boxes)",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "layouts": {f"bvhKind{k}": v for k, v in results.items()}, "fastest_layout": f"bvhKind{best}",
+        "hit_agreement": cmp, "setup_s": round(setup_s, 2),
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    f.dispose()
+    ck(rt.cudaFree(flush))
+    return line
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
     try:
-        if args.workload == "batch":
+        if args.workload == "large":
+            line = run_large(args, dist) if args.impl == "ours" else \
+                {"impl": "reference", "unavailable": "the large workload is measured on the GPU path only"}
+        elif args.workload == "batch":
             line = run_batch(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference has no batched multi-scene form"}
         elif args.workload == "adjoint":

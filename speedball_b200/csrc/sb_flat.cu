@@ -10,9 +10,11 @@
 // Per frame nothing is rebuilt: a slot whose transform changes, or whose BLAS
 // is refit, is marked; the traversal skips that slot's items and walks its
 // current BLAS instead. More than kMaxDynamic marked slots trigger a rebuild.
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 #include "sb_flat_scene.cuh"
 
@@ -90,54 +92,107 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
             uint32_t src = (order && s < orderCount) ? ord[s] : s;
             if (src < slots) srcToSlot[src] = s;
         }
-        std::vector<float> boxes;
-        std::vector<uint32_t> itTri, itSlot;
-        boxes.reserve((size_t)B.triCount * 6);
-        itTri.reserve(B.triCount);
-        itSlot.reserve(B.triCount);
+        // items per slot (every triangle of an active slot's BLAS leaves), then
+        // their world boxes, slots in parallel, each into its own range
+        std::vector<uint64_t> slotItems(slots + 1, 0);
         for (uint32_t s = 0; s < slots; ++s) {
             const float* R = inst.data() + (size_t)s * 16;
             uint32_t root = f_bits(R[12]), end = f_bits(R[13]);
             slotRoot[s] = root;
             slotEnd[s] = end;
-            if (!(R[15] > 0.5f) || !(root < end && end <= B.nodeCount)) continue;  // inactive or no BLAS
-            double M[12];
-            if (!invert_rows(R, M)) continue;  // singular: the local test never hits
-            for (uint32_t n = root; n < end; ++n) {
-                uint32_t payload = hn[8 * (size_t)n + 7];
-                if (payload == 0xFFFFFFFFu) continue;
-                uint32_t off = payload & 0x00FFFFFFu, cnt = payload >> 24;
-                for (uint32_t t = off; t < off + cnt && t < B.triCount; ++t) {
-                    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-                    bool ok = true;
-                    for (int k = 0; k < 3; ++k) {
-                        uint32_t v = tri[3 * (size_t)t + k];
-                        if (v >= B.vertexCount) { ok = false; break; }
-                        const float* p = vert.data() + 8 * (size_t)v;
-                        for (int a = 0; a < 3; ++a) {
-                            double w = M[4 * a] * p[0] + M[4 * a + 1] * p[1] + M[4 * a + 2] * p[2] + M[4 * a + 3];
-                            lo[a] = std::fmin(lo[a], w);
-                            hi[a] = std::fmax(hi[a], w);
+            uint64_t c = 0;
+            if (R[15] > 0.5f && root < end && end <= B.nodeCount)
+                for (uint32_t nd = root; nd < end; ++nd) {
+                    uint32_t payload = hn[8 * (size_t)nd + 7];
+                    if (payload != 0xFFFFFFFFu) c += payload >> 24;
+                }
+            slotItems[s + 1] = slotItems[s] + c;
+        }
+        const uint64_t cap = slotItems[slots];
+        if (cap >= (1ull << 24)) {
+            why = "scene BVH: too many (triangle, instance) items";
+            dirty = false;
+            return cudaSuccess;
+        }
+        std::vector<float> boxes(cap * 6);
+        std::vector<uint32_t> itTri(cap), itSlot(cap);
+        std::vector<uint8_t> keep(cap, 0);
+        std::atomic<uint32_t> nextSlot{0};
+        auto work = [&] {
+            for (uint32_t s; (s = nextSlot.fetch_add(1)) < slots;) {
+                const float* R = inst.data() + (size_t)s * 16;
+                const uint32_t root = slotRoot[s], end = slotEnd[s];
+                if (slotItems[s + 1] == slotItems[s]) continue;  // inactive or no BLAS
+                double M[12];
+                if (!invert_rows(R, M)) continue;  // singular: the local test never hits
+                uint64_t o = slotItems[s];
+                for (uint32_t nd = root; nd < end; ++nd) {
+                    uint32_t payload = hn[8 * (size_t)nd + 7];
+                    if (payload == 0xFFFFFFFFu) continue;
+                    uint32_t off = payload & 0x00FFFFFFu, cnt = payload >> 24;
+                    for (uint32_t t = off; t < off + cnt; ++t, ++o) {
+                        if (t >= B.triCount) continue;
+                        double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                        bool ok = true;
+                        for (int k = 0; k < 3; ++k) {
+                            uint32_t v = tri[3 * (size_t)t + k];
+                            if (v >= B.vertexCount) { ok = false; break; }
+                            const float* p = vert.data() + 8 * (size_t)v;
+                            for (int a = 0; a < 3; ++a) {
+                                double w = M[4 * a] * p[0] + M[4 * a + 1] * p[1] + M[4 * a + 2] * p[2] + M[4 * a + 3];
+                                lo[a] = std::fmin(lo[a], w);
+                                hi[a] = std::fmax(hi[a], w);
+                            }
                         }
+                        if (!ok || !std::isfinite(lo[0] + lo[1] + lo[2] + hi[0] + hi[1] + hi[2])) continue;
+                        // margin well above the FP32 rounding of the local ray and vertices
+                        double mag = 0.0, ext = 0.0;
+                        for (int a = 0; a < 3; ++a) {
+                            mag = std::fmax(mag, std::fmax(std::fabs(lo[a]), std::fabs(hi[a])));
+                            ext = std::fmax(ext, hi[a] - lo[a]);
+                        }
+                        const double m = 1e-5 * mag + 1e-5 * ext + 1e-7;
+                        float* bx = boxes.data() + 6 * o;
+                        for (int a = 0; a < 3; ++a) bx[a] = std::nextafterf((float)(lo[a] - m), -INFINITY);
+                        for (int a = 0; a < 3; ++a) bx[3 + a] = std::nextafterf((float)(hi[a] + m), INFINITY);
+                        itTri[o] = t;
+                        itSlot[o] = s;
+                        keep[o] = 1;
                     }
-                    if (!ok || !std::isfinite(lo[0] + lo[1] + lo[2] + hi[0] + hi[1] + hi[2])) continue;
-                    // margin well above the FP32 rounding of the local ray and vertices
-                    double mag = 0.0, ext = 0.0;
-                    for (int a = 0; a < 3; ++a) {
-                        mag = std::fmax(mag, std::fmax(std::fabs(lo[a]), std::fabs(hi[a])));
-                        ext = std::fmax(ext, hi[a] - lo[a]);
-                    }
-                    const double m = 1e-5 * mag + 1e-5 * ext + 1e-7;
-                    for (int a = 0; a < 3; ++a) boxes.push_back(std::nextafterf((float)(lo[a] - m), -INFINITY));
-                    for (int a = 0; a < 3; ++a) boxes.push_back(std::nextafterf((float)(hi[a] + m), INFINITY));
-                    itTri.push_back(t);
-                    itSlot.push_back(s);
                 }
             }
+        };
+        {
+            const unsigned th = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+            std::vector<std::thread> ts;
+            for (unsigned w = 1; w < th && cap > 65536; ++w) ts.emplace_back(work);
+            work();
+            for (auto& t : ts) t.join();
         }
+        // drop degenerate items, keeping slot order
+        uint64_t kept = 0;
+        for (uint64_t i = 0; i < cap; ++i) {
+            if (!keep[i]) continue;
+            if (kept != i) {
+                std::memcpy(boxes.data() + 6 * kept, boxes.data() + 6 * i, 24);
+                itTri[kept] = itTri[i];
+                itSlot[kept] = itSlot[i];
+            }
+            ++kept;
+        }
+        itTri.resize(kept);
+        itSlot.resize(kept);
         const uint32_t n = (uint32_t)itTri.size();
+        // the 8-wide tree builds beside the binary one
+        flat::WideTree wt;
+        bool wideOk = false;
+        std::thread wideBuild;
+        if (wide && n)
+            wideBuild = std::thread([&] { wideOk = flat::build_wide(boxes.data(), itTri.data(), itSlot.data(), n, wt); });
         flat::Tree tree;
-        if (!flat::build(boxes.data(), itTri.data(), itSlot.data(), n, tree)) {
+        const bool treeOk = flat::build(boxes.data(), itTri.data(), itSlot.data(), n, tree);
+        if (wideBuild.joinable()) wideBuild.join();
+        if (!treeOk) {
             why = "scene BVH: too many items";
             dirty = false;
             return cudaSuccess;
@@ -156,8 +211,7 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
         const uint32_t treeRoot = tree.root, treeDepth = tree.depth;
         wideReady = false;
         if (wide && n) {
-            flat::WideTree wt;
-            if (flat::build_wide(boxes.data(), itTri.data(), itSlot.data(), n, wt) && wt.depth + 1 <= (uint32_t)SB_STACK) {
+            if (wideOk && wt.depth + 1 <= (uint32_t)SB_STACK) {
                 const size_t wq = wt.nodes.size() / 4;
                 e = grow_dev(wnodes, wnodeCap, wq);
                 if (e == cudaSuccess) e = grow_dev(witems, witemCap, n);

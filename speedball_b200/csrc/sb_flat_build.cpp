@@ -11,8 +11,11 @@
 #include "sb_flat.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 namespace sb {
 namespace flat {
@@ -43,67 +46,150 @@ struct Box {
     }
 };
 
-struct Builder {
-    uint32_t maxLeaf = 4;
-    const float* boxes;  // 6 per item
-    std::vector<float> cen;
-    std::vector<uint32_t> order;
-    std::vector<Box> nodeBox;        // per tree node (interior and leaf)
-    std::vector<uint32_t> left, right, first, count;  // count == 0 -> interior
-
-    Box item_box(uint32_t i) const {
-        Box b;
-        std::memcpy(b.lo, boxes + 6 * (size_t)i, 12);
-        std::memcpy(b.hi, boxes + 6 * (size_t)i + 3, 12);
-        return b;
-    }
-
-    uint32_t make_node() {
-        nodeBox.emplace_back();
+// Tree nodes under construction (interior: count == 0).
+struct Nodes {
+    std::vector<Box> box;
+    std::vector<uint32_t> left, right, first, count;
+    uint32_t make() {
+        box.emplace_back();
         left.push_back(0);
         right.push_back(0);
         first.push_back(0);
         count.push_back(0);
-        return (uint32_t)nodeBox.size() - 1;
+        return (uint32_t)box.size() - 1;
+    }
+    size_t size() const { return box.size(); }
+};
+
+struct Bins {
+    Box bb[3][BINS];
+    uint32_t bc[3][BINS] = {};
+    void merge(const Bins& o) {
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < BINS; ++b) {
+                bb[a][b].grow(o.bb[a][b]);
+                bc[a][b] += o.bc[a][b];
+            }
+    }
+};
+
+// Runs f(lo, hi, part) over `parts` contiguous pieces of [lo, hi) in parallel.
+template <class F> void parallel_ranges(uint32_t lo, uint32_t hi, int parts, F&& f) {
+    if (parts <= 1) {
+        f(lo, hi, 0);
+        return;
+    }
+    std::vector<std::thread> ts;
+    const uint32_t n = hi - lo;
+    for (int p = 0; p < parts; ++p) {
+        const uint32_t a = lo + (uint32_t)((uint64_t)n * p / parts), b = lo + (uint32_t)((uint64_t)n * (p + 1) / parts);
+        ts.emplace_back([&f, a, b, p] { f(a, b, p); });
+    }
+    for (auto& t : ts) t.join();
+}
+
+// One item as the builder moves it: its box, centroid and input index. The
+// items themselves are partitioned (not an index array), so every pass over a
+// node's range reads memory in order.
+struct Prim {
+    float lo[3], hi[3], c[3];
+    uint32_t id;
+};
+
+struct Builder {
+    uint32_t maxLeaf = 4;
+    std::vector<Prim> prims;
+    std::vector<uint32_t> order;  // filled after build: order[k] = prims[k].id
+    Nodes N;
+
+    void init(const float* boxes, uint32_t n) {
+        prims.resize(n);
+        for (uint32_t i = 0; i < n; ++i) {
+            Prim& p = prims[i];
+            std::memcpy(p.lo, boxes + 6 * (size_t)i, 12);
+            std::memcpy(p.hi, boxes + 6 * (size_t)i + 3, 12);
+            for (int a = 0; a < 3; ++a) p.c[a] = 0.5f * (p.lo[a] + p.hi[a]);
+            p.id = i;
+        }
     }
 
-    // Splits [lo, hi) of `order`; returns the split point or hi for a leaf.
-    uint32_t split(uint32_t lo, uint32_t hi, const Box& nb) {
+    static void grow(Box& b, const Prim& p) {
+        for (int a = 0; a < 3; ++a) {
+            b.lo[a] = std::min(b.lo[a], p.lo[a]);
+            b.hi[a] = std::max(b.hi[a], p.hi[a]);
+        }
+    }
+
+    // Node box and centroid box of [lo, hi) (parallel over `parts`, at most 64).
+    void bounds(uint32_t lo, uint32_t hi, int parts, Box& nb, Box& cb) const {
+        Box pn[64], pc[64];
+        parallel_ranges(lo, hi, parts, [&](uint32_t a, uint32_t b, int p) {
+            Box bn, bc;
+            for (uint32_t k = a; k < b; ++k) {
+                grow(bn, prims[k]);
+                bc.grow(prims[k].c);
+            }
+            pn[p] = bn;
+            pc[p] = bc;
+        });
+        for (int p = 0; p < parts; ++p) {
+            nb.grow(pn[p]);
+            cb.grow(pc[p]);
+        }
+    }
+
+    // Splits [lo, hi) by binned SAH over all three axes at once; returns the
+    // split point, or hi for a leaf. `nb` receives the node box.
+    uint32_t split(uint32_t lo, uint32_t hi, Box& nb, int parts) {
         const uint32_t n = hi - lo;
-        if (n <= 1) return hi;
         Box cb;
-        for (uint32_t k = lo; k < hi; ++k) cb.grow(&cen[3 * (size_t)order[k]]);
+        bounds(lo, hi, parts, nb, cb);
+        if (n <= 1) return hi;
+        float scale[3];
+        for (int a = 0; a < 3; ++a) scale[a] = cb.hi[a] > cb.lo[a] ? BINS / (cb.hi[a] - cb.lo[a]) : 0.0f;
+        auto bin_of = [&](const Prim& p, int a) {
+            return std::min(BINS - 1, (int)((p.c[a] - cb.lo[a]) * scale[a]));
+        };
+        Bins local;
+        std::vector<Bins> pb(parts > 1 ? parts : 0);
+        parallel_ranges(lo, hi, parts, [&](uint32_t a0, uint32_t b0, int p) {
+            Bins& B = parts > 1 ? pb[p] : local;
+            for (uint32_t k = a0; k < b0; ++k) {
+                const Prim& q = prims[k];
+                for (int a = 0; a < 3; ++a) {
+                    if (scale[a] == 0.0f) continue;
+                    const int b = bin_of(q, a);
+                    grow(B.bb[a][b], q);
+                    ++B.bc[a][b];
+                }
+            }
+        });
+        if (parts > 1) {
+            local = pb[0];
+            for (int p = 1; p < parts; ++p) local.merge(pb[p]);
+        }
+        const Bins& B = local;
         float best = INFINITY;
         int bestAxis = -1, bestBin = 0;
         for (int a = 0; a < 3; ++a) {
-            float c0 = cb.lo[a], c1 = cb.hi[a];
-            if (!(c1 > c0)) continue;
-            const float scale = BINS / (c1 - c0);
-            Box bb[BINS];
-            uint32_t bc[BINS] = {};
-            for (uint32_t k = lo; k < hi; ++k) {
-                uint32_t i = order[k];
-                int b = std::min(BINS - 1, (int)((cen[3 * (size_t)i + a] - c0) * scale));
-                bb[b].grow(item_box(i));
-                ++bc[b];
-            }
+            if (scale[a] == 0.0f) continue;
             float la[BINS];
             uint32_t lc[BINS];
             Box L;
             uint32_t ln = 0;
             for (int b = 0; b < BINS - 1; ++b) {
-                L.grow(bb[b]);
-                ln += bc[b];
+                L.grow(B.bb[a][b]);
+                ln += B.bc[a][b];
                 la[b] = L.area();
                 lc[b] = ln;
             }
             Box R;
             uint32_t rn = 0;
             for (int b = BINS - 1; b > 0; --b) {
-                R.grow(bb[b]);
-                rn += bc[b];
+                R.grow(B.bb[a][b]);
+                rn += B.bc[a][b];
                 if (lc[b - 1] == 0 || rn == 0) continue;
-                float cost = la[b - 1] * lc[b - 1] + R.area() * rn;
+                const float cost = la[b - 1] * lc[b - 1] + R.area() * rn;
                 if (cost < best) {
                     best = cost;
                     bestAxis = a;
@@ -116,41 +202,117 @@ struct Builder {
         if (n <= maxLeaf && (bestAxis < 0 || best + nb.area() >= leafCost)) return hi;
         uint32_t mid = lo + n / 2;
         if (bestAxis >= 0) {
-            const float c0 = cb.lo[bestAxis], scale = BINS / (cb.hi[bestAxis] - c0);
-            auto it = std::partition(order.begin() + lo, order.begin() + hi, [&](uint32_t i) {
-                return std::min(BINS - 1, (int)((cen[3 * (size_t)i + bestAxis] - c0) * scale)) < bestBin;
-            });
-            mid = (uint32_t)(it - order.begin());
+            auto it = std::partition(prims.begin() + lo, prims.begin() + hi,
+                                     [&](const Prim& q) { return bin_of(q, bestAxis) < bestBin; });
+            mid = (uint32_t)(it - prims.begin());
         }
-        if (mid == lo || mid == hi) {  // coincident centroids: split by index
-            mid = lo + n / 2;
-        }
+        if (mid == lo || mid == hi) mid = lo + n / 2;  // coincident centroids: split by index
         return mid;
     }
 
-    void build(uint32_t n) {
+    // The subtree of [lo, hi) into T, rooted at T's node `root`.
+    void build_subtree(Nodes& T, uint32_t root, uint32_t lo, uint32_t hi) {
         struct Task { uint32_t lo, hi, node; };
-        std::vector<Task> st;
-        uint32_t root = make_node();
-        st.push_back({0, n, root});
+        std::vector<Task> st{{lo, hi, root}};
         while (!st.empty()) {
-            Task t = st.back();
+            const Task t = st.back();
             st.pop_back();
             Box nb;
-            for (uint32_t k = t.lo; k < t.hi; ++k) nb.grow(item_box(order[k]));
-            nodeBox[t.node] = nb;
-            uint32_t mid = split(t.lo, t.hi, nb);
+            const uint32_t mid = split(t.lo, t.hi, nb, 1);
+            T.box[t.node] = nb;
             if (mid >= t.hi) {
-                first[t.node] = t.lo;
-                count[t.node] = t.hi - t.lo;
+                T.first[t.node] = t.lo;
+                T.count[t.node] = t.hi - t.lo;
                 continue;
             }
-            uint32_t l = make_node(), r = make_node();
-            left[t.node] = l;
-            right[t.node] = r;
+            const uint32_t l = T.make(), r = T.make();
+            T.left[t.node] = l;
+            T.right[t.node] = r;
             st.push_back({mid, t.hi, r});
             st.push_back({t.lo, mid, l});
         }
+    }
+
+    // Large trees: the top splits run one at a time with parallel binning until
+    // there are enough independent ranges, then every range's subtree is built
+    // on its own thread and stitched in (node indices renumbered).
+    void build(uint32_t n) {
+        const int threads = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+        const uint32_t root = N.make();
+        if (n < 65536 || threads == 1) {
+            build_subtree(N, root, 0, n);
+        } else {
+            struct Task { uint32_t lo, hi, node; };
+            std::vector<Task> pending{{0, n, root}}, ready;
+            while (!pending.empty()) {
+                size_t big = 0;
+                for (size_t k = 1; k < pending.size(); ++k)
+                    if (pending[k].hi - pending[k].lo > pending[big].hi - pending[big].lo) big = k;
+                const Task t = pending[big];
+                if (pending.size() + ready.size() >= (size_t)8 * threads || t.hi - t.lo < 32768) break;
+                pending.erase(pending.begin() + (long)big);
+                Box nb;
+                const int parts = t.hi - t.lo >= 262144 ? threads : 1;
+                const uint32_t mid = split(t.lo, t.hi, nb, parts);
+                N.box[t.node] = nb;
+                if (mid >= t.hi) {
+                    N.first[t.node] = t.lo;
+                    N.count[t.node] = t.hi - t.lo;
+                    continue;
+                }
+                const uint32_t l = N.make(), r = N.make();
+                N.left[t.node] = l;
+                N.right[t.node] = r;
+                pending.push_back({t.lo, mid, l});
+                pending.push_back({mid, t.hi, r});
+            }
+            ready.insert(ready.end(), pending.begin(), pending.end());
+            std::vector<Nodes> sub(ready.size());
+            std::atomic<size_t> next{0};
+            std::vector<std::thread> ts;
+            for (int w = 0; w < threads; ++w)
+                ts.emplace_back([&] {
+                    for (size_t k; (k = next.fetch_add(1)) < ready.size();) {
+                        sub[k].make();
+                        build_subtree(sub[k], 0, ready[k].lo, ready[k].hi);
+                    }
+                });
+            for (auto& t : ts) t.join();
+            // subtree k's nodes 1.. land at base[k] ..; its node 0 is the task's node
+            std::vector<size_t> base(ready.size() + 1);
+            base[0] = N.size();
+            for (size_t k = 0; k < ready.size(); ++k) base[k + 1] = base[k] + sub[k].size() - 1;
+            const size_t total = base[ready.size()];
+            N.box.resize(total);
+            N.left.resize(total);
+            N.right.resize(total);
+            N.first.resize(total);
+            N.count.resize(total);
+            next = 0;
+            ts.clear();
+            for (int w = 0; w < threads; ++w)
+                ts.emplace_back([&] {
+                    for (size_t k; (k = next.fetch_add(1)) < ready.size();) {
+                        const Nodes& T = sub[k];
+                        const uint32_t node = ready[k].node;
+                        const size_t b0 = base[k];
+                        auto map = [&](uint32_t j) { return j == 0 ? node : (uint32_t)(b0 + j - 1); };
+                        for (size_t j = 0; j < T.size(); ++j) {
+                            const size_t d = j == 0 ? node : b0 + j - 1;
+                            N.box[d] = T.box[j];
+                            N.first[d] = T.first[j];
+                            N.count[d] = T.count[j];
+                            N.left[d] = T.count[j] ? 0u : map(T.left[j]);
+                            N.right[d] = T.count[j] ? 0u : map(T.right[j]);
+                        }
+                    }
+                });
+            for (auto& t : ts) t.join();
+        }
+        order.resize(n);
+        for (uint32_t k = 0; k < n; ++k) order[k] = prims[k].id;
+        prims.clear();
+        prims.shrink_to_fit();
     }
 };
 
@@ -170,19 +332,13 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
     }
     if (n >= (1u << 24)) return false;
     Builder B;
-    B.boxes = boxes;
-    B.cen.resize(3 * (size_t)n);
-    B.order.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (int a = 0; a < 3; ++a) B.cen[3 * (size_t)i + a] = 0.5f * (boxes[6 * (size_t)i + a] + boxes[6 * (size_t)i + 3 + a]);
-        B.order[i] = i;
-    }
+    B.init(boxes, n);
     B.build(n);
 
     // leaves: items ordered by slot, so consecutive tests reuse the local ray
-    for (size_t v = 0; v < B.count.size(); ++v) {
-        if (B.count[v] == 0) continue;
-        std::stable_sort(B.order.begin() + B.first[v], B.order.begin() + B.first[v] + B.count[v],
+    for (size_t v = 0; v < B.N.count.size(); ++v) {
+        if (B.N.count[v] == 0) continue;
+        std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
                          [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
     }
     out.items.resize(2 * (size_t)n);
@@ -192,7 +348,7 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
     }
 
     // pair nodes: one per interior tree node, numbered in pre-order
-    const size_t total = B.nodeBox.size();
+    const size_t total = B.N.box.size();
     std::vector<uint32_t> pairIndex(total, ENTRY_NONE);
     std::vector<uint32_t> depth(total, 0);
     uint32_t pairs = 0, maxDepth = 0;
@@ -202,33 +358,33 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
             uint32_t v = st.back();
             st.pop_back();
             maxDepth = std::max(maxDepth, depth[v]);
-            if (B.count[v]) continue;
+            if (B.N.count[v]) continue;
             pairIndex[v] = pairs++;
-            depth[B.left[v]] = depth[B.right[v]] = depth[v] + 1;
-            st.push_back(B.right[v]);
-            st.push_back(B.left[v]);
+            depth[B.N.left[v]] = depth[B.N.right[v]] = depth[v] + 1;
+            st.push_back(B.N.right[v]);
+            st.push_back(B.N.left[v]);
         }
     }
     auto entry = [&](uint32_t v) -> uint32_t {
-        if (B.count[v] == 0) return pairIndex[v];
-        return ENTRY_LEAF | (B.count[v] << 24) | B.first[v];
+        if (B.N.count[v] == 0) return pairIndex[v];
+        return ENTRY_LEAF | (B.N.count[v] << 24) | B.N.first[v];
     };
     out.nodes.assign(16 * (size_t)pairs, 0u);
     for (size_t v = 0; v < total; ++v) {
-        if (B.count[v]) continue;
+        if (B.N.count[v]) continue;
         uint32_t* q = out.nodes.data() + 16 * (size_t)pairIndex[v];
-        const Box& a = B.nodeBox[B.left[v]];
-        const Box& b = B.nodeBox[B.right[v]];
+        const Box& a = B.N.box[B.N.left[v]];
+        const Box& b = B.N.box[B.N.right[v]];
         q[0] = fbits(a.lo[0]); q[1] = fbits(a.hi[0]); q[2] = fbits(a.lo[1]); q[3] = fbits(a.hi[1]);
         q[4] = fbits(b.lo[0]); q[5] = fbits(b.hi[0]); q[6] = fbits(b.lo[1]); q[7] = fbits(b.hi[1]);
         q[8] = fbits(a.lo[2]); q[9] = fbits(a.hi[2]); q[10] = fbits(b.lo[2]); q[11] = fbits(b.hi[2]);
-        q[12] = entry(B.left[v]);
-        q[13] = entry(B.right[v]);
+        q[12] = entry(B.N.left[v]);
+        q[13] = entry(B.N.right[v]);
     }
     out.root = entry(0);
     out.depth = maxDepth;
-    std::memcpy(out.rootBox, B.nodeBox[0].lo, 12);
-    std::memcpy(out.rootBox + 3, B.nodeBox[0].hi, 12);
+    std::memcpy(out.rootBox, B.N.box[0].lo, 12);
+    std::memcpy(out.rootBox + 3, B.N.box[0].hi, 12);
     return true;
 }
 
@@ -261,17 +417,11 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     if (n >= (1u << 24)) return false;
     Builder B;
     B.maxLeaf = WIDE_LEAF_MAX;
-    B.boxes = boxes;
-    B.cen.resize(3 * (size_t)n);
-    B.order.resize(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        for (int a = 0; a < 3; ++a) B.cen[3 * (size_t)i + a] = 0.5f * (boxes[6 * (size_t)i + a] + boxes[6 * (size_t)i + 3 + a]);
-        B.order[i] = i;
-    }
+    B.init(boxes, n);
     B.build(n);
-    for (size_t v = 0; v < B.count.size(); ++v) {
-        if (B.count[v] == 0) continue;
-        std::stable_sort(B.order.begin() + B.first[v], B.order.begin() + B.first[v] + B.count[v],
+    for (size_t v = 0; v < B.N.count.size(); ++v) {
+        if (B.N.count[v] == 0) continue;
+        std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
                          [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
     }
 
@@ -284,30 +434,30 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
         maxDepth = std::max(maxDepth, t.depth);
         // children: open the largest interior child until eight (a leaf root is its own child)
         std::vector<uint32_t> kids;
-        if (B.count[t.v]) kids.push_back(t.v);
-        else { kids.push_back(B.left[t.v]); kids.push_back(B.right[t.v]); }
+        if (B.N.count[t.v]) kids.push_back(t.v);
+        else { kids.push_back(B.N.left[t.v]); kids.push_back(B.N.right[t.v]); }
         while (kids.size() < 8) {
             int best = -1;
             float bestArea = -1.0f;
             for (size_t k = 0; k < kids.size(); ++k)
-                if (B.count[kids[k]] == 0 && B.nodeBox[kids[k]].area() > bestArea) {
-                    bestArea = B.nodeBox[kids[k]].area();
+                if (B.N.count[kids[k]] == 0 && B.N.box[kids[k]].area() > bestArea) {
+                    bestArea = B.N.box[kids[k]].area();
                     best = (int)k;
                 }
             if (best < 0) break;
             uint32_t v = kids[best];
-            kids[best] = B.left[v];
-            kids.push_back(B.right[v]);
+            kids[best] = B.N.left[v];
+            kids.push_back(B.N.right[v]);
         }
         // slots by octant: slot bit a set = the child lies toward +a of the node centre
         Box nb;
-        for (uint32_t k : kids) nb.grow(B.nodeBox[k]);
+        for (uint32_t k : kids) nb.grow(B.N.box[k]);
         float ctr[3];
         for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
         struct Cand { float cost; int kid, slot; };
         std::vector<Cand> cands;
         for (size_t k = 0; k < kids.size(); ++k) {
-            const Box& b = B.nodeBox[kids[k]];
+            const Box& b = B.N.box[kids[k]];
             for (int s = 0; s < 8; ++s) {
                 float c = 0.0f;
                 for (int a = 0; a < 3; ++a) {
@@ -342,7 +492,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
             for (int a = 0; a < 3; ++a) { q[a][s] = 255; q[3 + a][s] = 0; }  // empty slots
             if (slotKid[s] < 0) continue;
             const uint32_t v = kids[slotKid[s]];
-            const Box& b = B.nodeBox[v];
+            const Box& b = B.N.box[v];
             for (int a = 0; a < 3; ++a) {
                 const double sc = std::ldexp(1.0, ex[a] - 127);
                 double lo = std::floor(((double)b.lo[a] - (double)nb.lo[a]) / sc);
@@ -350,16 +500,16 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                 q[a][s] = (uint8_t)std::min(255.0, std::max(0.0, lo));
                 q[3 + a][s] = (uint8_t)std::min(255.0, std::max(0.0, hi));
             }
-            if (B.count[v] == 0) {
+            if (B.N.count[v] == 0) {
                 imask |= 1u << s;
                 meta[s] = (uint8_t)((1u << 5) | (24u + s));
                 queue.push_back({v, 0, t.depth + 1});  // node index assigned below, in slot order
             } else {
-                const uint32_t cnt = B.count[v];
+                const uint32_t cnt = B.N.count[v];
                 meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
                 for (uint32_t k = 0; k < cnt; ++k) {
-                    out.items.push_back(itemTri[B.order[B.first[v] + k]]);
-                    out.items.push_back(itemSlot[B.order[B.first[v] + k]]);
+                    out.items.push_back(itemTri[B.order[B.N.first[v] + k]]);
+                    out.items.push_back(itemSlot[B.order[B.N.first[v] + k]]);
                 }
                 itemOff += cnt;
             }

@@ -302,6 +302,127 @@ def atrium_motion(scene: SceneDesc, frame: int, seed: int = 7):
     return mats, Pn.astype(np.float32)
 
 
+LARGE_ARCHETYPE_TRIS = (2_000, 9_000, 40_000, 120_000, 230_000, 500_000, 600_000, 600_000)
+LARGE_INSTANCES = (220, 110, 45, 1, 12, 5, 4, 3)   # 400 instances; archetype 3 is the skinned mesh
+LARGE_BONES = 8
+
+
+def skinned_tube(n_tris: int, rng, bones: int = LARGE_BONES, height: float = 12.0, radius: float = 1.2):
+    """A closed tube along +y with a chain of `bones` joints at even heights:
+    per vertex the two nearest joints and a linear weight between them."""
+    sides = 24
+    nu, nv = _dims_for(n_tris, aspect=sides / 8.0)
+
+    def fn(u, v):
+        a = u * 2 * math.pi
+        r = radius * (1.0 + 0.08 * np.cos(a * 5) + 0.15 * np.sin(v * 9.0))
+        return r * np.cos(a), v * height, r * np.sin(a)
+    P, F = grid_mesh(nu, nv, fn)
+    F = F[:n_tris]
+    seg = height / bones
+    s = np.clip(P[:, 1] / seg - 0.5, 0.0, bones - 1.0)
+    b0 = np.floor(s).astype(np.int32)
+    b1 = np.minimum(b0 + 1, bones - 1)
+    w1 = (s - b0).astype(np.float32)
+    joints = np.array([[0.0, seg * (j + 0.5), 0.0] for j in range(bones)], np.float64)
+    return P, F, dict(b0=b0, b1=b1, w1=w1, joints=joints)
+
+
+def skin(rest: np.ndarray, rig: dict, angles: np.ndarray) -> np.ndarray:
+    """Linear blend skinning of the tube: joint j rotates its subchain by
+    angles[j] (axis-angle vectors, radians) about the joint; each vertex blends
+    the world transforms of its two joints."""
+    J = rig["joints"]
+    n = J.shape[0]
+    Rw = [np.eye(3)]
+    tw = [np.zeros(3)]
+    R_acc, t_acc = np.eye(3), np.zeros(3)
+    mats = []
+    for j in range(n):
+        ang = float(np.linalg.norm(angles[j]))
+        Rj = _rot(angles[j] / ang, ang) if ang > 0 else np.eye(3)
+        # rotation about joint j applied after the parent chain
+        pj = R_acc @ J[j] + t_acc
+        R_acc = Rj @ R_acc
+        t_acc = Rj @ (t_acc - pj) + pj
+        mats.append((R_acc.copy(), t_acc.copy()))
+    P = rest.astype(np.float64)
+    out = np.empty_like(P)
+    w1 = rig["w1"].astype(np.float64)[:, None]
+    for j in range(n):
+        R, t = mats[j]
+        Q = P @ R.T + t
+        m0 = rig["b0"] == j
+        m1 = rig["b1"] == j
+        out[m0] = Q[m0] * (1.0 - w1[m0])
+        # second joint's share added below
+    for j in range(n):
+        R, t = mats[j]
+        m1 = rig["b1"] == j
+        out[m1] += (P[m1] @ R.T + t) * w1[m1]
+    return out.astype(np.float32)
+
+
+def large_scene(seed: int = 4):
+    """The large workload: 8 archetypes of 2k-600k triangles (2.1M unique),
+    400 instances scattered over a 160 x 40 x 160 m world, archetype 3 a
+    120k-triangle skinned tube (one instance) refit every frame, 64 point
+    lights (clustered), 32^3 probes x 256 rays."""
+    rng = np.random.default_rng(seed)
+    W, Hh, D = 160.0, 40.0, 160.0
+    n_materials = 32
+    mats = [material_record(rng.uniform(0.05, 0.95, 3), side=2) for _ in range(n_materials)]
+    meshes, instances = [], []
+    rig = None
+    for a, n in enumerate(LARGE_ARCHETYPE_TRIS):
+        if a == 3:
+            P, F, rig = skinned_tube(int(n), rng)
+        elif a in (6, 7):
+            P, F = floor_slab(int(n), rng, w=W if a == 6 else 40.0, d=D if a == 6 else 40.0)
+        elif a == 5:
+            P, F = arched_panel(int(n), rng, w=30.0, h=20.0)
+        elif a in (2, 4):
+            P, F = column_prism(int(n), rng)
+        else:
+            P, F = arched_panel(int(n), rng) if a == 1 else column_prism(int(n), rng)
+        assert F.shape[0] == n, (a, F.shape[0], n)
+        meshes.append(Mesh(P, F, np.full(F.shape[0], int(rng.integers(n_materials)), np.uint32)))
+    skinned_instance = -1
+    for a, count in enumerate(LARGE_INSTANCES):
+        for k in range(count):
+            if a == 6 and k == 0:
+                m = trs((W / 2, 0.0, D / 2))  # the ground
+            else:
+                s = float(rng.uniform(0.6, 1.6)) if a not in (6, 7) else 1.0
+                t = (rng.uniform(4, W - 4), rng.uniform(0.0, 2.0) if a in (6, 7) else 0.0, rng.uniform(4, D - 4))
+                m = trs(t, _rot((0, 1, 0), rng.uniform(0, 2 * math.pi)), s)
+            if a == 3:
+                skinned_instance = len(instances)
+            instances.append(Instance(a, m))
+    lights = []
+    for _ in range(64):
+        lights.append(light_record(1, pos=(rng.uniform(2, W - 2), rng.uniform(1.0, Hh - 2), rng.uniform(2, D - 2)),
+                                   intensity=float(rng.uniform(40, 200)), range_=float(rng.uniform(10, 24)),
+                                   decay=2.0))
+    grid = dict(gridMin=(2.0, 0.5, 2.0), gridSize=(W - 4.0, Hh - 1.0, D - 4.0), res=(32, 32, 32), rays=256)
+    return SceneDesc(meshes, instances, np.stack(mats), np.stack(lights), name="large",
+                     meta=dict(grid=grid, clustered=True, hysteresis=0.97, jitter="gated", seed=seed,
+                               skinned=3, skinnedInstance=skinned_instance, rig=rig))
+
+
+def large_pose(scene: SceneDesc, frame: int, seed: int = 11, max_deg: float = 15.0) -> np.ndarray:
+    """Skinned positions of the large scene's tube for `frame`: every joint
+    rotated by a random axis and an angle of at most `max_deg` degrees."""
+    rng = np.random.default_rng(seed * 1_000_003 + frame)
+    rig = scene.meta["rig"]
+    n = rig["joints"].shape[0]
+    axes = rng.normal(size=(n, 3))
+    axes /= np.linalg.norm(axes, axis=1, keepdims=True)
+    ang = np.radians(rng.uniform(0.0, max_deg, n))
+    rest = scene.meta.setdefault("restPositions", scene.meshes[scene.meta["skinned"]].positions.copy())
+    return skin(rest, rig, axes * ang[:, None])
+
+
 BATCH_SCENE_TRIS = (20_000, 45_000, 80_000, 120_000, 200_000, 262_000, 350_000, 500_000)
 
 
