@@ -127,7 +127,7 @@ class ProbeField:
         self._pendingTopology = False
         self._deformVersions = {}
         self._staging = {}
-        self._cascades = {}  # extra cascade boxes (ci >= 1) configured by configureCascade
+        self._extraCascades = {}  # extra cascade boxes (ci >= 1) configured by configureCascade
         self._params = _abi.default_params()
         self._params.hysteresis = self._hysteresis
         self._frameJitterOverride = None
@@ -281,10 +281,10 @@ class ProbeField:
         g.maxDist = float(np.linalg.norm(gs))
         g.cellMin = float(max(1e-4, min(gs[a] / max(1, g.res[a] - 1) for a in range(3))))
         self._ck(self._lib.sb_configure_cascade(self._ctx, ci, C.byref(g)))
-        self._cascades[ci] = g
+        self._extraCascades[ci] = g
 
     def cascadeProbes(self, ci: int) -> int:
-        g = self._grid if ci == 0 else self._cascades[ci]
+        g = self._grid if ci == 0 else self._extraCascades[ci]
         return int(g.res[0] * g.res[1] * g.res[2])
 
     def _refresh_lanes(self):

@@ -35,7 +35,7 @@ def _fields():
 
 
 def _state(f, ci):
-    g = f.grid if ci == 0 else f._cascades[ci]
+    g = f.grid if ci == 0 else f._extraCascades[ci]
     P = g.res[0] * g.res[1] * g.res[2]
     n = P * g.raysPerProbe
     W, H = g.res[0] * 8, g.res[1] * g.res[2] * 8
