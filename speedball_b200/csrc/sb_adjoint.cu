@@ -241,20 +241,21 @@ __global__ void __launch_bounds__(BWD_THREADS) k_blend_bwd(DevCascade C, DevPara
         S.texDir[tid] = make_float4(d.x, d.y, d.z, 0.0f);
     }
     float sr = 0.f, sg = 0.f, sb = 0.f, sl = 0.f, sl2 = 0.f, ws = 0.f;
+    float cr = 0.f, cg = 0.f, cb = 0.f, cl = 0.f, cl2 = 0.f, cws = 0.f;
     for (uint32_t c = 0; c < N; c += BWD_CHUNK) {
         const uint32_t n = min((uint32_t)BWD_CHUNK, N - c);
         __syncthreads();
         bwd_stage(S, C, P, rays, p, c, n, cosPow, cosUnit);
         if (tid < 36) {
-            for (uint32_t k = 0; k < n; ++k) {
+            for (uint32_t k = 0; k < n; ++k) {  // the forward's compensated sums, same order
                 float w = S.wc[k][tid];
                 float4 a = S.fa[k];
-                sr = fmaf(w, a.x, sr);
-                sg = fmaf(w, a.y, sg);
-                sb = fmaf(w, a.z, sb);
-                sl = fmaf(w, a.w, sl);
-                sl2 = fmaf(w, a.w * a.w, sl2);
-                ws += w;
+                kahan_fma(sr, cr, w, a.x);
+                kahan_fma(sg, cg, w, a.y);
+                kahan_fma(sb, cb, w, a.z);
+                kahan_fma(sl, cl, w, a.w);
+                kahan_fma(sl2, cl2, w, a.w * a.w);
+                kahan_fma(ws, cws, w, 1.0f);
             }
         }
     }

@@ -16,8 +16,8 @@ namespace sb {
 // reuses it; per (texel, ray) the loop is then 9 FMA/ADD on shared operands.
 // Per-ray features (radiance, luma, luma^2, hit distance, distance^2) are also
 // formed once per ray instead of once per (texel, ray). Sums run in ray order
-// in FP32; every term is non-negative, so the relative error of a sum stays
-// under rays * 2^-24 (1.5e-5 at 256 rays).
+// in FP32 with per-texel Kahan compensation (kahan_fma), so each of the nine
+// moments carries about 2 ulp of error whatever the ray count.
 constexpr int BLEND_PROBES = 8;
 constexpr int BLEND_TEXELS = OCT * OCT;
 constexpr int BLEND_THREADS = BLEND_PROBES * BLEND_TEXELS;  // 288 = 9 warps
@@ -37,6 +37,7 @@ struct BlendSmem {
     } u;
     float4 irr[BLEND_PROBES][BLEND_TEXELS];
     float2 dep[BLEND_PROBES][BLEND_TEXELS];
+    float wsum[BLEND_TEXELS], dwsum[BLEND_TEXELS];  // weight sums: the same for every probe
 };
 
 // Blend + upload of probe slots [block * BLEND_PROBES, + BLEND_PROBES) of one
@@ -61,6 +62,7 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
     }
 
     float sr = 0.f, sg = 0.f, sb = 0.f, sl = 0.f, sl2 = 0.f, ws = 0.f, sd = 0.f, sd2 = 0.f, dws = 0.f;
+    float cr = 0.f, cg = 0.f, cb = 0.f, cl = 0.f, cl2 = 0.f, cws = 0.f, cd = 0.f, cd2 = 0.f, cdw = 0.f;
     for (uint32_t c = 0; c < N; c += BLEND_CHUNK) {
         const uint32_t n = min((uint32_t)BLEND_CHUNK, N - c);
         __syncthreads();  // previous pass done with the table and features
@@ -104,19 +106,28 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
             for (uint32_t k = 0; k < n; ++k) {
                 float w = S.wc[k][lane], v = S.wd[k][lane];
                 float4 a = S.u.f.fa[p][k], b = S.u.f.fb[p][k];
-                sr = fmaf(w, a.x, sr);
-                sg = fmaf(w, a.y, sg);
-                sb = fmaf(w, a.z, sb);
-                sl = fmaf(w, a.w, sl);
-                sl2 = fmaf(w, b.x, sl2);
-                ws += w;
-                sd = fmaf(v, b.y, sd);
-                sd2 = fmaf(v, b.z, sd2);
-                dws += v;
+                kahan_fma(sr, cr, w, a.x);
+                kahan_fma(sg, cg, w, a.y);
+                kahan_fma(sb, cb, w, a.z);
+                kahan_fma(sl, cl, w, a.w);
+                kahan_fma(sl2, cl2, w, b.x);
+                kahan_fma(sd, cd, v, b.y);
+                kahan_fma(sd2, cd2, v, b.z);
             }
+            if (p == 0)  // the weight sums depend on (texel, ray) only: the first probe's lanes form them
+                for (uint32_t k = 0; k < n; ++k) {
+                    kahan_fma(ws, cws, S.wc[k][lane], 1.0f);
+                    kahan_fma(dws, cdw, S.wd[k][lane], 1.0f);
+                }
         }
     }
-    __syncthreads();  // features no longer read: S.u.out may be written
+    if (p == 0) {
+        S.wsum[lane] = ws;
+        S.dwsum[lane] = dws;
+    }
+    __syncthreads();  // features no longer read: S.u.out may be written; weight sums published
+    ws = S.wsum[lane];
+    dws = S.dwsum[lane];
 
     const uint32_t probeIndex = live ? (C.probeOffset + slot) % C.probeTotal : 0u;
     if (live) {

@@ -1603,13 +1603,12 @@ sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* src, const double* w
         }
         CK(cudaMemcpyAsync(ctx->dStage, src, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemcpyAsync(ctx->dStageM, world16, (size_t)count * 128, cudaMemcpyHostToDevice, ctx->stream));
-        CK(launch_update_instances(ctx->B, ctx->I, ctx->dStage, ctx->dStageM, count, 1, ctx->dErr, ctx->stream));
+        CK(launch_update_refit_tlas(ctx->B, ctx->I, ctx->dStage, ctx->dStageM, count, 1, ctx->dErr, ctx->stream));
         for (uint32_t i = 0; i < count; ++i) ctx->flat.mark_source(src[i]);  // moved: out of the scene BVH
     } else {
         // rewriteInstanceRows:false — bounds from the (refit) BLAS roots
-        CK(launch_update_instances(ctx->B, ctx->I, nullptr, nullptr, 0, 0, ctx->dErr, ctx->stream));
+        CK(launch_update_refit_tlas(ctx->B, ctx->I, nullptr, nullptr, 0, 0, ctx->dErr, ctx->stream));
     }
-    CK(launch_tlas_refit(ctx->B, ctx->I, ctx->dErr, ctx->stream));
     return SB_OK;
 }
 

@@ -110,6 +110,10 @@ cudaError_t launch_update_instances(const SceneBuffers& B, const InstanceTable& 
                                     const double* world16, uint32_t count, int rewriteRows, uint32_t* err,
                                     cudaStream_t st);
 cudaError_t launch_tlas_refit(const SceneBuffers& B, const InstanceTable& I, uint32_t* err, cudaStream_t st);
+// launch_update_instances followed by launch_tlas_refit, as one single-CTA launch.
+cudaError_t launch_update_refit_tlas(const SceneBuffers& B, const InstanceTable& I, const uint32_t* srcList,
+                                     const double* world16, uint32_t count, int rewriteRows, uint32_t* err,
+                                     cudaStream_t st);
 cudaError_t launch_tlas_index(const SceneBuffers& B, const InstanceTable& I, uint32_t* owner, uint32_t* err,
                               cudaStream_t st);
 

@@ -23,6 +23,16 @@ __device__ __forceinline__ float luma3(float3 c) { return c.x * 0.2126f + c.y * 
 __device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
 __device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 
+// Compensated (Kahan) accumulation s += w * x: the product enters through one
+// FMA with the running compensation c, and c keeps the low part that the
+// addition to s loses. The compiler does not reassociate these (no fast-math).
+__device__ __forceinline__ void kahan_fma(float& s, float& c, float w, float x) {
+    const float y = fmaf(w, x, -c);
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
 // ---- double-float (unevaluated sum hi + lo) arithmetic from FP32 error-free
 // transformations (Knuth two-sum, FMA two-product; Dekker 1971). Used where
 // FP32 alone would miss the FP64 tolerances: ray angles and the final hit t.

@@ -504,8 +504,9 @@ cudaError_t launch_update_instances(const SceneBuffers& B, const InstanceTable& 
     return cudaGetLastError();
 }
 
-// refitFlatTlasRange over the frozen partition, deepest level first.
-__global__ void __launch_bounds__(1024) k_tlas_refit(SceneBuffers B, InstanceTable I) {
+// refitFlatTlasRange over the frozen partition, deepest level first (the
+// body of one CTA; the caller's writes to liveBounds precede a barrier).
+__device__ __forceinline__ void tlas_refit_body(const SceneBuffers& B, const InstanceTable& I) {
     const uint32_t nn = B.tlasNodeCount;
     const int maxDepth = (int)*(volatile uint32_t*)I.scratch;
     for (int d = maxDepth; d >= 0; --d) {
@@ -553,6 +554,29 @@ __global__ void __launch_bounds__(1024) k_tlas_refit(SceneBuffers B, InstanceTab
     }
 }
 
+__global__ void __launch_bounds__(1024) k_tlas_refit(SceneBuffers B, InstanceTable I) { tlas_refit_body(B, I); }
+
+// The transform lane in one CTA: the listed (or every) source instance's rows
+// and bounds, then the TLAS refit over them, with one launch.
+__global__ void __launch_bounds__(512) k_update_refit_tlas(SceneBuffers B, InstanceTable I, const uint32_t* srcList,
+                                                            const double* world16, uint32_t count, int rewriteRows,
+                                                            uint32_t* err) {
+    const uint32_t total = srcList ? count : I.count;
+    for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) {
+        const uint32_t src = srcList ? srcList[i] : i;
+        if (src >= I.count) {
+            latch(err, ERR_LAYOUT);
+            continue;
+        }
+        if (srcList && world16)
+            for (int k = 0; k < 16; ++k) I.world[(size_t)src * 16u + k] = world16[(size_t)i * 16u + k];
+        compute_instance(B, I, src, err);
+        write_slot(B, I, I.slotOf[src], src, rewriteRows != 0);
+    }
+    __syncthreads();
+    tlas_refit_body(B, I);
+}
+
 // Depth of every TLAS node and the refit-index checks of
 // createFlatTlasRefitIndex (gi_refit.js:298-346); one thread, structural
 // changes only.
@@ -593,6 +617,13 @@ __global__ void k_tlas_index(SceneBuffers B, InstanceTable I, uint32_t* owner, u
     for (uint32_t s = 0; s < ic; ++s)
         if (owner[s] == NONE) { latch(err, ERR_LAYOUT); return; }
     *I.scratch = maxD;
+}
+
+cudaError_t launch_update_refit_tlas(const SceneBuffers& B, const InstanceTable& I, const uint32_t* srcList,
+                                     const double* world16, uint32_t count, int rewriteRows, uint32_t* err,
+                                     cudaStream_t st) {
+    k_update_refit_tlas<<<1, 512, 0, st>>>(B, I, srcList, world16, count, rewriteRows, err); note_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tlas_refit(const SceneBuffers& B, const InstanceTable& I, uint32_t* err, cudaStream_t st) {
