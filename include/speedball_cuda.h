@@ -369,6 +369,9 @@ typedef struct sb_tuning {
                                  boxes for closest hits + binary for any hits
                                  (default); 2 = binary only.
                                  0 = the reference's TLAS + BLASes                */
+    uint32_t smemWideNodes;   /* bvhKind 1: the first (top-level) 8-wide nodes staged
+                                 in shared memory per CTA of the closest-hit stage,
+                                 80 bytes each (0 = none, at most 512)             */
 } sb_tuning;
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);

@@ -111,7 +111,7 @@ class sb_grads(C.Structure):
 
 class sb_tuning(C.Structure):
     _fields_ = [("traceBlock", C.c_uint32), ("sortKey", C.c_uint32), ("smemTlasNodes", C.c_uint32),
-                ("bvhKind", C.c_uint32)]
+                ("bvhKind", C.c_uint32), ("smemWideNodes", C.c_uint32)]
 
 
 class sb_stats(C.Structure):

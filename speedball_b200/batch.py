@@ -84,7 +84,8 @@ def autotune(field: ProbeField, cascade: int = 0) -> dict:
     tunings for its scene, kept on its context; the probe state is restored."""
     t = _abi.sb_tuning()
     _abi.check(field._lib.sb_autotune(field.ctx, cascade, C.byref(t)), field.ctx)
-    return dict(traceBlock=t.traceBlock, sortKey=t.sortKey, smemTlasNodes=t.smemTlasNodes, bvhKind=t.bvhKind)
+    return dict(traceBlock=t.traceBlock, sortKey=t.sortKey, smemTlasNodes=t.smemTlasNodes, bvhKind=t.bvhKind,
+                smemWideNodes=t.smemWideNodes)
 
 
 def autotuneBatch(items) -> dict:

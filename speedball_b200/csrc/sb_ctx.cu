@@ -1229,17 +1229,21 @@ sb_status sb_autotune(sb_ctx* ctx, uint32_t ci, sb_tuning* chosen) {
     const uint32_t probes = ctx->casc[ci].probeTotal;
     CascadeSnapshot snap;
     CK(snap.save(ctx, ci));
-    const sb_tuning saved{ctx->tune.block, ctx->tune.sortKey, ctx->tune.smemTlasNodes, ctx->bvhKind};
+    const sb_tuning saved{ctx->tune.block, ctx->tune.sortKey, ctx->tune.smemTlasNodes, ctx->bvhKind,
+                          ctx->tune.smemWideNodes};
     const bool savedCounters = ctx->countersOn;
     ctx->countersOn = false;
     sb_tuning best = saved;
     float bestMs = 3.4e38f;
     const uint32_t kinds[3] = {1u, 2u, 0u}, blocks[3] = {128u, 192u, 256u};
+    const uint32_t wideDepth[3] = {0u, 73u, 512u};  // none, the top three levels, 512 nodes
+    // shared-memory staging: the TLAS for the two-level walk, the top 8-wide nodes for kind 1
     for (uint32_t kind : kinds)
         for (uint32_t block : blocks)
             for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort)
-                for (uint32_t sm = 0; sm < (kind == 0 ? 2u : 1u) && s == SB_OK; ++sm) {
-                    sb_tuning t{block, sort, kind == 0 ? (sm ? 512u : 0u) : saved.smemTlasNodes, kind};
+                for (uint32_t sm = 0; sm < (kind == 0 ? 2u : kind == 1 ? 3u : 1u) && s == SB_OK; ++sm) {
+                    sb_tuning t{block, sort, kind == 0 ? (sm ? 512u : 0u) : saved.smemTlasNodes, kind,
+                                kind == 1 ? wideDepth[sm] : 0u};
                     if ((s = sb_set_tuning(ctx, &t)) != SB_OK) break;
                     float ms = 0.0f;
                     s = time_min(ctx, {ctx}, [&] { return sb_solve(ctx, ci, 0, probes); }, 3, ms);
@@ -1275,13 +1279,14 @@ sb_status sb_autotune_batch(const sb_solve_item* items, uint32_t count, sb_tunin
         for (sb_ctx* c : all) seen = seen || c == items[i].ctx;
         if (!seen) all.push_back(items[i].ctx);
     }
-    const sb_tuning saved{lead->tune.block, lead->tune.sortKey, lead->tune.smemTlasNodes, lead->bvhKind};
+    const sb_tuning saved{lead->tune.block, lead->tune.sortKey, lead->tune.smemTlasNodes, lead->bvhKind,
+                          lead->tune.smemWideNodes};
     sb_tuning best = saved;
     float bestMs = 3.4e38f;
     const uint32_t blocks[3] = {128u, 192u, 256u};
     for (uint32_t block : blocks)
         for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort) {
-            sb_tuning t{block, sort, saved.smemTlasNodes, saved.bvhKind};
+            sb_tuning t{block, sort, saved.smemTlasNodes, saved.bvhKind, saved.smemWideNodes};
             if ((s = sb_set_tuning(lead, &t)) != SB_OK) break;
             float ms = 0.0f;
             s = time_min(lead, all, [&] { return sb_solve_batch(items, count); }, 3, ms);
@@ -1667,6 +1672,7 @@ sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out) {
     out->sortKey = ctx->tune.sortKey;
     out->smemTlasNodes = ctx->tune.smemTlasNodes;
     out->bvhKind = ctx->bvhKind;
+    out->smemWideNodes = ctx->tune.smemWideNodes;
     return SB_OK;
 }
 
@@ -1675,7 +1681,10 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (t->traceBlock == 0 || t->traceBlock > 256 || t->traceBlock % 32)
         return fail(ctx, SB_ERR_INVALID_ARG, "traceBlock %u: multiple of 32 in [32,256]", t->traceBlock);
     if (t->bvhKind > 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
+    if (t->smemWideNodes > 512)
+        return fail(ctx, SB_ERR_INVALID_ARG, "smemWideNodes %u > 512 (80 bytes each)", t->smemWideNodes);
     if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
+    ctx->tune.smemWideNodes = t->smemWideNodes;
     ctx->bvhKind = t->bvhKind;
     ++ctx->structGen;
     ctx->tune.block = t->traceBlock;

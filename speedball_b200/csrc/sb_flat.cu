@@ -219,6 +219,7 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
                 if (e == cudaSuccess) e = cudaMemcpy(witems, wt.items.data(), wt.items.size() * 4, cudaMemcpyHostToDevice);
                 if (e != cudaSuccess) return e;
                 wideReady = true;
+                wideCount = (uint32_t)(wt.nodes.size() / flat::WIDE_WORDS);
             }
         }
         root = treeRoot;
@@ -273,6 +274,7 @@ void FlatScene::fill(DevScene& S) const {
     S.flatItems = on ? items : nullptr;
     S.wideNodes = on && wide && wideReady ? wnodes : nullptr;
     S.wideItems = on && wide && wideReady ? witems : nullptr;
+    S.wideNodeCount = on && wide && wideReady ? wideCount : 0u;
     S.flatRoot = on ? root : flat::ENTRY_NONE;
     S.slotSkip = on ? dSkip : nullptr;
     S.dynList = on ? dDyn : nullptr;

@@ -79,6 +79,7 @@ struct DevScene {
     const uint32_t* dynList;
     const float* slotBounds;   // world AABB per slot (the TLAS leaf bounds), or null
     uint32_t flatRoot, dynCount;
+    uint32_t wideNodeCount;    // nodes of the 8-wide tree (0 when it is not built)
     int32_t flatOn;
     uint32_t nodeCount, triCount, instCount, tlasNodeCount, materialCount;
     uint32_t lightCount;
@@ -138,6 +139,7 @@ struct WaveCtx {
     uint32_t slotBegin, slotCount; // probe slots of this chunk
     uint32_t smemTlas;             // TLAS nodes staged in shared memory (0 = read from global)
     uint32_t order;                // 0 probe-major, 1 direction-major
+    uint32_t smemWide;             // top 8-wide nodes staged in shared memory by the closest-hit stage
 };
 
 // Several solves (scenes, cascades) through one launch of each stage: a

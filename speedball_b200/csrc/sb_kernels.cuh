@@ -13,6 +13,7 @@ struct TraceTuning {
     uint32_t smemTlasNodes;  // stage the TLAS in shared memory when it has at most this many nodes
     uint32_t sortKey;        // ray issue order (0 = probe-major)
     int numSms;
+    uint32_t smemWideNodes;  // top 8-wide scene-BVH nodes staged in shared memory per closest-hit CTA
 };
 
 // Scene buffers in the reference layouts plus the derived layouts.

@@ -45,7 +45,8 @@ __device__ __forceinline__ void add_visits(unsigned long long* c, int at, uint32
 
 // Stage A: the closest hit of one probe ray (item-local issue index g) as a
 // raw record (FP32 t, no facing bit): k_emit finishes it.
-__device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, bool pairs, uint32_t g, Visits& vis) {
+__device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, bool pairs, uint32_t g, Visits& vis,
+                                            const uint4* sWide = nullptr, uint32_t nWide = 0) {
     const DevCascade& C = W.C;
     const uint32_t N = C.rays;
     uint32_t slot, k;
@@ -55,7 +56,7 @@ __device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, b
     const float3 rd = ray_dir(k, N, W.P.frameJitter);
     float bestT, bu, bv;
     int tri, inst;
-    trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs);
+    trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs, sWide, nWide);
     uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
     uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
     C.hits[slot * N + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(bestT),
@@ -203,6 +204,13 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
     extern __shared__ uint4 sTlas[];
     const bool pairs = closest_pairs(W.S);
     const uint4* tl = stage_tlas(W, sTlas, pairs);
+    // the scene BVH's top 8-wide nodes (the TLAS is not read on that walk:
+    // the buffer is free), staged once per CTA
+    const uint32_t nWide = W.S.wideNodes ? W.smemWide : 0u;
+    if (nWide) {
+        for (uint32_t i = threadIdx.x; i < 5u * nWide; i += blockDim.x) sTlas[i] = __ldg(W.S.wideNodes + i);
+        __syncthreads();
+    }
     if (!*W.S.valid) return;
     const uint32_t total = W.slotCount * W.C.rays;
     const uint32_t lane = threadIdx.x & 31u;
@@ -215,7 +223,7 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
         if (base >= total) break;
         const uint32_t g = base + lane;
         if (g >= total) continue;
-        primary_ray(W, tl, pairs, g, vis);
+        primary_ray(W, tl, pairs, g, vis, sTlas, nWide);
         ++nRays;
     }
     add_visits(W.counters, 2, nRays, vis);
@@ -307,16 +315,22 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     // the scene-BVH walk reads no TLAS
     uint32_t smemNodes = !S.flatOn && S.tlasNodeCount <= tune.smemTlasNodes ? S.tlasNodeCount : 0u;
     W.smemTlas = smemNodes;
+    // the 8-wide walk's top nodes, staged by the closest-hit stage only
+    uint32_t wideNodes = S.wideNodes ? (tune.smemWideNodes < S.wideNodeCount ? tune.smemWideNodes : S.wideNodeCount) : 0u;
+    if (wideNodes > 512u) wideNodes = 512u;
+    W.smemWide = wideNodes;
     size_t smem = (size_t)smemNodes * 64u;  // room for the child-pair TLAS (the 32-byte nodes need half)
-    if (smem > 48u * 1024u) {
-        cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    size_t smemPrimary = smem > (size_t)wideNodes * 80u ? smem : (size_t)wideNodes * 80u;
+    if (smemPrimary > 48u * 1024u)
+        cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemPrimary);
+    if (smem > 48u * 1024u)
         cudaFuncSetAttribute(k_trace_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
     cudaError_t e = cudaMemsetAsync(work, 0, 3 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const uint32_t rays = slotCount * C.rays;
     int block = (int)tune.block;
-    k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smem, tune, rays), block, smem, st>>>(W);
+    k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smemPrimary, tune, rays), block, smemPrimary,
+                      st>>>(W);
     note_launch();
     k_emit<<<(rays + 127) / 128, 128, 0, st>>>(W);
     note_launch();

@@ -607,9 +607,12 @@ __device__ __forceinline__ float q_at(uint32_t w, uint32_t byteSel) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | byteSel)) - 8388608.0f;
 }
 
+// `sWide` holds the first `nWide` nodes of the tree (the top levels: nodes are
+// numbered breadth-first) staged in shared memory, or nWide == 0.
 template <bool ANY>
 __device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 wrd, float& tmax, int& bestTri,
-                                          int& bestInst, float& bu, float& bv, Visits& vis, uint32_t* err) {
+                                          int& bestInst, float& bu, float& bv, Visits& vis, uint32_t* err,
+                                          const uint4* sWide = nullptr, uint32_t nWide = 0) {
     const float3 winv = mk(1.0f / wrd.x, 1.0f / wrd.y, 1.0f / wrd.z);
     if (SB_DYN_FIRST && dyn_walk<ANY>(S, wro, wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
     // Box tests use the inverse clamped to +-1e30. An infinite one (a zero
@@ -663,8 +666,22 @@ __device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 
                 done = true;
                 break;
             }
-            const uint4* p = S.wideNodes + 5u * node;
-            const uint4 h0 = __ldg(p), h1 = __ldg(p + 1), qa = __ldg(p + 2), qb = __ldg(p + 3), qc = __ldg(p + 4);
+            uint4 h0, h1, qa, qb, qc;
+            if (node < nWide) {
+                const uint4* p = sWide + 5u * node;
+                h0 = p[0];
+                h1 = p[1];
+                qa = p[2];
+                qb = p[3];
+                qc = p[4];
+            } else {
+                const uint4* p = S.wideNodes + 5u * node;
+                h0 = __ldg(p);
+                h1 = __ldg(p + 1);
+                qa = __ldg(p + 2);
+                qb = __ldg(p + 3);
+                qc = __ldg(p + 4);
+            }
             node = FLAT_NONE;
             vis.blas += 8;
             // per axis: t = q * (2^e * inv) + (p - o) * inv, near plane first
@@ -766,16 +783,18 @@ __device__ __forceinline__ bool closest_pairs(const DevScene& S) { return SB_CLO
 __device__ __forceinline__ bool any_pairs(const DevScene& S) { return SB_ANY_PAIRS && pairs_usable(S); }
 
 // traverseClosest, spectral_traverse.js:441-474. With `pairs` (pairs_usable),
-// `tl` is the TLAS child-pair array, else the 32-byte TLAS nodes.
+// `tl` is the TLAS child-pair array, else the 32-byte TLAS nodes. On the
+// 8-wide scene BVH, `sWide` / `nWide` are its staged top nodes (wide_walk).
 __device__ __forceinline__ void trace_closest(const DevScene& S, const uint4* tl, float3 ro, float3 rd, float& bestT,
                                               int& bestTri, int& bestInst, float& bu, float& bv, Visits& vis,
-                                              uint32_t* err, bool pairs) {
+                                              uint32_t* err, bool pairs, const uint4* sWide = nullptr,
+                                              uint32_t nWide = 0) {
     bestT = T_MAX;
     bestTri = -1;
     bestInst = -1;
     bu = bv = 0.0f;
     if (S.wideNodes) {
-        wide_walk<false>(S, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, err);
+        wide_walk<false>(S, ro, rd, bestT, bestTri, bestInst, bu, bv, vis, err, sWide, nWide);
         return;
     }
     if (S.flatOn) {
