@@ -362,7 +362,9 @@ sb_status sb_graph_destroy(sb_ctx* ctx);
 typedef struct sb_tuning {
     uint32_t traceBlock;      /* threads per block of the trace kernels            */
     uint32_t sortKey;         /* ray issue order: 0 = direction-major (ray k of
-                                 neighbouring probes per warp), 1 = probe-major   */
+                                 neighbouring probes per warp), 1 = probe-major,
+                                 2 = direction-major over 4 x 4 x 2 probe tiles
+                                 (full updates from probe 0; else as 0)           */
     uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
     uint32_t bvhKind;         /* scene BVH over (triangle, instance) items, rebuilt
                                  on structural changes: 1 = 8-wide nodes with 8-bit

@@ -35,6 +35,7 @@ struct Cascade {
     uint4* hits = nullptr;
     uint4* vis = nullptr;
     size_t rayCap = 0;
+    uint32_t* tileOrder = nullptr;  // probe index per issue position in 4 x 4 x 2 tiles (sortKey 2)
 };
 
 }  // namespace
@@ -79,7 +80,8 @@ struct sb_ctx {
     bool lightGridDirty = false;
     std::vector<float> hostLights;
 
-    TraceTuning tune{256u, 512u, 0u, 148};  // 512 TLAS nodes = 32 KB of child pairs per CTA
+    // 512 TLAS nodes = 32 KB of child pairs per CTA; probe-tile issue order (1.5% faster closest hits)
+    TraceTuning tune{256u, 512u, 2u, 148};
     uint32_t bvhKind = 1;          // 1 = scene BVH, 8-wide for closest hits (default); 2 = binary scene
                                    // BVH only; 0 = the reference's TLAS + BLASes (sb_flat.h)
     FlatScene flat;
@@ -407,6 +409,7 @@ void sb_destroy(sb_ctx* ctx) {
     release(I.scratch); release(ctx->instOwner); release(ctx->dStage); release(ctx->dStageM);
     for (auto& K : ctx->casc) {
         release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.rayData); release(K.hits);
+        release(K.tileOrder);
         release(K.vis);
     }
     release(ctx->jobs);
@@ -689,12 +692,25 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
                     K.grid.res[2] == g->res[2];
     size_t rays = (size_t)probeTotal * g->raysPerProbe;
     if (!sameDims) {
-        release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas);
+        release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.tileOrder);
         size_t c = 0;
         CK(grow(K.irr, c, (size_t)probeTotal * 64)); c = 0;
         CK(grow(K.depth, c, (size_t)probeTotal * 64)); c = 0;
         CK(grow(K.atlas, c, (size_t)probeTotal * 64)); c = 0;
-        CK(grow(K.depthAtlas, c, (size_t)probeTotal * 64));
+        CK(grow(K.depthAtlas, c, (size_t)probeTotal * 64)); c = 0;
+        // the probes in 4 x 4 x 2 tiles (row-major over tiles, x fastest inside;
+        // edge tiles clipped): 32 consecutive entries form one compact block
+        std::vector<uint32_t> order;
+        order.reserve(probeTotal);
+        const uint32_t rx = g->res[0], ry = g->res[1], rz = g->res[2];
+        for (uint32_t tz = 0; tz < rz; tz += 2)
+            for (uint32_t ty = 0; ty < ry; ty += 4)
+                for (uint32_t tx = 0; tx < rx; tx += 4)
+                    for (uint32_t z = tz; z < tz + 2 && z < rz; ++z)
+                        for (uint32_t y = ty; y < ty + 4 && y < ry; ++y)
+                            for (uint32_t x = tx; x < tx + 4 && x < rx; ++x) order.push_back((z * ry + y) * rx + x);
+        CK(grow(K.tileOrder, c, (size_t)probeTotal));
+        CK(cudaMemcpy(K.tileOrder, order.data(), (size_t)probeTotal * 4, cudaMemcpyHostToDevice));
     }
     if (rays > K.rayCap || !K.rayData) {
         release(K.rayData); release(K.hits); release(K.vis);
@@ -764,6 +780,8 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
         ctx->jobCap = (uint32_t)want;
     }
     const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
+    if (ctx->tune.sortKey == 2 && probeOffset == 0 && updatedCount == K.probeTotal && updatedCount <= chunk)
+        D.issueOrder = K.tileOrder;  // every probe in one chunk: issue them tile by tile
     if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 128, ctx->stream));
     const bool timing = !ctx->capturing;  // events inside a capture would not be re-recorded by replays
     if (timing) CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -824,7 +842,8 @@ static sb_status build_batch(const sb_solve_item* items, uint32_t count, BatchAr
         I.W.slotBegin = 0;
         I.W.slotCount = cnt;
         I.W.smemTlas = 0;
-        I.W.order = lead->tune.sortKey == 0 ? 1u : 0u;
+        I.W.order = lead->tune.sortKey == 1 ? 0u : 1u;
+        if (lead->tune.sortKey == 2 && I.W.C.probeOffset == 0 && cnt == K.probeTotal) I.W.C.issueOrder = K.tileOrder;
         const uint64_t rays = (uint64_t)cnt * K.grid.raysPerProbe;
         I.rayBase = (uint32_t)rayBase;
         I.rays = (uint32_t)rays;
@@ -1240,7 +1259,7 @@ sb_status sb_autotune(sb_ctx* ctx, uint32_t ci, sb_tuning* chosen) {
     // shared-memory staging: the TLAS for the two-level walk, the top 8-wide nodes for kind 1
     for (uint32_t kind : kinds)
         for (uint32_t block : blocks)
-            for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort)
+            for (uint32_t sort = 0; sort < 3 && s == SB_OK; ++sort)
                 for (uint32_t sm = 0; sm < (kind == 0 ? 2u : kind == 1 ? 3u : 1u) && s == SB_OK; ++sm) {
                     sb_tuning t{block, sort, kind == 0 ? (sm ? 512u : 0u) : saved.smemTlasNodes, kind,
                                 kind == 1 ? wideDepth[sm] : 0u};
@@ -1285,7 +1304,7 @@ sb_status sb_autotune_batch(const sb_solve_item* items, uint32_t count, sb_tunin
     float bestMs = 3.4e38f;
     const uint32_t blocks[3] = {128u, 192u, 256u};
     for (uint32_t block : blocks)
-        for (uint32_t sort = 0; sort < 2 && s == SB_OK; ++sort) {
+        for (uint32_t sort = 0; sort < 3 && s == SB_OK; ++sort) {
             sb_tuning t{block, sort, saved.smemTlasNodes, saved.bvhKind, saved.smemWideNodes};
             if ((s = sb_set_tuning(lead, &t)) != SB_OK) break;
             float ms = 0.0f;
@@ -1683,6 +1702,7 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (t->bvhKind > 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
     if (t->smemWideNodes > 512)
         return fail(ctx, SB_ERR_INVALID_ARG, "smemWideNodes %u > 512 (80 bytes each)", t->smemWideNodes);
+    if (t->sortKey > 2) return fail(ctx, SB_ERR_INVALID_ARG, "sortKey %u: 0, 1 or 2", t->sortKey);
     if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
     ctx->tune.smemWideNodes = t->smemWideNodes;
     ctx->bvhKind = t->bvhKind;

@@ -107,6 +107,8 @@ struct DevCascade {
     uint2* atlas;              // RGBA16F output
     uint2* depthAtlas;
     float4* eOut;              // optional: FP32 upload output of the 36 interior texels per probe (adjoint tape)
+    const uint32_t* issueOrder;  // optional (full updates from slot 0): direction-major issue visits the
+                                 // probes in this order, 32 per compact 4 x 4 x 2 tile
 };
 
 struct DevParams {

@@ -311,7 +311,7 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     W.jobCap = jobCap;
     W.slotBegin = slotBegin;
     W.slotCount = slotCount;
-    W.order = tune.sortKey == 0 ? 1u : 0u;  // default direction-major; sortKey 1 = probe-major
+    W.order = tune.sortKey == 1 ? 0u : 1u;  // direction-major (sortKey 0, and 2 over probe tiles); 1 = probe-major
     // the scene-BVH walk reads no TLAS
     uint32_t smemNodes = !S.flatOn && S.tlasNodeCount <= tune.smemTlasNodes ? S.tlasNodeCount : 0u;
     W.smemTlas = smemNodes;

@@ -131,6 +131,10 @@ __device__ __forceinline__ void ray_of(const WaveCtx& W, uint32_t g, bool dirMaj
     if (dirMajor) {
         k = g / W.slotCount;
         s = g - k * W.slotCount;
+        if (W.C.issueOrder) {  // a permutation of every probe (the solve covers them all from slot 0)
+            slot = __ldg(W.C.issueOrder + s);
+            return;
+        }
     } else {
         s = g / N;
         k = g - s * N;

@@ -151,7 +151,8 @@ def test_autotune_picks_a_candidate_and_restores_the_probes():
         after = _state(f, 0)
         for key in ("irr", "depth", "atlas", "datlas"):
             assert np.array_equal(before[key], after[key]), key
-        assert t.bvhKind in (0, 1, 2) and t.traceBlock in (128, 192, 256) and t.sortKey in (0, 1)
+        assert t.bvhKind in (0, 1, 2) and t.traceBlock in (128, 192, 256) and t.sortKey in (0, 1, 2)
+        assert t.smemWideNodes in (0, 73, 512)
         cur = abi.sb_tuning()
         abi.check(f._lib.sb_get_tuning(f.ctx, C.byref(cur)), f.ctx)
         assert (cur.traceBlock, cur.sortKey, cur.smemTlasNodes, cur.bvhKind) == \
