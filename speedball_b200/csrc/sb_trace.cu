@@ -123,10 +123,12 @@ __device__ __forceinline__ uint32_t emit_ray(const WaveCtx& W, bool active, uint
         const uint32_t i = (uint32_t)(__ffsll((long long)pass) - 1);
         pass &= pass - 1ull;
         const uint32_t li = light_at(L, i);
-        const LightEval e = light_eval(W, li, fr.hitPos, fr.ng);
         if (j < W.jobCap) {
-            W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, e.dist - fr.traceBias);
-            W.jobs[2 * j + 1] = make_float4(e.wi.x, e.wi.y, e.wi.z, __uint_as_float(tag | li));
+            float3 wi;
+            float dist;
+            light_ray(W, li, fr.hitPos, wi, dist);
+            W.jobs[2 * j] = make_float4(fr.hitPos.x, fr.hitPos.y, fr.hitPos.z, dist - fr.traceBias);
+            W.jobs[2 * j + 1] = make_float4(wi.x, wi.y, wi.z, __uint_as_float(tag | li));
             if (li < 32) tested0 |= 1u << li;
             else tested1 |= 1u << (li - 32);
             ++nJobs;

@@ -109,6 +109,17 @@ __device__ __forceinline__ LightEval light_eval(const WaveCtx& W, uint32_t li, f
     return e;
 }
 
+// The shadow-ray geometry of a light that passed its gates: the direction
+// and distance light_eval forms, from the same record fields and expressions.
+__device__ __forceinline__ void light_ray(const WaveCtx& W, uint32_t li, float3 hitPos, float3& wi, float& dist) {
+    const float* L = W.S.lights + li * 17u;
+    const bool isDir = __ldg(L) < 0.5f;
+    const float3 toLight = isDir ? mk(__ldg(L + 4), __ldg(L + 5), __ldg(L + 6)) * -1.0f
+                                 : mk(__ldg(L + 1), __ldg(L + 2), __ldg(L + 3)) - hitPos;
+    dist = isDir ? 1e4f : fmaxf(sqrtf(dot3(toLight, toLight)), 1e-4f);
+    wi = normalize3(toLight);
+}
+
 // The unshadowed Lambert NEE term (gi_probes.js:2160-2171).
 __device__ __forceinline__ float3 light_term(const WaveCtx& W, const LightEval& e, float3 kd) {
     float falloff = 1.0f / fmaxf(powf(e.dist, e.ldecay), 0.01f);
