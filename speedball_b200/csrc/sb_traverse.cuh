@@ -607,6 +607,60 @@ __device__ __forceinline__ float q_at(uint32_t w, uint32_t byteSel) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | byteSel)) - 8388608.0f;
 }
 
+// Box-test instruction forms of sm_100 (each exact, so the hit decisions are
+// the same in every form): three-input min / max (PTX ISA 8.8), two children's
+// plane distances per packed f32x2 add + fma (PTX ISA 8.6), and child hits
+// gathered as an 8-bit slot mask turned into traversal bits once per node.
+#ifndef SB_WIDE_MINMAX3
+#define SB_WIDE_MINMAX3 1
+#endif
+#ifndef SB_WIDE_F32X2
+#define SB_WIDE_F32X2 1
+#endif
+#ifndef SB_WIDE_HITMASK
+#define SB_WIDE_HITMASK 1
+#endif
+
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+#if SB_WIDE_MINMAX3
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+#else
+    return fmaxf(fmaxf(a, b), c);
+#endif
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+#if SB_WIDE_MINMAX3
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+#else
+    return fminf(fminf(a, b), c);
+#endif
+}
+
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+// Plane distances of bytes b and b + 1 of w: q * s + o for both, where
+// s2 = (s, s) and o2 = (o, o); per lane the same IEEE operations as
+// fmaf(q_at(w, b), s, o).
+__device__ __forceinline__ void q_pair(uint32_t w, uint32_t b, unsigned long long s2, unsigned long long o2, float& t0,
+                                       float& t1) {
+    const uint32_t a0 = __byte_perm(w, 0x4B000000u, 0x7540u | b);
+    const uint32_t a1 = __byte_perm(w, 0x4B000000u, 0x7540u | (b + 1u));
+    const unsigned long long bias = 0xCB000000CB000000ull;  // (-2^23, -2^23)
+    unsigned long long r;
+    asm("{\n\t.reg .b64 a;\n\tmov.b64 a, {%1, %2};\n\tadd.rn.f32x2 a, a, %3;\n\tfma.rn.f32x2 %0, a, %4, %5;\n\t}"
+        : "=l"(r)
+        : "r"(a0), "r"(a1), "l"(bias), "l"(s2), "l"(o2));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(t0), "=f"(t1) : "l"(r));
+}
+
 // `sWide` holds the first `nWide` nodes of the tree (the top levels: nodes are
 // numbered breadth-first) staged in shared memory, or nWide == 0.
 template <bool ANY>
@@ -699,25 +753,67 @@ __device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 
             const uint32_t farY0 = ny ? qa.z : qc.x, farY1 = ny ? qa.w : qc.y;
             const uint32_t nearZ0 = nz ? qc.z : qb.x, nearZ1 = nz ? qc.w : qb.y;
             const uint32_t farZ0 = nz ? qb.x : qc.z, farZ1 = nz ? qb.y : qc.w;
-            uint32_t bits = 0;
-#pragma unroll
-            for (uint32_t s = 0; s < 8; ++s) {
-                const uint32_t b = s & 3u;
-                const float tnx = fmaf(q_at(s < 4 ? nearX0 : nearX1, b), sx, ox);
-                const float tny = fmaf(q_at(s < 4 ? nearY0 : nearY1, b), sy, oy);
-                const float tnz = fmaf(q_at(s < 4 ? nearZ0 : nearZ1, b), sz, oz);
-                const float tfx = fmaf(q_at(s < 4 ? farX0 : farX1, b), sx, ox);
-                const float tfy = fmaf(q_at(s < 4 ? farY0 : farY1, b), sy, oy);
-                const float tfz = fmaf(q_at(s < 4 ? farZ0 : farZ1, b), sz, oz);
-                const float tNear = fmaxf(fmaxf(tnx, tny), tnz);
-                const float tFar = fminf(fminf(tfx, tfy), tfz);
-                if (tFar >= fmaxf(tNear, 0.0f) && tNear < tmax) {
-                    const uint32_t m = (s < 4 ? h1.z : h1.w) >> (8u * b) & 0xFFu;
+            uint32_t bits = 0;  // hit mask over slots (SB_WIDE_HITMASK), else traversal bits
+            // child s's box against the ray from its six plane distances
+            auto child = [&](uint32_t s, float tnx, float tny, float tnz, float tfx, float tfy, float tfz) {
+                const float tNear = max3f(tnx, tny, tnz);
+                const float tFar = min3f(tfx, tfy, tfz);
+                const bool hit = tFar >= fmaxf(tNear, 0.0f) && tNear < tmax;
+#if SB_WIDE_HITMASK
+                bits |= (hit ? 1u : 0u) << s;
+#else
+                if (hit) {
+                    const uint32_t m = (s < 4 ? h1.z : h1.w) >> (8u * (s & 3u)) & 0xFFu;
                     uint32_t sh = m & 31u;
                     if (sh >= 24u) sh ^= oct;
                     bits |= (m >> 5) << sh;
                 }
+#endif
+            };
+#if SB_WIDE_F32X2
+            const unsigned long long sx2 = pack2(sx, sx), sy2 = pack2(sy, sy), sz2 = pack2(sz, sz);
+            const unsigned long long ox2 = pack2(ox, ox), oy2 = pack2(oy, oy), oz2 = pack2(oz, oz);
+#pragma unroll
+            for (uint32_t s = 0; s < 8; s += 2) {  // two children per packed operation
+                const uint32_t b = s & 3u;
+                float nx0, nx1, ny0, ny1, nz0, nz1, fx0, fx1, fy0, fy1, fz0, fz1;
+                q_pair(s < 4 ? nearX0 : nearX1, b, sx2, ox2, nx0, nx1);
+                q_pair(s < 4 ? nearY0 : nearY1, b, sy2, oy2, ny0, ny1);
+                q_pair(s < 4 ? nearZ0 : nearZ1, b, sz2, oz2, nz0, nz1);
+                q_pair(s < 4 ? farX0 : farX1, b, sx2, ox2, fx0, fx1);
+                q_pair(s < 4 ? farY0 : farY1, b, sy2, oy2, fy0, fy1);
+                q_pair(s < 4 ? farZ0 : farZ1, b, sz2, oz2, fz0, fz1);
+                child(s, nx0, ny0, nz0, fx0, fy0, fz0);
+                child(s + 1u, nx1, ny1, nz1, fx1, fy1, fz1);
             }
+#else
+#pragma unroll
+            for (uint32_t s = 0; s < 8; ++s) {
+                const uint32_t b = s & 3u;
+                child(s, fmaf(q_at(s < 4 ? nearX0 : nearX1, b), sx, ox), fmaf(q_at(s < 4 ? nearY0 : nearY1, b), sy, oy),
+                      fmaf(q_at(s < 4 ? nearZ0 : nearZ1, b), sz, oz), fmaf(q_at(s < 4 ? farX0 : farX1, b), sx, ox),
+                      fmaf(q_at(s < 4 ? farY0 : farY1, b), sy, oy), fmaf(q_at(s < 4 ? farZ0 : farZ1, b), sz, oz));
+            }
+#endif
+#if SB_WIDE_HITMASK
+            {
+                // interior hits to bit (slot XOR octant): visiting the lowest first goes near to far
+                const uint32_t imask = h0.w >> 24;
+                uint32_t ih = bits & imask;
+                if (oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+                if (oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+                if (oct & 4u) ih = ((ih & 0x0Fu) << 4) | (ih >> 4);
+                // leaf hits: each one's item bits at its offset
+                uint32_t lh = bits & ~imask & 0xFFu, items = 0;
+                while (lh) {
+                    const uint32_t s = __ffs(lh) - 1u;
+                    lh &= lh - 1u;
+                    const uint32_t m = __byte_perm(h1.z, h1.w, s) & 0xFFu;
+                    items |= (m >> 5) << (m & 31u);
+                }
+                bits = ih << 24 | items;
+            }
+#endif
             gBase = h1.x;
             gBits = (bits & 0xFF000000u) | ((h0.w >> 24) << 16);
             tBase = h1.y;
