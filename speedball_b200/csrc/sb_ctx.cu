@@ -963,6 +963,7 @@ static void graph_release(sb_ctx* ctx) {
     if (G.graph) cudaGraphDestroy(G.graph);
     G.exec = nullptr;
     G.graph = nullptr;
+    for (auto& n : G.nodes) n = nullptr;
     G.lanes.clear();
     G.items.clear();
     G.keys.clear();
@@ -1057,9 +1058,11 @@ static sb_status graph_capture(sb_ctx* lead, std::vector<sb_ctx::Graph::Lane> la
     CK(cudaGraphGetNodes(graph, nullptr, &n));
     std::vector<cudaGraphNode_t> nodes(n);
     CK(cudaGraphGetNodes(graph, nodes.data(), &n));
+    // stages without a kernel of their own (null) are done inside another one
     const void* fn[5] = {trace_batch_kernel(0), trace_batch_kernel(1), trace_batch_kernel(2), trace_batch_kernel(3),
                          blend_batch_kernel()};
-    int found = 0;
+    int found = 0, expected = 0;
+    for (const void* f : fn) expected += f ? 1 : 0;
     G.kernelNodes = 0;
     for (cudaGraphNode_t node : nodes) {
         cudaGraphNodeType t;
@@ -1069,15 +1072,15 @@ static sb_status graph_capture(sb_ctx* lead, std::vector<sb_ctx::Graph::Lane> la
         cudaKernelNodeParams p;
         CK(cudaGraphKernelNodeGetParams(node, &p));
         for (int k = 0; k < 5; ++k)
-            if (p.func == fn[k]) {
+            if (fn[k] && p.func == fn[k]) {
                 G.nodes[k] = node;
                 G.params[k] = p;
                 ++found;
             }
     }
-    if (found != 5) {
+    if (found != expected) {
         graph_release(lead);
-        return fail(lead, SB_ERR_CUDA, "captured frame holds %d of the 5 batched kernels", found);
+        return fail(lead, SB_ERR_CUDA, "captured frame holds %d of the %d batched kernels", found, expected);
     }
     CK(cudaGraphInstantiate(&G.exec, graph, 0));
     G.lanes = std::move(lanes);
@@ -1108,6 +1111,7 @@ static sb_status graph_launch(sb_ctx* lead) {
     if (s != SB_OK) return s;
     void* args[1] = {&B};
     for (int k = 0; k < 5; ++k) {
+        if (!G.nodes[k]) continue;
         cudaKernelNodeParams p = G.params[k];
         p.kernelParams = args;
         p.extra = nullptr;
