@@ -364,7 +364,11 @@ typedef struct sb_tuning {
     uint32_t sortKey;         /* ray issue order: 0 = direction-major (ray k of
                                  neighbouring probes per warp), 1 = probe-major,
                                  2 = direction-major over 4 x 4 x 2 probe tiles
-                                 (full updates from probe 0; else as 0)           */
+                                 (full updates from probe 0; else as 0),
+                                 3 = as 2, with the closest-hit stage's 32-ray
+                                 batches issued costliest first, by the cycles
+                                 each took in the previous full sb_solve of the
+                                 cascade (sb_solve only; batches run as 2)       */
     uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
     uint32_t bvhKind;         /* scene BVH over (triangle, instance) items, rebuilt
                                  on structural changes: 1 = 8-wide nodes with 8-bit
@@ -378,7 +382,8 @@ typedef struct sb_tuning {
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);
 /* Time full solves of `cascade` under candidate tunings (bvhKind 1 / 2 / 0,
- * traceBlock 128 / 192 / 256, both sort keys, and for bvhKind 0 TLAS staging
+ * traceBlock 128 / 192 / 256, sortKey 0-3, for bvhKind 1 smemWideNodes
+ * 0 / 73 / 512, and for bvhKind 0 TLAS staging
  * off / 512 nodes), keep the fastest on the context and return it. The
  * cascade's histories and atlases are restored afterwards. Synchronizes. */
 sb_status sb_autotune(sb_ctx* ctx, uint32_t cascade, sb_tuning* chosen);

@@ -36,6 +36,12 @@ struct Cascade {
     uint4* vis = nullptr;
     size_t rayCap = 0;
     uint32_t* tileOrder = nullptr;  // probe index per issue position in 4 x 4 x 2 tiles (sortKey 2)
+    // sortKey 3: cycles per 32-ray closest-hit batch of the last full solve, and the batch
+    // order (costliest first) built from them; ready once a full solve has recorded costs
+    uint32_t* batchCost = nullptr;
+    uint32_t* batchOrder = nullptr;
+    size_t batchCap = 0;
+    bool batchOrderReady = false;
 };
 
 }  // namespace
@@ -80,8 +86,9 @@ struct sb_ctx {
     bool lightGridDirty = false;
     std::vector<float> hostLights;
 
-    // 512 TLAS nodes = 32 KB of child pairs per CTA; probe-tile issue order (1.5% faster closest hits)
-    TraceTuning tune{256u, 512u, 2u, 148};
+    // 512 TLAS nodes = 32 KB of child pairs per CTA; probe-tile issue order with the closest-hit
+    // batches costliest first (atrium solve 0.400 -> 0.387 ms against tile order alone)
+    TraceTuning tune{256u, 512u, 3u, 148};
     uint32_t bvhKind = 1;          // 1 = scene BVH, 8-wide for closest hits (default); 2 = binary scene
                                    // BVH only; 0 = the reference's TLAS + BLASes (sb_flat.h)
     FlatScene flat;
@@ -409,7 +416,7 @@ void sb_destroy(sb_ctx* ctx) {
     release(I.scratch); release(ctx->instOwner); release(ctx->dStage); release(ctx->dStageM);
     for (auto& K : ctx->casc) {
         release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.rayData); release(K.hits);
-        release(K.tileOrder);
+        release(K.tileOrder); release(K.batchCost); release(K.batchOrder);
         release(K.vis);
     }
     release(ctx->jobs);
@@ -720,6 +727,19 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
         c = 0; CK(grow(K.vis, c, rays));
         K.rayCap = rays;
     }
+    {
+        const size_t batches = (rays + 31) / 32;
+        size_t c = K.batchCap;
+        CK(grow(K.batchCost, c, batches));
+        c = K.batchCap;
+        CK(grow(K.batchOrder, c, batches));
+        K.batchCap = c;
+        K.batchOrderReady = false;  // the batches are those of the new grid
+        // identity until a solve has ordered them: always a permutation of the batches
+        std::vector<uint32_t> iota(batches);
+        for (size_t i = 0; i < batches; ++i) iota[i] = (uint32_t)i;
+        CK(cudaMemcpy(K.batchOrder, iota.data(), batches * 4, cudaMemcpyHostToDevice));
+    }
     K.grid = *g;
     K.probeTotal = probeTotal;
     K.atlasW = g->res[0] * 8;
@@ -780,8 +800,14 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
         ctx->jobCap = (uint32_t)want;
     }
     const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
-    if (ctx->tune.sortKey == 2 && probeOffset == 0 && updatedCount == K.probeTotal && updatedCount <= chunk)
-        D.issueOrder = K.tileOrder;  // every probe in one chunk: issue them tile by tile
+    const bool fullSolve = probeOffset == 0 && updatedCount == K.probeTotal && updatedCount <= chunk;
+    if (ctx->tune.sortKey >= 2 && fullSolve) D.issueOrder = K.tileOrder;  // every probe in one chunk: tile by tile
+    const bool costOrder = ctx->tune.sortKey == 3 && fullSolve;
+    if (costOrder) {  // this solve records its batch costs and orders the next one by them
+        D.batchCost = K.batchCost;
+        D.batchOrder = K.batchOrderReady ? K.batchOrder : nullptr;
+        D.batchOrderOut = K.batchOrder;
+    }
     if (ctx->countersOn) CK(cudaMemsetAsync(ctx->dCounters, 0, 128, ctx->stream));
     const bool timing = !ctx->capturing;  // events inside a capture would not be re-recorded by replays
     if (timing) CK(cudaEventRecord(ctx->ev0, ctx->stream));
@@ -794,6 +820,7 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     }
     if (timing) CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
+    if (costOrder) K.batchOrderReady = true;
     if (timing) CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->timed = ctx->timed || timing;
     if (timing) ctx->lastWasGraph = false;
@@ -843,7 +870,7 @@ static sb_status build_batch(const sb_solve_item* items, uint32_t count, BatchAr
         I.W.slotCount = cnt;
         I.W.smemTlas = 0;
         I.W.order = lead->tune.sortKey == 1 ? 0u : 1u;
-        if (lead->tune.sortKey == 2 && I.W.C.probeOffset == 0 && cnt == K.probeTotal) I.W.C.issueOrder = K.tileOrder;
+        if (lead->tune.sortKey >= 2 && I.W.C.probeOffset == 0 && cnt == K.probeTotal) I.W.C.issueOrder = K.tileOrder;
         const uint64_t rays = (uint64_t)cnt * K.grid.raysPerProbe;
         I.rayBase = (uint32_t)rayBase;
         I.rays = (uint32_t)rays;
@@ -1241,9 +1268,10 @@ static sb_status time_min(sb_ctx* lead, const std::vector<sb_ctx*>& all, const s
 
 // Times full solves of cascade ci under each candidate tuning and keeps the
 // fastest. Candidates: the scene BVH kinds (8-wide / binary / the reference's
-// two-level walk), traversal block sizes 128 / 192 / 256, both ray issue
-// orders, and for the two-level walk TLAS staging in shared memory off / up to
-// 512 nodes. The cascade's histories and atlases are restored afterwards, so
+// two-level walk), traversal block sizes 128 / 192 / 256, the four ray issue
+// orders (sortKey 0-3), for the 8-wide tree 0 / 73 / 512 top nodes staged in
+// shared memory, and for the two-level walk TLAS staging in shared memory off /
+// up to 512 nodes. The cascade's histories and atlases are restored afterwards, so
 // tuning leaves the probe state as it found it.
 sb_status sb_autotune(sb_ctx* ctx, uint32_t ci, sb_tuning* chosen) {
     if (!ctx) return SB_ERR_INVALID_ARG;
@@ -1263,7 +1291,7 @@ sb_status sb_autotune(sb_ctx* ctx, uint32_t ci, sb_tuning* chosen) {
     // shared-memory staging: the TLAS for the two-level walk, the top 8-wide nodes for kind 1
     for (uint32_t kind : kinds)
         for (uint32_t block : blocks)
-            for (uint32_t sort = 0; sort < 3 && s == SB_OK; ++sort)
+            for (uint32_t sort = 0; sort < 4 && s == SB_OK; ++sort)
                 for (uint32_t sm = 0; sm < (kind == 0 ? 2u : kind == 1 ? 3u : 1u) && s == SB_OK; ++sm) {
                     sb_tuning t{block, sort, kind == 0 ? (sm ? 512u : 0u) : saved.smemTlasNodes, kind,
                                 kind == 1 ? wideDepth[sm] : 0u};
@@ -1706,7 +1734,7 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (t->bvhKind > 2) return fail(ctx, SB_ERR_UNSUPPORTED, "bvhKind %u not built", t->bvhKind);
     if (t->smemWideNodes > 512)
         return fail(ctx, SB_ERR_INVALID_ARG, "smemWideNodes %u > 512 (80 bytes each)", t->smemWideNodes);
-    if (t->sortKey > 2) return fail(ctx, SB_ERR_INVALID_ARG, "sortKey %u: 0, 1 or 2", t->sortKey);
+    if (t->sortKey > 3) return fail(ctx, SB_ERR_INVALID_ARG, "sortKey %u: 0, 1, 2 or 3", t->sortKey);
     if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
     ctx->tune.smemWideNodes = t->smemWideNodes;
     ctx->bvhKind = t->bvhKind;

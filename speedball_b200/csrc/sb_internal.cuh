@@ -109,6 +109,12 @@ struct DevCascade {
     float4* eOut;              // optional: FP32 upload output of the 36 interior texels per probe (adjoint tape)
     const uint32_t* issueOrder;  // optional (full updates from slot 0): direction-major issue visits the
                                  // probes in this order, 32 per compact 4 x 4 x 2 tile
+    // optional (sortKey 3, with issueOrder): the closest-hit stage hands out its 32-ray batches
+    // in batchOrder (costliest of the previous solve first) and records each batch's cycles in
+    // batchCost; the shadow stage's first idle CTA writes the next solve's order to batchOrderOut
+    const uint32_t* batchOrder;
+    uint32_t* batchCost;
+    uint32_t* batchOrderOut;
 };
 
 struct DevParams {

@@ -11,7 +11,8 @@ uint64_t launches();
 struct TraceTuning {
     uint32_t block;          // threads per block of the trace kernel
     uint32_t smemTlasNodes;  // stage the TLAS in shared memory when it has at most this many nodes
-    uint32_t sortKey;        // ray issue order: 0 direction-major, 1 probe-major, 2 direction-major over probe tiles
+    uint32_t sortKey;        // ray issue order: 0 direction-major, 1 probe-major, 2 direction-major over probe
+                             // tiles, 3 as 2 with closest-hit batches costliest first (last full solve's cycles)
     int numSms;
     uint32_t smemWideNodes;  // top 8-wide scene-BVH nodes staged in shared memory per closest-hit CTA
 };

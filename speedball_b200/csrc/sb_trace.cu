@@ -223,12 +223,59 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
         if (lane == 0) base = atomicAdd(&W.work[0], 32u);
         base = __shfl_sync(0xFFFFFFFFu, base, 0);
         if (base >= total) break;
-        const uint32_t g = base + lane;
-        if (g >= total) continue;
-        primary_ray(W, tl, pairs, g, vis, sTlas, nWide);
-        ++nRays;
+        // the batch at this issue position: costliest first when an order is given
+        // (a permutation of the (total + 31) / 32 batches; clamped all the same)
+        const uint32_t batch =
+            W.C.batchOrder ? min(__ldg(W.C.batchOrder + (base >> 5)), (total - 1u) >> 5) : base >> 5;
+        const uint32_t g = batch * 32u + lane;
+        const long long t0 = W.C.batchCost ? clock64() : 0;
+        if (g < total) {
+            primary_ray(W, tl, pairs, g, vis, sTlas, nWide);
+            ++nRays;
+        }
+        if (W.C.batchCost) {
+            __syncwarp();
+            if (lane == 0) W.C.batchCost[batch] = (uint32_t)min(clock64() - t0, 0xFFFFFFFFll);
+        }
     }
     add_visits(W.counters, 2, nRays, vis);
+}
+
+// The closest-hit batch order for the next full solve, by one CTA (all its
+// threads call it; blockDim a multiple of 32): batches by descending recorded
+// cycles, a counting sort over 128 log-spaced bins (4 per octave), so the
+// persistent kernel starts the long batches first and its last warps hold
+// short ones. Order within a bin is arbitrary; results do not depend on it.
+__device__ __forceinline__ uint32_t cost_bin(uint32_t c) {
+    if (c < 4u) return 0u;
+    const uint32_t msb = 31u - __clz(c);
+    return min(127u, msb * 4u + ((c >> (msb - 2u)) & 3u));
+}
+__device__ void order_batches(const uint32_t* cost, uint32_t* order, uint32_t n, uint32_t* at /* shared, 128 */) {
+    for (uint32_t i = threadIdx.x; i < 128u; i += blockDim.x) at[i] = 0u;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&at[cost_bin(__ldcg(cost + i))], 1u);
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan from the costliest bin down: 4 bins per lane
+        const uint32_t l = threadIdx.x;
+        uint32_t v[4], sum = 0;
+        for (uint32_t j = 0; j < 4; ++j) {
+            v[j] = at[127u - (4u * l + j)];
+            sum += v[j];
+        }
+        uint32_t incl = sum;
+        for (uint32_t d = 1; d < 32; d <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (l >= d) incl += u;
+        }
+        uint32_t run = incl - sum;
+        for (uint32_t j = 0; j < 4; ++j) {
+            at[127u - (4u * l + j)] = run;
+            run += v[j];
+        }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) order[atomicAdd(&at[cost_bin(__ldcg(cost + i))], 1u)] = i;
 }
 
 __global__ void __launch_bounds__(128) k_emit(WaveCtx W) {
@@ -261,6 +308,16 @@ __global__ void __launch_bounds__(256, SB_SHADOW_MIN_BLOCKS) k_trace_shadow(Wave
         shadow_job(W, tl, pairs, a, b, __float_as_uint(b.w) >> 6, vis);
     }
     add_visits(W.counters, 6, 0u, vis);
+    if (W.C.batchOrderOut) {
+        // the queue is drained: the first CTA whose warps are all done orders the
+        // closest-hit batches for the next solve while the others finish their jobs
+        __shared__ uint32_t at[128];
+        __shared__ uint32_t first;
+        __syncthreads();
+        if (threadIdx.x == 0) first = atomicAdd(&W.work[3], 1u) == 0u ? 1u : 0u;
+        __syncthreads();
+        if (first) order_batches(W.C.batchCost, W.C.batchOrderOut, (W.slotCount * W.C.rays + 31u) / 32u, at);
+    }
 }
 
 __global__ void __launch_bounds__(128) k_shade(WaveCtx W) {
@@ -327,7 +384,8 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
         cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemPrimary);
     if (smem > 48u * 1024u)
         cudaFuncSetAttribute(k_trace_shadow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaError_t e = cudaMemsetAsync(work, 0, 3 * sizeof(uint32_t), st);
+    // ray, job-read and job-write cursors, and the batch-order claim
+    cudaError_t e = cudaMemsetAsync(work, 0, 4 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const uint32_t rays = slotCount * C.rays;
     int block = (int)tune.block;

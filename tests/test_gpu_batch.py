@@ -137,6 +137,36 @@ def test_batch_rejects_bad_items():
         b.dispose()
 
 
+def _solve_with_sort_key(key: int, frames: int = 4):
+    import ctypes as C
+    at = synth.atrium(seed=100, total_tris=20_000)
+    at.meta["grid"] = dict(at.meta["grid"], res=(9, 9, 9), rays=48)
+    f = make_field(at, rays=48)
+    try:
+        t = _abi.sb_tuning()
+        _abi.check(f._lib.sb_get_tuning(f.ctx, C.byref(t)), f.ctx)
+        t.sortKey = key
+        _abi.check(f._lib.sb_set_tuning(f.ctx, C.byref(t)), f.ctx)
+        for _ in range(frames):
+            f.tick()
+        f.synchronize()
+        return _state(f, 0)
+    finally:
+        f.dispose()
+
+
+def test_cost_ordered_issue_matches_tile_order():
+    """sortKey 3 hands out the closest-hit batches costliest first (costs of
+    the previous solve, ordered inside the shadow stage); every frame after
+    the first runs in that order. Results do not depend on the issue order."""
+    tile = _solve_with_sort_key(2)
+    cost = _solve_with_sort_key(3)
+    for key in tile:
+        bad = np.flatnonzero(tile[key] != cost[key])
+        assert bad.size == 0, (key, bad.size, bad[:8])
+    assert (tile["hits"][0::4] != 0xFFFFFFFF).any()
+
+
 def test_autotune_picks_a_candidate_and_restores_the_probes():
     from speedball_b200 import _abi as abi
     import ctypes as C
@@ -151,7 +181,7 @@ def test_autotune_picks_a_candidate_and_restores_the_probes():
         after = _state(f, 0)
         for key in ("irr", "depth", "atlas", "datlas"):
             assert np.array_equal(before[key], after[key]), key
-        assert t.bvhKind in (0, 1, 2) and t.traceBlock in (128, 192, 256) and t.sortKey in (0, 1, 2)
+        assert t.bvhKind in (0, 1, 2) and t.traceBlock in (128, 192, 256) and t.sortKey in (0, 1, 2, 3)
         assert t.smemWideNodes in (0, 73, 512)
         cur = abi.sb_tuning()
         abi.check(f._lib.sb_get_tuning(f.ctx, C.byref(cur)), f.ctx)
