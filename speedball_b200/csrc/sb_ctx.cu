@@ -802,7 +802,8 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     const uint32_t chunk = (uint32_t)(ctx->jobCap / perProbe);
     const bool fullSolve = probeOffset == 0 && updatedCount == K.probeTotal && updatedCount <= chunk;
     if (ctx->tune.sortKey >= 2 && fullSolve) D.issueOrder = K.tileOrder;  // every probe in one chunk: tile by tile
-    const bool costOrder = ctx->tune.sortKey == 3 && fullSolve;
+    // (the refill form on the 8-wide tree has no fixed batches to order)
+    const bool costOrder = ctx->tune.sortKey == 3 && fullSolve && !(SB_PRIMARY_REFILL && S.wideNodes);
     if (costOrder) {  // this solve records its batch costs and orders the next one by them
         D.batchCost = K.batchCost;
         D.batchOrder = K.batchOrderReady ? K.batchOrder : nullptr;

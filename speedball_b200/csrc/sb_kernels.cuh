@@ -8,6 +8,13 @@ namespace sb {
 void note_launch();
 uint64_t launches();
 
+// The closest-hit stage on the 8-wide tree hands each lane a new ray as soon
+// as its walk ends (per-lane refill) instead of running fixed 32-ray batches
+// per warp; 0 keeps the batches (and with them the costliest-first order).
+#ifndef SB_PRIMARY_REFILL
+#define SB_PRIMARY_REFILL 1
+#endif
+
 struct TraceTuning {
     uint32_t block;          // threads per block of the trace kernel
     uint32_t smemTlasNodes;  // stage the TLAS in shared memory when it has at most this many nodes

@@ -43,25 +43,78 @@ __device__ __forceinline__ void add_visits(unsigned long long* c, int at, uint32
     atomicAdd(&c[at + 3], (unsigned long long)v.tri);
 }
 
-// Stage A: the closest hit of one probe ray (item-local issue index g) as a
-// raw record (FP32 t, no facing bit): k_emit finishes it.
+// The raw record of a closest hit (FP32 t, no facing bit): k_emit finishes it.
+__device__ __forceinline__ void write_hit(const DevCascade& C, uint32_t slot, uint32_t k, int tri, int inst, float t,
+                                          float bu, float bv) {
+    const uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
+    const uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
+    C.hits[slot * C.rays + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(t), uq | (vq << 16))
+                                         : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
+}
+
+// Stage A: the closest hit of one probe ray (item-local issue index g).
 __device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, bool pairs, uint32_t g, Visits& vis,
                                             const uint4* sWide = nullptr, uint32_t nWide = 0) {
     const DevCascade& C = W.C;
-    const uint32_t N = C.rays;
     uint32_t slot, k;
     ray_of(W, g, W.order != 0, slot, k);
     const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
     const float3 ro = probe_world_pos(C, probeIndex);
-    const float3 rd = ray_dir(k, N, W.P.frameJitter);
+    const float3 rd = ray_dir(k, C.rays, W.P.frameJitter);
     float bestT, bu, bv;
     int tri, inst;
     trace_closest(W.S, tl, ro, rd, bestT, tri, inst, bu, bv, vis, W.err, pairs, sWide, nWide);
-    uint32_t uq = (uint32_t)__float2uint_rn(clampf(bu, 0.f, 1.f) * 65535.0f);
-    uint32_t vq = (uint32_t)__float2uint_rn(clampf(bv, 0.f, 1.f) * 65535.0f);
-    C.hits[slot * N + k] = tri >= 0 ? make_uint4((uint32_t)tri, (uint32_t)inst, __float_as_uint(bestT),
-                                                 uq | (vq << 16))
-                                    : make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, __float_as_uint(-1.0f), 0u);
+    write_hit(C, slot, k, tri, inst, bestT, bu, bv);
+}
+
+// Stage A on the 8-wide tree with per-lane refill, for a whole persistent warp
+// (all 32 lanes call it): each lane walks its own ray in rounds (wide_step),
+// and a lane whose walk has ended takes the next ray of the issue order before
+// the next round, so the lanes keep working instead of waiting for the slowest
+// ray of a fixed 32-ray batch. One atomicAdd per round fetches rays for all
+// the warp's idle lanes. Returns the rays traced.
+__device__ __forceinline__ uint32_t primary_refill(const WaveCtx& W, uint32_t total, Visits& vis, const uint4* sWide,
+                                                   uint32_t nWide) {
+    const DevCascade& C = W.C;
+    const uint32_t lane = threadIdx.x & 31u;
+    WideWalk w;
+    uint32_t slot = 0, k = 0, nRays = 0;
+    float bestT = T_MAX, bu = 0.0f, bv = 0.0f;
+    int tri = -1, inst = -1;
+    bool has = false, more = true;
+    for (;;) {
+        if (more) {
+            const uint32_t need = __ballot_sync(0xFFFFFFFFu, !has);
+            if (need) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&W.work[0], (uint32_t)__popc(need));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= total) more = false;
+                const uint32_t g = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                if (!has && g < total) {
+                    ray_of(W, g, W.order != 0, slot, k);
+                    const float3 ro = probe_world_pos(C, (C.probeOffset + slot) % C.probeTotal);
+                    const float3 rd = ray_dir(k, C.rays, W.P.frameJitter);
+                    bestT = T_MAX;
+                    tri = inst = -1;
+                    bu = bv = 0.0f;
+                    wide_begin<false>(W.S, w, ro, rd, bestT, tri, inst, bu, bv, vis, W.err);
+                    has = true;
+                }
+            }
+        }
+        if (!__any_sync(0xFFFFFFFFu, has)) {
+            if (!more) break;
+            continue;
+        }
+        if (has && wide_step<false>(W.S, w, bestT, tri, inst, bu, bv, vis, W.err, sWide, nWide)) {
+            wide_end<false>(W.S, w, bestT, tri, inst, bu, bv, vis, W.err);
+            write_hit(C, slot, k, tri, inst, bestT, bu, bv);
+            ++nRays;
+            has = false;
+        }
+    }
+    return nRays;
 }
 
 // Stage A2, warp-collective (all 32 lanes call it; `active` lanes hold ray g):
@@ -218,6 +271,11 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
     const uint32_t lane = threadIdx.x & 31u;
     Visits vis = {0, 0, 0, 0};
     uint32_t nRays = 0;
+    if (SB_PRIMARY_REFILL && W.S.wideNodes) {
+        nRays = primary_refill(W, total, vis, sTlas, nWide);
+        add_visits(W.counters, 2, nRays, vis);
+        return;
+    }
     for (;;) {
         uint32_t base = 0;
         if (lane == 0) base = atomicAdd(&W.work[0], 32u);

@@ -661,6 +661,151 @@ __device__ __forceinline__ void q_pair(uint32_t w, uint32_t b, unsigned long lon
     asm("mov.b64 {%0, %1}, %2;" : "=f"(t0), "=f"(t1) : "l"(r));
 }
 
+// One node visit of the 8-wide walk: its eight child boxes against the ray
+// (nearer than tmax) -> the group of hit interior children (gBase; gBits holds
+// the hits at bit 24 + (slot XOR octant) and the interior mask at bit 16) and
+// the hit leaves' items (tBase, tBits).
+__device__ __forceinline__ void wide_visit(const DevScene& S, uint32_t node, float3 wro, float3 binv, uint32_t oct,
+                                           float tmax, const uint4* sWide, uint32_t nWide, Visits& vis,
+                                           uint32_t& gBase, uint32_t& gBits, uint32_t& tBase, uint32_t& tBits) {
+    uint4 h0, h1, qa, qb, qc;
+    if (node < nWide) {
+        const uint4* p = sWide + 5u * node;
+        h0 = p[0];
+        h1 = p[1];
+        qa = p[2];
+        qb = p[3];
+        qc = p[4];
+    } else {
+        const uint4* p = S.wideNodes + 5u * node;
+        h0 = __ldg(p);
+        h1 = __ldg(p + 1);
+        qa = __ldg(p + 2);
+        qb = __ldg(p + 3);
+        qc = __ldg(p + 4);
+    }
+    vis.blas += 8;
+    // per axis: t = q * (2^e * inv) + (p - o) * inv, near plane first
+    const float sx = __uint_as_float((h0.w & 0xFFu) << 23) * binv.x;
+    const float sy = __uint_as_float(((h0.w >> 8) & 0xFFu) << 23) * binv.y;
+    const float sz = __uint_as_float(((h0.w >> 16) & 0xFFu) << 23) * binv.z;
+    const float ox = (__uint_as_float(h0.x) - wro.x) * binv.x;
+    const float oy = (__uint_as_float(h0.y) - wro.y) * binv.y;
+    const float oz = (__uint_as_float(h0.z) - wro.z) * binv.z;
+    // lo words: x (qa.x, qa.y) y (qa.z, qa.w) z (qb.x, qb.y); hi words: x (qb.z, qb.w) y (qc.x, qc.y) z (qc.z, qc.w)
+    const bool nx = oct & 1u, ny = oct & 2u, nz = oct & 4u;
+    const uint32_t nearX0 = nx ? qb.z : qa.x, nearX1 = nx ? qb.w : qa.y;
+    const uint32_t farX0 = nx ? qa.x : qb.z, farX1 = nx ? qa.y : qb.w;
+    const uint32_t nearY0 = ny ? qc.x : qa.z, nearY1 = ny ? qc.y : qa.w;
+    const uint32_t farY0 = ny ? qa.z : qc.x, farY1 = ny ? qa.w : qc.y;
+    const uint32_t nearZ0 = nz ? qc.z : qb.x, nearZ1 = nz ? qc.w : qb.y;
+    const uint32_t farZ0 = nz ? qb.x : qc.z, farZ1 = nz ? qb.y : qc.w;
+    uint32_t bits = 0;  // hit mask over slots (SB_WIDE_HITMASK), else traversal bits
+    // child s's box against the ray from its six plane distances
+    auto child = [&](uint32_t s, float tnx, float tny, float tnz, float tfx, float tfy, float tfz) {
+        const float tNear = max3f(tnx, tny, tnz);
+        const float tFar = min3f(tfx, tfy, tfz);
+        const bool hit = tFar >= fmaxf(tNear, 0.0f) && tNear < tmax;
+#if SB_WIDE_HITMASK
+        bits |= (hit ? 1u : 0u) << s;
+#else
+        if (hit) {
+            const uint32_t m = (s < 4 ? h1.z : h1.w) >> (8u * (s & 3u)) & 0xFFu;
+            uint32_t sh = m & 31u;
+            if (sh >= 24u) sh ^= oct;
+            bits |= (m >> 5) << sh;
+        }
+#endif
+    };
+#if SB_WIDE_F32X2
+    const unsigned long long sx2 = pack2(sx, sx), sy2 = pack2(sy, sy), sz2 = pack2(sz, sz);
+    const unsigned long long ox2 = pack2(ox, ox), oy2 = pack2(oy, oy), oz2 = pack2(oz, oz);
+#pragma unroll
+    for (uint32_t s = 0; s < 8; s += 2) {  // two children per packed operation
+        const uint32_t b = s & 3u;
+        float nx0, nx1, ny0, ny1, nz0, nz1, fx0, fx1, fy0, fy1, fz0, fz1;
+        q_pair(s < 4 ? nearX0 : nearX1, b, sx2, ox2, nx0, nx1);
+        q_pair(s < 4 ? nearY0 : nearY1, b, sy2, oy2, ny0, ny1);
+        q_pair(s < 4 ? nearZ0 : nearZ1, b, sz2, oz2, nz0, nz1);
+        q_pair(s < 4 ? farX0 : farX1, b, sx2, ox2, fx0, fx1);
+        q_pair(s < 4 ? farY0 : farY1, b, sy2, oy2, fy0, fy1);
+        q_pair(s < 4 ? farZ0 : farZ1, b, sz2, oz2, fz0, fz1);
+        child(s, nx0, ny0, nz0, fx0, fy0, fz0);
+        child(s + 1u, nx1, ny1, nz1, fx1, fy1, fz1);
+    }
+#else
+#pragma unroll
+    for (uint32_t s = 0; s < 8; ++s) {
+        const uint32_t b = s & 3u;
+        child(s, fmaf(q_at(s < 4 ? nearX0 : nearX1, b), sx, ox), fmaf(q_at(s < 4 ? nearY0 : nearY1, b), sy, oy),
+              fmaf(q_at(s < 4 ? nearZ0 : nearZ1, b), sz, oz), fmaf(q_at(s < 4 ? farX0 : farX1, b), sx, ox),
+              fmaf(q_at(s < 4 ? farY0 : farY1, b), sy, oy), fmaf(q_at(s < 4 ? farZ0 : farZ1, b), sz, oz));
+    }
+#endif
+#if SB_WIDE_HITMASK
+    {
+        // interior hits to bit (slot XOR octant): visiting the lowest first goes near to far
+        const uint32_t imask = h0.w >> 24;
+        uint32_t ih = bits & imask;
+        if (oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+        if (oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+        if (oct & 4u) ih = ((ih & 0x0Fu) << 4) | (ih >> 4);
+        // leaf hits: each one's item bits at its offset
+        uint32_t lh = bits & ~imask & 0xFFu, items = 0;
+        while (lh) {
+            const uint32_t s = __ffs(lh) - 1u;
+            lh &= lh - 1u;
+            const uint32_t m = __byte_perm(h1.z, h1.w, s) & 0xFFu;
+            items |= (m >> 5) << (m & 31u);
+        }
+        bits = ih << 24 | items;
+    }
+#endif
+    gBase = h1.x;
+    gBits = (bits & 0xFF000000u) | ((h0.w >> 24) << 16);
+    tBase = h1.y;
+    tBits = bits & 0x00FFFFFFu;
+}
+
+// The items of the hit leaves (tBits over the run at tBase) against the ray,
+// in slot order so that consecutive items share the local ray. True on an any
+// hit (ANY); closest hits shrink tmax.
+template <bool ANY>
+__device__ __forceinline__ bool wide_items(const DevScene& S, uint32_t tBase, uint32_t tBits, float3 wro, float3 wrd,
+                                           uint32_t& lslot, float3& lro, float3& lrd, float& dSign, float& tmax,
+                                           int& bestTri, int& bestInst, float& bu, float& bv, Visits& vis) {
+    while (tBits) {
+        const uint32_t k = __ffs(tBits) - 1u;
+        tBits &= tBits - 1u;
+        const uint2 it = __ldg(S.wideItems + tBase + k);
+        const uint32_t tri = it.x, slot = it.y;
+        if (slot != lslot) {
+            if (__ldg(S.slotSkip + slot)) continue;
+            const float4 r0 = __ldg(S.inst + 4 * slot), r1 = __ldg(S.inst + 4 * slot + 1),
+                         r2 = __ldg(S.inst + 4 * slot + 2);
+            lro = mk(dot3(xyz(r0), wro) + r0.w, dot3(xyz(r1), wro) + r1.w, dot3(xyz(r2), wro) + r2.w);
+            lrd = mk(dot3(xyz(r0), wrd), dot3(xyz(r1), wrd), dot3(xyz(r2), wrd));
+            dSign = __ldg(&S.inst[4 * slot + 3].z);
+            lslot = slot;
+            ++vis.inst;
+        }
+        float t, det, u, v;
+        uint32_t hb;
+        ++vis.tri;
+        if (!mt_hit(S.tris, tri, lro, lrd, tmax, t, det, u, v, hb)) continue;
+        if (ANY) {
+            if ((hb & TB_SHADOW_OK) && side_ok(hb, det * dSign)) return true;
+        } else if (side_ok(hb, det * dSign) && (hb & TB_CLOSEST_OK)) {
+            tmax = t;
+            bestTri = (int)tri;
+            bestInst = (int)slot;
+            bu = u;
+            bv = v;
+        }
+    }
+    return false;
+}
+
 // `sWide` holds the first `nWide` nodes of the tree (the top levels: nodes are
 // numbered breadth-first) staged in shared memory, or nWide == 0.
 template <bool ANY>
@@ -720,140 +865,117 @@ __device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 
                 done = true;
                 break;
             }
-            uint4 h0, h1, qa, qb, qc;
-            if (node < nWide) {
-                const uint4* p = sWide + 5u * node;
-                h0 = p[0];
-                h1 = p[1];
-                qa = p[2];
-                qb = p[3];
-                qc = p[4];
-            } else {
-                const uint4* p = S.wideNodes + 5u * node;
-                h0 = __ldg(p);
-                h1 = __ldg(p + 1);
-                qa = __ldg(p + 2);
-                qb = __ldg(p + 3);
-                qc = __ldg(p + 4);
-            }
+            wide_visit(S, node, wro, binv, oct, tmax, sWide, nWide, vis, gBase, gBits, tBase, tBits);
             node = FLAT_NONE;
-            vis.blas += 8;
-            // per axis: t = q * (2^e * inv) + (p - o) * inv, near plane first
-            const float sx = __uint_as_float((h0.w & 0xFFu) << 23) * binv.x;
-            const float sy = __uint_as_float(((h0.w >> 8) & 0xFFu) << 23) * binv.y;
-            const float sz = __uint_as_float(((h0.w >> 16) & 0xFFu) << 23) * binv.z;
-            const float ox = (__uint_as_float(h0.x) - wro.x) * binv.x;
-            const float oy = (__uint_as_float(h0.y) - wro.y) * binv.y;
-            const float oz = (__uint_as_float(h0.z) - wro.z) * binv.z;
-            // lo words: x (qa.x, qa.y) y (qa.z, qa.w) z (qb.x, qb.y); hi words: x (qb.z, qb.w) y (qc.x, qc.y) z (qc.z, qc.w)
-            const bool nx = oct & 1u, ny = oct & 2u, nz = oct & 4u;
-            const uint32_t nearX0 = nx ? qb.z : qa.x, nearX1 = nx ? qb.w : qa.y;
-            const uint32_t farX0 = nx ? qa.x : qb.z, farX1 = nx ? qa.y : qb.w;
-            const uint32_t nearY0 = ny ? qc.x : qa.z, nearY1 = ny ? qc.y : qa.w;
-            const uint32_t farY0 = ny ? qa.z : qc.x, farY1 = ny ? qa.w : qc.y;
-            const uint32_t nearZ0 = nz ? qc.z : qb.x, nearZ1 = nz ? qc.w : qb.y;
-            const uint32_t farZ0 = nz ? qb.x : qc.z, farZ1 = nz ? qb.y : qc.w;
-            uint32_t bits = 0;  // hit mask over slots (SB_WIDE_HITMASK), else traversal bits
-            // child s's box against the ray from its six plane distances
-            auto child = [&](uint32_t s, float tnx, float tny, float tnz, float tfx, float tfy, float tfz) {
-                const float tNear = max3f(tnx, tny, tnz);
-                const float tFar = min3f(tfx, tfy, tfz);
-                const bool hit = tFar >= fmaxf(tNear, 0.0f) && tNear < tmax;
-#if SB_WIDE_HITMASK
-                bits |= (hit ? 1u : 0u) << s;
-#else
-                if (hit) {
-                    const uint32_t m = (s < 4 ? h1.z : h1.w) >> (8u * (s & 3u)) & 0xFFu;
-                    uint32_t sh = m & 31u;
-                    if (sh >= 24u) sh ^= oct;
-                    bits |= (m >> 5) << sh;
-                }
-#endif
-            };
-#if SB_WIDE_F32X2
-            const unsigned long long sx2 = pack2(sx, sx), sy2 = pack2(sy, sy), sz2 = pack2(sz, sz);
-            const unsigned long long ox2 = pack2(ox, ox), oy2 = pack2(oy, oy), oz2 = pack2(oz, oz);
-#pragma unroll
-            for (uint32_t s = 0; s < 8; s += 2) {  // two children per packed operation
-                const uint32_t b = s & 3u;
-                float nx0, nx1, ny0, ny1, nz0, nz1, fx0, fx1, fy0, fy1, fz0, fz1;
-                q_pair(s < 4 ? nearX0 : nearX1, b, sx2, ox2, nx0, nx1);
-                q_pair(s < 4 ? nearY0 : nearY1, b, sy2, oy2, ny0, ny1);
-                q_pair(s < 4 ? nearZ0 : nearZ1, b, sz2, oz2, nz0, nz1);
-                q_pair(s < 4 ? farX0 : farX1, b, sx2, ox2, fx0, fx1);
-                q_pair(s < 4 ? farY0 : farY1, b, sy2, oy2, fy0, fy1);
-                q_pair(s < 4 ? farZ0 : farZ1, b, sz2, oz2, fz0, fz1);
-                child(s, nx0, ny0, nz0, fx0, fy0, fz0);
-                child(s + 1u, nx1, ny1, nz1, fx1, fy1, fz1);
-            }
-#else
-#pragma unroll
-            for (uint32_t s = 0; s < 8; ++s) {
-                const uint32_t b = s & 3u;
-                child(s, fmaf(q_at(s < 4 ? nearX0 : nearX1, b), sx, ox), fmaf(q_at(s < 4 ? nearY0 : nearY1, b), sy, oy),
-                      fmaf(q_at(s < 4 ? nearZ0 : nearZ1, b), sz, oz), fmaf(q_at(s < 4 ? farX0 : farX1, b), sx, ox),
-                      fmaf(q_at(s < 4 ? farY0 : farY1, b), sy, oy), fmaf(q_at(s < 4 ? farZ0 : farZ1, b), sz, oz));
-            }
-#endif
-#if SB_WIDE_HITMASK
-            {
-                // interior hits to bit (slot XOR octant): visiting the lowest first goes near to far
-                const uint32_t imask = h0.w >> 24;
-                uint32_t ih = bits & imask;
-                if (oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
-                if (oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
-                if (oct & 4u) ih = ((ih & 0x0Fu) << 4) | (ih >> 4);
-                // leaf hits: each one's item bits at its offset
-                uint32_t lh = bits & ~imask & 0xFFu, items = 0;
-                while (lh) {
-                    const uint32_t s = __ffs(lh) - 1u;
-                    lh &= lh - 1u;
-                    const uint32_t m = __byte_perm(h1.z, h1.w, s) & 0xFFu;
-                    items |= (m >> 5) << (m & 31u);
-                }
-                bits = ih << 24 | items;
-            }
-#endif
-            gBase = h1.x;
-            gBits = (bits & 0xFF000000u) | ((h0.w >> 24) << 16);
-            tBase = h1.y;
-            tBits = bits & 0x00FFFFFFu;
             if (tBits) break;
         }
         if (done) break;
         // leaf phase (warp-aligned): items in slot order share the local ray
-        while (tBits) {
-            const uint32_t k = __ffs(tBits) - 1u;
-            tBits &= tBits - 1u;
-            const uint2 it = __ldg(S.wideItems + tBase + k);
-            const uint32_t tri = it.x, slot = it.y;
-            if (slot != lslot) {
-                if (__ldg(S.slotSkip + slot)) continue;
-                const float4 r0 = __ldg(S.inst + 4 * slot), r1 = __ldg(S.inst + 4 * slot + 1),
-                             r2 = __ldg(S.inst + 4 * slot + 2);
-                lro = mk(dot3(xyz(r0), wro) + r0.w, dot3(xyz(r1), wro) + r1.w, dot3(xyz(r2), wro) + r2.w);
-                lrd = mk(dot3(xyz(r0), wrd), dot3(xyz(r1), wrd), dot3(xyz(r2), wrd));
-                dSign = __ldg(&S.inst[4 * slot + 3].z);
-                lslot = slot;
-                ++vis.inst;
-            }
-            float t, det, u, v;
-            uint32_t hb;
-            ++vis.tri;
-            if (!mt_hit(S.tris, tri, lro, lrd, tmax, t, det, u, v, hb)) continue;
-            if (ANY) {
-                if ((hb & TB_SHADOW_OK) && side_ok(hb, det * dSign)) return true;
-            } else if (side_ok(hb, det * dSign) && (hb & TB_CLOSEST_OK)) {
-                tmax = t;
-                bestTri = (int)tri;
-                bestInst = (int)slot;
-                bu = u;
-                bv = v;
-            }
-        }
+        if (wide_items<ANY>(S, tBase, tBits, wro, wrd, lslot, lro, lrd, dSign, tmax, bestTri, bestInst, bu, bv, vis))
+            return true;
     }
     if (!SB_DYN_FIRST && dyn_walk<ANY>(S, wro, wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
     return ANY ? false : bestTri >= 0;
+}
+
+// The same walk held between rounds (wide_begin, wide_step, wide_end), so that
+// a persistent warp can give a lane a new ray as soon as its walk ends (the
+// closest-hit stage's per-lane refill). Only that caller uses it: wide_walk
+// keeps its state in registers, which a held walk cannot.
+struct WideWalk {
+    float3 wro, wrd, binv;
+    uint32_t oct;
+    uint32_t node;          // next node to visit, or FLAT_NONE
+    uint32_t gBase, gBits;  // the group of hit interior children being visited
+    uint32_t lslot;         // slot of the cached local ray
+    float3 lro, lrd;
+    float dSign;
+    uint32_t iter;
+    int sp;
+    uint2 stk[SB_STACK];
+};
+
+// The moved slots first (SB_DYN_FIRST) and the walk's start. True: an any hit
+// among the moved slots (the walk is over).
+template <bool ANY>
+__device__ __forceinline__ bool wide_begin(const DevScene& S, WideWalk& w, float3 wro, float3 wrd, float& tmax,
+                                           int& bestTri, int& bestInst, float& bu, float& bv, Visits& vis,
+                                           uint32_t* err) {
+    const float3 winv = mk(1.0f / wrd.x, 1.0f / wrd.y, 1.0f / wrd.z);
+    if (SB_DYN_FIRST && dyn_walk<ANY>(S, wro, wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
+    // the inverse clamped to +-1e30, as in wide_walk
+    w.binv = mk(fminf(fmaxf(winv.x, -1e30f), 1e30f), fminf(fmaxf(winv.y, -1e30f), 1e30f),
+                fminf(fmaxf(winv.z, -1e30f), 1e30f));
+    w.oct = (w.binv.x < 0.0f ? 1u : 0u) | (w.binv.y < 0.0f ? 2u : 0u) | (w.binv.z < 0.0f ? 4u : 0u);
+    w.wro = wro;
+    w.wrd = wrd;
+    w.sp = 0;
+    w.node = 0;  // the root (the wide tree is only built when non-empty)
+    w.gBase = 0;
+    w.gBits = 0;
+    w.lslot = FLAT_NONE;
+    w.lro = wro;
+    w.lrd = wrd;
+    w.dSign = 1.0f;
+    w.iter = 0;
+    return false;
+}
+
+// After the tree: the moved slots when they go last, and the walk's result.
+template <bool ANY>
+__device__ __forceinline__ bool wide_end(const DevScene& S, const WideWalk& w, float& tmax, int& bestTri,
+                                         int& bestInst, float& bu, float& bv, Visits& vis, uint32_t* err) {
+    if (!SB_DYN_FIRST) {
+        const float3 winv = mk(1.0f / w.wrd.x, 1.0f / w.wrd.y, 1.0f / w.wrd.z);
+        if (dyn_walk<ANY>(S, w.wro, w.wrd, winv, tmax, bestTri, bestInst, bu, bv, vis, err)) return true;
+    }
+    return ANY ? false : bestTri >= 0;
+}
+
+// One round: nodes until this lane holds items to test (or has nothing left),
+// then those items. Returns 0 to go on, 1 when the tree is done (or a capacity
+// / watchdog error ended it), 2 on an any hit.
+template <bool ANY>
+__device__ __forceinline__ int wide_step(const DevScene& S, WideWalk& w, float& tmax, int& bestTri, int& bestInst,
+                                         float& bu, float& bv, Visits& vis, uint32_t* err,
+                                         const uint4* sWide = nullptr, uint32_t nWide = 0) {
+    uint32_t tBase = 0, tBits = 0;
+    for (;;) {
+        if (w.node == FLAT_NONE) {
+            if (w.gBits >> 24) {
+                const uint32_t key = __ffs(w.gBits >> 24) - 1u;
+                w.gBits &= ~(1u << (24u + key));
+                const uint32_t slot = key ^ w.oct;
+                w.node = w.gBase + __popc((w.gBits >> 16) & 0xFFu & ((1u << slot) - 1u));
+                if (w.gBits >> 24) {
+                    if (w.sp >= SB_STACK) {  // unreachable: the tree's depth was checked on build
+                        latch(err, ERR_CAPACITY);
+                        return 1;
+                    }
+                    w.stk[w.sp++] = make_uint2(w.gBase, w.gBits);
+                }
+                w.gBits = 0;
+            } else if (w.sp > 0) {
+                --w.sp;
+                w.gBase = w.stk[w.sp].x;
+                w.gBits = w.stk[w.sp].y;
+                continue;
+            } else {
+                return 1;
+            }
+        }
+        if (++w.iter > (1u << 26)) {
+            latch(err, ERR_WATCHDOG);
+            return 1;
+        }
+        wide_visit(S, w.node, w.wro, w.binv, w.oct, tmax, sWide, nWide, vis, w.gBase, w.gBits, tBase, tBits);
+        w.node = FLAT_NONE;
+        if (tBits) break;
+    }
+    return wide_items<ANY>(S, tBase, tBits, w.wro, w.wrd, w.lslot, w.lro, w.lrd, w.dSign, tmax, bestTri, bestInst, bu,
+                           bv, vis)
+               ? 2
+               : 0;
 }
 
 // Traversal schedule per query kind: 0 nested (as the reference), 1 unified
