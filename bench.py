@@ -314,6 +314,9 @@ def run_ours(args, dist: Dist):
             parts = ln.split()
             if len(parts) >= 2 and parts[0].startswith("k_") and parts[1].isdigit():
                 traffic[parts[0]] = int(parts[1])
+        # the primary stage is timed over the closest-hit kernel and the emission kernel
+        if "k_trace_primary" in traffic and "k_emit" in traffic:
+            traffic["k_trace_primary"] += traffic["k_emit"]
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

@@ -470,17 +470,99 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary_ba
     const uint32_t lane = threadIdx.x & 31u;
     Visits vis = {0, 0, 0, 0};
     uint32_t nRays = 0;
+    if (!SB_PRIMARY_REFILL) {
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&B.work[0], 32u);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= B.totalRays) break;
+            const BatchItem& I = B.it[batch_item(B, base)];
+            const uint32_t g = base + lane - I.rayBase;
+            if (g >= I.rays || !*I.W.S.valid) continue;
+            const bool pairs = closest_pairs(I.W.S);
+            primary_ray(I.W, pairs ? I.W.S.tlasPairs : I.W.S.tlas, pairs, g, vis);
+            ++nRays;
+        }
+        add_visits(B.counters, 2, nRays, vis);
+        return;
+    }
+    // Per-lane refill within one item at a time (the item index stays
+    // warp-uniform, so the parameter-space reads of its context stay uniform):
+    // the warp takes 32-ray chunks and hands their rays to idle lanes; a chunk
+    // of another item waits until every lane is idle. Items without an 8-wide
+    // tree run their chunks as 32-ray batches (primary_ray).
+    const uint32_t NONE = 0xFFFFFFFFu;
+    uint32_t item = NONE, cur = 0, curEnd = 0, pend = NONE;  // warp-uniform
+    bool more = true;
+    WideWalk w;
+    uint32_t slot = 0, k = 0;
+    float bestT = T_MAX, bu = 0.0f, bv = 0.0f;
+    int tri = -1, inst = -1;
+    bool has = false;
     for (;;) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&B.work[0], 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= B.totalRays) break;
-        const BatchItem& I = B.it[batch_item(B, base)];
-        const uint32_t g = base + lane - I.rayBase;
-        if (g >= I.rays || !*I.W.S.valid) continue;
-        const bool pairs = closest_pairs(I.W.S);
-        primary_ray(I.W, pairs ? I.W.S.tlasPairs : I.W.S.tlas, pairs, g, vis);
-        ++nRays;
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !has);
+        if (cur == curEnd) {
+            if (pend == NONE && more) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&B.work[0], 32u);
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= B.totalRays) more = false;
+                else pend = base;
+            }
+            if (pend != NONE) {
+                const uint32_t pi = batch_item(B, pend);
+                if (pi == item || need == 0xFFFFFFFFu) {
+                    const BatchItem& P = B.it[pi];
+                    item = pi;
+                    cur = pend;
+                    curEnd = min(pend + 32u, P.rayBase + P.rays);  // item ranges are 32-aligned
+                    if (cur > curEnd || !*P.W.S.valid) cur = curEnd;
+                    pend = NONE;
+                }
+            }
+        }
+        if (cur < curEnd) {
+            const BatchItem& I = B.it[item];
+            if (!I.W.S.wideNodes) {
+                if (need == 0xFFFFFFFFu) {  // a 32-ray batch, as without refill
+                    const uint32_t g = cur + lane - I.rayBase;
+                    if (cur + lane < curEnd) {
+                        const bool pairs = closest_pairs(I.W.S);
+                        primary_ray(I.W, pairs ? I.W.S.tlasPairs : I.W.S.tlas, pairs, g, vis);
+                        ++nRays;
+                    }
+                    cur = curEnd;
+                }
+            } else if (need) {
+                const uint32_t rank = (uint32_t)__popc(need & ((1u << lane) - 1u));
+                const uint32_t n = min((uint32_t)__popc(need), curEnd - cur);
+                if (!has && rank < n) {
+                    ray_of(I.W, cur + rank - I.rayBase, I.W.order != 0, slot, k);
+                    const DevCascade& C = I.W.C;
+                    const float3 ro = probe_world_pos(C, (C.probeOffset + slot) % C.probeTotal);
+                    const float3 rd = ray_dir(k, C.rays, I.W.P.frameJitter);
+                    bestT = T_MAX;
+                    tri = inst = -1;
+                    bu = bv = 0.0f;
+                    wide_begin<false>(I.W.S, w, ro, rd, bestT, tri, inst, bu, bv, vis, I.W.err);
+                    has = true;
+                }
+                cur += n;
+            }
+        }
+        if (!__any_sync(0xFFFFFFFFu, has)) {
+            if (!more && pend == NONE && cur == curEnd) break;
+            continue;
+        }
+        if (has) {
+            const BatchItem& I = B.it[item];
+            if (wide_step<false>(I.W.S, w, bestT, tri, inst, bu, bv, vis, I.W.err)) {
+                wide_end<false>(I.W.S, w, bestT, tri, inst, bu, bv, vis, I.W.err);
+                write_hit(I.W.C, slot, k, tri, inst, bestT, bu, bv);
+                ++nRays;
+                has = false;
+            }
+        }
     }
     add_visits(B.counters, 2, nRays, vis);
 }
