@@ -271,6 +271,25 @@ uint32_t blend_blocks(uint32_t updatedCount) { return (updatedCount + BLEND_PROB
 
 // lightGridKernel, gi_probes.js:1893-1937. Every operation is separately
 // rounded (no contraction) so the lists match an FP32 evaluation exactly.
+// The gate fields of the 64 light records (17 floats each, not 16-byte
+// aligned) as three float4 per light, so the emission stage reads a light's
+// gates with three vector loads: (position, range), (direction, type),
+// (colour, emitter class) = record fields (1-3, 10), (4-6, 0), (7-9, 16).
+__global__ void k_light_gates(const float* lights, float4* gates) {
+    const uint32_t i = threadIdx.x;
+    if (i >= 64u) return;
+    const float* L = lights + i * 17u;
+    gates[3 * i] = make_float4(L[1], L[2], L[3], L[10]);
+    gates[3 * i + 1] = make_float4(L[4], L[5], L[6], L[0]);
+    gates[3 * i + 2] = make_float4(L[7], L[8], L[9], L[16]);
+}
+
+cudaError_t launch_light_gates(const float* lights, float4* gates, cudaStream_t st) {
+    k_light_gates<<<1, 64, 0, st>>>(lights, gates);
+    note_launch();
+    return cudaGetLastError();
+}
+
 __global__ void k_light_grid(float* lights, uint32_t lightCount, DevCascade g0, uint32_t cells) {
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cells) return;

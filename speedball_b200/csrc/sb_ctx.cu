@@ -84,6 +84,7 @@ struct sb_ctx {
     uint32_t lightCount = 0, emitterBase = 0, emitterCount = 0;
     int32_t clustered = 0;
     bool lightGridDirty = false;
+    bool lightGatesDirty = false;  // the gate table lags the light records
     std::vector<float> hostLights;
 
     // 512 TLAS nodes = 32 KB of child pairs per CTA; probe-tile issue order with the closest-hit
@@ -206,6 +207,7 @@ DevScene dev_scene(const sb_ctx* c) {
     S.inst = c->B.inst;
     S.tlas = c->B.tlas;
     S.lights = c->B.lights;
+    S.lightGates = c->B.lightGates;
     S.triIndex = c->B.triIndex;
     S.vertexData = c->B.vertexData;
     S.pairs = c->B.pairs;
@@ -288,6 +290,12 @@ sb_status flat_if_needed(sb_ctx* ctx) {
 }
 
 sb_status light_grid_if_needed(sb_ctx* ctx) {
+    if (ctx->lightGatesDirty) {  // the emission stage's gate table, from the current records
+        size_t cap = ctx->B.lightGates ? 64u * 3u : 0u;
+        CK(grow(ctx->B.lightGates, cap, (size_t)64 * 3));
+        CK(launch_light_gates(ctx->B.lights, ctx->B.lightGates, ctx->stream));
+        ctx->lightGatesDirty = false;
+    }
     if (!ctx->lightGridDirty || !ctx->clustered || !ctx->casc[0].configured) return SB_OK;
     DevCascade g0{};
     fill_grid(g0, ctx->casc[0].grid);
@@ -407,7 +415,7 @@ void sb_destroy(sb_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     SceneBuffers& B = ctx->B;
     release(B.nodes); release(B.triIndex); release(B.vertexData); release(B.triMaterial); release(B.materials);
-    release(B.lights); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
+    release(B.lights); release(B.lightGates); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
     release(B.arrive); release(B.valid); release(B.pairs); release(B.tlasPairs); release(B.depth);
     ctx->flat.release();
     InstanceTable& I = ctx->I;
@@ -599,6 +607,7 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
         ctx->flat.dirty = true;
     }
     if (buf == SB_BUF_LIGHTS && ctx->clustered) ctx->lightGridDirty = true;
+    if (buf == SB_BUF_LIGHTS) ctx->lightGatesDirty = true;
     return SB_OK;
 }
 
@@ -674,6 +683,7 @@ sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count, ui
     ctx->emitterCount = emitterCount;
     ctx->clustered = clustered ? 1 : 0;
     ctx->lightGridDirty = ctx->clustered != 0;
+    ctx->lightGatesDirty = true;
     ++ctx->epoch;
     return SB_OK;
 }

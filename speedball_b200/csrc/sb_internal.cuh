@@ -63,6 +63,7 @@ struct DevScene {
     const float4* inst;        // 4 x float4 per instance slot: 3 inverse rows, (root, end, dSign, active)
     const uint4* tlas;         // 2 x uint4 per TLAS node, same encoding as BLAS nodes, payload (cnt<<24)|off
     const float* lights;       // 64 x 17 records (+ C0 cell lists)
+    const float4* lightGates;  // the records' gate fields, 3 x float4 per light
     const uint32_t* triIndex;  // reference triangle indices (final-hit refinement)
     const float* vertexData;   // reference vertices, 8 floats each
     const uint4* pairs;        // 4 x uint4 per interior BLAS node: both children's boxes + entries

@@ -32,6 +32,7 @@ struct SceneBuffers {
     uint32_t* triMaterial = nullptr;  // triCount
     float* materials = nullptr;       // materialsLen
     float* lights = nullptr;          // lightsLen
+    float4* lightGates = nullptr;     // derived, 64 x 3 (light_gates)
     float4* tris = nullptr;           // derived, triCount*3
     float4* inst = nullptr;           // derived, instCount*4
     uint4* tlas = nullptr;            // derived, tlasNodeCount*2
@@ -81,6 +82,9 @@ cudaError_t launch_blend_bwd(const DevCascade& C, const DevParams& P, const floa
 cudaError_t launch_shade_bwd(const DevScene& S, const DevCascade& C, const DevParams& P, const float4* gR,
                              double* gParam, float4* gA, cudaStream_t st);
 cudaError_t launch_light_grid(float* lights, uint32_t lightCount, const DevCascade& g0, cudaStream_t st);
+// The 64 light records' gate fields as three aligned float4 each: (position, range),
+// (direction, type), (colour, emitter class).
+cudaError_t launch_light_gates(const float* lights, float4* gates, cudaStream_t st);
 cudaError_t launch_clear_cascade(const DevCascade& C, cudaStream_t st);
 
 // Validation + derived-layout packing (sb_pack.cu).

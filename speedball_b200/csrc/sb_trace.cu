@@ -156,7 +156,7 @@ __device__ __forceinline__ uint32_t emit_ray(const WaveCtx& W, bool active, uint
     if (tri >= 0) L = light_list(W, fr.hitPos);
     unsigned long long pass = 0ull;
     for (uint32_t i = 0; i < L.count; ++i)
-        if (light_eval(W, light_at(L, i), fr.hitPos, fr.ng).pass) pass |= 1ull << i;
+        if (light_gate(W, light_at(L, i), fr.hitPos, fr.ng)) pass |= 1ull << i;
     const uint32_t mine = (uint32_t)__popcll(pass);
     uint32_t incl = mine;
 #pragma unroll

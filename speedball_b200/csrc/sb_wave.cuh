@@ -109,13 +109,34 @@ __device__ __forceinline__ LightEval light_eval(const WaveCtx& W, uint32_t li, f
     return e;
 }
 
+// light_eval's pass decision from the gate table (S.lightGates: the same
+// record fields, read as three float4) with the same expressions, so the
+// emission stage decides exactly as the shading stage's light_eval.
+__device__ __forceinline__ bool light_gate(const WaveCtx& W, uint32_t li, float3 hitPos, float3 ng) {
+    const float4 g1 = __ldg(W.S.lightGates + 3u * li + 1u);
+    const float ltype = g1.w;
+    if (!(ltype < 2.5f)) return false;
+    const float4 g0 = __ldg(W.S.lightGates + 3u * li), g2 = __ldg(W.S.lightGates + 3u * li + 2u);
+    const bool isIr = fabsf(g2.w - 4.0f) < 0.25f;
+    const float irs = isIr ? W.P.nirGate * W.P.nirGain : 1.0f;
+    const float3 lcol = xyz(g2) * irs;
+    const bool isDir = ltype < 0.5f;
+    const float3 toLight = isDir ? xyz(g1) * -1.0f : xyz(g0) - hitPos;
+    const float dist = isDir ? 1e4f : fmaxf(sqrtf(dot3(toLight, toLight)), 1e-4f);
+    const float3 wi = normalize3(toLight);
+    const float ndl = fmaxf(dot3(ng, wi), 0.0f);
+    const float lpeak = fmaxf(fmaxf(lcol.x, lcol.y), lcol.z);
+    const float lrange = g0.w;
+    return ndl * lpeak > 0.0f && (isDir || lrange <= 0.0f || dist < lrange);
+}
+
 // The shadow-ray geometry of a light that passed its gates: the direction
-// and distance light_eval forms, from the same record fields and expressions.
+// and distance light_eval forms, from the same fields (gate table) and
+// expressions.
 __device__ __forceinline__ void light_ray(const WaveCtx& W, uint32_t li, float3 hitPos, float3& wi, float& dist) {
-    const float* L = W.S.lights + li * 17u;
-    const bool isDir = __ldg(L) < 0.5f;
-    const float3 toLight = isDir ? mk(__ldg(L + 4), __ldg(L + 5), __ldg(L + 6)) * -1.0f
-                                 : mk(__ldg(L + 1), __ldg(L + 2), __ldg(L + 3)) - hitPos;
+    const float4 g1 = __ldg(W.S.lightGates + 3u * li + 1u);
+    const bool isDir = g1.w < 0.5f;
+    const float3 toLight = isDir ? xyz(g1) * -1.0f : xyz(__ldg(W.S.lightGates + 3u * li)) - hitPos;
     dist = isDir ? 1e4f : fmaxf(sqrtf(dot3(toLight, toLight)), 1e-4f);
     wi = normalize3(toLight);
 }
