@@ -21,7 +21,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
-VARIANT_SOURCES = ("sb_trace.cu",)  # the only sources that read the tuning macros
+VARIANT_SOURCES = ("sb_trace.cu", "sb_refit.cu")  # the only sources that read the tuning macros
 
 
 def sources():

@@ -66,6 +66,9 @@ __global__ void k_refit_orphans(const uint32_t* parent, uint32_t root, uint32_t 
 
 __device__ __forceinline__ float vload(const uint32_t* p) { return __uint_as_float(*(const volatile uint32_t*)p); }
 
+#ifndef SB_REFIT_ACQREL
+#define SB_REFIT_ACQREL 1
+#endif
 __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
                             const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
                             const uint32_t* parent, uint32_t* arrive, uint32_t root, uint32_t end,
@@ -108,9 +111,17 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
     for (;;) {
         uint32_t p = parent[node];
         if (p == NONE) break;
+        // arrival: release publishes this thread's box stores, acquire orders the
+        // sibling's box reads below after the sibling's release (one acq_rel atomic)
+#if SB_REFIT_ACQREL
+        uint32_t prev;
+        asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(arrive + p) : "memory");
+        if (prev == 0u) break;
+#else
         __threadfence();
         if (atomicAdd(&arrive[p], 1u) == 0u) break;
         __threadfence();
+#endif
         arrive[p] = 0u;  // both children arrived: ready for the next refit of this range
         uint32_t l = p + 1;
         uint32_t r = *(const volatile uint32_t*)(nodes + 8 * l + 6);
