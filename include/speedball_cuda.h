@@ -368,7 +368,10 @@ typedef struct sb_tuning {
                                  3 = as 2, with the closest-hit stage's 32-ray
                                  batches issued costliest first, by the cycles
                                  each took in the previous full sb_solve of the
-                                 cascade (sb_solve only; batches run as 2)       */
+                                 cascade (sb_solve only; batches run as 2). On
+                                 the 8-wide tree (bvhKind 1) the closest-hit
+                                 stage refills lanes ray by ray, and 3 acts
+                                 as 2                                            */
     uint32_t smemTlasNodes;   /* TLAS nodes staged in shared memory (0 = none)     */
     uint32_t bvhKind;         /* scene BVH over (triangle, instance) items, rebuilt
                                  on structural changes: 1 = 8-wide nodes with 8-bit
