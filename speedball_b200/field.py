@@ -240,7 +240,8 @@ class ProbeField:
         if self._pendingTopology:
             self._pendingTopology = False
             self._rebuild()
-        self._refresh_lanes()
+        # the uniforms first (host work only), so that the solve is enqueued right
+        # behind the dirty lanes while the GPU runs them
         C0 = 0
         updated = min(self.updatedCap(), self._probeTotal)
         if nowMs is not None and self._lastSolveAt > 0:
@@ -257,6 +258,7 @@ class ProbeField:
         elif self._frameJitterOverride is not None:
             self._params.frameJitter = self._frameJitterOverride
         self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
+        self._refresh_lanes()
         return {"cascade": C0, "probeOffset": self._probeCursor, "updatedCount": updated}
 
     def endTick(self, frame: dict, nowMs: float | None = None) -> None:
