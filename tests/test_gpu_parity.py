@@ -282,3 +282,55 @@ def test_atrium_solve_parity(atrium_field):
     err = gu.texel_rel_err(ga, oa)
     assert err.max() <= gu.TEXEL_REL, (err.max(), int((err > gu.TEXEL_REL).sum()))
     assert (rec["tri"] >= 0).mean() > 0.5
+
+
+def _room_state(edit: str | None):
+    """Room-and-spheres (1 directional + 4 point lights): two solves, then
+    light 2 moved and recoloured through `edit` ('range': sb_upload_range on
+    its record; 'full': sb_upload_lights with every record; None: no edit),
+    then two more solves. Returns the final probe state."""
+    import ctypes as C
+    f = gu.make_field(synth.room_spheres(0))
+    try:
+        for _ in range(2):
+            f.tick()
+        f.synchronize()
+        n = f._lightCount
+        recs = gu.read(f, "LIGHTS", n * 17, np.float32).reshape(n, 17)
+        recs[2, 1:4] += np.float32(1.5)       # position
+        recs[2, 7:10] *= np.float32(0.5)      # colour
+        recs[2, 10] = np.float32(12.0)        # range
+        if edit == "range":
+            rec = np.ascontiguousarray(recs[2])
+            _abi.check(f._lib.sb_upload_range(f.ctx, _abi.BUF["LIGHTS"], 2 * 17, 17, _abi.ptr(rec)), f.ctx)
+        elif edit == "full":
+            allr = np.ascontiguousarray(recs)
+            _abi.check(f._lib.sb_upload_lights(f.ctx, _abi.ptr(allr), n, 0, 0, 0), f.ctx)
+        for _ in range(2):
+            f.tick()
+        f.synchronize()
+        P = f._probeTotal
+        nr = P * f.getRays()
+        r = f.getResolution()
+        W, H = r[0] * 8, r[1] * r[2] * 8
+        return dict(hits=gu.read(f, "HIT_RECORDS", nr * 4, np.uint32), vis=gu.read(f, "VISIBILITY", nr * 4, np.uint32),
+                    irr=gu.read(f, "IRRADIANCE_HISTORY", P * 256, np.float32),
+                    atlas=gu.read(f, "IRRADIANCE_ATLAS", W * H * 4, np.uint16))
+    finally:
+        f.dispose()
+
+
+def test_ranged_light_edit_reaches_the_emission_gates():
+    """The emission stage tests each candidate light's gates from a derived
+    table of the light records. A ranged write into the records must refresh
+    that table before the next solve: editing one light through
+    sb_upload_range gives bit for bit what a full sb_upload_lights of the
+    same records gives, and differs from not editing it."""
+    ranged = _room_state("range")
+    full = _room_state("full")
+    plain = _room_state(None)
+    for key in ranged:
+        bad = np.flatnonzero(ranged[key] != full[key])
+        assert bad.size == 0, (key, bad.size, bad[:8])
+    assert not np.array_equal(ranged["vis"], plain["vis"])
+    assert not np.array_equal(ranged["atlas"], plain["atlas"])
