@@ -517,9 +517,9 @@ cudaError_t launch_update_instances(const SceneBuffers& B, const InstanceTable& 
 
 // refitFlatTlasRange over the frozen partition, deepest level first (the
 // body of one CTA; the caller's writes to liveBounds precede a barrier).
-__device__ __forceinline__ void tlas_refit_body(const SceneBuffers& B, const InstanceTable& I) {
-    const uint32_t nn = B.tlasNodeCount;
-    const int maxDepth = (int)*(volatile uint32_t*)I.scratch;
+// The level pass on the records in global memory (larger TLASes).
+__device__ __forceinline__ void tlas_refit_levels(const SceneBuffers& B, const InstanceTable& I, uint32_t nn,
+                                                  int maxDepth) {
     for (int d = maxDepth; d >= 0; --d) {
         for (uint32_t i = threadIdx.x; i < nn; i += blockDim.x) {
             if (I.nodeDepth[i] != (uint32_t)d) continue;
@@ -551,7 +551,10 @@ __device__ __forceinline__ void tlas_refit_body(const SceneBuffers& B, const Ins
         }
         __syncthreads();
     }
-    // the traversal's child-pair copy of the refit bounds (entries are structural)
+}
+
+// The traversal's child-pair copy of the refit bounds (entries are structural).
+__device__ __forceinline__ void tlas_refit_pairs(const SceneBuffers& B, uint32_t nn) {
     if (!B.tlasPairs) return;
     for (uint32_t i = threadIdx.x; i < nn; i += blockDim.x) {
         uint4 b = B.tlas[2 * i + 1];
@@ -563,6 +566,66 @@ __device__ __forceinline__ void tlas_refit_body(const SceneBuffers& B, const Ins
         const uint32_t b1[6] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y};
         store_pair_boxes(B.tlasPairs + 4u * i, b0, b1);
     }
+}
+
+// TLASes of up to this many nodes run the level pass on a shared-memory copy
+// of the boxes, structure words and depths (the same min / max on the same
+// values; every node is still written to the records as it is refit), so a
+// level reads its children from shared memory instead of global memory.
+#ifndef SB_TLAS_STAGE_NODES
+#define SB_TLAS_STAGE_NODES 512
+#endif
+constexpr uint32_t TLAS_STAGE_NODES = SB_TLAS_STAGE_NODES > 0 ? SB_TLAS_STAGE_NODES : 1;
+
+__device__ __forceinline__ void tlas_refit_body(const SceneBuffers& B, const InstanceTable& I) {
+    const uint32_t nn = B.tlasNodeCount;
+    const int maxDepth = (int)*(volatile uint32_t*)I.scratch;
+    if (SB_TLAS_STAGE_NODES > 0 && nn <= TLAS_STAGE_NODES) {
+        __shared__ float sBox[6 * TLAS_STAGE_NODES];
+        __shared__ uint32_t sMiss[TLAS_STAGE_NODES], sOff[TLAS_STAGE_NODES], sCnt[TLAS_STAGE_NODES],
+            sDepth[TLAS_STAGE_NODES];
+        const float* T = B.materials + B.tlasBase;
+        for (uint32_t i = threadIdx.x; i < nn; i += blockDim.x) {
+            const float* N = T + (size_t)i * 12u;
+            for (int k = 0; k < 6; ++k) sBox[6 * i + k] = N[k];
+            sMiss[i] = (uint32_t)N[6];
+            sOff[i] = (uint32_t)N[7];
+            sCnt[i] = N[8] > 0.0f ? (uint32_t)N[8] : 0u;
+            sDepth[i] = I.nodeDepth[i];
+        }
+        __syncthreads();
+        for (int d = maxDepth; d >= 0; --d) {
+            for (uint32_t i = threadIdx.x; i < nn; i += blockDim.x) {
+                if (sDepth[i] != (uint32_t)d) continue;
+                float bx[6];
+                const uint32_t cnt = sCnt[i];
+                if (cnt > 0u) {
+                    const uint32_t off = sOff[i];
+                    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+                    for (uint32_t s = off; s < off + cnt; ++s) {
+                        const float* b = I.liveBounds + (size_t)s * 6u;
+                        for (int k = 0; k < 3; ++k) {
+                            if (b[k] < mn[k]) mn[k] = b[k];
+                            if (b[3 + k] > mx[k]) mx[k] = b[3 + k];
+                        }
+                    }
+                    for (int k = 0; k < 3; ++k) { bx[k] = mn[k]; bx[3 + k] = mx[k]; }
+                } else {
+                    const uint32_t l = i + 1, r = sMiss[l];
+                    for (int k = 0; k < 3; ++k) {
+                        bx[k] = js_min(sBox[6 * l + k], sBox[6 * r + k]);
+                        bx[3 + k] = js_max(sBox[6 * l + 3 + k], sBox[6 * r + 3 + k]);
+                    }
+                }
+                for (int k = 0; k < 6; ++k) sBox[6 * i + k] = bx[k];
+                write_tlas_node(B, i, bx, sMiss[i], sOff[i], cnt);
+            }
+            __syncthreads();
+        }
+    } else {
+        tlas_refit_levels(B, I, nn, maxDepth);
+    }
+    tlas_refit_pairs(B, nn);
 }
 
 __global__ void __launch_bounds__(1024) k_tlas_refit(SceneBuffers B, InstanceTable I) { tlas_refit_body(B, I); }
