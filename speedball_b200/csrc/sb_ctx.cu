@@ -69,7 +69,7 @@ struct sb_ctx {
     size_t stageCap = 0;
 
     uint32_t* dErr = nullptr;
-    uint32_t* dGate = nullptr;     // 16 layout verdicts, one per cached refit range
+    uint32_t* dGate = nullptr;     // 16 layout verdicts, one per cached refit range, then their 16 subtree counts
     // Refit ranges whose parent links and layout checks are current: valid while
     // packEpoch is unchanged (no upload touched nodes, indices or materials since).
     struct RefitRange { uint32_t root = 0, end = 0, epoch = 0; bool used = false; };
@@ -383,7 +383,7 @@ sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
         ctx->tune.numSms = ctx->numSms;
         if (cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking) != cudaSuccess) { st = SB_ERR_CUDA; break; }
         ctx->stream = ctx->ownStream;
-        if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 16 * 4) != cudaSuccess ||
+        if (cudaMalloc(&ctx->dErr, 4) != cudaSuccess || cudaMalloc(&ctx->dGate, 32 * 4) != cudaSuccess ||
             cudaMalloc(&ctx->dWork, 64) != cudaSuccess || cudaMalloc(&ctx->dCounters, 16 * 8) != cudaSuccess ||
             cudaMalloc(&ctx->B.valid, 4) != cudaSuccess || cudaMalloc(&ctx->B.depth, 8) != cudaSuccess) {
             st = SB_ERR_OOM;
@@ -416,7 +416,7 @@ void sb_destroy(sb_ctx* ctx) {
     SceneBuffers& B = ctx->B;
     release(B.nodes); release(B.triIndex); release(B.vertexData); release(B.triMaterial); release(B.materials);
     release(B.lights); release(B.lightGates); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
-    release(B.arrive); release(B.valid); release(B.pairs); release(B.tlasPairs); release(B.depth);
+    release(B.arrive); release(B.subRoots); release(B.valid); release(B.pairs); release(B.tlasPairs); release(B.depth);
     ctx->flat.release();
     InstanceTable& I = ctx->I;
     release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb); release(I.invRows);
@@ -517,8 +517,9 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     CK(grow(B.vertexData, ctx->cap[2], nV));
     CK(grow(B.triMaterial, ctx->cap[3], (size_t)v->triCount));
     CK(grow(B.materials, ctx->cap[4], matLen));
-    size_t cTris = 0, cInst = 0, cTlas = 0, cBits = 0, cPar = 0, cArr = 0, cPairs = 0, cTlasPairs = 0;
+    size_t cTris = 0, cInst = 0, cTlas = 0, cBits = 0, cPar = 0, cArr = 0, cSub = 0, cPairs = 0, cTlasPairs = 0;
     release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent); release(B.arrive);
+    release(B.subRoots);
     release(B.pairs); release(B.tlasPairs);
     CK(grow(B.tris, cTris, (size_t)v->triCount * 3));
     CK(grow(B.inst, cInst, (size_t)v->instCount * 4));
@@ -526,6 +527,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     CK(grow(B.matBits, cBits, (size_t)v->materialCount));
     CK(grow(B.parent, cPar, (size_t)v->nodeCount));
     CK(grow(B.arrive, cArr, (size_t)v->nodeCount));
+    CK(grow(B.subRoots, cSub, (size_t)v->nodeCount));
     if (v->nodeCount < PE_BLAS_MAX_NODES) CK(grow(B.pairs, cPairs, (size_t)v->nodeCount * 4));
     CK(grow(B.tlasPairs, cTlasPairs, (size_t)tlasNodes * 4));
     CK(cudaMemsetAsync(B.depth, 0xFF, 8, ctx->stream));  // no pair layout until the pack derives it

@@ -42,6 +42,7 @@ struct SceneBuffers {
     uint32_t* depth = nullptr;        // 2 words: deepest BLAS / TLAS node (DEPTH_UNKNOWN = no pairs)
     uint32_t* parent = nullptr;       // nodeCount: parent of each BLAS node (refit)
     uint32_t* arrive = nullptr;       // nodeCount: refit arrival counters
+    uint32_t* subRoots = nullptr;     // nodeCount: roots of the refit's CTA subtrees, per range from its root
     uint32_t* valid = nullptr;        // 1 word
     uint32_t nodeCount = 0, triCount = 0, vertexCount = 0, materialsLen = 0, materialCount = 0;
     uint32_t instBase = 0, instCount = 0, tlasBase = 0, tlasNodeCount = 0, lightsLen = 0;
@@ -94,7 +95,8 @@ cudaError_t launch_pack_dynamic(const SceneBuffers& B, uint32_t* err, cudaStream
 
 // Refit and TLAS lanes (sb_refit.cu). `validated`: the range's parent links
 // and layout checks from an earlier call on the same layout are still current
-// (their verdict is in *gate), so only the bottom-up pass runs.
+// (their verdict is in *gate, the range's subtree count in gate[16]), so only
+// the bottom-up pass runs.
 cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
                               cudaStream_t st, bool validated = false);
 

@@ -144,6 +144,156 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
     }
 }
 
+// Subtrees of at most REFIT_SUB nodes refit inside one CTA: the threaded
+// layout stores a node's subtree as [i, miss(i)) (to the range end on the right
+// spine), so a CTA takes one such range, computes its leaves, and climbs with
+// shared-memory arrival counters; the thread that completes the subtree root
+// carries on through the global climb above it. The partition (every node
+// whose subtree fits while its parent's does not) is made once per validated
+// range, next to the layout checks.
+#ifndef SB_REFIT_CTA
+#define SB_REFIT_CTA 1
+#endif
+constexpr uint32_t REFIT_SUB = 256;
+
+__device__ __forceinline__ uint32_t sub_size(const uint32_t* nodes, uint32_t i, uint32_t end) {
+    const uint32_t miss = nodes[8 * i + 6];
+    return (miss > i && miss <= end) ? miss - i : end - i;
+}
+
+__global__ void k_refit_partition(const uint32_t* nodes, const uint32_t* parent, uint32_t root, uint32_t end,
+                                  const uint32_t* gate, uint32_t* subRoots, uint32_t* count) {
+    const uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end || *gate == 0u) return;
+    if (sub_size(nodes, i, end) > REFIT_SUB) return;
+    const uint32_t p = parent[i];
+    if (p != NONE && sub_size(nodes, p, end) <= REFIT_SUB) return;
+    subRoots[root + atomicAdd(count, 1u)] = i;  // at most end - root entries
+}
+
+__global__ void __launch_bounds__(REFIT_SUB) k_refit_cta(uint32_t* nodes, const uint32_t* triIndex,
+                                                         const float* vertexData, const uint32_t* triMaterial,
+                                                         const uint32_t* matBits, float4* tris,
+                                                         const uint32_t* parent, uint32_t* arrive, uint32_t root,
+                                                         uint32_t end, const uint32_t* gate, uint4* pairs,
+                                                         const uint32_t* subRoots, const uint32_t* count,
+                                                         uint32_t* err) {
+    __shared__ float sBox[6 * REFIT_SUB];
+    __shared__ uint32_t sArr[REFIT_SUB];
+    if (*gate == 0u) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) latch(err, ERR_LAYOUT);  // the range's verdict stands
+        return;
+    }
+    const uint32_t nSub = *count;
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t t = blockIdx.x; t < nSub; t += gridDim.x) {
+        const uint32_t r0 = subRoots[root + t];
+        const uint32_t sz = min(sub_size(nodes, r0, end), REFIT_SUB);
+        sArr[tid] = 0u;
+        __syncthreads();
+        uint32_t node = NONE;  // the node this thread carries up
+        if (tid < sz) {
+            const uint32_t i = r0 + tid;
+            const uint32_t info = nodes[8 * i + 7];
+            if (info != INTERIOR) {
+                const uint32_t off = info & 0x00FFFFFFu, cnt = info >> 24;
+                uint32_t* n = nodes + 8 * i;
+                if (cnt != 0u) {
+                    float mnx = INFINITY, mny = INFINITY, mnz = INFINITY, mxx = -INFINITY, mxy = -INFINITY,
+                          mxz = -INFINITY;
+                    for (uint32_t tr = off; tr < off + cnt; ++tr) {
+                        float3 p[3];
+                        for (int k = 0; k < 3; ++k) {
+                            const float* v = vertexData + (size_t)triIndex[3 * tr + k] * 8u;
+                            const float x = v[0], y = v[1], z = v[2];
+                            p[k] = make_float3(x, y, z);
+                            if (x < mnx) mnx = x;
+                            if (x > mxx) mxx = x;
+                            if (y < mny) mny = y;
+                            if (y > mxy) mxy = y;
+                            if (z < mnz) mnz = z;
+                            if (z > mxz) mxz = z;
+                        }
+                        tris[3 * tr] = make_float4(p[0].x, p[0].y, p[0].z, __uint_as_float(matBits[triMaterial[tr]]));
+                        tris[3 * tr + 1] = make_float4(p[1].x - p[0].x, p[1].y - p[0].y, p[1].z - p[0].z, 0.0f);
+                        tris[3 * tr + 2] = make_float4(p[2].x - p[0].x, p[2].y - p[0].y, p[2].z - p[0].z, 0.0f);
+                    }
+                    n[0] = __float_as_uint(mnx); n[1] = __float_as_uint(mny); n[2] = __float_as_uint(mnz);
+                    n[3] = __float_as_uint(mxx); n[4] = __float_as_uint(mxy); n[5] = __float_as_uint(mxz);
+                }
+                for (int k = 0; k < 6; ++k) sBox[6 * tid + k] = __uint_as_float(n[k]);
+                node = i;
+            }
+        }
+        // inside the subtree: the second child to finish computes its parent
+        volatile float* vb = sBox;
+        while (node != NONE && node != r0) {
+            const uint32_t p = parent[node];
+            const uint32_t pl = p - r0;  // p lies in [r0, node): the subtree is [r0, r0 + sz)
+            if (p == NONE || pl >= sz) {  // a partition that does not match the layout
+                latch(err, ERR_LAYOUT);
+                node = NONE;
+                break;
+            }
+            __threadfence_block();
+            if (atomicAdd(&sArr[pl], 1u) == 0u) {
+                node = NONE;
+                break;
+            }
+            __threadfence_block();
+            const uint32_t l = p + 1, r = nodes[8 * l + 6];
+            const uint32_t ll = l - r0, rl = r - r0;
+            if (ll >= sz || rl >= sz) {
+                latch(err, ERR_LAYOUT);
+                node = NONE;
+                break;
+            }
+            uint32_t lb[6], rb[6];
+            for (int k = 0; k < 6; ++k) {
+                lb[k] = __float_as_uint(vb[6 * ll + k]);
+                rb[k] = __float_as_uint(vb[6 * rl + k]);
+            }
+            uint32_t* n = nodes + 8 * p;
+            for (int k = 0; k < 3; ++k) {
+                const float mn = js_min(__uint_as_float(lb[k]), __uint_as_float(rb[k]));
+                const float mx = js_max(__uint_as_float(lb[3 + k]), __uint_as_float(rb[3 + k]));
+                n[k] = __float_as_uint(mn);
+                n[3 + k] = __float_as_uint(mx);
+                vb[6 * pl + k] = mn;
+                vb[6 * pl + 3 + k] = mx;
+            }
+            if (pairs) store_pair_boxes(pairs + 4u * p, lb, rb);
+            node = p;
+        }
+        // the subtree root is done: the levels above through global memory
+        while (node != NONE) {
+            const uint32_t p = parent[node];
+            if (p == NONE) break;
+            uint32_t prev;
+            asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;" : "=r"(prev) : "l"(arrive + p) : "memory");
+            if (prev == 0u) break;
+            arrive[p] = 0u;
+            const uint32_t l = p + 1;
+            const uint32_t r = *(const volatile uint32_t*)(nodes + 8 * l + 6);
+            const uint32_t* L = nodes + 8 * l;
+            const uint32_t* Rn = nodes + 8 * r;
+            uint32_t lb[6], rb[6];
+            for (int k = 0; k < 6; ++k) {
+                lb[k] = *(const volatile uint32_t*)(L + k);
+                rb[k] = *(const volatile uint32_t*)(Rn + k);
+            }
+            uint32_t* n = nodes + 8 * p;
+            for (int k = 0; k < 3; ++k) {
+                n[k] = __float_as_uint(js_min(__uint_as_float(lb[k]), __uint_as_float(rb[k])));
+                n[3 + k] = __float_as_uint(js_max(__uint_as_float(lb[3 + k]), __uint_as_float(rb[3 + k])));
+            }
+            if (pairs) store_pair_boxes(pairs + 4u * p, lb, rb);
+            node = p;
+        }
+        __syncthreads();  // the shared arrays serve the next subtree
+    }
+}
+
 cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
                               cudaStream_t st, bool validated) {
     if (end <= root) return cudaSuccess;
@@ -156,6 +306,21 @@ cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end
         k_refit_link<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.triMaterial, B.triCount, B.vertexCount,
                                         B.materialCount, B.parent, root, end, gate, err); note_launch();
         k_refit_orphans<<<g, 256, 0, st>>>(B.parent, root, end, gate, err); note_launch();
+        if (SB_REFIT_CTA) {
+            cudaError_t e2 = cudaMemsetAsync(gate + 16, 0, sizeof(uint32_t), st);  // the range's subtree count
+            if (e2 != cudaSuccess) return e2;
+            k_refit_partition<<<g, 256, 0, st>>>(B.nodes, B.parent, root, end, gate, B.subRoots, gate + 16);
+            note_launch();
+        }
+    }
+    if (SB_REFIT_CTA) {
+        // one CTA per subtree (the count is on the device; idle CTAs return at once)
+        const unsigned ctas = n < 1184u ? n : 1184u;
+        k_refit_cta<<<ctas, REFIT_SUB, 0, st>>>(B.nodes, B.triIndex, B.vertexData, B.triMaterial, B.matBits, B.tris,
+                                                B.parent, B.arrive, root, end, gate, B.pairs, B.subRoots, gate + 16,
+                                                err);
+        note_launch();
+        return cudaGetLastError();
     }
     k_refit_run<<<g, 256, 0, st>>>(B.nodes, B.triIndex, B.vertexData, B.triMaterial, B.matBits, B.tris, B.parent,
                                    B.arrive, root, end, gate, B.pairs, err); note_launch();
