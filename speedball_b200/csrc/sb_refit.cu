@@ -154,7 +154,10 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
 #ifndef SB_REFIT_CTA
 #define SB_REFIT_CTA 1
 #endif
-constexpr uint32_t REFIT_SUB = 256;
+#ifndef SB_REFIT_SUB
+#define SB_REFIT_SUB 256
+#endif
+constexpr uint32_t REFIT_SUB = SB_REFIT_SUB;  // nodes per CTA subtree (= threads per CTA)
 
 __device__ __forceinline__ uint32_t sub_size(const uint32_t* nodes, uint32_t i, uint32_t end) {
     const uint32_t miss = nodes[8 * i + 6];
