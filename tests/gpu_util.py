@@ -11,7 +11,7 @@ from speedball_b200.field import ProbeField
 
 import orc
 
-# Tolerances written in the tests (north_star): hit t 1e-5 relative, texels
+# Parity tolerances of the update path: hit t 1e-5 relative, texels
 # 1e-3 relative; near-tie exemption when the two nearest candidates are within
 # 1e-6 relative.
 T_REL = 1e-5
