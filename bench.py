@@ -321,11 +321,7 @@ def run_ours(args, dist: Dist):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural atrium standing in for Sponza)",
-        "config": {"workload": "atrium 262,267 tris / 30 meshes, 16^3 probes x 64 rays, 32 clustered point + 1 "
-                               "directional light, 1 deforming + 3 moving meshes per frame",
-                   "probes": P, "rays_per_probe": f.getRays(), "primary_rays_per_step": rays,
-                   "triangles": int(pool.triIndex.shape[0]), "l2": "flushed (256 MiB write) before every timed step",
-                   "parallelism": "replicas" if dist.world > 1 else "single GPU"},
+        "config": atrium_config(P, f.getRays(), int(pool.triIndex.shape[0]), dist.world),
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e_ms, 4),
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
@@ -355,84 +351,140 @@ def _stats(lib, ctx):
 
 
 # ----------------------------------------------------- CPU (reference arm)
-def _cpu_setup(scene):
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import orc
-    from speedball_b200 import scene as sc
-    from speedball_b200.field import selectGiLightRecords
-    pool = sc.build_pool(scene)
-    mats, order, live, aabb = orc.compute_tail(pool)
-    keep = [pool]  # the scene struct points into the pool's arrays
-    S = orc.scene_struct(pool, mats, keep=keep)
-    g = dict(scene.meta["grid"])
-    gs = np.asarray(g["gridSize"], np.float32)
-    g["maxDist"] = float(np.linalg.norm(gs.astype(np.float64)))
-    res = g["res"]
-    g["cellMin"] = float(max(1e-4, min(gs[a] / max(1, res[a] - 1) for a in range(3))))
-    recs, _, _ = selectGiLightRecords(scene.lights, True, g["gridMin"], [g["gridMin"][a] + g["gridSize"][a] for a in range(3)])
-    arena = orc.light_arena(recs, True, g)
-    from speedball_b200 import _abi
-    p = _abi.default_params()
-    p.hysteresis = scene.meta["hysteresis"]
-    return orc, S, keep, g, orc.grid_struct(g), arena, recs.shape[0], p.to_array()
+class CpuAtrium:
+    """The reference's own CPU path for one atrium update, built and run by the
+    oracle alone (nothing here touches the CUDA library or its host code): the
+    pool from the MeshBVH restatement, the TLAS and instance records from
+    buildTlasRecords / computeDynamic, the uniforms at their defaults, the
+    light selection of selectGiLightRecords. A step is the reference's per-frame
+    work: updateDeforms (vertex gather + refitFlatBlasRange of the deforming
+    mesh), updateTransforms (the 3 movers' instance rows + the TLAS refit of the
+    frozen partition), then the FP32 solve of `probes` probes."""
+
+    def __init__(self, scene):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import orc
+        self.orc = orc
+        self.lib = orc.load()
+        self.scene = scene
+        pool = self.pool = orc.OrcPool(scene)
+        mats, order, live, aabb = orc.compute_tail(pool)
+        self.mats, self.order = mats, order
+        self.nodes = pool.bvhNodes
+        self.vertex = pool.vertexData
+        self.keep = [pool]
+        self.S = orc.scene_struct(pool, mats, nodes=self.nodes, vertex=self.vertex, keep=self.keep)
+        gm = scene.meta["grid"]
+        self.g = orc.grid_dict(gm["gridMin"], gm["gridSize"], gm["res"], gm["rays"])
+        gmax = [self.g["gridMin"][a] + self.g["gridSize"][a] for a in range(3)]
+        recs, _, _ = orc.select_light_records(scene.lights, True, self.g["gridMin"], gmax)
+        self.arena = orc.light_arena(recs, True, self.g)
+        self.nl = recs.shape[0]
+        self.prm = orc.default_params(scene.meta["hysteresis"])
+        self.G = orc.grid_struct(self.g)
+        self.irr, self.depth, self.atlas, self.datlas = orc.new_state(self.g, fp32=True)
+        self.probes = int(np.prod(self.g["res"]))
+        self.dm = scene.meta["deformer"]
+        self.movers = list(scene.meta["movers"])
+        n = pool.instCount
+        self.inv = np.zeros((n, 12), np.float32)
+        self.det = np.zeros(n, np.float32)
+        self.aabb = np.zeros((n, 9))
+        self.world = pool.inst_world.copy()
+        self.tl = np.ascontiguousarray(mats[pool.tlasBase:].copy())
+
+    def lanes(self, frame_motion):
+        """updateDeforms + updateTransforms of one frame on the host."""
+        orc, lib, pool = self.orc, self.lib, self.pool
+        mats_w, pos = frame_motion
+        vb, vc = int(pool.vert_base[self.dm]), int(pool.vert_count[self.dm])
+        self.vertex[vb:vb + vc, 0:3] = pos
+        ok = lib.orc_refit_blas(orc._p(self.nodes), self.nodes.size, orc._p(pool.triIndex), pool.triIndex.size,
+                                orc._p(self.vertex), self.vertex.size, int(pool.blas_root[self.dm]),
+                                int(pool.blas_end[self.dm]))
+        assert ok == 1
+        for i, m in mats_w.items():
+            self.world[i] = np.asarray(m, np.float64).T.reshape(16)
+        lb = np.ascontiguousarray(orc.local_bounds(self.nodes, pool.inst_root))
+        lib.orc_compute_instances(orc._p(self.world), orc._p(pool.inst_active), orc._p(lb), pool.instCount,
+                                  orc._p(self.inv), orc._p(self.det), orc._p(self.aabb))
+        ib = pool.instBase
+        for slot, src in enumerate(self.order):
+            self.mats[ib + slot * 28: ib + slot * 28 + 12] = self.inv[src]
+            self.mats[ib + slot * 28 + 14] = self.det[src]
+        live = np.ascontiguousarray(self.aabb[self.order, 0:6].astype(np.float32))
+        assert lib.orc_refit_tlas_range(orc._p(self.tl), self.tl.size, orc._p(live), live.size, 0, pool.tlasNodeCount)
+        self.mats[pool.tlasBase:] = self.tl
+
+    def solve(self, probes: int, offset: int = 0):
+        self.orc.solve(self.S, self.arena, self.nl, True, self.G, self.G, self.prm, offset, probes, self.irr,
+                       self.depth, self.atlas, self.datlas, fp32=True)
+
+    def step(self, frame_motion, probes: int, offset: int = 0) -> float:
+        t0 = time.perf_counter()
+        self.lanes(frame_motion)
+        self.solve(probes, offset)
+        return time.perf_counter() - t0
 
 
-def cpu_solve_rate(scene, probes: int, reps: int = 1):
-    orc, S, keep, g, G, arena, nl, prm = _cpu_setup(scene)
-    irr, depth, atlas, datlas = orc.new_state(g, fp32=True)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        orc.solve(S, arena, nl, True, G, G, prm, 0, probes, irr, depth, atlas, datlas, fp32=True)
-    dt = time.perf_counter() - t0
-    return probes * g["rays"] * reps / dt / 1e6, dt
+def atrium_config(probes: int, rays: int, tris: int, world: int) -> dict:
+    """The workload description both arms print (the same keys and values)."""
+    return {"workload": "atrium 262,267 tris / 30 meshes, 16^3 probes x 64 rays, 32 clustered point + 1 "
+                        "directional light, 1 deforming + 3 moving meshes per frame",
+            "probes": probes, "rays_per_probe": rays, "primary_rays_per_step": probes * rays, "triangles": tris,
+            "l2": "flushed (256 MiB write) before every timed step (GPU arm)",
+            "parallelism": "replicas" if world > 1 else "single GPU"}
 
 
 def cpu_baseline(scene, target_s=12.0):
-    """The FP32 CPU restatement on every host thread: whole-atrium solves
-    (all 4,096 probes) repeated for about `target_s` seconds."""
+    """The FP32 CPU restatement on every host thread: whole-atrium updates (the
+    motion lanes + all 4,096 probes) repeated for about `target_s` seconds."""
+    from speedball_b200 import synth
     threads = os.cpu_count() or 1
-    rate, dt = cpu_solve_rate(scene, 4096)
+    cpu = CpuAtrium(scene)
+    dt = cpu.step(synth.atrium_motion(scene, 0), cpu.probes)
     reps = max(1, int(round(target_s / max(dt, 1e-3))))
-    rate, dt = cpu_solve_rate(scene, 4096, reps)
+    frames = [synth.atrium_motion(scene, 1 + i) for i in range(reps)]
+    total = sum(cpu.step(fr, cpu.probes) for fr in frames)
+    rate = cpu.probes * cpu.g["rays"] * reps / total / 1e6
     return {"value": round(rate, 4), "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{reps} full atrium solves (4,096 probes x 64 rays each) on {threads} threads, "
-                      f"FP32 CPU restatement, {dt:.1f} s"}
+            "sample": f"{reps} full atrium updates (deformer refit + 3 movers + TLAS refit + 4,096 probes x 64 rays) "
+                      f"on {threads} threads, FP32 CPU restatement built by the oracle alone, {total:.1f} s"}
 
 
 def run_reference(args, dist: Dist):
     if dist.rank != 0:
         return None
+    from speedball_b200 import synth
     scene = make_workload()
     threads = os.cpu_count() or 1
-    rate, dt = cpu_solve_rate(scene, 4096)
-    # each step: a whole-atrium solve, or a probe sample sized so K+W steps fit ~2 minutes
+    cpu = CpuAtrium(scene)
+    W, K = args.warmup, args.steps
+    frames = [synth.atrium_motion(scene, fr) for fr in range(W + K + 1)]
+    dt = cpu.step(frames[-1], cpu.probes)
+    # each step a whole-atrium update, or a probe sample sized so the K + W steps fit about 2 minutes
     budget_s = 120.0
-    per_step = budget_s / max(1, args.steps + args.warmup)
-    probes = int(min(4096, max(64, 4096 * per_step / max(dt, 1e-3))))
-    orc, S, keep, g, G, arena, nl, prm = _cpu_setup(scene)
-    irr, depth, atlas, datlas = orc.new_state(g, fp32=True)
-
-    def step():
-        t0 = time.perf_counter()
-        orc.solve(S, arena, nl, True, G, G, prm, 0, probes, irr, depth, atlas, datlas, fp32=True)
-        return time.perf_counter() - t0
-
-    for _ in range(args.warmup):
-        step()
-    total, rays = 0.0, 0
-    for _ in range(args.steps):
-        total += step()
-        rays += probes * 64
-    value = rays / total / 1e6
+    per_step = budget_s / max(1, K + W)
+    probes = int(min(cpu.probes, max(64, cpu.probes * per_step / max(dt, 1e-3))))
+    for i in range(W):
+        cpu.step(frames[i], probes)
+    total = 0.0
+    offset = 0
+    for i in range(K):
+        total += cpu.step(frames[W + i], probes, offset)
+        offset = (offset + probes) % cpu.probes
+    value = K * probes * cpu.g["rays"] / total / 1e6
+    rays = cpu.probes * cpu.g["rays"]
+    sample = (f"{probes} of {cpu.probes} probes x 64 rays per step, with the step's deformer refit, 3 movers and "
+              f"TLAS refit; FP32 CPU restatement of the reference path built by the oracle alone, {threads} threads "
+              "(the reference itself is WebGPU/JS: no runtime here)")
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": dist.world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(4096 * 64 / (value * 1e6) * 1e3, 3),
+            "steps": K, "warmup": W, "ms_per_step": round(rays / (value * 1e6) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded procedural atrium)",
-            "config": {"workload": "atrium 262,267 tris, 16^3 probes x 64 rays (per-step sample of "
-                                   f"{probes} probes)"},
+            "data": "synthetic (seeded procedural atrium standing in for Sponza)",
+            "config": atrium_config(cpu.probes, cpu.g["rays"], int(cpu.pool.triIndex.shape[0]), dist.world),
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{probes} probes x 64 rays per step, FP32 CPU restatement of the reference "
-                                       f"path on {threads} threads (the reference itself is WebGPU/JS: no runtime here)"},
+                             "sample": sample},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 

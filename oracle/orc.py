@@ -81,6 +81,8 @@ def load() -> C.CDLL:
             "orc_refit_tlas_dirty": (C.c_int32, [P, C.c_uint64, P, C.c_uint64, C.c_int64, P, C.c_uint64, P, P]),
             "orc_build_tlas": (U, [P, U, P, P, P]),
             "orc_compute_instances": (None, [P, P, P, U, P, P, P]),
+            "orc_probe_rays": (None, [P, C.c_double, U, U, P, P]),
+            "orc_explain_hits": (None, [P, P, P, U, P, P, P, P, P, P, P, C.c_int32]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
@@ -248,3 +250,234 @@ def adjoint(scene: OrcScene, arena: np.ndarray, light_count: int, clustered: boo
                          C.byref(loss), _p(E), _p(g), nthreads or threads())
     assert rc == 0
     return loss.value, E, g
+
+
+# ------------------------------------------------- hit-ID disagreement proof
+HIT_CODES = {0: "same", 1: "near-tie", 2: "gpu edge graze", 3: "oracle edge graze", 4: "t order within FP32 error",
+             5: "unexplained"}
+
+
+def probe_rays(grid: OrcGrid, jitter: float, probe_offset: int, updated: int):
+    """FP64 world-space probe rays of a solve (origin, direction per ray)."""
+    n = updated * grid.rays
+    ro = np.zeros((n, 3), np.float64)
+    rd = np.zeros((n, 3), np.float64)
+    load().orc_probe_rays(C.byref(grid), float(jitter), probe_offset, updated, _p(ro), _p(rd))
+    return ro, rd
+
+
+def explain_hits(scene: OrcScene, ro: np.ndarray, rd: np.ndarray, g_tri, g_inst, o_tri, o_inst, o_t):
+    """Per ray, why the GPU's closest hit (g_tri, g_inst) differs from the FP64
+    oracle's (o_tri, o_inst, o_t): a code of HIT_CODES, plus the FP64 t of the
+    GPU's pair (-1 when it has none)."""
+    n = ro.shape[0]
+    ro = np.ascontiguousarray(ro, np.float64)
+    rd = np.ascontiguousarray(rd, np.float64)
+    arrs = [np.ascontiguousarray(a, np.int32) for a in (g_tri, g_inst, o_tri, o_inst)]
+    ot = np.ascontiguousarray(o_t, np.float64)
+    code = np.zeros(n, np.int32)
+    gt = np.zeros(n, np.float64)
+    load().orc_explain_hits(C.byref(scene), _p(ro), _p(rd), n, *[_p(a) for a in arrs], _p(ot), _p(code), _p(gt),
+                            threads())
+    return code, gt
+
+
+# ----------------------------------------------------- per-tick scheduling
+class Schedule:
+    """The reference's per-tick solve schedule for one cascade: probes per tick
+    (updatedCap / tickCap, gi_probes.js:2947-2962), the round-robin cursor and
+    the per-cascade service-interval EMA and hysteresis exponent (3737-3766,
+    3788, 3838-3839; probeUpdateIntervalTicks 197-202,
+    hysteresisExponentForInterval 235-251), and the montecarlo jitter epoch
+    (3776-3787). One C0 cascade, the fallback service interval of one tick."""
+
+    DT_REF_MS = 1000.0 / 60.0
+
+    def __init__(self, probe_total: int, rays: int, ray_budget: int, max_probes: int, montecarlo: bool,
+                 normalize: bool):
+        self.total = probe_total
+        self.rays = rays
+        self.cap = max(1, min(max_probes, ray_budget // max(1, rays)))
+        self.montecarlo = montecarlo
+        self.normalize = normalize
+        self.cursor = 0
+        self.last = 0.0
+        self.ema = 0.0
+        self.frame = 0
+        self.jitter = 0.0
+
+    def tick(self, now_ms: float) -> dict:
+        updated = min(self.cap, self.total)
+        ema = self.ema
+        if self.last > 0:
+            dt = now_ms - self.last
+            ema = (ema * 0.8 + dt * 0.2 if ema > 0 else dt) if 0 < dt < 200 else 0.0
+        service = ema if ema > 0 else self.DT_REF_MS
+        revisit = max(1.0, self.total / max(1, updated))
+        exponent = load().orc_hysteresis_exponent(service * revisit, 1 if self.normalize else 0)
+        if self.montecarlo:
+            self.frame = (self.frame + 1) & 0xFFFFFFFF
+            self.jitter = (self.frame * 0.61803398875) % 1
+        out = dict(probeOffset=self.cursor, updatedCount=updated, hysteresisExponent=exponent, frameJitter=self.jitter)
+        self.cursor = (self.cursor + updated) % self.total if self.total else 0
+        self.last = now_ms
+        self.ema = ema
+        return out
+
+
+# --------------------------------------------- scene pool on the oracle side
+# The reference arm of the benchmark and the pool cross-check build their
+# scene with these restatements only, never with the CUDA library's host code.
+
+ORC_PARAM_NAMES = [
+    "frameJitter", "emitterVisSeed", "hysteresis", "hysteresisExponent",
+    "depthSharpness", "radianceClamp", "classifyStrength", "filterStrength", "filterSmooth",
+    "tempChangeSigma1", "tempChangeHDrop", "tempClampSigma", "nirGate", "nirGain", "skyIntensity",
+] + [f"skySH{i}" for i in range(27)] + [
+    "debugTraceBiasScale", "debugRayEpsScale", "debugDirectScale", "debugEmissiveScale",
+    "debugAlbedoScale", "debugBounceScale", "debugCosinePower",
+    "debugTempNoiseHBoost", "debugTempChangeSigma0", "debugTempMinChangeH",
+    "debugTempVarEps", "debugTempVarRel", "debugDepthHistoryScale",
+    "debugFilterKScale", "debugFilterRelScale", "debugFilterEpsScale",
+]
+
+
+def default_params(hysteresis: float = 0.60) -> np.ndarray:
+    """The shared uniforms `U` at their initial values (gi_probes.js:1198-1255;
+    temporal constants 182-189; JITTER_HYSTERESIS_DEFAULTS.gated = 0.60), in the
+    order of the oracle's Params, each rounded to float32 as a uniform stores it."""
+    v = dict.fromkeys(ORC_PARAM_NAMES, 0.0)
+    v.update(hysteresis=hysteresis, hysteresisExponent=1.0, depthSharpness=7.0, radianceClamp=8.0,
+             filterStrength=1.0, filterSmooth=0.5, tempChangeSigma1=2.5, tempChangeHDrop=0.30, tempClampSigma=6.0,
+             nirGain=1.0, skyIntensity=1.0, debugTraceBiasScale=1.0, debugRayEpsScale=1.0, debugDirectScale=1.0,
+             debugEmissiveScale=1.0, debugAlbedoScale=1.0, debugBounceScale=1.0, debugCosinePower=1.0,
+             debugTempNoiseHBoost=0.25, debugTempChangeSigma0=0.75, debugTempMinChangeH=0.55,
+             debugTempVarEps=0.000025, debugTempVarRel=0.0025, debugDepthHistoryScale=1.0, debugFilterKScale=1.0,
+             debugFilterRelScale=1.0, debugFilterEpsScale=1.0)
+    out = np.array([np.float32(v[n]) for n in ORC_PARAM_NAMES], np.float64)
+    assert out.shape[0] == load().orc_params_size()
+    return out
+
+
+def select_light_records(records: np.ndarray, importance_ranked: bool, grid_min, grid_max):
+    """selectGiLightRecords / selectGiLights / giLightImportance
+    (gi_probes.js:4253-4289): analytic records (type < 2.5) first, importance
+    top-K by (score desc, index asc) when clustered, then up to 16 emitters.
+    Returns (records, analytic count, emitter count)."""
+    recs = [np.asarray(r, np.float32) for r in np.asarray(records, np.float32).reshape(-1, 17)]
+    analytic = [r for r in recs if abs(float(r[0]) - 3) >= 0.5 and float(r[0]) < 2.5]
+    emitters = [r for r in recs if abs(float(r[0]) - 3) < 0.5]
+    n_emit = min(16, len(emitters))
+    budget = 64 - n_emit
+
+    def score(r):
+        if r[0] < 0.5:
+            return float("inf")
+        power = max(float(r[7]), float(r[8]), float(r[9]))
+        cone = max(0.02, (1 - float(r[12])) * 0.5) if abs(float(r[0]) - 2) < 0.5 else 1.0
+        d = [max(grid_min[a] - float(r[1 + a]), 0.0, float(r[1 + a]) - grid_max[a]) for a in range(3)]
+        return (power * cone) / (1 + d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+
+    if importance_ranked and len(analytic) > budget:
+        keep = sorted(range(len(analytic)), key=lambda i: (-score(analytic[i]), i))[:budget]
+        analytic = [analytic[i] for i in keep]
+    else:
+        analytic = analytic[:budget]
+    out = analytic + emitters[:n_emit]
+    arr = np.stack(out) if out else np.zeros((0, 17), np.float32)
+    return arr, len(analytic), n_emit
+
+
+def build_blas(positions: np.ndarray, indices: np.ndarray, leaf: int = 8):
+    """MeshBVH + flattenBVHRoot of one mesh (orc_bvh.hpp): (nodes (N,8) u32,
+    triangle order, index triples in BVH order)."""
+    lib = load()
+    if not hasattr(lib, "_bvh"):
+        P = C.c_void_p
+        lib.orc_build_blas.restype = C.c_uint32
+        lib.orc_build_blas.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_uint32, P, C.c_uint64, P]
+        lib._bvh = True
+    pos = np.ascontiguousarray(positions, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32).copy()
+    T = idx.shape[0]
+    nodes = np.zeros((2 * T + 1, 8), np.uint32)
+    order = np.zeros(T, np.uint32)
+    n = lib.orc_build_blas(_p(pos), pos.shape[0], _p(idx), T, leaf, _p(nodes), nodes.shape[0], _p(order))
+    if n == 0:
+        raise ValueError("BLAS build failed (empty mesh, out-of-range index or oversized leaf)")
+    return nodes[:n].copy(), order, idx
+
+
+def tlas_node_count(n: int) -> int:
+    """Records of buildTlasRecords' median split with leaves of <= 2 instances
+    (spectral_scene.js:973-1003)."""
+    t = [1] * (n + 1)
+    for m in range(3, n + 1):
+        t[m] = 1 + t[m >> 1] + t[m - (m >> 1)]
+    return t[n] if n else 0
+
+
+class OrcPool:
+    """The typed arrays of buildSpectralScene for a plain mesh scene: pooled
+    BLASes with pool-absolute miss links and leaf offsets (spectral_scene.js:
+    1188-1240), the material records followed by room for the instance records
+    and the TLAS (1327-1334), and the instance table (column-major FP64 world
+    matrices, three's Matrix4.elements)."""
+
+    def __init__(self, scene, leaf: int = 8):
+        blas = [build_blas(m.positions, m.indices, leaf) for m in scene.meshes]
+        nV = sum(m.positions.shape[0] for m in scene.meshes)
+        nT = sum(m.indices.shape[0] for m in scene.meshes)
+        nN = sum(b[0].shape[0] for b in blas)
+        if nT >= 1 << 24 or nN >= 1 << 24:
+            raise ValueError("BVH pool exceeds the 24-bit index ceiling")
+        self.vertexData = np.zeros((nV, 8), np.float32)
+        self.triIndex = np.zeros((nT, 3), np.uint32)
+        self.triMaterial = np.zeros(nT, np.uint32)
+        self.bvhNodes = np.zeros((nN, 8), np.uint32)
+        M = len(scene.meshes)
+        self.blas_root = np.zeros(M, np.uint32); self.blas_end = np.zeros(M, np.uint32)
+        self.vert_base = np.zeros(M, np.uint32); self.vert_count = np.zeros(M, np.uint32)
+        v0 = t0 = n0 = 0
+        for i, (mesh, (nodes, order, idx)) in enumerate(zip(scene.meshes, blas)):
+            V, T, N = mesh.positions.shape[0], idx.shape[0], nodes.shape[0]
+            self.vertexData[v0:v0 + V, 0:3] = mesh.positions
+            if mesh.normals is not None:
+                self.vertexData[v0:v0 + V, 3:6] = mesh.normals
+            if mesh.uvs is not None:
+                self.vertexData[v0:v0 + V, 6:8] = mesh.uvs
+            self.triIndex[t0:t0 + T] = idx + v0
+            self.triMaterial[t0:t0 + T] = np.asarray(mesh.tri_material, np.uint32)[order]
+            b = nodes.copy()
+            b[:, 6] += n0
+            lf = b[:, 7] != 0xFFFFFFFF
+            b[lf, 7] = (b[lf, 7] & 0xFF000000) | (((b[lf, 7] & 0x00FFFFFF) + t0) & 0x00FFFFFF)
+            self.bvhNodes[n0:n0 + N] = b
+            self.blas_root[i], self.blas_end[i] = n0, n0 + N
+            self.vert_base[i], self.vert_count[i] = v0, V
+            v0 += V; t0 += T; n0 += N
+        ubers = np.asarray(scene.materials, np.float32).reshape(-1, 28)
+        I = len(scene.instances)
+        self.instCount = I
+        self.tlasNodeCount = tlas_node_count(I)
+        self.instBase = ubers.shape[0] * 28
+        self.tlasBase = self.instBase + I * 28
+        self.materials = np.zeros(self.tlasBase + self.tlasNodeCount * 12, np.float32)
+        self.materials[:self.instBase] = ubers.reshape(-1)
+        self.inst_world = np.zeros((I, 16), np.float64)
+        self.inst_active = np.zeros(I, np.uint8)
+        self.inst_root = np.zeros(I, np.uint32); self.inst_end = np.zeros(I, np.uint32)
+        for k, inst in enumerate(scene.instances):
+            self.inst_world[k] = np.asarray(inst.world, np.float64).T.reshape(16)
+            self.inst_active[k] = 1 if inst.active else 0
+            self.inst_root[k] = self.blas_root[inst.mesh]
+            self.inst_end[k] = self.blas_end[inst.mesh]
+
+
+def grid_dict(grid_min, grid_size, res, rays) -> dict:
+    """A cascade's grid uniforms (makeCascadeU, gi_probes.js:1010-1024): maxDist =
+    |gridSize|, cellMin = the smallest probe spacing (floor 1e-4)."""
+    gs = np.asarray(grid_size, np.float64)
+    return dict(gridMin=list(grid_min), gridSize=list(grid_size), res=list(res), rays=rays,
+                maxDist=float(np.linalg.norm(gs)),
+                cellMin=float(max(1e-4, min(gs[a] / max(1, res[a] - 1) for a in range(3)))))

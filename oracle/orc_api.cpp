@@ -2,6 +2,7 @@
 // bench.py's CPU baseline. TEST INFRASTRUCTURE ONLY (see orc_core.hpp).
 #include "orc_probes.hpp"
 #include "orc_scene.hpp"
+#include "orc_bvh.hpp"
 
 #include <atomic>
 #include <thread>
@@ -94,6 +95,124 @@ void orc_any(const OrcScene* s, const float* ro, const float* rd, const float* m
         Traverser<double> tr(sc);
         V3<double> o(ro[i * 3], ro[i * 3 + 1], ro[i * 3 + 2]), d(rd[i * 3], rd[i * 3 + 1], rd[i * 3 + 2]);
         blocked[i] = tr.any(o, d, (double)maxDist[i]) ? 1 : 0;
+    });
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ hit-ID disagreement proof
+// One (triangle, instance slot) pair evaluated on a world ray in FP64 with the
+// reference's Möller–Trumbore (spectral_traverse.js:393-409) and its closest-hit
+// acceptance (side, alpha/const-alpha flags, 193-220), plus a first-order bound
+// on how far an FP32 evaluation of the same test can move u, v and t. The bound
+// sums the magnitudes of the terms each FP32 operation rounds: the world-to-local
+// transform (inverse rows · origin + translation), the edge vectors, the two
+// cross products and the three dot products, each term rounded at most a few
+// times with unit roundoff 2^-24; a factor 16 covers the operation count.
+struct PairEval {
+    bool valid = false;    // tri >= 0 and the slot is live
+    bool accepted = false; // MT passes and the pair is accepted as a closest hit
+    bool rejectedByBary = false;  // only u/v (edge) conditions reject it
+    double t = 0, u = 0, v = 0, margin = 0;  // margin = min(u, v, 1-u-v)
+    double tauBary = 0, tauT = 0;
+};
+
+static PairEval eval_pair(const Traverser<double>& tr, const Scene& s, int tri, int inst, V3<double> wro, V3<double> wrd) {
+    PairEval e;
+    if (tri < 0 || inst < 0 || (uint32_t)tri >= s.triCount || (uint32_t)inst >= s.instCount) return e;
+    e.valid = true;
+    V3<double> ro = tr.inst_inv_point((uint32_t)inst, wro), rd = tr.inst_inv_dir((uint32_t)inst, wrd);
+    double dSign = tr.inst_f((uint32_t)inst, 14);
+    double Mn = 0, Wn = 0;
+    for (int r = 0; r < 3; ++r) {
+        Mn += length(tr.inst_row((uint32_t)inst, r));
+        Wn += std::fabs(tr.inst_f((uint32_t)inst, r * 4 + 3));
+    }
+    V3<double> p0 = tr.fetch_vert(tr.tri_vert(tri, 0)), p1 = tr.fetch_vert(tr.tri_vert(tri, 1)),
+               p2 = tr.fetch_vert(tr.tri_vert(tri, 2));
+    V3<double> e1 = p1 - p0, e2 = p2 - p0, pv = cross(rd, e2), tv = ro - p0, qv = cross(tv, e1);
+    double det = dot(e1, pv);
+    if (!(std::fabs(det) > 1e-12)) return e;
+    double inv = 1.0 / det;
+    e.u = dot(tv, pv) * inv;
+    e.v = dot(rd, qv) * inv;
+    e.t = dot(e2, qv) * inv;
+    e.margin = std::min(std::min(e.u, e.v), 1.0 - e.u - e.v);
+    const double eps = 16.0 * std::ldexp(1.0, -24);
+    // magnitudes entering the FP32 evaluation
+    double S = Mn * length(wro) + Wn + length(ro) + length(p0) + length(p1) + length(p2);  // origin side
+    double D = Mn * length(wrd) + length(rd);                                                // direction side
+    double E1 = length(e1) + length(p0) + length(p1), E2 = length(e2) + length(p0) + length(p2);
+    double dDet = eps * (E1 * D * E2);
+    double dNu = eps * (S * length(pv) + length(tv) * D * E2);
+    double dNv = eps * (D * S * E1 + length(qv) * D);
+    double dNt = eps * (E2 * length(qv) + E2 * S * E1);
+    double ad = std::fabs(det);
+    double du = (dNu + std::fabs(e.u) * dDet) / ad, dv = (dNv + std::fabs(e.v) * dDet) / ad;
+    e.tauBary = du + dv;
+    e.tauT = (dNt + std::fabs(e.t) * dDet) / ad;
+    bool baryOk = e.u >= 0.0 && e.u <= 1.0 && e.v >= 0.0 && e.u + e.v <= 1.0;
+    uint32_t m = s.triMaterial[tri];
+    uint32_t fl = tr.flags(m);
+    bool acc = tr.side_accepts(m, det * dSign) && ((fl & 1u) ? tr.alpha_accepts(m) : (fl & 2u) != 0);
+    bool active = tr.inst_f((uint32_t)inst, 15) > 0.5;
+    bool tOk = e.t > RAY_EPS;
+    e.accepted = active && acc && tOk && baryOk;
+    e.rejectedByBary = active && acc && tOk && !baryOk;
+    return e;
+}
+
+extern "C" {
+
+// World-space probe rays of a solve in FP64: ray i = (slot i / rays, k i % rays),
+// probe (probeOffset + slot) mod probeTotal (gi_probes.js:1977-1987).
+void orc_probe_rays(const OrcGrid* gp, double jitter, uint32_t probeOffset, uint32_t updated, double* roOut,
+                    double* rdOut) {
+    Grid g = to_grid(gp);
+    const uint32_t N = g.rays, total = g.probeTotal();
+    for (size_t i = 0; i < (size_t)updated * N; ++i) {
+        uint32_t slot = (uint32_t)(i / N), k = (uint32_t)(i % N);
+        V3<double> o = probe_world_pos<double>(g, (probeOffset + slot) % total);
+        V3<double> d = ray_dir<double>(k, N, jitter);
+        roOut[i * 3] = o.x; roOut[i * 3 + 1] = o.y; roOut[i * 3 + 2] = o.z;
+        rdOut[i * 3] = d.x; rdOut[i * 3 + 1] = d.y; rdOut[i * 3 + 2] = d.z;
+    }
+}
+
+// Classifies every ray whose GPU closest hit (gTri, gInst) differs from the FP64
+// oracle's (oTri, oInst, oT). Codes:
+//   0 same pair;
+//   1 near-tie: both pairs accepted in FP64, their t within 1e-6 relative;
+//   2 the GPU's pair is an edge graze: FP64 rejects it only by its barycentric
+//     bounds, by less than the FP32 bound, and it lies no farther than the
+//     oracle's hit (or the oracle missed);
+//   3 the oracle's pair is an edge graze: accepted in FP64 within the FP32 bound
+//     of an edge, and the GPU's hit (if any) is an accepted pair no nearer;
+//   4 t-order within FP32 error: both accepted, |t_g - t_o| within the FP32 t
+//     bounds of the two pairs;
+//   5 unexplained.
+// gTOut receives the FP64 t of the GPU's pair (or -1).
+void orc_explain_hits(const OrcScene* s, const double* ro, const double* rd, uint32_t n, const int32_t* gTri,
+                      const int32_t* gInst, const int32_t* oTri, const int32_t* oInst, const double* oT,
+                      int32_t* codeOut, double* gTOut, int32_t threads) {
+    Scene sc = to_scene(s);
+    parallel_for(n, threads, [&](size_t i, int) {
+        gTOut[i] = -1.0;
+        if (gTri[i] == oTri[i] && (gTri[i] < 0 || gInst[i] == oInst[i])) { codeOut[i] = 0; return; }
+        Traverser<double> tr(sc);
+        V3<double> o(ro[i * 3], ro[i * 3 + 1], ro[i * 3 + 2]), d(rd[i * 3], rd[i * 3 + 1], rd[i * 3 + 2]);
+        PairEval g = eval_pair(tr, sc, gTri[i], gInst[i], o, d);
+        PairEval r = eval_pair(tr, sc, oTri[i], oInst[i], o, d);
+        if (g.valid) gTOut[i] = g.t;
+        const double tO = oTri[i] >= 0 ? oT[i] : INFINITY;
+        int code = 5;
+        if (g.accepted && r.accepted && std::fabs(g.t - r.t) <= 1e-6 * std::fabs(r.t)) code = 1;
+        else if (g.valid && g.rejectedByBary && g.margin >= -g.tauBary && g.t <= tO * (1 + 1e-6)) code = 2;
+        else if (r.valid && r.accepted && r.margin <= r.tauBary && (!g.valid || (g.accepted && g.t >= tO * (1 - 1e-6)) ||
+                 (g.rejectedByBary && g.margin >= -g.tauBary)))
+            code = 3;
+        else if (g.accepted && r.accepted && std::fabs(g.t - r.t) <= g.tauT + r.tauT) code = 4;
+        codeOut[i] = code;
     });
 }
 
@@ -223,6 +342,17 @@ int32_t orc_refit_tlas_dirty(float* nodes, uint64_t nodesLen, const float* ib, u
     for (size_t i = 0; i < t.size(); ++i) touchedOut[i] = t[i];
     *touchedCount = (uint32_t)t.size();
     return 1;
+}
+// MeshBVH build + flattenBVHRoot of one mesh (orc_bvh.hpp). index3 is permuted
+// in place into BVH order; orderOut[i] = source triangle at position i.
+uint32_t orc_build_blas(const float* pos3, uint32_t vertCount, uint32_t* index3, uint32_t triCount, uint32_t leafSize,
+                        uint32_t* nodesOut, uint64_t nodesCap, uint32_t* orderOut) {
+    std::vector<uint32_t> nodes, order;
+    uint32_t n = build_mesh_bvh(pos3, vertCount, index3, triCount, leafSize, nodes, order);
+    if (!n || n > nodesCap) return 0;
+    std::memcpy(nodesOut, nodes.data(), (size_t)n * 32);
+    std::memcpy(orderOut, order.data(), (size_t)triCount * 4);
+    return n;
 }
 // aabbs9: per instance min xyz, max xyz, centroid xyz (FP64)
 uint32_t orc_build_tlas(const double* aabbs9, uint32_t n, float* nodes12Out, uint32_t* orderOut, double* bounds64Out) {
