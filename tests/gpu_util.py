@@ -70,7 +70,8 @@ class OracleMirror:
     def params(self) -> np.ndarray:
         return self.field._params.to_array()
 
-    def solve(self, offset: int, updated: int, replay: dict | None = None, want: bool = True):
+    def solve(self, offset: int, updated: int, replay: dict | None = None, want: bool = True,
+              params: np.ndarray | None = None):
         n = updated * self.gdict["rays"]
         io = orc.OrcSolveIO()
         out = {}
@@ -83,7 +84,8 @@ class OracleMirror:
         if replay is not None:
             io.replayTri = orc._p(replay["tri"]); io.replayInst = orc._p(replay["inst_word"])
             io.replayBlocked = orc._p(replay["blocked"])
-        orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid, self.params(),
+        orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid,
+                  self.params() if params is None else params,
                   offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io)
         return out
 
@@ -113,3 +115,111 @@ def texel_rel_err(g: np.ndarray, o: np.ndarray) -> np.ndarray:
     of the largest magnitude for near-black texels."""
     floor = max(1e-3 * float(np.abs(o).max()), 1e-12)
     return np.abs(g - o) / np.maximum(np.abs(o), floor)
+
+
+def check_hits(scene: orc.OrcScene, ro: np.ndarray, rd: np.ndarray, g_tri, g_inst, g_t, o_tri, o_inst, o_t) -> dict:
+    """Hit-ID parity at the near-tie bar: every ray whose GPU closest hit
+    differs from the FP64 oracle's must be explained, ray by ray, by the oracle
+    (orc.explain_hits: a near-tie within 1e-6 relative, an edge graze within
+    the FP32 rounding bound of that triangle's barycentric test, or a t order
+    within the FP32 bound of the two t); no share of rays is waived. Hit t of
+    the GPU is within 1e-5 relative of the FP64 t of the pair it reports.
+    Returns the count of rays per code."""
+    code, gt = orc.explain_hits(scene, ro, rd, g_tri, g_inst, o_tri, o_inst, o_t)
+    counts = {orc.HIT_CODES[k]: int(v) for k, v in enumerate(np.bincount(code, minlength=6))}
+    bad = np.flatnonzero(code == 5)
+    assert bad.size == 0, (counts, [(int(i), int(g_tri[i]), int(o_tri[i]), float(g_t[i]), float(o_t[i]), float(gt[i]))
+                                    for i in bad[:6]])
+    g_hit = np.asarray(g_tri) >= 0
+    same = (code == 0) & g_hit
+    o_t = np.asarray(o_t, np.float64)
+    g_t = np.asarray(g_t, np.float64)
+    rel_max = 0.0
+    if same.any():
+        rel = np.abs(g_t[same] - o_t[same]) / o_t[same]
+        rel_max = float(rel.max())
+        assert rel_max <= T_REL, rel_max
+    other = (code != 0) & g_hit & (gt > 0)
+    if other.any():
+        rel2 = np.abs(g_t[other] - gt[other]) / gt[other]
+        assert rel2.max() <= T_REL, rel2.max()
+    counts["t_rel_max"] = rel_max
+    return counts
+
+
+class SceneTail:
+    """The oracle's own per-frame scene state for motion: the deforming mesh's
+    vertices and BLAS refit (updateDeforms, spectral_scene.js:1831-1927 with
+    refitFlatBlasRange), the moved instances' rows and the TLAS refit of the
+    partition frozen at the build (updateTransforms, 1402-1514). It writes into
+    an OracleMirror's arrays in place and checks them bit for bit against the
+    GPU's copies."""
+
+    def __init__(self, mirror: OracleMirror):
+        self.m = mirror
+        pool = mirror.pool
+        mats0, order0, live0, aabb0 = orc.compute_tail(pool, nodes=mirror.nodes)
+        self.order = order0
+        self.tl = np.ascontiguousarray(mats0[pool.tlasBase:].copy())
+        self.world = pool.inst_world.copy()
+        n = pool.instCount
+        self.inv = np.zeros((n, 12), np.float32)
+        self.det = np.zeros(n, np.float32)
+        self.aabb = np.zeros((n, 9))
+
+    def apply(self, deformed: dict, moved: dict):
+        """deformed: mesh -> (V,3) float32 positions; moved: instance -> 4x4 world."""
+        lib = orc.load()
+        m, pool = self.m, self.m.pool
+        for mesh, pos in deformed.items():
+            vb, vc = int(pool.vert_base[mesh]), int(pool.vert_count[mesh])
+            m.vertex[vb:vb + vc, 0:3] = pos
+            assert lib.orc_refit_blas(orc._p(m.nodes), m.nodes.size, orc._p(pool.triIndex), pool.triIndex.size,
+                                      orc._p(m.vertex), m.vertex.size, int(pool.blas_root[mesh]),
+                                      int(pool.blas_end[mesh])) == 1
+        for i, w in moved.items():
+            self.world[i] = np.asarray(w, np.float64).T.reshape(16)
+        lb = np.ascontiguousarray(orc.local_bounds(m.nodes, pool.inst_root))
+        lib.orc_compute_instances(orc._p(self.world), orc._p(pool.inst_active), orc._p(lb), pool.instCount,
+                                  orc._p(self.inv), orc._p(self.det), orc._p(self.aabb))
+        ib = pool.instBase
+        for slot, src in enumerate(self.order):
+            m.materials[ib + slot * 28: ib + slot * 28 + 12] = self.inv[src]
+            m.materials[ib + slot * 28 + 14] = self.det[src]
+        live = np.ascontiguousarray(self.aabb[self.order, 0:6].astype(np.float32))
+        assert lib.orc_refit_tlas_range(orc._p(self.tl), self.tl.size, orc._p(live), live.size, 0,
+                                        pool.tlasNodeCount)
+        m.materials[pool.tlasBase:] = self.tl
+
+    def check_gpu(self):
+        f, m = self.m.field, self.m
+        for key, arr in (("BVH_NODES", m.nodes), ("VERTEX_DATA", m.vertex), ("MATERIALS", m.materials)):
+            got = read(f, key, arr.size, arr.dtype).reshape(arr.shape)
+            assert np.array_equal(got.view(np.uint32), arr.view(np.uint32)), key
+
+
+def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params: np.ndarray) -> dict:
+    """After the GPU tick `frame`: independent FP64 solve (hit IDs and t of every
+    ray of the solve), then the oracle's replay of the GPU's hit and shadow
+    decisions advances its state; irradiance and depth atlases within 1e-3."""
+    off, upd = frame["probeOffset"], frame["updatedCount"]
+    n = upd * f.getRays()
+    rec = gpu_records(f, n)
+    saved = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy())
+    ind = mirror.solve(off, upd, replay=None, params=sched_params)
+    mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = saved
+    ro, rd = orc.probe_rays(mirror.grid, sched_params[0], off, upd)
+    counts = check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], ind["tri"], ind["inst"],
+                        ind["rays"][3::4])
+    mirror.solve(off, upd, replay=rec, params=sched_params)
+    ga = half_to_f(read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16))
+    oa = half_to_f(mirror.atlas.reshape(-1))
+    err = texel_rel_err(ga, oa)
+    gd = half_to_f(read(f, "DEPTH_ATLAS", mirror.depth_atlas.size, np.uint16))
+    od = half_to_f(mirror.depth_atlas.reshape(-1))
+    derr = texel_rel_err(gd, od)
+    assert err.max() <= TEXEL_REL, (err.max(), int((err > TEXEL_REL).sum()))
+    assert derr.max() <= TEXEL_REL, (derr.max(), int((derr > TEXEL_REL).sum()))
+    counts.update(irr_err=float(err.max()), depth_err=float(derr.max()), lit=float(np.abs(oa).max()),
+                  hit_share=float((rec["tri"] >= 0).mean()))
+    return counts

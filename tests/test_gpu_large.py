@@ -3,7 +3,8 @@
 256 rays) against the FP64 oracle, for every scene-BVH layout:
 
   - hit triangle / instance of sampled probe rays (sb_raycast) identical to the
-    oracle's FP64 closest hit except near-ties, t within 1e-5 relative;
+    oracle's FP64 closest hit except where the oracle explains the difference
+    ray by ray (near-tie or FP32 graze), t within 1e-5 relative;
   - a block of 64 probes of each cascade, replayed by the oracle from the GPU's
     hit records and shadow bits and its previous state, within 1e-3 relative
     on every irradiance and depth texel of their tiles.
@@ -103,16 +104,10 @@ def test_large_hits_match_oracle(large, kind):
     orc.load().orc_closest(C.byref(mirror.scene), orc._p(ro), orc._p(rd), n, 1, 0, orc._p(ot), orc._p(otri),
                            orc._p(oinst), orc._p(o2), orc.threads())
     hit = otri >= 0
+    counts = gu.check_hits(mirror.scene, ro.astype(np.float64), rd.astype(np.float64), tri, inst, t, otri, oinst, ot)
     same = (tri == otri) & (inst == oinst)
-    near_tie = hit & (np.abs(o2 - ot) <= gu.TIE_REL * np.abs(ot))
-    mismatch = ~same & ~near_tie
-    both = same & hit
-    rel = np.abs(t[both] - ot[both]) / ot[both]
-    _report(f"hits_kind{kind}", dict(rays=n, hits=int(hit.sum()), id_agreement=float(same.mean()),
-                                     mismatches_beyond_ties=int(mismatch.sum()), t_rel_max=float(rel.max())))
+    _report(f"hits_kind{kind}", dict(rays=n, hits=int(hit.sum()), id_agreement=float(same.mean()), **counts))
     assert hit.mean() > 0.3  # the world is open above: about half the probe rays reach the sky
-    assert mismatch.mean() < 5e-4, int(mismatch.sum())
-    assert rel.max() <= gu.T_REL, rel.max()
 
 
 def _tile_texels(res, probes, W):

@@ -3,8 +3,10 @@
 Tolerances (from the task's statement of the reference path):
   * TLAS order, TLAS node bounds, instance records, BLAS refit bounds and the
     clustered light lists: bit-exact;
-  * hit triangle IDs identical except on near-ties (two nearest candidate t
-    within 1e-6 relative); hit t within 1e-5 relative;
+  * hit triangle IDs identical to the FP64 oracle's on every ray, except where
+    the oracle explains the difference for that ray (near-tie within 1e-6
+    relative, or an FP32 edge graze within the rounding bound of the triangle
+    test); hit t within 1e-5 relative;
   * irradiance / depth atlas texels (RGBA16F) within 1e-3 relative.
 """
 import ctypes as C
@@ -63,25 +65,22 @@ def test_raycast_hits_match_oracle(room):
     ot, otri, oinst, o2 = np.zeros(n), np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n)
     orc.load().orc_closest(C.byref(mirror.scene), orc._p(ro), orc._p(rd), n, 1, 0, orc._p(ot), orc._p(otri),
                            orc._p(oinst), orc._p(o2), orc.threads())
-    hit = otri >= 0
-    same = (tri == otri) & (inst == oinst)
-    near_tie = hit & (np.abs(o2 - ot) <= gu.TIE_REL * np.abs(ot))
-    mismatch = ~same & ~near_tie
-    # a GPU hit on a triangle that FP64 places within 1e-5 of the best is an FP32 edge graze of the
-    # same surface point; count them, they must be rare
-    assert mismatch.mean() < 2e-4, mismatch.sum()
-    both = same & hit
-    rel = np.abs(t[both] - ot[both]) / ot[both]
-    assert rel.max() <= gu.T_REL, rel.max()
+    counts = gu.check_hits(mirror.scene, ro.astype(np.float64), rd.astype(np.float64), tri, inst, t, otri, oinst, ot)
+    print("raycast", counts)
+    code, _ = orc.explain_hits(mirror.scene, ro.astype(np.float64), rd.astype(np.float64), tri, inst, otri, oinst, ot)
     # occlusion queries
     md = np.random.default_rng(12).uniform(0.1, 8.0, n).astype(np.float32)
     blk = np.zeros(n, np.uint8)
     _abi.check(lib.sb_occluded(f.ctx, _abi.ptr(ro), _abi.ptr(rd), _abi.ptr(md), n, _abi.ptr(blk)), f.ctx)
     oblk = np.zeros(n, np.uint8)
     orc.load().orc_any(C.byref(mirror.scene), orc._p(ro), orc._p(rd), orc._p(md), n, orc._p(oblk), orc.threads())
+    # an occlusion answer may differ only where the nearest surface sits at the
+    # shadow ray's end (within 1e-5 of maxDist), or where that ray's closest
+    # hits differ by an explained near-tie or FP32 graze
     disagree = blk != oblk
-    near = np.abs(ot - md) <= 1e-5 * md  # closest surface at the shadow-ray end
-    assert (disagree & ~near).mean() < 2e-4
+    near = np.abs(ot - md) <= 1e-5 * md
+    explained = near | ((code >= 1) & (code <= 4))
+    assert (disagree & ~explained).sum() == 0, np.flatnonzero(disagree & ~explained)[:8]
 
 
 def test_solve_parity_room_four_solves(room):
@@ -101,10 +100,9 @@ def test_solve_parity_room_four_solves(room):
             mirror_state = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy())
             out_ind = mirror.solve(0, P, replay=None)
             mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = mirror_state
-            same = (out_ind["tri"] == rec["tri"]) & (out_ind["inst"] == rec["inst"])
-            t_ind = out_ind["rays"][3::4]
-            tie = (out_ind["tri"] >= 0) & (np.abs(out_ind["second"] - t_ind) <= gu.TIE_REL * np.abs(t_ind))
-            assert (~same & ~tie).mean() < 1e-3, (~same & ~tie).sum()
+            ro, rd = orc.probe_rays(mirror.grid, 0.0, 0, P)
+            gu.check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], out_ind["tri"], out_ind["inst"],
+                          out_ind["rays"][3::4])
             mirror.solve(0, P, replay=rec)
             ga = gu.half_to_f(gu.read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16))
             oa = gu.half_to_f(mirror.atlas.reshape(-1))
