@@ -87,6 +87,14 @@ uint32_t sb_abi_version(void);
 sb_status sb_set_stream(sb_ctx* ctx, void* cuda_stream);
 /* Wait for the context's stream and return the latched device error, if any. */
 sb_status sb_synchronize(sb_ctx* ctx);
+/* Per-ray node-step limit of every traversal walk (0 = the defaults: 2^26
+ * steps on the scene BVH, 2^28 on the reference's TLAS + BLAS walk, and never
+ * more BLAS steps than the pool has nodes). A walk that reaches the limit
+ * ends, and the next sb_synchronize returns SB_ERR_DEVICE_WATCHDOG. Validated
+ * layouts always end well inside the defaults (the reference's walks have no
+ * such limit: its miss links only move forward, spectral_traverse.js:361,
+ * 445); a small limit is how the watchdog path is exercised from the host. */
+sb_status sb_set_walk_step_limit(sb_ctx* ctx, uint32_t steps);
 /* Page-locked host staging memory for the per-frame uploads (vertex gathers,
  * matrices) and read-backs, so copies run at full PCIe / C2C rate. The JS addon
  * wraps such blocks as external ArrayBuffers. */
@@ -247,13 +255,19 @@ sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end);
  * gate) is one file-scope device array of 2 * SB_REFIT_STATIC_MAX_NODES + 64
  * u32 (4 MiB), held by every device that loads the library until exit; ranges
  * of more than SB_REFIT_STATIC_MAX_NODES nodes return SB_ERR_INVALID_ARG.
- * The first call on a device, with that device current, looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any stream
- * capture. Every call shares the array and clears the part it uses; calls that
- * overlap on the GPU (other streams or host threads) race on it. The call runs
- * on `cuda_stream` (NULL = legacy default stream) and synchronises it to read
- * the gate. Errors: SB_ERR_INVALID_ARG, SB_ERR_LAYOUT_VIOLATION (rebuild),
- * SB_ERR_NO_DEVICE, SB_ERR_CUDA; `msg` (may be NULL) receives the text. */
+ * Every call looks up the array's device address for the current device
+ * (cudaGetSymbolAddress, with that device current; the first call on a device
+ * may load the library's device code there, so make it before any stream
+ * capture), so a cudaDeviceReset that reloads the array is followed. Every
+ * call shares the array and clears the part it uses; calls that overlap on the
+ * GPU (other streams or host threads) race on it. The call runs on
+ * `cuda_stream` (NULL = legacy default stream) and synchronises it to read the
+ * gate. Its layout check is stricter than refitFlatBlasRange's: a range whose
+ * nodes do not form one tree (a node no parent reaches, or two roots) is
+ * refused, where the reference would refit it; the per-BLAS ranges of a pool
+ * always form one tree. Errors: SB_ERR_INVALID_ARG, SB_ERR_LAYOUT_VIOLATION
+ * (rebuild), SB_ERR_NO_DEVICE, SB_ERR_CUDA; `msg` (may be NULL) receives the
+ * text. */
 #define SB_REFIT_STATIC_MAX_NODES 524288u
 sb_status sb_refit_blas_static(uint32_t* nodes, uint32_t nodeCount, const uint32_t* triIndex,
                                uint32_t triCount, const float* vertexData, uint32_t vertexCount,
@@ -270,7 +284,9 @@ sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCou
 
 /* Per-source-instance transform table (computeDynamic inputs,
  * spectral_scene.js:1256-1298): column-major 4x4 world matrices in FP64
- * (three's Matrix4.elements), the active flag and the BLAS node range. */
+ * (three's Matrix4.elements), the active flag and the BLAS node range.
+ * A matrix holding a NaN or an infinity returns SB_ERR_INVALID_ARG and a BLAS
+ * range outside the pool SB_ERR_LAYOUT_VIOLATION, before anything changes. */
 sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16,
                            const uint8_t* active, const uint32_t* blasRoot,
                            const uint32_t* blasEnd);
@@ -283,7 +299,9 @@ sb_status sb_build_tlas(sb_ctx* ctx);
  * matrices for `count` source instances; rewrites their instance rows and
  * bounds, then refits the frozen TLAS exactly (refitFlatTlasRange /
  * refitFlatTlasDirty, gi_refit.js:245-430). count == 0 with src == NULL re-derives
- * every slot's bounds from the current BLAS roots (rewriteInstanceRows:false). */
+ * every slot's bounds from the current BLAS roots (rewriteInstanceRows:false).
+ * A non-finite matrix or an instance index out of range returns
+ * SB_ERR_INVALID_ARG with nothing enqueued. */
 sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* srcInstances, const double* world16,
                                uint32_t count);
 

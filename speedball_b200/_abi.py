@@ -135,6 +135,7 @@ SIGNATURES = {
     "sb_last_error": (C.c_char_p, [_P]),
     "sb_abi_version": (_U32, []),
     "sb_set_stream": (C.c_int, [_P, _P]),
+    "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
     "sb_synchronize": (C.c_int, [_P]),
     "sb_upload_scene": (C.c_int, [_P, C.POINTER(sb_scene_view)]),
     "sb_upload_range": (C.c_int, [_P, _U32, _U32, _U32, _P]),

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <functional>
 #include <string>
@@ -49,6 +50,7 @@ struct Cascade {
 struct sb_ctx {
     int device = 0;
     uint32_t flags = 0;
+    uint32_t walkStepLimit = 0;  // sb_set_walk_step_limit (0 = the defaults)
     cudaStream_t stream = nullptr;
     cudaStream_t ownStream = nullptr;
     std::string err;
@@ -223,6 +225,8 @@ DevScene dev_scene(const sb_ctx* c) {
     S.lightCount = c->lightCount;
     S.clustered = c->clustered;
     S.valid = c->B.valid;
+    S.iterCap = c->walkStepLimit ? c->walkStepLimit : SB_WALK_STEPS_DEFAULT;
+    S.iterCapRef = c->walkStepLimit ? c->walkStepLimit : SB_WALK_STEPS_REF_DEFAULT;
     return S;
 }
 
@@ -471,6 +475,12 @@ void sb_host_free(void* p) {
 sb_status sb_set_stream(sb_ctx* ctx, void* s) {
     if (!ctx) return SB_ERR_INVALID_ARG;
     ctx->stream = s ? (cudaStream_t)s : ctx->ownStream;
+    return SB_OK;
+}
+
+sb_status sb_set_walk_step_limit(sb_ctx* ctx, uint32_t steps) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    ctx->walkStepLimit = steps;
     return SB_OK;
 }
 
@@ -1582,17 +1592,29 @@ sb_status sb_refit_blas(sb_ctx* ctx, uint32_t root, uint32_t end) {
     return SB_OK;
 }
 
+// Index of the first of `count` 16-double matrices holding a NaN or an
+// infinity, or `count` when all are finite. A non-finite world matrix would
+// give NaN instance rows, bounds and TLAS build keys.
+static uint32_t first_nonfinite_matrix(const double* world16, uint32_t count) {
+    for (uint32_t i = 0; i < count; ++i)
+        for (int k = 0; k < 16; ++k)
+            if (!std::isfinite(world16[(size_t)i * 16 + k])) return i;
+    return count;
+}
+
 sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, const uint8_t* active,
                            const uint32_t* blasRoot, const uint32_t* blasEnd) {
     if (!ctx || !world16 || !active || !blasRoot || !blasEnd) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
-    ++ctx->epoch;
-    ++ctx->structGen;
     if (count != ctx->B.instCount)
         return fail(ctx, SB_ERR_INVALID_ARG, "instance count %u != scene instCount %u", count, ctx->B.instCount);
     for (uint32_t i = 0; i < count; ++i)
         if (!(blasRoot[i] < blasEnd[i] && blasEnd[i] <= ctx->B.nodeCount))
             return fail(ctx, SB_ERR_LAYOUT_VIOLATION, "instance %u BLAS range [%u,%u) invalid", i, blasRoot[i], blasEnd[i]);
+    if (uint32_t bad = first_nonfinite_matrix(world16, count); bad < count)
+        return fail(ctx, SB_ERR_INVALID_ARG, "instance %u world matrix is not finite", bad);
+    ++ctx->epoch;
+    ++ctx->structGen;
     cudaSetDevice(ctx->device);
     InstanceTable& I = ctx->I;
     if (!ctx->instancesSet || I.count != count) {
@@ -1659,6 +1681,8 @@ sb_status sb_update_transforms(sb_ctx* ctx, const uint32_t* src, const double* w
     cudaSetDevice(ctx->device);
     for (uint32_t i = 0; i < count; ++i)
         if (src[i] >= ctx->I.count) return fail(ctx, SB_ERR_INVALID_ARG, "instance %u out of range", src[i]);
+    if (uint32_t bad = count ? first_nonfinite_matrix(world16, count) : 0u; bad < count)
+        return fail(ctx, SB_ERR_INVALID_ARG, "instance %u world matrix is not finite", src[bad]);
     sb_status s = pack_if_needed(ctx);
     if (s != SB_OK) return s;
     if (count) {

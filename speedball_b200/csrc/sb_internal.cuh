@@ -42,6 +42,9 @@ constexpr uint32_t DEPTH_UNKNOWN = 0xFFFFFFFFu;
 // Entries of the per-thread traversal stack (child-pair and scene-BVH walks).
 #ifndef SB_STACK
 #define SB_STACK 40
+// default per-ray node-step limits of the walks (sb_set_walk_step_limit)
+#define SB_WALK_STEPS_DEFAULT (1u << 26)
+#define SB_WALK_STEPS_REF_DEFAULT (1u << 28)
 #endif
 
 // Per-triangle accept bits packed in the w lane of the first float4 of a
@@ -86,6 +89,10 @@ struct DevScene {
     uint32_t lightCount;
     int32_t clustered;
     const uint32_t* valid;     // nonzero when the last pack validated the layout
+    // per-ray step limits of the walks (node visits; a walk that reaches its
+    // limit latches ERR_WATCHDOG and ends): iterCap for the scene-BVH walks,
+    // iterCapRef for the reference's TLAS + BLAS walks
+    uint32_t iterCap, iterCapRef;
 };
 
 // One cascade solve as the kernels see it.

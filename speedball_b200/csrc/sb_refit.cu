@@ -32,6 +32,21 @@ __global__ void k_refit_reset(uint32_t* parent, uint32_t* arrive, uint32_t root,
     arrive[i] = 0u;
 }
 
+// The end of node i's subtree as its own miss word states it: miss(i) when it
+// lies in (i, end], else the range end (the right spine of the range).
+__device__ __forceinline__ uint32_t subtree_end(const uint32_t* nodes, uint32_t i, uint32_t end) {
+    const uint32_t miss = nodes[8 * i + 6];
+    return (miss > i && miss <= end) ? miss : end;
+}
+
+// A range's gate word: 0 = the layout check failed (the refit reports
+// SB_ERR_LAYOUT_VIOLATION until the next upload); 1 = valid, and every node's
+// own miss word ends its subtree (a leaf: i + 1; an interior node: where its
+// right child's subtree ends), so subtrees can be cut out by index range;
+// 2 = valid for the reference's refit, which reads only left children's miss
+// words (gi_refit.js:96-139), while some other miss word is stale: the range is
+// refit node by node without the subtree partition.
+//
 // Link children to parents and check the layout contract (gi_refit.js:96-139):
 // right child = left child's miss, inside (left, end); leaves index inside the
 // triangle and vertex pools. A node claimed twice, or an orphan, also fails.
@@ -48,6 +63,7 @@ __global__ void k_refit_link(const uint32_t* nodes, const uint32_t* triIndex, co
             for (int k = 0; k < 3; ++k)
                 if (triIndex[3 * t + k] >= vertexCount) { bad(gate, err); return; }
         }
+        if (subtree_end(nodes, i, end) != i + 1u) atomicCAS(gate, 1u, 2u);
         return;
     }
     uint32_t l = i + 1;
@@ -56,6 +72,7 @@ __global__ void k_refit_link(const uint32_t* nodes, const uint32_t* triIndex, co
     if (!(r > l && r < end)) { bad(gate, err); return; }
     if (atomicCAS(&parent[l], NONE, i) != NONE) bad(gate, err);
     if (atomicCAS(&parent[r], NONE, i) != NONE) bad(gate, err);
+    if (subtree_end(nodes, i, end) != subtree_end(nodes, r, end)) atomicCAS(gate, 1u, 2u);
 }
 
 __global__ void k_refit_orphans(const uint32_t* parent, uint32_t root, uint32_t end, uint32_t* gate, uint32_t* err) {
@@ -69,16 +86,11 @@ __device__ __forceinline__ float vload(const uint32_t* p) { return __uint_as_flo
 #ifndef SB_REFIT_ACQREL
 #define SB_REFIT_ACQREL 1
 #endif
-__global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
-                            const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
-                            const uint32_t* parent, uint32_t* arrive, uint32_t root, uint32_t end,
-                            const uint32_t* gate, uint4* pairs, uint32_t* err) {
-    uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end) return;
-    if (*gate == 0u) {
-        if (i == root) latch(err, ERR_LAYOUT);  // the range's layout verdict stands until a new upload
-        return;
-    }
+// One node of the node-by-node refit: a leaf's box (and its re-gathered
+// triangles), then the climb: the second child to finish computes its parent.
+__device__ __forceinline__ void refit_node_climb(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
+                                                 const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
+                                                 const uint32_t* parent, uint32_t* arrive, uint32_t i, uint4* pairs) {
     uint32_t info = nodes[8 * i + 7];
     if (info == INTERIOR) return;
     uint32_t off = info & 0x00FFFFFFu, cnt = info >> 24;
@@ -106,7 +118,6 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
         n[0] = __float_as_uint(mnx); n[1] = __float_as_uint(mny); n[2] = __float_as_uint(mnz);
         n[3] = __float_as_uint(mxx); n[4] = __float_as_uint(mxy); n[5] = __float_as_uint(mxz);
     }
-    // climb: the second child to finish computes its parent
     uint32_t node = i;
     for (;;) {
         uint32_t p = parent[node];
@@ -144,6 +155,19 @@ __global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const flo
     }
 }
 
+__global__ void k_refit_run(uint32_t* nodes, const uint32_t* triIndex, const float* vertexData,
+                            const uint32_t* triMaterial, const uint32_t* matBits, float4* tris,
+                            const uint32_t* parent, uint32_t* arrive, uint32_t root, uint32_t end,
+                            const uint32_t* gate, uint4* pairs, uint32_t* err) {
+    uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= end) return;
+    if (*gate == 0u) {
+        if (i == root) latch(err, ERR_LAYOUT);  // the range's layout verdict stands until a new upload
+        return;
+    }
+    refit_node_climb(nodes, triIndex, vertexData, triMaterial, matBits, tris, parent, arrive, i, pairs);
+}
+
 // Subtrees of at most REFIT_SUB nodes refit inside one CTA: the threaded
 // layout stores a node's subtree as [i, miss(i)) (to the range end on the right
 // spine), so a CTA takes one such range, computes its leaves, and climbs with
@@ -167,7 +191,7 @@ __device__ __forceinline__ uint32_t sub_size(const uint32_t* nodes, uint32_t i, 
 __global__ void k_refit_partition(const uint32_t* nodes, const uint32_t* parent, uint32_t root, uint32_t end,
                                   const uint32_t* gate, uint32_t* subRoots, uint32_t* count) {
     const uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= end || *gate == 0u) return;
+    if (i >= end || *gate != 1u) return;
     if (sub_size(nodes, i, end) > REFIT_SUB) return;
     const uint32_t p = parent[i];
     if (p != NONE && sub_size(nodes, p, end) <= REFIT_SUB) return;
@@ -183,8 +207,14 @@ __global__ void __launch_bounds__(REFIT_SUB) k_refit_cta(uint32_t* nodes, const 
                                                          uint32_t* err) {
     __shared__ float sBox[6 * REFIT_SUB];
     __shared__ uint32_t sArr[REFIT_SUB];
-    if (*gate == 0u) {
+    const uint32_t g = *gate;
+    if (g == 0u) {
         if (blockIdx.x == 0 && threadIdx.x == 0) latch(err, ERR_LAYOUT);  // the range's verdict stands
+        return;
+    }
+    if (g != 1u) {  // no subtree partition for this layout: node by node, grid-stride
+        for (uint32_t i = root + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x)
+            refit_node_climb(nodes, triIndex, vertexData, triMaterial, matBits, tris, parent, arrive, i, pairs);
         return;
     }
     const uint32_t nSub = *count;

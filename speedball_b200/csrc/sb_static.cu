@@ -11,12 +11,11 @@
 // The array is shared by every call on a device and keeps the last call's
 // contents; each call clears the part it uses. Calls that overlap on the GPU
 // (two host threads, or two streams, refitting at once) race on it.
-// The first call on a device resolves the array's device address
-// (cudaGetSymbolAddress) with that device current; make that first call before
-// any stream capture.
+// Every call resolves the array's device address (cudaGetSymbolAddress) with
+// the device current; the first call on a device may load the library's device
+// code there, so make it before any stream capture.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "sb_kernels.cuh"
 
@@ -119,10 +118,6 @@ __global__ void k_static_run(uint32_t* nodes, const uint32_t* triIndex, const fl
     }
 }
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-uint32_t* g_scratchPtr[kMaxDevices] = {};
-
 void put_msg(char* msg, size_t len, const char* text) {
     if (msg && len) {
         std::strncpy(msg, text, len - 1);
@@ -151,29 +146,23 @@ extern "C" sb_status sb_refit_blas_static(uint32_t* nodes, uint32_t nodeCount, c
         return SB_ERR_INVALID_ARG;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         put_msg(msg, msgLen, "sb_refit_blas_static: no current CUDA device");
         return SB_ERR_NO_DEVICE;
     }
-    uint32_t* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratchPtr[dev]) {
-            // once per device, with that device current: the host-side name of a
-            // __device__ array is not a device address
-            void* p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_refitScratch);
-            if (e != cudaSuccess || !p) {
-                char buf[160];
-                std::snprintf(buf, sizeof buf, "sb_refit_blas_static: cudaGetSymbolAddress failed: %s",
-                              cudaGetErrorString(e));
-                put_msg(msg, msgLen, buf);
-                return SB_ERR_CUDA;
-            }
-            g_scratchPtr[dev] = static_cast<uint32_t*>(p);
-        }
-        scratch = g_scratchPtr[dev];
+    // The host-side name of a __device__ array is not a device address: look
+    // the address up with the device current. Every call looks it up again (a
+    // lookup, no allocation), so an address cached across a cudaDeviceReset,
+    // after which the module and its array are loaded anew, is never used.
+    void* sym = nullptr;
+    cudaError_t se = cudaGetSymbolAddress(&sym, g_refitScratch);
+    if (se != cudaSuccess || !sym) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "sb_refit_blas_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(se));
+        put_msg(msg, msgLen, buf);
+        return SB_ERR_CUDA;
     }
+    uint32_t* scratch = static_cast<uint32_t*>(sym);
     cudaStream_t st = (cudaStream_t)cudaStream;
     const uint32_t n = end - root;
     const unsigned g = (n + 255) / 256;
@@ -182,6 +171,11 @@ extern "C" sb_status sb_refit_blas_static(uint32_t* nodes, uint32_t nodeCount, c
     k_static_orphans<<<g, 256, 0, st>>>(scratch, scratch, root, end);
     k_static_run<<<g, 256, 0, st>>>(nodes, triIndex, vertexData, scratch, root, end);
     for (int k = 0; k < 4; ++k) sb::note_launch();
+    cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+        put_msg(msg, msgLen, cudaGetErrorString(le));
+        return SB_ERR_CUDA;
+    }
     uint32_t gate = 0;
     cudaError_t e = cudaMemcpyAsync(&gate, scratch + 2 * kMaxNodes, sizeof gate, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -107,7 +107,7 @@ __device__ __forceinline__ bool walk(const DevScene& S, const uint4* tl, float3 
                 done = true;
                 break;
             }
-            if (++iter > (1u << 28)) {
+            if (++iter > S.iterCapRef) {
                 latch(err, ERR_WATCHDOG);
                 done = true;
                 break;
@@ -192,7 +192,7 @@ __device__ __forceinline__ bool blas_walk(const DevScene& S, uint32_t inst, floa
         uint32_t leafOff = 0, leafCnt = 0, leafMiss = 0;
         bool leaf = false;
         while (cursor < end) {
-            if (++it > S.nodeCount) {
+            if (++it > min(S.nodeCount, S.iterCapRef)) {
                 latch(err, ERR_WATCHDOG);
                 return ANY ? false : bestTri >= 0;
             }
@@ -381,7 +381,7 @@ __device__ __forceinline__ bool pair_walk(const DevScene& S, const uint4* tp, fl
                 if (!ANY && __uint_as_float(e.y) >= tmax) continue;  // behind the nearest hit now
                 cur = e.x;
             }
-            if (++iter > (1u << 28)) {
+            if (++iter > S.iterCapRef) {
                 latch(err, ERR_WATCHDOG);
                 done = true;
                 break;
@@ -528,7 +528,7 @@ __device__ __forceinline__ bool flat_walk(const DevScene& S, float3 wro, float3 
                 cur = FLAT_NONE;
                 break;
             }
-            if (++iter > (1u << 26)) {
+            if (++iter > S.iterCap) {
                 latch(err, ERR_WATCHDOG);
                 done = true;
                 break;
@@ -860,7 +860,7 @@ __device__ __forceinline__ bool wide_walk(const DevScene& S, float3 wro, float3 
                     break;
                 }
             }
-            if (++iter > (1u << 26)) {
+            if (++iter > S.iterCap) {
                 latch(err, ERR_WATCHDOG);
                 done = true;
                 break;
@@ -964,7 +964,7 @@ __device__ __forceinline__ int wide_step(const DevScene& S, WideWalk& w, float& 
                 return 1;
             }
         }
-        if (++w.iter > (1u << 26)) {
+        if (++w.iter > S.iterCap) {
             latch(err, ERR_WATCHDOG);
             return 1;
         }

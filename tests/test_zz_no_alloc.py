@@ -70,7 +70,7 @@ def test_static_refit_matches_context_refit_on_consecutive_calls():
             before = pool.bvhNodes.reshape(-1)[root * 8:end * 8]
             assert not np.array_equal(got[root * 8:end * 8], before)  # the refit moved the bounds
 
-        deform_and_compare(1)   # first call on the device: sets up the scratch address
+        deform_and_compare(1)   # first call on the device: its device code and scratch address
         deform_and_compare(1)   # same range again: scratch from the last call is cleared
         # a range whose right child escapes it fails closed and leaves the pool usable
         r, e = int(pool.blas_root[3]), int(pool.blas_end[3])
