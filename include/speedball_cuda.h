@@ -235,6 +235,42 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
 sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist,
                       uint32_t n, uint8_t* blockedOut);
 
+/* ------------------------------------------------------- receiver gather */
+
+/* The receiver's uniforms (GiProbeNode, gi_probes.js:306-358). */
+typedef struct sb_gather_params {
+    float normalBias[2];       /* sample-point offset along the stable normal; the
+                                  point uses normalBias[0] for both cascades, as
+                                  GiProbeNode.setup does (0.04)                   */
+    float chebyBias[2];        /* Chebyshev depth tolerance per cascade (0)       */
+    float chebyStrength;       /* 0 = pure trilinear (default), 1 = full
+                                  Chebyshev visibility and wrap weights           */
+    float detailStrength;      /* dual-detail blend toward the detail normal (1)  */
+    float intensity;           /* output scale (1)                                */
+    float enabled;             /* output gate (1)                                 */
+    float samplePositionScale; /* debug position scale (1)                        */
+    float sampleBiasScale;     /* debug bias scale (1)                            */
+    float borderBand;          /* fine-box blend band as a fraction of it (0.15)  */
+    uint32_t cascades;         /* 1: cascade 0 alone; 2: cascade 1 of the context
+                                  is the fine box blended inside cascade 0        */
+    uint32_t dualDetail;       /* 1: fetch at both normals and blend by
+                                  detailStrength (one cascade only)               */
+} sb_gather_params;
+void sb_gather_params_defaults(sb_gather_params* p);
+/* Receiver gather (GiProbeNode.sampleIrradiance and setup, gi_probes.js:530-657,
+ * 816-850, 884-928): per G-buffer sample the irradiance of the context's
+ * current atlases, E = max(trilinear 8-tap gather, 0) * intensity * enabled.
+ * position, stableNormal (the bias / visibility normal) and detailNormal (the
+ * fetch direction) are DEVICE arrays of `count` float4 (xyz used, 16-byte
+ * aligned), out a device array of `count` float4 (rgb, 1). Enqueued on the
+ * context's stream; reads the atlases of the last enqueued solve. Classification
+ * is inert (no state atlas); the two-cascade path picks each cage at the
+ * unbiased surface position. Errors: SB_ERR_INVALID_ARG (null, misaligned,
+ * cascades not 1 or 2, dualDetail with 2 cascades), SB_ERR_NOT_READY (a
+ * cascade not configured). */
+sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* params, const float* position,
+                               const float* stableNormal, const float* detailNormal, uint32_t count, float* out);
+
 /* ------------------------------------------------- refit / TLAS lanes (GPU) */
 
 /* BLAS refit over node range [root, end) from the current vertexData

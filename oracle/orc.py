@@ -83,6 +83,8 @@ def load() -> C.CDLL:
             "orc_compute_instances": (None, [P, P, P, U, P, P, P]),
             "orc_probe_rays": (None, [P, C.c_double, U, U, P, P]),
             "orc_explain_hits": (None, [P, P, P, U, P, P, P, P, P, P, P, C.c_int32]),
+            "orc_gather": (None, [P, P, P, P, P, P, P, P, P, P, U, P, P, C.c_int32]),
+            "orc_gather_params_size": (U, []),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
@@ -481,3 +483,39 @@ def grid_dict(grid_min, grid_size, res, rays) -> dict:
     return dict(gridMin=list(grid_min), gridSize=list(grid_size), res=list(res), rays=rays,
                 maxDist=float(np.linalg.norm(gs)),
                 cellMin=float(max(1e-4, min(gs[a] / max(1, res[a] - 1) for a in range(3)))))
+
+
+
+# ---------------------------------------------------------- receiver gather
+GATHER_PARAM_NAMES = ["normalBias0", "normalBias1", "chebyBias0", "chebyBias1", "chebyStrength", "detailStrength",
+                      "intensity", "enabled", "samplePositionScale", "sampleBiasScale", "borderBand", "cascades",
+                      "dualDetail"]
+
+
+def gather_params(**kw) -> np.ndarray:
+    """The receiver's uniforms at their initial values (gi_probes.js:314-358:
+    normalBias 0.04, chebyBias 0, detailStrength 1, intensity 1, chebyStrength
+    0, borderBand 0.15, the sample scales 1, one cascade), overridden by `kw`,
+    each rounded to float32 as a uniform stores it."""
+    v = dict(normalBias0=0.04, normalBias1=0.04, chebyBias0=0.0, chebyBias1=0.0, chebyStrength=0.0,
+             detailStrength=1.0, intensity=1.0, enabled=1.0, samplePositionScale=1.0, sampleBiasScale=1.0,
+             borderBand=0.15, cascades=1.0, dualDetail=0.0)
+    v.update(kw)
+    out = np.array([np.float32(v[k]) for k in GATHER_PARAM_NAMES], np.float64)
+    assert out.shape[0] == load().orc_gather_params_size()
+    return out
+
+
+def gather(grid0: OrcGrid, atlas0: np.ndarray, depth0: np.ndarray, params: np.ndarray, pos4: np.ndarray,
+           nvis4: np.ndarray, ndir4: np.ndarray, grid1: OrcGrid | None = None, atlas1: np.ndarray | None = None,
+           depth1: np.ndarray | None = None):
+    """FP64 receiver irradiance at n surface points (n x 3) and each point's
+    distance to a discontinuity of the gather (cage floor, Chebyshev select)."""
+    n = pos4.shape[0]
+    out = np.zeros((n, 3), np.float64)
+    near = np.zeros(n, np.float64)
+    arr = [np.ascontiguousarray(a, np.float32) for a in (pos4, nvis4, ndir4)]
+    load().orc_gather(C.byref(grid0), C.byref(grid1) if grid1 is not None else None, _p(atlas0), _p(depth0),
+                      _p(atlas1), _p(depth1), _p(np.ascontiguousarray(params, np.float64)), *[_p(a) for a in arr], n,
+                      _p(out), _p(near), threads())
+    return out, near

@@ -3,6 +3,7 @@
 #include "orc_probes.hpp"
 #include "orc_scene.hpp"
 #include "orc_bvh.hpp"
+#include "orc_gather.hpp"
 
 #include <atomic>
 #include <thread>
@@ -293,6 +294,31 @@ int orc_solve_f32(const OrcScene* s, const OrcLights* l, const OrcGrid* g, const
 }
 
 uint32_t orc_params_size(void) { return (uint32_t)(sizeof(Params) / sizeof(double)); }
+
+// Receiver gather (orc_gather.hpp) of n surface points, FP64. pos/nvis/ndir are
+// 4 floats per point (xyz used); out is 3 doubles per point; near (may be null)
+// receives each point's distance to a discontinuity of the gather.
+void orc_gather(const OrcGrid* g0, const OrcGrid* g1, const uint16_t* atlas0, const uint16_t* depth0,
+                const uint16_t* atlas1, const uint16_t* depth1, const double* params, const float* pos4,
+                const float* nvis4, const float* ndir4, uint32_t n, double* out3, double* near, int32_t threads) {
+    Grid G0 = to_grid(g0), G1;
+    if (g1) G1 = to_grid(g1);
+    GatherParams prm;
+    std::memcpy(&prm, params, sizeof prm);
+    GatherCascade C[2];
+    C[0].g = &G0; C[0].atlas = atlas0; C[0].depth = depth0;
+    if (g1) { C[1].g = &G1; C[1].atlas = atlas1; C[1].depth = depth1; }
+    parallel_for(n, threads, [&](size_t i, int) {
+        V3<double> p(pos4[i * 4], pos4[i * 4 + 1], pos4[i * 4 + 2]);
+        V3<double> a(nvis4[i * 4], nvis4[i * 4 + 1], nvis4[i * 4 + 2]);
+        V3<double> b(ndir4[i * 4], ndir4[i * 4 + 1], ndir4[i * 4 + 2]);
+        double nr = INFINITY;
+        V3<double> e = gather_point<double>(C, prm, p, a, b, nr);
+        out3[i * 3] = e.x; out3[i * 3 + 1] = e.y; out3[i * 3 + 2] = e.z;
+        if (near) near[i] = nr;
+    });
+}
+uint32_t orc_gather_params_size(void) { return (uint32_t)(sizeof(GatherParams) / sizeof(double)); }
 
 // ------------------------------------------------------------ light grid
 void orc_light_grid(const OrcGrid* g0, const float* lights, uint32_t lightCount, float* out, int32_t fp32) {

@@ -114,6 +114,13 @@ class sb_tuning(C.Structure):
                 ("bvhKind", C.c_uint32), ("smemWideNodes", C.c_uint32)]
 
 
+class sb_gather_params(C.Structure):
+    _fields_ = [("normalBias", C.c_float * 2), ("chebyBias", C.c_float * 2), ("chebyStrength", C.c_float),
+                ("detailStrength", C.c_float), ("intensity", C.c_float), ("enabled", C.c_float),
+                ("samplePositionScale", C.c_float), ("sampleBiasScale", C.c_float), ("borderBand", C.c_float),
+                ("cascades", C.c_uint32), ("dualDetail", C.c_uint32)]
+
+
 class sb_stats(C.Structure):
     _fields_ = [("primaryRays", C.c_uint64), ("shadowRays", C.c_uint64),
                 ("tlasNodeVisits", C.c_uint64), ("instanceVisits", C.c_uint64),
@@ -136,6 +143,8 @@ SIGNATURES = {
     "sb_abi_version": (_U32, []),
     "sb_set_stream": (C.c_int, [_P, _P]),
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
+    "sb_gather_params_defaults": (None, [_P]),
+    "sb_gather_irradiance": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "sb_synchronize": (C.c_int, [_P]),
     "sb_upload_scene": (C.c_int, [_P, C.POINTER(sb_scene_view)]),
     "sb_upload_range": (C.c_int, [_P, _U32, _U32, _U32, _P]),

@@ -1538,6 +1538,67 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
     return sb_synchronize(ctx);
 }
 
+void sb_gather_params_defaults(sb_gather_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof *p);
+    p->normalBias[0] = p->normalBias[1] = 0.04f;
+    p->detailStrength = 1.0f;
+    p->intensity = 1.0f;
+    p->enabled = 1.0f;
+    p->samplePositionScale = 1.0f;
+    p->sampleBiasScale = 1.0f;
+    p->borderBand = 0.15f;
+    p->cascades = 1;
+}
+
+sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const float* position,
+                               const float* stableNormal, const float* detailNormal, uint32_t count, float* out) {
+    if (!ctx || !prm || (count && (!position || !stableNormal || !detailNormal || !out)))
+        return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    if (!aligned(position) || !aligned(stableNormal) || !aligned(detailNormal) || !aligned(out))
+        return fail(ctx, SB_ERR_INVALID_ARG, "gather arrays must be 16-byte aligned float4 arrays");
+    if (prm->cascades < 1 || prm->cascades > 2) return fail(ctx, SB_ERR_INVALID_ARG, "cascades must be 1 or 2");
+    if (prm->cascades == 2 && prm->dualDetail) return fail(ctx, SB_ERR_INVALID_ARG, "dual detail needs one cascade");
+    for (uint32_t c = 0; c < prm->cascades; ++c)
+        if (!ctx->casc[c].configured || !ctx->casc[c].atlas)
+            return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", c);
+    if (count == 0) return SB_OK;
+    cudaSetDevice(ctx->device);
+    GatherArgs A{};
+    for (uint32_t c = 0; c < prm->cascades; ++c) {
+        const Cascade& K = ctx->casc[c];
+        for (int a = 0; a < 3; ++a) {
+            A.c[c].gridMin[a] = K.grid.gridMin[a];
+            A.c[c].gridSize[a] = K.grid.gridSize[a];
+            A.c[c].res[a] = float(K.grid.res[a]);
+        }
+        A.c[c].atlasW = K.atlasW;
+        A.c[c].atlasH = K.atlasH;
+        A.c[c].atlas = K.atlas;
+        A.c[c].depth = K.depthAtlas;
+    }
+    A.cascades = prm->cascades;
+    A.dualDetail = prm->dualDetail ? 1u : 0u;
+    A.count = count;
+    A.normalBias0 = prm->normalBias[0];
+    A.chebyBias[0] = prm->chebyBias[0];
+    A.chebyBias[1] = prm->chebyBias[1];
+    A.chebyStrength = prm->chebyStrength;
+    A.detailStrength = prm->detailStrength;
+    A.intensity = prm->intensity;
+    A.enabled = prm->enabled;
+    A.samplePositionScale = prm->samplePositionScale;
+    A.sampleBiasScale = prm->sampleBiasScale;
+    A.borderBand = prm->borderBand;
+    A.position = reinterpret_cast<const float4*>(position);
+    A.stableNormal = reinterpret_cast<const float4*>(stableNormal);
+    A.detailNormal = reinterpret_cast<const float4*>(detailNormal);
+    A.out = reinterpret_cast<float4*>(out);
+    CK(launch_gather(A, ctx->stream));
+    return SB_OK;
+}
+
 sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist, uint32_t n, uint8_t* out) {
     if (!ctx || (n && (!ro || !rd || !maxDist || !out))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (!ctx->sceneLoaded || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "scene / TLAS not ready");

@@ -1,0 +1,148 @@
+// sb_gather.cu — the receiver gather: the irradiance the probe field gives a
+// surface point, the consumer of the atlases this library updates. The
+// reference evaluates it per fragment in GiProbeNode (gi_probes.js:530-657,
+// 816-850, 884-928); here one thread evaluates one G-buffer sample.
+//
+// Per sample: P = position * samplePositionScale + Nvis * normalBias[0] *
+// sampleBiasScale; with one cascade, _sampleCascade at P; with two, the coarse
+// and fine looped gathers blended by the fine box's border band, each choosing
+// its cage at the unbiased surface position (the looped gather's stated intent,
+// gi_probes.js:628-631). Each of the 8 cage taps fetches the RGBA16F atlas
+// bilinearly (clamp to edge, exact weights) in the detail normal's octahedral
+// direction; with chebyStrength > 0 it also fetches the depth moments toward
+// the surface for the Chebyshev visibility weight and applies the wrap weight.
+// Output E = max(sample, 0) * intensity * enabled as float4 (rgb, 1).
+//
+// Work is one probe field's worth of tiny atlases (L1/L2-resident) against a
+// streamed G-buffer: 48 bytes in and 16 bytes out per sample are the HBM
+// traffic, so the kernel is HBM-bound on the G-buffer stream. Classification
+// is inert (classifyStrength 0): no state atlas is read.
+#include "sb_kernels.cuh"
+#include "sb_math.cuh"
+
+namespace sb {
+
+namespace {
+
+__device__ __forceinline__ float3 bilinear3(const uint2* atlas, uint32_t W, uint32_t H, float u, float v) {
+    const float x = u * float(W) - 0.5f, y = v * float(H) - 0.5f;
+    const float fx0 = floorf(x), fy0 = floorf(y);
+    const float fx = x - fx0, fy = y - fy0;
+    const int x0 = (int)fx0, y0 = (int)fy0;
+    const int Wi = (int)W, Hi = (int)H;
+    const int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
+    const int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
+    const float4 t00 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xa));
+    const float4 t10 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xb));
+    const float4 t01 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xa));
+    const float4 t11 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xb));
+    const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
+    return mk(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
+              t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
+              t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
+}
+
+__device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, float chebyBias, float3 cageP,
+                                 float3 P, float3 Nvis, float3 Ndir, bool dual) {
+    float base[3], frac[3], rm1[3];
+    const float cp[3] = {cageP.x, cageP.y, cageP.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        rm1[a] = fmaxf(C.res[a] - 1.0f, 1.0f);
+        const float cell = C.gridSize[a] / rm1[a];
+        const float gf = (cp[a] - C.gridMin[a]) / fmaxf(cell, 1e-6f);
+        base[a] = clampf(floorf(gf), 0.0f, fmaxf(C.res[a] - 2.0f, 0.0f));
+        frac[a] = clampf(gf - base[a], 0.0f, 1.0f);
+    }
+    const float3 Nn = normalize3(Nvis);
+    const float2 oN = oct_encode(normalize3(Ndir));
+    const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
+    const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
+    const float cs = A.chebyStrength;
+    float3 acc = mk(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f;
+#pragma unroll 2
+    for (int i = 0; i < 8; ++i) {
+        const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+        const float px = base[0] + float(dx), py = base[1] + float(dy), pz = base[2] + float(dz);
+        const float wx = dx ? frac[0] : 1.0f - frac[0];
+        const float wy = dy ? frac[1] : 1.0f - frac[1];
+        const float wz = dz ? frac[2] : 1.0f - frac[2];
+        const float wTri = wx * wy * wz + 1e-4f;
+        const float col = px, row = pz * C.res[1] + py;
+        const float ox0 = col * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
+        float w = wTri;
+        if (cs != 0.0f) {
+            const float3 probePos = mk(C.gridMin[0] + px / rm1[0] * C.gridSize[0],
+                                       C.gridMin[1] + py / rm1[1] * C.gridSize[1],
+                                       C.gridMin[2] + pz / rm1[2] * C.gridSize[2]);
+            const float3 toSurf = P - probePos;
+            const float dist = sqrtf(dot3(toSurf, toSurf));
+            const float inv = 1.0f / fmaxf(dist, 1e-6f);
+            const float2 oD = oct_encode(toSurf * inv);
+            const float3 m = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oD.x * 6.0f) * invW,
+                                       (oy0 + oD.y * 6.0f) * invH);
+            const float m1 = m.x, m2 = m.y;
+            const float variance = fabsf(m2 - m1 * m1);
+            const float dm = fmaxf(dist - m1 - chebyBias, 0.0f);
+            const float chebyRaw = variance / fmaxf(variance + dm * dm, 1e-6f);
+            const float cheby = dist <= m1 + chebyBias ? 1.0f : chebyRaw;
+            const float visW = (1.0f - cs) + fmaxf(cheby * cheby * cheby, 0.05f) * cs;
+            const float3 toProbe = (probePos - P) * inv;
+            const float wrap = dot3(toProbe, Nn) * 0.5f + 0.5f;
+            const float wrapW = (1.0f - cs) + fmaxf(wrap * wrap, 0.05f) * cs;
+            w = wTri * wrapW * visW;
+        }
+        float3 e = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oN.x * 6.0f) * invW, (oy0 + oN.y * 6.0f) * invH);
+        if (dual) {
+            const float3 eS = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oS.x * 6.0f) * invW,
+                                        (oy0 + oS.y * 6.0f) * invH);
+            const float t = A.detailStrength;
+            e = eS * (1.0f - t) + e * t;
+        }
+        acc = acc + e * w;
+        wsum += w;
+    }
+    return acc * (1.0f / fmaxf(wsum, 1e-4f));
+}
+
+__global__ void __launch_bounds__(256) k_gather(const GatherArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.count) return;
+    const float4 p4 = __ldcs(A.position + i), n4 = __ldcs(A.stableNormal + i), d4 = __ldcs(A.detailNormal + i);
+    const float3 Nvis = xyz(n4), Ndir = xyz(d4);
+    const float3 reflP = xyz(p4) * A.samplePositionScale;
+    const float3 P = reflP + Nvis * A.normalBias0 * A.sampleBiasScale;
+    float3 E;
+    if (A.cascades < 2) {
+        E = gather_cascade(A.c[0], A, A.chebyBias[0], P, P, Nvis, Ndir, A.dualDetail != 0);
+    } else {
+        const GatherCascade& F = A.c[1];
+        const float f0 = (P.x - F.gridMin[0]) / fmaxf(F.gridSize[0], 1e-6f);
+        const float f1 = (P.y - F.gridMin[1]) / fmaxf(F.gridSize[1], 1e-6f);
+        const float f2 = (P.z - F.gridMin[2]) / fmaxf(F.gridSize[2], 1e-6f);
+        const float fLo = fminf(fminf(f0, f1), f2);
+        const float fHi = fminf(fminf(1.0f - f0, 1.0f - f1), 1.0f - f2);
+        const float wIn = clampf(fminf(fLo, fHi) / fmaxf(A.borderBand, 1e-4f), 0.0f, 1.0f);
+        const float wFine = wIn * clampf(float(A.cascades) - 1.0f, 0.0f, 1.0f);
+        E = mk(0.0f, 0.0f, 0.0f);
+        if (wFine < 1.0f) E = gather_cascade(A.c[0], A, A.chebyBias[0], reflP, P, Nvis, Ndir, false);
+        if (wFine > 0.0f) {
+            const float3 Ef = gather_cascade(A.c[1], A, A.chebyBias[1], reflP, P, Nvis, Ndir, false);
+            E = E * (1.0f - wFine) + Ef * wFine;
+        }
+    }
+    const float k = A.intensity * A.enabled;
+    __stcs(A.out + i, make_float4(fmaxf(E.x, 0.0f) * k, fmaxf(E.y, 0.0f) * k, fmaxf(E.z, 0.0f) * k, 1.0f));
+}
+
+}  // namespace
+
+cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st) {
+    if (A.count == 0) return cudaSuccess;
+    k_gather<<<(A.count + 255) / 256, 256, 0, st>>>(A);
+    note_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace sb

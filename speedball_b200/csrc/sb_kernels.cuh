@@ -139,6 +139,26 @@ cudaError_t launch_tlas_index(const SceneBuffers& B, const InstanceTable& I, uin
 cudaError_t launch_blas_pairs(const SceneBuffers& B, cudaStream_t st);
 cudaError_t launch_tlas_pairs(const SceneBuffers& B, cudaStream_t st);
 
+// Receiver gather (sb_gather.cu): one cascade's atlases and grid as the gather
+// reads them, and one launch's G-buffer.
+struct GatherCascade {
+    float gridMin[3], gridSize[3], res[3];
+    uint32_t atlasW, atlasH;
+    const uint2* atlas;   // RGBA16F irradiance atlas
+    const uint2* depth;   // RGBA16F depth-moment atlas
+};
+struct GatherArgs {
+    GatherCascade c[2];
+    uint32_t cascades, dualDetail, count;
+    float normalBias0, chebyBias[2], chebyStrength, detailStrength, intensity, enabled;
+    float samplePositionScale, sampleBiasScale, borderBand;
+    const float4* position;
+    const float4* stableNormal;
+    const float4* detailNormal;
+    float4* out;
+};
+cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st);
+
 // Arbitrary-ray queries through the same traversal (raycastFirst-like).
 cudaError_t launch_raycast(const DevScene& S, const float* ro, const float* rd, uint32_t n, float* tOut,
                            int32_t* triOut, int32_t* instOut, uint32_t* err, cudaStream_t st);
