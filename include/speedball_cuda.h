@@ -437,6 +437,13 @@ typedef struct sb_tuning {
                                  80 bytes each (0 = none, at most 512)             */
 } sb_tuning;
 sb_status sb_get_tuning(const sb_ctx* ctx, sb_tuning* out);
+/* The ray/triangle test this library was built with: 0 = the reference's
+ * Moller-Trumbore test (spectral_traverse.js:393-409), the parity default of
+ * libspeedball_cuda.so; 1 = the watertight test of Woop, Benthin & Wald 2013
+ * (libspeedball_cuda_watertight.so, built with SB_WATERTIGHT=1): no ray passes
+ * between two triangles that share an edge or a vertex. Both apply the
+ * reference's side and alpha acceptance to the same (u, v, t, det sign). */
+uint32_t sb_triangle_test(void);
 sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t);
 /* Time full solves of `cascade` under candidate tunings (bvhKind 1 / 2 / 0,
  * traceBlock 128 / 192 / 256, sortKey 0-3, for bvhKind 1 smemWideNodes

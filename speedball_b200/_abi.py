@@ -143,6 +143,7 @@ SIGNATURES = {
     "sb_abi_version": (_U32, []),
     "sb_set_stream": (C.c_int, [_P, _P]),
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
+    "sb_triangle_test": (C.c_uint32, []),
     "sb_gather_params_defaults": (None, [_P]),
     "sb_gather_irradiance": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "sb_synchronize": (C.c_int, [_P]),
@@ -209,19 +210,30 @@ class PinnedArray:
 _lib = None
 
 
-def load() -> C.CDLL:
-    """Load the library once; raise LibraryMissing when it is not built."""
+_variants: dict = {}
+
+
+def load(variant: str | None = None) -> C.CDLL:
+    """Load the library once; raise LibraryMissing when it is not built.
+    `variant` names a build variant next to it, libspeedball_cuda_<variant>.so
+    ("watertight": the watertight ray/triangle test)."""
     global _lib
-    if _lib is not None:
+    if variant is None and _lib is not None:
         return _lib
-    if not LIB_PATH.exists():
-        raise LibraryMissing(f"{LIB_PATH} is missing: build it with `python speedball_b200/build.py`")
-    lib = C.CDLL(str(LIB_PATH))
+    if variant is not None and variant in _variants:
+        return _variants[variant]
+    path = LIB_PATH if variant is None else LIB_PATH.with_name(f"libspeedball_cuda_{variant}.so")
+    if not path.exists():
+        raise LibraryMissing(f"{path} is missing: build it with `python speedball_b200/build.py`")
+    lib = C.CDLL(str(path))
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
+    if variant is None:
+        _lib = lib
+    else:
+        _variants[variant] = lib
     return lib
 
 

@@ -21,7 +21,8 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 
 
-VARIANT_SOURCES = ("sb_trace.cu", "sb_refit.cu")  # the only sources that read the tuning macros
+VARIANT_SOURCES = ("sb_trace.cu", "sb_refit.cu", "sb_adjoint.cu")  # the sources that read the build macros
+WATERTIGHT_LIB = HERE / "libspeedball_cuda_watertight.so"
 
 
 def sources():
@@ -66,6 +67,11 @@ def build(verbose: bool = False, force: bool = False, defines=(), out: Path | No
     return lib
 
 
+def build_all(verbose: bool = False, force: bool = False) -> list:
+    """The default library and the watertight-triangle-test variant."""
+    return [build(verbose, force), build(verbose, force, defines=["SB_WATERTIGHT=1"], out=WATERTIGHT_LIB)]
+
+
 if __name__ == "__main__":
-    build(verbose="-v" in sys.argv, force="--force" in sys.argv)
-    print(LIB)
+    for lib in build_all(verbose="-v" in sys.argv, force="--force" in sys.argv):
+        print(lib)

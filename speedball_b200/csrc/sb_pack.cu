@@ -59,8 +59,8 @@ __global__ void k_pack_tris(const uint32_t* triIndex, const float* vertexData, c
     const float* c = vertexData + (size_t)i2 * 8u;
     float3 p0 = make_float3(a[0], a[1], a[2]);
     tris[3 * t] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(matBits[m]));
-    tris[3 * t + 1] = make_float4(b[0] - p0.x, b[1] - p0.y, b[2] - p0.z, 0.0f);
-    tris[3 * t + 2] = make_float4(c[0] - p0.x, c[1] - p0.y, c[2] - p0.z, 0.0f);
+    tris[3 * t + 1] = make_float4(b[0], b[1], b[2], 0.0f);
+    tris[3 * t + 2] = make_float4(c[0], c[1], c[2], 0.0f);
 }
 
 // Threaded-layout checks that make every BLAS walk memory-safe and finite:

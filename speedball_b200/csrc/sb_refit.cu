@@ -111,8 +111,8 @@ __device__ __forceinline__ void refit_node_climb(uint32_t* nodes, const uint32_t
             }
             // re-gather the pre-gathered triangle from the deformed vertices
             tris[3 * t] = make_float4(p[0].x, p[0].y, p[0].z, __uint_as_float(matBits[triMaterial[t]]));
-            tris[3 * t + 1] = make_float4(p[1].x - p[0].x, p[1].y - p[0].y, p[1].z - p[0].z, 0.0f);
-            tris[3 * t + 2] = make_float4(p[2].x - p[0].x, p[2].y - p[0].y, p[2].z - p[0].z, 0.0f);
+            tris[3 * t + 1] = make_float4(p[1].x, p[1].y, p[1].z, 0.0f);
+            tris[3 * t + 2] = make_float4(p[2].x, p[2].y, p[2].z, 0.0f);
         }
         uint32_t* n = nodes + 8 * i;
         n[0] = __float_as_uint(mnx); n[1] = __float_as_uint(mny); n[2] = __float_as_uint(mnz);
@@ -248,8 +248,8 @@ __global__ void __launch_bounds__(REFIT_SUB) k_refit_cta(uint32_t* nodes, const 
                             if (z > mxz) mxz = z;
                         }
                         tris[3 * tr] = make_float4(p[0].x, p[0].y, p[0].z, __uint_as_float(matBits[triMaterial[tr]]));
-                        tris[3 * tr + 1] = make_float4(p[1].x - p[0].x, p[1].y - p[0].y, p[1].z - p[0].z, 0.0f);
-                        tris[3 * tr + 2] = make_float4(p[2].x - p[0].x, p[2].y - p[0].y, p[2].z - p[0].z, 0.0f);
+                        tris[3 * tr + 1] = make_float4(p[1].x, p[1].y, p[1].z, 0.0f);
+                        tris[3 * tr + 2] = make_float4(p[2].x, p[2].y, p[2].z, 0.0f);
                     }
                     n[0] = __float_as_uint(mnx); n[1] = __float_as_uint(mny); n[2] = __float_as_uint(mnz);
                     n[3] = __float_as_uint(mxx); n[4] = __float_as_uint(mxy); n[5] = __float_as_uint(mxz);

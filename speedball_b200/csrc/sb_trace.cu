@@ -688,3 +688,5 @@ cudaError_t launch_occluded(const DevScene& S, const float* ro, const float* rd,
 }
 
 }  // namespace sb
+
+extern "C" uint32_t sb_triangle_test(void) { return SB_WATERTIGHT ? 1u : 0u; }

@@ -33,10 +33,12 @@ __device__ __forceinline__ bool slab(float3 bmin, float3 bmax, float3 ro, float3
 }
 
 // Möller–Trumbore on a pre-gathered triangle, spectral_traverse.js:393-409.
+// The triangle is stored as its three vertices; the edges are formed here with
+// the same FP32 subtractions the reference's test makes.
 __device__ __forceinline__ bool mt_hit(const float4* tris, uint32_t tri, float3 ro, float3 rd, float tmax, float& t,
                                        float& det, float& u, float& v, uint32_t& bits) {
     float4 a = __ldg(tris + 3 * tri), b = __ldg(tris + 3 * tri + 1), c = __ldg(tris + 3 * tri + 2);
-    float3 p0 = xyz(a), e1 = xyz(b), e2 = xyz(c);
+    float3 p0 = xyz(a), e1 = xyz(b) - p0, e2 = xyz(c) - p0;
     float3 pv = cross3(rd, e2);
     det = dot3(e1, pv);
     if (!(fabsf(det) > 1e-12f)) return false;
@@ -55,6 +57,71 @@ __device__ __forceinline__ bool mt_hit(const float4* tris, uint32_t tri, float3 
 __device__ __forceinline__ bool side_ok(uint32_t bits, float det) {
     uint32_t side = bits & TB_SIDE_MASK;
     return side == 2u || (side == 0u && det > 0.0f) || (side == 1u && det < 0.0f);
+}
+
+// Watertight ray/triangle test (Woop, Benthin & Wald, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1), 2013): the vertices are translated to the ray
+// origin and sheared so the ray runs along +z of a permuted frame (kz = the
+// dominant axis of the direction, kx/ky swapped when it is negative to keep the
+// winding); the three 2D edge functions of the projected triangle decide the
+// hit. An edge shared by two triangles gets the same function value (negated)
+// in both, since it is formed from the same two sheared vertices with the same
+// separately rounded operations, so no ray passes between them; a value that
+// comes out exactly zero is formed again in double precision. det = U + V + W
+// has the sign of the Möller–Trumbore determinant (both are -dot(d, n) times a
+// positive factor), so the reference's side test applies unchanged; (u, v) are
+// the weights of vertices 1 and 2, as Möller–Trumbore's.
+__device__ __forceinline__ bool wt_hit(const float4* tris, uint32_t tri, float3 ro, float3 rd, float tmax, float& t,
+                                       float& det, float& u, float& v, uint32_t& bits) {
+    const float4 a = __ldg(tris + 3 * tri), b = __ldg(tris + 3 * tri + 1), c = __ldg(tris + 3 * tri + 2);
+    const float ax = fabsf(rd.x), ay = fabsf(rd.y), az = fabsf(rd.z);
+    int kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+    const float d[3] = {rd.x, rd.y, rd.z};
+    if (d[kz] < 0.0f) { const int tmp = kx; kx = ky; ky = tmp; }
+    const float Sz = __frcp_rn(d[kz]);
+    const float Sx = __fmul_rn(d[kx], Sz), Sy = __fmul_rn(d[ky], Sz);
+    const float o[3] = {ro.x, ro.y, ro.z};
+    const float A[3] = {__fsub_rn(a.x, o[0]), __fsub_rn(a.y, o[1]), __fsub_rn(a.z, o[2])};
+    const float B[3] = {__fsub_rn(b.x, o[0]), __fsub_rn(b.y, o[1]), __fsub_rn(b.z, o[2])};
+    const float C[3] = {__fsub_rn(c.x, o[0]), __fsub_rn(c.y, o[1]), __fsub_rn(c.z, o[2])};
+    const float Ax = __fsub_rn(A[kx], __fmul_rn(Sx, A[kz])), Ay = __fsub_rn(A[ky], __fmul_rn(Sy, A[kz]));
+    const float Bx = __fsub_rn(B[kx], __fmul_rn(Sx, B[kz])), By = __fsub_rn(B[ky], __fmul_rn(Sy, B[kz]));
+    const float Cx = __fsub_rn(C[kx], __fmul_rn(Sx, C[kz])), Cy = __fsub_rn(C[ky], __fmul_rn(Sy, C[kz]));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    det = U + V + W;
+    if (det == 0.0f) return false;
+    const float T = __fmul_rn(Sz, U * A[kz] + V * B[kz] + W * C[kz]);
+    const float inv = 1.0f / det;
+    t = T * inv;
+    u = V * inv;
+    v = W * inv;
+    bits = __float_as_uint(a.w);
+    return t > RAY_EPS && t < tmax;
+}
+
+// The triangle test of this build: the reference's Möller–Trumbore (the
+// parity default) or, built with SB_WATERTIGHT=1, the watertight test. A build
+// switch rather than a runtime one: both tests inlined side by side in the
+// traversal loops spill the closest-hit kernel's registers.
+#ifndef SB_WATERTIGHT
+#define SB_WATERTIGHT 0
+#endif
+__device__ __forceinline__ bool tri_hit(const DevScene& S, uint32_t tri, float3 ro, float3 rd, float tmax, float& t,
+                                        float& det, float& u, float& v, uint32_t& bits) {
+#if SB_WATERTIGHT
+    return wt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits);
+#else
+    return mt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits);
+#endif
 }
 
 // Both levels, one loop. ANY = traverseAny semantics (stop at the first
@@ -157,7 +224,7 @@ __device__ __forceinline__ bool walk(const DevScene& S, const uint4* tl, float3 
             float t, det, u, v;
             uint32_t bits;
             ++vis.tri;
-            if (!mt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
+            if (!tri_hit(S, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
             if (ANY) {
                 if ((bits & TB_SHADOW_OK) && side_ok(bits, det * dSign)) return true;
             } else if (side_ok(bits, det * dSign) && (bits & TB_CLOSEST_OK)) {
@@ -215,7 +282,7 @@ __device__ __forceinline__ bool blas_walk(const DevScene& S, uint32_t inst, floa
                     float t, det, u, v;
                     uint32_t bits;
                     ++vis.tri;
-                    if (!mt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
+                    if (!tri_hit(S, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
                     if (ANY) {
                         if ((bits & TB_SHADOW_OK) && side_ok(bits, det * dSign)) return true;
                     } else if (side_ok(bits, det * dSign) && (bits & TB_CLOSEST_OK)) {
@@ -233,7 +300,7 @@ __device__ __forceinline__ bool blas_walk(const DevScene& S, uint32_t inst, floa
                 float t, det, u, v;
                 uint32_t bits;
                 ++vis.tri;
-                if (!mt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
+                if (!tri_hit(S, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
                 if (ANY) {
                     if ((bits & TB_SHADOW_OK) && side_ok(bits, det * dSign)) return true;
                 } else if (side_ok(bits, det * dSign) && (bits & TB_CLOSEST_OK)) {
@@ -436,7 +503,7 @@ __device__ __forceinline__ bool pair_walk(const DevScene& S, const uint4* tp, fl
             float t, det, u, v;
             uint32_t bits;
             ++vis.tri;
-            if (!mt_hit(S.tris, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
+            if (!tri_hit(S, tri, ro, rd, tmax, t, det, u, v, bits)) continue;
             if (ANY) {
                 if ((bits & TB_SHADOW_OK) && side_ok(bits, det * dSign)) return true;
             } else if (side_ok(bits, det * dSign) && (bits & TB_CLOSEST_OK)) {
@@ -575,7 +642,7 @@ __device__ __forceinline__ bool flat_walk(const DevScene& S, float3 wro, float3 
             float t, det, u, v;
             uint32_t bits;
             ++vis.tri;
-            if (!mt_hit(S.tris, tri, lro, lrd, tmax, t, det, u, v, bits)) continue;
+            if (!tri_hit(S, tri, lro, lrd, tmax, t, det, u, v, bits)) continue;
             if (ANY) {
                 if ((bits & TB_SHADOW_OK) && side_ok(bits, det * dSign)) return true;
             } else if (side_ok(bits, det * dSign) && (bits & TB_CLOSEST_OK)) {
@@ -792,7 +859,7 @@ __device__ __forceinline__ bool wide_items(const DevScene& S, uint32_t tBase, ui
         float t, det, u, v;
         uint32_t hb;
         ++vis.tri;
-        if (!mt_hit(S.tris, tri, lro, lrd, tmax, t, det, u, v, hb)) continue;
+        if (!tri_hit(S, tri, lro, lrd, tmax, t, det, u, v, hb)) continue;
         if (ANY) {
             if ((hb & TB_SHADOW_OK) && side_ok(hb, det * dSign)) return true;
         } else if (side_ok(hb, det * dSign) && (hb & TB_CLOSEST_OK)) {

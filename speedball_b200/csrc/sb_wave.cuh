@@ -30,8 +30,8 @@ struct HitFrame {
 // hit position (gi_probes.js:2003-2017).
 __device__ __forceinline__ HitFrame hit_frame(const WaveCtx& W, uint32_t tri, uint32_t inst, float3 ro, float3 rd,
                                               float t, int facing) {
-    float4 b = __ldg(W.S.tris + 3 * tri + 1), c = __ldg(W.S.tris + 3 * tri + 2);
-    float3 nl = normalize3(cross3(xyz(b), xyz(c)));
+    float4 a = __ldg(W.S.tris + 3 * tri), b = __ldg(W.S.tris + 3 * tri + 1), c = __ldg(W.S.tris + 3 * tri + 2);
+    float3 nl = normalize3(cross3(xyz(b) - xyz(a), xyz(c) - xyz(a)));
     float4 r0 = __ldg(W.S.inst + 4 * inst), r1 = __ldg(W.S.inst + 4 * inst + 1), r2 = __ldg(W.S.inst + 4 * inst + 2);
     float3 ngRaw = normalize3(xyz(r0) * nl.x + xyz(r1) * nl.y + xyz(r2) * nl.z);
     HitFrame f;

@@ -97,8 +97,8 @@ class ProbeField:
 
     def __init__(self, scene: SceneDesc, *, intensity=1.0, hysteresis=None, jitterMode="gated", divisions=12,
                  rays=RAYS_PER_PROBE_DEFAULT, cascades=2, clusteredLighting=False, volumes=None, device=0,
-                 recordHits=False, onRebuilt: Callable | None = None):
-        self._lib = _abi.load()
+                 recordHits=False, onRebuilt: Callable | None = None, variant: str | None = None):
+        self._lib = _abi.load(variant)
         self._scene = scene
         self._intensity = float(intensity)
         self._jitterMode = _normalize_jitter_mode(jitterMode)
