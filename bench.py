@@ -47,13 +47,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch", "large"], default="atrium",
+    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch", "large", "gather"], default="atrium",
                     help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
                          "differentiated update (64 materials, 32 point lights, 2 feedback solves); batch: 3 "
                          "nested cascades of the atrium + 8 independent atria per frame, batched vs plain; "
                          "large: 2.1M unique / 12.8M instanced triangles, 32^3 probes x 256 rays x 2 cascades, "
                          "binary vs 8-wide scene BVH vs the reference two-level walk")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-aux", action="store_true",
+                    help="atrium only: skip the batched-form and adjoint measurements added to the line")
     return ap.parse_args()
 
 
@@ -745,6 +747,151 @@ def run_batch(args, dist: Dist):
     return line
 
 
+GATHER_METRIC = "receiver gather Msamples/s (1920x1080 G-buffer)"
+
+
+def camera_gbuffer(f, scene, width=1920, height=1080):
+    """A deferred G-buffer of the atrium from a pinhole camera at the probe
+    grid's centre looking along +x (90 degree horizontal field of view): per
+    covered pixel the hit position and the geometric world normal facing the
+    camera (sky pixels dropped, as a deferred pass skips them). float4 rows."""
+    from speedball_b200 import _abi
+    g = scene.meta["grid"]
+    c = np.asarray(g["gridMin"], np.float64) + 0.5 * np.asarray(g["gridSize"], np.float64)
+    xs = (np.arange(width) + 0.5) / width * 2 - 1
+    ys = ((np.arange(height) + 0.5) / height * 2 - 1) * height / width
+    X, Y = np.meshgrid(xs, ys)
+    d = np.stack([np.ones_like(X), -Y, X], -1).reshape(-1, 3)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    n = d.shape[0]
+    ro = np.ascontiguousarray(np.broadcast_to(c, (n, 3)), np.float32)
+    rd = np.ascontiguousarray(d, np.float32)
+    t = np.zeros(n, np.float32)
+    tri = np.zeros(n, np.int32)
+    slot = np.zeros(n, np.int32)
+    _abi.check(f._lib.sb_raycast(f.ctx, _abi.ptr(ro), _abi.ptr(rd), n, _abi.ptr(t), _abi.ptr(tri), _abi.ptr(slot)),
+               f.ctx)
+    hit = tri >= 0
+    pool = f.pool
+    order = np.zeros(pool.instCount, np.uint32)
+    _abi.check(f._lib.sb_read_buffer(f.ctx, _abi.BUF["TLAS_ORDER"], 0, pool.instCount, _abi.ptr(order)), f.ctx)
+    src = order[slot[hit]]
+    idx = pool.triIndex[tri[hit]]
+    v = pool.vertexData[:, 0:3].astype(np.float64)
+    p0, p1, p2 = v[idx[:, 0]], v[idx[:, 1]], v[idx[:, 2]]
+    nl = np.cross(p1 - p0, p2 - p0)
+    W = np.stack([scene.instances[i].world for i in range(pool.instCount)])[src]
+    Minv = np.linalg.inv(W[:, :3, :3])
+    nw = np.einsum("nji,nj->ni", Minv, nl)  # (M^-1)^T n
+    nw /= np.linalg.norm(nw, axis=1, keepdims=True)
+    dh = d[hit]
+    nw *= np.where(np.einsum("ni,ni->n", nw, dh) > 0, -1.0, 1.0)[:, None]
+    m = int(hit.sum())
+    pos = np.zeros((m, 4), np.float32)
+    pos[:, :3] = ro[hit] + rd[hit] * t[hit, None]
+    nrm = np.zeros((m, 4), np.float32)
+    nrm[:, :3] = nw
+    return pos, nrm
+
+
+def run_gather(args, dist: Dist):
+    """One step = one receiver gather of a 1920x1080 deferred G-buffer of the
+    atrium (covered pixels) from the atlases of 4 updates: position, stable
+    normal and detail normal in (48 B per sample), irradiance out (16 B).
+    value = samples / device time; e2e = the same through host buffers
+    (G-buffer up, irradiance down, page-locked)."""
+    from speedball_b200 import _abi
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    scene = make_workload()
+    f = field_for(scene, device)
+    for _ in range(4):
+        f.tick()
+    f.synchronize()
+    pos, nrm = camera_gbuffer(f, scene)
+    n = pos.shape[0]
+    lib, ctx = f._lib, f.ctx
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
+    flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
+    bufs = [ck(rt.cudaMalloc(n * 16)) for _ in range(4)]  # position, stable normal, detail normal, out
+    for b, a in zip(bufs[:3], (pos, nrm, nrm)):
+        ck(rt.cudaMemcpy(b, a.ctypes.data, n * 16, rt.cudaMemcpyKind.cudaMemcpyHostToDevice))
+    prm = _abi.sb_gather_params()
+    lib.sb_gather_params_defaults(C.byref(prm))
+    prm.normalBias[0] = max(1e-4, f.grid.cellMin * 0.04)
+
+    def gather():
+        _abi.check(lib.sb_gather_irradiance(ctx, C.byref(prm), C.c_void_p(int(bufs[0])), C.c_void_p(int(bufs[1])),
+                                            C.c_void_p(int(bufs[2])), n, C.c_void_p(int(bufs[3]))), ctx)
+
+    e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
+    W, K = args.warmup, args.steps
+    for i in range(W):
+        ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+        gather()
+    ck(rt.cudaStreamSynchronize(stream))
+    dist.barrier()
+    clocks = Clocks(device)
+    clocks.start()
+    total = 0.0
+    for i in range(K):
+        ck(rt.cudaMemsetAsync(flush, i & 0xFF, L2_FLUSH_BYTES, stream))
+        ck(rt.cudaEventRecord(e0, stream))
+        gather()
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        total += ck(rt.cudaEventElapsedTime(e0, e1))
+    ms = dist.max(total / K)
+    # end to end: page-locked G-buffer up, gather, irradiance down
+    hp = [_abi.PinnedArray((n, 4), np.float32) for _ in range(4)]
+    hp[0].array[...] = pos
+    hp[1].array[...] = nrm
+    hp[2].array[...] = nrm
+    H2D, D2H = rt.cudaMemcpyKind.cudaMemcpyHostToDevice, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost
+    e2e = 0.0
+    for i in range(W + K):
+        ck(rt.cudaStreamSynchronize(stream))
+        t0 = time.perf_counter()
+        for b, h in zip(bufs[:3], hp[:3]):
+            ck(rt.cudaMemcpyAsync(b, h.array.ctypes.data, n * 16, H2D, stream))
+        gather()
+        ck(rt.cudaMemcpyAsync(hp[3].array.ctypes.data, bufs[3], n * 16, D2H, stream))
+        ck(rt.cudaStreamSynchronize(stream))
+        if i >= W:
+            e2e += time.perf_counter() - t0
+    e2e_ms = dist.max(e2e / K * 1e3)
+    clk = clocks.stop()
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = 64.0 * n / (ms * 1e-3) / 1e9
+    out = hp[3].array
+    line = {
+        "metric": GATHER_METRIC, "value": round(dist.world * n / (ms * 1e-3) / 1e6, 2), "unit": "Msamples/s",
+        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(ms, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (RGBA16F atlases)",
+        "data": "synthetic (seeded procedural atrium, atlases of 4 updates)",
+        "config": {"workload": "receiver gather of a 1920x1080 deferred G-buffer of the atrium (covered pixels), "
+                               "16^3 probes, default receiver uniforms (8-tap trilinear)", "samples": n,
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "e2e": {"value": round(dist.world * n / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Msamples/s",
+                "ms_per_step": round(e2e_ms, 4), "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 16 * n},
+        "gpu_launches": K,
+        "roofline": {"bound": "hbm", "kernel": "k_gather", "achieved": round(achieved, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "algorithmic_bytes_per_launch": 64 * n,
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s"},
+        "irradiance_mean": [round(float(x), 5) for x in out[:, :3].mean(0)],
+        "clocks": clk,
+    }
+    for b in bufs:
+        ck(rt.cudaFree(b))
+    ck(rt.cudaFree(flush))
+    f.dispose()
+    return line
+
+
 LARGE_METRIC = "probe Mrays/s (large scene, 2 cascades)"
 
 
@@ -866,6 +1013,34 @@ def run_large(args, dist: Dist):
     return line
 
 
+def aux_measurements(args, dist: Dist) -> dict:
+    """The batched form's and the adjoint's ratios, measured in the same run
+    as the headline (each its own workload, set-up outside its timed region):
+    `batch` = the 9-scene batched frame against the same frame as per-solve
+    launches (target >= 3x), `adjoint` = backward / forward-record device time
+    (target <= 3x)."""
+    import types
+    sub = types.SimpleNamespace(**vars(args))
+    sub.steps = min(args.steps, 50)
+    sub.warmup = max(3, min(args.warmup, 5))
+    sub.no_cpu_baseline = True
+    out = {}
+    b = run_batch(sub, dist)
+    out["batch"] = {k: b[k] for k in ("metric", "value", "unit", "ms_per_step", "plain_value", "plain_ms_per_step",
+                                      "batched_no_graph_ms_per_step", "batched_over_plain", "gpu_launches",
+                                      "clocks")}
+    out["batch"]["steps"], out["batch"]["warmup"] = sub.steps, sub.warmup
+    out["batch"]["workload"] = b["config"]["workload"]
+    a = run_adjoint(sub, dist)
+    out["adjoint"] = {k: a[k] for k in ("metric", "value", "unit", "ms_per_step", "forward_record_ms", "backward_ms",
+                                        "plain_forward_ms", "backward_over_plain_forward", "gpu_launches", "clocks")}
+    out["adjoint"]["steps"], out["adjoint"]["warmup"] = sub.steps, sub.warmup
+    out["adjoint"]["workload"] = a["config"]["workload"]
+    out["batch_over_plain"] = b["batched_over_plain"]
+    out["adjoint_over_forward"] = a["value"]
+    return out
+
+
 def main():
     args = parse()
     dist = Dist(args.gpus)
@@ -876,11 +1051,16 @@ def main():
         elif args.workload == "batch":
             line = run_batch(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference has no batched multi-scene form"}
+        elif args.workload == "gather":
+            line = run_gather(args, dist) if args.impl == "ours" else \
+                {"impl": "reference", "unavailable": "the reference's gather is a WebGPU fragment shader"}
         elif args.workload == "adjoint":
             line = run_adjoint(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference has no adjoint of the probe update"}
         else:
             line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+            if args.impl == "ours" and dist.world == 1 and not args.no_aux:
+                line.update(aux_measurements(args, dist))
         if dist.rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
     finally:

@@ -235,6 +235,15 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
 sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist,
                       uint32_t n, uint8_t* blockedOut);
 
+/* The FP32 probe rays of a solve of `cascade` over probes [probeOffset,
+ * probeOffset + updatedCount) (mod the probe count) with the current
+ * sb_params, exactly as the trace forms them (gi_probes.js:1977-1987): host
+ * arrays of updatedCount * raysPerProbe * 3 floats, ray slot * rays + k. A
+ * read-back seam for checks (the reference's _debugRead, 4830-4841).
+ * Synchronizes. */
+sb_status sb_probe_rays(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount, float* roOut,
+                        float* rdOut);
+
 /* ------------------------------------------------------- receiver gather */
 
 /* The receiver's uniforms (GiProbeNode, gi_probes.js:306-358). */

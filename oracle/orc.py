@@ -85,6 +85,7 @@ def load() -> C.CDLL:
             "orc_explain_hits": (None, [P, P, P, U, P, P, P, P, P, P, P, C.c_int32]),
             "orc_gather": (None, [P, P, P, P, P, P, P, P, P, P, U, P, P, C.c_int32]),
             "orc_gather_params_size": (U, []),
+            "orc_pair_t": (None, [P, P, P, U, P, P, P, C.c_int32]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
@@ -282,6 +283,16 @@ def explain_hits(scene: OrcScene, ro: np.ndarray, rd: np.ndarray, g_tri, g_inst,
     load().orc_explain_hits(C.byref(scene), _p(ro), _p(rd), n, *[_p(a) for a in arrs], _p(ot), _p(code), _p(gt),
                             threads())
     return code, gt
+
+
+def pair_t(scene: OrcScene, ro: np.ndarray, rd: np.ndarray, tri, inst) -> np.ndarray:
+    """FP64 t of each ray's (tri, inst) pair on that ray (-1 without a pair)."""
+    n = ro.shape[0]
+    out = np.zeros(n, np.float64)
+    load().orc_pair_t(C.byref(scene), _p(np.ascontiguousarray(ro, np.float64)), _p(np.ascontiguousarray(rd, np.float64)),
+                      n, _p(np.ascontiguousarray(tri, np.int32)), _p(np.ascontiguousarray(inst, np.int32)), _p(out),
+                      threads())
+    return out
 
 
 # ----------------------------------------------------- per-tick scheduling

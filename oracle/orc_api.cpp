@@ -180,6 +180,20 @@ void orc_probe_rays(const OrcGrid* gp, double jitter, uint32_t probeOffset, uint
     }
 }
 
+// FP64 t of the pair (tri[i], inst[i]) on ray i (-1 where there is no pair or
+// the Möller–Trumbore determinant vanishes): the exact ray parameter of a
+// reported hit, for checking the reported t on the ray that was traced.
+void orc_pair_t(const OrcScene* s, const double* ro, const double* rd, uint32_t n, const int32_t* tri,
+                const int32_t* inst, double* tOut, int32_t threads) {
+    Scene sc = to_scene(s);
+    parallel_for(n, threads, [&](size_t i, int) {
+        Traverser<double> tr(sc);
+        V3<double> o(ro[i * 3], ro[i * 3 + 1], ro[i * 3 + 2]), d(rd[i * 3], rd[i * 3 + 1], rd[i * 3 + 2]);
+        PairEval e = eval_pair(tr, sc, tri[i], inst[i], o, d);
+        tOut[i] = e.valid && e.t != 0.0 ? e.t : -1.0;
+    });
+}
+
 // Classifies every ray whose GPU closest hit (gTri, gInst) differs from the FP64
 // oracle's (oTri, oInst, oT). Codes:
 //   0 same pair;

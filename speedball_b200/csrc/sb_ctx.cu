@@ -1538,6 +1538,29 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
     return sb_synchronize(ctx);
 }
 
+sb_status sb_probe_rays(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount, float* roOut,
+                        float* rdOut) {
+    if (!ctx || (updatedCount && (!roOut || !rdOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (cascade >= SB_MAX_CASCADES || !ctx->casc[cascade].configured)
+        return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", cascade);
+    const Cascade& K = ctx->casc[cascade];
+    if (updatedCount > K.probeTotal || probeOffset >= K.probeTotal)
+        return fail(ctx, SB_ERR_INVALID_ARG, "probe range outside the cascade");
+    if (updatedCount == 0) return SB_OK;
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)updatedCount * K.grid.raysPerProbe;
+    float *dro = nullptr, *drd = nullptr;
+    CK(cudaMallocAsync(&dro, n * 12, ctx->stream));
+    CK(cudaMallocAsync(&drd, n * 12, ctx->stream));
+    CK(launch_probe_rays(dev_cascade(ctx, cascade, probeOffset, updatedCount), ctx->params.frameJitter, dro, drd,
+                         ctx->stream));
+    CK(cudaMemcpyAsync(roOut, dro, n * 12, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(rdOut, drd, n * 12, cudaMemcpyDeviceToHost, ctx->stream));
+    cudaFreeAsync(dro, ctx->stream);
+    cudaFreeAsync(drd, ctx->stream);
+    return sb_synchronize(ctx);
+}
+
 void sb_gather_params_defaults(sb_gather_params* p) {
     if (!p) return;
     std::memset(p, 0, sizeof *p);

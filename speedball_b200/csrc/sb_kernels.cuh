@@ -158,6 +158,8 @@ struct GatherArgs {
     float4* out;
 };
 cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st);
+// The FP32 probe rays of a solve as the trace forms them (sb_probe_rays).
+cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st);
 
 // Arbitrary-ray queries through the same traversal (raycastFirst-like).
 cudaError_t launch_raycast(const DevScene& S, const float* ro, const float* rd, uint32_t n, float* tOut,

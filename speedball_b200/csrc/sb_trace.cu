@@ -689,4 +689,25 @@ cudaError_t launch_occluded(const DevScene& S, const float* ro, const float* rd,
 
 }  // namespace sb
 
+namespace sb {
+// The probe rays of a solve exactly as the trace stage forms them (probe
+// origin and ray_dir with the current frame jitter): ray slot * rays + k.
+__global__ void k_probe_rays(const DevCascade C, float jitter, float* ro, float* rd) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.updatedCount * C.rays) return;
+    const uint32_t slot = i / C.rays, k = i % C.rays;
+    const float3 o = probe_world_pos(C, (C.probeOffset + slot) % C.probeTotal);
+    const float3 d = ray_dir(k, C.rays, jitter);
+    ro[3 * i] = o.x; ro[3 * i + 1] = o.y; ro[3 * i + 2] = o.z;
+    rd[3 * i] = d.x; rd[3 * i + 1] = d.y; rd[3 * i + 2] = d.z;
+}
+cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st) {
+    const uint32_t n = C.updatedCount * C.rays;
+    if (n == 0) return cudaSuccess;
+    k_probe_rays<<<(n + 255) / 256, 256, 0, st>>>(C, jitter, ro, rd);
+    note_launch();
+    return cudaGetLastError();
+}
+}  // namespace sb
+
 extern "C" uint32_t sb_triangle_test(void) { return SB_WATERTIGHT ? 1u : 0u; }

@@ -117,33 +117,47 @@ def texel_rel_err(g: np.ndarray, o: np.ndarray) -> np.ndarray:
     return np.abs(g - o) / np.maximum(np.abs(o), floor)
 
 
-def check_hits(scene: orc.OrcScene, ro: np.ndarray, rd: np.ndarray, g_tri, g_inst, g_t, o_tri, o_inst, o_t) -> dict:
+def check_hits(scene: orc.OrcScene, ro: np.ndarray, rd: np.ndarray, g_tri, g_inst, g_t, o_tri, o_inst, o_t,
+               g_ro: np.ndarray | None = None, g_rd: np.ndarray | None = None) -> dict:
     """Hit-ID parity at the near-tie bar: every ray whose GPU closest hit
-    differs from the FP64 oracle's must be explained, ray by ray, by the oracle
-    (orc.explain_hits: a near-tie within 1e-6 relative, an edge graze within
-    the FP32 rounding bound of that triangle's barycentric test, or a t order
-    within the FP32 bound of the two t); no share of rays is waived. Hit t of
-    the GPU is within 1e-5 relative of the FP64 t of the pair it reports.
-    Returns the count of rays per code."""
+    differs from the FP64 oracle's on ray (ro, rd) must be explained, ray by
+    ray, by the oracle (orc.explain_hits: a near-tie within 1e-6 relative, an
+    edge graze within the FP32 rounding bound of that triangle's barycentric
+    test, or a t order within the FP32 bound of the two t); no share of rays is
+    waived. Hit t: the GPU's t is within 1e-5 relative of the FP64 t of the
+    pair it reports, on the ray it traced ((g_ro, g_rd), the FP32 ray, when
+    given; else (ro, rd)). Returns the count of rays per code, and the largest
+    relative t difference against the FP64 ray as well."""
     code, gt = orc.explain_hits(scene, ro, rd, g_tri, g_inst, o_tri, o_inst, o_t)
     counts = {orc.HIT_CODES[k]: int(v) for k, v in enumerate(np.bincount(code, minlength=6))}
     bad = np.flatnonzero(code == 5)
     assert bad.size == 0, (counts, [(int(i), int(g_tri[i]), int(o_tri[i]), float(g_t[i]), float(o_t[i]), float(gt[i]))
                                     for i in bad[:6]])
     g_hit = np.asarray(g_tri) >= 0
-    same = (code == 0) & g_hit
-    o_t = np.asarray(o_t, np.float64)
     g_t = np.asarray(g_t, np.float64)
-    rel_max = 0.0
-    if same.any():
-        rel = np.abs(g_t[same] - o_t[same]) / o_t[same]
-        rel_max = float(rel.max())
-        assert rel_max <= T_REL, rel_max
-    other = (code != 0) & g_hit & (gt > 0)
-    if other.any():
-        rel2 = np.abs(g_t[other] - gt[other]) / gt[other]
-        assert rel2.max() <= T_REL, rel2.max()
-    counts["t_rel_max"] = rel_max
+    if g_ro is not None:
+        tt = orc.pair_t(scene, g_ro.astype(np.float64), g_rd.astype(np.float64), g_tri, g_inst)
+    else:
+        tt = orc.pair_t(scene, ro, rd, g_tri, g_inst)
+    ok = g_hit & (tt > 0)
+    assert ok.sum() == g_hit.sum(), (int(g_hit.sum()), int(ok.sum()))
+    rel = np.abs(g_t[ok] - tt[ok]) / tt[ok]
+    counts["t_rel_max"] = float(rel.max()) if rel.size else 0.0
+    assert counts["t_rel_max"] <= T_REL, counts["t_rel_max"]
+    if g_ro is not None:
+        # the FP32 ray against the FP64 one, and what that rounding does to t
+        t64 = orc.pair_t(scene, ro, rd, g_tri, g_inst)
+        both = ok & (t64 > 0)
+        counts["t_rel_max_vs_fp64_ray"] = float((np.abs(g_t[both] - t64[both]) / t64[both]).max()) if both.any() else 0.0
+        counts["t_rel_gt_1e-5_vs_fp64_ray"] = int((np.abs(g_t[both] - t64[both]) > T_REL * t64[both]).sum())
+        dang = np.linalg.norm(g_rd.astype(np.float64) / np.linalg.norm(g_rd.astype(np.float64), axis=1, keepdims=True)
+                              - rd, axis=1)
+        counts["ray_dir_err_max_rad"] = float(dang.max())
+        assert dang.max() <= 4e-7, dang.max()
+        # FP32 probe origins: a few roundings at the scale of the grid's coordinates
+        dorg = np.abs(g_ro.astype(np.float64) - ro).max(axis=1) / max(float(np.abs(ro).max()), 1.0)
+        counts["ray_origin_rel_err_max"] = float(dorg.max())
+        assert dorg.max() <= 4e-7, dorg.max()
     return counts
 
 
@@ -198,6 +212,15 @@ class SceneTail:
             assert np.array_equal(got.view(np.uint32), arr.view(np.uint32)), key
 
 
+def gpu_probe_rays(f: ProbeField, offset: int, updated: int, cascade: int = 0):
+    """The FP32 probe rays the GPU traced for a solve (sb_probe_rays)."""
+    n = updated * f.getRays()
+    ro = np.zeros((n, 3), np.float32)
+    rd = np.zeros((n, 3), np.float32)
+    _abi.check(f._lib.sb_probe_rays(f.ctx, cascade, offset, updated, _abi.ptr(ro), _abi.ptr(rd)), f.ctx)
+    return ro, rd
+
+
 def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params: np.ndarray) -> dict:
     """After the GPU tick `frame`: independent FP64 solve (hit IDs and t of every
     ray of the solve), then the oracle's replay of the GPU's hit and shadow
@@ -209,8 +232,9 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
     ind = mirror.solve(off, upd, replay=None, params=sched_params)
     mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = saved
     ro, rd = orc.probe_rays(mirror.grid, sched_params[0], off, upd)
+    g_ro, g_rd = gpu_probe_rays(f, off, upd)
     counts = check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], ind["tri"], ind["inst"],
-                        ind["rays"][3::4])
+                        ind["rays"][3::4], g_ro, g_rd)
     mirror.solve(off, upd, replay=rec, params=sched_params)
     ga = half_to_f(read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16))
     oa = half_to_f(mirror.atlas.reshape(-1))

@@ -101,8 +101,9 @@ def test_solve_parity_room_four_solves(room):
             out_ind = mirror.solve(0, P, replay=None)
             mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = mirror_state
             ro, rd = orc.probe_rays(mirror.grid, 0.0, 0, P)
+            g_ro, g_rd = gu.gpu_probe_rays(f, 0, P)
             gu.check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], out_ind["tri"], out_ind["inst"],
-                          out_ind["rays"][3::4])
+                          out_ind["rays"][3::4], g_ro, g_rd)
             mirror.solve(0, P, replay=rec)
             ga = gu.half_to_f(gu.read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16))
             oa = gu.half_to_f(mirror.atlas.reshape(-1))
