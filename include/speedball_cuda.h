@@ -244,6 +244,33 @@ sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float
 sb_status sb_probe_rays(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount, float* roOut,
                         float* rdOut);
 
+/* ---------------------------------------------------- BLAS build (GPU) */
+
+/* BLAS build on the GPU, replacing the CPU MeshBVH build + flattenBVHRoot of
+ * each mesh (spectral_scene.js:898-966, 658-721): a linear BVH over the
+ * triangles' bounds centres (30-bit Morton codes, stable radix sort, binary
+ * radix tree), collapsed to leaves of at most `leafSize` (1..255) triangles,
+ * emitted in the reference's threaded layout: 8 x u32 per node, pre-order
+ * with the left child at i+1, miss = first node after the subtree, payload
+ * (count << 24 | first position) or 0xFFFFFFFF; node bounds are the exact
+ * min/max of their triangles' vertices (what a refit gives). triOrderOut[i] =
+ * the source triangle at BVH position i; miss links and leaf offsets are
+ * relative to this BLAS, as sbh_build_blas's. The tree differs from MeshBVH's
+ * (LBVH instead of CENTER splits); closest hits are the same up to exact-t
+ * ties, as for any valid BVH.
+ * sb_build_blas_device: positions (vertexCount x 3 f32) and indices (triCount x
+ * 3 u32) are device arrays; nodesOut (2 * triCount x 8 u32), triOrderOut and
+ * nodeCountOut (1 u32) device outputs; enqueued on the context's stream, an
+ * out-of-range index is reported by sb_synchronize (SB_ERR_LAYOUT_VIOLATION).
+ * sb_build_blas_gpu: the same with host arrays in and out (index range
+ * checked first); synchronizes. */
+sb_status sb_build_blas_device(sb_ctx* ctx, const float* positions, uint32_t vertexCount, const uint32_t* indices,
+                               uint32_t triCount, uint32_t leafSize, uint32_t* nodesOut, uint32_t* triOrderOut,
+                               uint32_t* nodeCountOut);
+sb_status sb_build_blas_gpu(sb_ctx* ctx, const float* pos3, uint32_t vertexCount, const uint32_t* index3,
+                            uint32_t triCount, uint32_t leafSize, uint32_t* nodesOut, uint32_t* triOrderOut,
+                            uint32_t* nodeCountOut);
+
 /* ------------------------------------------------------- receiver gather */
 
 /* The receiver's uniforms (GiProbeNode, gi_probes.js:306-358). */

@@ -144,6 +144,8 @@ SIGNATURES = {
     "sb_set_stream": (C.c_int, [_P, _P]),
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
     "sb_triangle_test": (C.c_uint32, []),
+    "sb_build_blas_device": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "sb_build_blas_gpu": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_probe_rays": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
     "sb_gather_params_defaults": (None, [_P]),
     "sb_gather_irradiance": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),

@@ -51,6 +51,7 @@ struct sb_ctx {
     int device = 0;
     uint32_t flags = 0;
     uint32_t walkStepLimit = 0;  // sb_set_walk_step_limit (0 = the defaults)
+    BlasBuilder* builder = nullptr;  // GPU BLAS build scratch (sb_build_blas_*)
     cudaStream_t stream = nullptr;
     cudaStream_t ownStream = nullptr;
     std::string err;
@@ -422,6 +423,10 @@ void sb_destroy(sb_ctx* ctx) {
     release(B.lights); release(B.lightGates); release(B.tris); release(B.inst); release(B.tlas); release(B.matBits); release(B.parent);
     release(B.arrive); release(B.subRoots); release(B.valid); release(B.pairs); release(B.tlasPairs); release(B.depth);
     ctx->flat.release();
+    if (ctx->builder) {
+        blas_builder_destroy(ctx->builder);
+        ctx->builder = nullptr;
+    }
     InstanceTable& I = ctx->I;
     release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb); release(I.invRows);
     release(I.detSign); release(I.order); release(I.slotOf); release(I.liveBounds); release(I.nodeDepth);
@@ -1558,6 +1563,57 @@ sb_status sb_probe_rays(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uin
     CK(cudaMemcpyAsync(rdOut, drd, n * 12, cudaMemcpyDeviceToHost, ctx->stream));
     cudaFreeAsync(dro, ctx->stream);
     cudaFreeAsync(drd, ctx->stream);
+    return sb_synchronize(ctx);
+}
+
+sb_status sb_build_blas_device(sb_ctx* ctx, const float* positions, uint32_t vertexCount, const uint32_t* indices,
+                               uint32_t triCount, uint32_t leafSize, uint32_t* nodesOut, uint32_t* triOrderOut,
+                               uint32_t* nodeCountOut) {
+    if (!ctx || !positions || !indices || !nodesOut || !triOrderOut || !nodeCountOut)
+        return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (triCount == 0 || vertexCount == 0) return fail(ctx, SB_ERR_INVALID_ARG, "empty mesh");
+    if (leafSize == 0 || leafSize > 255) return fail(ctx, SB_ERR_INVALID_ARG, "leaf size %u: 1..255", leafSize);
+    if (triCount >= (1u << 24)) return fail(ctx, SB_ERR_INVALID_ARG, "%u triangles: the leaf offset has 24 bits", triCount);
+    cudaSetDevice(ctx->device);
+    if (!ctx->builder) ctx->builder = blas_builder_create();
+    CK(blas_build(ctx->builder, positions, vertexCount, indices, triCount, leafSize, nodesOut, triOrderOut,
+                  nodeCountOut, ctx->dErr, ctx->stream));
+    return SB_OK;
+}
+
+sb_status sb_build_blas_gpu(sb_ctx* ctx, const float* pos3, uint32_t vertexCount, const uint32_t* index3,
+                            uint32_t triCount, uint32_t leafSize, uint32_t* nodesOut, uint32_t* triOrderOut,
+                            uint32_t* nodeCountOut) {
+    if (!ctx || !pos3 || !index3 || !nodesOut || !triOrderOut || !nodeCountOut)
+        return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (triCount == 0 || vertexCount == 0) return fail(ctx, SB_ERR_INVALID_ARG, "empty mesh");
+    for (size_t i = 0; i < (size_t)triCount * 3; ++i)
+        if (index3[i] >= vertexCount) return fail(ctx, SB_ERR_INVALID_ARG, "triangle %zu: vertex index out of range", i / 3);
+    cudaSetDevice(ctx->device);
+    float* dp = nullptr;
+    uint32_t *di = nullptr, *dn = nullptr, *dord = nullptr, *dc = nullptr;
+    CK(cudaMallocAsync(&dp, (size_t)vertexCount * 12, ctx->stream));
+    CK(cudaMallocAsync(&di, (size_t)triCount * 12, ctx->stream));
+    CK(cudaMallocAsync(&dn, (size_t)triCount * 64, ctx->stream));
+    CK(cudaMallocAsync(&dord, (size_t)triCount * 4, ctx->stream));
+    CK(cudaMallocAsync(&dc, 4, ctx->stream));
+    CK(cudaMemcpyAsync(dp, pos3, (size_t)vertexCount * 12, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(di, index3, (size_t)triCount * 12, cudaMemcpyHostToDevice, ctx->stream));
+    sb_status s = sb_build_blas_device(ctx, dp, vertexCount, di, triCount, leafSize, dn, dord, dc);
+    uint32_t count = 0;
+    if (s == SB_OK) {
+        CK(cudaMemcpyAsync(&count, dc, 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (count == 0 || count > 2 * triCount) s = fail(ctx, SB_ERR_CUDA, "BLAS build produced %u nodes", count);
+    }
+    if (s == SB_OK) {
+        CK(cudaMemcpyAsync(nodesOut, dn, (size_t)count * 32, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(triOrderOut, dord, (size_t)triCount * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        *nodeCountOut = count;
+    }
+    cudaFreeAsync(dp, ctx->stream); cudaFreeAsync(di, ctx->stream); cudaFreeAsync(dn, ctx->stream);
+    cudaFreeAsync(dord, ctx->stream); cudaFreeAsync(dc, ctx->stream);
+    if (s != SB_OK) return s;
     return sb_synchronize(ctx);
 }
 

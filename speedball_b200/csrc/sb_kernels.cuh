@@ -158,6 +158,15 @@ struct GatherArgs {
     float4* out;
 };
 cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st);
+// GPU BLAS build in the threaded layout (sb_build.cu); device scratch lives in
+// the builder and grows to the largest mesh built. Out-of-range vertex indices
+// latch ERR_LAYOUT.
+struct BlasBuilder;
+BlasBuilder* blas_builder_create();
+void blas_builder_destroy(BlasBuilder* b);
+cudaError_t blas_build(BlasBuilder* b, const float* pos, uint32_t V, const uint32_t* idx, uint32_t T,
+                       uint32_t leafSize, uint32_t* nodes, uint32_t* order, uint32_t* nodeCount, uint32_t* err,
+                       cudaStream_t st);
 // The FP32 probe rays of a solve as the trace forms them (sb_probe_rays).
 cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st);
 

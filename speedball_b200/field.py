@@ -97,8 +97,12 @@ class ProbeField:
 
     def __init__(self, scene: SceneDesc, *, intensity=1.0, hysteresis=None, jitterMode="gated", divisions=12,
                  rays=RAYS_PER_PROBE_DEFAULT, cascades=2, clusteredLighting=False, volumes=None, device=0,
-                 recordHits=False, onRebuilt: Callable | None = None, variant: str | None = None):
+                 recordHits=False, onRebuilt: Callable | None = None, variant: str | None = None,
+                 blasBuilder: str = "host"):
         self._lib = _abi.load(variant)
+        if blasBuilder not in ("host", "gpu"):
+            raise ValueError("blasBuilder: 'host' or 'gpu'")
+        self._blasBuilder = blasBuilder
         self._scene = scene
         self._intensity = float(intensity)
         self._jitterMode = _normalize_jitter_mode(jitterMode)
@@ -146,7 +150,7 @@ class ProbeField:
     def _rebuild(self):
         """rebuild() (gi_probes.js:3269-3455): pool, upload, TLAS, grid fit, lights."""
         lib = self._lib
-        self._pool = pool = build_pool(self._scene)
+        self._pool = pool = build_pool(self._scene, self._ctx if self._blasBuilder == "gpu" else None, lib)
         self._ck(lib.sb_upload_scene(self._ctx, C.byref(pool.view())))
         self._ck(lib.sb_set_instances(self._ctx, pool.instCount, _abi.ptr(pool.inst_world),
                                       _abi.ptr(pool.inst_active), _abi.ptr(pool.inst_root), _abi.ptr(pool.inst_end)))

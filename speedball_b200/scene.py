@@ -87,14 +87,23 @@ def tlas_node_count(n: int) -> int:
     return t[n] if n else 0
 
 
-def build_blas(mesh: Mesh):
-    lib = _abi.load()
+def build_blas(mesh: Mesh, ctx=None, lib=None):
+    """One mesh's BLAS in the threaded layout: on the host (sbh_build_blas), or
+    on the GPU of context `ctx` (sb_build_blas_gpu, a linear BVH)."""
+    lib = lib or _abi.load()
     pos = np.ascontiguousarray(mesh.positions, dtype=np.float32)
     idx = np.ascontiguousarray(mesh.indices, dtype=np.uint32)
     T = idx.shape[0]
     nodes = np.zeros((2 * T, 8), dtype=np.uint32)
     order = np.zeros(T, dtype=np.uint32)
-    n = lib.sbh_build_blas(_abi.ptr(pos), pos.shape[0], _abi.ptr(idx), T, MAX_LEAF, _abi.ptr(nodes), _abi.ptr(order))
+    if ctx is not None:
+        n = C.c_uint32(0)
+        _abi.check(lib.sb_build_blas_gpu(ctx, _abi.ptr(pos), pos.shape[0], _abi.ptr(idx), T, MAX_LEAF,
+                                         _abi.ptr(nodes), _abi.ptr(order), C.byref(n)), ctx)
+        n = n.value
+    else:
+        n = lib.sbh_build_blas(_abi.ptr(pos), pos.shape[0], _abi.ptr(idx), T, MAX_LEAF, _abi.ptr(nodes),
+                               _abi.ptr(order))
     if n == 0:
         raise ValueError("BLAS build failed (empty mesh or out-of-range index)")
     return nodes[:n].copy(), order
@@ -148,8 +157,9 @@ def column_major(m4: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(np.asarray(m4, dtype=np.float64).T.reshape(16))
 
 
-def build_pool(scene: SceneDesc) -> Pool:
-    blas = [build_blas(m) for m in scene.meshes]
+def build_pool(scene: SceneDesc, ctx=None, lib=None) -> Pool:
+    """The pool of `scene`; with a context, every BLAS is built on its GPU."""
+    blas = [build_blas(m, ctx, lib) for m in scene.meshes]
     nV = sum(m.positions.shape[0] for m in scene.meshes)
     nT = sum(m.indices.shape[0] for m in scene.meshes)
     nN = sum(b[0].shape[0] for b in blas)
