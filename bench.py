@@ -47,7 +47,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch", "large", "gather"], default="atrium",
+    ap.add_argument("--workload", choices=["atrium", "adjoint", "batch", "large", "gather", "build"],
+                    default="atrium",
                     help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
                          "differentiated update (64 materials, 32 point lights, 2 feedback solves); batch: 3 "
                          "nested cascades of the atrium + 8 independent atria per frame, batched vs plain; "
@@ -892,6 +893,110 @@ def run_gather(args, dist: Dist):
     return line
 
 
+BUILD_METRIC = "BLAS build Mtris/s (GPU linear BVH, threaded layout)"
+
+
+def run_build(args, dist: Dist):
+    """One step = the BLAS builds of every mesh of the atrium (30 meshes,
+    262,267 triangles) and of the large scene's 8 archetypes (2.1M triangles)
+    on the GPU (sb_build_blas_device: device arrays in, threaded nodes out),
+    the meshes resident in HBM. Beside it, once per mesh on the host: the
+    library's host builder and the oracle's MeshBVH restatement (the
+    reference's CPU build)."""
+    from speedball_b200 import _abi, synth
+    from speedball_b200 import scene as sc
+    device = dist.local
+    rt = cudart()
+    ck(rt.cudaSetDevice(device))
+    lib = _abi.load()
+    h = C.c_void_p()
+    _abi.check(lib.sb_create(C.byref(_abi.sb_device_opts(device, 0)), C.byref(h)))
+    stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
+    _abi.check(lib.sb_set_stream(h, C.c_void_p(int(stream))), h)
+    meshes = synth.atrium(1).meshes + synth.large_scene().meshes
+    H2D = rt.cudaMemcpyKind.cudaMemcpyHostToDevice
+    dev = []
+    for m in meshes:
+        pos = np.ascontiguousarray(m.positions, np.float32)
+        idx = np.ascontiguousarray(m.indices, np.uint32)
+        T = idx.shape[0]
+        bufs = [ck(rt.cudaMalloc(pos.nbytes)), ck(rt.cudaMalloc(idx.nbytes)), ck(rt.cudaMalloc(T * 64)),
+                ck(rt.cudaMalloc(T * 4)), ck(rt.cudaMalloc(4))]
+        ck(rt.cudaMemcpy(bufs[0], pos.ctypes.data, pos.nbytes, H2D))
+        ck(rt.cudaMemcpy(bufs[1], idx.ctypes.data, idx.nbytes, H2D))
+        dev.append((pos.shape[0], T, bufs))
+    tris = sum(T for _, T, _ in dev)
+
+    def step():
+        for V, T, b in dev:
+            _abi.check(lib.sb_build_blas_device(h, C.c_void_p(int(b[0])), V, C.c_void_p(int(b[1])), T, 8,
+                                                C.c_void_p(int(b[2])), C.c_void_p(int(b[3])), C.c_void_p(int(b[4]))),
+                       h)
+
+    e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
+    W, K = args.warmup, args.steps
+    for _ in range(W):
+        step()
+    ck(rt.cudaStreamSynchronize(stream))
+    clocks = Clocks(device)
+    clocks.start()
+    total = 0.0
+    for _ in range(K):
+        ck(rt.cudaEventRecord(e0, stream))
+        step()
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        total += ck(rt.cudaEventElapsedTime(e0, e1))
+    clk = clocks.stop()
+    _abi.check(lib.sb_synchronize(h), h)
+    ms = dist.max(total / K)
+    # the largest mesh alone
+    big = max(range(len(dev)), key=lambda i: dev[i][1])
+    V, T, b = dev[big]
+    tb = 0.0
+    for _ in range(K):
+        ck(rt.cudaEventRecord(e0, stream))
+        _abi.check(lib.sb_build_blas_device(h, C.c_void_p(int(b[0])), V, C.c_void_p(int(b[1])), T, 8,
+                                            C.c_void_p(int(b[2])), C.c_void_p(int(b[3])), C.c_void_p(int(b[4]))), h)
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        tb += ck(rt.cudaEventElapsedTime(e0, e1))
+    big_ms = tb / K
+    # host builders on the same meshes, once
+    t0 = time.perf_counter()
+    for m in meshes:
+        sc.build_blas(m)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import orc
+    t0 = time.perf_counter()
+    for m in meshes:
+        orc.build_blas(m.positions, m.indices)
+    orc_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    orc.build_blas(meshes[big].positions, meshes[big].indices)
+    orc_big_ms = (time.perf_counter() - t0) * 1e3
+    for _, _, bufs in dev:
+        for p in bufs:
+            ck(rt.cudaFree(p))
+    lib.sb_destroy(h)
+    line = {
+        "metric": BUILD_METRIC, "value": round(dist.world * tris / (ms * 1e-3) / 1e6, 2), "unit": "Mtris/s",
+        "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(ms, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 bounds, u32 keys",
+        "data": "synthetic (the atrium's 30 meshes + the large scene's 8 archetypes)",
+        "config": {"workload": f"BLAS builds of {len(dev)} meshes, {tris} triangles, leaves of <= 8", "meshes": len(dev),
+                   "triangles": int(tris)},
+        "largest_mesh": {"triangles": int(T), "gpu_ms": round(big_ms, 4), "oracle_meshbvh_ms": round(orc_big_ms, 1)},
+        "host_builder_ms_all": round(host_ms, 1), "oracle_meshbvh_ms_all": round(orc_ms, 1),
+        "cpu_baseline": {"value": round(tris / (orc_ms * 1e-3) / 1e6, 3), "unit": "Mtris/s", "cores": 1,
+                         "kind": "port", "sample": "the oracle's MeshBVH restatement (one thread) on every mesh once"},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    return line
+
+
 LARGE_METRIC = "probe Mrays/s (large scene, 2 cascades)"
 
 
@@ -1051,6 +1156,9 @@ def main():
         elif args.workload == "batch":
             line = run_batch(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference has no batched multi-scene form"}
+        elif args.workload == "build":
+            line = run_build(args, dist) if args.impl == "ours" else \
+                {"impl": "reference", "unavailable": "the reference builds its BVHs with three-mesh-bvh in JS"}
         elif args.workload == "gather":
             line = run_gather(args, dist) if args.impl == "ours" else \
                 {"impl": "reference", "unavailable": "the reference's gather is a WebGPU fragment shader"}

@@ -42,6 +42,9 @@ __device__ __forceinline__ float3 bilinear3(const uint2* atlas, uint32_t W, uint
               t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
 }
 
+// FULL = false compiles the default receiver alone (chebyStrength 0, no dual
+// detail): no depth fetch and no second fetch direction.
+template <bool FULL>
 __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, float chebyBias, float3 cageP,
                                  float3 P, float3 Nvis, float3 Ndir, bool dual) {
     float base[3], frac[3], rm1[3];
@@ -58,7 +61,8 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
     const float2 oN = oct_encode(normalize3(Ndir));
     const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
     const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
-    const float cs = A.chebyStrength;
+    const float cs = FULL ? A.chebyStrength : 0.0f;
+    if (!FULL) dual = false;
     float3 acc = mk(0.0f, 0.0f, 0.0f);
     float wsum = 0.0f;
 #pragma unroll 2
@@ -72,7 +76,7 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float col = px, row = pz * C.res[1] + py;
         const float ox0 = col * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
         float w = wTri;
-        if (cs != 0.0f) {
+        if (FULL && cs != 0.0f) {
             const float3 probePos = mk(C.gridMin[0] + px / rm1[0] * C.gridSize[0],
                                        C.gridMin[1] + py / rm1[1] * C.gridSize[1],
                                        C.gridMin[2] + pz / rm1[2] * C.gridSize[2]);
@@ -94,7 +98,7 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
             w = wTri * wrapW * visW;
         }
         float3 e = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oN.x * 6.0f) * invW, (oy0 + oN.y * 6.0f) * invH);
-        if (dual) {
+        if (FULL && dual) {
             const float3 eS = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oS.x * 6.0f) * invW,
                                         (oy0 + oS.y * 6.0f) * invH);
             const float t = A.detailStrength;
@@ -106,7 +110,8 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
     return acc * (1.0f / fmaxf(wsum, 1e-4f));
 }
 
-__global__ void __launch_bounds__(256) k_gather(const GatherArgs A) {
+template <bool FULL>
+__global__ void __launch_bounds__(256, FULL ? 3 : 4) k_gather(const GatherArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.count) return;
     const float4 p4 = __ldcs(A.position + i), n4 = __ldcs(A.stableNormal + i), d4 = __ldcs(A.detailNormal + i);
@@ -115,7 +120,7 @@ __global__ void __launch_bounds__(256) k_gather(const GatherArgs A) {
     const float3 P = reflP + Nvis * A.normalBias0 * A.sampleBiasScale;
     float3 E;
     if (A.cascades < 2) {
-        E = gather_cascade(A.c[0], A, A.chebyBias[0], P, P, Nvis, Ndir, A.dualDetail != 0);
+        E = gather_cascade<FULL>(A.c[0], A, A.chebyBias[0], P, P, Nvis, Ndir, A.dualDetail != 0);
     } else {
         const GatherCascade& F = A.c[1];
         const float f0 = (P.x - F.gridMin[0]) / fmaxf(F.gridSize[0], 1e-6f);
@@ -126,9 +131,9 @@ __global__ void __launch_bounds__(256) k_gather(const GatherArgs A) {
         const float wIn = clampf(fminf(fLo, fHi) / fmaxf(A.borderBand, 1e-4f), 0.0f, 1.0f);
         const float wFine = wIn * clampf(float(A.cascades) - 1.0f, 0.0f, 1.0f);
         E = mk(0.0f, 0.0f, 0.0f);
-        if (wFine < 1.0f) E = gather_cascade(A.c[0], A, A.chebyBias[0], reflP, P, Nvis, Ndir, false);
+        if (wFine < 1.0f) E = gather_cascade<FULL>(A.c[0], A, A.chebyBias[0], reflP, P, Nvis, Ndir, false);
         if (wFine > 0.0f) {
-            const float3 Ef = gather_cascade(A.c[1], A, A.chebyBias[1], reflP, P, Nvis, Ndir, false);
+            const float3 Ef = gather_cascade<FULL>(A.c[1], A, A.chebyBias[1], reflP, P, Nvis, Ndir, false);
             E = E * (1.0f - wFine) + Ef * wFine;
         }
     }
@@ -140,7 +145,9 @@ __global__ void __launch_bounds__(256) k_gather(const GatherArgs A) {
 
 cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st) {
     if (A.count == 0) return cudaSuccess;
-    k_gather<<<(A.count + 255) / 256, 256, 0, st>>>(A);
+    const bool full = A.cascades > 1 || A.chebyStrength != 0.0f || A.dualDetail;
+    if (full) k_gather<true><<<(A.count + 255) / 256, 256, 0, st>>>(A);
+    else k_gather<false><<<(A.count + 255) / 256, 256, 0, st>>>(A);
     note_launch();
     return cudaGetLastError();
 }

@@ -95,16 +95,30 @@ __device__ __forceinline__ float3 probe_world_pos(const DevCascade& C, uint32_t 
 //   z = 1 - 2 frac((k + 0.5)/N + j),  phi = k * pi (3 - sqrt 5) + 2 pi j.
 // phi reaches hundreds of radians; evaluated naively in FP32 its rounding tilts
 // the ray by ~1e-5 rad. Here phi / pi is formed in double-float, reduced mod 2
-// exactly and fed to sincospif with a first-order correction for the low part,
-// so the direction carries ~1e-7 rad of error.
+// exactly and fed to sincospif with a first-order correction for the low part.
+// The polar part is double-float too: u = (k + 0.5)/N + j rounded to FP32 moves
+// z by ~1e-7, which near the poles (small r) tilts the ray by ~1e-6 rad; with
+// u, z and r = sqrt(1 - z^2) = 2 sqrt(u (1 - u)) carried as hi + lo the
+// direction keeps ~1e-7 rad of error for every jitter.
 __device__ __forceinline__ float3 ray_dir(uint32_t k, uint32_t N, float jitter) {
     const float G_HI = 0.7639320492744446f;       // 3 - sqrt(5) = G_HI + G_LO
     const float G_LO = -2.6774234385129603e-08f;
-    float sk = (float(k) + 0.5f) / float(N);
-    float u = sk + jitter;
-    float uw = u - floorf(u);
-    float z = 1.0f - uw * 2.0f;
-    float r = sqrtf(fmaxf(0.0f, 1.0f - z * z));
+    const float kk = float(k) + 0.5f, fN = float(N);
+    const float q = kk / fN;
+    const dfl sk = fast_two_sum(q, fmaf(-q, fN, kk) / fN);  // (k + 0.5) / N, the remainder is exact
+    dfl u = df_add(sk, df(jitter));
+    float fl = floorf(u.hi);
+    if (u.hi == fl && u.lo < 0.0f) fl -= 1.0f;
+    const dfl uw = df_add(u, df(-fl));                      // frac, in [0, 1)
+    const dfl z = df_add(df(1.0f), dfl{-2.0f * uw.hi, -2.0f * uw.lo});
+    // 1 - z^2 = 4 uw (1 - uw); its square root with one Newton step in double-float
+    const dfl s4 = df_mul(uw, df_add(df(1.0f), df_neg(uw)));
+    float r = 0.0f;
+    if (s4.hi > 0.0f) {
+        const float r0 = sqrtf(s4.hi);
+        const dfl e = df_add(s4, df_neg(two_prod(r0, r0)));
+        r = 2.0f * (r0 + (e.hi + e.lo) / (2.0f * r0));
+    }
     dfl x = df_add(two_prod(float(k), G_HI), df(float(k) * G_LO));
     x = df_add(x, df(2.0f * jitter));
     float n2 = 2.0f * floorf(x.hi * 0.5f);
@@ -113,7 +127,7 @@ __device__ __forceinline__ float3 ray_dir(uint32_t k, uint32_t N, float jitter) 
     sincospif(x.hi, &s, &c);
     float d = 3.141592653589793f * x.lo;
     float s1 = fmaf(c, d, s), c1 = fmaf(-s, d, c);
-    return normalize3(mk(r * c1, r * s1, z));
+    return normalize3(mk(r * c1, r * s1, z.hi + z.lo));
 }
 
 // octEncodeNode / octDecodeNode, gi_oct.js:61-85
