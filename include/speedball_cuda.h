@@ -507,8 +507,19 @@ typedef struct sb_stats {
     uint64_t shadowTlasNodeVisits, shadowInstanceVisits, shadowBlasNodeVisits, shadowTriangleTests;
     float lastForwardRecordMs;  /* device time of the last sb_forward_record (all solves + loss) */
     float lastBackwardMs;       /* device time of the last sb_backward                       */
+    uint64_t sceneBvhBuilds;    /* host builds of the scene BVH (bvhKind 1, 2) so far        */
+    uint32_t sceneBvhActive;    /* 1 while the scene BVH answers the walks; 0 while the
+                                   reference's TLAS + BLAS walk does (bvhKind 0, or more
+                                   than 256 instance slots moved since the last build)       */
+    float lastSceneBvhBuildMs;  /* host time of the last scene-BVH build                     */
 } sb_stats;
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
+/* Rebuild the scene BVH over the current instance placements before the next
+ * trace (the reference rebuilds its BVHs only in an idle-gated rebuild,
+ * gi_probes.js:3269-3455). Moved instances stay correct without it: up to 256
+ * moved slots are walked through their own BLAS, beyond that the reference's
+ * two-level walk, refit on the GPU every frame, answers until a rebuild. */
+sb_status sb_rebuild_scene_bvh(sb_ctx* ctx);
 /* Counting costs a few percent; off by default. */
 sb_status sb_enable_counters(sb_ctx* ctx, int32_t on);
 

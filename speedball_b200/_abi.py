@@ -130,7 +130,8 @@ class sb_stats(C.Structure):
                 ("lastShadeMs", C.c_float), ("shadowTlasNodeVisits", C.c_uint64),
                 ("shadowInstanceVisits", C.c_uint64), ("shadowBlasNodeVisits", C.c_uint64),
                 ("shadowTriangleTests", C.c_uint64), ("lastForwardRecordMs", C.c_float),
-                ("lastBackwardMs", C.c_float)]
+                ("lastBackwardMs", C.c_float), ("sceneBvhBuilds", C.c_uint64), ("sceneBvhActive", C.c_uint32),
+                ("lastSceneBvhBuildMs", C.c_float)]
 
 
 _P = C.c_void_p
@@ -144,6 +145,7 @@ SIGNATURES = {
     "sb_set_stream": (C.c_int, [_P, _P]),
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
     "sb_triangle_test": (C.c_uint32, []),
+    "sb_rebuild_scene_bvh": (C.c_int, [_P]),
     "sb_build_blas_device": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_build_blas_gpu": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_probe_rays": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),

@@ -1852,9 +1852,18 @@ sb_status sb_enable_counters(sb_ctx* ctx, int32_t on) {
     return SB_OK;
 }
 
+sb_status sb_rebuild_scene_bvh(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    ctx->flat.dirty = true;
+    return SB_OK;
+}
+
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
     if (!ctx || !out) return SB_ERR_INVALID_ARG;
     std::memset(out, 0, sizeof *out);
+    out->sceneBvhBuilds = ctx->flat.builds;
+    out->sceneBvhActive = ctx->flat.enabled && ctx->flat.ready && !ctx->flat.overflowed ? 1u : 0u;
+    out->lastSceneBvhBuildMs = ctx->flat.lastBuildMs;
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->stream));
     if (ctx->countersOn) {

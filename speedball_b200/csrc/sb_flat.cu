@@ -9,7 +9,8 @@
 //
 // Per frame nothing is rebuilt: a slot whose transform changes, or whose BLAS
 // is refit, is marked; the traversal skips that slot's items and walks its
-// current BLAS instead. More than kMaxDynamic marked slots trigger a rebuild.
+// current BLAS instead. Beyond kMaxDynamic marked slots the tree stands aside
+// and the reference's two-level walk (GPU-refit TLAS + BLASes) answers instead.
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -230,6 +231,8 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
         marksDirty = true;
         dirty = false;
         ready = true;
+        overflowed = false;
+        ++builds;
         lastBuildMs = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
     if (ready && marksDirty) {
@@ -250,7 +253,7 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
 void FlatScene::mark_slot(uint32_t s) {
     if (!ready || dirty || s >= skip.size() || skip[s]) return;
     if (dyn.size() >= kMaxDynamic) {
-        dirty = true;  // rebuild with the current placements instead
+        overflowed = true;  // the two-level walk takes over until the next rebuild
         return;
     }
     skip[s] = 1;
@@ -268,7 +271,7 @@ void FlatScene::mark_blas_range(uint32_t r0, uint32_t r1) {
 }
 
 void FlatScene::fill(DevScene& S) const {
-    const bool on = enabled && ready;
+    const bool on = enabled && ready && !overflowed;
     S.flatOn = on ? 1 : 0;
     S.flatNodes = on ? nodes : nullptr;
     S.flatItems = on ? items : nullptr;

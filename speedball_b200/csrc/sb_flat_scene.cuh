@@ -10,12 +10,18 @@
 namespace sb {
 
 struct FlatScene {
-    static constexpr uint32_t kMaxDynamic = 256;  // more moved slots than this: rebuild
+    // More moved slots than this: the scene BVH stands aside (`overflowed`) and
+    // the traversal walks the reference's TLAS + BLASes, which the GPU refits
+    // every frame, until the next rebuild (a structural change, or
+    // sb_rebuild_scene_bvh at a moment the host chooses).
+    static constexpr uint32_t kMaxDynamic = 256;
 
     bool enabled = true;  // bvhKind 1 or 2
     bool wide = true;     // bvhKind 1: also the 8-wide tree, which answers closest hits
     bool dirty = true;    // rebuild before the next trace
     bool ready = false;   // device copy current
+    bool overflowed = false;  // more than kMaxDynamic moved slots since the build
+    uint64_t builds = 0;      // scene-BVH builds of this context
     uint4* nodes = nullptr;   // binary child-pair tree (any hit; closest hit without `wide`)
     size_t nodeCap = 0;
     uint2* items = nullptr;

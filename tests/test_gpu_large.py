@@ -173,3 +173,48 @@ def test_large_probe_block_matches_oracle(large, ci):
     assert changed > 0.05, changed
     assert err.max() <= gu.TEXEL_REL, err.max()
     assert derr.max() <= gu.TEXEL_REL, derr.max()
+
+
+def test_all_instances_moving_stays_on_the_gpu(large):
+    """Every one of the 400 instances moves in one frame: no host rebuild of the
+    scene BVH (the reference's GPU-refit TLAS + BLAS walk answers while more
+    than 256 slots are out of the tree), and the hits still match the FP64
+    oracle ray by ray; sb_rebuild_scene_bvh brings the tree back, again with
+    matching hits."""
+    scene, f = large
+    _set_kind(f, 1)
+    _frame(scene, f, 2)
+    st0 = _abi.sb_stats()
+    _abi.check(f._lib.sb_get_stats(f.ctx, C.byref(st0)), f.ctx)
+    assert st0.sceneBvhActive == 1
+    rng = np.random.default_rng(8)
+    for inst in scene.instances:
+        inst.world = inst.world.copy()
+        inst.world[:3, 3] += rng.uniform(-0.05, 0.05, 3)
+    f.markTransformsDirty()
+    _frame(scene, f, 3)
+    st1 = _abi.sb_stats()
+    _abi.check(f._lib.sb_get_stats(f.ctx, C.byref(st1)), f.ctx)
+    assert st1.sceneBvhBuilds == st0.sceneBvhBuilds and st1.sceneBvhActive == 0
+
+    def hits_match():
+        mirror = gu.OracleMirror(f)
+        ro, rd = _probe_rays(f, SAMPLE_RAYS, 77)
+        n = SAMPLE_RAYS
+        t = np.zeros(n, np.float32); tri = np.zeros(n, np.int32); inst = np.zeros(n, np.int32)
+        _abi.check(f._lib.sb_raycast(f.ctx, _abi.ptr(ro), _abi.ptr(rd), n, _abi.ptr(t), _abi.ptr(tri),
+                                     _abi.ptr(inst)), f.ctx)
+        ot, otri, oinst, o2 = np.zeros(n), np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n)
+        orc.load().orc_closest(C.byref(mirror.scene), orc._p(ro), orc._p(rd), n, 1, 0, orc._p(ot), orc._p(otri),
+                               orc._p(oinst), orc._p(o2), orc.threads())
+        return gu.check_hits(mirror.scene, ro.astype(np.float64), rd.astype(np.float64), tri, inst, t, otri, oinst,
+                             ot)
+
+    moved = hits_match()
+    _abi.check(f._lib.sb_rebuild_scene_bvh(f.ctx), f.ctx)
+    _frame(scene, f, 4)
+    st2 = _abi.sb_stats()
+    _abi.check(f._lib.sb_get_stats(f.ctx, C.byref(st2)), f.ctx)
+    assert st2.sceneBvhBuilds == st1.sceneBvhBuilds + 1 and st2.sceneBvhActive == 1
+    rebuilt = hits_match()
+    _report("all_instances_moving", dict(moved=moved, rebuilt=rebuilt, rebuild_ms=float(st2.lastSceneBvhBuildMs)))
