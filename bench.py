@@ -101,7 +101,7 @@ def make_workload():
 def field_for(scene, device):
     from speedball_b200.field import ProbeField
     g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
                    clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)  # one solve updates all 4,096 probes
@@ -500,7 +500,7 @@ def adjoint_field(device):
     from speedball_b200.field import ProbeField
     scene = synth.room_spheres(0, n_materials=64, n_point=32, n_dir=0)
     g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
                    hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)
@@ -628,7 +628,7 @@ def batch_fields(device):
 
     def make(scene, jitter):
         g = scene.meta["grid"]
-        f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]),
+        f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1,
                        rays=g["rays"], clusteredLighting=True, hysteresis=scene.meta["hysteresis"],
                        jitterMode=jitter, device=device)
         f.setHysteresisNormalization(False)
@@ -1008,7 +1008,7 @@ def large_field(device):
     from speedball_b200.field import ProbeField
     scene = synth.large_scene()
     g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
                    clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)

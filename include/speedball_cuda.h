@@ -271,6 +271,17 @@ sb_status sb_build_blas_gpu(sb_ctx* ctx, const float* pos3, uint32_t vertexCount
                             uint32_t triCount, uint32_t leafSize, uint32_t* nodesOut, uint32_t* triOrderOut,
                             uint32_t* nodeCountOut);
 
+/* Fine-cascade placement (fitFineBox, gi_probes.js:2963-3030): over the coarse
+ * box (boxMin, boxSize: the Box3 min and getSize() of C0's grid, doubles), a
+ * 16^3 histogram of the pooled triangles' centroids (the pool's vertexData as
+ * uploaded, as the reference bins it), the bins of >= 0.4 x the peak united,
+ * padded by one bin, each axis clamped to [0.25, 0.60] of the coarse box and
+ * moved inside it. *found = 0 when the histogram is empty or the cluster spans
+ * the whole box (the reference then places no C1). The histogram runs on the
+ * GPU; synchronizes. */
+sb_status sb_fit_fine_box(sb_ctx* ctx, const double boxMin[3], const double boxSize[3], double outMin[3],
+                          double outSize[3], int32_t* found);
+
 /* ------------------------------------------------------- receiver gather */
 
 /* The receiver's uniforms (GiProbeNode, gi_probes.js:306-358). */

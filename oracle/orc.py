@@ -530,3 +530,159 @@ def gather(grid0: OrcGrid, atlas0: np.ndarray, depth0: np.ndarray, params: np.nd
                       _p(atlas1), _p(depth1), _p(np.ascontiguousarray(params, np.float64)), *[_p(a) for a in arr], n,
                       _p(out), _p(near), threads())
     return out, near
+
+
+# ------------------------------------------------- fine cascade placement
+def js_to_int32(x: np.ndarray) -> np.ndarray:
+    """ECMAScript ToInt32 (the `| 0` operator) of float64 values."""
+    x = np.asarray(x, np.float64)
+    out = np.zeros(x.shape, np.int64)
+    fin = np.isfinite(x)
+    t = np.trunc(x[fin])
+    m = np.fmod(t, 4294967296.0)
+    m = np.where(m < 0, m + 4294967296.0, m)
+    m = np.where(m >= 2147483648.0, m - 4294967296.0, m)
+    out[fin] = m.astype(np.int64)
+    return out
+
+
+def fit_fine_box(vertex_data: np.ndarray, tri_index: np.ndarray, box_min, box_size):
+    """fitFineBox (gi_probes.js:2968-3030) in float64, JS semantics: 16^3
+    histogram of the pooled triangles' centroids ((v0 + v1 + v2) / 3 of the
+    pooled vertexData), bins >= 0.4 x peak united, padded by one bin, each
+    axis clamped to [0.25, 0.60] of the box and slid inside it. Returns
+    (min[3], size[3]) or None."""
+    G = 16
+    mn = [float(v) for v in box_min]
+    size = [float(v) for v in box_size]
+    inv = [G / max(1e-6, size[a]) for a in range(3)]
+    vd = np.asarray(vertex_data, np.float32).reshape(-1, 8)[:, 0:3].astype(np.float64)
+    ti = np.asarray(tri_index, np.int64).reshape(-1, 3)
+    c = ((vd[ti[:, 0]] + vd[ti[:, 1]]) + vd[ti[:, 2]]) / 3.0
+    g = [np.clip(js_to_int32((c[:, a] - mn[a]) * inv[a]), 0, G - 1) for a in range(3)]
+    hist = np.bincount((g[2] * G + g[1]) * G + g[0], minlength=G ** 3)
+    peak = int(hist.max()) if hist.size else 0
+    if peak == 0:
+        return None
+    thr = peak * 0.4
+    sel = np.flatnonzero(hist >= thr)
+    if sel.size == 0:
+        return None
+    xs, ys, zs = sel % G, (sel // G) % G, sel // (G * G)
+    bx0, bx1, by0, by1, bz0, bz1 = int(xs.min()), int(xs.max()), int(ys.min()), int(ys.max()), int(zs.min()), int(zs.max())
+    if bx0 == 0 and by0 == 0 and bz0 == 0 and bx1 == G - 1 and by1 == G - 1 and bz1 == G - 1:
+        return None
+    cell = [size[a] / G for a in range(3)]
+    lo_b, hi_b = (bx0, by0, bz0), (bx1, by1, bz1)
+    fmin = [mn[a] + lo_b[a] * cell[a] for a in range(3)]
+    fmax = [mn[a] + (hi_b[a] + 1) * cell[a] for a in range(3)]
+    pad = min(cell[0], cell[1], cell[2])
+    fmin = [v - pad for v in fmin]
+    fmax = [v + pad for v in fmax]
+    fsize = [fmax[a] - fmin[a] for a in range(3)]
+    box0max = [mn[a] + size[a] for a in range(3)]
+    for a in range(3):
+        lo, hi = 0.25 * size[a], 0.60 * size[a]
+        s = max(lo, min(hi, fsize[a]))
+        center = (fmin[a] + fmax[a]) * 0.5
+        m0, m1 = center - s * 0.5, center + s * 0.5
+        if m0 < mn[a]:
+            m1 += (mn[a] - m0)
+            m0 = mn[a]
+        if m1 > box0max[a]:
+            m0 -= (m1 - box0max[a])
+            m1 = box0max[a]
+        m0 = max(m0, mn[a])
+        m1 = min(m1, box0max[a])
+        fmin[a] = m0
+        fsize[a] = max(1e-4, m1 - m0)
+    return fmin, fsize
+
+
+def js_round(x: float) -> int:
+    """Math.round: floor(x + 0.5)."""
+    return int(np.floor(x + 0.5))
+
+
+def compute_grid_resolution(size, target_long_axis: int):
+    """computeGridResolution (gi_probes.js:938-943)."""
+    longest = max(size[0], size[1], size[2], 1e-3)
+    spacing = longest / max(1, target_long_axis)
+    return [int(min(32, max(2, js_round(s / spacing) + 1))) for s in size]
+
+
+def fine_cascade_res(fine_size, target_long_axis: int, c0_probes: int):
+    """C1's resolution (gi_probes.js:3396-3406): ~2x the coarse long-axis
+    density, then shrunk by 0.85 per axis (at most 12 times) while above
+    max(64, 2 x C0's probes)."""
+    res = compute_grid_resolution(fine_size, min(32, js_round(target_long_axis * 2.0)))
+    cap = max(64, 2 * c0_probes)
+    for _ in range(12):
+        if res[0] * res[1] * res[2] <= cap:
+            break
+        res = [max(2, int(np.floor(r * 0.85))) for r in res]
+    return res
+
+
+class Schedule2:
+    """The per-tick schedule with a fine cascade (gi_probes.js:3581-3618,
+    3715-3788): the solve list (both cascades when the tick budget covers
+    their union, else one per tick in turn), per cascade the probe count,
+    cursor, service-interval EMA and hysteresis exponent, the tick-interval EMA
+    as the fallback service interval (x2 when the cascades alternate), and the
+    montecarlo epoch advanced on ticks that solve C0."""
+
+    DT_REF_MS = 1000.0 / 60.0
+
+    def __init__(self, totals, rays: int, ray_budget: int, max_probes: int, montecarlo: bool, normalize: bool):
+        self.totals = list(totals)
+        self.cap = max(1, min(max_probes, ray_budget // max(1, rays)))
+        self.montecarlo = montecarlo
+        self.normalize = normalize
+        n = len(self.totals)
+        self.cursor, self.last, self.ema = [0] * n, [0.0] * n, [0.0] * n
+        self.turn = 0
+        self.frame = 0
+        self.jitter = 0.0
+        self.seed_counter = 0
+        self.seed = 0.0
+        self.last_tick = 0.0
+        self.tick_ema = 0.0
+
+    def tick(self, now_ms: float) -> list:
+        if self.last_tick > 0:
+            dt = now_ms - self.last_tick
+            self.tick_ema = (self.tick_ema * 0.8 + dt * 0.2 if self.tick_ema > 0 else dt) if 0 < dt < 100 else 0.0
+        self.last_tick = now_ms
+        have_c1 = len(self.totals) > 1
+        full = self.cap >= sum(self.totals)
+        if not have_c1:
+            lst = [0]
+        elif full:
+            lst = [0, 1]
+        else:
+            lst = [self.turn % 2]
+            self.turn = (self.turn + 1) & 0xFFFFFFFF
+        fallback_ticks = 1 if (not have_c1 or full) else 2
+        out = []
+        for ci in lst:
+            total = self.totals[ci]
+            updated = min(self.cap, total)
+            ema = self.ema[ci]
+            if self.last[ci] > 0:
+                dt = now_ms - self.last[ci]
+                ema = (ema * 0.8 + dt * 0.2 if ema > 0 else dt) if 0 < dt < 200 else 0.0
+            service = ema if ema > 0 else (self.tick_ema if self.tick_ema > 0 else self.DT_REF_MS) * fallback_ticks
+            revisit = max(1.0, total / max(1, updated))
+            exponent = load().orc_hysteresis_exponent(service * revisit, 1 if self.normalize else 0)
+            if ci == 0 and self.montecarlo:
+                self.seed_counter = (self.seed_counter + 1) & 0xFFFFFFFF
+                self.seed = (self.seed_counter * 0.61803398875) % 1
+                self.frame = (self.frame + 1) & 0xFFFFFFFF
+                self.jitter = (self.frame * 0.61803398875) % 1
+            out.append(dict(cascade=ci, probeOffset=self.cursor[ci], updatedCount=updated,
+                            hysteresisExponent=exponent, frameJitter=self.jitter, emitterVisSeed=self.seed))
+            self.cursor[ci] = (self.cursor[ci] + updated) % total if total else 0
+            self.last[ci] = now_ms
+            self.ema[ci] = ema
+        return out

@@ -145,6 +145,7 @@ SIGNATURES = {
     "sb_set_stream": (C.c_int, [_P, _P]),
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
     "sb_triangle_test": (C.c_uint32, []),
+    "sb_fit_fine_box": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "sb_rebuild_scene_bvh": (C.c_int, [_P]),
     "sb_build_blas_device": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_build_blas_gpu": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),

@@ -52,6 +52,7 @@ struct sb_ctx {
     uint32_t flags = 0;
     uint32_t walkStepLimit = 0;  // sb_set_walk_step_limit (0 = the defaults)
     BlasBuilder* builder = nullptr;  // GPU BLAS build scratch (sb_build_blas_*)
+    uint32_t* dHist = nullptr;       // sb_fit_fine_box's 16^3 histogram
     cudaStream_t stream = nullptr;
     cudaStream_t ownStream = nullptr;
     std::string err;
@@ -427,6 +428,7 @@ void sb_destroy(sb_ctx* ctx) {
         blas_builder_destroy(ctx->builder);
         ctx->builder = nullptr;
     }
+    release(ctx->dHist);
     InstanceTable& I = ctx->I;
     release(I.world); release(I.active); release(I.blasRoot); release(I.blasEnd); release(I.aabb); release(I.invRows);
     release(I.detSign); release(I.order); release(I.slotOf); release(I.liveBounds); release(I.nodeDepth);
@@ -1615,6 +1617,24 @@ sb_status sb_build_blas_gpu(sb_ctx* ctx, const float* pos3, uint32_t vertexCount
     cudaFreeAsync(dord, ctx->stream); cudaFreeAsync(dc, ctx->stream);
     if (s != SB_OK) return s;
     return sb_synchronize(ctx);
+}
+
+sb_status sb_fit_fine_box(sb_ctx* ctx, const double boxMin[3], const double boxSize[3], double outMin[3],
+                          double outSize[3], int32_t* found) {
+    if (!ctx || !boxMin || !boxSize || !outMin || !outSize || !found) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    *found = 0;
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    cudaSetDevice(ctx->device);
+    if (!ctx->dHist) CK(cudaMalloc(&ctx->dHist, 4096 * sizeof(uint32_t)));
+    double inv[3];
+    for (int a = 0; a < 3; ++a) inv[a] = 16.0 / std::fmax(1e-6, boxSize[a]);
+    CK(launch_fine_hist(ctx->B, boxMin, inv, ctx->dHist, ctx->stream));
+    std::vector<uint32_t> h(4096);
+    CK(cudaMemcpyAsync(h.data(), ctx->dHist, 4096 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    sb_status s = sb_synchronize(ctx);
+    if (s != SB_OK) return s;
+    *found = fine_box_from_hist(h.data(), boxMin, boxSize, outMin, outSize) ? 1 : 0;
+    return SB_OK;
 }
 
 void sb_gather_params_defaults(sb_gather_params* p) {

@@ -167,6 +167,12 @@ void blas_builder_destroy(BlasBuilder* b);
 cudaError_t blas_build(BlasBuilder* b, const float* pos, uint32_t V, const uint32_t* idx, uint32_t T,
                        uint32_t leafSize, uint32_t* nodes, uint32_t* order, uint32_t* nodeCount, uint32_t* err,
                        cudaStream_t st);
+// Fine-cascade placement (sb_cascade.cu): the 16^3 centroid histogram on the
+// GPU, then the box on the host.
+cudaError_t launch_fine_hist(const SceneBuffers& B, const double mn[3], const double inv[3], uint32_t* hist,
+                             cudaStream_t st);
+bool fine_box_from_hist(const uint32_t* hist, const double mn[3], const double size[3], double outMin[3],
+                        double outSize[3]);
 // The FP32 probe rays of a solve as the trace forms them (sb_probe_rays).
 cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st);
 

@@ -37,6 +37,8 @@ GI_EMITTER_INJECT_CAP = 16
 SURFACE_NORMAL_BIAS_CELL = 0.03
 JITTER_HYSTERESIS_DEFAULTS = {"gated": 0.60, "montecarlo": 0.90}
 HYSTERESIS_DT_REF_MS = 1000.0 / 60.0
+TICK_OVERLOAD_MS = 100.0
+C1_RES_SCALE = 2.0
 
 
 def hysteresisExponentForInterval(updateDtMs: float, normalize: bool = True) -> float:
@@ -111,17 +113,24 @@ class ProbeField:
         self._hysteresis = min(0.99, max(0.0, float(base_h)))
         self._targetLongAxis = int(min(MAX_PROBES_PER_AXIS, max(2, round(divisions) or TARGET_PROBES_LONG_AXIS)))
         self._rays = int(min(RAYS_MAX, max(RAYS_MIN, round(float(rays) / 16) * 16 or RAYS_PER_PROBE_DEFAULT)))
-        # one cascade is solved here; C1 placement (fitFineBox) is outside the built scope
-        self._cascades = 1
+        # cascades=2 places the fine cascade C1 with fitFineBox at every rebuild
+        self._cascades = 2 if int(cascades or 1) >= 2 else 1
+        self._haveC1 = False
+        self._c1Grid = None
         self._clustered = clusteredLighting is True or isinstance(clusteredLighting, dict)
         self._volumes = volumes
         self._rayBudget = RAYS_PER_TICK
         self._maxProbesPerTick = MAX_PROBES_PER_TICK
         self._hysteresisNormalize = True
         self._frameCounter = 0
-        self._probeCursor = 0
-        self._lastSolveAt = 0.0
-        self._solveDtEma = 0.0
+        self._emitterVisSeedCounter = 0
+        self._solveTurn = 0
+        self._lastTickAt = 0.0
+        self._hysteresisTickDtEma = 0.0
+        # per cascade (C0, C1): round-robin cursor, last solve time, service-interval EMA
+        self._cursor = [0, 0]
+        self._lastSolveAt = [0.0, 0.0]
+        self._solveDtEma = [0.0, 0.0]
         self._disposed = False
         self._onRebuilt = onRebuilt
         self._pendingTransforms: set[int] = set()
@@ -159,7 +168,9 @@ class ProbeField:
         self._fit_grid()
         self._upload_lights()
         self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
-        self._probeCursor = 0
+        self._cursor = [0, 0]
+        self._lastSolveAt = [0.0, 0.0]
+        self._solveDtEma = [0.0, 0.0]
         self.stats["rebuilds"] += 1
         if self._onRebuilt:
             self._onRebuilt()
@@ -211,6 +222,42 @@ class ProbeField:
         self._res = res
         self._probeTotal = int(res[0] * res[1] * res[2])
         self._ck(self._lib.sb_configure_cascade(self._ctx, 0, C.byref(g)))
+        self._haveC1 = False
+        self._c0Box = ([float(v) for v in box_min], [float(v) for v in size])
+        if self._cascades >= 2:
+            self._place_fine_cascade(box_min, size)
+
+    def _place_fine_cascade(self, box_min, size):
+        """C1 dims (gi_probes.js:3386-3410): fitFineBox over C0's box, ~2x the
+        coarse long-axis density, shrunk while above max(64, 2 x C0's probes).
+        No fine box (empty or uniform histogram): one cascade this build."""
+        mn = (C.c_double * 3)(*[float(v) for v in box_min])
+        # Box3(min, min + size).getSize(): (min + size) - min in doubles
+        sz = (C.c_double * 3)(*[float(box_min[a] + size[a]) - float(box_min[a]) for a in range(3)])
+        omin, osize, found = (C.c_double * 3)(), (C.c_double * 3)(), C.c_int32(0)
+        self._ck(self._lib.sb_fit_fine_box(self._ctx, mn, sz, omin, osize, C.byref(found)))
+        if not found.value:
+            return
+        fsize = [osize[a] for a in range(3)]
+        self._c1Box = ([omin[a] for a in range(3)], fsize, [sz[a] for a in range(3)])
+        res = computeGridResolution(fsize, min(MAX_PROBES_PER_AXIS, math.floor(self._targetLongAxis * C1_RES_SCALE + 0.5)))
+        cap = max(64, 2 * self._probeTotal)
+        for _ in range(12):
+            if res[0] * res[1] * res[2] <= cap:
+                break
+            res = tuple(max(2, math.floor(r * 0.85)) for r in res)
+        g = _abi.sb_grid()
+        for a in range(3):
+            g.gridMin[a] = omin[a]
+            g.gridSize[a] = fsize[a]
+            g.res[a] = int(res[a])
+        g.raysPerProbe = self._rays
+        g.maxDist = float(np.linalg.norm(np.asarray(fsize, np.float64)))
+        g.cellMin = float(max(1e-4, min(fsize[a] / max(1, res[a] - 1) for a in range(3))))
+        self._ck(self._lib.sb_configure_cascade(self._ctx, 1, C.byref(g)))
+        self._c1Grid = g
+        self._c1Total = int(res[0] * res[1] * res[2])
+        self._haveC1 = True
 
     def _upload_lights(self):
         gmin = [self._grid.gridMin[a] for a in range(3)]
@@ -227,50 +274,113 @@ class ProbeField:
         return max(1, min(self._maxProbesPerTick, self._rayBudget // max(1, self._rays)))
 
     def tick(self, idleMs: float = math.inf, playing: bool = False, nowMs: float | None = None) -> dict:
-        """One tick: dirty lanes, then one solve of C0 (gi_probes.js:3472-3849)."""
+        """One tick (gi_probes.js:3472-3849): dirty lanes, then the solves of
+        this tick: C0, or with a fine cascade both cascades when the ray budget
+        covers their union, else one cascade per tick in turn. Returns the
+        first solve's frame with every solve under "solves"."""
         if self._disposed:
             return {}
-        frame = self.beginTick(nowMs)
-        self._ck(self._lib.sb_solve(self._ctx, frame["cascade"], frame["probeOffset"], frame["updatedCount"]))
-        self.endTick(frame, nowMs)
-        return frame
-
-    def beginTick(self, nowMs: float | None = None) -> dict:
-        """The part of a tick ahead of its solve: dirty lanes, the solve's probe
-        range and its uniforms (jitter epoch, hysteresis exponent). A batched
-        frame (speedball_b200.batch) solves several fields' ranges in one launch
-        between beginTick and endTick."""
-        lib = self._lib
+        self._tick_clock(nowMs)
         if self._pendingTopology:
             self._pendingTopology = False
             self._rebuild()
-        # the uniforms first (host work only), so that the solve is enqueued right
-        # behind the dirty lanes while the GPU runs them
-        C0 = 0
-        updated = min(self.updatedCap(), self._probeTotal)
-        if nowMs is not None and self._lastSolveAt > 0:
-            dt = nowMs - self._lastSolveAt
-            self._solveDtEma = (self._solveDtEma * 0.8 + dt * 0.2 if self._solveDtEma > 0 else dt) \
-                if 0 < dt < 200 else 0.0
-        serviceDt = self._solveDtEma if self._solveDtEma > 0 else HYSTERESIS_DT_REF_MS
-        revisit = probeUpdateIntervalTicks(self._probeTotal, updated)
-        self._params.hysteresisExponent = hysteresisExponentForInterval(serviceDt * revisit, self._hysteresisNormalize)
+        lst = self._solve_list()
+        fallback = 1 if (not self._haveC1 or len(lst) == 2) else 2
+        if 0 in lst:
+            self._advance_epoch()
+        solves = []
+        for n, ci in enumerate(lst):
+            s = self._plan_solve(ci, nowMs, fallback)
+            self._params.hysteresisExponent = s["hysteresisExponent"]
+            self._params.hysteresis = self._hysteresis
+            self._ck(self._lib.sb_set_params(self._ctx, C.byref(self._params)))
+            if n == 0:
+                self._refresh_lanes()
+            self._ck(self._lib.sb_solve(self._ctx, ci, s["probeOffset"], s["updatedCount"]))
+            self._commit_solve(s, nowMs)
+            solves.append(s)
+        out = dict(solves[0])
+        out["solves"] = solves
+        return out
+
+    def _tick_clock(self, nowMs):
+        """The tick-interval EMA (gi_probes.js:3581-3618): the fallback service
+        interval of a cascade that has none of its own yet."""
+        if nowMs is None:
+            return
+        if self._lastTickAt > 0:
+            dt = nowMs - self._lastTickAt
+            ema = self._hysteresisTickDtEma
+            self._hysteresisTickDtEma = (ema * 0.8 + dt * 0.2 if ema > 0 else dt) if 0 < dt < TICK_OVERLOAD_MS else 0.0
+        self._lastTickAt = nowMs
+
+    def _solve_list(self) -> list:
+        """gi_probes.js:3715-3727."""
+        if not self._haveC1:
+            return [0]
+        if self.updatedCap() >= self._probeTotal + self._c1Total:
+            return [0, 1]
+        ci = self._solveTurn % 2
+        self._solveTurn = (self._solveTurn + 1) & 0xFFFFFFFF
+        return [ci]
+
+    def _advance_epoch(self):
+        """Montecarlo: a new ray basis and emitter target on every C0 solve
+        (gi_probes.js:3766-3787); gated keeps both."""
         if self._jitterMode == "montecarlo":
+            self._emitterVisSeedCounter = (self._emitterVisSeedCounter + 1) & 0xFFFFFFFF
+            self._params.emitterVisSeed = (self._emitterVisSeedCounter * 0.61803398875) % 1
             self._frameCounter = (self._frameCounter + 1) & 0xFFFFFFFF
             self._params.frameJitter = self._frameJitterOverride if self._frameJitterOverride is not None \
                 else (self._frameCounter * 0.61803398875) % 1
         elif self._frameJitterOverride is not None:
             self._params.frameJitter = self._frameJitterOverride
+
+    def _plan_solve(self, ci: int, nowMs, fallbackTicks: int) -> dict:
+        """One cascade's probe range and hysteresis exponent (gi_probes.js:3737-3766)."""
+        total = self.cascadeProbes(ci)
+        updated = min(self.updatedCap(), total)
+        ema = self._solveDtEma[ci]
+        if nowMs is not None and self._lastSolveAt[ci] > 0:
+            dt = nowMs - self._lastSolveAt[ci]
+            ema = (ema * 0.8 + dt * 0.2 if ema > 0 else dt) if 0 < dt < 200 else 0.0
+        serviceDt = ema if ema > 0 else \
+            (self._hysteresisTickDtEma if self._hysteresisTickDtEma > 0 else HYSTERESIS_DT_REF_MS) * fallbackTicks
+        revisit = probeUpdateIntervalTicks(total, updated)
+        return {"cascade": ci, "probeOffset": self._cursor[ci], "updatedCount": updated,
+                "hysteresisExponent": hysteresisExponentForInterval(serviceDt * revisit, self._hysteresisNormalize),
+                "_ema": ema}
+
+    def _commit_solve(self, s: dict, nowMs):
+        ci, total = s["cascade"], self.cascadeProbes(s["cascade"])
+        self._cursor[ci] = (self._cursor[ci] + s["updatedCount"]) % total if total else 0
+        self._solveDtEma[ci] = s["_ema"]
+        if nowMs is not None:
+            self._lastSolveAt[ci] = nowMs
+        self.stats["solves"] += 1
+
+    def beginTick(self, nowMs: float | None = None) -> dict:
+        """The part of a C0 tick ahead of its solve: dirty lanes, the solve's
+        probe range and its uniforms (jitter epoch, hysteresis exponent). A
+        batched frame (speedball_b200.batch) solves several fields' ranges in
+        one launch between beginTick and endTick; a field with a fine cascade
+        ticks through tick()."""
+        lib = self._lib
+        self._tick_clock(nowMs)
+        if self._pendingTopology:
+            self._pendingTopology = False
+            self._rebuild()
+        # the uniforms first (host work only), so that the solve is enqueued right
+        # behind the dirty lanes while the GPU runs them
+        s = self._plan_solve(0, nowMs, 1)
+        self._advance_epoch()
+        self._params.hysteresisExponent = s["hysteresisExponent"]
         self._ck(lib.sb_set_params(self._ctx, C.byref(self._params)))
         self._refresh_lanes()
-        return {"cascade": C0, "probeOffset": self._probeCursor, "updatedCount": updated}
+        return s
 
     def endTick(self, frame: dict, nowMs: float | None = None) -> None:
-        updated = frame["updatedCount"]
-        self._probeCursor = (self._probeCursor + updated) % self._probeTotal if self._probeTotal else 0
-        if nowMs is not None:
-            self._lastSolveAt = nowMs
-        self.stats["solves"] += 1
+        self._commit_solve(frame, nowMs)
 
     def configureCascade(self, ci: int, gridMin, gridSize, res, rays: int | None = None) -> None:
         """An extra cascade box of this field (ci >= 1), solved through
@@ -290,8 +400,16 @@ class ProbeField:
         self._extraCascades[ci] = g
 
     def cascadeProbes(self, ci: int) -> int:
-        g = self._grid if ci == 0 else self._extraCascades[ci]
+        if ci == 0:
+            g = self._grid
+        elif ci == 1 and self._haveC1 and ci not in self._extraCascades:
+            g = self._c1Grid
+        else:
+            g = self._extraCascades[ci]
         return int(g.res[0] * g.res[1] * g.res[2])
+
+    def hasFineCascade(self) -> bool:
+        return self._haveC1
 
     def _refresh_lanes(self):
         lib = self._lib

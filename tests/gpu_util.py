@@ -27,7 +27,7 @@ def grid_dict(g: _abi.sb_grid) -> dict:
 def make_field(scene, record=True, rays=None) -> ProbeField:
     m = scene.meta
     g = m["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]),
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1,
                    rays=rays or g["rays"], clusteredLighting=m.get("clustered", False),
                    hysteresis=m.get("hysteresis"), jitterMode=m.get("jitter", "gated"), recordHits=record)
     f.setHysteresisNormalization(False)
@@ -45,8 +45,9 @@ def read(field: ProbeField, key: str, count: int, dtype, cascade: int = 0) -> np
 class OracleMirror:
     """The oracle's copy of a field's scene, grid, lights and FP64 state."""
 
-    def __init__(self, field: ProbeField, fp32: bool = False):
+    def __init__(self, field: ProbeField, fp32: bool = False, cascade: int = 0):
         self.field = field
+        self.cascade = cascade
         pool = field.pool
         self.pool = pool
         self.materials = read(field, "MATERIALS", pool.materials.shape[0], np.float32)
@@ -54,16 +55,19 @@ class OracleMirror:
         self.vertex = read(field, "VERTEX_DATA", pool.vertexData.size, np.float32).reshape(-1, 8)
         self.keep = []
         self.scene = orc.scene_struct(pool, self.materials, nodes=self.nodes, vertex=self.vertex, keep=self.keep)
-        self.gdict = grid_dict(field.grid)
+        self.gdict = grid_dict(field.grid if cascade == 0 else field._c1Grid)
         self.grid = orc.grid_struct(self.gdict)
+        self.g0dict = grid_dict(field.grid)
+        self.grid0 = orc.grid_struct(self.g0dict)
         sc = field._scene
         from speedball_b200.field import selectGiLightRecords
         g = self.gdict
-        recs, analytic, _ = selectGiLightRecords(sc.lights, field._clustered, g["gridMin"],
-                                                 [g["gridMin"][a] + g["gridSize"][a] for a in range(3)])
+        g0 = self.g0dict
+        recs, analytic, _ = selectGiLightRecords(sc.lights, field._clustered, g0["gridMin"],
+                                                 [g0["gridMin"][a] + g0["gridSize"][a] for a in range(3)])
         self.light_count = recs.shape[0]
         self.clustered = field._clustered
-        self.arena = orc.light_arena(recs, self.clustered, g)
+        self.arena = orc.light_arena(recs, self.clustered, g0)
         self.fp32 = fp32
         self.irr, self.depth, self.atlas, self.depth_atlas = orc.new_state(g, fp32)
 
@@ -84,15 +88,15 @@ class OracleMirror:
         if replay is not None:
             io.replayTri = orc._p(replay["tri"]); io.replayInst = orc._p(replay["inst_word"])
             io.replayBlocked = orc._p(replay["blocked"])
-        orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid,
+        orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid0,
                   self.params() if params is None else params,
                   offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io)
         return out
 
 
-def gpu_records(field: ProbeField, n: int) -> dict:
-    hits = read(field, "HIT_RECORDS", n * 4, np.uint32).reshape(n, 4)
-    vis = read(field, "VISIBILITY", n * 4, np.uint32).reshape(n, 4)
+def gpu_records(field: ProbeField, n: int, cascade: int = 0) -> dict:
+    hits = read(field, "HIT_RECORDS", n * 4, np.uint32, cascade).reshape(n, 4)
+    vis = read(field, "VISIBILITY", n * 4, np.uint32, cascade).reshape(n, 4)
     tri = hits[:, 0].view(np.int32).copy()
     word = hits[:, 1].copy()
     inst = np.where(tri >= 0, word & 0x7FFFFFFF, 0xFFFFFFFF).astype(np.uint32).view(np.int32)
@@ -226,20 +230,21 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
     ray of the solve), then the oracle's replay of the GPU's hit and shadow
     decisions advances its state; irradiance and depth atlases within 1e-3."""
     off, upd = frame["probeOffset"], frame["updatedCount"]
+    ci = mirror.cascade
     n = upd * f.getRays()
-    rec = gpu_records(f, n)
+    rec = gpu_records(f, n, ci)
     saved = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy())
     ind = mirror.solve(off, upd, replay=None, params=sched_params)
     mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = saved
     ro, rd = orc.probe_rays(mirror.grid, sched_params[0], off, upd)
-    g_ro, g_rd = gpu_probe_rays(f, off, upd)
+    g_ro, g_rd = gpu_probe_rays(f, off, upd, ci)
     counts = check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], ind["tri"], ind["inst"],
                         ind["rays"][3::4], g_ro, g_rd)
     mirror.solve(off, upd, replay=rec, params=sched_params)
-    ga = half_to_f(read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16))
+    ga = half_to_f(read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16, ci))
     oa = half_to_f(mirror.atlas.reshape(-1))
     err = texel_rel_err(ga, oa)
-    gd = half_to_f(read(f, "DEPTH_ATLAS", mirror.depth_atlas.size, np.uint16))
+    gd = half_to_f(read(f, "DEPTH_ATLAS", mirror.depth_atlas.size, np.uint16, ci))
     od = half_to_f(mirror.depth_atlas.reshape(-1))
     derr = texel_rel_err(gd, od)
     assert err.max() <= TEXEL_REL, (err.max(), int((err > TEXEL_REL).sum()))

@@ -116,7 +116,7 @@ def test_scene_with_gpu_built_blases_matches_oracle():
     from speedball_b200.field import ProbeField
     s = synth.room_spheres(0)
     g = s.meta["grid"]
-    f = ProbeField(s, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+    f = ProbeField(s, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
                    hysteresis=s.meta.get("hysteresis"), recordHits=True, blasBuilder="gpu")
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)

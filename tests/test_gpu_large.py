@@ -32,7 +32,7 @@ BLOCK = 64
 def large():
     scene = synth.large_scene()
     g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), rays=g["rays"],
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
                    clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", recordHits=True)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)

@@ -133,3 +133,73 @@ def test_partial_updates_parity(case):
         assert min(exps) < 1.0
     finally:
         f.dispose()
+
+
+def test_fine_box_placement_matches_oracle():
+    """fitFineBox on the GPU-resident pool equals the oracle's float64
+    restatement bit for bit, and C1's resolution follows the reference's rule."""
+    for s in (synth.atrium(1), synth.room_spheres(0), synth.atrium(3)):
+        g = s.meta["grid"]
+        f = gu.ProbeField(s, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=2,
+                          rays=g["rays"], clusteredLighting=s.meta.get("clustered", False))
+        try:
+            pool = f.pool
+            mn, size = f._c0Box
+            box_size = [(mn[a] + size[a]) - mn[a] for a in range(3)]
+            want = orc.fit_fine_box(pool.vertexData, pool.triIndex, mn, box_size)
+            assert want is not None and f.hasFineCascade()
+            got_min, got_size, got_box = f._c1Box
+            assert got_box == box_size
+            assert got_min == list(want[0]) and got_size == list(want[1]), (got_min, got_size, want)
+            res = orc.fine_cascade_res(want[1], f._targetLongAxis, f._probeTotal)
+            assert [f._c1Grid.res[a] for a in range(3)] == res
+        finally:
+            f.dispose()
+
+
+def _tick2(f, sched, now_ms):
+    frame = f.tick(nowMs=now_ms)
+    f.synchronize()
+    want = sched.tick(now_ms)
+    got = frame["solves"]
+    assert [(x["cascade"], x["probeOffset"], x["updatedCount"]) for x in got] == \
+           [(w["cascade"], w["probeOffset"], w["updatedCount"]) for w in want]
+    prms = []
+    for x, w in zip(got, want):
+        assert np.float32(x["hysteresisExponent"]) == np.float32(w["hysteresisExponent"]), (x, w)
+        prm = f._params.to_array()
+        prm[IDX_EXPONENT] = np.float32(w["hysteresisExponent"])
+        assert prm[IDX_JITTER] == np.float32(w["frameJitter"])
+        prms.append(prm)
+    return got, prms
+
+
+@pytest.mark.parametrize("budget", ["both", "alternating"])
+def test_fine_cascade_parity(budget):
+    """The atrium with its fitted fine cascade C1 (clustered NEE through C0's
+    cell lists, each cascade's own bounce atlas): with a budget covering both
+    cascades every tick solves C0 then C1; with the default 98,304-ray budget
+    the cascades alternate with partial updates, and the exponent of a
+    cascade's first solve falls back to twice the tick interval. Every solve
+    is checked against the oracle (schedule, hit IDs ray by ray, texels)."""
+    s = synth.atrium(1)
+    g = s.meta["grid"]
+    f = gu.ProbeField(s, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=2,
+                      rays=g["rays"], clusteredLighting=True, hysteresis=s.meta["hysteresis"], recordHits=True)
+    try:
+        assert f.hasFineCascade()
+        f.setHysteresisNormalization(True)
+        if budget == "both":
+            f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)
+        mirrors = [gu.OracleMirror(f, cascade=0), gu.OracleMirror(f, cascade=1)]
+        sched = orc.Schedule2([f._probeTotal, f.cascadeProbes(1)], f.getRays(), f._rayBudget, f._maxProbesPerTick,
+                              False, True)
+        seen = set()
+        for k in range(4):
+            got, prms = _tick2(f, sched, 100.0 + 5.0 * k)
+            for x, prm in zip(got, prms):
+                seen.add(x["cascade"])
+                gu.solve_parity(f, mirrors[x["cascade"]], x, prm)
+        assert seen == {0, 1}
+    finally:
+        f.dispose()

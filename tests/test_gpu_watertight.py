@@ -26,7 +26,7 @@ def _field(scene, variant):
     from speedball_b200.field import ProbeField
     m = scene.meta
     g = m["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]),
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1,
                    rays=g["rays"], clusteredLighting=m.get("clustered", False), hysteresis=m.get("hysteresis"),
                    jitterMode="gated", recordHits=True, variant=variant)
     f.setHysteresisNormalization(False)
