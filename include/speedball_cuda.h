@@ -137,9 +137,11 @@ typedef enum sb_buffer {
                                       left unblocked (lo, hi), bit = light index 0..63   */
     SB_BUF_TLAS_ORDER = 13,        /* u32, slot -> source instance                       */
     SB_BUF_INSTANCE_BOUNDS = 14,   /* f32, 6 per slot (liveInstanceBounds)               */
-    SB_BUF_RECORD_E = 15           /* f32, 4 per interior texel (rgb, 1), probeTotal*36:
+    SB_BUF_RECORD_E = 15,          /* f32, 4 per interior texel (rgb, 1), probeTotal*36:
                                       the FP32 upload output of the last solve of the
                                       last sb_forward_record (read-only)                 */
+    SB_BUF_EMITTER_VIS = 16        /* f32, 16 per probe: giEmitter visibility history
+                                      (per cascade, read-only)                          */
 } sb_buffer;
 
 /* Ranged host->device write into a reference buffer (the copySceneStorageRanges /
@@ -164,7 +166,15 @@ sb_status sb_read_buffer_async(sb_ctx* ctx, uint32_t which, uint32_t start, uint
 /* Light records of stride 17 (collectLights, spectral_scene.js:724-813), already
  * selected into the fixed arena by the host (fillLegacyLightArena /
  * fillGiLightArena, gi_probes.js:4297-4349). clustered != 0 builds the C0 cell
- * lists on device (lightGridKernel, gi_probes.js:1888-1938) from cascade 0's grid. */
+ * lists on device (lightGridKernel, gi_probes.js:1888-1938) from cascade 0's grid.
+ * Records [emitterBase, emitterBase + emitterCount) are giEmitter spheres (type
+ * 3: centre [1..3], surface radiance [7..9], radius [14], projected area A/4
+ * [15]; collectEmitterRecords, spectral_scene.js:815-888), at most 16: every
+ * sb_solve then runs emitterVisKernel (a shadow ray per updated probe and
+ * emitter into a visibility history of retention 0.8, gi_probes.js:2216-2260)
+ * and the blend adds each emitter as virtual rays (2262-2310). NEE skips them.
+ * Batched solves and the adjoint return SB_ERR_UNSUPPORTED while emitters are
+ * uploaded. */
 sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count,
                            uint32_t emitterBase, uint32_t emitterCount, int32_t clustered);
 

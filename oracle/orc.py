@@ -37,7 +37,8 @@ class OrcScene(C.Structure):
 
 
 class OrcLights(C.Structure):
-    _fields_ = [("data", C.c_void_p), ("dataLen", C.c_uint32), ("lightCount", C.c_uint32), ("clustered", C.c_int32)]
+    _fields_ = [("data", C.c_void_p), ("dataLen", C.c_uint32), ("lightCount", C.c_uint32), ("clustered", C.c_int32),
+                ("emitterBase", C.c_uint32), ("emitterCount", C.c_uint32)]
 
 
 class OrcGrid(C.Structure):
@@ -49,7 +50,8 @@ class OrcSolveIO(C.Structure):
     _fields_ = [("rayOut", C.c_void_p), ("hitTri", C.c_void_p), ("hitInst", C.c_void_p), ("secondT", C.c_void_p),
                 ("tested", C.c_void_p), ("blocked", C.c_void_p), ("replayTri", C.c_void_p),
                 ("replayInst", C.c_void_p), ("replayBlocked", C.c_void_p), ("rayIn", C.c_void_p),
-                ("preRound", C.c_void_p), ("counters", C.c_void_p), ("hitFacing", C.c_void_p)]
+                ("preRound", C.c_void_p), ("counters", C.c_void_p), ("hitFacing", C.c_void_p),
+                ("emitterVis", C.c_void_p), ("emitterVisReplay", C.c_void_p), ("emitterSampleOut", C.c_void_p)]
 
 
 def load() -> C.CDLL:
@@ -194,10 +196,13 @@ def light_arena(records: np.ndarray, clustered: bool, grid0: dict | None) -> np.
 def solve(scene: OrcScene, arena: np.ndarray, light_count: int, clustered: bool, grid: OrcGrid, grid0: OrcGrid,
           params: np.ndarray, probe_offset: int, updated: int, irr: np.ndarray, depth: np.ndarray,
           atlas: np.ndarray, depth_atlas: np.ndarray, fp32: bool = False, io: OrcSolveIO | None = None,
-          nthreads: int | None = None) -> None:
+          nthreads: int | None = None, emitters: tuple = (0, 0)) -> None:
+    """One solve; `emitters` = (emitterBase, emitterCount) of the arena's
+    giEmitter records, whose visibility history lives in io.emitterVis."""
     lib = load()
     L = OrcLights()
     L.data = _p(arena); L.dataLen = arena.shape[0]; L.lightCount = light_count; L.clustered = 1 if clustered else 0
+    L.emitterBase, L.emitterCount = int(emitters[0]), int(emitters[1])
     prm = np.ascontiguousarray(params, np.float64)
     assert prm.shape[0] == lib.orc_params_size()
     f = lib.orc_solve_f32 if fp32 else lib.orc_solve_f64

@@ -19,7 +19,10 @@ struct OrcScene {
     const float* materials; uint32_t materialsLen;
     uint32_t instBase, instCount, tlasBase, tlasNodeCount;
 };
-struct OrcLights { const float* data; uint32_t dataLen; uint32_t lightCount; int32_t clustered; };
+struct OrcLights {
+    const float* data; uint32_t dataLen; uint32_t lightCount; int32_t clustered;
+    uint32_t emitterBase, emitterCount;
+};
 struct OrcGrid { double gridMin[3], gridSize[3]; uint32_t res[3]; uint32_t rays; double maxDist, cellMin; };
 
 // Optional per-ray outputs / replay inputs of a solve. Any pointer may be null.
@@ -33,6 +36,10 @@ struct OrcSolveIO {
     void* preRound;           // R[probeTotal*36*3]: unrounded upload RGB
     uint64_t* counters;       // [tlasNodes, instances, blasNodes, triTests] (primary + shadow)
     int32_t* hitFacing;       // per ray: 1 front, 0 back, -1 miss
+    void* emitterVis;         // R[probeTotal*16]: emitter visibility history (in/out), or null
+    const void* emitterVisReplay;  // R[probeTotal*16]: the GPU's history after the solve, taken for the
+                                   // updated probes before the blend (replay), or null
+    void* emitterSampleOut;   // R[updated*16]: this solve's own visibility samples, or null
 };
 
 
@@ -244,6 +251,7 @@ static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, 
     std::memcpy(&P, params, sizeof(Params));
     Lights L;
     L.data = l->data; L.dataLen = l->dataLen; L.lightCount = l->lightCount; L.clustered = l->clustered;
+    L.emitterBase = l->emitterBase; L.emitterCount = l->emitterCount;
     const uint32_t N = g.rays, total = g.probeTotal();
     if (updated > total) updated = total;
     const size_t nr = (size_t)updated * N;
@@ -282,9 +290,34 @@ static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, 
         if (io && io->rayOut) std::memcpy(io->rayOut, rays.data(), nr * 4 * sizeof(R));
     }
     R* pre = io ? static_cast<R*>(io->preRound) : nullptr;
+    // emitterVisKernel (gi_probes.js:2216-2260), after the trace and before the blend
+    R* evis = io ? static_cast<R*>(io->emitterVis) : nullptr;
+    if (evis && L.emitterCount) {
+        const uint32_t EC = GI_EMITTER_INJECT_CAP;
+        R* sampleOut = static_cast<R*>(io->emitterSampleOut);
+        parallel_for((size_t)updated * EC, std::max(1, threads), [&](size_t i, int) {
+            uint32_t slot = (uint32_t)(i / EC), e = (uint32_t)(i % EC);
+            if (e >= L.emitterCount) return;
+            uint32_t p = (uint32_t)((probeOffset + slot) % total);
+            R smp = emitter_sample<R>(sc, L, g, P, p, e);
+            if (sampleOut) sampleOut[i] = smp;
+            R& v = evis[(size_t)p * EC + e];
+            v = smp * (R(1) - R(GI_EMITTER_VIS_RETENTION)) + v * R(GI_EMITTER_VIS_RETENTION);
+        });
+        if (io->emitterVisReplay) {
+            const R* rv = static_cast<const R*>(io->emitterVisReplay);
+            for (uint32_t slot = 0; slot < updated; ++slot) {
+                uint32_t p = (uint32_t)((probeOffset + slot) % total);
+                for (uint32_t e = 0; e < EC; ++e) evis[(size_t)p * EC + e] = rv[(size_t)p * EC + e];
+            }
+        }
+    }
+    EmitterInject<R> inj;
+    inj.L = &L;
+    inj.vis = evis;
     parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
         uint32_t p = (uint32_t)((probeOffset + slot) % total);
-        blend_probe<R>(g, P, rayBuf + slot * N * 4, p, irr, depth);
+        blend_probe<R>(g, P, rayBuf + slot * N * 4, p, irr, depth, evis ? &inj : nullptr);
     });
     // the upload runs after every blend of the solve (separate kernel)
     parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {

@@ -31,7 +31,11 @@ struct Lights {
     uint32_t dataLen = 0;
     uint32_t lightCount = 0;
     int clustered = 0;
+    uint32_t emitterBase = 0, emitterCount = 0;  // the giEmitter records (type 3), after the analytic ones
 };
+
+constexpr uint32_t GI_EMITTER_INJECT_CAP = 16;      // gi_probes.js:133
+constexpr double GI_EMITTER_VIS_RETENTION = 0.8;    // gi_probes.js:134
 
 // One ray's outputs. hitT = -1 on a miss (gi_probes.js:1987, 2209-2213).
 template <class R> struct RayOut {
@@ -359,7 +363,47 @@ inline int gutter_source_lane(int lane) {
 // blendKernel (gi_probes.js:2317-2532) for one probe slot: reads the slot's rays
 // (rgb + hitT, 4 per ray), updates the irradiance (4/texel) and depth (2/texel)
 // histories of its 36 interior texels.
-template <class R> void blend_probe(const Grid& g, const Params& P, const R* rays, uint32_t probeIndex, R* irr, R* depth) {
+// emitterVisKernel's sample for (probe, emitter) (gi_probes.js:2216-2260): a
+// shadow ray from the probe to a point of the emitter's disk (a sin hash of
+// the probe, the emitter and the epoch seed, evaluated in float32 as the GPU
+// does), 1 when unblocked. With sourceRadius 0 the point is the centre.
+template <class R> R emitter_sample(const Scene& s, const Lights& L, const Grid& g, const Params& P, uint32_t probeIndex,
+                                    uint32_t e) {
+    const float* rec = L.data + (size_t)(L.emitterBase + e) * LIGHT_STRIDE;
+    const V3<R> ro = probe_world_pos<R>(g, probeIndex);
+    const V3<R> center = V3<R>(R(rec[1]), R(rec[2]), R(rec[3]));
+    R sourceRadius = std::max(R(rec[14]), R(0));
+    V3<R> axis = center - ro;
+    R dist = length(axis);
+    if (!(dist > std::max(sourceRadius, R(1e-3)))) return R(0);
+    V3<R> d = axis * (R(1) / dist);
+    V3<R> up = std::fabs(d.y) < R(0.999) ? V3<R>(R(0), R(1), R(0)) : V3<R>(R(1), R(0), R(0));
+    V3<R> tangent = normalize(cross(up, d));
+    V3<R> bitangent = cross(d, tangent);
+    const float seed = (float(probeIndex) * 12.9898f + float(e) * 78.233f) + float(P.emitterVisSeed) * 37.719f;
+    const float h0 = std::sin(seed) * 43758.5453f;
+    const float h1 = std::sin(seed + 19.19f) * 24634.6345f;
+    const float u = h0 - std::floor(h0), v = h1 - std::floor(h1);
+    R diskRadius = std::sqrt(R(u)) * sourceRadius;
+    R diskAngle = R(v) * R(2.0 * PI);
+    V3<R> target = center + (tangent * (std::cos(diskAngle) * diskRadius) + bitangent * (std::sin(diskAngle) * diskRadius));
+    V3<R> sdir = normalize(target - ro);
+    R traceBias = std::max(R(g.cellMin) * R(TRACE_SURFACE_BIAS_CELL) * R(P.debugTraceBiasScale),
+                           R(RAY_EPS) * R(P.debugRayEpsScale));
+    Traverser<R> tr(s);
+    bool blocked = tr.any(ro, sdir, std::max(dist - sourceRadius - traceBias, R(1e-4)));
+    return blocked ? R(0) : R(1);
+}
+
+// The emitters a blend injects as virtual rays (injectEmitterVirtualRays,
+// gi_probes.js:2262-2310): the records and this probe's visibility per emitter.
+template <class R> struct EmitterInject {
+    const Lights* L = nullptr;
+    const R* vis = nullptr;  // probeTotal x GI_EMITTER_INJECT_CAP
+};
+
+template <class R> void blend_probe(const Grid& g, const Params& P, const R* rays, uint32_t probeIndex, R* irr, R* depth,
+                                    const EmitterInject<R>* em = nullptr) {
     const uint32_t N = g.rays;
     std::vector<V3<R>> dirs(N);
     for (uint32_t k = 0; k < N; ++k) dirs[k] = ray_dir<R>(k, N, R(P.frameJitter));
@@ -389,6 +433,32 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
             dAcc += rdist * dw;
             dAcc2 += rdist * rdist * dw;
             dwsum += dw;
+        }
+        if (em && em->L && em->L->emitterCount) {
+            // each emitter as kVirtual rays toward its centre, radiance x visibility
+            const V3<R> ro = probe_world_pos<R>(g, probeIndex);
+            for (uint32_t e = 0; e < em->L->emitterCount; ++e) {
+                const float* rec = em->L->data + (size_t)(em->L->emitterBase + e) * LIGHT_STRIDE;
+                const V3<R> center = V3<R>(R(rec[1]), R(rec[2]), R(rec[3]));
+                R sourceRadius = std::max(R(rec[14]), R(0));
+                V3<R> axis = center - ro;
+                R dist = length(axis);
+                if (!(dist > std::max(sourceRadius, R(1e-3)))) continue;
+                V3<R> d = axis * (R(1) / dist);
+                R projArea = std::max(R(rec[15]), R(0));
+                R Omega = std::min(R(2.0 * PI), projArea / (dist * dist));
+                R kVirtual = std::min(R(N), R(N) * Omega / R(4.0 * PI));
+                R vis = em->vis[(size_t)probeIndex * GI_EMITTER_INJECT_CAP + e];
+                V3<R> Lc = V3<R>(R(rec[7]), R(rec[8]), R(rec[9])) * vis;
+                R cd = std::max(dot(dir, d), R(0));
+                R w = std::pow(cd, std::max(R(P.debugCosinePower), R(1e-4)));
+                R wk = w * kVirtual;
+                acc = acc + Lc * wk;
+                wsum += wk;
+                R lum = luma(Lc);
+                lAcc += lum * wk;
+                lAcc2 += lum * lum * wk;
+            }
         }
         R wden = std::max(wsum, R(1e-4));
         V3<R> meanRad(acc.x / wden, acc.y / wden, acc.z / wden);

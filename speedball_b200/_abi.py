@@ -31,7 +31,7 @@ SB_CTX_RECORD_HITS = 1
 BUF = dict(
     BVH_NODES=0, TRI_INDEX=1, VERTEX_DATA=2, TRI_MATERIAL=3, MATERIALS=4, LIGHTS=5,
     IRRADIANCE_HISTORY=6, DEPTH_HISTORY=7, IRRADIANCE_ATLAS=8, DEPTH_ATLAS=9, RAY_DATA=10,
-    HIT_RECORDS=11, VISIBILITY=12, TLAS_ORDER=13, INSTANCE_BOUNDS=14, RECORD_E=15,
+    HIT_RECORDS=11, VISIBILITY=12, TLAS_ORDER=13, INSTANCE_BOUNDS=14, RECORD_E=15, EMITTER_VIS=16,
 )
 
 

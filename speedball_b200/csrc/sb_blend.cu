@@ -130,6 +130,33 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
     dws = S.dwsum[lane];
 
     const uint32_t probeIndex = live ? (C.probeOffset + slot) % C.probeTotal : 0u;
+    if (live && C.emitterCount) {
+        // injectEmitterVirtualRays (gi_probes.js:2262-2310): each emitter as
+        // kVirtual = min(N, N Omega / 4 pi) rays toward its centre carrying its
+        // radiance x visibility, Omega = min(2 pi, projectedArea / d^2)
+        const float3 ro = probe_world_pos(C, probeIndex);
+        const float4 td = S.texDir[lane];
+        for (uint32_t e = 0; e < C.emitterCount; ++e) {
+            const float* L = C.lights + (size_t)(C.emitterBase + e) * 17u;
+            const float3 axis = mk(L[1], L[2], L[3]) - ro;
+            const float dist = sqrtf(dot3(axis, axis));
+            if (!(dist > fmaxf(fmaxf(L[14], 0.0f), 1e-3f))) continue;
+            const float3 d = axis * (1.0f / dist);
+            const float omega = fminf(6.283185307179586f, fmaxf(L[15], 0.0f) / (dist * dist));
+            const float kVirtual = fminf(float(N), float(N) * omega / 12.566370614359172f);
+            const float vis = C.emitterVis[(size_t)probeIndex * EMITTER_CAP + e];
+            const float3 Lc = mk(L[7] * vis, L[8] * vis, L[9] * vis);
+            const float cdot = fmaxf(td.x * d.x + td.y * d.y + td.z * d.z, 0.0f);
+            const float wk = (cosUnit ? cdot : powf(cdot, cosPow)) * kVirtual;
+            const float lum = luma3(Lc);
+            kahan_fma(sr, cr, wk, Lc.x);
+            kahan_fma(sg, cg, wk, Lc.y);
+            kahan_fma(sb, cb, wk, Lc.z);
+            kahan_fma(sl, cl, wk, lum);
+            kahan_fma(sl2, cl2, wk, lum * lum);
+            ws += wk;
+        }
+    }
     if (live) {
         const uint32_t lx = lane % OCT + BORDER, ly = lane / OCT + BORDER;
         const uint32_t local = ly * TILE + lx;

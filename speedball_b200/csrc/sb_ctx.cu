@@ -43,6 +43,7 @@ struct Cascade {
     uint32_t* batchOrder = nullptr;
     size_t batchCap = 0;
     bool batchOrderReady = false;
+    float* emitterVis = nullptr;  // probeTotal x 16 emitter visibility history
 };
 
 }  // namespace
@@ -267,6 +268,10 @@ DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint3
     D.atlas = K.atlas;
     D.depthAtlas = K.depthAtlas;
     D.eOut = c->recordE;
+    D.lights = c->B.lights;
+    D.emitterBase = c->emitterBase;
+    D.emitterCount = c->emitterCount;
+    D.emitterVis = K.emitterVis;
     return D;
 }
 
@@ -435,6 +440,7 @@ void sb_destroy(sb_ctx* ctx) {
     release(I.scratch); release(ctx->instOwner); release(ctx->dStage); release(ctx->dStageM);
     for (auto& K : ctx->casc) {
         release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.rayData); release(K.hits);
+        release(K.emitterVis);
         release(K.tileOrder); release(K.batchCost); release(K.batchOrder);
         release(K.vis);
     }
@@ -656,6 +662,7 @@ static sb_status read_enqueue(sb_ctx* ctx, uint32_t which, uint32_t start, uint3
         case SB_BUF_TLAS_ORDER: srcp = ctx->I.order; len = ctx->instancesSet ? ctx->I.count : 0; break;
         case SB_BUF_INSTANCE_BOUNDS: srcp = ctx->I.liveBounds; len = ctx->instancesSet ? (size_t)ctx->I.count * 6 : 0; break;
         case SB_BUF_RECORD_E: srcp = ctx->tape.E; len = ctx->tape.ready ? (size_t)ctx->tape.probes * 36 * 4 : 0; break;
+        case SB_BUF_EMITTER_VIS: if (K) { srcp = K->emitterVis; len = K->emitterVis ? (size_t)K->probeTotal * EMITTER_CAP : 0; } break;
         default: return fail(ctx, SB_ERR_INVALID_ARG, "unknown buffer %u", buf);
     }
     if (!srcp) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not available", buf);
@@ -680,8 +687,12 @@ sb_status sb_upload_lights(sb_ctx* ctx, const float* records, uint32_t count, ui
                            uint32_t emitterCount, int32_t clustered) {
     if (!ctx || (!records && count)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     if (count > SB_MAX_LIGHTS) return fail(ctx, SB_ERR_INVALID_ARG, "%u lights > %u", count, SB_MAX_LIGHTS);
-    if (emitterCount > 0)
-        return fail(ctx, SB_ERR_UNSUPPORTED, "giEmitter records (emitter visibility / virtual rays) are not built");
+    if (emitterCount > EMITTER_CAP) return fail(ctx, SB_ERR_INVALID_ARG, "%u emitters > %u", emitterCount, EMITTER_CAP);
+    if (emitterCount && (uint64_t)emitterBase + emitterCount > count)
+        return fail(ctx, SB_ERR_INVALID_ARG, "emitter records [%u,+%u) outside the %u records", emitterBase, emitterCount, count);
+    for (uint32_t e = 0; e < emitterCount; ++e)
+        if (std::fabs(records[(size_t)(emitterBase + e) * SB_LIGHT_STRIDE] - 3.0f) >= 0.5f)
+            return fail(ctx, SB_ERR_INVALID_ARG, "record %u in the emitter range is not a giEmitter (type 3)", emitterBase + e);
     cudaSetDevice(ctx->device);
     uint32_t cells = 0;
     if (clustered) {
@@ -729,7 +740,10 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
     size_t rays = (size_t)probeTotal * g->raysPerProbe;
     if (!sameDims) {
         release(K.irr); release(K.depth); release(K.atlas); release(K.depthAtlas); release(K.tileOrder);
+        release(K.emitterVis);
         size_t c = 0;
+        CK(grow(K.emitterVis, c, (size_t)probeTotal * EMITTER_CAP)); c = 0;
+        CK(cudaMemsetAsync(K.emitterVis, 0, (size_t)probeTotal * EMITTER_CAP * sizeof(float), ctx->stream));
         CK(grow(K.irr, c, (size_t)probeTotal * 64)); c = 0;
         CK(grow(K.depth, c, (size_t)probeTotal * 64)); c = 0;
         CK(grow(K.atlas, c, (size_t)probeTotal * 64)); c = 0;
@@ -848,6 +862,7 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
                         ctx->stream, ctx->jobs, ctx->jobCap, s0, n, timing ? ctx->evA : nullptr,
                         timing ? ctx->evB : nullptr));
     }
+    if (ctx->emitterCount) CK(launch_emitter_vis(S, D, P, ctx->dErr, ctx->stream));
     if (timing) CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
     if (costOrder) K.batchOrderReady = true;
@@ -993,6 +1008,8 @@ static sb_status check_batch(const sb_solve_item* items, uint32_t count) {
     for (uint32_t i = 0; i < count; ++i) {
         sb_ctx* c = items[i].ctx;
         if (!c || c->device != lead->device) return fail(lead, SB_ERR_INVALID_ARG, "item %u: null context or another device", i);
+        if (c->emitterCount)
+            return fail(lead, SB_ERR_UNSUPPORTED, "item %u: giEmitter records are solved by sb_solve only", i);
         for (uint32_t j = 0; j < i; ++j)
             if (items[j].ctx == c && items[j].cascade == items[i].cascade)
                 return fail(lead, SB_ERR_INVALID_ARG, "items %u and %u solve the same cascade", j, i);
@@ -1403,6 +1420,8 @@ sb_status sb_forward_record(sb_ctx* ctx, uint32_t ci, uint32_t solves, const flo
     if (target && !loss) return fail(ctx, SB_ERR_INVALID_ARG, "loss is null");
     if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
         return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
+    if (ctx->emitterCount)
+        return fail(ctx, SB_ERR_UNSUPPORTED, "the adjoint does not cover giEmitter virtual rays");
     cudaSetDevice(ctx->device);
     Cascade& K = ctx->casc[ci];
     auto& T = ctx->tape;

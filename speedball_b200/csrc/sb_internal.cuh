@@ -123,7 +123,14 @@ struct DevCascade {
     const uint32_t* batchOrder;
     uint32_t* batchCost;
     uint32_t* batchOrderOut;
+    // giEmitter records (type 3) and this cascade's emitter visibility history,
+    // probeTotal x EMITTER_CAP (gi_probes.js:1873, 2216-2310)
+    const float* lights;
+    uint32_t emitterBase, emitterCount;
+    float* emitterVis;
 };
+constexpr uint32_t EMITTER_CAP = 16;          // GI_EMITTER_INJECT_CAP, gi_probes.js:133
+constexpr float EMITTER_VIS_RETENTION = 0.8f;  // GI_EMITTER_VIS_RETENTION, gi_probes.js:134
 
 struct DevParams {
     float frameJitter, emitterVisSeed;

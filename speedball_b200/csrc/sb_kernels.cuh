@@ -173,6 +173,9 @@ cudaError_t launch_fine_hist(const SceneBuffers& B, const double mn[3], const do
                              cudaStream_t st);
 bool fine_box_from_hist(const uint32_t* hist, const double mn[3], const double size[3], double outMin[3],
                         double outSize[3]);
+// emitterVisKernel (sb_trace.cu): one thread per (updated probe, emitter).
+cudaError_t launch_emitter_vis(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
+                               cudaStream_t st);
 // The FP32 probe rays of a solve as the trace forms them (sb_probe_rays).
 cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st);
 

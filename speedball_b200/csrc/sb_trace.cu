@@ -701,6 +701,56 @@ __global__ void k_probe_rays(const DevCascade C, float jitter, float* ro, float*
     ro[3 * i] = o.x; ro[3 * i + 1] = o.y; ro[3 * i + 2] = o.z;
     rd[3 * i] = d.x; rd[3 * i + 1] = d.y; rd[3 * i + 2] = d.z;
 }
+// emitterVisKernel (gi_probes.js:2216-2260): per (updated probe, emitter) a
+// shadow ray from the probe to a point of the emitter's disk, chosen by a sin
+// hash of (probe, emitter, epoch seed) evaluated in separately rounded FP32,
+// folded into the emitter's visibility history with retention 0.8.
+__global__ void k_emitter_vis(DevScene S, DevCascade C, DevParams P, uint32_t* err) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slot = gid / EMITTER_CAP, e = gid % EMITTER_CAP;
+    if (slot >= C.updatedCount || e >= C.emitterCount || !*S.valid) return;
+    const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+    const float3 ro = probe_world_pos(C, probeIndex);
+    const float* L = C.lights + (size_t)(C.emitterBase + e) * 17u;
+    const float3 center = mk(L[1], L[2], L[3]);
+    const float sourceRadius = fmaxf(L[14], 0.0f);
+    const float3 axis = center - ro;
+    const float dist = sqrtf(dot3(axis, axis));
+    float sample = 0.0f;
+    if (dist > fmaxf(sourceRadius, 1e-3f)) {
+        const float3 d = axis * (1.0f / dist);
+        const float3 up = fabsf(d.y) < 0.999f ? mk(0.0f, 1.0f, 0.0f) : mk(1.0f, 0.0f, 0.0f);
+        const float3 tangent = normalize3(cross3(up, d));
+        const float3 bitangent = cross3(d, tangent);
+        const float seed = __fadd_rn(__fadd_rn(__fmul_rn(float(probeIndex), 12.9898f), __fmul_rn(float(e), 78.233f)),
+                                     __fmul_rn(P.emitterVisSeed, 37.719f));
+        const float h0 = __fmul_rn(sinf(seed), 43758.5453f);
+        const float h1 = __fmul_rn(sinf(__fadd_rn(seed, 19.19f)), 24634.6345f);
+        const float u = h0 - floorf(h0), v = h1 - floorf(h1);
+        const float diskRadius = sqrtf(u) * sourceRadius;
+        const float diskAngle = v * 6.283185307179586f;
+        const float3 target = center + (tangent * (cosf(diskAngle) * diskRadius) + bitangent * (sinf(diskAngle) * diskRadius));
+        const float3 sdir = normalize3(target - ro);
+        const float traceBias = fmaxf(C.cellMin * 0.005f * P.debugTraceBiasScale, RAY_EPS * P.debugRayEpsScale);
+        Visits vis = {0, 0, 0, 0};
+        const bool pairs = any_pairs(S);
+        const bool blocked = trace_any(S, pairs ? S.tlasPairs : S.tlas, ro, sdir,
+                                       fmaxf(dist - sourceRadius - traceBias, 1e-4f), vis, err, pairs);
+        sample = blocked ? 0.0f : 1.0f;
+    }
+    float* vp = C.emitterVis + (size_t)probeIndex * EMITTER_CAP + e;
+    *vp = sample * (1.0f - EMITTER_VIS_RETENTION) + *vp * EMITTER_VIS_RETENTION;
+}
+
+cudaError_t launch_emitter_vis(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
+                               cudaStream_t st) {
+    const uint32_t n = C.updatedCount * EMITTER_CAP;
+    if (n == 0 || C.emitterCount == 0) return cudaSuccess;
+    k_emitter_vis<<<(n + 127) / 128, 128, 0, st>>>(S, C, P, err);
+    note_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_probe_rays(const DevCascade& C, float jitter, float* ro, float* rd, cudaStream_t st) {
     const uint32_t n = C.updatedCount * C.rays;
     if (n == 0) return cudaSuccess;

@@ -185,6 +185,42 @@ def room_spheres(seed: int = 0, n_materials: int = 16, n_point: int = 4, n_dir: 
                      meta=dict(grid=grid, clustered=False, hysteresis=0.97, jitter="gated", seed=seed))
 
 
+def emitter_record(center, radiance, radius: float, proj_area: float) -> np.ndarray:
+    """A giEmitter light record (collectEmitterRecords, spectral_scene.js:815-888):
+    type 3, centre, surface radiance, range from power, radius, A/4."""
+    rng_ = float(np.sqrt(max(0.0, *radiance) * proj_area / 0.005))
+    return np.array([3, *center, 0, 0, -1, *radiance, rng_, 2, -1, -1, radius, proj_area, 0], dtype=np.float32)
+
+
+def add_emitters(scene: SceneDesc, seed: int = 5, sphere: int = 1, points: int = 2) -> SceneDesc:
+    """Emissive giEmitter lights for a room scene: icosphere instance `sphere`
+    gets its own emissive material and a sphere emitter record (its bounding
+    radius and A/4 of its world surface), plus `points` free point-like
+    emitters of radius 0 (their visibility rays end at their centres)."""
+    rng = np.random.default_rng(seed)
+    mats = np.asarray(scene.materials, np.float32).reshape(-1, 28)
+    inst = scene.instances[sphere]
+    mesh = scene.meshes[inst.mesh]
+    radiance = tuple(float(x) for x in rng.uniform(2.0, 6.0, 3))
+    rec = material_record((0.8, 0.8, 0.8), emissive=radiance)
+    mats = np.concatenate([mats, rec[None]], 0)
+    mesh.tri_material = np.full(mesh.indices.shape[0], mats.shape[0] - 1, np.uint32)
+    W = np.asarray(inst.world, np.float64)
+    P = mesh.positions.astype(np.float64) @ W[:3, :3].T + W[:3, 3]
+    tri = P[mesh.indices.astype(np.int64)]
+    area = float(np.linalg.norm(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]), axis=1).sum() * 0.5)
+    center = W[:3, 3]
+    radius = float(np.linalg.norm(P - center, axis=1).max())
+    recs = [emitter_record(tuple(center), radiance, radius, area / 4.0)]
+    for _ in range(points):
+        recs.append(emitter_record(tuple(rng.uniform(1.0, 9.0, 3)), tuple(float(x) for x in rng.uniform(2, 5, 3)),
+                                   0.0, float(rng.uniform(0.1, 0.4))))
+    scene.materials = mats
+    scene.lights = np.concatenate([np.asarray(scene.lights, np.float32).reshape(-1, 17), np.stack(recs)], 0)
+    scene.meta = dict(scene.meta, emitters=len(recs))
+    return scene
+
+
 ATRIUM_TRIS = 262_267
 
 

@@ -63,21 +63,32 @@ class OracleMirror:
         from speedball_b200.field import selectGiLightRecords
         g = self.gdict
         g0 = self.g0dict
-        recs, analytic, _ = selectGiLightRecords(sc.lights, field._clustered, g0["gridMin"],
-                                                 [g0["gridMin"][a] + g0["gridSize"][a] for a in range(3)])
+        recs, analytic, n_emit = selectGiLightRecords(sc.lights, field._clustered, g0["gridMin"],
+                                                      [g0["gridMin"][a] + g0["gridSize"][a] for a in range(3)])
+        self.emitters = (analytic, n_emit)
         self.light_count = recs.shape[0]
         self.clustered = field._clustered
         self.arena = orc.light_arena(recs, self.clustered, g0)
         self.fp32 = fp32
         self.irr, self.depth, self.atlas, self.depth_atlas = orc.new_state(g, fp32)
+        r = g["res"]
+        self.evis = np.zeros(r[0] * r[1] * r[2] * 16, np.float32 if fp32 else np.float64)
 
     def params(self) -> np.ndarray:
         return self.field._params.to_array()
 
     def solve(self, offset: int, updated: int, replay: dict | None = None, want: bool = True,
-              params: np.ndarray | None = None):
+              params: np.ndarray | None = None, evis_replay: np.ndarray | None = None):
         n = updated * self.gdict["rays"]
         io = orc.OrcSolveIO()
+        self.evis_samples = None
+        if self.emitters[1]:
+            io.emitterVis = orc._p(self.evis)
+            self.evis_samples = np.zeros(updated * 16, self.evis.dtype)
+            io.emitterSampleOut = orc._p(self.evis_samples)
+            if evis_replay is not None:
+                self._evis_replay = np.ascontiguousarray(evis_replay, self.evis.dtype)
+                io.emitterVisReplay = orc._p(self._evis_replay)
         out = {}
         if want:
             out = dict(rays=np.zeros(n * 4, np.float32 if self.fp32 else np.float64), tri=np.zeros(n, np.int32),
@@ -90,7 +101,7 @@ class OracleMirror:
             io.replayBlocked = orc._p(replay["blocked"])
         orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid0,
                   self.params() if params is None else params,
-                  offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io)
+                  offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io, emitters=self.emitters)
         return out
 
 
@@ -233,14 +244,29 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
     ci = mirror.cascade
     n = upd * f.getRays()
     rec = gpu_records(f, n, ci)
-    saved = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy())
+    saved = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy(),
+             mirror.evis.copy())
     ind = mirror.solve(off, upd, replay=None, params=sched_params)
-    mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas = saved
+    samples = mirror.evis_samples
+    mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas, evis_before = saved
+    mirror.evis[...] = evis_before
+    gpu_evis = None
+    if mirror.emitters[1]:
+        # the GPU's visibility history after this solve, and the samples it implies
+        # (after = 0.2 sample + 0.8 before, gi_probes.js:2258-2259)
+        gpu_evis = read(f, "EMITTER_VIS", mirror.evis.size, np.float32, ci).astype(np.float64)
+        probes = (off + np.arange(upd)) % (mirror.evis.size // 16)
+        ne = mirror.emitters[1]
+        before = evis_before.reshape(-1, 16)[probes, :ne]
+        after = gpu_evis.reshape(-1, 16)[probes, :ne]
+        g_samp = np.rint((after - np.float32(0.8) * before) / np.float32(0.2))
+        o_samp = samples.reshape(upd, 16)[:, :ne]
+        emitter_agree = (g_samp == o_samp).mean(axis=0)
     ro, rd = orc.probe_rays(mirror.grid, sched_params[0], off, upd)
     g_ro, g_rd = gpu_probe_rays(f, off, upd, ci)
     counts = check_hits(mirror.scene, ro, rd, rec["tri"], rec["inst"], rec["t"], ind["tri"], ind["inst"],
                         ind["rays"][3::4], g_ro, g_rd)
-    mirror.solve(off, upd, replay=rec, params=sched_params)
+    mirror.solve(off, upd, replay=rec, params=sched_params, evis_replay=gpu_evis)
     ga = half_to_f(read(f, "IRRADIANCE_ATLAS", mirror.atlas.size, np.uint16, ci))
     oa = half_to_f(mirror.atlas.reshape(-1))
     err = texel_rel_err(ga, oa)
@@ -251,4 +277,6 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
     assert derr.max() <= TEXEL_REL, (derr.max(), int((derr > TEXEL_REL).sum()))
     counts.update(irr_err=float(err.max()), depth_err=float(derr.max()), lit=float(np.abs(oa).max()),
                   hit_share=float((rec["tri"] >= 0).mean()))
+    if gpu_evis is not None:
+        counts["emitter_sample_agreement"] = [float(x) for x in emitter_agree]
     return counts
