@@ -52,7 +52,7 @@ def parse():
                     help="atrium: the plain probe update (headline); adjoint: one gradient evaluation of the "
                          "differentiated update (64 materials, 32 point lights, 2 feedback solves); batch: 3 "
                          "nested cascades of the atrium + 8 independent atria per frame, batched vs plain; "
-                         "large: 2.1M unique / 12.8M instanced triangles, 32^3 probes x 256 rays x 2 cascades, "
+                         "large: 2.1M unique / 12.8M instanced triangles, C0 32^3 probes + fitted fine cascade C1, 256 rays, "
                          "binary vs 8-wide scene BVH vs the reference two-level walk")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-aux", action="store_true",
@@ -941,6 +941,7 @@ def run_build(args, dist: Dist):
     clocks = Clocks(device)
     clocks.start()
     total = 0.0
+    l0 = _stats(lib, h).kernelLaunches
     for _ in range(K):
         ck(rt.cudaEventRecord(e0, stream))
         step()
@@ -948,6 +949,7 @@ def run_build(args, dist: Dist):
         ck(rt.cudaEventSynchronize(e1))
         total += ck(rt.cudaEventElapsedTime(e0, e1))
     clk = clocks.stop()
+    launches = _stats(lib, h).kernelLaunches - l0
     _abi.check(lib.sb_synchronize(h), h)
     ms = dist.max(total / K)
     # the largest mesh alone
@@ -991,7 +993,7 @@ def run_build(args, dist: Dist):
         "host_builder_ms_all": round(host_ms, 1), "oracle_meshbvh_ms_all": round(orc_ms, 1),
         "cpu_baseline": {"value": round(tris / (orc_ms * 1e-3) / 1e6, 3), "unit": "Mtris/s", "cores": 1,
                          "kind": "port", "sample": "the oracle's MeshBVH restatement (one thread) on every mesh once"},
-        "gpu_launches": None,
+        "gpu_launches": int(launches),
         "clocks": clk,
     }
     return line
@@ -1002,19 +1004,12 @@ LARGE_METRIC = "probe Mrays/s (large scene, 2 cascades)"
 
 def large_field(device):
     """The large scene's field: 32^3 probes x 256 rays over the world box, and
-    a second cascade of 32^3 probes over the half-extent box around its
-    centre; clustered lights, gated jitter, full updates."""
+    the fine cascade C1 that fitFineBox places inside it (the reference's
+    two-cascade install, divisions 32 so that C1 may reach the 32-per-axis
+    cap); clustered lights, gated jitter, full updates."""
     from speedball_b200 import synth
-    from speedball_b200.field import ProbeField
     scene = synth.large_scene()
-    g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
-                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
-    f.setHysteresisNormalization(False)
-    f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)
-    c1 = synth.nested_cascades(g, res=(g["res"], g["res"]), scale=0.5)[1]
-    f.configureCascade(1, c1["gridMin"], c1["gridSize"], c1["res"])
-    return scene, f
+    return scene, synth.large_field(scene, device=device)
 
 
 def run_large(args, dist: Dist):
@@ -1105,7 +1100,10 @@ def run_large(args, dist: Dist):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded large instanced scene)",
         "config": {"workload": "8 archetypes of 2k-600k tris (2,101,000 unique), 400 instances (12,810,000 "
                                "instanced), a 120k-tri skinned tube refit every frame (8 bones, <=15 deg), 64 "
-                               "clustered point lights, 2 cascades of 32^3 probes x 256 rays",
+                               "clustered point lights, C0 32^3 probes + the fitted fine cascade C1 (fitFineBox), 256 rays",
+                   "c1": {"res": [int(f._c1Grid.res[a]) for a in range(3)] if f.hasFineCascade() else None,
+                          "gridMin": [round(v, 4) for v in f._c1Box[0]] if f.hasFineCascade() else None,
+                          "gridSize": [round(v, 4) for v in f._c1Box[1]] if f.hasFineCascade() else None},
                    "primary_rays_per_step": int(rays), "layout_of_value": "bvhKind 1 (8-wide, 8-bit boxes)",
                    "l2": "flushed (256 MiB write) before every timed step"},
         "layouts": {f"bvhKind{k}": v for k, v in results.items()}, "fastest_layout": f"bvhKind{best}",

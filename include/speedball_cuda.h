@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define SB_ABI_VERSION 1u
+#define SB_ABI_VERSION 2u
 
 /* Geometry of the reference's layouts (spectral_scene.js:35-55, gi_probes.js:53-56). */
 #define SB_NODE_STRIDE_U32 8u   /* bvhNodes: 6 f32 bounds + miss + payload        */
@@ -140,8 +140,17 @@ typedef enum sb_buffer {
     SB_BUF_RECORD_E = 15,          /* f32, 4 per interior texel (rgb, 1), probeTotal*36:
                                       the FP32 upload output of the last solve of the
                                       last sb_forward_record (read-only)                 */
-    SB_BUF_EMITTER_VIS = 16        /* f32, 16 per probe: giEmitter visibility history
+    SB_BUF_EMITTER_VIS = 16,       /* f32, 16 per probe: giEmitter visibility history
                                       (per cascade, read-only)                          */
+    SB_BUF_ROUGH_SPECULAR = 17,    /* f32, 4 per texel, probeTotal*64: the rough
+                                      reflection history (rgb, coverage); reflection
+                                      tiers rough/high/ultra                             */
+    SB_BUF_ROUGH_ATLAS = 18,       /* u16 binary16 RGBA, atlasW*atlasH*4                 */
+    SB_BUF_GLOSSY_SPECULAR = 19,   /* f32, 4 per glossy texel, probeTotal*glossyTile^2:
+                                      per-ray-mean numerator (rgb, coverage); tiers
+                                      high/ultra                                         */
+    SB_BUF_GLOSSY_WEIGHT = 20,     /* f32, 1 per glossy texel: per-ray-mean support      */
+    SB_BUF_GLOSSY_ATLAS = 21       /* u16 binary16 RGBA, glossyAtlasW*glossyAtlasH*4     */
 } sb_buffer;
 
 /* Ranged host->device write into a reference buffer (the copySceneStorageRanges /
@@ -205,6 +214,9 @@ typedef struct sb_params {
     float debugTempNoiseHBoost, debugTempChangeSigma0, debugTempMinChangeH;
     float debugTempVarEps, debugTempVarRel, debugDepthHistoryScale;
     float debugFilterKScale, debugFilterRelScale, debugFilterEpsScale;
+    float reflectionSkyFallback; /* 1: a true miss feeds the reflection lobes with the
+                                    sky (setReflectionSkyFallback, gi_probes.js:1320-1324) */
+    float skyConfigured;         /* 1 once a sky has been given (gi_probes.js:1316)      */
 } sb_params;
 
 /* The reference's defaults (hysteresis = gated 0.60, gi_probes.js:146-149). */
@@ -216,6 +228,41 @@ void sb_params_defaults(sb_params* p);
  * (gi_probes.js:3124-3197). */
 sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t cascade, const sb_grid* grid);
 sb_status sb_set_params(sb_ctx* ctx, const sb_params* params);
+
+/* Reflection lobes, the reference's structural tier (reflectionQuality,
+ * REFLECTION_QUALITY_TIERS and resolveReflectionQuality, gi_probes.js:60-75):
+ *   SB_REFLECT_OFF   no lobe (the default);
+ *   SB_REFLECT_ROUGH the blend also accumulates a power-8 lobe into a rough
+ *                    specular history and atlas in the irradiance tile layout,
+ *                    and hits on surfaces with no diffuse energy and no
+ *                    emission are stored as hitT = -(t + 2) (gi_probes.js:
+ *                    2055-2062, 2358-2404, 2505-2522, 2838-2843);
+ *   SB_REFLECT_HIGH  rough + a power-64 glossy lobe on 8x8 octahedral tiles
+ *                    (10x10 with the gutter), half of each tile's texels per
+ *                    solve (glossyKernel, 2538-2686);
+ *   SB_REFLECT_ULTRA rough + the glossy lobe on 16x16 tiles, every texel every
+ *                    solve.
+ * Applies to every configured cascade and to later configures: reallocates and
+ * clears the reflection histories and atlases and resets the glossy phase.
+ * Batched solves and the adjoint return SB_ERR_UNSUPPORTED while a tier other
+ * than off is set. */
+typedef enum sb_reflect_tier {
+    SB_REFLECT_OFF = 0, SB_REFLECT_ROUGH = 1, SB_REFLECT_HIGH = 2, SB_REFLECT_ULTRA = 3
+} sb_reflect_tier;
+sb_status sb_set_reflection_quality(sb_ctx* ctx, uint32_t tier);
+
+/* A cascade's reflection layout. The glossy atlas packs probe p's tile at
+ * column p % glossyTilesX, row p / glossyTilesX (glossyTilesX = ceil(sqrt(
+ * probeTotal)), gi_probes.js:3103-3110); glossyPhase is the texel phase the
+ * next solve of the cascade resolves (texels with local % glossyInterval ==
+ * phase; 2561-2567, 3832-3835). */
+typedef struct sb_reflection_layout {
+    uint32_t tier;
+    uint32_t glossyOct, glossyTile, glossyInterval;
+    uint32_t glossyTilesX, glossyTilesY, glossyAtlasW, glossyAtlasH;
+    uint32_t glossyPhase;
+} sb_reflection_layout;
+sb_status sb_get_reflection_layout(sb_ctx* ctx, uint32_t cascade, sb_reflection_layout* out);
 
 /* One solve of one cascade: trace -> NEE/bounce shade -> blend -> upload for
  * probes (probeOffset + slot) mod probeTotal, slot < updatedCount (the

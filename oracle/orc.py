@@ -9,6 +9,7 @@ unpinned (see orc_core.hpp).
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -51,7 +52,10 @@ class OrcSolveIO(C.Structure):
                 ("tested", C.c_void_p), ("blocked", C.c_void_p), ("replayTri", C.c_void_p),
                 ("replayInst", C.c_void_p), ("replayBlocked", C.c_void_p), ("rayIn", C.c_void_p),
                 ("preRound", C.c_void_p), ("counters", C.c_void_p), ("hitFacing", C.c_void_p),
-                ("emitterVis", C.c_void_p), ("emitterVisReplay", C.c_void_p), ("emitterSampleOut", C.c_void_p)]
+                ("emitterVis", C.c_void_p), ("emitterVisReplay", C.c_void_p), ("emitterSampleOut", C.c_void_p),
+                ("reflectTier", C.c_uint32), ("glossyPhase", C.c_uint32), ("roughSpec", C.c_void_p),
+                ("roughAtlas", C.c_void_p), ("glossyNum", C.c_void_p), ("glossyDen", C.c_void_p),
+                ("glossyAtlas", C.c_void_p)]
 
 
 def load() -> C.CDLL:
@@ -222,6 +226,44 @@ def new_state(grid: dict, fp32: bool = False):
     return (np.zeros(P * 64 * 4, dt), np.zeros(P * 64 * 2, dt), atlas, atlas.copy())
 
 
+REFLECT_TIERS = {"off": 0, "rough": 1, "high": 2, "ultra": 3}
+
+
+class ReflectState:
+    """The oracle's reflection lobe state of one cascade for a tier (1 rough,
+    2 high, 3 ultra; REFLECTION_QUALITY_TIERS, gi_probes.js:60-75): the rough
+    history and atlas in the irradiance layout, and for high / ultra the
+    glossy numerator, support and atlas (tiles of glossyOct + 2 texels packed
+    ceil(sqrt(probes)) to a row, gi_probes.js:3103-3110) and the glossy phase."""
+
+    def __init__(self, grid: dict, tier: int, fp32: bool = False):
+        r = grid["res"]
+        P = r[0] * r[1] * r[2]
+        dt = np.float32 if fp32 else np.float64
+        self.tier = int(tier)
+        self.rough = np.zeros(P * 64 * 4, dt)
+        self.rough_atlas = np.zeros((r[1] * r[2] * 8, r[0] * 8, 4), np.uint16)
+        self.oct = 8 if tier == 2 else 16 if tier == 3 else 1
+        self.tile = self.oct + 2 if tier >= 2 else 1
+        self.interval = 2 if tier == 2 else 1 if tier == 3 else 0
+        self.tiles_x = max(1, math.ceil(math.sqrt(P))) if tier >= 2 else 1
+        self.tiles_y = max(1, -(-P // self.tiles_x)) if tier >= 2 else 1
+        self.glossy_num = np.zeros(P * self.tile * self.tile * 4, dt)
+        self.glossy_den = np.zeros(P * self.tile * self.tile, dt)
+        self.glossy_atlas = np.zeros((self.tiles_y * self.tile, self.tiles_x * self.tile, 4), np.uint16)
+        self.phase = 0
+
+    def attach(self, io: OrcSolveIO) -> None:
+        io.reflectTier, io.glossyPhase = self.tier, self.phase
+        io.roughSpec, io.roughAtlas = _p(self.rough), _p(self.rough_atlas)
+        io.glossyNum, io.glossyDen, io.glossyAtlas = _p(self.glossy_num), _p(self.glossy_den), _p(self.glossy_atlas)
+
+    def advance(self) -> None:
+        """After a solve: the next solve resolves the next glossy phase."""
+        if self.interval:
+            self.phase = (self.phase + 1) % self.interval
+
+
 def adjoint(scene: OrcScene, arena: np.ndarray, light_count: int, clustered: bool, grid: OrcGrid,
             params: np.ndarray, tri: np.ndarray, inst: np.ndarray, blocked: np.ndarray, solves: int,
             albedo: np.ndarray, emissive: np.ndarray, light_scale: np.ndarray, target: np.ndarray | None = None,
@@ -357,6 +399,7 @@ ORC_PARAM_NAMES = [
     "debugTempNoiseHBoost", "debugTempChangeSigma0", "debugTempMinChangeH",
     "debugTempVarEps", "debugTempVarRel", "debugDepthHistoryScale",
     "debugFilterKScale", "debugFilterRelScale", "debugFilterEpsScale",
+    "reflectionSkyFallback", "skyConfigured",
 ]
 
 

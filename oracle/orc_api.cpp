@@ -40,6 +40,14 @@ struct OrcSolveIO {
     const void* emitterVisReplay;  // R[probeTotal*16]: the GPU's history after the solve, taken for the
                                    // updated probes before the blend (replay), or null
     void* emitterSampleOut;   // R[updated*16]: this solve's own visibility samples, or null
+    // reflection lobes (tier 0 off, 1 rough, 2 high, 3 ultra); the buffers are
+    // in/out and sized for the tier (glossy tile = 10 / 18 texels a side)
+    uint32_t reflectTier, glossyPhase;
+    void* roughSpec;          // R[probeTotal*64*4]
+    uint16_t* roughAtlas;     // RGBA16F, atlasW*atlasH*4
+    void* glossyNum;          // R[probeTotal*tile^2*4]
+    void* glossyDen;          // R[probeTotal*tile^2]
+    uint16_t* glossyAtlas;    // RGBA16F, (tilesX*tile)*(tilesY*tile)*4
 };
 
 
@@ -267,6 +275,7 @@ static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, 
         std::vector<Counters> cnts(nt);
         parallel_for(nr, nt, [&](size_t i, int t) {
             Tracer<R> tc(sc, L, g, g0, P, atlas);
+            tc.roughEncode = io && io->reflectTier >= 1;
             if (io && io->counters) tc.tr.cnt = &cnts[t];
             RayOut<R> o;
             uint32_t slot = (uint32_t)(i / N), k = (uint32_t)(i % N);
@@ -315,14 +324,32 @@ static int solve_impl(const OrcScene* s, const OrcLights* l, const OrcGrid* gp, 
     EmitterInject<R> inj;
     inj.L = &L;
     inj.vis = evis;
+    Reflect<R> rf;
+    if (io && io->reflectTier) {
+        rf.tier = io->reflectTier;
+        rf.roughSpec = static_cast<R*>(io->roughSpec);
+        rf.roughAtlas = io->roughAtlas;
+        rf.glossyNum = static_cast<R*>(io->glossyNum);
+        rf.glossyDen = static_cast<R*>(io->glossyDen);
+        rf.glossyAtlas = io->glossyAtlas;
+        rf.glossyPhase = io->glossyPhase;
+        if (!rf.roughSpec || !rf.roughAtlas) return 2;
+        if (rf.tier >= 2 && (!rf.glossyNum || !rf.glossyDen || !rf.glossyAtlas)) return 2;
+    }
+    Reflect<R>* rfp = rf.tier ? &rf : nullptr;
     parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
         uint32_t p = (uint32_t)((probeOffset + slot) % total);
-        blend_probe<R>(g, P, rayBuf + slot * N * 4, p, irr, depth, evis ? &inj : nullptr);
+        blend_probe<R>(g, P, rayBuf + slot * N * 4, p, irr, depth, evis ? &inj : nullptr, rfp);
     });
-    // the upload runs after every blend of the solve (separate kernel)
+    // glossyKernel, then the upload (gi_probes.js:3829-3836)
+    if (rf.tier >= 2)
+        parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
+            uint32_t p = (uint32_t)((probeOffset + slot) % total);
+            glossy_probe<R>(g, P, rayBuf + slot * N * 4, p, rf, evis ? &inj : nullptr);
+        });
     parallel_for(updated, std::max(1, threads), [&](size_t slot, int) {
         uint32_t p = (uint32_t)((probeOffset + slot) % total);
-        upload_probe<R>(g, P, p, irr, depth, atlas, depthAtlas, pre);
+        upload_probe<R>(g, P, p, irr, depth, atlas, depthAtlas, pre, rfp);
     });
     return 0;
 }

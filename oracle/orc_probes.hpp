@@ -24,6 +24,7 @@ struct Params {
     double debugTempNoiseHBoost, debugTempChangeSigma0, debugTempMinChangeH;
     double debugTempVarEps, debugTempVarRel, debugDepthHistoryScale;
     double debugFilterKScale, debugFilterRelScale, debugFilterEpsScale;
+    double reflectionSkyFallback, skyConfigured;  // gi_probes.js:1234, 1238, 1316-1324
 };
 
 struct Lights {
@@ -36,6 +37,7 @@ struct Lights {
 
 constexpr uint32_t GI_EMITTER_INJECT_CAP = 16;      // gi_probes.js:133
 constexpr double GI_EMITTER_VIS_RETENTION = 0.8;    // gi_probes.js:134
+constexpr double ROUGH_UNSHADED_T_BIAS = 2.0;        // gi_probes.js:94
 
 // One ray's outputs. hitT = -1 on a miss (gi_probes.js:1987, 2209-2213).
 template <class R> struct RayOut {
@@ -173,6 +175,9 @@ template <class R> struct Tracer {
     const double* albedo = nullptr;
     const double* emissive = nullptr;
     const double* lightScale = nullptr;
+    // Reflection lobes on (tier rough and above): hits on surfaces with no
+    // diffuse energy and no emission are encoded as -(t + 2).
+    bool roughEncode = false;
     // Intermediates of one hit's shading, filled when non-null (adjoint checks):
     // the unblocked lights' terms are kd (.) X[i].
     struct ShadeRecord {
@@ -291,6 +296,11 @@ template <class R> struct Tracer {
             R metal = tr.mat_f(m, 4), transm = tr.mat_f(m, 5);
             V3<R> kdr = baseColor * R(P.debugAlbedoScale) * (R(1) - metal) * (R(1) - transm);
             V3<R> kd(clampv(kdr.x, R(0), R(0.95)), clampv(kdr.y, R(0), R(0.95)), clampv(kdr.z, R(0), R(0.95)));
+            if (roughEncode) {  // gi_probes.js:2055-2062
+                R diffuseEnergy = (R(1) - metal) * (R(1) - transm);
+                R emissivePeak = std::max(std::max(emis.x, emis.y), emis.z);
+                if (!(diffuseEnergy > R(0.02) || emissivePeak > R(1e-6))) hitT = -(bestT + R(ROUGH_UNSHADED_T_BIAS));
+            }
             if (rec) {
                 rec->hit = true;
                 rec->m = m;
@@ -402,8 +412,30 @@ template <class R> struct EmitterInject {
     const R* vis = nullptr;  // probeTotal x GI_EMITTER_INJECT_CAP
 };
 
+// Reflection lobe state of one cascade (REFLECTION_QUALITY_TIERS,
+// gi_probes.js:60-75; buffers 1796-1840): tier 1 rough, 2 high, 3 ultra.
+template <class R> struct Reflect {
+    uint32_t tier = 0;
+    R* roughSpec = nullptr;         // probeTotal x 64 texels x 4 (rgb, coverage)
+    uint16_t* roughAtlas = nullptr; // RGBA16F, the irradiance atlas layout
+    R* glossyNum = nullptr;         // probeTotal x glossyTile^2 x 4
+    R* glossyDen = nullptr;         // probeTotal x glossyTile^2
+    uint16_t* glossyAtlas = nullptr;
+    uint32_t glossyPhase = 0;
+    uint32_t oct() const { return tier == 2 ? 8u : tier == 3 ? 16u : 1u; }
+    uint32_t tile() const { return tier >= 2 ? oct() + 2u * BORDER : 1u; }
+    uint32_t interval() const { return tier == 2 ? 2u : tier == 3 ? 1u : 0u; }
+    // glossy tiles packed near-square (gi_probes.js:3107-3110)
+    static uint32_t tiles_x(uint32_t probeTotal) {
+        return std::max(1u, (uint32_t)std::ceil(std::sqrt((double)probeTotal)));
+    }
+};
+
 template <class R> void blend_probe(const Grid& g, const Params& P, const R* rays, uint32_t probeIndex, R* irr, R* depth,
-                                    const EmitterInject<R>* em = nullptr) {
+                                    const EmitterInject<R>* em = nullptr, Reflect<R>* rf = nullptr) {
+    const bool rough = rf && rf->tier >= 1;
+    // a true miss feeds the lobe only with the explicit sky fallback (gi_probes.js:2361-2367)
+    const R skyValid = R(P.reflectionSkyFallback) * R(P.skyConfigured) * (P.skyIntensity > 0 ? R(1) : R(0));
     const uint32_t N = g.rays;
     std::vector<V3<R>> dirs(N);
     for (uint32_t k = 0; k < N; ++k) dirs[k] = ray_dir<R>(k, N, R(P.frameJitter));
@@ -413,8 +445,8 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
         R u = (R(lx) - R(BORDER) + R(0.5)) / R(OCT_RES);
         R v = (R(ly) - R(BORDER) + R(0.5)) / R(OCT_RES);
         V3<R> dir = oct_decode(u, v);
-        V3<R> acc;
-        R wsum = 0, dAcc = 0, dAcc2 = 0, dwsum = 0, lAcc = 0, lAcc2 = 0;
+        V3<R> acc, sAcc;
+        R wsum = 0, dAcc = 0, dAcc2 = 0, dwsum = 0, lAcc = 0, lAcc2 = 0, sHit = 0, sWsum = 0;
         for (uint32_t k = 0; k < N; ++k) {
             const R* rr = rays + (size_t)k * 4;
             V3<R> rrgb(rr[0], rr[1], rr[2]);
@@ -433,6 +465,13 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
             dAcc += rdist * dw;
             dAcc2 += rdist * rdist * dw;
             dwsum += dw;
+            if (rough) {  // power-8 lobe (gi_probes.js:2388-2404)
+                R cd2 = cd * cd, cd4 = cd2 * cd2, sw = cd4 * cd4;
+                R valid = hitT >= R(0) ? R(1) : (hitT == R(-1) ? skyValid : R(0));
+                sAcc = sAcc + rrgb * sw * valid;
+                sHit += sw * valid;
+                sWsum += sw;
+            }
         }
         if (em && em->L && em->L->emitterCount) {
             // each emitter as kVirtual rays toward its centre, radiance x visibility
@@ -458,6 +497,13 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
                 R lum = luma(Lc);
                 lAcc += lum * wk;
                 lAcc2 += lum * lum * wk;
+                if (rough) {
+                    R cd2 = cd * cd, cd4 = cd2 * cd2;
+                    R swk = cd4 * cd4 * kVirtual;
+                    sAcc = sAcc + Lc * swk;
+                    sHit += swk;
+                    sWsum += swk;
+                }
             }
         }
         R wden = std::max(wsum, R(1e-4));
@@ -500,6 +546,14 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
         size_t db = ((size_t)probeIndex * TILE * TILE + local) * 2;
         R dpx = depth[db], dpy = depth[db + 1];
         bool dWasZero = dpx < R(1e-6);
+        if (rough) {  // rough history: steady / noisy reference retention (gi_probes.js:2478-2484, 2505-2522)
+            R steadyH = std::pow(clampv(rawNoiseH, R(1e-6), R(1)), R(P.hysteresisExponent));
+            R sh = dWasZero ? R(0) : steadyH;
+            R sDen = std::max(sWsum, R(1e-4));
+            R sCur[4] = {sAcc.x / sDen, sAcc.y / sDen, sAcc.z / sDen, clampv(sHit / sDen, R(0), R(1))};
+            R* sp = rf->roughSpec + ib;
+            for (int c = 0; c < 4; ++c) sp[c] = mixv(sCur[c], sp[c], sh);
+        }
         R rawDepthH = clampv(H * R(P.debugDepthHistoryScale), R(0), R(0.999));
         R depthH = std::pow(std::max(rawDepthH, R(1e-6)), R(P.hysteresisExponent));
         R dh = dWasZero ? R(0) : depthH;
@@ -513,7 +567,7 @@ template <class R> void blend_probe(const Grid& g, const Params& P, const R* ray
 // preRound != nullptr, the unrounded RGB of the 36 interior texels (the value
 // that the fp16 store rounds) is also returned, probe-major, 3 per texel.
 template <class R> void upload_probe(const Grid& g, const Params& P, uint32_t probeIndex, const R* irr, const R* depth,
-                                     uint16_t* atlas, uint16_t* depthAtlas, R* preRound) {
+                                     uint16_t* atlas, uint16_t* depthAtlas, R* preRound, const Reflect<R>* rf = nullptr) {
     R cacheI[36][3], cacheD[36][2];
     size_t probeBase = (size_t)probeIndex * TILE * TILE;
     for (int lane = 0; lane < OCT_RES * OCT_RES; ++lane) {
@@ -568,6 +622,90 @@ template <class R> void upload_probe(const Grid& g, const Params& P, uint32_t pr
         depthAtlas[t + 1] = to_half(cacheD[src][1]);
         depthAtlas[t + 2] = to_half(0.0);
         depthAtlas[t + 3] = to_half(1.0);
+        if (rf && rf->tier >= 1) {  // the rough history, unfiltered (gi_probes.js:2789-2795, 2841-2843)
+            int ssx = src % OCT_RES + BORDER, ssy = src / OCT_RES + BORDER;
+            const R* sp = rf->roughSpec + (probeBase + ssy * TILE + ssx) * 4;
+            for (int c = 0; c < 4; ++c) rf->roughAtlas[t + c] = to_half(sp[c]);
+        }
+    }
+}
+
+// glossyKernel (gi_probes.js:2538-2686) for one probe: the power-64 lobe on the
+// glossy tile (glossyOct^2 texels and a mirrored one-texel gutter, each gutter
+// texel evaluated at its source texel's direction), the per-ray-mean numerator
+// and support histories and the resolved RGBA16F glossy atlas. Tier high
+// resolves the texels with local % 2 == glossyPhase.
+template <class R> void glossy_probe(const Grid& g, const Params& P, const R* rays, uint32_t probeIndex,
+                                     Reflect<R>& rf, const EmitterInject<R>* em = nullptr) {
+    const uint32_t N = g.rays, tile = rf.tile(), oct = rf.oct(), interval = rf.interval();
+    std::vector<V3<R>> dirs(N);
+    for (uint32_t k = 0; k < N; ++k) dirs[k] = ray_dir<R>(k, N, R(P.frameJitter));
+    const R skyValid = R(P.reflectionSkyFallback) * R(P.skyConfigured) * (P.skyIntensity > 0 ? R(1) : R(0));
+    const uint32_t tilesX = Reflect<R>::tiles_x(g.probeTotal());
+    const uint32_t atlasW = tilesX * tile;
+    auto pow64 = [](R c) { R c2 = c * c, c4 = c2 * c2, c8 = c4 * c4, c16 = c8 * c8, c32 = c16 * c16; return c32 * c32; };
+    for (uint32_t local = 0; local < tile * tile; ++local) {
+        if (interval > 1 && local % interval != rf.glossyPhase) continue;
+        const int lx = (int)(local % tile), ly = (int)(local / tile);
+        const int edge = (int)tile - 1, lo = BORDER, hi = BORDER + (int)oct - 1;
+        bool onLeft = lx == 0, onRight = lx == edge, onTop = ly == 0, onBottom = ly == edge;
+        bool colB = onLeft || onRight, rowB = onTop || onBottom, corner = colB && rowB;
+        int sx = corner ? (onLeft ? hi : lo) : (rowB ? edge - lx : (colB ? (onLeft ? lo : hi) : lx));
+        int sy = corner ? (onTop ? hi : lo) : (rowB ? (onTop ? lo : hi) : (colB ? edge - ly : ly));
+        R u = (R(sx) - R(BORDER) + R(0.5)) / R(oct);
+        R v = (R(sy) - R(BORDER) + R(0.5)) / R(oct);
+        V3<R> dir = oct_decode(u, v);
+        V3<R> gAcc;
+        R gHit = 0, gWsum = 0;
+        for (uint32_t k = 0; k < N; ++k) {
+            const R* rr = rays + (size_t)k * 4;
+            R hitT = rr[3];
+            R gw = pow64(std::max(dot(dir, dirs[k]), R(0)));
+            R valid = hitT >= R(0) ? R(1) : (hitT == R(-1) ? skyValid : R(0));
+            gAcc = gAcc + V3<R>(rr[0], rr[1], rr[2]) * gw * valid;
+            gHit += gw * valid;
+            gWsum += gw;
+        }
+        if (em && em->L && em->L->emitterCount) {
+            const V3<R> ro = probe_world_pos<R>(g, probeIndex);
+            for (uint32_t e = 0; e < em->L->emitterCount; ++e) {
+                const float* rec = em->L->data + (size_t)(em->L->emitterBase + e) * LIGHT_STRIDE;
+                const V3<R> center = V3<R>(R(rec[1]), R(rec[2]), R(rec[3]));
+                R sourceRadius = std::max(R(rec[14]), R(0));
+                V3<R> axis = center - ro;
+                R dist = length(axis);
+                if (!(dist > std::max(sourceRadius, R(1e-3)))) continue;
+                V3<R> d = axis * (R(1) / dist);
+                R Omega = std::min(R(2.0 * PI), std::max(R(rec[15]), R(0)) / (dist * dist));
+                R kVirtual = std::min(R(N), R(N) * Omega / R(4.0 * PI));
+                R vis = em->vis[(size_t)probeIndex * GI_EMITTER_INJECT_CAP + e];
+                V3<R> Lc = V3<R>(R(rec[7]), R(rec[8]), R(rec[9])) * vis;
+                R wk = pow64(std::max(dot(dir, d), R(0))) * kVirtual;
+                gAcc = gAcc + Lc * wk;
+                gWsum += wk;
+                gHit += wk;
+            }
+        }
+        const size_t gt = (size_t)probeIndex * tile * tile + local;
+        R* num = rf.glossyNum + gt * 4;
+        R& den = rf.glossyDen[gt];
+        // the reference forms 1 / raysPerProbe in double and stores it as a float uniform
+        R invRays = R(float(1.0 / double(N)));
+        R curNum[4] = {gAcc.x * invRays, gAcc.y * invRays, gAcc.z * invRays, gHit * invRays};
+        R curDen = gWsum * invRays;
+        bool empty = den < R(1e-6);
+        R H = R(P.hysteresis);
+        R refH = H + (R(1) - H) * R(P.debugTempNoiseHBoost);
+        R glossyH = std::pow(clampv(refH, R(1e-6), R(1)), R(P.hysteresisExponent) * R(interval));
+        R gh = empty ? R(0) : glossyH;
+        for (int c = 0; c < 4; ++c) num[c] = mixv(curNum[c], num[c], gh);
+        den = std::max(mixv(curDen, den, gh), R(1e-6));
+        uint32_t col = probeIndex % tilesX, row = probeIndex / tilesX;
+        size_t t = ((size_t)(row * tile + ly) * atlasW + col * tile + lx) * 4;
+        rf.glossyAtlas[t] = to_half(num[0] / den);
+        rf.glossyAtlas[t + 1] = to_half(num[1] / den);
+        rf.glossyAtlas[t + 2] = to_half(num[2] / den);
+        rf.glossyAtlas[t + 3] = to_half(clampv(num[3] / den, R(0), R(1)));
     }
 }
 

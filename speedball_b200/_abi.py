@@ -32,6 +32,7 @@ BUF = dict(
     BVH_NODES=0, TRI_INDEX=1, VERTEX_DATA=2, TRI_MATERIAL=3, MATERIALS=4, LIGHTS=5,
     IRRADIANCE_HISTORY=6, DEPTH_HISTORY=7, IRRADIANCE_ATLAS=8, DEPTH_ATLAS=9, RAY_DATA=10,
     HIT_RECORDS=11, VISIBILITY=12, TLAS_ORDER=13, INSTANCE_BOUNDS=14, RECORD_E=15, EMITTER_VIS=16,
+    ROUGH_SPECULAR=17, ROUGH_ATLAS=18, GLOSSY_SPECULAR=19, GLOSSY_WEIGHT=20, GLOSSY_ATLAS=21,
 )
 
 
@@ -79,6 +80,7 @@ PARAM_NAMES = [
     "debugTempNoiseHBoost", "debugTempChangeSigma0", "debugTempMinChangeH",
     "debugTempVarEps", "debugTempVarRel", "debugDepthHistoryScale",
     "debugFilterKScale", "debugFilterRelScale", "debugFilterEpsScale",
+    "reflectionSkyFallback", "skyConfigured",
 ]
 
 
@@ -114,6 +116,14 @@ class sb_tuning(C.Structure):
                 ("bvhKind", C.c_uint32), ("smemWideNodes", C.c_uint32)]
 
 
+REFLECT_TIERS = {"off": 0, "rough": 1, "high": 2, "ultra": 3}
+
+
+class sb_reflection_layout(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("tier", "glossyOct", "glossyTile", "glossyInterval", "glossyTilesX",
+                                          "glossyTilesY", "glossyAtlasW", "glossyAtlasH", "glossyPhase")]
+
+
 class sb_gather_params(C.Structure):
     _fields_ = [("normalBias", C.c_float * 2), ("chebyBias", C.c_float * 2), ("chebyStrength", C.c_float),
                 ("detailStrength", C.c_float), ("intensity", C.c_float), ("enabled", C.c_float),
@@ -146,6 +156,8 @@ SIGNATURES = {
     "sb_set_walk_step_limit": (C.c_int, [_P, C.c_uint32]),
     "sb_triangle_test": (C.c_uint32, []),
     "sb_fit_fine_box": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "sb_set_reflection_quality": (C.c_int, [_P, _U32]),
+    "sb_get_reflection_layout": (C.c_int, [_P, _U32, C.POINTER(sb_reflection_layout)]),
     "sb_rebuild_scene_bvh": (C.c_int, [_P]),
     "sb_build_blas_device": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_build_blas_gpu": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),

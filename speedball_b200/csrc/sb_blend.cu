@@ -21,29 +21,36 @@ namespace sb {
 constexpr int BLEND_PROBES = 8;
 constexpr int BLEND_TEXELS = OCT * OCT;
 constexpr int BLEND_THREADS = BLEND_PROBES * BLEND_TEXELS;  // 288 = 9 warps
-constexpr int BLEND_CHUNK = 64;                             // rays staged per pass
 
-struct BlendSmem {
+// ROUGH adds the rough reflection lobe (power 8, gi_probes.js:2388-2404): a
+// third weight table, a coverage flag per ray and the blended rough history
+// per texel; it stages 32 rays per pass so that the block stays within 48 KB.
+template <bool ROUGH> struct BlendSmem {
+    static constexpr int CH = ROUGH ? 32 : 64;  // rays staged per pass
     float4 texDir[BLEND_TEXELS];
-    float4 rayDir[BLEND_CHUNK];
-    float wc[BLEND_CHUNK][BLEND_TEXELS];  // cosine weight  [ray][texel]
-    float wd[BLEND_CHUNK][BLEND_TEXELS];  // depth weight   [ray][texel]
+    float4 rayDir[CH];
+    float wc[CH][BLEND_TEXELS];               // cosine weight  [ray][texel]
+    float wd[CH][BLEND_TEXELS];               // depth weight   [ray][texel]
+    float wr[ROUGH ? CH : 1][BLEND_TEXELS];   // rough lobe weight cd^8
     union {
         struct {
-            float4 fa[BLEND_PROBES][BLEND_CHUNK + 1];  // r, g, b, luma (row pad shifts banks)
-            float4 fb[BLEND_PROBES][BLEND_CHUNK + 1];  // luma^2, dist, dist^2, -
+            float4 fa[BLEND_PROBES][CH + 1];  // r, g, b, luma (row pad shifts banks)
+            float4 fb[BLEND_PROBES][CH + 1];  // luma^2, dist, dist^2, reflection coverage (0 / 1)
         } f;
         float4 out[BLEND_PROBES][BLEND_TEXELS];        // filtered irradiance (after the sums)
     } u;
     float4 irr[BLEND_PROBES][BLEND_TEXELS];
     float2 dep[BLEND_PROBES][BLEND_TEXELS];
-    float wsum[BLEND_TEXELS], dwsum[BLEND_TEXELS];  // weight sums: the same for every probe
+    float4 rough[ROUGH ? BLEND_PROBES : 1][BLEND_TEXELS];  // blended rough history
+    float wsum[BLEND_TEXELS], dwsum[BLEND_TEXELS], swsum[BLEND_TEXELS];  // the same for every probe
 };
 
 // Blend + upload of probe slots [block * BLEND_PROBES, + BLEND_PROBES) of one
 // solve; the body of the per-solve and the batched kernels.
+template <bool ROUGH>
 __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const DevParams& P, uint32_t block,
-                                                   BlendSmem& S) {
+                                                   BlendSmem<ROUGH>& S) {
+    constexpr int CH = BlendSmem<ROUGH>::CH;
     const int tid = threadIdx.x;
     const int p = tid / BLEND_TEXELS, lane = tid % BLEND_TEXELS;
     const uint32_t base = block * BLEND_PROBES;
@@ -63,8 +70,14 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
 
     float sr = 0.f, sg = 0.f, sb = 0.f, sl = 0.f, sl2 = 0.f, ws = 0.f, sd = 0.f, sd2 = 0.f, dws = 0.f;
     float cr = 0.f, cg = 0.f, cb = 0.f, cl = 0.f, cl2 = 0.f, cws = 0.f, cd = 0.f, cd2 = 0.f, cdw = 0.f;
-    for (uint32_t c = 0; c < N; c += BLEND_CHUNK) {
-        const uint32_t n = min((uint32_t)BLEND_CHUNK, N - c);
+    // rough lobe sums (sAcc, sHit, sWsum of gi_probes.js:2358-2360) and their compensations
+    float xr = 0.f, xg = 0.f, xb = 0.f, xh = 0.f, xws = 0.f;
+    float kxr = 0.f, kxg = 0.f, kxb = 0.f, kxh = 0.f, kxws = 0.f;
+    // a true miss feeds the lobe only with an explicit sky fallback (gi_probes.js:2364-2367)
+    const float skyValid = ROUGH ? P.reflectionSkyFallback * P.skyConfigured * (P.skyIntensity > 0.0f ? 1.0f : 0.0f)
+                                 : 0.0f;
+    for (uint32_t c = 0; c < N; c += CH) {
+        const uint32_t n = min((uint32_t)CH, N - c);
         __syncthreads();  // previous pass done with the table and features
         for (uint32_t e = tid; e < nProbes * n; e += BLEND_THREADS) {
             uint32_t q = e / n, k = e % n;
@@ -74,7 +87,9 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
             float decoded = hitT < -1.5f ? -hitT - 2.0f : hitT;
             float rdist = hitT == -1.0f ? C.maxDist : decoded;
             S.u.f.fa[q][k] = make_float4(r.x, r.y, r.z, rl);
-            S.u.f.fb[q][k] = make_float4(rl * rl, rdist, rdist * rdist, 0.0f);
+            // local hits count, a miss counts with the sky fallback, encoded unshaded hits never
+            const float valid = hitT >= 0.0f ? 1.0f : (hitT == -1.0f ? skyValid : 0.0f);
+            S.u.f.fb[q][k] = make_float4(rl * rl, rdist, rdist * rdist, valid);
         }
         if ((uint32_t)tid < n) {
             float3 d = ray_dir(c + tid, N, P.frameJitter);
@@ -99,6 +114,10 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
             }
             S.wc[k][j] = cw;
             S.wd[k][j] = dw;
+            if (ROUGH) {  // fixed power-8 lobe as ((cd^2)^2)^2 (gi_probes.js:2389-2393)
+                const float c2 = cd * cd, c4 = c2 * c2;
+                S.wr[k][j] = c4 * c4;
+            }
         }
         __syncthreads();
         if (live) {
@@ -113,21 +132,32 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
                 kahan_fma(sl2, cl2, w, b.x);
                 kahan_fma(sd, cd, v, b.y);
                 kahan_fma(sd2, cd2, v, b.z);
+                if (ROUGH) {
+                    const float r = S.wr[k][lane];
+                    const float rv = r * b.w;  // coverage is 0 or 1: exact
+                    kahan_fma(xr, kxr, rv, a.x);
+                    kahan_fma(xg, kxg, rv, a.y);
+                    kahan_fma(xb, kxb, rv, a.z);
+                    kahan_fma(xh, kxh, rv, 1.0f);
+                }
             }
             if (p == 0)  // the weight sums depend on (texel, ray) only: the first probe's lanes form them
                 for (uint32_t k = 0; k < n; ++k) {
                     kahan_fma(ws, cws, S.wc[k][lane], 1.0f);
                     kahan_fma(dws, cdw, S.wd[k][lane], 1.0f);
+                    if (ROUGH) kahan_fma(xws, kxws, S.wr[k][lane], 1.0f);
                 }
         }
     }
     if (p == 0) {
         S.wsum[lane] = ws;
         S.dwsum[lane] = dws;
+        S.swsum[lane] = xws;
     }
     __syncthreads();  // features no longer read: S.u.out may be written; weight sums published
     ws = S.wsum[lane];
     dws = S.dwsum[lane];
+    xws = S.swsum[lane];
 
     const uint32_t probeIndex = live ? (C.probeOffset + slot) % C.probeTotal : 0u;
     if (live && C.emitterCount) {
@@ -155,6 +185,15 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
             kahan_fma(sl, cl, wk, lum);
             kahan_fma(sl2, cl2, wk, lum * lum);
             ws += wk;
+            if (ROUGH) {  // the secondary (power-8) weight of the same virtual rays
+                const float c2 = cdot * cdot, c4 = c2 * c2;
+                const float sk = c4 * c4 * kVirtual;
+                kahan_fma(xr, kxr, sk, Lc.x);
+                kahan_fma(xg, kxg, sk, Lc.y);
+                kahan_fma(xb, kxb, sk, Lc.z);
+                kahan_fma(xh, kxh, sk, 1.0f);
+                xws += sk;
+            }
         }
     }
     if (live) {
@@ -198,6 +237,19 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
 
         float2 dprev = C.depth[ib];
         bool dWasZero = dprev.x < 1e-6f;
+        if (ROUGH) {
+            // rough history (gi_probes.js:2505-2522): the steady / noisy reference retention,
+            // independent of the diffuse change detector; seeded where depth is unseeded
+            const float sDen = fmaxf(xws, 1e-4f);
+            const float4 sCur = make_float4(xr / sDen, xg / sDen, xb / sDen, clampf(xh / sDen, 0.0f, 1.0f));
+            const float steadyH = powf(clampf(rawNoiseH, 1e-6f, 1.0f), P.hysteresisExponent);
+            const float sh = dWasZero ? 0.0f : steadyH;
+            const float4 sPrev = C.roughSpec[ib];
+            const float4 sOut = make_float4(mixf(sCur.x, sPrev.x, sh), mixf(sCur.y, sPrev.y, sh),
+                                            mixf(sCur.z, sPrev.z, sh), mixf(sCur.w, sPrev.w, sh));
+            C.roughSpec[ib] = sOut;
+            S.rough[p][lane] = sOut;
+        }
         float rawDepthH = clampf(H * P.debugDepthHistoryScale, 0.0f, 0.999f);
         float depthH = powf(fmaxf(rawDepthH, 1e-6f), P.hysteresisExponent);
         float dh = dWasZero ? 0.0f : depthH;
@@ -261,28 +313,34 @@ __device__ __forceinline__ void blend_upload_block(const DevCascade& C, const De
         C.atlas[t] = float4_to_half4(S.u.out[q][src]);
         float2 d = S.dep[q][src];
         C.depthAtlas[t] = float4_to_half4(make_float4(d.x, d.y, 0.0f, 1.0f));
+        if (ROUGH) C.roughAtlas[t] = float4_to_half4(S.rough[q][src]);  // unfiltered (gi_probes.js:2789-2795, 2841-2843)
     }
 }
 
+template <bool ROUGH>
 __global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload(DevCascade C, DevParams P) {
-    __shared__ BlendSmem S;
-    blend_upload_block(C, P, blockIdx.x, S);
+    __shared__ BlendSmem<ROUGH> S;
+    blend_upload_block<ROUGH>(C, P, blockIdx.x, S);
 }
 
 // Every item of a batch: CTAs [blendBase, blendBase + blendBlocks) belong to item i.
 __global__ void __launch_bounds__(BLEND_THREADS) k_blend_upload_batch(const __grid_constant__ BatchArgs B) {
-    __shared__ BlendSmem S;
+    __shared__ BlendSmem<false> S;  // batches carry no reflection lobes
     uint32_t i = 0;
     while (i + 1 < B.n && blockIdx.x >= B.it[i + 1].blendBase) ++i;
     const BatchItem& I = B.it[i];
     if (blockIdx.x - I.blendBase >= I.blendBlocks) return;
-    blend_upload_block(I.W.C, I.W.P, blockIdx.x - I.blendBase, S);
+    blend_upload_block<false>(I.W.C, I.W.P, blockIdx.x - I.blendBase, S);
 }
 
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st) {
     if (C.updatedCount == 0) return cudaSuccess;
     const uint32_t blocks = (C.updatedCount + BLEND_PROBES - 1) / BLEND_PROBES;
-    k_blend_upload<<<blocks, BLEND_THREADS, 0, st>>>(C, P); note_launch();
+    if (C.reflect && C.roughSpec)
+        k_blend_upload<true><<<blocks, BLEND_THREADS, 0, st>>>(C, P);
+    else
+        k_blend_upload<false><<<blocks, BLEND_THREADS, 0, st>>>(C, P);
+    note_launch();
     return cudaGetLastError();
 }
 
@@ -295,6 +353,106 @@ cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st) {
 }
 
 uint32_t blend_blocks(uint32_t updatedCount) { return (updatedCount + BLEND_PROBES - 1) / BLEND_PROBES; }
+
+// glossyKernel (gi_probes.js:2538-2686): the power-64 lobe on the glossy tiles
+// (glossyOct^2 texels + a one-texel mirrored gutter), one CTA per updated
+// probe, one thread per tile texel. Tier high resolves the texels with
+// local % 2 == glossyPhase, ultra every texel. Each texel keeps a per-ray-mean
+// numerator (rgb, coverage) and support in its history, blended with one
+// retention, and stores their ratio to the glossy atlas.
+constexpr int GLOSSY_THREADS = 128;
+constexpr uint32_t GLOSSY_MAX_RAYS = 256;  // raysPerProbe <= 256 (gi_probes.js:988-992)
+
+__device__ __forceinline__ float pow64(float c) {
+    const float c2 = c * c, c4 = c2 * c2, c8 = c4 * c4, c16 = c8 * c8, c32 = c16 * c16;
+    return c32 * c32;
+}
+
+__global__ void __launch_bounds__(GLOSSY_THREADS) k_glossy(DevCascade C, DevParams P) {
+    __shared__ float4 rad[GLOSSY_MAX_RAYS];  // rgb, coverage
+    __shared__ float4 dir[GLOSSY_MAX_RAYS];
+    const uint32_t slot = blockIdx.x, N = C.rays;
+    if (slot >= C.updatedCount || N > GLOSSY_MAX_RAYS) return;
+    const float skyValid = P.reflectionSkyFallback * P.skyConfigured * (P.skyIntensity > 0.0f ? 1.0f : 0.0f);
+    for (uint32_t k = threadIdx.x; k < N; k += blockDim.x) {
+        const float4 r = C.rayData[(size_t)slot * N + k];
+        const float valid = r.w >= 0.0f ? 1.0f : (r.w == -1.0f ? skyValid : 0.0f);
+        rad[k] = make_float4(r.x, r.y, r.z, valid);
+        const float3 d = ray_dir(k, N, P.frameJitter);
+        dir[k] = make_float4(d.x, d.y, d.z, 0.0f);
+    }
+    __syncthreads();
+    const uint32_t tile = C.glossyTile, oct = C.glossyOct, texels = tile * tile;
+    const uint32_t probeIndex = (C.probeOffset + slot) % C.probeTotal;
+    const float3 ro = probe_world_pos(C, probeIndex);
+    const float invRays = 1.0f / float(N);  // equals float(1 / N) for every allowed N
+    for (uint32_t local = threadIdx.x; local < texels; local += blockDim.x) {
+        if (C.glossyInterval > 1u && local % C.glossyInterval != C.glossyPhase) continue;
+        const int lx = (int)(local % tile), ly = (int)(local / tile);
+        // canonical mirrored gutter, resolved before the direction (gi_probes.js:2571-2593)
+        const int edge = (int)tile - 1, lo = BORDER, hi = BORDER + (int)oct - 1;
+        const bool onLeft = lx == 0, onRight = lx == edge, onTop = ly == 0, onBottom = ly == edge;
+        const bool colB = onLeft || onRight, rowB = onTop || onBottom, corner = colB && rowB;
+        const int sx = corner ? (onLeft ? hi : lo) : (rowB ? edge - lx : (colB ? (onLeft ? lo : hi) : lx));
+        const int sy = corner ? (onTop ? hi : lo) : (rowB ? (onTop ? lo : hi) : (colB ? edge - ly : ly));
+        const float3 td = oct_decode((float(sx - BORDER) + 0.5f) / float(oct), (float(sy - BORDER) + 0.5f) / float(oct));
+        float ar = 0.f, ag = 0.f, ab = 0.f, ah = 0.f, aw = 0.f;
+        float kr = 0.f, kg = 0.f, kb = 0.f, kh = 0.f, kw = 0.f;
+        for (uint32_t k = 0; k < N; ++k) {
+            const float4 d = dir[k], r = rad[k];
+            const float gw = pow64(fmaxf(td.x * d.x + td.y * d.y + td.z * d.z, 0.0f));
+            const float gv = gw * r.w;  // coverage is 0 or 1: exact
+            kahan_fma(ar, kr, gv, r.x);
+            kahan_fma(ag, kg, gv, r.y);
+            kahan_fma(ab, kb, gv, r.z);
+            kahan_fma(ah, kh, gv, 1.0f);
+            kahan_fma(aw, kw, gw, 1.0f);
+        }
+        // the emitters' virtual rays with the power-64 weight (gi_probes.js:2624-2638)
+        for (uint32_t e = 0; e < C.emitterCount; ++e) {
+            const float* L = C.lights + (size_t)(C.emitterBase + e) * 17u;
+            const float3 axis = mk(L[1], L[2], L[3]) - ro;
+            const float dist = sqrtf(dot3(axis, axis));
+            if (!(dist > fmaxf(fmaxf(L[14], 0.0f), 1e-3f))) continue;
+            const float3 d = axis * (1.0f / dist);
+            const float omega = fminf(6.283185307179586f, fmaxf(L[15], 0.0f) / (dist * dist));
+            const float kVirtual = fminf(float(N), float(N) * omega / 12.566370614359172f);
+            const float vis = C.emitterVis[(size_t)probeIndex * EMITTER_CAP + e];
+            const float wk = pow64(fmaxf(td.x * d.x + td.y * d.y + td.z * d.z, 0.0f)) * kVirtual;
+            kahan_fma(ar, kr, wk, L[7] * vis);
+            kahan_fma(ag, kg, wk, L[8] * vis);
+            kahan_fma(ab, kb, wk, L[9] * vis);
+            kahan_fma(ah, kh, wk, 1.0f);
+            aw += wk;
+        }
+        // numerator / support history (gi_probes.js:2640-2674)
+        const size_t gt = (size_t)probeIndex * texels + local;
+        const float4 prevNum = C.glossyNum[gt];
+        const float prevDen = C.glossyDen[gt];
+        const float4 curNum = make_float4(ar * invRays, ag * invRays, ab * invRays, ah * invRays);
+        const float curDen = aw * invRays;
+        const bool empty = prevDen < 1e-6f;
+        const float H = P.hysteresis;
+        const float refH = H + (1.0f - H) * P.debugTempNoiseHBoost;
+        const float glossyH = powf(clampf(refH, 1e-6f, 1.0f), P.hysteresisExponent * float(C.glossyInterval));
+        const float gh = empty ? 0.0f : glossyH;
+        const float4 num = make_float4(mixf(curNum.x, prevNum.x, gh), mixf(curNum.y, prevNum.y, gh),
+                                       mixf(curNum.z, prevNum.z, gh), mixf(curNum.w, prevNum.w, gh));
+        const float den = fmaxf(mixf(curDen, prevDen, gh), 1e-6f);
+        C.glossyNum[gt] = num;
+        C.glossyDen[gt] = den;
+        const uint32_t col = probeIndex % C.glossyTilesX, row = probeIndex / C.glossyTilesX;
+        const size_t t = (size_t)(row * tile + (uint32_t)ly) * C.glossyAtlasW + col * tile + (uint32_t)lx;
+        C.glossyAtlas[t] = float4_to_half4(make_float4(num.x / den, num.y / den, num.z / den,
+                                                       clampf(num.w / den, 0.0f, 1.0f)));
+    }
+}
+
+cudaError_t launch_glossy(const DevCascade& C, const DevParams& P, cudaStream_t st) {
+    if (C.updatedCount == 0 || !C.glossyNum || C.glossyInterval == 0) return cudaSuccess;
+    k_glossy<<<C.updatedCount, GLOSSY_THREADS, 0, st>>>(C, P); note_launch();
+    return cudaGetLastError();
+}
 
 // lightGridKernel, gi_probes.js:1893-1937. Every operation is separately
 // rounded (no contraction) so the lists match an FP32 evaluation exactly.

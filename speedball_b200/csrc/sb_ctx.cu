@@ -2,6 +2,7 @@
 // light uploads in the reference layouts, cascade configuration, solves, the
 // refit / TLAS lanes and read-back. Host code; all device work is enqueued on
 // the context's stream.
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -44,6 +45,15 @@ struct Cascade {
     size_t batchCap = 0;
     bool batchOrderReady = false;
     float* emitterVis = nullptr;  // probeTotal x 16 emitter visibility history
+    // reflection lobes, allocated for reflTier (sb_set_reflection_quality)
+    uint32_t reflTier = 0;
+    float4* roughSpec = nullptr;
+    uint2* roughAtlas = nullptr;
+    float4* glossyNum = nullptr;
+    float* glossyDen = nullptr;
+    uint2* glossyAtlas = nullptr;
+    uint32_t glossyOct = 1, glossyTile = 1, glossyInterval = 0, glossyPhase = 0;
+    uint32_t glossyTilesX = 1, glossyTilesY = 1;
 };
 
 }  // namespace
@@ -87,6 +97,7 @@ struct sb_ctx {
     Cascade casc[SB_MAX_CASCADES];
     sb_params params{};
     uint32_t lightCount = 0, emitterBase = 0, emitterCount = 0;
+    uint32_t reflectTier = 0;  // sb_set_reflection_quality
     int32_t clustered = 0;
     bool lightGridDirty = false;
     bool lightGatesDirty = false;  // the gate table lags the light records
@@ -272,7 +283,55 @@ DevCascade dev_cascade(const sb_ctx* c, uint32_t ci, uint32_t probeOffset, uint3
     D.emitterBase = c->emitterBase;
     D.emitterCount = c->emitterCount;
     D.emitterVis = K.emitterVis;
+    D.reflect = K.reflTier;
+    D.roughSpec = K.roughSpec;
+    D.roughAtlas = K.roughAtlas;
+    D.glossyNum = K.glossyNum;
+    D.glossyDen = K.glossyDen;
+    D.glossyAtlas = K.glossyAtlas;
+    D.glossyOct = K.glossyOct;
+    D.glossyTile = K.glossyTile;
+    D.glossyInterval = K.glossyInterval;
+    D.glossyPhase = K.glossyPhase;
+    D.glossyTilesX = K.glossyTilesX;
+    D.glossyAtlasW = K.glossyTilesX * K.glossyTile;
     return D;
+}
+
+// The reflection buffers of one cascade for ctx->reflectTier
+// (REFLECTION_QUALITY_TIERS, gi_probes.js:60-65; glossy tiles and their packing
+// 970-975, 3103-3110), all cleared: histories and supports to 0, the rough
+// and glossy atlases to vec4(0) (clearAtlasKernel / clearGlossyAtlasKernel,
+// 2703-2724). The glossy phase restarts at 0.
+sb_status alloc_reflection(sb_ctx* ctx, Cascade& K) {
+    release(K.roughSpec); release(K.roughAtlas); release(K.glossyNum); release(K.glossyDen);
+    release(K.glossyAtlas);
+    const uint32_t tier = ctx->reflectTier, P = K.probeTotal;
+    K.reflTier = tier;
+    K.glossyPhase = 0;
+    K.glossyOct = tier == SB_REFLECT_HIGH ? 8u : tier == SB_REFLECT_ULTRA ? 16u : 1u;
+    K.glossyTile = tier >= SB_REFLECT_HIGH ? K.glossyOct + 2u : 1u;
+    K.glossyInterval = tier == SB_REFLECT_HIGH ? 2u : tier == SB_REFLECT_ULTRA ? 1u : 0u;
+    K.glossyTilesX = tier >= SB_REFLECT_HIGH ? std::max(1u, (uint32_t)std::ceil(std::sqrt((double)P))) : 1u;
+    K.glossyTilesY = tier >= SB_REFLECT_HIGH ? std::max(1u, (P + K.glossyTilesX - 1) / K.glossyTilesX) : 1u;
+    if (tier == SB_REFLECT_OFF || P == 0) return SB_OK;
+    size_t c = 0;
+    const size_t texels = (size_t)P * 64u;
+    CK(grow(K.roughSpec, c, texels)); c = 0;
+    CK(grow(K.roughAtlas, c, texels)); c = 0;
+    CK(cudaMemsetAsync(K.roughSpec, 0, texels * sizeof(float4), ctx->stream));
+    CK(cudaMemsetAsync(K.roughAtlas, 0, texels * sizeof(uint2), ctx->stream));
+    if (tier >= SB_REFLECT_HIGH) {
+        const size_t gt = (size_t)P * K.glossyTile * K.glossyTile;
+        const size_t ga = (size_t)K.glossyTilesX * K.glossyTile * K.glossyTilesY * K.glossyTile;
+        CK(grow(K.glossyNum, c, gt)); c = 0;
+        CK(grow(K.glossyDen, c, gt)); c = 0;
+        CK(grow(K.glossyAtlas, c, ga)); c = 0;
+        CK(cudaMemsetAsync(K.glossyNum, 0, gt * sizeof(float4), ctx->stream));
+        CK(cudaMemsetAsync(K.glossyDen, 0, gt * sizeof(float), ctx->stream));
+        CK(cudaMemsetAsync(K.glossyAtlas, 0, ga * sizeof(uint2), ctx->stream));
+    }
+    return SB_OK;
 }
 
 sb_status pack_if_needed(sb_ctx* ctx) {
@@ -443,6 +502,8 @@ void sb_destroy(sb_ctx* ctx) {
         release(K.emitterVis);
         release(K.tileOrder); release(K.batchCost); release(K.batchOrder);
         release(K.vis);
+        release(K.roughSpec); release(K.roughAtlas); release(K.glossyNum); release(K.glossyDen);
+        release(K.glossyAtlas);
     }
     release(ctx->jobs);
     auto& G = ctx->graph;
@@ -663,6 +724,21 @@ static sb_status read_enqueue(sb_ctx* ctx, uint32_t which, uint32_t start, uint3
         case SB_BUF_INSTANCE_BOUNDS: srcp = ctx->I.liveBounds; len = ctx->instancesSet ? (size_t)ctx->I.count * 6 : 0; break;
         case SB_BUF_RECORD_E: srcp = ctx->tape.E; len = ctx->tape.ready ? (size_t)ctx->tape.probes * 36 * 4 : 0; break;
         case SB_BUF_EMITTER_VIS: if (K) { srcp = K->emitterVis; len = K->emitterVis ? (size_t)K->probeTotal * EMITTER_CAP : 0; } break;
+        case SB_BUF_ROUGH_SPECULAR: if (K) { srcp = K->roughSpec; len = K->roughSpec ? (size_t)K->probeTotal * 256 : 0; } break;
+        case SB_BUF_ROUGH_ATLAS: if (K) { srcp = K->roughAtlas; len = K->roughAtlas ? (size_t)K->atlasW * K->atlasH * 4 : 0; esz = 2; } break;
+        case SB_BUF_GLOSSY_SPECULAR:
+            if (K) { srcp = K->glossyNum; len = K->glossyNum ? (size_t)K->probeTotal * K->glossyTile * K->glossyTile * 4 : 0; }
+            break;
+        case SB_BUF_GLOSSY_WEIGHT:
+            if (K) { srcp = K->glossyDen; len = K->glossyDen ? (size_t)K->probeTotal * K->glossyTile * K->glossyTile : 0; }
+            break;
+        case SB_BUF_GLOSSY_ATLAS:
+            if (K) {
+                srcp = K->glossyAtlas;
+                len = K->glossyAtlas ? (size_t)K->glossyTilesX * K->glossyTile * K->glossyTilesY * K->glossyTile * 4 : 0;
+                esz = 2;
+            }
+            break;
         default: return fail(ctx, SB_ERR_INVALID_ARG, "unknown buffer %u", buf);
     }
     if (!srcp) return fail(ctx, SB_ERR_NOT_READY, "buffer %u not available", buf);
@@ -727,6 +803,39 @@ sb_status sb_set_params(sb_ctx* ctx, const sb_params* p) {
     return SB_OK;
 }
 
+sb_status sb_set_reflection_quality(sb_ctx* ctx, uint32_t tier) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (tier > SB_REFLECT_ULTRA) return fail(ctx, SB_ERR_INVALID_ARG, "reflection tier %u (off, rough, high, ultra)", tier);
+    if (ctx->capturing) return fail(ctx, SB_ERR_NOT_READY, "reflection buffers cannot be reallocated inside a graph capture");
+    cudaSetDevice(ctx->device);
+    ctx->reflectTier = tier;
+    for (auto& K : ctx->casc) {
+        if (!K.configured) continue;
+        sb_status s = alloc_reflection(ctx, K);
+        if (s != SB_OK) return s;
+    }
+    ++ctx->epoch;
+    ++ctx->structGen;
+    return SB_OK;
+}
+
+sb_status sb_get_reflection_layout(sb_ctx* ctx, uint32_t ci, sb_reflection_layout* out) {
+    if (!ctx || !out) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (ci >= SB_MAX_CASCADES || !ctx->casc[ci].configured)
+        return fail(ctx, SB_ERR_INVALID_ARG, "cascade %u is not configured", ci);
+    const Cascade& K = ctx->casc[ci];
+    out->tier = K.reflTier;
+    out->glossyOct = K.reflTier >= SB_REFLECT_HIGH ? K.glossyOct : 0u;
+    out->glossyTile = K.reflTier >= SB_REFLECT_HIGH ? K.glossyTile : 0u;
+    out->glossyInterval = K.glossyInterval;
+    out->glossyTilesX = K.glossyTilesX;
+    out->glossyTilesY = K.glossyTilesY;
+    out->glossyAtlasW = K.reflTier >= SB_REFLECT_HIGH ? K.glossyTilesX * K.glossyTile : 0u;
+    out->glossyAtlasH = K.reflTier >= SB_REFLECT_HIGH ? K.glossyTilesY * K.glossyTile : 0u;
+    out->glossyPhase = K.glossyPhase;
+    return SB_OK;
+}
+
 sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
     if (!ctx) return SB_ERR_INVALID_ARG;
     if (ci >= SB_MAX_CASCADES) return fail(ctx, SB_ERR_INVALID_ARG, "cascade %u >= %u", ci, SB_MAX_CASCADES);
@@ -788,6 +897,11 @@ sb_status sb_configure_cascade(sb_ctx* ctx, uint32_t ci, const sb_grid* g) {
     K.atlasW = g->res[0] * 8;
     K.atlasH = g->res[1] * g->res[2] * 8;
     K.configured = true;
+    if (!sameDims || K.reflTier != ctx->reflectTier) {
+        s = alloc_reflection(ctx, K);
+        if (s != SB_OK) return s;
+    }
+    K.glossyPhase = 0;  // every rebuild restarts the glossy interleave (gi_probes.js:3162, 3193, 3224)
     ++ctx->epoch;
     ++ctx->structGen;
     if (!sameDims) {
@@ -865,6 +979,12 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
     if (ctx->emitterCount) CK(launch_emitter_vis(S, D, P, ctx->dErr, ctx->stream));
     if (timing) CK(cudaEventRecord(ctx->evMid, ctx->stream));
     CK(launch_blend_upload(D, P, ctx->stream));
+    if (K.reflTier >= SB_REFLECT_HIGH) {
+        // glossyKernel after the blend (gi_probes.js:3829-3835): this solve resolves
+        // the texels of phase D.glossyPhase, the next one the following phase
+        CK(launch_glossy(D, P, ctx->stream));
+        K.glossyPhase = (K.glossyPhase + 1u) % K.glossyInterval;
+    }
     if (costOrder) K.batchOrderReady = true;
     if (timing) CK(cudaEventRecord(ctx->ev1, ctx->stream));
     ctx->timed = ctx->timed || timing;
@@ -1010,6 +1130,8 @@ static sb_status check_batch(const sb_solve_item* items, uint32_t count) {
         if (!c || c->device != lead->device) return fail(lead, SB_ERR_INVALID_ARG, "item %u: null context or another device", i);
         if (c->emitterCount)
             return fail(lead, SB_ERR_UNSUPPORTED, "item %u: giEmitter records are solved by sb_solve only", i);
+        if (c->reflectTier)
+            return fail(lead, SB_ERR_UNSUPPORTED, "item %u: reflection lobes are solved by sb_solve only", i);
         for (uint32_t j = 0; j < i; ++j)
             if (items[j].ctx == c && items[j].cascade == items[i].cascade)
                 return fail(lead, SB_ERR_INVALID_ARG, "items %u and %u solve the same cascade", j, i);
@@ -1258,19 +1380,18 @@ sb_status sb_graph_launch(sb_ctx* ctx) {
 struct CascadeSnapshot {
     sb_ctx* ctx = nullptr;
     uint32_t ci = 0;
-    float4* irr = nullptr;
-    float2* depth = nullptr;
-    uint2 *atlas = nullptr, *datlas = nullptr;
+    uint32_t glossyPhase = 0;
+    struct Region { void* live; void* copy; size_t bytes; };
+    std::vector<Region> regions;  // histories, atlases, emitter visibility, reflection lobes
+    CascadeSnapshot() = default;
+    CascadeSnapshot(const CascadeSnapshot&) = delete;
+    CascadeSnapshot& operator=(const CascadeSnapshot&) = delete;
 
     cudaError_t copy(bool save) {
-        Cascade& K = ctx->casc[ci];
-        const size_t hist = (size_t)K.probeTotal * 64, texels = (size_t)K.atlasW * K.atlasH;
-        struct { void* a; void* b; size_t n; } m[4] = {{irr, K.irr, hist * 16}, {depth, K.depth, hist * 8},
-                                                      {atlas, K.atlas, texels * 8}, {datlas, K.depthAtlas, texels * 8}};
-        for (auto& x : m) {
-            cudaError_t r = cudaMemcpyAsync(save ? x.a : x.b, save ? x.b : x.a, x.n, cudaMemcpyDeviceToDevice,
-                                            ctx->stream);
-            if (r != cudaSuccess) return r;
+        for (auto& r : regions) {
+            cudaError_t e = cudaMemcpyAsync(save ? r.copy : r.live, save ? r.live : r.copy, r.bytes,
+                                            cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
     }
@@ -1278,23 +1399,32 @@ struct CascadeSnapshot {
         ctx = c;
         ci = cascade;
         Cascade& K = c->casc[cascade];
+        glossyPhase = K.glossyPhase;
         const size_t hist = (size_t)K.probeTotal * 64, texels = (size_t)K.atlasW * K.atlasH;
-        size_t c0 = 0, c1 = 0, c2 = 0, c3 = 0;
-        cudaError_t e = grow(irr, c0, hist);
-        if (e == cudaSuccess) e = grow(depth, c1, hist);
-        if (e == cudaSuccess) e = grow(atlas, c2, texels);
-        if (e == cudaSuccess) e = grow(datlas, c3, texels);
-        return e == cudaSuccess ? copy(true) : e;
+        const size_t gt = (size_t)K.probeTotal * K.glossyTile * K.glossyTile;
+        const size_t ga = (size_t)K.glossyTilesX * K.glossyTile * K.glossyTilesY * K.glossyTile;
+        const Region want[] = {{K.irr, nullptr, hist * 16}, {K.depth, nullptr, hist * 8},
+                               {K.atlas, nullptr, texels * 8}, {K.depthAtlas, nullptr, texels * 8},
+                               {K.emitterVis, nullptr, (size_t)K.probeTotal * EMITTER_CAP * 4},
+                               {K.roughSpec, nullptr, hist * 16}, {K.roughAtlas, nullptr, texels * 8},
+                               {K.glossyNum, nullptr, gt * 16}, {K.glossyDen, nullptr, gt * 4},
+                               {K.glossyAtlas, nullptr, ga * 8}};
+        for (const Region& r : want) {
+            if (!r.live || !r.bytes) continue;
+            Region x = r;
+            cudaError_t e = cudaMalloc(&x.copy, x.bytes);
+            if (e != cudaSuccess) return e;
+            regions.push_back(x);
+        }
+        return copy(true);
     }
     cudaError_t restore() {
+        ctx->casc[ci].glossyPhase = glossyPhase;
         cudaError_t e = copy(false);
         return e == cudaSuccess ? cudaStreamSynchronize(ctx->stream) : e;
     }
     ~CascadeSnapshot() {
-        release(irr);
-        release(depth);
-        release(atlas);
-        release(datlas);
+        for (auto& r : regions) release(r.copy);
     }
 };
 
@@ -1422,6 +1552,8 @@ sb_status sb_forward_record(sb_ctx* ctx, uint32_t ci, uint32_t solves, const flo
         return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", ci);
     if (ctx->emitterCount)
         return fail(ctx, SB_ERR_UNSUPPORTED, "the adjoint does not cover giEmitter virtual rays");
+    if (ctx->reflectTier)
+        return fail(ctx, SB_ERR_UNSUPPORTED, "the adjoint does not cover the reflection lobes");
     cudaSetDevice(ctx->device);
     Cascade& K = ctx->casc[ci];
     auto& T = ctx->tape;

@@ -128,9 +128,21 @@ struct DevCascade {
     const float* lights;
     uint32_t emitterBase, emitterCount;
     float* emitterVis;
+    // reflection lobes (tier 0 off, 1 rough, 2 high, 3 ultra; gi_probes.js:60-75):
+    // rough history probeTotal*64 and its RGBA16F atlas in the irradiance layout;
+    // glossy numerator / support per glossy texel (probeTotal*glossyTile^2) and
+    // the glossy atlas, tile of probe p at (p % glossyTilesX, p / glossyTilesX)
+    uint32_t reflect;
+    float4* roughSpec;
+    uint2* roughAtlas;
+    float4* glossyNum;
+    float* glossyDen;
+    uint2* glossyAtlas;
+    uint32_t glossyOct, glossyTile, glossyInterval, glossyPhase, glossyTilesX, glossyAtlasW;
 };
 constexpr uint32_t EMITTER_CAP = 16;          // GI_EMITTER_INJECT_CAP, gi_probes.js:133
 constexpr float EMITTER_VIS_RETENTION = 0.8f;  // GI_EMITTER_VIS_RETENTION, gi_probes.js:134
+constexpr float ROUGH_UNSHADED_T_BIAS = 2.0f;  // gi_probes.js:94
 
 struct DevParams {
     float frameJitter, emitterVisSeed;
@@ -146,6 +158,7 @@ struct DevParams {
     float debugTempNoiseHBoost, debugTempChangeSigma0, debugTempMinChangeH;
     float debugTempVarEps, debugTempVarRel, debugDepthHistoryScale;
     float debugFilterKScale, debugFilterRelScale, debugFilterEpsScale;
+    float reflectionSkyFallback, skyConfigured;
 };
 static_assert(sizeof(DevParams) == sizeof(sb_params), "DevParams mirrors sb_params");
 

@@ -55,6 +55,7 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
                          float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
                          cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
+cudaError_t launch_glossy(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t slotCount,
                          cudaStream_t st);
 

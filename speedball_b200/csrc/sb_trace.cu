@@ -235,6 +235,14 @@ __device__ __forceinline__ void shade_ray(const WaveCtx& W, uint32_t g) {
         float metal = __ldg(M + 4), transm = __ldg(M + 5);
         float3 kdr = baseColor * W.P.debugAlbedoScale * (1.0f - metal) * (1.0f - transm);
         float3 kd = mk(clampf(kdr.x, 0.f, 0.95f), clampf(kdr.y, 0.f, 0.95f), clampf(kdr.z, 0.f, 0.95f));
+        if (C.reflect) {
+            // with the reflection lobes on, a hit on a surface with no diffuse energy
+            // and no emission is stored as -(t + 2): the blend keeps its depth, the
+            // lobes ignore it (gi_probes.js:2055-2062)
+            const float diffuseEnergy = (1.0f - metal) * (1.0f - transm);
+            const float emissivePeak = fmaxf(fmaxf(emissive.x, emissive.y), emissive.z);
+            if (!(diffuseEnergy > 0.02f || emissivePeak > 1e-6f)) hitT = -(t + ROUGH_UNSHADED_T_BIAS);
+        }
         uint4 v = C.vis[rayIdx];
         unsigned long long ok = (unsigned long long)v.z | ((unsigned long long)v.w << 32);
         while (ok) {

@@ -41,6 +41,20 @@ TICK_OVERLOAD_MS = 100.0
 C1_RES_SCALE = 2.0
 
 
+REFLECTION_QUALITY_TIERS = ("off", "rough", "high", "ultra")
+
+
+def resolveReflectionQuality(reflectionQuality=None, roughReflections=False) -> str:
+    """resolveReflectionQuality (gi_probes.js:67-73): a tier name (off, rough,
+    high, ultra; case and surrounding space ignored) or, when None, the legacy
+    boolean (True = ultra, False = off)."""
+    fallback = "ultra" if roughReflections is True else "off"
+    name = fallback if reflectionQuality is None else str(reflectionQuality).strip().lower()
+    if name not in REFLECTION_QUALITY_TIERS:
+        raise ValueError(f'Unknown reflectionQuality "{reflectionQuality}". Expected off, rough, high, or ultra.')
+    return name
+
+
 def hysteresisExponentForInterval(updateDtMs: float, normalize: bool = True) -> float:
     """gi_probes.js:235-251."""
     if not normalize:
@@ -100,8 +114,10 @@ class ProbeField:
     def __init__(self, scene: SceneDesc, *, intensity=1.0, hysteresis=None, jitterMode="gated", divisions=12,
                  rays=RAYS_PER_PROBE_DEFAULT, cascades=2, clusteredLighting=False, volumes=None, device=0,
                  recordHits=False, onRebuilt: Callable | None = None, variant: str | None = None,
-                 blasBuilder: str = "host"):
+                 blasBuilder: str = "host", reflectionQuality: str | None = None, roughReflections=False,
+                 reflectionSkyFallback=False):
         self._lib = _abi.load(variant)
+        self._reflection = resolveReflectionQuality(reflectionQuality, roughReflections)
         if blasBuilder not in ("host", "gpu"):
             raise ValueError("blasBuilder: 'host' or 'gpu'")
         self._blasBuilder = blasBuilder
@@ -143,6 +159,7 @@ class ProbeField:
         self._extraCascades = {}  # extra cascade boxes (ci >= 1) configured by configureCascade
         self._params = _abi.default_params()
         self._params.hysteresis = self._hysteresis
+        self._params.reflectionSkyFallback = 1.0 if reflectionSkyFallback is True else 0.0
         self._frameJitterOverride = None
         flags = _abi.SB_CTX_RECORD_HITS if recordHits else 0
         opts = _abi.sb_device_opts(device, flags)
@@ -150,6 +167,8 @@ class ProbeField:
         _abi.check(self._lib.sb_create(C.byref(opts), C.byref(h)))
         self._ctx = h
         self.stats = {"solves": 0, "refits": 0, "transformUpdates": 0, "rebuilds": 0}
+        # structural: the reflection buffers of every cascade follow the tier
+        self._ck(self._lib.sb_set_reflection_quality(h, _abi.REFLECT_TIERS[self._reflection]))
         self._rebuild()
 
     # ------------------------------------------------------------- plumbing
@@ -399,13 +418,17 @@ class ProbeField:
         self._ck(self._lib.sb_configure_cascade(self._ctx, ci, C.byref(g)))
         self._extraCascades[ci] = g
 
-    def cascadeProbes(self, ci: int) -> int:
+    def cascadeGrid(self, ci: int):
+        """The sb_grid cascade `ci` was configured with: C0, the fitted fine
+        cascade C1, or a cascade set by configureCascade."""
         if ci == 0:
-            g = self._grid
-        elif ci == 1 and self._haveC1 and ci not in self._extraCascades:
-            g = self._c1Grid
-        else:
-            g = self._extraCascades[ci]
+            return self._grid
+        if ci == 1 and self._haveC1 and ci not in self._extraCascades:
+            return self._c1Grid
+        return self._extraCascades[ci]
+
+    def cascadeProbes(self, ci: int) -> int:
+        g = self.cascadeGrid(ci)
         return int(g.res[0] * g.res[1] * g.res[2])
 
     def hasFineCascade(self) -> bool:
@@ -560,9 +583,29 @@ class ProbeField:
         self._params.filterSmooth = min(1.0, max(0.0, float(v)))
 
     def setSky(self, sh9=None):
+        """setSky (gi_probes.js:1312-1318): nine SH coefficients x RGB; None
+        clears the sky and marks it unconfigured (no reflection sky fallback)."""
         sh = np.zeros(27, np.float32) if sh9 is None else np.asarray(sh9, np.float32).reshape(27)
         for i in range(27):
             self._params.skySH[i] = float(sh[i])
+        self._params.skyConfigured = 0.0 if sh9 is None else 1.0
+
+    def setReflectionSkyFallback(self, on):
+        """A true miss feeds the reflection lobes with the sky (gi_probes.js:1320-1324)."""
+        self._params.reflectionSkyFallback = 1.0 if on is True else 0.0
+
+    def getReflectionSkyFallback(self):
+        return self._params.reflectionSkyFallback > 0.5
+
+    def getReflectionQuality(self) -> str:
+        return self._reflection
+
+    def reflectionLayout(self, ci: int = 0) -> dict:
+        """The cascade's reflection layout: tier, glossy tile geometry and the
+        glossy phase of its next solve."""
+        lay = _abi.sb_reflection_layout()
+        self._ck(self._lib.sb_get_reflection_layout(self._ctx, ci, C.byref(lay)))
+        return {n: int(getattr(lay, n)) for n, _ in lay._fields_}
 
     def setSkyIntensity(self, v):
         self._params.skyIntensity = max(0.0, float(v))
@@ -710,12 +753,14 @@ class SpeedballGIHandle:
 
 
 def installSpeedballGI(scene: SceneDesc, *, enabled=True, intensity=10, divisions=16, rays=64, cascades=2,
-                       hysteresis=None, jitterMode="gated", clusteredLighting=False, volumes=None, device=0,
+                       hysteresis=None, jitterMode="gated", roughReflections=False, reflectionQuality=None,
+                       reflectionSkyFallback=False, clusteredLighting=False, volumes=None, device=0,
                        onError=None, **_ignored) -> SpeedballGIHandle:
     """install.js:216-239 with the renderer/camera replaced by the scene description."""
     if onError is not None and not callable(onError):
         raise TypeError("installSpeedballGI: onError must be a function when provided.")
     field = createProbeField(scene, intensity=intensity, hysteresis=hysteresis, jitterMode=jitterMode,
                              divisions=divisions, rays=rays, cascades=cascades, clusteredLighting=clusteredLighting,
-                             volumes=volumes, device=device)
+                             volumes=volumes, device=device, reflectionQuality=reflectionQuality,
+                             roughReflections=roughReflections, reflectionSkyFallback=reflectionSkyFallback)
     return SpeedballGIHandle(field, onError)

@@ -459,6 +459,26 @@ def large_pose(scene: SceneDesc, frame: int, seed: int = 11, max_deg: float = 15
     return skin(rest, rig, axes * ang[:, None])
 
 
+def large_field(scene: SceneDesc, device: int = 0, recordHits: bool = False):
+    """The large scene's probe field: C0 = 32^3 probes x 256 rays over the
+    world box; C1 = the fine cascade that fitFineBox places inside it
+    (gi_probes.js:3370-3410) at up to 32 probes per axis (divisions 32, so
+    the C1 density target 2 x 32 meets the per-axis cap). Clustered lights,
+    gated jitter, normalisation off, full updates. A pool whose centroid
+    histogram gives no fine box gets the half-extent box around C0's centre."""
+    from .field import ProbeField
+    g = scene.meta["grid"]
+    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=2,
+                   divisions=32, rays=g["rays"], clusteredLighting=True, hysteresis=scene.meta["hysteresis"],
+                   jitterMode="gated", recordHits=recordHits, device=device)
+    f.setHysteresisNormalization(False)
+    f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)
+    if not f.hasFineCascade():
+        c1 = nested_cascades(g, res=(g["res"], g["res"]), scale=0.5)[1]
+        f.configureCascade(1, c1["gridMin"], c1["gridSize"], c1["res"])
+    return f
+
+
 BATCH_SCENE_TRIS = (20_000, 45_000, 80_000, 120_000, 200_000, 262_000, 350_000, 500_000)
 
 

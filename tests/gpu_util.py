@@ -24,12 +24,12 @@ def grid_dict(g: _abi.sb_grid) -> dict:
                 res=[g.res[a] for a in range(3)], rays=g.raysPerProbe, maxDist=g.maxDist, cellMin=g.cellMin)
 
 
-def make_field(scene, record=True, rays=None) -> ProbeField:
+def make_field(scene, record=True, rays=None, **opts) -> ProbeField:
     m = scene.meta
     g = m["grid"]
     f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1,
                    rays=rays or g["rays"], clusteredLighting=m.get("clustered", False),
-                   hysteresis=m.get("hysteresis"), jitterMode=m.get("jitter", "gated"), recordHits=record)
+                   hysteresis=m.get("hysteresis"), jitterMode=m.get("jitter", "gated"), recordHits=record, **opts)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)  # one solve covers every probe
     return f
@@ -55,7 +55,7 @@ class OracleMirror:
         self.vertex = read(field, "VERTEX_DATA", pool.vertexData.size, np.float32).reshape(-1, 8)
         self.keep = []
         self.scene = orc.scene_struct(pool, self.materials, nodes=self.nodes, vertex=self.vertex, keep=self.keep)
-        self.gdict = grid_dict(field.grid if cascade == 0 else field._c1Grid)
+        self.gdict = grid_dict(field.cascadeGrid(cascade))
         self.grid = orc.grid_struct(self.gdict)
         self.g0dict = grid_dict(field.grid)
         self.grid0 = orc.grid_struct(self.g0dict)
@@ -73,6 +73,22 @@ class OracleMirror:
         self.irr, self.depth, self.atlas, self.depth_atlas = orc.new_state(g, fp32)
         r = g["res"]
         self.evis = np.zeros(r[0] * r[1] * r[2] * 16, np.float32 if fp32 else np.float64)
+        tier = _abi.REFLECT_TIERS[field.getReflectionQuality()]
+        self.rf = orc.ReflectState(g, tier, fp32) if tier else None
+
+    def reflect_state(self):
+        rf = self.rf
+        if rf is None:
+            return None
+        return (rf.rough.copy(), rf.rough_atlas.copy(), rf.glossy_num.copy(), rf.glossy_den.copy(),
+                rf.glossy_atlas.copy(), rf.phase)
+
+    def restore_reflect(self, st):
+        if st is None:
+            return
+        rf = self.rf
+        rf.rough[...], rf.rough_atlas[...], rf.glossy_num[...], rf.glossy_den[...], rf.glossy_atlas[...] = st[:5]
+        rf.phase = st[5]
 
     def params(self) -> np.ndarray:
         return self.field._params.to_array()
@@ -99,9 +115,13 @@ class OracleMirror:
         if replay is not None:
             io.replayTri = orc._p(replay["tri"]); io.replayInst = orc._p(replay["inst_word"])
             io.replayBlocked = orc._p(replay["blocked"])
+        if self.rf is not None:
+            self.rf.attach(io)
         orc.solve(self.scene, self.arena, self.light_count, self.clustered, self.grid, self.grid0,
                   self.params() if params is None else params,
                   offset, updated, self.irr, self.depth, self.atlas, self.depth_atlas, fp32=self.fp32, io=io, emitters=self.emitters)
+        if self.rf is not None:
+            self.rf.advance()
         return out
 
 
@@ -246,10 +266,12 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
     rec = gpu_records(f, n, ci)
     saved = (mirror.irr.copy(), mirror.depth.copy(), mirror.atlas.copy(), mirror.depth_atlas.copy(),
              mirror.evis.copy())
+    saved_rf = mirror.reflect_state()
     ind = mirror.solve(off, upd, replay=None, params=sched_params)
     samples = mirror.evis_samples
     mirror.irr, mirror.depth, mirror.atlas, mirror.depth_atlas, evis_before = saved
     mirror.evis[...] = evis_before
+    mirror.restore_reflect(saved_rf)
     gpu_evis = None
     if mirror.emitters[1]:
         # the GPU's visibility history after this solve, and the samples it implies
@@ -279,4 +301,39 @@ def solve_parity(f: ProbeField, mirror: OracleMirror, frame: dict, sched_params:
                   hit_share=float((rec["tri"] >= 0).mean()))
     if gpu_evis is not None:
         counts["emitter_sample_agreement"] = [float(x) for x in emitter_agree]
+    if mirror.rf is not None:
+        counts.update(reflection_parity(f, mirror))
     return counts
+
+
+def reflection_parity(f: ProbeField, mirror: OracleMirror) -> dict:
+    """The reflection lobes after a replayed solve: the rough history and atlas
+    and (tiers high / ultra) the glossy numerator, support and atlas, each
+    within 1e-3 relative of the oracle's (colour and coverage separately, floor
+    1e-3 of the largest magnitude)."""
+    rf, ci = mirror.rf, mirror.cascade
+    out = {}
+
+    def cmp(name, g, o, stride):
+        g = g.reshape(-1, stride)
+        o = o.reshape(-1, stride)
+        errs = [texel_rel_err(g[:, :3], o[:, :3]).max()] + ([texel_rel_err(g[:, 3], o[:, 3]).max()] if stride == 4 else [])
+        e = float(max(errs))
+        assert e <= TEXEL_REL, (name, e)
+        out[name] = e
+
+    cmp("rough_hist_err", read(f, "ROUGH_SPECULAR", rf.rough.size, np.float32, ci), rf.rough, 4)
+    cmp("rough_atlas_err", half_to_f(read(f, "ROUGH_ATLAS", rf.rough_atlas.size, np.uint16, ci)),
+        half_to_f(rf.rough_atlas.reshape(-1)), 4)
+    out["rough_coverage_mean"] = float(rf.rough.reshape(-1, 4)[:, 3].mean())
+    if rf.tier >= 2:
+        gd = read(f, "GLOSSY_WEIGHT", rf.glossy_den.size, np.float32, ci)
+        err = texel_rel_err(gd, rf.glossy_den)
+        assert err.max() <= TEXEL_REL, ("glossy_den", float(err.max()))
+        out["glossy_den_err"] = float(err.max())
+        cmp("glossy_num_err", read(f, "GLOSSY_SPECULAR", rf.glossy_num.size, np.float32, ci), rf.glossy_num, 4)
+        cmp("glossy_atlas_err", half_to_f(read(f, "GLOSSY_ATLAS", rf.glossy_atlas.size, np.uint16, ci)),
+            half_to_f(rf.glossy_atlas.reshape(-1)), 4)
+        lay = f.reflectionLayout(ci)
+        assert lay["glossyPhase"] == rf.phase, (lay, rf.phase)
+    return out

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(_abi.SIGNATURES), set(names) - set(_abi.SIGNATURES)
-    assert lib.sb_abi_version() == 1
+    assert lib.sb_abi_version() == 2
 
 
 def test_params_defaults_match_reference():
@@ -41,7 +41,8 @@ def test_params_defaults_match_reference():
     assert p.filterStrength == 1.0 and p.filterSmooth == 0.5
     assert p.tempChangeSigma1 == 2.5 and p.tempClampSigma == 6.0
     assert p.debugTempVarEps == pytest.approx(0.000025) and p.debugTempMinChangeH == pytest.approx(0.55)
-    assert len(p.to_array()) == len(_abi.PARAM_NAMES) == 58
+    assert p.reflectionSkyFallback == 0.0 and p.skyConfigured == 0.0
+    assert len(p.to_array()) == len(_abi.PARAM_NAMES) == 60
 
 
 def test_params_vector_matches_oracle(orc):

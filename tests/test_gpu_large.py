@@ -1,6 +1,6 @@
 """The large instanced scene (2.1M unique / 12.8M instanced triangles, a
-120k-triangle skinned mesh re-posed every frame, 2 cascades of 32^3 probes x
-256 rays) against the FP64 oracle, for every scene-BVH layout:
+120k-triangle skinned mesh re-posed every frame, C0 of 32^3 probes and the
+fine cascade C1 that fitFineBox places, 256 rays) against the FP64 oracle, for every scene-BVH layout:
 
   - hit triangle / instance of sampled probe rays (sb_raycast) identical to the
     oracle's FP64 closest hit except where the oracle explains the difference
@@ -18,7 +18,6 @@ import pytest
 
 import orc
 from speedball_b200 import _abi, synth
-from speedball_b200.field import ProbeField
 
 import gpu_util as gu
 
@@ -31,13 +30,7 @@ BLOCK = 64
 @pytest.fixture(scope="module")
 def large():
     scene = synth.large_scene()
-    g = scene.meta["grid"]
-    f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
-                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", recordHits=True)
-    f.setHysteresisNormalization(False)
-    f.setRayBudget(1 << 30, maxProbesPerTick=1 << 20)
-    c1 = synth.nested_cascades(g, res=(g["res"], g["res"]), scale=0.5)[1]
-    f.configureCascade(1, c1["gridMin"], c1["gridSize"], c1["res"])
+    f = synth.large_field(scene, recordHits=True)
     yield scene, f
     f.dispose()
 
@@ -126,7 +119,7 @@ def test_large_probe_block_matches_oracle(large, ci):
     scene, f = large
     _set_kind(f, 1)
     _frame(scene, f, 1)
-    g = f.grid if ci == 0 else f._extraCascades[ci]
+    g = f.cascadeGrid(ci)
     res = [g.res[a] for a in range(3)]
     P = res[0] * res[1] * res[2]
     W, H = res[0] * 8, res[1] * res[2] * 8
