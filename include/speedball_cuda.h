@@ -359,6 +359,8 @@ typedef struct sb_gather_params {
                                   is the fine box blended inside cascade 0        */
     uint32_t dualDetail;       /* 1: fetch at both normals and blend by
                                   detailStrength (one cascade only)               */
+    float reflectionIntensity; /* reflection layer scale, 0..1 (1)                */
+    float roughnessLimit;      /* receivers rougher than this get no reflection (1) */
 } sb_gather_params;
 void sb_gather_params_defaults(sb_gather_params* p);
 /* Receiver gather (GiProbeNode.sampleIrradiance and setup, gi_probes.js:530-657,
@@ -374,6 +376,24 @@ void sb_gather_params_defaults(sb_gather_params* p);
  * cascade not configured). */
 sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* params, const float* position,
                                const float* stableNormal, const float* detailNormal, uint32_t count, float* out);
+/* The combined receiver with the reflection lobes (GiProbeNode.
+ * sampleIrradianceAndRough / _sampleCombinedCascadeLooped and the reflection
+ * branch of setup, gi_probes.js:658-806, 893-925): per sample the irradiance
+ * (as sb_gather_irradiance, except that each cage is chosen at the biased
+ * point and the fine-box band at the surface position, as that path does)
+ * and the local reflection layer. reflection: DEVICE float4 per sample,
+ * xyz = the receiver's reflection direction (not necessarily unit), w = its
+ * roughness. Per cage tap with a live lobe the reflection ray is intersected
+ * with the sphere of the probe's mean depth toward it (parallax), and the rough
+ * atlas (and for tiers high / ultra the glossy atlas, blended by
+ * smoothstep(0.22, 0.58, roughness)) is fetched in the corrected direction,
+ * weighted by the tap weight squared. outReflection = (rgb * rw, coverage * rw)
+ * with rw = clamp(reflectionIntensity * enabled * (roughness <= roughnessLimit),
+ * 0, 1): the renderer composites radiance * (1 - w) + rgb. Needs a reflection
+ * tier other than off (SB_ERR_NOT_READY otherwise). */
+sb_status sb_gather_reflections(sb_ctx* ctx, const sb_gather_params* params, const float* position,
+                                const float* stableNormal, const float* detailNormal, const float* reflection,
+                                uint32_t count, float* outIrradiance, float* outReflection);
 
 /* ------------------------------------------------- refit / TLAS lanes (GPU) */
 

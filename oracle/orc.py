@@ -548,7 +548,7 @@ def grid_dict(grid_min, grid_size, res, rays) -> dict:
 # ---------------------------------------------------------- receiver gather
 GATHER_PARAM_NAMES = ["normalBias0", "normalBias1", "chebyBias0", "chebyBias1", "chebyStrength", "detailStrength",
                       "intensity", "enabled", "samplePositionScale", "sampleBiasScale", "borderBand", "cascades",
-                      "dualDetail"]
+                      "dualDetail", "reflectionIntensity", "roughnessLimit"]
 
 
 def gather_params(**kw) -> np.ndarray:
@@ -558,7 +558,7 @@ def gather_params(**kw) -> np.ndarray:
     each rounded to float32 as a uniform stores it."""
     v = dict(normalBias0=0.04, normalBias1=0.04, chebyBias0=0.0, chebyBias1=0.0, chebyStrength=0.0,
              detailStrength=1.0, intensity=1.0, enabled=1.0, samplePositionScale=1.0, sampleBiasScale=1.0,
-             borderBand=0.15, cascades=1.0, dualDetail=0.0)
+             borderBand=0.15, cascades=1.0, dualDetail=0.0, reflectionIntensity=1.0, roughnessLimit=1.0)
     v.update(kw)
     out = np.array([np.float32(v[k]) for k in GATHER_PARAM_NAMES], np.float64)
     assert out.shape[0] == load().orc_gather_params_size()
@@ -578,6 +578,50 @@ def gather(grid0: OrcGrid, atlas0: np.ndarray, depth0: np.ndarray, params: np.nd
                       _p(atlas1), _p(depth1), _p(np.ascontiguousarray(params, np.float64)), *[_p(a) for a in arr], n,
                       _p(out), _p(near), threads())
     return out, near
+
+
+class OrcReflectAtlas(C.Structure):
+    _fields_ = [("rough", C.c_void_p), ("glossy", C.c_void_p), ("glossyOct", C.c_uint32), ("glossyTile", C.c_uint32),
+                ("glossyTilesX", C.c_uint32), ("glossyW", C.c_uint32), ("glossyH", C.c_uint32)]
+
+
+def reflect_atlas(rough: np.ndarray, glossy: np.ndarray | None = None, oct_: int = 0, tiles_x: int = 1):
+    """A cascade's reflection atlases for gather_combined: the rough atlas (H x
+    W x 4 binary16) and, for tiers high / ultra, the glossy atlas with its
+    octahedral resolution and tiles per row."""
+    r = OrcReflectAtlas()
+    r.rough = _p(rough)
+    r._keep = (rough, glossy)
+    if glossy is not None:
+        r.glossy = _p(glossy)
+        r.glossyOct, r.glossyTile, r.glossyTilesX = oct_, oct_ + 2, tiles_x
+        r.glossyH, r.glossyW = glossy.shape[0], glossy.shape[1]
+    return r
+
+
+def gather_combined(grid0: OrcGrid, atlas0, depth0, refl0: OrcReflectAtlas, params: np.ndarray, pos4, nvis4, ndir4,
+                    rdir4, grid1: OrcGrid | None = None, atlas1=None, depth1=None,
+                    refl1: OrcReflectAtlas | None = None):
+    """FP64 combined receiver at n points: irradiance (n x 3), the reflection
+    layer (n x 4: rgb x weight, coverage x weight) and each point's distance to
+    a discontinuity (cage floor, Chebyshev select, parallax root selects,
+    roughness limit)."""
+    lib = load()
+    if not hasattr(lib, "_gc"):
+        P = C.c_void_p
+        lib.orc_gather_combined.restype = None
+        lib.orc_gather_combined.argtypes = [P] * 13 + [C.c_uint32, P, P, P, C.c_int32]
+        lib._gc = True
+    n = pos4.shape[0]
+    irr = np.zeros((n, 3), np.float64)
+    refl = np.zeros((n, 4), np.float64)
+    near = np.zeros(n, np.float64)
+    arr = [np.ascontiguousarray(a, np.float32) for a in (pos4, nvis4, ndir4, rdir4)]
+    lib.orc_gather_combined(C.byref(grid0), C.byref(grid1) if grid1 is not None else None, _p(atlas0), _p(depth0),
+                            _p(atlas1), _p(depth1), C.byref(refl0), C.byref(refl1) if refl1 is not None else None,
+                            _p(np.ascontiguousarray(params, np.float64)), *[_p(a) for a in arr], n, _p(irr), _p(refl),
+                            _p(near), threads())
+    return irr, refl, near
 
 
 # ------------------------------------------------- fine cascade placement

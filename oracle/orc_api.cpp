@@ -394,6 +394,48 @@ void orc_gather(const OrcGrid* g0, const OrcGrid* g1, const uint16_t* atlas0, co
 }
 uint32_t orc_gather_params_size(void) { return (uint32_t)(sizeof(GatherParams) / sizeof(double)); }
 
+// The reflection atlases of one cascade for the combined receiver: rough in the
+// irradiance layout; glossy (null below tier high) with its tile geometry.
+struct OrcReflectAtlas {
+    const uint16_t* rough; const uint16_t* glossy;
+    uint32_t glossyOct, glossyTile, glossyTilesX, glossyW, glossyH;
+};
+
+// Combined receiver (orc_gather.hpp combined_point) of n points, FP64.
+// rdir4: reflection direction xyz + roughness w; outIrr 3 doubles and outRefl
+// 4 doubles per point; near (may be null) as orc_gather.
+void orc_gather_combined(const OrcGrid* g0, const OrcGrid* g1, const uint16_t* atlas0, const uint16_t* depth0,
+                         const uint16_t* atlas1, const uint16_t* depth1, const OrcReflectAtlas* r0,
+                         const OrcReflectAtlas* r1, const double* params, const float* pos4, const float* nvis4,
+                         const float* ndir4, const float* rdir4, uint32_t n, double* outIrr, double* outRefl,
+                         double* near, int32_t threads) {
+    Grid G0 = to_grid(g0), G1;
+    if (g1) G1 = to_grid(g1);
+    GatherParams prm;
+    std::memcpy(&prm, params, sizeof prm);
+    GatherCascade C[2];
+    C[0].g = &G0; C[0].atlas = atlas0; C[0].depth = depth0;
+    if (g1) { C[1].g = &G1; C[1].atlas = atlas1; C[1].depth = depth1; }
+    const OrcReflectAtlas* rs[2] = {r0, r1};
+    for (int c = 0; c < 2; ++c) {
+        if (!rs[c]) continue;
+        C[c].rough = rs[c]->rough; C[c].glossy = rs[c]->glossy;
+        C[c].glossyOct = rs[c]->glossyOct; C[c].glossyTile = rs[c]->glossyTile;
+        C[c].glossyTilesX = rs[c]->glossyTilesX; C[c].glossyW = rs[c]->glossyW; C[c].glossyH = rs[c]->glossyH;
+    }
+    parallel_for(n, threads, [&](size_t i, int) {
+        V3<double> p(pos4[i * 4], pos4[i * 4 + 1], pos4[i * 4 + 2]);
+        V3<double> a(nvis4[i * 4], nvis4[i * 4 + 1], nvis4[i * 4 + 2]);
+        V3<double> b(ndir4[i * 4], ndir4[i * 4 + 1], ndir4[i * 4 + 2]);
+        V3<double> r(rdir4[i * 4], rdir4[i * 4 + 1], rdir4[i * 4 + 2]);
+        double nr = INFINITY;
+        V3<double> e;
+        combined_point<double>(C, prm, p, a, b, r, (double)rdir4[i * 4 + 3], nr, e, outRefl + i * 4);
+        outIrr[i * 3] = e.x; outIrr[i * 3 + 1] = e.y; outIrr[i * 3 + 2] = e.z;
+        if (near) near[i] = nr;
+    });
+}
+
 // ------------------------------------------------------------ light grid
 void orc_light_grid(const OrcGrid* g0, const float* lights, uint32_t lightCount, float* out, int32_t fp32) {
     Grid g = to_grid(g0);

@@ -128,7 +128,8 @@ class sb_gather_params(C.Structure):
     _fields_ = [("normalBias", C.c_float * 2), ("chebyBias", C.c_float * 2), ("chebyStrength", C.c_float),
                 ("detailStrength", C.c_float), ("intensity", C.c_float), ("enabled", C.c_float),
                 ("samplePositionScale", C.c_float), ("sampleBiasScale", C.c_float), ("borderBand", C.c_float),
-                ("cascades", C.c_uint32), ("dualDetail", C.c_uint32)]
+                ("cascades", C.c_uint32), ("dualDetail", C.c_uint32), ("reflectionIntensity", C.c_float),
+                ("roughnessLimit", C.c_float)]
 
 
 class sb_stats(C.Structure):
@@ -164,6 +165,7 @@ SIGNATURES = {
     "sb_probe_rays": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
     "sb_gather_params_defaults": (None, [_P]),
     "sb_gather_irradiance": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
+    "sb_gather_reflections": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_uint32, _P, _P]),
     "sb_synchronize": (C.c_int, [_P]),
     "sb_upload_scene": (C.c_int, [_P, C.POINTER(sb_scene_view)]),
     "sb_upload_range": (C.c_int, [_P, _U32, _U32, _U32, _P]),

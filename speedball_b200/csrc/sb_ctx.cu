@@ -1799,10 +1799,13 @@ void sb_gather_params_defaults(sb_gather_params* p) {
     p->sampleBiasScale = 1.0f;
     p->borderBand = 0.15f;
     p->cascades = 1;
+    p->reflectionIntensity = 1.0f;
+    p->roughnessLimit = 1.0f;
 }
 
-sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const float* position,
-                               const float* stableNormal, const float* detailNormal, uint32_t count, float* out) {
+// Validates a gather's arguments and fills its launch arguments.
+static sb_status gather_args(sb_ctx* ctx, const sb_gather_params* prm, const float* position, const float* stableNormal,
+                             const float* detailNormal, uint32_t count, float* out, GatherArgs& A) {
     if (!ctx || !prm || (count && (!position || !stableNormal || !detailNormal || !out)))
         return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
     auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
@@ -1813,9 +1816,7 @@ sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const f
     for (uint32_t c = 0; c < prm->cascades; ++c)
         if (!ctx->casc[c].configured || !ctx->casc[c].atlas)
             return fail(ctx, SB_ERR_NOT_READY, "cascade %u not configured", c);
-    if (count == 0) return SB_OK;
-    cudaSetDevice(ctx->device);
-    GatherArgs A{};
+    A = GatherArgs{};
     for (uint32_t c = 0; c < prm->cascades; ++c) {
         const Cascade& K = ctx->casc[c];
         for (int a = 0; a < 3; ++a) {
@@ -1827,6 +1828,13 @@ sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const f
         A.c[c].atlasH = K.atlasH;
         A.c[c].atlas = K.atlas;
         A.c[c].depth = K.depthAtlas;
+        A.c[c].rough = K.roughAtlas;
+        A.c[c].glossy = K.reflTier >= SB_REFLECT_HIGH ? K.glossyAtlas : nullptr;
+        A.c[c].glossyOct = K.glossyOct;
+        A.c[c].glossyTile = K.glossyTile;
+        A.c[c].glossyTilesX = K.glossyTilesX;
+        A.c[c].glossyW = K.glossyTilesX * K.glossyTile;
+        A.c[c].glossyH = K.glossyTilesY * K.glossyTile;
     }
     A.cascades = prm->cascades;
     A.dualDetail = prm->dualDetail ? 1u : 0u;
@@ -1841,11 +1849,44 @@ sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const f
     A.samplePositionScale = prm->samplePositionScale;
     A.sampleBiasScale = prm->sampleBiasScale;
     A.borderBand = prm->borderBand;
+    A.reflectionIntensity = prm->reflectionIntensity;
+    A.roughnessLimit = prm->roughnessLimit;
     A.position = reinterpret_cast<const float4*>(position);
     A.stableNormal = reinterpret_cast<const float4*>(stableNormal);
     A.detailNormal = reinterpret_cast<const float4*>(detailNormal);
     A.out = reinterpret_cast<float4*>(out);
+    return SB_OK;
+}
+
+sb_status sb_gather_irradiance(sb_ctx* ctx, const sb_gather_params* prm, const float* position,
+                               const float* stableNormal, const float* detailNormal, uint32_t count, float* out) {
+    GatherArgs A;
+    sb_status s = gather_args(ctx, prm, position, stableNormal, detailNormal, count, out, A);
+    if (s != SB_OK || count == 0) return s;
+    cudaSetDevice(ctx->device);
     CK(launch_gather(A, ctx->stream));
+    return SB_OK;
+}
+
+sb_status sb_gather_reflections(sb_ctx* ctx, const sb_gather_params* prm, const float* position,
+                                const float* stableNormal, const float* detailNormal, const float* reflection,
+                                uint32_t count, float* outIrradiance, float* outReflection) {
+    GatherArgs A;
+    sb_status s = gather_args(ctx, prm, position, stableNormal, detailNormal, count, outIrradiance, A);
+    if (s != SB_OK) return s;
+    if (count && (!reflection || !outReflection)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if ((reinterpret_cast<uintptr_t>(reflection) & 15u) || (reinterpret_cast<uintptr_t>(outReflection) & 15u))
+        return fail(ctx, SB_ERR_INVALID_ARG, "gather arrays must be 16-byte aligned float4 arrays");
+    for (uint32_t c = 0; c < prm->cascades; ++c)
+        if (!ctx->casc[c].roughAtlas)
+            return fail(ctx, SB_ERR_NOT_READY, "cascade %u has no reflection lobes (sb_set_reflection_quality)", c);
+    if (prm->cascades == 2 && (ctx->casc[0].reflTier >= SB_REFLECT_HIGH) != (ctx->casc[1].reflTier >= SB_REFLECT_HIGH))
+        return fail(ctx, SB_ERR_NOT_READY, "the cascades' reflection tiers differ");
+    if (count == 0) return SB_OK;
+    cudaSetDevice(ctx->device);
+    A.reflection = reinterpret_cast<const float4*>(reflection);
+    A.outReflection = reinterpret_cast<float4*>(outReflection);
+    CK(launch_gather_combined(A, ctx->stream));
     return SB_OK;
 }
 

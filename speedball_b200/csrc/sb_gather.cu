@@ -141,7 +141,199 @@ __global__ void __launch_bounds__(256, FULL ? 3 : 4) k_gather(const GatherArgs A
     __stcs(A.out + i, make_float4(fmaxf(E.x, 0.0f) * k, fmaxf(E.y, 0.0f) * k, fmaxf(E.z, 0.0f) * k, 1.0f));
 }
 
+__device__ __forceinline__ float4 bilinear4(const uint2* atlas, uint32_t W, uint32_t H, float u, float v) {
+    const float x = u * float(W) - 0.5f, y = v * float(H) - 0.5f;
+    const float fx0 = floorf(x), fy0 = floorf(y);
+    const float fx = x - fx0, fy = y - fy0;
+    const int x0 = (int)fx0, y0 = (int)fy0;
+    const int Wi = (int)W, Hi = (int)H;
+    const int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
+    const int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
+    const float4 t00 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xa));
+    const float4 t10 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xb));
+    const float4 t01 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xa));
+    const float4 t11 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xb));
+    const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
+    return make_float4(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
+                       t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
+                       t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11,
+                       t00.w * w00 + t10.w * w10 + t01.w * w01 + t11.w * w11);
+}
+
+__device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
+    const float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+// One cascade of the combined receiver (_sampleCombinedCascadeLooped,
+// gi_probes.js:662-771): the irradiance taps with the cage at the biased point
+// P, and per tap with a live lobe the parallax-corrected rough / glossy fetch.
+__device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, float chebyBias, float3 P, float3 reflP,
+                                 float3 Nvis, float3 Ndir, float3 Rn, bool dual, float rw, float lobeMix,
+                                 float3& irr, float4& refl) {
+    float base[3], frac[3], rm1[3];
+    const float cp[3] = {P.x, P.y, P.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        rm1[a] = fmaxf(C.res[a] - 1.0f, 1.0f);
+        const float cell = C.gridSize[a] / rm1[a];
+        const float gf = (cp[a] - C.gridMin[a]) / fmaxf(cell, 1e-6f);
+        base[a] = clampf(floorf(gf), 0.0f, fmaxf(C.res[a] - 2.0f, 0.0f));
+        frac[a] = clampf(gf - base[a], 0.0f, 1.0f);
+    }
+    const float3 Nn = normalize3(Nvis);
+    const float2 oN = oct_encode(normalize3(Ndir));
+    const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
+    const float2 oR = oct_encode(Rn);
+    const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
+    const float cs = A.chebyStrength;
+    const bool glossyOn = C.glossy != nullptr;
+    const bool wantsRough = lobeMix > 0.0f, wantsGlossy = glossyOn && lobeMix < 1.0f;
+    const bool wantsTap = rw > 0.0f && (wantsRough || wantsGlossy);
+    float3 acc = mk(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f, roughW = 0.0f, glossyW = 0.0f;
+    float4 roughAcc = make_float4(0.f, 0.f, 0.f, 0.f), glossyAcc = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = 0; i < 8; ++i) {
+        const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
+        const float px = base[0] + float(dx), py = base[1] + float(dy), pz = base[2] + float(dz);
+        const float wx = dx ? frac[0] : 1.0f - frac[0];
+        const float wy = dy ? frac[1] : 1.0f - frac[1];
+        const float wz = dz ? frac[2] : 1.0f - frac[2];
+        const float wTri = wx * wy * wz + 1e-4f;
+        const float row = pz * C.res[1] + py;
+        const float ox0 = px * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
+        const float3 probePos = mk(C.gridMin[0] + px / rm1[0] * C.gridSize[0],
+                                   C.gridMin[1] + py / rm1[1] * C.gridSize[1],
+                                   C.gridMin[2] + pz / rm1[2] * C.gridSize[2]);
+        float w = wTri;
+        if (cs != 0.0f) {
+            const float3 toSurf = P - probePos;
+            const float dist = sqrtf(dot3(toSurf, toSurf));
+            const float inv = 1.0f / fmaxf(dist, 1e-6f);
+            const float2 oD = oct_encode(toSurf * inv);
+            const float3 m = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oD.x * 6.0f) * invW,
+                                       (oy0 + oD.y * 6.0f) * invH);
+            const float variance = fabsf(m.y - m.x * m.x);
+            const float dm = fmaxf(dist - m.x - chebyBias, 0.0f);
+            const float chebyRaw = variance / fmaxf(variance + dm * dm, 1e-6f);
+            const float cheby = dist <= m.x + chebyBias ? 1.0f : chebyRaw;
+            const float visW = (1.0f - cs) + fmaxf(cheby * cheby * cheby, 0.05f) * cs;
+            const float wrap = dot3((probePos - P) * inv, Nn) * 0.5f + 0.5f;
+            const float wrapW = (1.0f - cs) + fmaxf(wrap * wrap, 0.05f) * cs;
+            w = wTri * wrapW * visW;
+        }
+        float3 e = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oN.x * 6.0f) * invW, (oy0 + oN.y * 6.0f) * invH);
+        if (dual) {
+            const float3 eS = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oS.x * 6.0f) * invW,
+                                        (oy0 + oS.y * 6.0f) * invH);
+            e = eS * (1.0f - A.detailStrength) + e * A.detailStrength;
+        }
+        acc = acc + e * w;
+        wsum += w;
+        if (!wantsTap) continue;
+        // the reflection ray against the sphere of the probe's mean depth toward R
+        const float3 dR = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oR.x * 6.0f) * invW, (oy0 + oR.y * 6.0f) * invH);
+        const float radius = fmaxf(dR.x, 1e-4f), radius2 = radius * radius;
+        const float3 q = reflP - probePos;
+        const float q2 = dot3(q, q), qDotR = dot3(q, Rn);
+        const float disc = radius2 - q2 + qDotR * qDotR;
+        const float sqrtDisc = sqrtf(fmaxf(disc, 0.0f));
+        const float nearT = -qDotR - sqrtDisc, farT = -qDotR + sqrtDisc;
+        const float rayT = nearT > 1e-4f ? nearT : farT;
+        const float relVar = fmaxf(dR.y - radius2, 0.0f) / fmaxf(radius2, 1e-4f);
+        const float stableDepth = 1.0f - smoothstepf(0.02f, 0.20f, relVar);
+        const float validHit = (disc > 1e-6f && rayT > 1e-4f) ? 1.0f : 0.0f;
+        const float insideWeight = smoothstepf(0.0f, 0.12f, (radius2 - q2) / fmaxf(radius2, 1e-4f));
+        const float pw = stableDepth * validHit * insideWeight;
+        const float3 corrected = normalize3(q + Rn * fmaxf(rayT, 0.0f));
+        const float2 oSR = oct_encode(normalize3(Rn * (1.0f - pw) + corrected * pw));
+        const float probeW = w * w;
+        if (wantsGlossy) {
+            const float probeIndex = px + py * C.res[0] + pz * (C.res[0] * C.res[1]);
+            const float tx = float(C.glossyTilesX);
+            const float grow = floorf(probeIndex / tx), gcol = probeIndex - tx * grow;
+            const float ox = gcol * float(C.glossyTile) + 1.0f + oSR.x * float(C.glossyOct);
+            const float oy = grow * float(C.glossyTile) + 1.0f + oSR.y * float(C.glossyOct);
+            const float4 gl = bilinear4(C.glossy, C.glossyW, C.glossyH, ox / float(C.glossyW), oy / float(C.glossyH));
+            const float gw = probeW * (0.2f * (1.0f - pw) + pw);
+            glossyAcc = make_float4(glossyAcc.x + gl.x * gw, glossyAcc.y + gl.y * gw, glossyAcc.z + gl.z * gw,
+                                    glossyAcc.w + gl.w * gw);
+            glossyW += gw;
+        }
+        if (wantsRough) {
+            const float4 br = bilinear4(C.rough, C.atlasW, C.atlasH, (ox0 + oSR.x * 6.0f) * invW,
+                                        (oy0 + oSR.y * 6.0f) * invH);
+            roughAcc = make_float4(roughAcc.x + br.x * probeW, roughAcc.y + br.y * probeW, roughAcc.z + br.z * probeW,
+                                   roughAcc.w + br.w * probeW);
+            roughW += probeW;
+        }
+    }
+    irr = acc * (1.0f / fmaxf(wsum, 1e-4f));
+    const float ri = 1.0f / fmaxf(roughW, 1e-4f);
+    refl = make_float4(roughAcc.x * ri, roughAcc.y * ri, roughAcc.z * ri, roughAcc.w * ri);
+    if (glossyOn) {
+        const float gi = 1.0f / fmaxf(glossyW, 1e-4f);
+        refl = make_float4(glossyAcc.x * gi * (1.0f - lobeMix) + refl.x * lobeMix,
+                           glossyAcc.y * gi * (1.0f - lobeMix) + refl.y * lobeMix,
+                           glossyAcc.z * gi * (1.0f - lobeMix) + refl.z * lobeMix,
+                           glossyAcc.w * gi * (1.0f - lobeMix) + refl.w * lobeMix);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gather_combined(const GatherArgs A) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.count) return;
+    const float4 p4 = __ldcs(A.position + i), n4 = __ldcs(A.stableNormal + i), d4 = __ldcs(A.detailNormal + i);
+    const float4 r4 = __ldcs(A.reflection + i);
+    const float3 Nvis = xyz(n4), Ndir = xyz(d4), Rn = normalize3(xyz(r4));
+    const float roughness = r4.w;
+    const float3 reflP = xyz(p4) * A.samplePositionScale;
+    const float3 P = reflP + Nvis * A.normalBias0 * A.sampleBiasScale;
+    const float part = roughness <= A.roughnessLimit ? 1.0f : 0.0f;
+    const float rw = clampf(A.reflectionIntensity * A.enabled * part, 0.0f, 1.0f);
+    const float lobeMix = A.c[0].glossy ? smoothstepf(0.22f, 0.58f, roughness) : 1.0f;
+    float3 E;
+    float4 S;
+    if (A.cascades < 2) {
+        combined_cascade(A.c[0], A, A.chebyBias[0], P, reflP, Nvis, Ndir, Rn, A.dualDetail != 0, rw, lobeMix, E, S);
+    } else {
+        // cascade ownership at the surface position (gi_probes.js:787-792)
+        const GatherCascade& F = A.c[1];
+        const float f0 = (reflP.x - F.gridMin[0]) / fmaxf(F.gridSize[0], 1e-6f);
+        const float f1 = (reflP.y - F.gridMin[1]) / fmaxf(F.gridSize[1], 1e-6f);
+        const float f2 = (reflP.z - F.gridMin[2]) / fmaxf(F.gridSize[2], 1e-6f);
+        const float fLo = fminf(fminf(f0, f1), f2);
+        const float fHi = fminf(fminf(1.0f - f0, 1.0f - f1), 1.0f - f2);
+        const float wIn = clampf(fminf(fLo, fHi) / fmaxf(A.borderBand, 1e-4f), 0.0f, 1.0f);
+        const float wFine = wIn * clampf(float(A.cascades) - 1.0f, 0.0f, 1.0f);
+        E = mk(0.0f, 0.0f, 0.0f);
+        S = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (wFine < 1.0f) combined_cascade(A.c[0], A, A.chebyBias[0], P, reflP, Nvis, Ndir, Rn, false, rw, lobeMix, E, S);
+        if (wFine > 0.0f) {
+            float3 Ef;
+            float4 Sf;
+            combined_cascade(A.c[1], A, A.chebyBias[1], P, reflP, Nvis, Ndir, Rn, false, rw, lobeMix, Ef, Sf);
+            E = E * (1.0f - wFine) + Ef * wFine;
+            S = make_float4(S.x * (1.0f - wFine) + Sf.x * wFine, S.y * (1.0f - wFine) + Sf.y * wFine,
+                            S.z * (1.0f - wFine) + Sf.z * wFine, S.w * (1.0f - wFine) + Sf.w * wFine);
+        }
+    }
+    const float k = A.intensity * A.enabled;
+    __stcs(A.out + i, make_float4(fmaxf(E.x, 0.0f) * k, fmaxf(E.y, 0.0f) * k, fmaxf(E.z, 0.0f) * k, 1.0f));
+    const float4 o = rw > 0.0f ? make_float4(fmaxf(S.x, 0.0f) * rw, fmaxf(S.y, 0.0f) * rw, fmaxf(S.z, 0.0f) * rw,
+                                             clampf(fmaxf(S.w, 0.0f), 0.0f, 1.0f) * rw)
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
+    __stcs(A.outReflection + i, o);
+}
+
 }  // namespace
+
+cudaError_t launch_gather_combined(const GatherArgs& A, cudaStream_t st) {
+    if (A.count == 0) return cudaSuccess;
+    k_gather_combined<<<(A.count + 255) / 256, 256, 0, st>>>(A);
+    note_launch();
+    return cudaGetLastError();
+}
 
 cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st) {
     if (A.count == 0) return cudaSuccess;

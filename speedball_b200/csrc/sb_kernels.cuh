@@ -147,18 +147,27 @@ struct GatherCascade {
     uint32_t atlasW, atlasH;
     const uint2* atlas;   // RGBA16F irradiance atlas
     const uint2* depth;   // RGBA16F depth-moment atlas
+    // reflection lobes (combined receiver): rough atlas in the irradiance
+    // layout; glossy atlas (null below tier high) of glossyTile-texel tiles
+    const uint2* rough;
+    const uint2* glossy;
+    uint32_t glossyOct, glossyTile, glossyTilesX, glossyW, glossyH;
 };
 struct GatherArgs {
     GatherCascade c[2];
     uint32_t cascades, dualDetail, count;
     float normalBias0, chebyBias[2], chebyStrength, detailStrength, intensity, enabled;
     float samplePositionScale, sampleBiasScale, borderBand;
+    float reflectionIntensity, roughnessLimit;
     const float4* position;
     const float4* stableNormal;
     const float4* detailNormal;
+    const float4* reflection;  // combined receiver: direction xyz, roughness w
     float4* out;
+    float4* outReflection;
 };
 cudaError_t launch_gather(const GatherArgs& A, cudaStream_t st);
+cudaError_t launch_gather_combined(const GatherArgs& A, cudaStream_t st);
 // GPU BLAS build in the threaded layout (sb_build.cu); device scratch lives in
 // the builder and grows to the largest mesh built. Out-of-range vertex indices
 // latch ERR_LAYOUT.

@@ -96,3 +96,102 @@ def test_reflection_tiers_refuse_batch_and_adjoint():
         f.synchronize()
     finally:
         f.dispose()
+
+
+def _reflect_atlases(f, ci):
+    g = f.cascadeGrid(ci)
+    r = [g.res[a] for a in range(3)]
+    W, H = r[0] * 8, r[1] * r[2] * 8
+    a = gu.read(f, "IRRADIANCE_ATLAS", W * H * 4, np.uint16, ci)
+    d = gu.read(f, "DEPTH_ATLAS", W * H * 4, np.uint16, ci)
+    rough = gu.read(f, "ROUGH_ATLAS", W * H * 4, np.uint16, ci)
+    lay = f.reflectionLayout(ci)
+    glossy = None
+    if lay["glossyTile"]:
+        glossy = gu.read(f, "GLOSSY_ATLAS", lay["glossyAtlasW"] * lay["glossyAtlasH"] * 4, np.uint16, ci)
+        glossy = glossy.reshape(lay["glossyAtlasH"], lay["glossyAtlasW"], 4)
+    ra = orc.reflect_atlas(rough, glossy, lay["glossyOct"], lay["glossyTilesX"])
+    return orc.grid_struct(gu.grid_dict(g)), a, d, ra
+
+
+@pytest.mark.parametrize("case", ["one_cascade", "two_cascades_chebyshev"])
+def test_combined_receiver_matches_oracle(case):
+    """sb_gather_reflections on the atlases of 4 solves (room with metals, tier
+    high, a fine box as cascade 1): irradiance and the reflection layer of
+    200,000 receivers (roughness uniform in [0, 1], limit 0.9, intensity 0.8)
+    within 1e-3 of the FP64 combined receiver; samples within 1e-4 of a
+    discontinuity (cage floor, Chebyshev select, parallax root selects, the
+    roughness limit) are counted, must be rare, and are not compared."""
+    torch = pytest.importorskip("torch")
+    s = synth.room_spheres(0)
+    s.materials = s.materials.copy()
+    s.materials[::2, 4] = 1.0
+    f = gu.make_field(s, reflectionQuality="high")
+    try:
+        g = s.meta["grid"]
+        gmin = np.asarray(g["gridMin"], np.float64)
+        gsz = np.asarray(g["gridSize"], np.float64)
+        f.configureCascade(1, (gmin + gsz * 0.25).tolist(), (gsz * 0.5).tolist(), (8, 8, 8))
+        for _ in range(4):
+            fr = f.beginTick()
+            _abi.check(f._lib.sb_solve(f.ctx, 0, fr["probeOffset"], fr["updatedCount"]), f.ctx)
+            _abi.check(f._lib.sb_solve(f.ctx, 1, 0, f.cascadeProbes(1)), f.ctx)
+            f.endTick(fr)
+        f.synchronize()
+        n = 200_000
+        rng = np.random.default_rng(9)
+        lo = gmin - 0.1
+        pos = np.zeros((n, 4), np.float32)
+        pos[:, :3] = rng.uniform(lo, lo + gsz + 0.2, (n, 3))
+        nv = rng.normal(size=(n, 3))
+        nv /= np.linalg.norm(nv, axis=1, keepdims=True)
+        a4 = np.zeros((n, 4), np.float32); a4[:, :3] = nv
+        rd = rng.normal(size=(n, 3))
+        rd /= np.linalg.norm(rd, axis=1, keepdims=True)
+        r4 = np.zeros((n, 4), np.float32); r4[:, :3] = rd; r4[:, 3] = rng.uniform(0, 1, n)
+        two = case != "one_cascade"
+        kw = dict(reflectionIntensity=0.8, roughnessLimit=0.9)
+        if two:
+            kw.update(cascades=2.0, chebyStrength=1.0, chebyBias0=0.02, chebyBias1=0.01, borderBand=0.2)
+        prm = _abi.sb_gather_params()
+        f._lib.sb_gather_params_defaults(_abi.C.byref(prm))
+        prm.reflectionIntensity, prm.roughnessLimit = 0.8, 0.9
+        if two:
+            prm.cascades, prm.chebyStrength, prm.borderBand = 2, 1.0, 0.2
+            prm.chebyBias[0], prm.chebyBias[1] = 0.02, 0.01
+        dev = torch.device("cuda", 0)
+        tp, tn, tr = (torch.from_numpy(x).to(dev) for x in (pos, a4, r4))
+        oi = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        orf = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        torch.cuda.synchronize()
+        _abi.check(f._lib.sb_gather_reflections(f.ctx, _abi.C.byref(prm), tp.data_ptr(), tn.data_ptr(), tn.data_ptr(),
+                                                tr.data_ptr(), n, oi.data_ptr(), orf.data_ptr()), f.ctx)
+        f.synchronize()
+        gi, gr = oi.cpu().numpy(), orf.cpu().numpy()
+        G0, a0, d0, r0 = _reflect_atlases(f, 0)
+        G1, a1, d1, r1 = _reflect_atlases(f, 1)
+        wi, wr, near = orc.gather_combined(G0, a0, d0, r0, orc.gather_params(**kw), pos, a4, a4, r4,
+                                           G1 if two else None, a1 if two else None, d1 if two else None,
+                                           r1 if two else None)
+        edge = near < 1e-4
+        assert edge.mean() < 5e-3, edge.mean()
+        ei = gu.texel_rel_err(gi[~edge, :3].astype(np.float64), wi[~edge])
+        er = gu.texel_rel_err(gr[~edge, :3].astype(np.float64), wr[~edge, :3])
+        ec = gu.texel_rel_err(gr[~edge, 3].astype(np.float64), wr[~edge, 3])
+        print(case, "irr", ei.max(), "refl", er.max(), "coverage", ec.max(), "edge", int(edge.sum()),
+              "covered share", float((wr[:, 3] > 0).mean()))
+        assert max(ei.max(), er.max(), ec.max()) <= gu.TEXEL_REL
+        assert (wr[:, 3] > 0).mean() > 0.5 and wr[:, :3].max() > 0.01
+        assert lib_refuses_without_lobes(f)
+    finally:
+        f.dispose()
+
+
+def lib_refuses_without_lobes(f) -> bool:
+    prm = _abi.sb_gather_params()
+    f._lib.sb_gather_params_defaults(_abi.C.byref(prm))
+    _abi.check(f._lib.sb_set_reflection_quality(f.ctx, 0), f.ctx)
+    torch = pytest.importorskip("torch")
+    buf = torch.zeros((64, 4), dtype=torch.float32, device=torch.device("cuda", 0))
+    p = buf.data_ptr()
+    return f._lib.sb_gather_reflections(f.ctx, _abi.C.byref(prm), p, p, p, p, 8, p, p) == _abi.SB_ERR_NOT_READY

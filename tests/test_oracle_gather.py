@@ -83,3 +83,66 @@ def test_visible_surfaces_leave_only_the_wrap_weight():
     assert np.all(np.isfinite(vis)) and np.abs(vis - plain).max() > 1e-3
     # wrap weights are >= 0.05^2 of the trilinear weights: the result stays in the atlas' value range
     assert vis.min() >= 0.0 and vis.max() <= 2.0 + 1e-9
+
+
+# ------------------------------------------------------- combined receiver
+def _const_atlas(shape_hw, rgba):
+    a = np.zeros(shape_hw + (4,), np.float16)
+    a[...] = np.asarray(rgba, np.float16)
+    return a.view(np.uint16).copy()
+
+
+def _rdirs(n, seed, rough=(0.0, 1.0)):
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    out = np.zeros((n, 4), np.float32)
+    out[:, :3] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    out[:, 3] = rng.uniform(rough[0], rough[1], n)
+    return out
+
+
+def test_combined_receiver_irradiance_is_the_plain_gather_and_zero_intensity_has_no_layer():
+    g = _grid()
+    G = orc.grid_struct(g)
+    a = _random_atlas(g, 11)
+    d = _random_atlas(g, 12)
+    r = g["res"]
+    rough = _const_atlas((r[1] * r[2] * 8, r[0] * 8), (0.5, 0.6, 0.7, 0.8))
+    pos, nv = _points(300, 13)
+    rd = _rdirs(300, 14)
+    for prm in (orc.gather_params(), orc.gather_params(chebyStrength=1.0, chebyBias0=0.02)):
+        plain, _ = orc.gather(G, a, d, prm, pos, nv, nv)
+        irr, refl, _ = orc.gather_combined(G, a, d, orc.reflect_atlas(rough), prm, pos, nv, nv, rd)
+        assert np.allclose(irr, plain, rtol=1e-12, atol=1e-15)
+        assert (refl[:, 3] > 0).all()
+    p0 = orc.gather_params(reflectionIntensity=0.0)
+    _, refl, _ = orc.gather_combined(G, a, d, orc.reflect_atlas(rough), p0, pos, nv, nv, rd)
+    assert np.abs(refl).max() == 0.0
+
+
+def test_combined_receiver_constant_lobes_resolve_to_their_values():
+    """Normalised tap weights: a constant rough atlas gives its value times the
+    reflection weight; with a glossy atlas the two blend by smoothstep(0.22,
+    0.58, roughness); receivers rougher than the limit get no layer."""
+    g = _grid()
+    G = orc.grid_struct(g)
+    a = _random_atlas(g, 21)
+    d = _random_atlas(g, 22)
+    r = g["res"]
+    P = r[0] * r[1] * r[2]
+    rough_v, glossy_v = np.array([0.5, 0.25, 0.75, 0.5]), np.array([1.5, 1.0, 0.5, 1.0])
+    rough = _const_atlas((r[1] * r[2] * 8, r[0] * 8), rough_v)
+    tx = int(np.ceil(np.sqrt(P)))
+    ty = -(-P // tx)
+    glossy = _const_atlas((ty * 10, tx * 10), glossy_v)
+    pos, nv = _points(400, 23)
+    rd = _rdirs(400, 24)
+    prm = orc.gather_params(reflectionIntensity=0.75, roughnessLimit=0.9)
+    _, refl, near = orc.gather_combined(G, a, d, orc.reflect_atlas(rough), prm, pos, nv, nv, rd)
+    rw = np.where(rd[:, 3] <= np.float32(0.9), 0.75, 0.0)[:, None]
+    assert np.allclose(refl, rough_v[None, :] * rw, rtol=1e-12, atol=1e-15)
+    _, refl, _ = orc.gather_combined(G, a, d, orc.reflect_atlas(rough, glossy, 8, tx), prm, pos, nv, nv, rd)
+    t = np.clip((rd[:, 3].astype(np.float64) - 0.22) / (0.58 - 0.22), 0, 1)
+    m = (t * t * (3 - 2 * t))[:, None]
+    want = (glossy_v[None, :] * (1 - m) + rough_v[None, :] * m) * rw
+    assert np.allclose(refl, want, rtol=1e-12, atol=1e-15)
