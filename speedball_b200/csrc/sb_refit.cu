@@ -531,6 +531,11 @@ __device__ __forceinline__ void red_max(double& v, uint32_t& p, double v2, uint3
 
 struct Seg { uint16_t lo, hi, idx; };
 
+// Up to this many instances a level orders its segments by rank (the summed
+// squared segment lengths stay below n^2 / 2 per level); above it by one
+// bitonic sort of all positions per level.
+constexpr uint32_t TLAS_RANK_SORT_MAX = 512;
+
 __host__ __device__ inline size_t tlas_build_smem(uint32_t n) {
     uint32_t P = 1;
     while (P < n) P <<= 1;
@@ -614,42 +619,74 @@ __global__ void __launch_bounds__(1024) k_tlas_build(SceneBuffers B, InstanceTab
             }
         }
         __syncthreads();
-        // (b) sort records grouped by the first position of their segment (or by their
-        // own position when finished), so every group stays inside its range; leaf
-        // segments and finished positions keep their order (constant key)
-        for (uint32_t j = threadIdx.x; j < P; j += blockDim.x) {
-            BuildRec r;
-            if (j < n) {
-                uint32_t s = segOf[j];
-                uint32_t ax = s == NONE ? 255u : axisOf[s];
-                uint32_t group = s == NONE ? j : (uint32_t)cur[s].lo;
-                r.segpos = (group << 13) | j;
-                r.key = ax == 255 ? 0ull : sortable(I.aabb[(size_t)order[j] * 9u + 6u + ax]);
-            } else {
-                r.segpos = 0xFFFFFFFFu;
-                r.key = ~0ull;
+        if (n <= TLAS_RANK_SORT_MAX) {
+            // (b) the stable order of every interior segment by its split axis's FP64
+            // centroid key: each position's rank among its segment's positions by
+            // (key, position), one thread per position; leaf segments and finished
+            // positions keep their place. The keys are staged once per level.
+            unsigned long long* keys = reinterpret_cast<unsigned long long*>(rec);  // n keys, then n slots
+            uint32_t* newOrder = reinterpret_cast<uint32_t*>(keys + n);
+            for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+                const uint32_t s = segOf[j];
+                const uint32_t ax = s == NONE ? 255u : axisOf[s];
+                keys[j] = ax == 255u ? 0ull : sortable(I.aabb[(size_t)order[j] * 9u + 6u + ax]);
             }
-            r.pad = 0;
-            rec[j] = r;
-        }
-        __syncthreads();
-        // (c) bitonic sort of P records
-        for (uint32_t k = 2; k <= P; k <<= 1)
-            for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
-                for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
-                    uint32_t ixj = i ^ jj;
-                    if (ixj > i) {
-                        bool up = (i & k) == 0;
-                        BuildRec a = rec[i], b = rec[ixj];
-                        bool sw = up ? rec_less(b, a) : rec_less(a, b);
-                        if (sw) { rec[i] = b; rec[ixj] = a; }
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+                const uint32_t s = segOf[j];
+                uint32_t dest = j;
+                if (s != NONE && axisOf[s] != 255u) {
+                    const uint32_t lo = cur[s].lo, hi = cur[s].hi;
+                    const unsigned long long kj = keys[j];
+                    uint32_t r = 0;
+                    for (uint32_t q = lo; q < hi; ++q) {
+                        const unsigned long long kq = keys[q];
+                        r += (kq < kj || (kq == kj && q < j)) ? 1u : 0u;
                     }
+                    dest = lo + r;
                 }
-                __syncthreads();
+                newOrder[dest] = order[j];
             }
-        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) segOf[j] = order[rec[j].segpos & 0x1FFFu];
-        __syncthreads();
-        for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) order[j] = segOf[j];
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) order[j] = newOrder[j];
+        } else {
+            // (b) sort records grouped by the first position of their segment (or by their
+            // own position when finished), so every group stays inside its range; leaf
+            // segments and finished positions keep their order (constant key)
+            for (uint32_t j = threadIdx.x; j < P; j += blockDim.x) {
+                BuildRec r;
+                if (j < n) {
+                    uint32_t s = segOf[j];
+                    uint32_t ax = s == NONE ? 255u : axisOf[s];
+                    uint32_t group = s == NONE ? j : (uint32_t)cur[s].lo;
+                    r.segpos = (group << 13) | j;
+                    r.key = ax == 255 ? 0ull : sortable(I.aabb[(size_t)order[j] * 9u + 6u + ax]);
+                } else {
+                    r.segpos = 0xFFFFFFFFu;
+                    r.key = ~0ull;
+                }
+                r.pad = 0;
+                rec[j] = r;
+            }
+            __syncthreads();
+            // (c) bitonic sort of P records
+            for (uint32_t k = 2; k <= P; k <<= 1)
+                for (uint32_t jj = k >> 1; jj > 0; jj >>= 1) {
+                    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                        uint32_t ixj = i ^ jj;
+                        if (ixj > i) {
+                            bool up = (i & k) == 0;
+                            BuildRec a = rec[i], b = rec[ixj];
+                            bool sw = up ? rec_less(b, a) : rec_less(a, b);
+                            if (sw) { rec[i] = b; rec[ixj] = a; }
+                        }
+                    }
+                    __syncthreads();
+                }
+            for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) segOf[j] = order[rec[j].segpos & 0x1FFFu];
+            __syncthreads();
+            for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) order[j] = segOf[j];
+        }
         // (d) children of interior segments, in order of lo
         if (threadIdx.x == 0) {
             uint32_t m = 0;
