@@ -11,11 +11,31 @@
 #include "sb_flat.h"
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <functional>
 #include <cmath>
 #include <cstring>
 #include <thread>
 #include <vector>
+
+// The 8-wide tree is collapsed from a binary SAH tree. SB_WIDE_COLLAPSE_SAH 1
+// (default): the binary tree has one item per leaf and the SAH-optimal
+// dynamic program forms the wide nodes and leaves of up to WIDE_LEAF_MAX items,
+// an item test costing SB_WIDE_ITEM_COST wide-node visits; 0: the binary tree
+// has leaves of up to WIDE_LEAF_MAX items and each wide node opens the largest
+// interior child until eight. On the atrium (CPU walk of 200,000 rays over the
+// triangles' boxes) the program gives 6.46 against 6.73 node visits and 1.80
+// against 1.91 item tests per ray, 7.2 against 4.3 children per node.
+#ifndef SB_WIDE_COLLAPSE_SAH
+#define SB_WIDE_COLLAPSE_SAH 1
+#endif
+#ifndef SB_WIDE_BINARY_LEAF
+#define SB_WIDE_BINARY_LEAF (SB_WIDE_COLLAPSE_SAH ? 1u : WIDE_LEAF_MAX)
+#endif
+#ifndef SB_WIDE_ITEM_COST
+#define SB_WIDE_ITEM_COST 0.5f
+#endif
 
 namespace sb {
 namespace flat {
@@ -416,7 +436,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     if (n == 0) return true;
     if (n >= (1u << 24)) return false;
     Builder B;
-    B.maxLeaf = WIDE_LEAF_MAX;
+    B.maxLeaf = SB_WIDE_BINARY_LEAF;
     B.init(boxes, n);
     B.build(n);
     for (size_t v = 0; v < B.N.count.size(); ++v) {
@@ -425,6 +445,75 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                          [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
     }
 
+#if SB_WIDE_COLLAPSE_SAH
+    // SAH-optimal collapse (Ylitie, Karras and Laine 2017, "Efficient incoherent
+    // ray traversal on GPUs through compressed wide BVHs"): per binary node v and
+    // slot budget i = 1..8 the least cost of covering v's subtree with at most i
+    // slots of the parent; a slot is a leaf of at most WIDE_LEAF_MAX items (a
+    // binary leaf, or an interior node whose subtree is that small) or an
+    // interior wide node. Costs: area x 1 per wide node, area x 0.3 per item.
+    const size_t nv = B.N.size();
+    std::vector<uint32_t> sFirst(nv), sCount(nv), post;
+    post.reserve(nv);
+    {
+        std::vector<std::pair<uint32_t, bool>> st{{0u, false}};
+        while (!st.empty()) {
+            auto [v, done] = st.back();
+            st.pop_back();
+            if (B.N.count[v] || done) { post.push_back(v); continue; }
+            st.push_back({v, true});
+            st.push_back({B.N.right[v], false});
+            st.push_back({B.N.left[v], false});
+        }
+    }
+    constexpr float C_NODE = 1.0f, C_ITEM = SB_WIDE_ITEM_COST;
+    std::vector<std::array<float, 9>> cost(nv);
+    std::vector<std::array<uint8_t, 9>> how(nv), splitK(nv);  // how: 0 reuse i-1, 1 leaf, 2 interior, 3 split
+    for (uint32_t v : post) {
+        const float A = B.N.box[v].area();
+        if (B.N.count[v]) {
+            sFirst[v] = B.N.first[v];
+            sCount[v] = B.N.count[v];
+            for (int i = 1; i <= 8; ++i) { cost[v][i] = A * C_ITEM * (float)sCount[v]; how[v][i] = 1; }
+            continue;
+        }
+        const uint32_t L = B.N.left[v], R = B.N.right[v];
+        sFirst[v] = std::min(sFirst[L], sFirst[R]);
+        sCount[v] = sCount[L] + sCount[R];
+        float D[9];
+        for (int j = 2; j <= 8; ++j) {
+            D[j] = INFINITY;
+            for (int k = 1; k < j; ++k) {
+                const float c = cost[L][k] + cost[R][j - k];
+                if (c < D[j]) { D[j] = c; splitK[v][j] = (uint8_t)k; }
+            }
+        }
+        const float leafC = sCount[v] <= WIDE_LEAF_MAX ? A * C_ITEM * (float)sCount[v] : INFINITY;
+        const float intC = A * C_NODE + D[8];
+        cost[v][1] = std::min(leafC, intC);
+        how[v][1] = leafC <= intC ? 1 : 2;
+        for (int i = 2; i <= 8; ++i) {
+            if (D[i] < cost[v][i - 1]) { cost[v][i] = D[i]; how[v][i] = 3; }
+            else { cost[v][i] = cost[v][i - 1]; how[v][i] = 0; }
+        }
+    }
+    // the slots covering v's subtree with budget i
+    std::function<void(uint32_t, int, std::vector<uint32_t>&)> gather = [&](uint32_t v, int i,
+                                                                             std::vector<uint32_t>& kids) {
+        while (i > 1 && how[v][i] == 0) --i;
+        if (i == 1 || B.N.count[v]) { kids.push_back(v); return; }
+        const int k = splitK[v][i];
+        gather(B.N.left[v], k, kids);
+        gather(B.N.right[v], i - k, kids);
+    };
+    // a slot is a leaf when its node is a binary leaf or the collapse chose one
+    auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0 || how[v][1] == 1; };
+    for (size_t v = 0; v < nv; ++v)  // merged leaves: their items in slot order too
+        if (!B.N.count[v] && how[v][1] == 1)
+            std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + sCount[v],
+                             [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+#endif
+
     struct Task { uint32_t v, w, depth; };
     std::vector<Task> queue{{0, 0, 0}};
     out.nodes.assign(WIDE_WORDS, 0u);
@@ -432,8 +521,16 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     for (size_t qi = 0; qi < queue.size(); ++qi) {
         const Task t = queue[qi];
         maxDepth = std::max(maxDepth, t.depth);
-        // children: open the largest interior child until eight (a leaf root is its own child)
         std::vector<uint32_t> kids;
+#if SB_WIDE_COLLAPSE_SAH
+        if (is_leaf_slot(t.v)) kids.push_back(t.v);  // a small root is one leaf slot
+        else {
+            const int k = splitK[t.v][8];
+            gather(B.N.left[t.v], k, kids);
+            gather(B.N.right[t.v], 8 - k, kids);
+        }
+#else
+        // children: open the largest interior child until eight (a leaf root is its own child)
         if (B.N.count[t.v]) kids.push_back(t.v);
         else { kids.push_back(B.N.left[t.v]); kids.push_back(B.N.right[t.v]); }
         while (kids.size() < 8) {
@@ -449,6 +546,10 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
             kids[best] = B.N.left[v];
             kids.push_back(B.N.right[v]);
         }
+        auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0; };
+        const std::vector<uint32_t>& sFirst = B.N.first;
+        const std::vector<uint32_t>& sCount = B.N.count;
+#endif
         // slots by octant: slot bit a set = the child lies toward +a of the node centre
         Box nb;
         for (uint32_t k : kids) nb.grow(B.N.box[k]);
@@ -500,16 +601,16 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                 q[a][s] = (uint8_t)std::min(255.0, std::max(0.0, lo));
                 q[3 + a][s] = (uint8_t)std::min(255.0, std::max(0.0, hi));
             }
-            if (B.N.count[v] == 0) {
+            if (!is_leaf_slot(v)) {
                 imask |= 1u << s;
                 meta[s] = (uint8_t)((1u << 5) | (24u + s));
                 queue.push_back({v, 0, t.depth + 1});  // node index assigned below, in slot order
             } else {
-                const uint32_t cnt = B.N.count[v];
+                const uint32_t cnt = sCount[v];
                 meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
                 for (uint32_t k = 0; k < cnt; ++k) {
-                    out.items.push_back(itemTri[B.order[B.N.first[v] + k]]);
-                    out.items.push_back(itemSlot[B.order[B.N.first[v] + k]]);
+                    out.items.push_back(itemTri[B.order[sFirst[v] + k]]);
+                    out.items.push_back(itemSlot[B.order[sFirst[v] + k]]);
                 }
                 itemOff += cnt;
             }
