@@ -357,7 +357,7 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
 
     // leaves: items ordered by slot, so consecutive tests reuse the local ray
     for (size_t v = 0; v < B.N.count.size(); ++v) {
-        if (B.N.count[v] == 0) continue;
+        if (B.N.count[v] < 2) continue;
         std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
                          [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
     }
@@ -440,7 +440,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     B.init(boxes, n);
     B.build(n);
     for (size_t v = 0; v < B.N.count.size(); ++v) {
-        if (B.N.count[v] == 0) continue;
+        if (B.N.count[v] < 2) continue;
         std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
                          [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
     }
@@ -452,24 +452,15 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     // slots of the parent; a slot is a leaf of at most WIDE_LEAF_MAX items (a
     // binary leaf, or an interior node whose subtree is that small) or an
     // interior wide node. Costs: area x 1 per wide node, area x 0.3 per item.
+    // The builder numbers every child after its parent, so descending node
+    // order visits children before parents.
     const size_t nv = B.N.size();
-    std::vector<uint32_t> sFirst(nv), sCount(nv), post;
-    post.reserve(nv);
-    {
-        std::vector<std::pair<uint32_t, bool>> st{{0u, false}};
-        while (!st.empty()) {
-            auto [v, done] = st.back();
-            st.pop_back();
-            if (B.N.count[v] || done) { post.push_back(v); continue; }
-            st.push_back({v, true});
-            st.push_back({B.N.right[v], false});
-            st.push_back({B.N.left[v], false});
-        }
-    }
+    std::vector<uint32_t> sFirst(nv), sCount(nv);
     constexpr float C_NODE = 1.0f, C_ITEM = SB_WIDE_ITEM_COST;
     std::vector<std::array<float, 9>> cost(nv);
     std::vector<std::array<uint8_t, 9>> how(nv), splitK(nv);  // how: 0 reuse i-1, 1 leaf, 2 interior, 3 split
-    for (uint32_t v : post) {
+    for (size_t vi = nv; vi-- > 0;) {
+        const uint32_t v = (uint32_t)vi;
         const float A = B.N.box[v].area();
         if (B.N.count[v]) {
             sFirst[v] = B.N.first[v];
@@ -509,7 +500,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     // a slot is a leaf when its node is a binary leaf or the collapse chose one
     auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0 || how[v][1] == 1; };
     for (size_t v = 0; v < nv; ++v)  // merged leaves: their items in slot order too
-        if (!B.N.count[v] && how[v][1] == 1)
+        if (!B.N.count[v] && how[v][1] == 1 && sCount[v] > 1)
             std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + sCount[v],
                              [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
 #endif
@@ -518,10 +509,12 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     std::vector<Task> queue{{0, 0, 0}};
     out.nodes.assign(WIDE_WORDS, 0u);
     uint32_t maxDepth = 0;
+    std::vector<uint32_t> kids;
+    kids.reserve(8);
     for (size_t qi = 0; qi < queue.size(); ++qi) {
         const Task t = queue[qi];
         maxDepth = std::max(maxDepth, t.depth);
-        std::vector<uint32_t> kids;
+        kids.clear();
 #if SB_WIDE_COLLAPSE_SAH
         if (is_leaf_slot(t.v)) kids.push_back(t.v);  // a small root is one leaf slot
         else {
@@ -555,8 +548,10 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
         for (uint32_t k : kids) nb.grow(B.N.box[k]);
         float ctr[3];
         for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
+        // (cost, kid, slot) by increasing cost, ties in generation order
         struct Cand { float cost; int kid, slot; };
-        std::vector<Cand> cands;
+        Cand cands[64];
+        int nc = 0;
         for (size_t k = 0; k < kids.size(); ++k) {
             const Box& b = B.N.box[kids[k]];
             for (int s = 0; s < 8; ++s) {
@@ -565,17 +560,24 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                     float d = 0.5f * (b.lo[a] + b.hi[a]) - ctr[a];
                     c += (s >> a & 1) ? -d : d;
                 }
-                cands.push_back({c, (int)k, s});
+                cands[nc++] = {c, (int)k, s};
             }
         }
-        std::stable_sort(cands.begin(), cands.end(), [](const Cand& x, const Cand& y) { return x.cost < y.cost; });
+        for (int i = 1; i < nc; ++i) {  // stable insertion sort (at most 64)
+            const Cand c = cands[i];
+            int j = i;
+            for (; j > 0 && c.cost < cands[j - 1].cost; --j) cands[j] = cands[j - 1];
+            cands[j] = c;
+        }
         int slotKid[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
-        std::vector<int> kidSlot(kids.size(), -1);
-        for (const Cand& c : cands)
+        int kidSlot[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+        for (int ci = 0; ci < nc; ++ci) {
+            const Cand& c = cands[ci];
             if (slotKid[c.slot] < 0 && kidSlot[c.kid] < 0) {
                 slotKid[c.slot] = c.kid;
                 kidSlot[c.kid] = c.slot;
             }
+        }
         // header, children and items
         uint32_t* w = out.nodes.data() + (size_t)t.w * WIDE_WORDS;
         int ex[3];
