@@ -54,6 +54,10 @@ def parse():
                          "nested cascades of the atrium + 8 independent atria per frame, batched vs plain; "
                          "large: 2.1M unique / 12.8M instanced triangles, C0 32^3 probes + fitted fine cascade C1, 256 rays, "
                          "binary vs 8-wide scene BVH vs the reference two-level walk")
+    ap.add_argument("--reflection", choices=["off", "rough", "high", "ultra"], default="off",
+                    help="atrium: the reflection tier of the probe field (both arms); gather: off times "
+                         "sb_gather_irradiance, a tier the combined receiver sb_gather_reflections on that tier's "
+                         "atlases")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-aux", action="store_true",
                     help="atrium only: skip the batched-form and adjoint measurements added to the line")
@@ -98,11 +102,12 @@ def make_workload():
     return scene
 
 
-def field_for(scene, device):
+def field_for(scene, device, reflection="off"):
     from speedball_b200.field import ProbeField
     g = scene.meta["grid"]
     f = ProbeField(scene, volumes=dict(gridMin=g["gridMin"], gridSize=g["gridSize"], res=g["res"]), cascades=1, rays=g["rays"],
-                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device)
+                   clusteredLighting=True, hysteresis=scene.meta["hysteresis"], jitterMode="gated", device=device,
+                   reflectionQuality=reflection)
     f.setHysteresisNormalization(False)
     f.setRayBudget(1 << 24, maxProbesPerTick=1 << 20)  # one solve updates all 4,096 probes
     return f
@@ -180,7 +185,7 @@ def run_ours(args, dist: Dist):
     rt = cudart()
     ck(rt.cudaSetDevice(device))
     scene = make_workload()
-    f = field_for(scene, device)
+    f = field_for(scene, device, args.reflection)
     lib, ctx, pool = f._lib, f.ctx, f.pool
     stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
     _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
@@ -324,7 +329,7 @@ def run_ours(args, dist: Dist):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded procedural atrium standing in for Sponza)",
-        "config": atrium_config(P, f.getRays(), int(pool.triIndex.shape[0]), dist.world),
+        "config": atrium_config(P, f.getRays(), int(pool.triIndex.shape[0]), dist.world, args.reflection),
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "ms_per_step": round(e2e_ms, 4),
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
@@ -340,7 +345,7 @@ def run_ours(args, dist: Dist):
         "clocks": clk,
     }
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scene, target_s=12.0)
+        line["cpu_baseline"] = cpu_baseline(scene, target_s=12.0, reflection=args.reflection)
     f.dispose()
     ck(rt.cudaFree(flush))
     return line
@@ -364,7 +369,7 @@ class CpuAtrium:
     mesh), updateTransforms (the 3 movers' instance rows + the TLAS refit of the
     frozen partition), then the FP32 solve of `probes` probes."""
 
-    def __init__(self, scene):
+    def __init__(self, scene, reflection: str = "off"):
         sys.path.insert(0, str(ROOT / "oracle"))
         import orc
         self.orc = orc
@@ -386,6 +391,8 @@ class CpuAtrium:
         self.prm = orc.default_params(scene.meta["hysteresis"])
         self.G = orc.grid_struct(self.g)
         self.irr, self.depth, self.atlas, self.datlas = orc.new_state(self.g, fp32=True)
+        tier = orc.REFLECT_TIERS[reflection]
+        self.rf = orc.ReflectState(self.g, tier, fp32=True) if tier else None
         self.probes = int(np.prod(self.g["res"]))
         self.dm = scene.meta["deformer"]
         self.movers = list(scene.meta["movers"])
@@ -420,8 +427,14 @@ class CpuAtrium:
         self.mats[pool.tlasBase:] = self.tl
 
     def solve(self, probes: int, offset: int = 0):
+        io = None
+        if self.rf is not None:
+            io = self.orc.OrcSolveIO()
+            self.rf.attach(io)
         self.orc.solve(self.S, self.arena, self.nl, True, self.G, self.G, self.prm, offset, probes, self.irr,
-                       self.depth, self.atlas, self.datlas, fp32=True)
+                       self.depth, self.atlas, self.datlas, fp32=True, io=io)
+        if self.rf is not None:
+            self.rf.advance()
 
     def step(self, frame_motion, probes: int, offset: int = 0) -> float:
         t0 = time.perf_counter()
@@ -430,21 +443,24 @@ class CpuAtrium:
         return time.perf_counter() - t0
 
 
-def atrium_config(probes: int, rays: int, tris: int, world: int) -> dict:
+def atrium_config(probes: int, rays: int, tris: int, world: int, reflection: str = "off") -> dict:
     """The workload description both arms print (the same keys and values)."""
-    return {"workload": "atrium 262,267 tris / 30 meshes, 16^3 probes x 64 rays, 32 clustered point + 1 "
-                        "directional light, 1 deforming + 3 moving meshes per frame",
-            "probes": probes, "rays_per_probe": rays, "primary_rays_per_step": probes * rays, "triangles": tris,
-            "l2": "flushed (256 MiB write) before every timed step (GPU arm)",
-            "parallelism": "replicas" if world > 1 else "single GPU"}
+    out = {"workload": "atrium 262,267 tris / 30 meshes, 16^3 probes x 64 rays, 32 clustered point + 1 "
+                       "directional light, 1 deforming + 3 moving meshes per frame",
+           "probes": probes, "rays_per_probe": rays, "primary_rays_per_step": probes * rays, "triangles": tris,
+           "l2": "flushed (256 MiB write) before every timed step (GPU arm)",
+           "parallelism": "replicas" if world > 1 else "single GPU"}
+    if reflection != "off":
+        out["reflection"] = reflection
+    return out
 
 
-def cpu_baseline(scene, target_s=12.0):
+def cpu_baseline(scene, target_s=12.0, reflection="off"):
     """The FP32 CPU restatement on every host thread: whole-atrium updates (the
     motion lanes + all 4,096 probes) repeated for about `target_s` seconds."""
     from speedball_b200 import synth
     threads = os.cpu_count() or 1
-    cpu = CpuAtrium(scene)
+    cpu = CpuAtrium(scene, reflection)
     dt = cpu.step(synth.atrium_motion(scene, 0), cpu.probes)
     reps = max(1, int(round(target_s / max(dt, 1e-3))))
     frames = [synth.atrium_motion(scene, 1 + i) for i in range(reps)]
@@ -461,7 +477,7 @@ def run_reference(args, dist: Dist):
     from speedball_b200 import synth
     scene = make_workload()
     threads = os.cpu_count() or 1
-    cpu = CpuAtrium(scene)
+    cpu = CpuAtrium(scene, args.reflection)
     W, K = args.warmup, args.steps
     frames = [synth.atrium_motion(scene, fr) for fr in range(W + K + 1)]
     dt = cpu.step(frames[-1], cpu.probes)
@@ -485,7 +501,8 @@ def run_reference(args, dist: Dist):
             "steps": K, "warmup": W, "ms_per_step": round(rays / (value * 1e6) * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural atrium standing in for Sponza)",
-            "config": atrium_config(cpu.probes, cpu.g["rays"], int(cpu.pool.triIndex.shape[0]), dist.world),
+            "config": atrium_config(cpu.probes, cpu.g["rays"], int(cpu.pool.triIndex.shape[0]), dist.world,
+                                    args.reflection),
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -799,33 +816,54 @@ def run_gather(args, dist: Dist):
     """One step = one receiver gather of a 1920x1080 deferred G-buffer of the
     atrium (covered pixels) from the atlases of 4 updates: position, stable
     normal and detail normal in (48 B per sample), irradiance out (16 B).
+    With --reflection rough / high / ultra the step is the combined receiver
+    (sb_gather_reflections) on that tier's atlases: the mirror reflection of
+    the camera ray about the normal and a seeded roughness in [0, 1) also in
+    (16 B), the reflection layer also out (16 B).
     value = samples / device time; e2e = the same through host buffers
-    (G-buffer up, irradiance down, page-locked)."""
+    (G-buffer up, outputs down, page-locked)."""
     from speedball_b200 import _abi
     device = dist.local
     rt = cudart()
     ck(rt.cudaSetDevice(device))
     scene = make_workload()
-    f = field_for(scene, device)
+    combined = args.reflection != "off"
+    f = field_for(scene, device, args.reflection)
     for _ in range(4):
         f.tick()
     f.synchronize()
     pos, nrm = camera_gbuffer(f, scene)
     n = pos.shape[0]
+    inputs = [pos, nrm, nrm]
+    if combined:
+        g = scene.meta["grid"]
+        cam = np.asarray(g["gridMin"], np.float64) + 0.5 * np.asarray(g["gridSize"], np.float64)
+        v = pos[:, :3].astype(np.float64) - cam
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        nn = nrm[:, :3].astype(np.float64)
+        refl = np.zeros((n, 4), np.float32)
+        refl[:, :3] = v - 2.0 * np.einsum("ni,ni->n", v, nn)[:, None] * nn
+        refl[:, 3] = np.random.default_rng(31).uniform(0.0, 1.0, n)
+        inputs.append(refl)
+    n_out = 2 if combined else 1
     lib, ctx = f._lib, f.ctx
     stream = ck(rt.cudaStreamCreateWithFlags(rt.cudaStreamNonBlocking))
     _abi.check(lib.sb_set_stream(ctx, C.c_void_p(int(stream))), ctx)
     flush = ck(rt.cudaMalloc(L2_FLUSH_BYTES))
-    bufs = [ck(rt.cudaMalloc(n * 16)) for _ in range(4)]  # position, stable normal, detail normal, out
-    for b, a in zip(bufs[:3], (pos, nrm, nrm)):
+    bufs = [ck(rt.cudaMalloc(n * 16)) for _ in range(len(inputs) + n_out)]
+    for b, a in zip(bufs, inputs):
         ck(rt.cudaMemcpy(b, a.ctypes.data, n * 16, rt.cudaMemcpyKind.cudaMemcpyHostToDevice))
     prm = _abi.sb_gather_params()
     lib.sb_gather_params_defaults(C.byref(prm))
     prm.normalBias[0] = max(1e-4, f.grid.cellMin * 0.04)
+    ptr = [C.c_void_p(int(b)) for b in bufs]
 
     def gather():
-        _abi.check(lib.sb_gather_irradiance(ctx, C.byref(prm), C.c_void_p(int(bufs[0])), C.c_void_p(int(bufs[1])),
-                                            C.c_void_p(int(bufs[2])), n, C.c_void_p(int(bufs[3]))), ctx)
+        if combined:
+            _abi.check(lib.sb_gather_reflections(ctx, C.byref(prm), ptr[0], ptr[1], ptr[2], ptr[3], n, ptr[4],
+                                                 ptr[5]), ctx)
+        else:
+            _abi.check(lib.sb_gather_irradiance(ctx, C.byref(prm), ptr[0], ptr[1], ptr[2], n, ptr[3]), ctx)
 
     e0, e1 = ck(rt.cudaEventCreate()), ck(rt.cudaEventCreate())
     W, K = args.warmup, args.steps
@@ -845,20 +883,20 @@ def run_gather(args, dist: Dist):
         ck(rt.cudaEventSynchronize(e1))
         total += ck(rt.cudaEventElapsedTime(e0, e1))
     ms = dist.max(total / K)
-    # end to end: page-locked G-buffer up, gather, irradiance down
-    hp = [_abi.PinnedArray((n, 4), np.float32) for _ in range(4)]
-    hp[0].array[...] = pos
-    hp[1].array[...] = nrm
-    hp[2].array[...] = nrm
+    # end to end: page-locked G-buffer up, gather, outputs down
+    hp = [_abi.PinnedArray((n, 4), np.float32) for _ in range(len(bufs))]
+    for h, a in zip(hp, inputs):
+        h.array[...] = a
     H2D, D2H = rt.cudaMemcpyKind.cudaMemcpyHostToDevice, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost
     e2e = 0.0
     for i in range(W + K):
         ck(rt.cudaStreamSynchronize(stream))
         t0 = time.perf_counter()
-        for b, h in zip(bufs[:3], hp[:3]):
+        for b, h in zip(bufs[:len(inputs)], hp[:len(inputs)]):
             ck(rt.cudaMemcpyAsync(b, h.array.ctypes.data, n * 16, H2D, stream))
         gather()
-        ck(rt.cudaMemcpyAsync(hp[3].array.ctypes.data, bufs[3], n * 16, D2H, stream))
+        for b, h in zip(bufs[len(inputs):], hp[len(inputs):]):
+            ck(rt.cudaMemcpyAsync(h.array.ctypes.data, b, n * 16, D2H, stream))
         ck(rt.cudaStreamSynchronize(stream))
         if i >= W:
             e2e += time.perf_counter() - t0
@@ -866,26 +904,34 @@ def run_gather(args, dist: Dist):
     clk = clocks.stop()
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = 64.0 * n / (ms * 1e-3) / 1e9
-    out = hp[3].array
+    bytes_per = 16.0 * len(bufs)
+    achieved = bytes_per * n / (ms * 1e-3) / 1e9
+    out = hp[len(inputs)].array
     line = {
         "metric": GATHER_METRIC, "value": round(dist.world * n / (ms * 1e-3) / 1e6, 2), "unit": "Msamples/s",
         "n_gpus": dist.world, "steps": K, "warmup": W, "ms_per_step": round(ms, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (RGBA16F atlases)",
         "data": "synthetic (seeded procedural atrium, atlases of 4 updates)",
-        "config": {"workload": "receiver gather of a 1920x1080 deferred G-buffer of the atrium (covered pixels), "
-                               "16^3 probes, default receiver uniforms (8-tap trilinear)", "samples": n,
+        "config": {"workload": ("combined receiver (irradiance + reflection layer, reflection tier "
+                                f"{args.reflection})" if combined else "receiver gather") +
+                               " of a 1920x1080 deferred G-buffer of the atrium (covered pixels), 16^3 probes, "
+                               "default receiver uniforms (8-tap trilinear)", "samples": n,
                    "l2": "flushed (256 MiB write) before every timed step"},
         "e2e": {"value": round(dist.world * n / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Msamples/s",
-                "ms_per_step": round(e2e_ms, 4), "h2d_bytes_per_step": 48 * n, "d2h_bytes_per_step": 16 * n},
+                "ms_per_step": round(e2e_ms, 4), "h2d_bytes_per_step": 16 * len(inputs) * n,
+                "d2h_bytes_per_step": 16 * n_out * n},
         "gpu_launches": K,
-        "roofline": {"bound": "hbm", "kernel": "k_gather", "achieved": round(achieved, 1), "peak": peak,
+        "roofline": {"bound": "hbm", "kernel": "k_gather_combined" if combined else "k_gather",
+                     "achieved": round(achieved, 1), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
-                     "algorithmic_bytes_per_launch": 64 * n,
+                     "algorithmic_bytes_per_launch": int(bytes_per * n),
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s"},
         "irradiance_mean": [round(float(x), 5) for x in out[:, :3].mean(0)],
         "clocks": clk,
     }
+    if combined:
+        r = hp[len(inputs) + 1].array
+        line["reflection_mean"] = [round(float(x), 5) for x in r.mean(0)]
     for b in bufs:
         ck(rt.cudaFree(b))
     ck(rt.cudaFree(flush))
