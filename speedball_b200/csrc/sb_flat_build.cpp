@@ -499,10 +499,6 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     };
     // a slot is a leaf when its node is a binary leaf or the collapse chose one
     auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0 || how[v][1] == 1; };
-    for (size_t v = 0; v < nv; ++v)  // merged leaves: their items in slot order too
-        if (!B.N.count[v] && how[v][1] == 1 && sCount[v] > 1)
-            std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + sCount[v],
-                             [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
 #endif
 
     struct Task { uint32_t v, w, depth; };
@@ -609,6 +605,11 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                 queue.push_back({v, 0, t.depth + 1});  // node index assigned below, in slot order
             } else {
                 const uint32_t cnt = sCount[v];
+                // a leaf merged from an interior node: its items in slot order too (its
+                // range is its own; the parts of a node split across slots are not sorted)
+                if (!B.N.count[v] && cnt > 1)
+                    std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + cnt,
+                                     [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
                 meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
                 for (uint32_t k = 0; k < cnt; ++k) {
                     out.items.push_back(itemTri[B.order[sFirst[v] + k]]);

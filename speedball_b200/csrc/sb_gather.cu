@@ -236,7 +236,10 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float radius = fmaxf(dR.x, 1e-4f), radius2 = radius * radius;
         const float3 q = reflP - probePos;
         const float q2 = dot3(q, q), qDotR = dot3(q, Rn);
-        const float disc = radius2 - q2 + qDotR * qDotR;
+        // radius^2 - q^2 + (q.R)^2 with |R| = 1 is radius^2 - |q x R|^2: the cross
+        // product keeps the two nearly equal squares from cancelling in FP32
+        const float3 qxR = cross3(q, Rn);
+        const float disc = radius2 - dot3(qxR, qxR);
         const float sqrtDisc = sqrtf(fmaxf(disc, 0.0f));
         const float nearT = -qDotR - sqrtDisc, farT = -qDotR + sqrtDisc;
         const float rayT = nearT > 1e-4f ? nearT : farT;

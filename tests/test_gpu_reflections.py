@@ -53,13 +53,15 @@ def _run(scene, tier, solves, budget=None, sky=False):
 def test_rough_tier_room_with_metals():
     s = synth.room_spheres(0)
     s.materials = s.materials.copy()
-    s.materials[::2, 4] = 1.0  # every other material fully metallic: no diffuse energy
-    s.materials[::2, 7:10] = 0.0
+    walls = int(s.meshes[0].tri_material[0])
+    metal = [m for m in range(0, s.materials.shape[0], 2) if m != walls]
+    s.materials[metal, 4] = 1.0  # every other sphere material fully metallic: no diffuse energy
+    s.materials[metal, 7:10] = 0.0
     lay, reports, mirror = _run(s, "rough", 3)
     assert lay["tier"] == 1 and lay["glossyTile"] == 0
     print("rough room", reports[-1])
     cov = reports[-1]["rough_coverage_mean"]
-    assert 0.2 < cov < 0.9, cov  # the metallic hits are left out of the lobe
+    assert 0.3 < cov < 0.999, cov  # the metallic hits are left out of the lobe
 
 
 @pytest.mark.parametrize("tier", ["high", "ultra"])
@@ -125,7 +127,8 @@ def test_combined_receiver_matches_oracle(case):
     torch = pytest.importorskip("torch")
     s = synth.room_spheres(0)
     s.materials = s.materials.copy()
-    s.materials[::2, 4] = 1.0
+    walls = int(s.meshes[0].tri_material[0])
+    s.materials[[m for m in range(0, s.materials.shape[0], 2) if m != walls], 4] = 1.0
     f = gu.make_field(s, reflectionQuality="high")
     try:
         g = s.meta["grid"]
@@ -180,6 +183,13 @@ def test_combined_receiver_matches_oracle(case):
         ec = gu.texel_rel_err(gr[~edge, 3].astype(np.float64), wr[~edge, 3])
         print(case, "irr", ei.max(), "refl", er.max(), "coverage", ec.max(), "edge", int(edge.sum()),
               "covered share", float((wr[:, 3] > 0).mean()))
+        keep = np.flatnonzero(~edge)
+        for name, e, gv, ov in (("refl", er.max(1), gr[keep, :3], wr[keep, :3]), ("coverage", ec, gr[keep, 3], wr[keep, 3])):
+            worst = np.argsort(e)[-5:]
+            print(name, "abs err max", float(np.abs(gv.astype(np.float64) - ov).max()), "scale", float(np.abs(ov).max()),
+                  "over 1e-3:", int((e > 1e-3).sum()),
+                  [(float(e[k]), np.asarray(gv[k]).tolist(), np.asarray(ov[k]).tolist(), float(r4[keep[k], 3]),
+                    float(near[keep[k]])) for k in worst])
         assert max(ei.max(), er.max(), ec.max()) <= gu.TEXEL_REL
         assert (wr[:, 3] > 0).mean() > 0.5 and wr[:, :3].max() > 0.01
         assert lib_refuses_without_lobes(f)
