@@ -160,10 +160,13 @@ __device__ __forceinline__ float4 bilinear4(const uint2* atlas, uint32_t W, uint
                        t00.w * w00 + t10.w * w10 + t01.w * w01 + t11.w * w11);
 }
 
-__device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
-    const float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+// smoothstep with the reciprocal of its (constant) edge span supplied
+__device__ __forceinline__ float smoothstepf(float e0, float invSpan, float x) {
+    const float t = clampf((x - e0) * invSpan, 0.0f, 1.0f);
     return t * t * (3.0f - 2.0f * t);
 }
+
+__device__ __forceinline__ float3 fast_normalize(float3 a) { return a * rsqrtf(dot3(a, a)); }
 
 // One cascade of the combined receiver (_sampleCombinedCascadeLooped,
 // gi_probes.js:662-771): the irradiance taps with the cage at the biased point
@@ -171,13 +174,12 @@ __device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
 __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, float chebyBias, float3 P, float3 reflP,
                                  float3 Nvis, float3 Ndir, float3 Rn, bool dual, float rw, float lobeMix,
                                  float3& irr, float4& refl) {
-    float base[3], frac[3], rm1[3];
+    float base[3], frac[3], cell[3];
     const float cp[3] = {P.x, P.y, P.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        rm1[a] = fmaxf(C.res[a] - 1.0f, 1.0f);
-        const float cell = C.gridSize[a] / rm1[a];
-        const float gf = (cp[a] - C.gridMin[a]) / fmaxf(cell, 1e-6f);
+        cell[a] = C.gridSize[a] / fmaxf(C.res[a] - 1.0f, 1.0f);
+        const float gf = (cp[a] - C.gridMin[a]) / fmaxf(cell[a], 1e-6f);
         base[a] = clampf(floorf(gf), 0.0f, fmaxf(C.res[a] - 2.0f, 0.0f));
         frac[a] = clampf(gf - base[a], 0.0f, 1.0f);
     }
@@ -185,6 +187,7 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
     const float2 oN = oct_encode(normalize3(Ndir));
     const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
     const float2 oR = oct_encode(Rn);
+    const uint32_t resX = (uint32_t)C.res[0], resXY = resX * (uint32_t)C.res[1];
     const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
     const float cs = A.chebyStrength;
     const bool glossyOn = C.glossy != nullptr;
@@ -193,6 +196,7 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
     float3 acc = mk(0.0f, 0.0f, 0.0f);
     float wsum = 0.0f, roughW = 0.0f, glossyW = 0.0f;
     float4 roughAcc = make_float4(0.f, 0.f, 0.f, 0.f), glossyAcc = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
     for (int i = 0; i < 8; ++i) {
         const int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
         const float px = base[0] + float(dx), py = base[1] + float(dy), pz = base[2] + float(dz);
@@ -202,9 +206,10 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float wTri = wx * wy * wz + 1e-4f;
         const float row = pz * C.res[1] + py;
         const float ox0 = px * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
-        const float3 probePos = mk(C.gridMin[0] + px / rm1[0] * C.gridSize[0],
-                                   C.gridMin[1] + py / rm1[1] * C.gridSize[1],
-                                   C.gridMin[2] + pz / rm1[2] * C.gridSize[2]);
+        // the probe at grid index (px, py, pz): gridMin + p * cell (within an ulp of
+        // the reference's gridMin + p / (res - 1) * gridSize)
+        const float3 probePos = mk(fmaf(px, cell[0], C.gridMin[0]), fmaf(py, cell[1], C.gridMin[1]),
+                                   fmaf(pz, cell[2], C.gridMin[2]));
         float w = wTri;
         if (cs != 0.0f) {
             const float3 toSurf = P - probePos;
@@ -243,18 +248,19 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float sqrtDisc = sqrtf(fmaxf(disc, 0.0f));
         const float nearT = -qDotR - sqrtDisc, farT = -qDotR + sqrtDisc;
         const float rayT = nearT > 1e-4f ? nearT : farT;
-        const float relVar = fmaxf(dR.y - radius2, 0.0f) / fmaxf(radius2, 1e-4f);
-        const float stableDepth = 1.0f - smoothstepf(0.02f, 0.20f, relVar);
+        const float invR2 = 1.0f / fmaxf(radius2, 1e-4f);
+        const float relVar = fmaxf(dR.y - radius2, 0.0f) * invR2;
+        const float stableDepth = 1.0f - smoothstepf(0.02f, 1.0f / 0.18f, relVar);
         const float validHit = (disc > 1e-6f && rayT > 1e-4f) ? 1.0f : 0.0f;
-        const float insideWeight = smoothstepf(0.0f, 0.12f, (radius2 - q2) / fmaxf(radius2, 1e-4f));
+        const float insideWeight = smoothstepf(0.0f, 1.0f / 0.12f, (radius2 - q2) * invR2);
         const float pw = stableDepth * validHit * insideWeight;
-        const float3 corrected = normalize3(q + Rn * fmaxf(rayT, 0.0f));
-        const float2 oSR = oct_encode(normalize3(Rn * (1.0f - pw) + corrected * pw));
+        const float3 corrected = fast_normalize(q + Rn * fmaxf(rayT, 0.0f));
+        const float2 oSR = oct_encode(fast_normalize(Rn * (1.0f - pw) + corrected * pw));
         const float probeW = w * w;
         if (wantsGlossy) {
-            const float probeIndex = px + py * C.res[0] + pz * (C.res[0] * C.res[1]);
-            const float tx = float(C.glossyTilesX);
-            const float grow = floorf(probeIndex / tx), gcol = probeIndex - tx * grow;
+            // the probe's glossy tile: the index and its row and column are exact integers
+            const uint32_t probeIndex = (uint32_t)px + (uint32_t)py * resX + (uint32_t)pz * resXY;
+            const float grow = float(probeIndex / C.glossyTilesX), gcol = float(probeIndex % C.glossyTilesX);
             const float ox = gcol * float(C.glossyTile) + 1.0f + oSR.x * float(C.glossyOct);
             const float oy = grow * float(C.glossyTile) + 1.0f + oSR.y * float(C.glossyOct);
             const float4 gl = bilinear4(C.glossy, C.glossyW, C.glossyH, ox / float(C.glossyW), oy / float(C.glossyH));
@@ -283,7 +289,7 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
     }
 }
 
-__global__ void __launch_bounds__(256) k_gather_combined(const GatherArgs A) {
+__global__ void __launch_bounds__(256, 3) k_gather_combined(const GatherArgs A) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.count) return;
     const float4 p4 = __ldcs(A.position + i), n4 = __ldcs(A.stableNormal + i), d4 = __ldcs(A.detailNormal + i);
@@ -294,7 +300,7 @@ __global__ void __launch_bounds__(256) k_gather_combined(const GatherArgs A) {
     const float3 P = reflP + Nvis * A.normalBias0 * A.sampleBiasScale;
     const float part = roughness <= A.roughnessLimit ? 1.0f : 0.0f;
     const float rw = clampf(A.reflectionIntensity * A.enabled * part, 0.0f, 1.0f);
-    const float lobeMix = A.c[0].glossy ? smoothstepf(0.22f, 0.58f, roughness) : 1.0f;
+    const float lobeMix = A.c[0].glossy ? smoothstepf(0.22f, 1.0f / 0.36f, roughness) : 1.0f;
     float3 E;
     float4 S;
     if (A.cascades < 2) {
