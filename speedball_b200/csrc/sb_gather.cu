@@ -8,7 +8,8 @@
 // and fine looped gathers blended by the fine box's border band, each choosing
 // its cage at the unbiased surface position (the looped gather's stated intent,
 // gi_probes.js:628-631). Each of the 8 cage taps fetches the RGBA16F atlas
-// bilinearly (clamp to edge, exact weights) in the detail normal's octahedral
+// bilinearly (exact weights; the footprint stays inside the probe's tile, so the
+// sampler's edge clamp never applies) in the detail normal's octahedral
 // direction; with chebyStrength > 0 it also fetches the depth moments toward
 // the surface for the Chebyshev visibility weight and applies the wrap weight.
 // Output E = max(sample, 0) * intensity * enabled as float4 (rgb, 1).
@@ -24,22 +25,35 @@ namespace sb {
 
 namespace {
 
-__device__ __forceinline__ float3 bilinear3(const uint2* atlas, uint32_t W, uint32_t H, float u, float v) {
-    const float x = u * float(W) - 0.5f, y = v * float(H) - 0.5f;
-    const float fx0 = floorf(x), fy0 = floorf(y);
-    const float fx = x - fx0, fy = y - fy0;
-    const int x0 = (int)fx0, y0 = (int)fy0;
-    const int Wi = (int)W, Hi = (int)H;
-    const int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
-    const int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
-    const float4 t00 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xa));
-    const float4 t10 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xb));
-    const float4 t01 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xa));
-    const float4 t11 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xb));
-    const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
-    return mk(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
-              t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
-              t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
+// A bilinear read inside one probe's octahedral tile. The atlas coordinate of
+// direction o is tileOrigin + BORDER + o * octRes - 0.5 (texel centres), so the
+// tile-local coordinate 0.5 + o * octRes lies in [0.5, octRes + 0.5]: the 2x2
+// footprint never leaves the tile (gutter included), edge clamping never
+// applies, and the offset and weights are the same for every tap that reads the
+// same direction. Formed once, without the atlas-wide coordinate's rounding.
+struct TileTap {
+    uint32_t off;  // first texel of the footprint, from the tile origin (row * W + column)
+    float fx, fy;
+};
+__device__ __forceinline__ TileTap tile_tap(float2 o, uint32_t W, float octRes) {
+    const float xl = fmaf(o.x, octRes, 0.5f), yl = fmaf(o.y, octRes, 0.5f);
+    const float x0 = floorf(xl), y0 = floorf(yl);
+    TileTap t;
+    t.off = (uint32_t)y0 * W + (uint32_t)x0;
+    t.fx = xl - x0;
+    t.fy = yl - y0;
+    return t;
+}
+__device__ __forceinline__ float4 tile_fetch(const uint2* atlas, uint32_t W, uint32_t tileOrigin, const TileTap& t) {
+    const uint2* p = atlas + tileOrigin + t.off;
+    const float4 t00 = half4_to_float4(__ldg(p)), t10 = half4_to_float4(__ldg(p + 1));
+    const float4 t01 = half4_to_float4(__ldg(p + W)), t11 = half4_to_float4(__ldg(p + W + 1));
+    const float w00 = (1.0f - t.fx) * (1.0f - t.fy), w10 = t.fx * (1.0f - t.fy), w01 = (1.0f - t.fx) * t.fy,
+                w11 = t.fx * t.fy;
+    return make_float4(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
+                       t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
+                       t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11,
+                       t00.w * w00 + t10.w * w10 + t01.w * w01 + t11.w * w11);
 }
 
 // FULL = false compiles the default receiver alone (chebyStrength 0, no dual
@@ -58,9 +72,9 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
         frac[a] = clampf(gf - base[a], 0.0f, 1.0f);
     }
     const float3 Nn = normalize3(Nvis);
-    const float2 oN = oct_encode(normalize3(Ndir));
-    const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
-    const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
+    const TileTap tN = tile_tap(oct_encode(normalize3(Ndir)), C.atlasW, 6.0f);
+    const TileTap tS = dual ? tile_tap(oct_encode(Nn), C.atlasW, 6.0f) : tN;
+    const uint32_t resY = (uint32_t)C.res[1];
     const float cs = FULL ? A.chebyStrength : 0.0f;
     if (!FULL) dual = false;
     float3 acc = mk(0.0f, 0.0f, 0.0f);
@@ -73,8 +87,7 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float wy = dy ? frac[1] : 1.0f - frac[1];
         const float wz = dz ? frac[2] : 1.0f - frac[2];
         const float wTri = wx * wy * wz + 1e-4f;
-        const float col = px, row = pz * C.res[1] + py;
-        const float ox0 = col * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
+        const uint32_t tile = ((uint32_t)pz * resY + (uint32_t)py) * 8u * C.atlasW + (uint32_t)px * 8u;
         float w = wTri;
         if (FULL && cs != 0.0f) {
             const float3 probePos = mk(C.gridMin[0] + px / rm1[0] * C.gridSize[0],
@@ -83,9 +96,7 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
             const float3 toSurf = P - probePos;
             const float dist = sqrtf(dot3(toSurf, toSurf));
             const float inv = 1.0f / fmaxf(dist, 1e-6f);
-            const float2 oD = oct_encode(toSurf * inv);
-            const float3 m = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oD.x * 6.0f) * invW,
-                                       (oy0 + oD.y * 6.0f) * invH);
+            const float4 m = tile_fetch(C.depth, C.atlasW, tile, tile_tap(oct_encode(toSurf * inv), C.atlasW, 6.0f));
             const float m1 = m.x, m2 = m.y;
             const float variance = fabsf(m2 - m1 * m1);
             const float dm = fmaxf(dist - m1 - chebyBias, 0.0f);
@@ -97,12 +108,12 @@ __device__ float3 gather_cascade(const GatherCascade& C, const GatherArgs& A, fl
             const float wrapW = (1.0f - cs) + fmaxf(wrap * wrap, 0.05f) * cs;
             w = wTri * wrapW * visW;
         }
-        float3 e = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oN.x * 6.0f) * invW, (oy0 + oN.y * 6.0f) * invH);
+        const float4 e4 = tile_fetch(C.atlas, C.atlasW, tile, tN);
+        float3 e = mk(e4.x, e4.y, e4.z);
         if (FULL && dual) {
-            const float3 eS = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oS.x * 6.0f) * invW,
-                                        (oy0 + oS.y * 6.0f) * invH);
+            const float4 eS = tile_fetch(C.atlas, C.atlasW, tile, tS);
             const float t = A.detailStrength;
-            e = eS * (1.0f - t) + e * t;
+            e = mk(eS.x, eS.y, eS.z) * (1.0f - t) + e * t;
         }
         acc = acc + e * w;
         wsum += w;
@@ -141,24 +152,6 @@ __global__ void __launch_bounds__(256, FULL ? 3 : 4) k_gather(const GatherArgs A
     __stcs(A.out + i, make_float4(fmaxf(E.x, 0.0f) * k, fmaxf(E.y, 0.0f) * k, fmaxf(E.z, 0.0f) * k, 1.0f));
 }
 
-__device__ __forceinline__ float4 bilinear4(const uint2* atlas, uint32_t W, uint32_t H, float u, float v) {
-    const float x = u * float(W) - 0.5f, y = v * float(H) - 0.5f;
-    const float fx0 = floorf(x), fy0 = floorf(y);
-    const float fx = x - fx0, fy = y - fy0;
-    const int x0 = (int)fx0, y0 = (int)fy0;
-    const int Wi = (int)W, Hi = (int)H;
-    const int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
-    const int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
-    const float4 t00 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xa));
-    const float4 t10 = half4_to_float4(__ldg(atlas + (size_t)ya * W + xb));
-    const float4 t01 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xa));
-    const float4 t11 = half4_to_float4(__ldg(atlas + (size_t)yb * W + xb));
-    const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
-    return make_float4(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
-                       t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
-                       t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11,
-                       t00.w * w00 + t10.w * w10 + t01.w * w01 + t11.w * w11);
-}
 
 // smoothstep with the reciprocal of its (constant) edge span supplied
 __device__ __forceinline__ float smoothstepf(float e0, float invSpan, float x) {
@@ -184,11 +177,10 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         frac[a] = clampf(gf - base[a], 0.0f, 1.0f);
     }
     const float3 Nn = normalize3(Nvis);
-    const float2 oN = oct_encode(normalize3(Ndir));
-    const float2 oS = dual ? oct_encode(Nn) : make_float2(0.0f, 0.0f);
-    const float2 oR = oct_encode(Rn);
-    const uint32_t resX = (uint32_t)C.res[0], resXY = resX * (uint32_t)C.res[1];
-    const float invW = 1.0f / float(C.atlasW), invH = 1.0f / float(C.atlasH);
+    const TileTap tN = tile_tap(oct_encode(normalize3(Ndir)), C.atlasW, 6.0f);
+    const TileTap tS = dual ? tile_tap(oct_encode(Nn), C.atlasW, 6.0f) : tN;
+    const TileTap tR = tile_tap(oct_encode(Rn), C.atlasW, 6.0f);
+    const uint32_t resX = (uint32_t)C.res[0], resY = (uint32_t)C.res[1], resXY = resX * resY;
     const float cs = A.chebyStrength;
     const bool glossyOn = C.glossy != nullptr;
     const bool wantsRough = lobeMix > 0.0f, wantsGlossy = glossyOn && lobeMix < 1.0f;
@@ -204,8 +196,7 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         const float wy = dy ? frac[1] : 1.0f - frac[1];
         const float wz = dz ? frac[2] : 1.0f - frac[2];
         const float wTri = wx * wy * wz + 1e-4f;
-        const float row = pz * C.res[1] + py;
-        const float ox0 = px * 8.0f + 1.0f, oy0 = row * 8.0f + 1.0f;
+        const uint32_t tile = ((uint32_t)pz * resY + (uint32_t)py) * 8u * C.atlasW + (uint32_t)px * 8u;
         // the probe at grid index (px, py, pz): gridMin + p * cell (within an ulp of
         // the reference's gridMin + p / (res - 1) * gridSize)
         const float3 probePos = mk(fmaf(px, cell[0], C.gridMin[0]), fmaf(py, cell[1], C.gridMin[1]),
@@ -215,9 +206,7 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
             const float3 toSurf = P - probePos;
             const float dist = sqrtf(dot3(toSurf, toSurf));
             const float inv = 1.0f / fmaxf(dist, 1e-6f);
-            const float2 oD = oct_encode(toSurf * inv);
-            const float3 m = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oD.x * 6.0f) * invW,
-                                       (oy0 + oD.y * 6.0f) * invH);
+            const float4 m = tile_fetch(C.depth, C.atlasW, tile, tile_tap(oct_encode(toSurf * inv), C.atlasW, 6.0f));
             const float variance = fabsf(m.y - m.x * m.x);
             const float dm = fmaxf(dist - m.x - chebyBias, 0.0f);
             const float chebyRaw = variance / fmaxf(variance + dm * dm, 1e-6f);
@@ -227,17 +216,17 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
             const float wrapW = (1.0f - cs) + fmaxf(wrap * wrap, 0.05f) * cs;
             w = wTri * wrapW * visW;
         }
-        float3 e = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oN.x * 6.0f) * invW, (oy0 + oN.y * 6.0f) * invH);
+        const float4 e4 = tile_fetch(C.atlas, C.atlasW, tile, tN);
+        float3 e = mk(e4.x, e4.y, e4.z);
         if (dual) {
-            const float3 eS = bilinear3(C.atlas, C.atlasW, C.atlasH, (ox0 + oS.x * 6.0f) * invW,
-                                        (oy0 + oS.y * 6.0f) * invH);
-            e = eS * (1.0f - A.detailStrength) + e * A.detailStrength;
+            const float4 eS = tile_fetch(C.atlas, C.atlasW, tile, tS);
+            e = mk(eS.x, eS.y, eS.z) * (1.0f - A.detailStrength) + e * A.detailStrength;
         }
         acc = acc + e * w;
         wsum += w;
         if (!wantsTap) continue;
         // the reflection ray against the sphere of the probe's mean depth toward R
-        const float3 dR = bilinear3(C.depth, C.atlasW, C.atlasH, (ox0 + oR.x * 6.0f) * invW, (oy0 + oR.y * 6.0f) * invH);
+        const float4 dR = tile_fetch(C.depth, C.atlasW, tile, tR);
         const float radius = fmaxf(dR.x, 1e-4f), radius2 = radius * radius;
         const float3 q = reflP - probePos;
         const float q2 = dot3(q, q), qDotR = dot3(q, Rn);
@@ -260,18 +249,16 @@ __device__ void combined_cascade(const GatherCascade& C, const GatherArgs& A, fl
         if (wantsGlossy) {
             // the probe's glossy tile: the index and its row and column are exact integers
             const uint32_t probeIndex = (uint32_t)px + (uint32_t)py * resX + (uint32_t)pz * resXY;
-            const float grow = float(probeIndex / C.glossyTilesX), gcol = float(probeIndex % C.glossyTilesX);
-            const float ox = gcol * float(C.glossyTile) + 1.0f + oSR.x * float(C.glossyOct);
-            const float oy = grow * float(C.glossyTile) + 1.0f + oSR.y * float(C.glossyOct);
-            const float4 gl = bilinear4(C.glossy, C.glossyW, C.glossyH, ox / float(C.glossyW), oy / float(C.glossyH));
+            const uint32_t gtile = (probeIndex / C.glossyTilesX) * C.glossyTile * C.glossyW +
+                                   (probeIndex % C.glossyTilesX) * C.glossyTile;
+            const float4 gl = tile_fetch(C.glossy, C.glossyW, gtile, tile_tap(oSR, C.glossyW, float(C.glossyOct)));
             const float gw = probeW * (0.2f * (1.0f - pw) + pw);
             glossyAcc = make_float4(glossyAcc.x + gl.x * gw, glossyAcc.y + gl.y * gw, glossyAcc.z + gl.z * gw,
                                     glossyAcc.w + gl.w * gw);
             glossyW += gw;
         }
         if (wantsRough) {
-            const float4 br = bilinear4(C.rough, C.atlasW, C.atlasH, (ox0 + oSR.x * 6.0f) * invW,
-                                        (oy0 + oSR.y * 6.0f) * invH);
+            const float4 br = tile_fetch(C.rough, C.atlasW, tile, tile_tap(oSR, C.atlasW, 6.0f));
             roughAcc = make_float4(roughAcc.x + br.x * probeW, roughAcc.y + br.y * probeW, roughAcc.z + br.z * probeW,
                                    roughAcc.w + br.w * probeW);
             roughW += probeW;
