@@ -416,9 +416,11 @@ __device__ __forceinline__ void atlas_taps(const DevCascade& C, float3 P, float3
         base[a] = clampf(floorf(gf[a]), 0.0f, fmaxf(float(C.res[a]) - 2.0f, 0.0f));
         frac[a] = clampf(gf[a] - base[a], 0.0f, 1.0f);
     }
-    float2 ouv = oct_encode(normalize3(N));
-    const float W = float(C.atlasW), H = float(C.atlasH);
-    const int Wi = (int)C.atlasW, Hi = (int)C.atlasH;
+    // the footprint and weights of sample_atlas (tile-local, the same for all taps)
+    const float2 ouv = oct_encode(normalize3(N));
+    const float xl = fmaf(ouv.x, 6.0f, 0.5f), yl = fmaf(ouv.y, 6.0f, 0.5f);
+    const float fx0 = floorf(xl), fy0 = floorf(yl), fx = xl - fx0, fy = yl - fy0;
+    const uint32_t Wu = C.atlasW, off = (uint32_t)fy0 * Wu + (uint32_t)fx0;
     float wsum = 0.0f;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -428,19 +430,11 @@ __device__ __forceinline__ void atlas_taps(const DevCascade& C, float3 P, float3
         float wy = dy ? frac[1] : 1.0f - frac[1];
         float wz = dz ? frac[2] : 1.0f - frac[2];
         float w = wx * wy * wz + 1e-4f;
-        float row = pz * float(C.res[1]) + py;
-        float ox = px * 8.0f + 1.0f + ouv.x * 6.0f;
-        float oy = row * 8.0f + 1.0f + ouv.y * 6.0f;
-        float x = (ox / W) * W - 0.5f, y = (oy / H) * H - 0.5f;
-        float fx0 = floorf(x), fy0 = floorf(y);
-        float fx = x - fx0, fy = y - fy0;
-        int x0 = (int)fx0, y0 = (int)fy0;
-        int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
-        int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
-        idx[4 * i] = (uint32_t)(ya * Wi + xa);
-        idx[4 * i + 1] = (uint32_t)(ya * Wi + xb);
-        idx[4 * i + 2] = (uint32_t)(yb * Wi + xa);
-        idx[4 * i + 3] = (uint32_t)(yb * Wi + xb);
+        const uint32_t t = ((uint32_t)pz * C.res[1] + (uint32_t)py) * 8u * Wu + (uint32_t)px * 8u + off;
+        idx[4 * i] = t;
+        idx[4 * i + 1] = t + 1u;
+        idx[4 * i + 2] = t + Wu;
+        idx[4 * i + 3] = t + Wu + 1u;
         wt[4 * i] = w * (1.0f - fx) * (1.0f - fy);
         wt[4 * i + 1] = w * fx * (1.0f - fy);
         wt[4 * i + 2] = w * (1.0f - fx) * fy;

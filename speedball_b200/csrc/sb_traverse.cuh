@@ -1141,7 +1141,8 @@ static __device__ float refine_t(const DevScene& S, uint32_t tri, uint32_t inst,
 }
 
 // sampleAtlas, gi_probes.js:1941-1974: 8-tap trilinear over the cage probes,
-// each tap a bilinear fetch of the previous RGBA16F atlas (exact weights).
+// each tap a bilinear fetch of the previous RGBA16F atlas (exact weights; the
+// 2x2 footprint stays inside the probe's tile, so no edge clamp applies).
 static __device__ float3 sample_atlas(const DevCascade& C, float3 P, float3 N) {
     float3 cell = mk(C.gridSize[0] / fmaxf(1.0f, float(C.res[0]) - 1.0f),
                      C.gridSize[1] / fmaxf(1.0f, float(C.res[1]) - 1.0f),
@@ -1154,11 +1155,15 @@ static __device__ float3 sample_atlas(const DevCascade& C, float3 P, float3 N) {
         base[a] = clampf(floorf(gf[a]), 0.0f, fmaxf(float(C.res[a]) - 2.0f, 0.0f));
         frac[a] = clampf(gf[a] - base[a], 0.0f, 1.0f);
     }
-    float2 ouv = oct_encode(normalize3(N));
+    // the bilinear footprint inside each cage probe's tile: tile-local coordinate
+    // 0.5 + uv * 6 in [0.5, 6.5], the same offset and weights for all 8 taps
+    const float2 ouv = oct_encode(normalize3(N));
+    const float xl = fmaf(ouv.x, 6.0f, 0.5f), yl = fmaf(ouv.y, 6.0f, 0.5f);
+    const float fx0 = floorf(xl), fy0 = floorf(yl), fx = xl - fx0, fy = yl - fy0;
+    const uint32_t Wu = C.atlasW, off = (uint32_t)fy0 * Wu + (uint32_t)fx0;
+    const float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
     float3 acc = mk(0.f, 0.f, 0.f);
     float wsum = 0.0f;
-    const float W = float(C.atlasW), H = float(C.atlasH);
-    const int Wi = (int)C.atlasW, Hi = (int)C.atlasH;
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         int dx = i & 1, dy = (i >> 1) & 1, dz = (i >> 2) & 1;
@@ -1167,20 +1172,10 @@ static __device__ float3 sample_atlas(const DevCascade& C, float3 P, float3 N) {
         float wy = dy ? frac[1] : 1.0f - frac[1];
         float wz = dz ? frac[2] : 1.0f - frac[2];
         float w = wx * wy * wz + 1e-4f;
-        float row = pz * float(C.res[1]) + py;
-        float ox = px * 8.0f + 1.0f + ouv.x * 6.0f;
-        float oy = row * 8.0f + 1.0f + ouv.y * 6.0f;
-        float x = (ox / W) * W - 0.5f, y = (oy / H) * H - 0.5f;
-        float fx0 = floorf(x), fy0 = floorf(y);
-        float fx = x - fx0, fy = y - fy0;
-        int x0 = (int)fx0, y0 = (int)fy0;
-        int xa = min(max(x0, 0), Wi - 1), xb = min(max(x0 + 1, 0), Wi - 1);
-        int ya = min(max(y0, 0), Hi - 1), yb = min(max(y0 + 1, 0), Hi - 1);
-        float4 t00 = half4_to_float4(__ldg(C.atlasPrev + (size_t)ya * Wi + xa));
-        float4 t10 = half4_to_float4(__ldg(C.atlasPrev + (size_t)ya * Wi + xb));
-        float4 t01 = half4_to_float4(__ldg(C.atlasPrev + (size_t)yb * Wi + xa));
-        float4 t11 = half4_to_float4(__ldg(C.atlasPrev + (size_t)yb * Wi + xb));
-        float w00 = (1.0f - fx) * (1.0f - fy), w10 = fx * (1.0f - fy), w01 = (1.0f - fx) * fy, w11 = fx * fy;
+        const uint32_t tile = ((uint32_t)pz * C.res[1] + (uint32_t)py) * 8u * Wu + (uint32_t)px * 8u;
+        const uint2* p = C.atlasPrev + tile + off;
+        float4 t00 = half4_to_float4(__ldg(p)), t10 = half4_to_float4(__ldg(p + 1));
+        float4 t01 = half4_to_float4(__ldg(p + Wu)), t11 = half4_to_float4(__ldg(p + Wu + 1));
         float3 s = mk(t00.x * w00 + t10.x * w10 + t01.x * w01 + t11.x * w11,
                       t00.y * w00 + t10.y * w10 + t01.y * w01 + t11.y * w11,
                       t00.z * w00 + t10.z * w10 + t01.z * w01 + t11.z * w11);
