@@ -291,6 +291,15 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
                      int32_t* triOut, int32_t* instOut);
 sb_status sb_occluded(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist,
                       uint32_t n, uint8_t* blockedOut);
+/* The same two queries on DEVICE arrays (3 floats per ray; t, tri, inst per
+ * ray; one byte per ray), enqueued on the context's stream with no copy and
+ * no synchronisation: the traversal reused by a GPU path tracer, as the
+ * reference's spectral kernel reuses traverseClosest / traverseAny
+ * (spectral_kernel.js:288, 451). Results equal sb_raycast / sb_occluded. */
+sb_status sb_raycast_device(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, float* tOut,
+                            int32_t* triOut, int32_t* instOut);
+sb_status sb_occluded_device(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist,
+                             uint32_t n, uint8_t* blockedOut);
 
 /* The FP32 probe rays of a solve of `cascade` over probes [probeOffset,
  * probeOffset + updatedCount) (mod the probe count) with the current

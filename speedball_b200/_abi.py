@@ -166,6 +166,8 @@ SIGNATURES = {
     "sb_gather_params_defaults": (None, [_P]),
     "sb_gather_irradiance": (C.c_int, [_P, _P, _P, _P, _P, C.c_uint32, _P]),
     "sb_gather_reflections": (C.c_int, [_P, _P, _P, _P, _P, _P, C.c_uint32, _P, _P]),
+    "sb_raycast_device": (C.c_int, [_P, _P, _P, C.c_uint32, _P, _P, _P]),
+    "sb_occluded_device": (C.c_int, [_P, _P, _P, _P, C.c_uint32, _P]),
     "sb_synchronize": (C.c_int, [_P]),
     "sb_upload_scene": (C.c_int, [_P, C.POINTER(sb_scene_view)]),
     "sb_upload_range": (C.c_int, [_P, _U32, _U32, _U32, _P]),

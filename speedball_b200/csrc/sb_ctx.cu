@@ -1696,6 +1696,38 @@ sb_status sb_raycast(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, 
     return sb_synchronize(ctx);
 }
 
+// The traversal queries on the caller's device arrays, enqueued on the
+// context's stream: a GPU path tracer reusing the walks (the reference's
+// spectral kernel calls traverseClosest / traverseAny, spectral_kernel.js:288,
+// 451).
+static sb_status device_query_ready(sb_ctx* ctx) {
+    if (!ctx->sceneLoaded || ctx->tlasPending) return fail(ctx, SB_ERR_NOT_READY, "scene / TLAS not ready");
+    cudaSetDevice(ctx->device);
+    sb_status s = pack_if_needed(ctx);
+    if (s != SB_OK) return s;
+    return flat_if_needed(ctx);
+}
+
+sb_status sb_raycast_device(sb_ctx* ctx, const float* ro, const float* rd, uint32_t n, float* tOut, int32_t* triOut,
+                            int32_t* instOut) {
+    if (!ctx || (n && (!ro || !rd || !tOut || !triOut || !instOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (n == 0) return ctx->sceneLoaded ? SB_OK : fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    sb_status s = device_query_ready(ctx);
+    if (s != SB_OK) return s;
+    CK(launch_raycast(dev_scene(ctx), ro, rd, n, tOut, triOut, instOut, ctx->dErr, ctx->stream));
+    return SB_OK;
+}
+
+sb_status sb_occluded_device(sb_ctx* ctx, const float* ro, const float* rd, const float* maxDist, uint32_t n,
+                             uint8_t* blockedOut) {
+    if (!ctx || (n && (!ro || !rd || !maxDist || !blockedOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (n == 0) return ctx->sceneLoaded ? SB_OK : fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    sb_status s = device_query_ready(ctx);
+    if (s != SB_OK) return s;
+    CK(launch_occluded(dev_scene(ctx), ro, rd, maxDist, n, blockedOut, ctx->dErr, ctx->stream));
+    return SB_OK;
+}
+
 sb_status sb_probe_rays(sb_ctx* ctx, uint32_t cascade, uint32_t probeOffset, uint32_t updatedCount, float* roOut,
                         float* rdOut) {
     if (!ctx || (updatedCount && (!roOut || !rdOut))) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");

@@ -333,3 +333,35 @@ def test_ranged_light_edit_reaches_the_emission_gates():
         assert bad.size == 0, (key, bad.size, bad[:8])
     assert not np.array_equal(ranged["vis"], plain["vis"])
     assert not np.array_equal(ranged["atlas"], plain["atlas"])
+
+
+def test_device_queries_equal_the_host_queries(room):
+    """sb_raycast_device / sb_occluded_device (device arrays, enqueue only: the
+    traversal reused by a GPU path tracer) give the host queries' results bit
+    for bit on the same rays."""
+    torch = pytest.importorskip("torch")
+    s, f = room
+    lib = f._lib
+    n = 100_000
+    ro, rd = _random_rays(n, 23)
+    md = np.random.default_rng(24).uniform(0.1, 12.0, n).astype(np.float32)
+    t = np.zeros(n, np.float32); tri = np.zeros(n, np.int32); inst = np.zeros(n, np.int32)
+    _abi.check(lib.sb_raycast(f.ctx, _abi.ptr(ro), _abi.ptr(rd), n, _abi.ptr(t), _abi.ptr(tri), _abi.ptr(inst)), f.ctx)
+    blocked = np.zeros(n, np.uint8)
+    _abi.check(lib.sb_occluded(f.ctx, _abi.ptr(ro), _abi.ptr(rd), _abi.ptr(md), n, _abi.ptr(blocked)), f.ctx)
+    dev = torch.device("cuda", 0)
+    dro, drd, dmd = (torch.from_numpy(x).to(dev) for x in (ro, rd, md))
+    dt = torch.zeros(n, dtype=torch.float32, device=dev)
+    dtri = torch.zeros(n, dtype=torch.int32, device=dev)
+    dinst = torch.zeros(n, dtype=torch.int32, device=dev)
+    dbl = torch.zeros(n, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    _abi.check(lib.sb_raycast_device(f.ctx, dro.data_ptr(), drd.data_ptr(), n, dt.data_ptr(), dtri.data_ptr(),
+                                     dinst.data_ptr()), f.ctx)
+    _abi.check(lib.sb_occluded_device(f.ctx, dro.data_ptr(), drd.data_ptr(), dmd.data_ptr(), n, dbl.data_ptr()),
+               f.ctx)
+    f.synchronize()
+    assert np.array_equal(dt.cpu().numpy().view(np.uint32), t.view(np.uint32))
+    assert np.array_equal(dtri.cpu().numpy(), tri) and np.array_equal(dinst.cpu().numpy(), inst)
+    assert np.array_equal(dbl.cpu().numpy(), blocked)
+    assert 0.05 < blocked.mean() < 0.95 and (tri >= 0).mean() > 0.9
