@@ -205,3 +205,25 @@ def lib_refuses_without_lobes(f) -> bool:
     buf = torch.zeros((64, 4), dtype=torch.float32, device=torch.device("cuda", 0))
     p = buf.data_ptr()
     return f._lib.sb_gather_reflections(f.ctx, _abi.C.byref(prm), p, p, p, p, 8, p, p) == _abi.SB_ERR_NOT_READY
+
+
+@pytest.mark.parametrize("tier", ["rough", "ultra"])
+def test_reflection_lobes_with_emitters(tier):
+    """giEmitter virtual rays enter the rough lobe (power-8 secondary weight)
+    and the glossy lobe (power 64) as well as the diffuse moments
+    (gi_probes.js:2262-2310, 2624-2638): the room with one sphere and two
+    point emitters, montecarlo ticks, every lobe against the oracle given the
+    GPU's emitter visibility history."""
+    s = synth.add_emitters(synth.room_spheres(0))
+    f = gu.make_field(s, reflectionQuality=tier)
+    try:
+        f.setJitterMode("montecarlo")
+        mirror = gu.OracleMirror(f)
+        assert mirror.emitters == (5, 3)
+        for k in range(3):
+            frame = f.tick(nowMs=100.0 + 16.0 * k)
+            f.synchronize()
+            r = gu.solve_parity(f, mirror, frame, f._params.to_array())
+            print(tier, k, {key: r[key] for key in r if "err" in key or "agreement" in key})
+    finally:
+        f.dispose()
