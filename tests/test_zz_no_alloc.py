@@ -80,3 +80,72 @@ def test_static_refit_matches_context_refit_on_consecutive_calls():
         deform_and_compare(7)   # a different range after the failed call
     finally:
         f.dispose()
+
+
+def _tiny_pool():
+    """Three triangles of three vertices each; a root over two leaves (pre-order,
+    left child at i + 1): node 0 interior, node 1 leaf of triangles 0-1, node 2
+    leaf of triangle 2. Bounds start as a stale unit box."""
+    rng = np.random.default_rng(5)
+    vert = np.zeros((9, 8), np.float32)
+    vert[:, 0:3] = rng.uniform(-2, 2, (9, 3))
+    tri = np.arange(9, dtype=np.uint32)
+    nodes = np.zeros((3, 8), np.uint32)
+    stale = np.array([-1, -1, -1, 1, 1, 1], np.float32).view(np.uint32)
+    for i in range(3):
+        nodes[i, 0:6] = stale
+    nodes[0, 6], nodes[0, 7] = 3, 0xFFFFFFFF
+    nodes[1, 6], nodes[1, 7] = 2, (2 << 24) | 0
+    nodes[2, 6], nodes[2, 7] = 3, (1 << 24) | 2
+    return nodes, tri, vert
+
+
+@pytest.mark.gpu
+def test_static_refit_edge_pools():
+    """The static path's own branches on tiny pools: an empty leaf keeps its
+    stale bounds exactly as the oracle's refitFlatBlasRange restatement does;
+    a leaf whose triangles lie past triCount, and a range holding a node no
+    parent reaches, fail with SB_ERR_LAYOUT_VIOLATION and leave the nodes
+    untouched."""
+    import torch
+    import orc
+
+    lib = _abi.load()
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def run(nodes, tri, vert, root, end):
+        nd = torch.from_numpy(nodes.reshape(-1).view(np.int32).copy()).to(dev)
+        td = torch.from_numpy(tri.view(np.int32).copy()).to(dev)
+        vd = torch.from_numpy(vert.reshape(-1).copy()).to(dev)
+        st, msg = _call(lib, nd.data_ptr(), nodes.shape[0], td.data_ptr(), tri.size // 3, vd.data_ptr(),
+                        vert.shape[0], root, end, stream)
+        torch.cuda.synchronize()
+        return st, msg, nd.cpu().numpy().view(np.uint32).reshape(-1, 8)
+
+    # an empty leaf (count 0): bit-equal to the oracle's refit of the same pool
+    nodes, tri, vert = _tiny_pool()
+    nodes[2, 7] = (0 << 24) | 2
+    st, msg, got = run(nodes, tri, vert, 0, 3)
+    want = nodes.copy()
+    assert orc.load().orc_refit_blas(orc._p(want), want.size, orc._p(tri), tri.size, orc._p(vert), vert.size, 0, 3) == 1
+    assert st == _abi.SB_OK, msg
+    assert np.array_equal(got, want)
+    assert np.array_equal(got[2, 0:6], nodes[2, 0:6])  # the empty leaf kept its stale box
+    assert not np.array_equal(got[1, 0:6], nodes[1, 0:6])
+
+    # a leaf whose triangles run past triCount
+    nodes, tri, vert = _tiny_pool()
+    nodes[2, 7] = (2 << 24) | 2  # triangles 2 and 3 of 3
+    st, msg, got = run(nodes, tri, vert, 0, 3)
+    assert st == _abi.SB_ERR_LAYOUT_VIOLATION, msg
+    assert np.array_equal(got, nodes)
+
+    # a node that no parent reaches: node 3 after the root's subtree, inside the range
+    nodes, tri, vert = _tiny_pool()
+    extra = nodes[2:3].copy()
+    extra[0, 6] = 4
+    nodes4 = np.concatenate([nodes, extra])
+    st, msg, got = run(nodes4, tri, vert, 0, 4)
+    assert st == _abi.SB_ERR_LAYOUT_VIOLATION, msg
+    assert np.array_equal(got, nodes4)
