@@ -1021,6 +1021,9 @@ static sb_status build_batch(const sb_solve_item* items, uint32_t count, BatchAr
     uint32_t blend = 0;
     for (uint32_t i = 0; i < count; ++i) {
         sb_ctx* c = items[i].ctx;
+        // emitters or reflection lobes set after a capture: the batched kernels cover neither
+        if (c->emitterCount || c->reflectTier)
+            return fail(lead, SB_ERR_UNSUPPORTED, "item %u: emitters / reflection lobes are solved by sb_solve only", i);
         const uint32_t ci = items[i].cascade;
         Cascade& K = c->casc[ci];
         const uint32_t cnt = items[i].updatedCount > K.probeTotal ? K.probeTotal : items[i].updatedCount;

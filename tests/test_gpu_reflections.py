@@ -227,3 +227,23 @@ def test_reflection_lobes_with_emitters(tier):
             print(tier, k, {key: r[key] for key in r if "err" in key or "agreement" in key})
     finally:
         f.dispose()
+
+
+def test_captured_frame_refuses_lobes_set_after_capture():
+    """A frame graph captured without lobes does not replay once a tier is set:
+    the batched kernels have no lobes, so the replay (and its re-capture) return
+    SB_ERR_UNSUPPORTED instead of leaving the lobes unwritten."""
+    s = synth.room_spheres(0)
+    f = gu.make_field(s)
+    try:
+        fr = f.beginTick()
+        _abi.check(f._lib.sb_graph_capture_frame(f.ctx, 0, fr["probeOffset"], fr["updatedCount"], None, None, 0, 0),
+                   f.ctx)
+        f.endTick(fr)
+        _abi.check(f._lib.sb_graph_launch(f.ctx), f.ctx)
+        f.synchronize()
+        _abi.check(f._lib.sb_set_reflection_quality(f.ctx, 1), f.ctx)
+        assert f._lib.sb_graph_launch(f.ctx) == _abi.SB_ERR_UNSUPPORTED
+        _abi.check(f._lib.sb_graph_destroy(f.ctx), f.ctx)
+    finally:
+        f.dispose()
