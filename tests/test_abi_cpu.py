@@ -153,3 +153,26 @@ def test_light_selection_and_scheduling():
     assert fld.probeUpdateIntervalTicks(4096, 1536) == pytest.approx(4096 / 1536)
     assert fld.hysteresisExponentForInterval(1000 / 120) == pytest.approx(0.5)
     assert fld.hysteresisExponentForInterval(100.0, False) == 1.0
+
+
+def test_reflection_quality_resolution_and_abi_without_device():
+    """resolveReflectionQuality (gi_probes.js:67-73): names in any case with
+    surrounding space, the legacy boolean when no name is given (True = ultra),
+    an unknown name rejected; the library refuses a tier above ultra and a null
+    context before touching a device."""
+    from speedball_b200.field import resolveReflectionQuality
+    assert resolveReflectionQuality(None) == "off"
+    assert resolveReflectionQuality(None, True) == "ultra"
+    assert resolveReflectionQuality(" High ", True) == "high"
+    assert resolveReflectionQuality("rough") == "rough"
+    with pytest.raises(ValueError):
+        resolveReflectionQuality("mirror")
+    lib = _abi.load()
+    assert lib.sb_set_reflection_quality(None, 1) == _abi.SB_ERR_INVALID_ARG
+    assert lib.sb_get_reflection_layout(None, 0, None) == _abi.SB_ERR_INVALID_ARG
+    prm = _abi.sb_gather_params()
+    lib.sb_gather_params_defaults(C.byref(prm))
+    assert prm.reflectionIntensity == 1.0 and prm.roughnessLimit == 1.0 and prm.cascades == 1
+    assert lib.sb_gather_reflections(None, C.byref(prm), None, None, None, None, 0, None, None) == \
+        _abi.SB_ERR_INVALID_ARG
+    assert lib.sb_raycast_device(None, None, None, 0, None, None, None) == _abi.SB_ERR_INVALID_ARG
