@@ -223,10 +223,13 @@ def run_ours(args, dist: Dist):
                    shadow_blas=st.shadowBlasNodeVisits, shadow_tri=st.shadowTriangleTests)
     # algorithmic bytes per launch of each stage. Per-unit figures: 32 B TLAS node, 64 B instance
     # record, 48 B pre-gathered triangle; per box test 32 B (a BLAS node, or half a 64 B child-pair
-    # node) or 10 B on the 8-wide closest-hit tree (80 B node / 8 boxes); 16 B hit record + 16 B
-    # visibility mask per ray; 32 B per shadow job (written by the primary stage, read by the shadow
-    # stage); per hit 80 B of triangle/instance rows, 40 B material, 256 B of bounce taps (8 taps x
-    # 4 texels x 8 B); 16 B ray record write; 3,776 B per probe for blend + upload.
+    # node) or 10 B on the 8-wide closest-hit tree (80 B node / 8 boxes); 16 B raw hit record per ray
+    # (written by the closest-hit stage, read by the emission stage); emission per ray 16 B visibility
+    # mask, per hit 16 B final hit record + 48 B instance rows + 48 B pre-gathered triangle + 48 B
+    # reference triangle (3 indices, 3 vertices) for the refined t, 32 B per shadow job (written by the
+    # emission stage, read by the shadow stage); per hit 80 B of triangle/instance rows, 40 B material,
+    # 256 B of bounce taps (8 taps x 4 texels x 8 B); 16 B ray record write; 3,776 B per probe for
+    # blend + upload.
     tun = _abi.sb_tuning()
     _abi.check(lib.sb_get_tuning(ctx, C.byref(tun)), ctx)
     closest_box = 10 if tun.bvhKind == 1 else 32
@@ -238,7 +241,8 @@ def run_ours(args, dist: Dist):
         "k_trace_primary": trav(counted["tlas"] - counted["shadow_tlas"], counted["inst"] - counted["shadow_inst"],
                                 counted["blas"] - counted["shadow_blas"], counted["tri"] - counted["shadow_tri"],
                                 closest_box)
-        + 32 * rays + 32 * jobs,
+        + 16 * rays,
+        "k_emit": 32 * rays + 160 * hits + 32 * jobs,
         "k_trace_shadow": trav(counted["shadow_tlas"], counted["shadow_inst"], counted["shadow_blas"],
                                counted["shadow_tri"]) + 32 * jobs,
         "k_shade": 48 * rays + 376 * hits,
@@ -265,8 +269,9 @@ def run_ours(args, dist: Dist):
         ck(rt.cudaEventSynchronize(e1))
         total_ms += ck(rt.cudaEventElapsedTime(e0, e1))
         s = _stats(lib, ctx)
-        for k, v in (("k_trace_primary", s.lastPrimaryMs), ("k_trace_shadow", s.lastShadowMs),
-                     ("k_shade", s.lastShadeMs), ("k_blend_upload", s.lastBlendMs)):
+        for k, v in (("k_trace_primary", s.lastPrimaryMs), ("k_emit", s.lastEmitMs),
+                     ("k_trace_shadow", s.lastShadowMs), ("k_shade", s.lastShadeMs),
+                     ("k_blend_upload", s.lastBlendMs)):
             stage_ms[k].append(v)
     launches = _stats(lib, ctx).kernelLaunches - launches0
     clk = clocks.stop()
@@ -322,9 +327,6 @@ def run_ours(args, dist: Dist):
             parts = ln.split()
             if len(parts) >= 2 and parts[0].startswith("k_") and parts[1].isdigit():
                 traffic[parts[0]] = int(parts[1])
-        # the primary stage is timed over the closest-hit kernel and the emission kernel
-        if "k_trace_primary" in traffic and "k_emit" in traffic:
-            traffic["k_trace_primary"] += traffic["k_emit"]
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
         "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -338,7 +340,8 @@ def run_ours(args, dist: Dist):
                      "traffic": traffic.get(dominant),
                      "algorithmic_bytes_per_launch": int(stage_bytes[dominant]),
                      "stage_ms": {k: round(v, 4) for k, v in stage_avg.items()},
-                     "stage_gbs": {k: round(stage_bytes[k] / (stage_avg[k] * 1e-3) / 1e9, 1) for k in stage_avg},
+                     "stage_gbs": {k: round(stage_bytes[k] / (stage_avg[k] * 1e-3) / 1e9, 1) for k in stage_avg
+                                   if stage_avg[k] > 0},
                      "update_algorithmic_bytes": int(trace_bytes),
                      "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650 GB/s"},
         "work": {k: int(v) for k, v in counted.items()},

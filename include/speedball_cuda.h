@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define SB_ABI_VERSION 2u
+#define SB_ABI_VERSION 3u
 
 /* Geometry of the reference's layouts (spectral_scene.js:35-55, gi_probes.js:53-56). */
 #define SB_NODE_STRIDE_U32 8u   /* bvhNodes: 6 f32 bounds + miss + payload        */
@@ -597,7 +597,8 @@ typedef struct sb_stats {
     float lastTraceMs;        /* the three trace stages (primary, shadow, shade)          */
     float lastBlendMs;        /* blend + upload kernel alone                              */
     uint64_t kernelLaunches;  /* kernels this library launched, process-wide              */
-    float lastPrimaryMs;      /* per stage, for solves that fit one shadow-job chunk      */
+    float lastPrimaryMs;      /* per stage, for solves that fit one shadow-job chunk: the
+                                 closest-hit stage (k_trace_primary)                     */
     float lastShadowMs;
     float lastShadeMs;
     /* the shadow-ray share of the visit counters above */
@@ -609,6 +610,7 @@ typedef struct sb_stats {
                                    reference's TLAS + BLAS walk does (bvhKind 0, or more
                                    than 256 instance slots moved since the last build)       */
     float lastSceneBvhBuildMs;  /* host time of the last scene-BVH build                     */
+    float lastEmitMs;           /* the emission stage (k_emit: hit frames, light gates, jobs) */
 } sb_stats;
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
 /* Rebuild the scene BVH over the current instance placements before the next

@@ -142,7 +142,7 @@ class sb_stats(C.Structure):
                 ("shadowInstanceVisits", C.c_uint64), ("shadowBlasNodeVisits", C.c_uint64),
                 ("shadowTriangleTests", C.c_uint64), ("lastForwardRecordMs", C.c_float),
                 ("lastBackwardMs", C.c_float), ("sceneBvhBuilds", C.c_uint64), ("sceneBvhActive", C.c_uint32),
-                ("lastSceneBvhBuildMs", C.c_float)]
+                ("lastSceneBvhBuildMs", C.c_float), ("lastEmitMs", C.c_float)]
 
 
 _P = C.c_void_p

@@ -111,7 +111,7 @@ struct sb_ctx {
     FlatScene flat;
     float4* jobs = nullptr;        // shadow-ray job queue (2 float4 per job)
     uint32_t jobCap = 0;
-    cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr;
+    cudaEvent_t ev0 = nullptr, evMid = nullptr, ev1 = nullptr, evA = nullptr, evB = nullptr, evC = nullptr;
     cudaEvent_t syncEv = nullptr;  // cross-context ordering of batched solves
     bool timed = false;
     bool lastWasGraph = false;     // ev0..ev1 bracket a graph launch (whole frame, no stage events)
@@ -468,6 +468,7 @@ sb_status sb_create(const sb_device_opts* opts, sb_ctx** out) {
         cudaEventCreate(&ctx->ev1);
         cudaEventCreate(&ctx->evA);
         cudaEventCreate(&ctx->evB);
+        cudaEventCreate(&ctx->evC);
         sb_params_defaults(&ctx->params);
         if (cudaDeviceSynchronize() != cudaSuccess) { st = SB_ERR_CUDA; break; }
     } while (0);
@@ -524,6 +525,7 @@ void sb_destroy(sb_ctx* ctx) {
     if (ctx->evMid) cudaEventDestroy(ctx->evMid);
     if (ctx->evA) cudaEventDestroy(ctx->evA);
     if (ctx->evB) cudaEventDestroy(ctx->evB);
+    if (ctx->evC) cudaEventDestroy(ctx->evC);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
     delete ctx;
@@ -974,7 +976,7 @@ sb_status sb_solve(sb_ctx* ctx, uint32_t ci, uint32_t probeOffset, uint32_t upda
         uint32_t n = updatedCount - s0 < chunk ? updatedCount - s0 : chunk;
         CK(launch_trace(S, D, P, ctx->dErr, ctx->countersOn ? ctx->dCounters : nullptr, ctx->dWork, ctx->tune,
                         ctx->stream, ctx->jobs, ctx->jobCap, s0, n, timing ? ctx->evA : nullptr,
-                        timing ? ctx->evB : nullptr));
+                        timing ? ctx->evB : nullptr, timing ? ctx->evC : nullptr));
     }
     if (ctx->emitterCount) CK(launch_emitter_vis(S, D, P, ctx->dErr, ctx->stream));
     if (timing) CK(cudaEventRecord(ctx->evMid, ctx->stream));
@@ -1111,7 +1113,8 @@ static sb_status enqueue_batch(const sb_solve_item* items, uint32_t count) {
     const bool timing = !lead->capturing;
     if (B.counters) CK(cudaMemsetAsync(lead->dCounters, 0, 128, lead->stream));
     if (timing) CK(cudaEventRecord(lead->ev0, lead->stream));
-    CK(launch_trace_batch(B, lead->tune, lead->stream, timing ? lead->evA : nullptr, timing ? lead->evB : nullptr));
+    CK(launch_trace_batch(B, lead->tune, lead->stream, timing ? lead->evA : nullptr, timing ? lead->evB : nullptr,
+                          timing ? lead->evC : nullptr));
     if (timing) CK(cudaEventRecord(lead->evMid, lead->stream));
     CK(launch_blend_upload_batch(B, lead->stream));
     if (timing) {
@@ -2136,7 +2139,8 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
         if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evMid) == cudaSuccess) out->lastTraceMs = ms;
         if (cudaEventElapsedTime(&ms, ctx->evMid, ctx->ev1) == cudaSuccess) out->lastBlendMs = ms;
         if (ctx->singleChunk) {
-            if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evA) == cudaSuccess) out->lastPrimaryMs = ms;
+            if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->evC) == cudaSuccess) out->lastPrimaryMs = ms;
+            if (cudaEventElapsedTime(&ms, ctx->evC, ctx->evA) == cudaSuccess) out->lastEmitMs = ms;
             if (cudaEventElapsedTime(&ms, ctx->evA, ctx->evB) == cudaSuccess) out->lastShadowMs = ms;
             if (cudaEventElapsedTime(&ms, ctx->evB, ctx->evMid) == cudaSuccess) out->lastShadeMs = ms;
         }

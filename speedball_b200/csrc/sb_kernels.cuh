@@ -53,7 +53,8 @@ struct SceneBuffers {
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
                          unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
                          float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
-                         cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
+                         cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr,
+                         cudaEvent_t afterClosest = nullptr);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_glossy(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t slotCount,
@@ -62,7 +63,8 @@ cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams
 // Batched stages (every item of B in one launch per stage). B.work must hold
 // 3 words; every item's W.jobs / W.jobCap / W.work are the batch's shared ones.
 cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cudaStream_t st,
-                               cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr);
+                               cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr,
+                         cudaEvent_t afterClosest = nullptr);
 cudaError_t launch_blend_upload_batch(const BatchArgs& B, cudaStream_t st);
 uint32_t blend_blocks(uint32_t updatedCount);  // CTAs of the blend for one solve
 // The batched kernels (stage 0 primary, 1 emit, 2 shadow, 3 shade; blend):

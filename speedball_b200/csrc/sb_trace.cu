@@ -423,7 +423,7 @@ static int persistent_grid(const void* kernel, int block, size_t smem, const Tra
 cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t* err,
                          unsigned long long* counters, uint32_t* work, const TraceTuning& tune, cudaStream_t st,
                          float4* jobs, uint32_t jobCap, uint32_t slotBegin, uint32_t slotCount,
-                         cudaEvent_t afterPrimary, cudaEvent_t afterShadow) {
+                         cudaEvent_t afterPrimary, cudaEvent_t afterShadow, cudaEvent_t afterClosest) {
     if (slotCount == 0) return cudaSuccess;
     WaveCtx W;
     W.S = S;
@@ -458,6 +458,7 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     k_trace_primary<<<persistent_grid((const void*)k_trace_primary, block, smemPrimary, tune, rays), block, smemPrimary,
                       st>>>(W);
     note_launch();
+    if (afterClosest) cudaEventRecord(afterClosest, st);
     k_emit<<<(rays + 127) / 128, 128, 0, st>>>(W);
     note_launch();
     if (afterPrimary) cudaEventRecord(afterPrimary, st);
@@ -629,7 +630,7 @@ const void* trace_batch_kernel(int stage) {
 }
 
 cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cudaStream_t st,
-                               cudaEvent_t afterPrimary, cudaEvent_t afterShadow) {
+                               cudaEvent_t afterPrimary, cudaEvent_t afterShadow, cudaEvent_t afterClosest) {
     if (B.n == 0 || B.totalRays == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(B.work, 0, 3 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
@@ -638,6 +639,7 @@ cudaError_t launch_trace_batch(const BatchArgs& B, const TraceTuning& tune, cuda
     k_trace_primary_batch<<<persistent_grid((const void*)k_trace_primary_batch, block, 0, tune, rays), block, 0,
                             st>>>(B);
     note_launch();
+    if (afterClosest) cudaEventRecord(afterClosest, st);
     k_emit_batch<<<(rays + 127) / 128, 128, 0, st>>>(B);
     note_launch();
     if (afterPrimary) cudaEventRecord(afterPrimary, st);

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
     assert set(names) <= set(_abi.SIGNATURES), set(names) - set(_abi.SIGNATURES)
-    assert lib.sb_abi_version() == 2
+    assert lib.sb_abi_version() == 3
 
 
 def test_params_defaults_match_reference():
