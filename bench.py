@@ -1131,6 +1131,35 @@ def run_large(args, dist: Dist):
         records[kind] = (hits(0), hits(1))
         results[kind] = {"ms_per_step": round(ms, 3), "mrays_s": round(dist.world * rays / (ms * 1e-3) / 1e6, 2),
                          "warmup_s": round(warm_s, 2)}
+    # a structural rebuild of the bvhKind 1 trees: blocking (inside the next frame), then in
+    # background mode, where frames go on with the two-level walk until the tree is installed
+    t = _abi.sb_tuning()
+    _abi.check(lib.sb_get_tuning(ctx, C.byref(t)), ctx)
+    t.bvhKind = 1
+    _abi.check(lib.sb_set_tuning(ctx, C.byref(t)), ctx)  # a layout change: the trees are rebuilt
+    tb = time.perf_counter()
+    frame(0)
+    f.synchronize()
+    blocking_frame_s = time.perf_counter() - tb
+    blocking_build_ms = _stats(lib, ctx).lastSceneBvhBuildMs
+    _abi.check(lib.sb_set_scene_bvh_build_mode(ctx, 1), ctx)
+    _abi.check(lib.sb_rebuild_scene_bvh(ctx), ctx)
+    during, n, tb = [], 0, time.perf_counter()
+    while True:
+        ck(rt.cudaEventRecord(e0, stream))
+        frame(n % (W + K))
+        ck(rt.cudaEventRecord(e1, stream))
+        ck(rt.cudaEventSynchronize(e1))
+        n += 1
+        s = _stats(lib, ctx)
+        if s.sceneBvhActive or time.perf_counter() - tb > 300.0:
+            break
+        during.append(ck(rt.cudaEventElapsedTime(e0, e1)))
+    background = {"frames_before_install": len(during), "installed": bool(s.sceneBvhActive),
+                  "ms_per_frame_while_building": round(float(np.mean(during)), 3) if during else None,
+                  "max_frame_ms_while_building": round(float(np.max(during)), 3) if during else None,
+                  "build_s": round(s.lastSceneBvhBuildMs / 1e3, 2), "wall_s": round(time.perf_counter() - tb, 2)}
+    _abi.check(lib.sb_set_scene_bvh_build_mode(ctx, 0), ctx)
     clk = clocks.stop()
 
     def agree(a, b):
@@ -1157,6 +1186,8 @@ def run_large(args, dist: Dist):
                    "l2": "flushed (256 MiB write) before every timed step"},
         "layouts": {f"bvhKind{k}": v for k, v in results.items()}, "fastest_layout": f"bvhKind{best}",
         "hit_agreement": cmp, "setup_s": round(setup_s, 2),
+        "scene_bvh_rebuild": {"blocking_frame_s": round(blocking_frame_s, 2),
+                              "blocking_build_s": round(blocking_build_ms / 1e3, 2), "background": background},
         "gpu_launches": int(launches),
         "clocks": clk,
     }

@@ -611,6 +611,7 @@ typedef struct sb_stats {
                                    than 256 instance slots moved since the last build)       */
     float lastSceneBvhBuildMs;  /* host time of the last scene-BVH build                     */
     float lastEmitMs;           /* the emission stage (k_emit: hit frames, light gates, jobs) */
+    uint32_t sceneBvhBuilding;  /* 1 while a background scene-BVH build runs                 */
 } sb_stats;
 sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
 /* Rebuild the scene BVH over the current instance placements before the next
@@ -619,6 +620,21 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out);
  * moved slots are walked through their own BLAS, beyond that the reference's
  * two-level walk, refit on the GPU every frame, answers until a rebuild. */
 sb_status sb_rebuild_scene_bvh(sb_ctx* ctx);
+/* How a scene-BVH rebuild runs (a structural change, or sb_rebuild_scene_bvh).
+ * BLOCKING (default): the next trace reads the scene back, builds the trees on
+ * the host and uploads them before it runs. BACKGROUND: the next trace reads
+ * the scene back and starts the build on a host thread; traces meanwhile use
+ * the reference's two-level walk (GPU-refit TLAS + BLASes), and the first trace
+ * after the build finished installs the tree, marking the slots that moved or
+ * were refit since it read the scene. A build overtaken by another structural
+ * change is dropped and the next trace starts a new one. The scene-BVH walks
+ * and the two-level walk agree on hit IDs up to near-ties (the parity bar), so
+ * a solve's results do not depend on which one answered beyond that. */
+enum { SB_SCENE_BVH_BLOCKING = 0, SB_SCENE_BVH_BACKGROUND = 1 };
+sb_status sb_set_scene_bvh_build_mode(sb_ctx* ctx, uint32_t mode);
+/* Waits for a running background build and installs it (drops it when the
+ * scene changed structurally since it started). No-op when none runs. */
+sb_status sb_finish_scene_bvh(sb_ctx* ctx);
 /* Counting costs a few percent; off by default. */
 sb_status sb_enable_counters(sb_ctx* ctx, int32_t on);
 

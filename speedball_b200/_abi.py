@@ -142,7 +142,8 @@ class sb_stats(C.Structure):
                 ("shadowInstanceVisits", C.c_uint64), ("shadowBlasNodeVisits", C.c_uint64),
                 ("shadowTriangleTests", C.c_uint64), ("lastForwardRecordMs", C.c_float),
                 ("lastBackwardMs", C.c_float), ("sceneBvhBuilds", C.c_uint64), ("sceneBvhActive", C.c_uint32),
-                ("lastSceneBvhBuildMs", C.c_float), ("lastEmitMs", C.c_float)]
+                ("lastSceneBvhBuildMs", C.c_float), ("lastEmitMs", C.c_float),
+                ("sceneBvhBuilding", C.c_uint32)]
 
 
 _P = C.c_void_p
@@ -160,6 +161,8 @@ SIGNATURES = {
     "sb_set_reflection_quality": (C.c_int, [_P, _U32]),
     "sb_get_reflection_layout": (C.c_int, [_P, _U32, C.POINTER(sb_reflection_layout)]),
     "sb_rebuild_scene_bvh": (C.c_int, [_P]),
+    "sb_set_scene_bvh_build_mode": (C.c_int, [_P, _U32]),
+    "sb_finish_scene_bvh": (C.c_int, [_P]),
     "sb_build_blas_device": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_build_blas_gpu": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, _P]),
     "sb_probe_rays": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),

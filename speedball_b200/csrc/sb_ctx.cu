@@ -636,7 +636,7 @@ sb_status sb_upload_scene(sb_ctx* ctx, const sb_scene_view* v) {
     ctx->tlasPending = v->tlasNodeCount == 0;
     ctx->tlasOnDevice = false;
     ctx->sceneLoaded = true;
-    ctx->flat.dirty = true;
+    ctx->flat.invalidate();
     ++ctx->epoch;
     ++ctx->structGen;
     if (ctx->instancesSet && ctx->I.count != v->instCount) ctx->instancesSet = false;
@@ -692,7 +692,7 @@ sb_status sb_upload_range(sb_ctx* ctx, uint32_t which, uint32_t start, uint32_t 
     if (buf <= SB_BUF_MATERIALS && !(buf == SB_BUF_MATERIALS && shading_only(B, start, count))) {
         ++ctx->structGen;
         ctx->needPack = true;
-        ctx->flat.dirty = true;
+        ctx->flat.invalidate();
     }
     if (buf == SB_BUF_LIGHTS && ctx->clustered) ctx->lightGridDirty = true;
     if (buf == SB_BUF_LIGHTS) ctx->lightGatesDirty = true;
@@ -2032,7 +2032,7 @@ sb_status sb_set_instances(sb_ctx* ctx, uint32_t count, const double* world16, c
     CK(cudaMemcpyAsync(I.blasRoot, blasRoot, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(I.blasEnd, blasEnd, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
     ctx->instancesSet = true;
-    ctx->flat.dirty = true;
+    ctx->flat.invalidate();
     if (!ctx->tlasPending) {
         // the uploaded TLAS stays; derive the slot maps from it on the next pack
         ctx->needPack = true;
@@ -2055,7 +2055,7 @@ sb_status sb_build_tlas(sb_ctx* ctx) {
     if (s != SB_OK) return s;
     CK(launch_tlas_build(ctx->B, ctx->I, ctx->dErr, ctx->stream));
     CK(launch_tlas_pairs(ctx->B, ctx->stream));
-    ctx->flat.dirty = true;
+    ctx->flat.invalidate();
     ctx->tlasPending = false;
     ctx->tlasOnDevice = true;
     return SB_OK;
@@ -2104,7 +2104,22 @@ sb_status sb_enable_counters(sb_ctx* ctx, int32_t on) {
 
 sb_status sb_rebuild_scene_bvh(sb_ctx* ctx) {
     if (!ctx) return SB_ERR_INVALID_ARG;
-    ctx->flat.dirty = true;
+    ctx->flat.invalidate();
+    return SB_OK;
+}
+
+sb_status sb_set_scene_bvh_build_mode(sb_ctx* ctx, uint32_t mode) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    if (mode > SB_SCENE_BVH_BACKGROUND) return fail(ctx, SB_ERR_INVALID_ARG, "scene BVH build mode %u", mode);
+    ctx->flat.background = mode == SB_SCENE_BVH_BACKGROUND;
+    return SB_OK;
+}
+
+sb_status sb_finish_scene_bvh(sb_ctx* ctx) {
+    if (!ctx) return SB_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    std::string why;
+    CK(ctx->flat.finish(ctx->stream, why));
     return SB_OK;
 }
 
@@ -2113,6 +2128,7 @@ sb_status sb_get_stats(sb_ctx* ctx, sb_stats* out) {
     std::memset(out, 0, sizeof *out);
     out->sceneBvhBuilds = ctx->flat.builds;
     out->sceneBvhActive = ctx->flat.enabled && ctx->flat.ready && !ctx->flat.overflowed ? 1u : 0u;
+    out->sceneBvhBuilding = ctx->flat.building() ? 1u : 0u;
     out->lastSceneBvhBuildMs = ctx->flat.lastBuildMs;
     cudaSetDevice(ctx->device);
     CK(cudaStreamSynchronize(ctx->stream));
@@ -2172,7 +2188,7 @@ sb_status sb_set_tuning(sb_ctx* ctx, const sb_tuning* t) {
     if (t->smemWideNodes > 512)
         return fail(ctx, SB_ERR_INVALID_ARG, "smemWideNodes %u > 512 (80 bytes each)", t->smemWideNodes);
     if (t->sortKey > 3) return fail(ctx, SB_ERR_INVALID_ARG, "sortKey %u: 0, 1, 2 or 3", t->sortKey);
-    if (t->bvhKind != ctx->bvhKind) ctx->flat.dirty = true;
+    if (t->bvhKind != ctx->bvhKind) ctx->flat.invalidate();
     ctx->tune.smemWideNodes = t->smemWideNodes;
     ctx->bvhKind = t->bvhKind;
     ++ctx->structGen;

@@ -108,6 +108,9 @@ def selectGiLightRecords(records: np.ndarray, importanceRanked: bool, gridMin=No
     return arr, len(selected), emitter_count
 
 
+# sb_set_scene_bvh_build_mode
+SCENE_BVH_BUILD_MODES = {"blocking": 0, "background": 1}
+
 class ProbeField:
     """createProbeField (gi_probes.js:945) over one scene and one GPU."""
 
@@ -115,11 +118,13 @@ class ProbeField:
                  rays=RAYS_PER_PROBE_DEFAULT, cascades=2, clusteredLighting=False, volumes=None, device=0,
                  recordHits=False, onRebuilt: Callable | None = None, variant: str | None = None,
                  blasBuilder: str = "host", reflectionQuality: str | None = None, roughReflections=False,
-                 reflectionSkyFallback=False):
+                 reflectionSkyFallback=False, sceneBvhBuild: str = "blocking"):
         self._lib = _abi.load(variant)
         self._reflection = resolveReflectionQuality(reflectionQuality, roughReflections)
         if blasBuilder not in ("host", "gpu"):
             raise ValueError("blasBuilder: 'host' or 'gpu'")
+        if sceneBvhBuild not in SCENE_BVH_BUILD_MODES:
+            raise ValueError("sceneBvhBuild: 'blocking' or 'background'")
         self._blasBuilder = blasBuilder
         self._scene = scene
         self._intensity = float(intensity)
@@ -169,6 +174,7 @@ class ProbeField:
         self.stats = {"solves": 0, "refits": 0, "transformUpdates": 0, "rebuilds": 0}
         # structural: the reflection buffers of every cascade follow the tier
         self._ck(self._lib.sb_set_reflection_quality(h, _abi.REFLECT_TIERS[self._reflection]))
+        self._ck(self._lib.sb_set_scene_bvh_build_mode(h, SCENE_BVH_BUILD_MODES[sceneBvhBuild]))
         self._rebuild()
 
     # ------------------------------------------------------------- plumbing
@@ -632,8 +638,28 @@ class ProbeField:
         st = _abi.sb_stats()
         self._ck(self._lib.sb_get_stats(self._ctx, C.byref(st)))
         d = dict(self.stats)
-        d.update(probeTotal=self._probeTotal, rays=self._rays, lastSolveMs=st.lastSolveMs)
+        d.update(probeTotal=self._probeTotal, rays=self._rays, lastSolveMs=st.lastSolveMs,
+                 sceneBvhActive=bool(st.sceneBvhActive), sceneBvhBuilding=bool(st.sceneBvhBuilding),
+                 sceneBvhBuilds=int(st.sceneBvhBuilds))
         return d
+
+    # ----------------------------------------------------------- scene BVH
+    def rebuildSceneBvh(self):
+        """Rebuild the scene BVH over the current placements (the reference's
+        idle-gated rebuild, gi_probes.js:3269-3455); never needed for correctness."""
+        self._ck(self._lib.sb_rebuild_scene_bvh(self._ctx))
+
+    def setSceneBvhBuild(self, mode: str):
+        """'blocking': a rebuild completes inside the next tick. 'background': the
+        next tick starts it on a host thread and ticks use the two-level walk
+        until a later tick installs it."""
+        if mode not in SCENE_BVH_BUILD_MODES:
+            raise ValueError("sceneBvhBuild: 'blocking' or 'background'")
+        self._ck(self._lib.sb_set_scene_bvh_build_mode(self._ctx, SCENE_BVH_BUILD_MODES[mode]))
+
+    def finishSceneBvh(self):
+        """Wait for a background scene-BVH build and install it."""
+        self._ck(self._lib.sb_finish_scene_bvh(self._ctx))
 
     # ------------------------------------------------------------- read-back
     def synchronize(self):
