@@ -13,7 +13,6 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
-#include <functional>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -459,14 +458,13 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     constexpr float C_NODE = 1.0f, C_ITEM = SB_WIDE_ITEM_COST;
     std::vector<std::array<float, 9>> cost(nv);
     std::vector<std::array<uint8_t, 9>> how(nv), splitK(nv);  // how: 0 reuse i-1, 1 leaf, 2 interior, 3 split
-    for (size_t vi = nv; vi-- > 0;) {
-        const uint32_t v = (uint32_t)vi;
+    auto dp = [&](uint32_t v) {
         const float A = B.N.box[v].area();
         if (B.N.count[v]) {
             sFirst[v] = B.N.first[v];
             sCount[v] = B.N.count[v];
             for (int i = 1; i <= 8; ++i) { cost[v][i] = A * C_ITEM * (float)sCount[v]; how[v][i] = 1; }
-            continue;
+            return;
         }
         const uint32_t L = B.N.left[v], R = B.N.right[v];
         sFirst[v] = std::min(sFirst[L], sFirst[R]);
@@ -487,68 +485,119 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
             if (D[i] < cost[v][i - 1]) { cost[v][i] = D[i]; how[v][i] = 3; }
             else { cost[v][i] = cost[v][i - 1]; how[v][i] = 0; }
         }
+    };
+    // bottom-up by depth: the nodes of one depth depend only on deeper ones, so
+    // each depth runs in parallel (children are numbered after their parents)
+    {
+        std::vector<uint32_t> dep(nv, 0);
+        uint32_t maxDep = 0;
+        for (size_t v = 0; v < nv; ++v)
+            if (!B.N.count[v]) {
+                dep[B.N.left[v]] = dep[B.N.right[v]] = dep[v] + 1;
+                maxDep = std::max(maxDep, dep[v] + 1);
+            }
+        std::vector<uint32_t> at(maxDep + 2, 0), byDep(nv);
+        for (size_t v = 0; v < nv; ++v) ++at[dep[v] + 1];
+        for (uint32_t d = 0; d <= maxDep; ++d) at[d + 1] += at[d];
+        {
+            std::vector<uint32_t> fill(at.begin(), at.end() - 1);
+            for (size_t v = 0; v < nv; ++v) byDep[fill[dep[v]]++] = (uint32_t)v;
+        }
+        const unsigned hwd = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+        for (uint32_t d = maxDep + 1; d-- > 0;) {
+            const uint32_t lo = at[d], hi = at[d + 1];
+            if (hi - lo < 16384 || hwd == 1) {
+                for (uint32_t k = lo; k < hi; ++k) dp(byDep[k]);
+                continue;
+            }
+            std::atomic<uint32_t> next{lo};
+            auto run = [&] {
+                for (uint32_t k; (k = next.fetch_add(1024)) < hi;)
+                    for (uint32_t j = k; j < std::min(hi, k + 1024); ++j) dp(byDep[j]);
+            };
+            std::vector<std::thread> ts;
+            for (unsigned t = 1; t < hwd; ++t) ts.emplace_back(run);
+            run();
+            for (auto& t : ts) t.join();
+        }
     }
-    // the slots covering v's subtree with budget i
-    std::function<void(uint32_t, int, std::vector<uint32_t>&)> gather = [&](uint32_t v, int i,
-                                                                             std::vector<uint32_t>& kids) {
-        while (i > 1 && how[v][i] == 0) --i;
-        if (i == 1 || B.N.count[v]) { kids.push_back(v); return; }
-        const int k = splitK[v][i];
-        gather(B.N.left[v], k, kids);
-        gather(B.N.right[v], i - k, kids);
+    // the slots covering v's subtree with budget i, left subtree first
+    auto gather = [&](uint32_t v0, int i0, uint32_t* kids, int& nk) {
+        struct Entry { uint32_t v; int i; };
+        Entry st[16];
+        int sp = 0;
+        st[sp++] = {v0, i0};
+        while (sp) {
+            const Entry e = st[--sp];
+            const uint32_t v = e.v;
+            int i = e.i;
+            while (i > 1 && how[v][i] == 0) --i;
+            if (i == 1 || B.N.count[v]) {
+                kids[nk++] = v;
+                continue;
+            }
+            const int k = splitK[v][i];
+            st[sp++] = {B.N.right[v], i - k};
+            st[sp++] = {B.N.left[v], k};
+        }
     };
     // a slot is a leaf when its node is a binary leaf or the collapse chose one
     auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0 || how[v][1] == 1; };
+#else
+    auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0; };
+    const std::vector<uint32_t>& sFirst = B.N.first;
+    const std::vector<uint32_t>& sCount = B.N.count;
 #endif
 
-    struct Task { uint32_t v, w, depth; };
-    std::vector<Task> queue{{0, 0, 0}};
-    out.nodes.assign(WIDE_WORDS, 0u);
-    uint32_t maxDepth = 0;
-    std::vector<uint32_t> kids;
-    kids.reserve(8);
-    for (size_t qi = 0; qi < queue.size(); ++qi) {
-        const Task t = queue[qi];
-        maxDepth = std::max(maxDepth, t.depth);
-        kids.clear();
+    // One wide node formed from binary node v: its child set, slot assignment,
+    // quantised boxes and slot metadata (all words but the child and item
+    // bases), its interior children and its leaf slots in slot order.
+    struct Formed {
+        uint32_t words[WIDE_WORDS];
+        uint32_t interior[8], leaf[8];
+        int nInterior, nLeaf;
+    };
+    auto form = [&](uint32_t tv, Formed& F) {
+        uint32_t kids[8];
+        int nk = 0;
 #if SB_WIDE_COLLAPSE_SAH
-        if (is_leaf_slot(t.v)) kids.push_back(t.v);  // a small root is one leaf slot
+        if (is_leaf_slot(tv)) kids[nk++] = tv;  // a small root is one leaf slot
         else {
-            const int k = splitK[t.v][8];
-            gather(B.N.left[t.v], k, kids);
-            gather(B.N.right[t.v], 8 - k, kids);
+            const int k = splitK[tv][8];
+            gather(B.N.left[tv], k, kids, nk);
+            gather(B.N.right[tv], 8 - k, kids, nk);
         }
 #else
         // children: open the largest interior child until eight (a leaf root is its own child)
-        if (B.N.count[t.v]) kids.push_back(t.v);
-        else { kids.push_back(B.N.left[t.v]); kids.push_back(B.N.right[t.v]); }
-        while (kids.size() < 8) {
+        if (B.N.count[tv]) kids[nk++] = tv;
+        else {
+            kids[nk++] = B.N.left[tv];
+            kids[nk++] = B.N.right[tv];
+        }
+        while (nk < 8) {
             int best = -1;
             float bestArea = -1.0f;
-            for (size_t k = 0; k < kids.size(); ++k)
+            for (int k = 0; k < nk; ++k)
                 if (B.N.count[kids[k]] == 0 && B.N.box[kids[k]].area() > bestArea) {
                     bestArea = B.N.box[kids[k]].area();
-                    best = (int)k;
+                    best = k;
                 }
             if (best < 0) break;
-            uint32_t v = kids[best];
+            const uint32_t v = kids[best];
             kids[best] = B.N.left[v];
-            kids.push_back(B.N.right[v]);
+            kids[nk++] = B.N.right[v];
         }
-        auto is_leaf_slot = [&](uint32_t v) { return B.N.count[v] != 0; };
-        const std::vector<uint32_t>& sFirst = B.N.first;
-        const std::vector<uint32_t>& sCount = B.N.count;
 #endif
         // slots by octant: slot bit a set = the child lies toward +a of the node centre
         Box nb;
-        for (uint32_t k : kids) nb.grow(B.N.box[k]);
+        for (int k = 0; k < nk; ++k) nb.grow(B.N.box[kids[k]]);
         float ctr[3];
         for (int a = 0; a < 3; ++a) ctr[a] = 0.5f * (nb.lo[a] + nb.hi[a]);
         // (cost, kid, slot) by increasing cost, ties in generation order
         struct Cand { float cost; int kid, slot; };
         Cand cands[64];
         int nc = 0;
-        for (size_t k = 0; k < kids.size(); ++k) {
+        for (int k = 0; k < nk; ++k) {
             const Box& b = B.N.box[kids[k]];
             for (int s = 0; s < 8; ++s) {
                 float c = 0.0f;
@@ -556,7 +605,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                     float d = 0.5f * (b.lo[a] + b.hi[a]) - ctr[a];
                     c += (s >> a & 1) ? -d : d;
                 }
-                cands[nc++] = {c, (int)k, s};
+                cands[nc++] = {c, k, s};
             }
         }
         for (int i = 1; i < nc; ++i) {  // stable insertion sort (at most 64)
@@ -574,19 +623,17 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                 kidSlot[c.kid] = c.slot;
             }
         }
-        // header, children and items
-        uint32_t* w = out.nodes.data() + (size_t)t.w * WIDE_WORDS;
+        uint32_t* w = F.words;
+        std::memset(w, 0, sizeof F.words);
         int ex[3];
         for (int a = 0; a < 3; ++a) ex[a] = axis_exponent(nb.lo[a], nb.hi[a]);
         std::memcpy(w + 0, &nb.lo[0], 4);
         std::memcpy(w + 1, &nb.lo[1], 4);
         std::memcpy(w + 2, &nb.lo[2], 4);
-        uint32_t imask = 0;
-        const uint32_t childBase = (uint32_t)(out.nodes.size() / WIDE_WORDS);
-        const uint32_t itemBase = (uint32_t)(out.items.size() / 2);
-        uint32_t itemOff = 0;
+        uint32_t imask = 0, itemOff = 0;
         uint8_t meta[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         uint8_t q[6][8];
+        F.nInterior = F.nLeaf = 0;
         for (int s = 0; s < 8; ++s) {
             for (int a = 0; a < 3; ++a) { q[a][s] = 255; q[3 + a][s] = 0; }  // empty slots
             if (slotKid[s] < 0) continue;
@@ -602,7 +649,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
             if (!is_leaf_slot(v)) {
                 imask |= 1u << s;
                 meta[s] = (uint8_t)((1u << 5) | (24u + s));
-                queue.push_back({v, 0, t.depth + 1});  // node index assigned below, in slot order
+                F.interior[F.nInterior++] = v;
             } else {
                 const uint32_t cnt = sCount[v];
                 // a leaf merged from an interior node: its items in slot order too (its
@@ -611,27 +658,67 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                     std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + cnt,
                                      [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
                 meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
-                for (uint32_t k = 0; k < cnt; ++k) {
-                    out.items.push_back(itemTri[B.order[sFirst[v] + k]]);
-                    out.items.push_back(itemSlot[B.order[sFirst[v] + k]]);
-                }
+                F.leaf[F.nLeaf++] = v;
                 itemOff += cnt;
             }
         }
-        // interior children get consecutive node indices in slot order
-        uint32_t next = childBase;
-        for (size_t k = queue.size() - __builtin_popcount(imask); k < queue.size(); ++k) queue[k].w = next++;
-        out.nodes.resize((size_t)next * WIDE_WORDS, 0u);
-        w = out.nodes.data() + (size_t)t.w * WIDE_WORDS;
         w[3] = (uint32_t)ex[0] | (uint32_t)ex[1] << 8 | (uint32_t)ex[2] << 16 | imask << 24;
-        w[4] = childBase;
-        w[5] = itemBase;
         w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | (uint32_t)meta[3] << 24;
         w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | (uint32_t)meta[7] << 24;
         for (int r = 0; r < 6; ++r) {
             w[8 + 2 * r] = q[r][0] | q[r][1] << 8 | q[r][2] << 16 | (uint32_t)q[r][3] << 24;
             w[9 + 2 * r] = q[r][4] | q[r][5] << 8 | q[r][6] << 16 | (uint32_t)q[r][7] << 24;
         }
+    };
+
+    // Breadth first, one level at a time: the level's nodes are formed in
+    // parallel (forming reads the collapse tables at random, which is memory
+    // latency), then numbered in queue order. Each node's interior children take
+    // the next node indices and its leaf items the next item positions, so the
+    // layout is the one a sequential breadth-first pass gives.
+    out.nodes.assign(WIDE_WORDS, 0u);
+    std::vector<uint32_t> level{0}, levelW{0};  // binary node and wide index per node of the level
+    std::vector<Formed> formed;
+    const unsigned hw = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    uint32_t maxDepth = 0;
+    for (uint32_t depth = 0; !level.empty(); ++depth) {
+        maxDepth = depth;
+        formed.resize(level.size());
+        const size_t m = level.size();
+        const unsigned nth = m >= 4096 ? hw : 1u;
+        std::atomic<size_t> next{0};
+        auto run = [&] {
+            for (size_t i; (i = next.fetch_add(256)) < m;)
+                for (size_t k = i; k < std::min(m, i + 256); ++k) form(level[k], formed[k]);
+        };
+        std::vector<std::thread> ts;
+        for (unsigned t = 1; t < nth; ++t) ts.emplace_back(run);
+        run();
+        for (auto& t : ts) t.join();
+        std::vector<uint32_t> nextLevel, nextW;
+        for (size_t i = 0; i < m; ++i) {
+            const Formed& F = formed[i];
+            const uint32_t childBase = (uint32_t)(out.nodes.size() / WIDE_WORDS);
+            const uint32_t itemBase = (uint32_t)(out.items.size() / 2);
+            for (int k = 0; k < F.nLeaf; ++k) {
+                const uint32_t v = F.leaf[k];
+                for (uint32_t j = 0; j < sCount[v]; ++j) {
+                    out.items.push_back(itemTri[B.order[sFirst[v] + j]]);
+                    out.items.push_back(itemSlot[B.order[sFirst[v] + j]]);
+                }
+            }
+            for (int k = 0; k < F.nInterior; ++k) {
+                nextLevel.push_back(F.interior[k]);
+                nextW.push_back(childBase + (uint32_t)k);
+            }
+            out.nodes.resize((size_t)(childBase + F.nInterior) * WIDE_WORDS, 0u);
+            uint32_t* w = out.nodes.data() + (size_t)levelW[i] * WIDE_WORDS;
+            std::memcpy(w, F.words, sizeof F.words);
+            w[4] = childBase;
+            w[5] = itemBase;
+        }
+        level.swap(nextLevel);
+        levelW.swap(nextW);
     }
     out.depth = maxDepth;
     return true;
