@@ -92,6 +92,23 @@ struct Bins {
     }
 };
 
+// Items of a leaf range by instance slot, stable (equal slots keep their
+// order): insertion sort in place for the small ranges leaves have (a library
+// stable sort allocates a buffer per call), the library's above that.
+template <class It>
+void sort_by_slot(It first, It last, const uint32_t* itemSlot) {
+    if (last - first > 32) {
+        std::stable_sort(first, last, [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+        return;
+    }
+    for (It i = first + 1; i < last; ++i) {
+        const uint32_t x = *i;
+        It j = i;
+        for (; j > first && itemSlot[x] < itemSlot[*(j - 1)]; --j) *j = *(j - 1);
+        *j = x;
+    }
+}
+
 // Runs f(lo, hi, part) over `parts` contiguous pieces of [lo, hi) in parallel.
 template <class F> void parallel_ranges(uint32_t lo, uint32_t hi, int parts, F&& f) {
     if (parts <= 1) {
@@ -357,8 +374,7 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
     // leaves: items ordered by slot, so consecutive tests reuse the local ray
     for (size_t v = 0; v < B.N.count.size(); ++v) {
         if (B.N.count[v] < 2) continue;
-        std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
-                         [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+        sort_by_slot(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v], itemSlot);
     }
     out.items.resize(2 * (size_t)n);
     for (uint32_t k = 0; k < n; ++k) {
@@ -440,8 +456,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
     B.build(n);
     for (size_t v = 0; v < B.N.count.size(); ++v) {
         if (B.N.count[v] < 2) continue;
-        std::stable_sort(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v],
-                         [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+        sort_by_slot(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v], itemSlot);
     }
 
 #if SB_WIDE_COLLAPSE_SAH
@@ -655,8 +670,7 @@ bool build_wide(const float* boxes, const uint32_t* itemTri, const uint32_t* ite
                 // a leaf merged from an interior node: its items in slot order too (its
                 // range is its own; the parts of a node split across slots are not sorted)
                 if (!B.N.count[v] && cnt > 1)
-                    std::stable_sort(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + cnt,
-                                     [&](uint32_t a, uint32_t b) { return itemSlot[a] < itemSlot[b]; });
+                    sort_by_slot(B.order.begin() + sFirst[v], B.order.begin() + sFirst[v] + cnt, itemSlot);
                 meta[s] = (uint8_t)((((1u << cnt) - 1u) << 5) | itemOff);
                 F.leaf[F.nLeaf++] = v;
                 itemOff += cnt;
