@@ -310,7 +310,9 @@ def run_ours(args, dist: Dist):
         e2e_total += time.perf_counter() - t0
     e2e_ms = dist.max(e2e_total / K * 1e3)
     e2e_value = dist.world * rays / (e2e_ms * 1e-3) / 1e6
-    h2d = base_pos.shape[0] * 32 + len(movers) * (16 * 8 + 4)
+    # the deformer's positions (and normals, when the mesh has them) at 12 B per vertex each,
+    # and per moved instance its FP64 4x4 matrix and source index
+    h2d = base_pos.shape[0] * (12 if scene.meshes[dm].normals is None else 24) + len(movers) * (16 * 8 + 4)
     d2h = atl.array.nbytes + datl.array.nbytes
     scene.meshes[dm].positions = base_pos
 

@@ -450,6 +450,14 @@ sb_status sb_refit_blas_static(uint32_t* nodes, uint32_t nodeCount, const uint32
  * to carry the new root bounds into the TLAS, as the reference does. */
 sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCount,
                            const float* vertexData, uint32_t root, uint32_t end);
+/* The same lane from the mesh's own attribute arrays, as updateDeforms gathers
+ * them: positions (3 floats per vertex) and, when not NULL, normals (3 floats
+ * per vertex) replace the first six floats of each pooled vertex; the rest of
+ * the record (uv) keeps its build-time value, and so do the normals when NULL
+ * (spectral_scene.js:1866-1900). The arrays are copied before the call
+ * returns, so the caller may reuse them at once. */
+sb_status sb_update_deform_xyz(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCount,
+                               const float* positions, const float* normals, uint32_t root, uint32_t end);
 
 /* Per-source-instance transform table (computeDynamic inputs,
  * spectral_scene.js:1256-1298): column-major 4x4 world matrices in FP64

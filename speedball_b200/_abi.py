@@ -187,6 +187,7 @@ SIGNATURES = {
     "sb_refit_blas": (C.c_int, [_P, _U32, _U32]),
     "sb_refit_blas_static": (C.c_int, [_P, _U32, _P, _U32, _P, _U32, _U32, _U32, _P, C.c_char_p, C.c_size_t]),
     "sb_update_deform": (C.c_int, [_P, _U32, _U32, _P, _U32, _U32]),
+    "sb_update_deform_xyz": (C.c_int, [_P, _U32, _U32, _P, _P, _U32, _U32]),
     "sb_set_instances": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "sb_build_tlas": (C.c_int, [_P]),
     "sb_update_transforms": (C.c_int, [_P, _P, _P, _U32]),

@@ -80,6 +80,13 @@ struct sb_ctx {
     bool instancesSet = false;
     uint32_t* instOwner = nullptr;
     uint32_t* dStage = nullptr;   // staging for src lists
+    // sb_update_deform_xyz: page-locked and device staging of positions + normals,
+    // and the event after the copy that last read the page-locked buffer
+    float* hDeform = nullptr;
+    float* dDeform = nullptr;
+    size_t deformCap = 0;  // floats
+    cudaEvent_t evDeform = nullptr;
+    bool deformPending = false;
     double* dStageM = nullptr;    // staging for matrices
     size_t stageCap = 0;
 
@@ -526,6 +533,9 @@ void sb_destroy(sb_ctx* ctx) {
     if (ctx->evA) cudaEventDestroy(ctx->evA);
     if (ctx->evB) cudaEventDestroy(ctx->evB);
     if (ctx->evC) cudaEventDestroy(ctx->evC);
+    if (ctx->evDeform) cudaEventDestroy(ctx->evDeform);
+    if (ctx->hDeform) cudaFreeHost(ctx->hDeform);
+    if (ctx->dDeform) cudaFree(ctx->dDeform);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
     delete ctx;
@@ -2210,5 +2220,41 @@ extern "C" sb_status sb_update_deform(sb_ctx* ctx, uint32_t vertexStart, uint32_
     cudaSetDevice(ctx->device);
     CK(cudaMemcpyAsync(ctx->B.vertexData + (size_t)vertexStart * 8, vertexData, (size_t)vertexCount * 32,
                        cudaMemcpyHostToDevice, ctx->stream));
+    return sb_refit_blas(ctx, root, end);
+}
+
+extern "C" sb_status sb_update_deform_xyz(sb_ctx* ctx, uint32_t vertexStart, uint32_t vertexCount,
+                                          const float* positions, const float* normals, uint32_t root,
+                                          uint32_t end) {
+    if (!ctx || (vertexCount && !positions)) return fail(ctx, SB_ERR_INVALID_ARG, "null argument");
+    if (!ctx->sceneLoaded) return fail(ctx, SB_ERR_NOT_READY, "no scene uploaded");
+    if ((uint64_t)vertexStart + vertexCount > ctx->B.vertexCount)
+        return fail(ctx, SB_ERR_INVALID_ARG, "vertex range [%u,+%u) outside the pool", vertexStart, vertexCount);
+    ++ctx->epoch;
+    cudaSetDevice(ctx->device);
+    const size_t n = vertexCount, floats = n * (normals ? 6u : 3u);
+    // the previous call's copy must have read the page-locked buffer before it is refilled
+    if (ctx->deformPending) CK(cudaEventSynchronize(ctx->evDeform));
+    ctx->deformPending = false;
+    if (floats > ctx->deformCap) {
+        if (ctx->hDeform) cudaFreeHost(ctx->hDeform);
+        if (ctx->dDeform) cudaFree(ctx->dDeform);
+        ctx->hDeform = nullptr;
+        ctx->dDeform = nullptr;
+        ctx->deformCap = 0;
+        CK(cudaHostAlloc((void**)&ctx->hDeform, floats * sizeof(float), cudaHostAllocDefault));
+        CK(cudaMalloc((void**)&ctx->dDeform, floats * sizeof(float)));
+        ctx->deformCap = floats;
+    }
+    if (!ctx->evDeform) CK(cudaEventCreateWithFlags(&ctx->evDeform, cudaEventDisableTiming));
+    if (n) {
+        std::memcpy(ctx->hDeform, positions, n * 3 * sizeof(float));
+        if (normals) std::memcpy(ctx->hDeform + 3 * n, normals, n * 3 * sizeof(float));
+        CK(cudaMemcpyAsync(ctx->dDeform, ctx->hDeform, floats * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaEventRecord(ctx->evDeform, ctx->stream));
+        ctx->deformPending = true;
+        CK(launch_scatter_vertices(ctx->B.vertexData + (size_t)vertexStart * 8, ctx->dDeform,
+                                   normals ? ctx->dDeform + 3 * n : nullptr, vertexCount, ctx->stream));
+    }
     return sb_refit_blas(ctx, root, end);
 }

@@ -56,6 +56,10 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
                          cudaEvent_t afterPrimary = nullptr, cudaEvent_t afterShadow = nullptr,
                          cudaEvent_t afterClosest = nullptr);
 cudaError_t launch_blend_upload(const DevCascade& C, const DevParams& P, cudaStream_t st);
+// Positions (and normals when given), 3 floats per vertex, into the first six
+// floats of n pooled 8-float vertices.
+cudaError_t launch_scatter_vertices(float* vertexData8, const float* positions, const float* normals, uint32_t n,
+                                    cudaStream_t st);
 cudaError_t launch_glossy(const DevCascade& C, const DevParams& P, cudaStream_t st);
 cudaError_t launch_shade(const DevScene& S, const DevCascade& C, const DevParams& P, uint32_t slotCount,
                          cudaStream_t st);

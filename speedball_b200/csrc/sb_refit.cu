@@ -327,6 +327,28 @@ __global__ void __launch_bounds__(REFIT_SUB) k_refit_cta(uint32_t* nodes, const 
     }
 }
 
+__global__ void k_scatter_vertices(float* v8, const float* p3, const float* n3, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* v = v8 + 8u * (size_t)i;
+    v[0] = p3[3u * (size_t)i];
+    v[1] = p3[3u * (size_t)i + 1u];
+    v[2] = p3[3u * (size_t)i + 2u];
+    if (n3) {
+        v[3] = n3[3u * (size_t)i];
+        v[4] = n3[3u * (size_t)i + 1u];
+        v[5] = n3[3u * (size_t)i + 2u];
+    }
+}
+
+cudaError_t launch_scatter_vertices(float* vertexData8, const float* positions, const float* normals, uint32_t n,
+                                    cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_scatter_vertices<<<(n + 255) / 256, 256, 0, st>>>(vertexData8, positions, normals, n);
+    note_launch();
+    return cudaGetLastError();
+}
+
 cudaError_t launch_refit_blas(const SceneBuffers& B, uint32_t root, uint32_t end, uint32_t* err, uint32_t* gate,
                               cudaStream_t st, bool validated) {
     if (end <= root) return cudaSuccess;

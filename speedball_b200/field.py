@@ -160,7 +160,6 @@ class ProbeField:
         self._pendingMaterials: set[int] = set()
         self._pendingTopology = False
         self._deformVersions = {}
-        self._staging = {}
         self._extraCascades = {}  # extra cascade boxes (ci >= 1) configured by configureCascade
         self._params = _abi.default_params()
         self._params.hysteresis = self._hysteresis
@@ -494,18 +493,14 @@ class ProbeField:
             if m.positions.shape[0] != int(pool.vert_count[i]):
                 raise _abi.SbError(_abi.SB_ERR_LAYOUT_VIOLATION, f"mesh {i}: vertex count changed (topology edit)")
             self._deformVersions[i] = self._version(m)
-            stage = self._staging.get(i)
-            if stage is None or stage.array.shape[0] != m.positions.shape[0]:
-                stage = _abi.PinnedArray((m.positions.shape[0], 8), np.float32)
-                self._staging[i] = stage
-            vd = stage.array
-            vd[:, 0:3] = m.positions
-            if m.normals is not None:
-                vd[:, 3:6] = m.normals
-            if m.uvs is not None:
-                vd[:, 6:8] = m.uvs
-            self._ck(self._lib.sb_update_deform(self._ctx, int(pool.vert_base[i]), int(pool.vert_count[i]),
-                                                _abi.ptr(vd), int(pool.blas_root[i]), int(pool.blas_end[i])))
+            # positions, and normals when the mesh has them; uv keeps its build-time
+            # value (spectral_scene.js:1866-1900). The library copies both arrays
+            # before it returns.
+            pos = np.ascontiguousarray(m.positions, np.float32)
+            nrm = None if m.normals is None else np.ascontiguousarray(m.normals, np.float32)
+            self._ck(self._lib.sb_update_deform_xyz(self._ctx, int(pool.vert_base[i]), int(pool.vert_count[i]),
+                                                    _abi.ptr(pos), None if nrm is None else _abi.ptr(nrm),
+                                                    int(pool.blas_root[i]), int(pool.blas_end[i])))
             n += 1
         if n:
             if carryTlas:
@@ -716,9 +711,6 @@ class ProbeField:
         self._disposed = True
         self._lib.sb_destroy(self._ctx)
         self._ctx = None
-        for st in self._staging.values():
-            st.free()
-        self._staging.clear()
 
     def __del__(self):
         try:
