@@ -308,18 +308,19 @@ class ProbeField:
         if self._pendingTopology:
             self._pendingTopology = False
             self._rebuild()
+        # the dirty lanes first: their refits are the tick's first GPU work, and the
+        # solve planning below (host only) overlaps them
+        self._refresh_lanes()
         lst = self._solve_list()
         fallback = 1 if (not self._haveC1 or len(lst) == 2) else 2
         if 0 in lst:
             self._advance_epoch()
         solves = []
-        for n, ci in enumerate(lst):
+        for ci in lst:
             s = self._plan_solve(ci, nowMs, fallback)
             self._params.hysteresisExponent = s["hysteresisExponent"]
             self._params.hysteresis = self._hysteresis
             self._ck(self._lib.sb_set_params(self._ctx, C.byref(self._params)))
-            if n == 0:
-                self._refresh_lanes()
             self._ck(self._lib.sb_solve(self._ctx, ci, s["probeOffset"], s["updatedCount"]))
             self._commit_solve(s, nowMs)
             solves.append(s)
