@@ -89,3 +89,36 @@ def test_build_mode_argument_checked():
             f.setSceneBvhBuild("lazy")
     finally:
         f.dispose()
+
+
+def test_dispose_and_layout_change_while_building():
+    """A context destroyed while its background build runs waits for the build
+    and frees it; a layout change (bvhKind) during a build drops it, and the
+    next tick builds the new layout's trees."""
+    import ctypes as C
+    s = synth.atrium(1)
+    f = gu.make_field(s, sceneBvhBuild="background")
+    f.tick(nowMs=100.0)
+    assert f.getStats()["sceneBvhBuilding"]
+    f.dispose()  # joins the build thread
+
+    f = gu.make_field(s, sceneBvhBuild="background")
+    try:
+        f.tick(nowMs=100.0)
+        assert f.getStats()["sceneBvhBuilding"]
+        from speedball_b200 import _abi
+        t = _abi.sb_tuning()
+        _abi.check(f._lib.sb_get_tuning(f.ctx, C.byref(t)), f.ctx)
+        t.bvhKind = 2  # binary only: a structural change for the scene BVH
+        _abi.check(f._lib.sb_set_tuning(f.ctx, C.byref(t)), f.ctx)
+        f.finishSceneBvh()  # the build of the 8-wide layout is dropped
+        st = f.getStats()
+        assert not st["sceneBvhActive"] and st["sceneBvhBuilds"] == 0, st
+        f.tick(nowMs=116.0)  # starts the binary-only build
+        f.finishSceneBvh()
+        f.tick(nowMs=132.0)
+        f.synchronize()
+        st = f.getStats()
+        assert st["sceneBvhActive"] and st["sceneBvhBuilds"] == 1, st
+    finally:
+        f.dispose()
