@@ -274,6 +274,7 @@ cudaError_t FlatScene::install(Job& j, cudaStream_t st, std::string& why) {
         if (e != cudaSuccess) return e;
         wideReady = true;
         wideCount = (uint32_t)(j.wt.nodes.size() / flat::WIDE_WORDS);
+        wideDepth = j.wt.depth;
     }
     root = j.tree.root;
     depth = j.tree.depth;
@@ -388,6 +389,7 @@ void FlatScene::fill(DevScene& S) const {
     S.wideNodes = on && wide && wideReady ? wnodes : nullptr;
     S.wideItems = on && wide && wideReady ? witems : nullptr;
     S.wideNodeCount = on && wide && wideReady ? wideCount : 0u;
+    S.wideDepth = on && wide && wideReady ? wideDepth : 0u;
     S.flatRoot = on ? root : flat::ENTRY_NONE;
     S.slotSkip = on ? dSkip : nullptr;
     S.dynList = on ? dDyn : nullptr;

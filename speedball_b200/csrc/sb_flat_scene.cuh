@@ -43,7 +43,7 @@ struct FlatScene {
     size_t skipCap = 0;
     uint32_t* dDyn = nullptr;
     size_t dynCap = 0;
-    uint32_t root = flat::ENTRY_NONE, depth = 0, itemCount = 0, wideCount = 0;
+    uint32_t root = flat::ENTRY_NONE, depth = 0, itemCount = 0, wideCount = 0, wideDepth = 0;
     std::vector<uint8_t> skip;        // per slot
     std::vector<uint32_t> dyn;        // slots walked through their BLAS
     std::vector<uint32_t> slotRoot, slotEnd, srcToSlot;

@@ -84,6 +84,7 @@ struct DevScene {
     const float* slotBounds;   // world AABB per slot (the TLAS leaf bounds), or null
     uint32_t flatRoot, dynCount;
     uint32_t wideNodeCount;    // nodes of the 8-wide tree (0 when it is not built)
+    uint32_t wideDepth;        // its depth (levels below the root)
     int32_t flatOn;
     uint32_t nodeCount, triCount, instCount, tlasNodeCount, materialCount;
     uint32_t lightCount;
@@ -176,6 +177,7 @@ struct WaveCtx {
     uint32_t smemTlas;             // TLAS nodes staged in shared memory (0 = read from global)
     uint32_t order;                // 0 probe-major, 1 direction-major
     uint32_t smemWide;             // top 8-wide nodes staged in shared memory by the closest-hit stage
+    uint32_t sstk;                 // closest-hit walk stack entries per thread in shared memory (0: local)
 };
 
 // Several solves (scenes, cascades) through one launch of each stage: a

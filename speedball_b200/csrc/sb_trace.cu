@@ -28,6 +28,12 @@ namespace sb {
 #ifndef SB_SHADOW_MIN_BLOCKS
 #define SB_SHADOW_MIN_BLOCKS 4
 #endif
+// Group-stack entries per thread held in shared memory by the closest-hit
+// stage's 8-wide walk (8 bytes each, one [entry][thread] array per CTA) when
+// the tree's depth fits; 0, or a deeper tree: the stack in local memory.
+#ifndef SB_SMEM_STACK
+#define SB_SMEM_STACK 16
+#endif
 
 // ---------------------------------------------------------------- bodies
 // Each stage's per-item work is a device function over `const WaveCtx&`; the
@@ -73,8 +79,11 @@ __device__ __forceinline__ void primary_ray(const WaveCtx& W, const uint4* tl, b
 // the next round, so the lanes keep working instead of waiting for the slowest
 // ray of a fixed 32-ray batch. One atomicAdd per round fetches rays for all
 // the warp's idle lanes. Returns the rays traced.
+//
+// sStack: this thread's column of the walk stack in shared memory (W.sstk
+// entries), or null for the stack in local memory.
 __device__ __forceinline__ uint32_t primary_refill(const WaveCtx& W, uint32_t total, Visits& vis, const uint4* sWide,
-                                                   uint32_t nWide) {
+                                                   uint32_t nWide, uint2* sStack = nullptr) {
     const DevCascade& C = W.C;
     const uint32_t lane = threadIdx.x & 31u;
     WideWalk w;
@@ -107,7 +116,8 @@ __device__ __forceinline__ uint32_t primary_refill(const WaveCtx& W, uint32_t to
             if (!more) break;
             continue;
         }
-        if (has && wide_step<false>(W.S, w, bestT, tri, inst, bu, bv, vis, W.err, sWide, nWide)) {
+        if (has && wide_step<false>(W.S, w, bestT, tri, inst, bu, bv, vis, W.err, sWide, nWide, sStack,
+                                    (int)W.sstk)) {
             wide_end<false>(W.S, w, bestT, tri, inst, bu, bv, vis, W.err);
             write_hit(C, slot, k, tri, inst, bestT, bu, bv);
             ++nRays;
@@ -280,7 +290,9 @@ __global__ void __launch_bounds__(256, SB_PRIMARY_MIN_BLOCKS) k_trace_primary(Wa
     Visits vis = {0, 0, 0, 0};
     uint32_t nRays = 0;
     if (SB_PRIMARY_REFILL && W.S.wideNodes) {
-        nRays = primary_refill(W, total, vis, sTlas, nWide);
+        // the walk stack after the staged nodes, one column per thread
+        uint2* sStack = W.sstk ? reinterpret_cast<uint2*>(sTlas + 5u * nWide) + threadIdx.x : nullptr;
+        nRays = primary_refill(W, total, vis, sTlas, nWide, sStack);
         add_visits(W.counters, 2, nRays, vis);
         return;
     }
@@ -446,6 +458,10 @@ cudaError_t launch_trace(const DevScene& S, const DevCascade& C, const DevParams
     W.smemWide = wideNodes;
     size_t smem = (size_t)smemNodes * 64u;  // room for the child-pair TLAS (the 32-byte nodes need half)
     size_t smemPrimary = smem > (size_t)wideNodes * 80u ? smem : (size_t)wideNodes * 80u;
+    // the walk stack in shared memory when the 8-wide tree's depth fits it (the
+    // stack holds at most one group per level below the root)
+    W.sstk = (SB_PRIMARY_REFILL && S.wideNodes && S.wideDepth + 1u <= (uint32_t)SB_SMEM_STACK) ? SB_SMEM_STACK : 0u;
+    smemPrimary += (size_t)W.sstk * (size_t)tune.block * 8u;
     if (smemPrimary > 48u * 1024u)
         cudaFuncSetAttribute(k_trace_primary, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smemPrimary);
     if (smem > 48u * 1024u)

@@ -1002,10 +1002,16 @@ __device__ __forceinline__ bool wide_end(const DevScene& S, const WideWalk& w, f
 // One round: nodes until this lane holds items to test (or has nothing left),
 // then those items. Returns 0 to go on, 1 when the tree is done (or a capacity
 // / watchdog error ended it), 2 on an any hit.
+//
+// sStack, when given, holds the group stack in shared memory instead: this
+// thread's column of a [entry][thread] array (entry e at sStack[e * blockDim.x],
+// so the lanes of a warp use distinct banks whatever their stack depths), with
+// room for sDepth entries.
 template <bool ANY>
 __device__ __forceinline__ int wide_step(const DevScene& S, WideWalk& w, float& tmax, int& bestTri, int& bestInst,
                                          float& bu, float& bv, Visits& vis, uint32_t* err,
-                                         const uint4* sWide = nullptr, uint32_t nWide = 0) {
+                                         const uint4* sWide = nullptr, uint32_t nWide = 0, uint2* sStack = nullptr,
+                                         int sDepth = 0) {
     uint32_t tBase = 0, tBits = 0;
     for (;;) {
         if (w.node == FLAT_NONE) {
@@ -1015,17 +1021,20 @@ __device__ __forceinline__ int wide_step(const DevScene& S, WideWalk& w, float& 
                 const uint32_t slot = key ^ w.oct;
                 w.node = w.gBase + __popc((w.gBits >> 16) & 0xFFu & ((1u << slot) - 1u));
                 if (w.gBits >> 24) {
-                    if (w.sp >= SB_STACK) {  // unreachable: the tree's depth was checked on build
+                    if (w.sp >= (sStack ? sDepth : SB_STACK)) {  // unreachable: the depth was checked
                         latch(err, ERR_CAPACITY);
                         return 1;
                     }
-                    w.stk[w.sp++] = make_uint2(w.gBase, w.gBits);
+                    if (sStack) sStack[(uint32_t)w.sp * blockDim.x] = make_uint2(w.gBase, w.gBits);
+                    else w.stk[w.sp] = make_uint2(w.gBase, w.gBits);
+                    ++w.sp;
                 }
                 w.gBits = 0;
             } else if (w.sp > 0) {
                 --w.sp;
-                w.gBase = w.stk[w.sp].x;
-                w.gBits = w.stk[w.sp].y;
+                const uint2 e = sStack ? sStack[(uint32_t)w.sp * blockDim.x] : w.stk[w.sp];
+                w.gBase = e.x;
+                w.gBits = e.y;
                 continue;
             } else {
                 return 1;
