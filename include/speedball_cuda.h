@@ -635,7 +635,8 @@ sb_status sb_rebuild_scene_bvh(sb_ctx* ctx);
  * the reference's two-level walk (GPU-refit TLAS + BLASes), and the first trace
  * after the build finished installs the tree, marking the slots that moved or
  * were refit since it read the scene. A build overtaken by another structural
- * change is dropped and the next trace starts a new one. The scene-BVH walks
+ * change is dropped and the next trace starts a new one. Back in BLOCKING mode,
+ * the next trace waits for a build still running. The scene-BVH walks
  * and the two-level walk agree on hit IDs up to near-ties (the parity bar), so
  * a solve's results do not depend on which one answered beyond that. */
 enum { SB_SCENE_BVH_BLOCKING = 0, SB_SCENE_BVH_BACKGROUND = 1 };

@@ -309,7 +309,9 @@ cudaError_t FlatScene::prepare(const SceneBuffers& B, const uint32_t* order, uin
         ready = false;
         return cudaSuccess;
     }
-    if (job && job->done.load(std::memory_order_acquire)) {
+    // a finished build is installed; in blocking mode (switched back while a
+    // build ran) the trace waits for it
+    if (job && (!background || job->done.load(std::memory_order_acquire))) {
         cudaError_t e = finish(st, why);
         if (e != cudaSuccess) return e;
     }

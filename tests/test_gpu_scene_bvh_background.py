@@ -122,3 +122,20 @@ def test_dispose_and_layout_change_while_building():
         assert st["sceneBvhActive"] and st["sceneBvhBuilds"] == 1, st
     finally:
         f.dispose()
+
+
+def test_blocking_mode_waits_for_a_running_build():
+    """Switched back to blocking mode while a background build runs: the next
+    tick waits for that build and traces with the new tree."""
+    s = synth.atrium(1)
+    f = gu.make_field(s, sceneBvhBuild="background")
+    try:
+        f.tick(nowMs=100.0)
+        assert f.getStats()["sceneBvhBuilding"]
+        f.setSceneBvhBuild("blocking")
+        f.tick(nowMs=116.0)
+        f.synchronize()
+        st = f.getStats()
+        assert st["sceneBvhActive"] and not st["sceneBvhBuilding"] and st["sceneBvhBuilds"] == 1, st
+    finally:
+        f.dispose()
