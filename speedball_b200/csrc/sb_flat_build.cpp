@@ -174,6 +174,40 @@ struct Builder {
         }
     }
 
+    // Stable partition of [lo, hi) by `left` over `parts` threads: each piece
+    // counts its left items, then every piece scatters its items to their
+    // places in a scratch copy, which goes back in place. Returns the split.
+    std::vector<Prim> scratch;
+    template <class Pred>
+    uint32_t partition_parallel(uint32_t lo, uint32_t hi, int parts, Pred&& left) {
+        std::vector<uint32_t> nl(parts), at(parts), ar(parts);
+        parallel_ranges(lo, hi, parts, [&](uint32_t a, uint32_t b, int p) {
+            uint32_t c = 0;
+            for (uint32_t k = a; k < b; ++k) c += left(prims[k]) ? 1u : 0u;
+            nl[p] = c;
+        });
+        uint32_t totalL = 0;
+        for (int p = 0; p < parts; ++p) totalL += nl[p];
+        uint32_t l = 0, r = totalL;
+        for (int p = 0; p < parts; ++p) {
+            const uint32_t a = lo + (uint32_t)((uint64_t)(hi - lo) * p / parts);
+            const uint32_t b = lo + (uint32_t)((uint64_t)(hi - lo) * (p + 1) / parts);
+            at[p] = l;
+            ar[p] = r;
+            l += nl[p];
+            r += (b - a) - nl[p];
+        }
+        if (scratch.size() < hi - lo) scratch.resize(hi - lo);
+        parallel_ranges(lo, hi, parts, [&](uint32_t a, uint32_t b, int p) {
+            uint32_t il = at[p], ir = ar[p];
+            for (uint32_t k = a; k < b; ++k) scratch[left(prims[k]) ? il++ : ir++] = prims[k];
+        });
+        parallel_ranges(lo, hi, parts, [&](uint32_t a, uint32_t b, int) {
+            std::memcpy(&prims[a], &scratch[a - lo], (size_t)(b - a) * sizeof(Prim));
+        });
+        return lo + totalL;
+    }
+
     // Splits [lo, hi) by binned SAH over all three axes at once; returns the
     // split point, or hi for a leaf. `nb` receives the node box.
     uint32_t split(uint32_t lo, uint32_t hi, Box& nb, int parts) {
@@ -238,9 +272,13 @@ struct Builder {
         if (n <= maxLeaf && (bestAxis < 0 || best + nb.area() >= leafCost)) return hi;
         uint32_t mid = lo + n / 2;
         if (bestAxis >= 0) {
-            auto it = std::partition(prims.begin() + lo, prims.begin() + hi,
-                                     [&](const Prim& q) { return bin_of(q, bestAxis) < bestBin; });
-            mid = (uint32_t)(it - prims.begin());
+            auto left = [&](const Prim& q) { return bin_of(q, bestAxis) < bestBin; };
+            if (parts > 1) {
+                mid = partition_parallel(lo, hi, parts, left);
+            } else {
+                auto it = std::partition(prims.begin() + lo, prims.begin() + hi, left);
+                mid = (uint32_t)(it - prims.begin());
+            }
         }
         if (mid == lo || mid == hi) mid = lo + n / 2;  // coincident centroids: split by index
         return mid;
@@ -370,17 +408,24 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
     Builder B;
     B.init(boxes, n);
     B.build(n);
+    // the passes below touch every node or item once, independently: split over threads
+    const int parts = n >= 65536 ? (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency())) : 1;
 
     // leaves: items ordered by slot, so consecutive tests reuse the local ray
-    for (size_t v = 0; v < B.N.count.size(); ++v) {
-        if (B.N.count[v] < 2) continue;
-        sort_by_slot(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v], itemSlot);
-    }
+    // (leaf ranges are disjoint)
+    parallel_ranges(0, (uint32_t)B.N.count.size(), parts, [&](uint32_t a, uint32_t b, int) {
+        for (uint32_t v = a; v < b; ++v) {
+            if (B.N.count[v] < 2) continue;
+            sort_by_slot(B.order.begin() + B.N.first[v], B.order.begin() + B.N.first[v] + B.N.count[v], itemSlot);
+        }
+    });
     out.items.resize(2 * (size_t)n);
-    for (uint32_t k = 0; k < n; ++k) {
-        out.items[2 * (size_t)k] = itemTri[B.order[k]];
-        out.items[2 * (size_t)k + 1] = itemSlot[B.order[k]];
-    }
+    parallel_ranges(0, n, parts, [&](uint32_t a, uint32_t b, int) {
+        for (uint32_t k = a; k < b; ++k) {
+            out.items[2 * (size_t)k] = itemTri[B.order[k]];
+            out.items[2 * (size_t)k + 1] = itemSlot[B.order[k]];
+        }
+    });
 
     // pair nodes: one per interior tree node, numbered in pre-order
     const size_t total = B.N.box.size();
@@ -405,7 +450,8 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
         return ENTRY_LEAF | (B.N.count[v] << 24) | B.N.first[v];
     };
     out.nodes.assign(16 * (size_t)pairs, 0u);
-    for (size_t v = 0; v < total; ++v) {
+    parallel_ranges(0, (uint32_t)total, parts, [&](uint32_t a0, uint32_t b0, int) {
+      for (uint32_t v = a0; v < b0; ++v) {
         if (B.N.count[v]) continue;
         uint32_t* q = out.nodes.data() + 16 * (size_t)pairIndex[v];
         const Box& a = B.N.box[B.N.left[v]];
@@ -415,7 +461,8 @@ bool build(const float* boxes, const uint32_t* itemTri, const uint32_t* itemSlot
         q[8] = fbits(a.lo[2]); q[9] = fbits(a.hi[2]); q[10] = fbits(b.lo[2]); q[11] = fbits(b.hi[2]);
         q[12] = entry(B.N.left[v]);
         q[13] = entry(B.N.right[v]);
-    }
+      }
+    });
     out.root = entry(0);
     out.depth = maxDepth;
     std::memcpy(out.rootBox, B.N.box[0].lo, 12);
